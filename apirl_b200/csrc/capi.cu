@@ -1,0 +1,381 @@
+// The C ABI declared in include/apirl_b200.h: projector objects, argument
+// checks, error reporting, and the MLEM / OSEM drivers.
+#include <cuda_runtime.h>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+#include "internal.h"
+#include "../../include/apirl_b200.h"
+
+using apirl::HostTables;
+using apirl::ImgGeom;
+using apirl::LorTable;
+using apirl::SubsetSel;
+
+namespace {
+
+thread_local std::string g_err;
+
+}  // namespace
+
+apirl_status apirl_internal_fail(apirl_status code, const char* msg) {
+  g_err = msg;
+  return code;
+}
+
+namespace {
+
+apirl_status fail(apirl_status code, const char* fmt, ...) {
+  char buf[512];
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(buf, sizeof buf, fmt, ap);
+  va_end(ap);
+  g_err = buf;
+  return code;
+}
+
+apirl_status cuda_fail(cudaError_t e, const char* what) {
+  if (e == cudaErrorMemoryAllocation) return fail(APIRL_ERR_OOM, "%s: %s", what, cudaGetErrorString(e));
+  return fail(APIRL_ERR_CUDA, "%s: %s", what, cudaGetErrorString(e));
+}
+
+#define CK(call)                                                  \
+  do {                                                            \
+    cudaError_t e_ = (call);                                      \
+    if (e_ != cudaSuccess) return cuda_fail(e_, #call);           \
+  } while (0)
+
+// Makes `dev` current for the scope and restores the caller's device after.
+struct DeviceScope {
+  int prev = -1;
+  cudaError_t err = cudaSuccess;
+  explicit DeviceScope(int dev) {
+    if (cudaGetDevice(&prev) != cudaSuccess) prev = -1;
+    if (prev != dev) err = cudaSetDevice(dev);
+  }
+  ~DeviceScope() {
+    int cur = -1;
+    if (prev >= 0 && cudaGetDevice(&cur) == cudaSuccess && cur != prev) cudaSetDevice(prev);
+  }
+};
+
+#define DEVICE_SCOPE(dev)                                                   \
+  DeviceScope scope_(dev);                                                  \
+  if (scope_.err != cudaSuccess) return cuda_fail(scope_.err, "cudaSetDevice")
+
+bool valid_img(const apirl_image_geom* g) {
+  return g && g->nx > 0 && g->ny > 0 && g->nz > 0 && g->dx > 0 && g->dy > 0 && g->dz > 0 &&
+         (int64_t)g->nx * g->ny * g->nz < (int64_t)1 << 31;
+}
+
+// Bounds the length of every Siddon walk: a LOR spans at most the scanner
+// diameter, so it records at most about 2 R / d segments per axis.  Geometries
+// that would give walks of more than ~1e5 segments per axis are rejected.
+bool walk_bounded(const apirl_image_geom* g, float r_scanner, float axial) {
+  const float d = fminf(g->dx, fminf(g->dy, g->dz));
+  const float span = fmaxf(2.f * r_scanner, axial);
+  return span / d < 1.0e5f && (float)g->nx * g->dx < 1.0e6f && (float)g->nz * g->dz < 1.0e6f;
+}
+
+SubsetSel make_subset(const apirl_projector* p, int subset, int nsub) {
+  SubsetSel s;
+  s.subset = subset < 0 ? -1 : subset;
+  s.nsub = subset < 0 ? 1 : nsub;
+  s.nk = apirl::subset_nproj(p->t.n_proj, s.subset, s.nsub);
+  return s;
+}
+
+apirl_status check_subset(const apirl_projector* p, int subset, int nsub) {
+  if (!p) return fail(APIRL_ERR_INVALID, "null projector");
+  if (subset >= 0 && (nsub <= 0 || subset >= nsub || nsub > p->t.n_proj))
+    return fail(APIRL_ERR_INVALID, "subset %d of %d is out of range (%d angles)", subset, nsub, p->t.n_proj);
+  return APIRL_OK;
+}
+
+apirl_status finish_create(apirl_projector* p, apirl_projector** out) {
+  const size_t nl = p->host.lor.size() / 4;
+  CK(cudaMalloc(&p->d_lor, nl * sizeof(float4)));
+  CK(cudaMemcpy(p->d_lor, p->host.lor.data(), nl * sizeof(float4), cudaMemcpyHostToDevice));
+  CK(cudaMalloc(&p->d_z, p->host.z.size() / 2 * sizeof(float2)));
+  CK(cudaMemcpy(p->d_z, p->host.z.data(), p->host.z.size() * sizeof(float), cudaMemcpyHostToDevice));
+  CK(cudaMalloc(&p->d_ok, p->host.ok.size()));
+  CK(cudaMemcpy(p->d_ok, p->host.ok.data(), p->host.ok.size(), cudaMemcpyHostToDevice));
+  p->t.lor = p->d_lor;
+  p->t.z = p->d_z;
+  p->t.ok = p->d_ok;
+  SubsetSel all = make_subset(p, -1, 1);
+  p->n_partials = apirl::em_pass_blocks(p->t, all);
+  const int64_t lb = apirl::likelihood_blocks((int64_t)p->t.n_sinos * p->t.n_proj * p->t.n_r);
+  if (lb > p->n_partials) p->n_partials = lb;
+  CK(cudaMalloc(&p->d_partials, p->n_partials * sizeof(double)));
+  CK(cudaMalloc(&p->d_minmax, 2 * sizeof(unsigned)));
+  CK(cudaMalloc(&p->d_scalars, 8 * sizeof(double)));
+  *out = p;
+  return APIRL_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+const char* apirl_last_error(void) { return g_err.c_str(); }
+const char* apirl_version(void) { return "apirl_b200 0.1 (sm_100a)"; }
+
+apirl_status apirl_lor_table(int n_proj, int n_r, float r_fov, float r_scanner, float* h_lor) {
+  if (n_proj <= 0 || n_r <= 0 || !h_lor || !(r_scanner > r_fov)) return fail(APIRL_ERR_INVALID, "bad arguments");
+  HostTables t;
+  apirl::build_tables_2d(n_proj, n_r, r_fov, r_scanner, t);
+  memcpy(h_lor, t.lor.data(), t.lor.size() * sizeof(float));
+  return APIRL_OK;
+}
+
+int apirl_sino3d_ring_z(const apirl_sino3d_geom* sino, float* h_z) {
+  if (!sino || sino->n_rings <= 0 || sino->n_segments <= 0 || !sino->min_ring_diff || !sino->max_ring_diff) {
+    fail(APIRL_ERR_INVALID, "invalid 3D sinogram geometry");
+    return -1;
+  }
+  HostTables t;
+  if (!apirl::build_tables_3d(1, 1, sino->n_rings, 1.f, sino->axial_fov, 2.f, sino->n_segments,
+                              sino->min_ring_diff, sino->max_ring_diff, t))
+    return 0;
+  if (h_z) memcpy(h_z, t.z.data(), t.z.size() * sizeof(float));
+  return t.n_sinos;
+}
+
+apirl_status apirl_projector_create_2d(const apirl_image_geom* img, const apirl_sino2d_geom* sino, int device,
+                                       apirl_projector** out) {
+  if (!out) return fail(APIRL_ERR_INVALID, "null output pointer");
+  *out = nullptr;
+  if (!valid_img(img)) return fail(APIRL_ERR_INVALID, "invalid image geometry");
+  if (!sino || sino->n_proj <= 0 || sino->n_r <= 0 || !(sino->r_fov > 0) || !(sino->r_scanner > sino->r_fov))
+    return fail(APIRL_ERR_INVALID, "invalid 2D sinogram geometry (need n_proj, n_r > 0 and 0 < r_fov < r_scanner)");
+  if (!walk_bounded(img, sino->r_scanner, 0.f))
+    return fail(APIRL_ERR_INVALID, "voxels too small for the scanner radius (walks above 1e5 segments)");
+  DEVICE_SCOPE(device);
+  apirl_projector* p = new apirl_projector;
+  p->device = device;
+  p->is3d = 0;
+  p->g = apirl::make_img_geom(img->nx, img->ny, img->nz, img->dx, img->dy, img->dz);
+  apirl::build_tables_2d(sino->n_proj, sino->n_r, sino->r_fov, sino->r_scanner, p->host);
+  p->t.n_proj = sino->n_proj;
+  p->t.n_r = sino->n_r;
+  p->t.n_sinos = 1;
+  p->t.is3d = 0;
+  apirl_status st = finish_create(p, out);
+  if (st != APIRL_OK) { std::string m = g_err; apirl_projector_destroy(p); g_err = m; }
+  return st;
+}
+
+apirl_status apirl_projector_create_3d(const apirl_image_geom* img, const apirl_sino3d_geom* sino, int device,
+                                       apirl_projector** out) {
+  if (!out) return fail(APIRL_ERR_INVALID, "null output pointer");
+  *out = nullptr;
+  if (!valid_img(img)) return fail(APIRL_ERR_INVALID, "invalid image geometry");
+  if (!sino || sino->n_proj <= 0 || sino->n_r <= 0 || sino->n_rings <= 0 || sino->n_segments <= 0 ||
+      !sino->min_ring_diff || !sino->max_ring_diff || !(sino->r_fov > 0) || !(sino->axial_fov > 0) ||
+      !(sino->r_scanner > sino->r_fov))
+    return fail(APIRL_ERR_INVALID, "invalid 3D sinogram geometry");
+  if (!walk_bounded(img, sino->r_scanner, sino->axial_fov))
+    return fail(APIRL_ERR_INVALID, "voxels too small for the scanner size (walks above 1e5 segments)");
+  for (int i = 0; i < sino->n_segments; i++)
+    if (sino->min_ring_diff[i] > sino->max_ring_diff[i])
+      return fail(APIRL_ERR_INVALID, "segment %d: minimum ring difference above maximum", i);
+  DEVICE_SCOPE(device);
+  apirl_projector* p = new apirl_projector;
+  p->device = device;
+  p->is3d = 1;
+  p->g = apirl::make_img_geom(img->nx, img->ny, img->nz, img->dx, img->dy, img->dz);
+  if (!apirl::build_tables_3d(sino->n_proj, sino->n_r, sino->n_rings, sino->r_fov, sino->axial_fov,
+                              sino->r_scanner, sino->n_segments, sino->min_ring_diff, sino->max_ring_diff,
+                              p->host)) {
+    delete p;
+    return fail(APIRL_ERR_INVALID, "segment table yields no sinograms");
+  }
+  p->t.n_proj = sino->n_proj;
+  p->t.n_r = sino->n_r;
+  p->t.n_sinos = p->host.n_sinos;
+  p->t.is3d = 1;
+  if ((int64_t)p->t.n_sinos * p->t.n_proj * p->t.n_r >= ((int64_t)1 << 40)) {
+    delete p;
+    return fail(APIRL_ERR_INVALID, "sinogram too large");
+  }
+  apirl_status st = finish_create(p, out);
+  if (st != APIRL_OK) { std::string m = g_err; apirl_projector_destroy(p); g_err = m; }
+  return st;
+}
+
+void apirl_projector_destroy(apirl_projector* p) {
+  if (!p) return;
+  DeviceScope scope(p->device);
+  cudaFree(p->d_lor);
+  cudaFree(p->d_z);
+  cudaFree(p->d_ok);
+  cudaFree(p->d_partials);
+  cudaFree(p->d_minmax);
+  cudaFree(p->d_scalars);
+  delete p;
+}
+
+int64_t apirl_projector_num_bins(const apirl_projector* p, int subset, int nsubsets) {
+  if (!p || (subset >= 0 && (nsubsets <= 0 || subset >= nsubsets))) return -1;
+  SubsetSel s = make_subset(p, subset, nsubsets);
+  return (int64_t)p->t.n_sinos * s.nk * p->t.n_r;
+}
+
+int apirl_projector_num_sinograms(const apirl_projector* p) { return p ? p->t.n_sinos : -1; }
+
+apirl_status apirl_projector_tables(const apirl_projector* p, float* h_lor, float* h_z) {
+  if (!p) return fail(APIRL_ERR_INVALID, "null projector");
+  if (h_lor) memcpy(h_lor, p->host.lor.data(), p->host.lor.size() * sizeof(float));
+  if (h_z && p->is3d) memcpy(h_z, p->host.z.data(), p->host.z.size() * sizeof(float));
+  return APIRL_OK;
+}
+
+apirl_status apirl_count_steps(apirl_projector* p, int subset, int nsubsets, int32_t* d_steps, void* stream) {
+  apirl_status st = check_subset(p, subset, nsubsets);
+  if (st) return st;
+  if (!d_steps) return fail(APIRL_ERR_INVALID, "null output");
+  DEVICE_SCOPE(p->device);
+  CK(apirl::launch_count_steps(p->g, p->t, make_subset(p, subset, nsubsets), d_steps, (cudaStream_t)stream));
+  return APIRL_OK;
+}
+
+apirl_status apirl_project(apirl_projector* p, const float* d_image, float* d_sino, int subset, int nsubsets,
+                           void* stream) {
+  apirl_status st = check_subset(p, subset, nsubsets);
+  if (st) return st;
+  if (!d_image || !d_sino) return fail(APIRL_ERR_INVALID, "null image or sinogram");
+  DEVICE_SCOPE(p->device);
+  CK(apirl::launch_project(p->g, p->t, make_subset(p, subset, nsubsets), d_image, d_sino, (cudaStream_t)stream));
+  return APIRL_OK;
+}
+
+apirl_status apirl_backproject(apirl_projector* p, const float* d_sino, float* d_image, int subset, int nsubsets,
+                               void* stream) {
+  apirl_status st = check_subset(p, subset, nsubsets);
+  if (st) return st;
+  if (!d_image || !d_sino) return fail(APIRL_ERR_INVALID, "null image or sinogram");
+  DEVICE_SCOPE(p->device);
+  CK(apirl::launch_backproject(p->g, p->t, make_subset(p, subset, nsubsets), d_sino, 0, nullptr, 0, d_image,
+                               (cudaStream_t)stream));
+  return APIRL_OK;
+}
+
+apirl_status apirl_divide_and_backproject(apirl_projector* p, const float* d_meas, const float* d_est,
+                                          float* d_image, int subset, int nsubsets, void* stream) {
+  apirl_status st = check_subset(p, subset, nsubsets);
+  if (st) return st;
+  if (!d_image || !d_meas || !d_est) return fail(APIRL_ERR_INVALID, "null image or sinogram");
+  DEVICE_SCOPE(p->device);
+  CK(apirl::launch_backproject(p->g, p->t, make_subset(p, subset, nsubsets), d_meas, 0, d_est, 1, d_image,
+                               (cudaStream_t)stream));
+  return APIRL_OK;
+}
+
+apirl_status apirl_inverse_divide(int64_t n, const float* d_meas, float* d_est, void* stream) {
+  if (n < 0 || (n > 0 && (!d_meas || !d_est))) return fail(APIRL_ERR_INVALID, "bad arguments");
+  CK(apirl::launch_inverse_divide(n, d_meas, d_est, (cudaStream_t)stream));
+  return APIRL_OK;
+}
+
+apirl_status apirl_add_bins(int64_t n, const float* d_add, float* d_est, void* stream) {
+  if (n < 0 || (n > 0 && (!d_add || !d_est))) return fail(APIRL_ERR_INVALID, "bad arguments");
+  CK(apirl::launch_add_bins(n, d_add, d_est, (cudaStream_t)stream));
+  return APIRL_OK;
+}
+
+apirl_status apirl_likelihood(int64_t n, const float* d_est, const float* d_meas, int gt0, double* d_out,
+                              void* stream) {
+  if (n <= 0 || !d_est || !d_meas || !d_out) return fail(APIRL_ERR_INVALID, "bad arguments");
+  // The per-block partials live in a small allocation owned by this call path.
+  const int64_t nb = apirl::likelihood_blocks(n);
+  double* part = nullptr;
+  CK(cudaMallocAsync(&part, nb * sizeof(double), (cudaStream_t)stream));
+  cudaError_t e = apirl::launch_likelihood(n, d_est, d_meas, gt0, part, nb, d_out, (cudaStream_t)stream);
+  cudaFreeAsync(part, (cudaStream_t)stream);
+  CK(e);
+  return APIRL_OK;
+}
+
+apirl_status apirl_mlem_threshold(int64_t n, const float* d_sens, float* d_thr, void* stream) {
+  if (n <= 0 || !d_sens || !d_thr) return fail(APIRL_ERR_INVALID, "bad arguments");
+  unsigned* mm = nullptr;
+  CK(cudaMallocAsync(&mm, 2 * sizeof(unsigned), (cudaStream_t)stream));
+  cudaError_t e = apirl::launch_threshold(n, d_sens, mm, d_thr, (cudaStream_t)stream);
+  cudaFreeAsync(mm, (cudaStream_t)stream);
+  CK(e);
+  return APIRL_OK;
+}
+
+apirl_status apirl_update_pixels(int64_t n, float* d_x, float* d_bp, const float* d_sens, const float* d_thr,
+                                 float thr_value, int ge, int zero_bp, void* stream) {
+  if (n < 0 || (n > 0 && (!d_x || !d_bp || !d_sens))) return fail(APIRL_ERR_INVALID, "bad arguments");
+  CK(apirl::launch_update(n, d_x, d_bp, d_sens, d_thr, thr_value, ge, zero_bp, (cudaStream_t)stream));
+  return APIRL_OK;
+}
+
+apirl_status apirl_force_positive(int64_t n, float* d_x, void* stream) {
+  if (n < 0 || (n > 0 && !d_x)) return fail(APIRL_ERR_INVALID, "bad arguments");
+  CK(apirl::launch_force_positive(n, d_x, (cudaStream_t)stream));
+  return APIRL_OK;
+}
+
+apirl_status apirl_em_pass(apirl_projector* p, const void* d_counts, int counts_dtype, int counts_packed,
+                           const float* d_add, float* d_x, float* d_bp, const float* d_sens, const float* d_thr,
+                           float thr_value, int ge, int subset, int nsubsets, double* d_lik, void* stream) {
+  apirl_status st = check_subset(p, subset, nsubsets);
+  if (st) return st;
+  if (!d_counts || !d_x || !d_bp || !d_sens) return fail(APIRL_ERR_INVALID, "null buffer");
+  if (counts_dtype != APIRL_F32 && counts_dtype != APIRL_U32 && counts_dtype != APIRL_U16)
+    return fail(APIRL_ERR_INVALID, "unknown counts dtype %d", counts_dtype);
+  DEVICE_SCOPE(p->device);
+  cudaStream_t s = (cudaStream_t)stream;
+  SubsetSel ss = make_subset(p, subset, nsubsets);
+  CK(apirl::launch_em_pass(p->g, p->t, ss, d_counts, counts_dtype, counts_packed, d_add, d_x, d_bp, 1,
+                           p->is3d ? 0 : 1, p->d_partials, d_lik, s));
+  const int64_t nv = (int64_t)p->g.nx * p->g.ny * p->g.nz;
+  CK(apirl::launch_update(nv, d_x, d_bp, d_sens, d_thr, thr_value, ge, 1, s));
+  return APIRL_OK;
+}
+
+apirl_status apirl_em_project_backproject(apirl_projector* p, const void* d_counts, int counts_dtype,
+                                          int counts_packed, const float* d_add, const float* d_x, float* d_bp,
+                                          int subset, int nsubsets, double* d_lik, void* stream) {
+  apirl_status st = check_subset(p, subset, nsubsets);
+  if (st) return st;
+  if (!d_counts || !d_x || !d_bp) return fail(APIRL_ERR_INVALID, "null buffer");
+  if (counts_dtype != APIRL_F32 && counts_dtype != APIRL_U32 && counts_dtype != APIRL_U16)
+    return fail(APIRL_ERR_INVALID, "unknown counts dtype %d", counts_dtype);
+  DEVICE_SCOPE(p->device);
+  CK(apirl::launch_em_pass(p->g, p->t, make_subset(p, subset, nsubsets), d_counts, counts_dtype, counts_packed,
+                           d_add, d_x, d_bp, 1, p->is3d ? 0 : 1, p->d_partials, d_lik, (cudaStream_t)stream));
+  return APIRL_OK;
+}
+
+apirl_status apirl_em_pass_host(apirl_projector* p, const void* h_counts_subset, int counts_dtype,
+                                void* d_counts_stage, float* d_x, float* d_bp, const float* d_sens,
+                                float thr_value, int ge, int subset, int nsubsets, float* h_x_out, double* h_lik,
+                                void* stream) {
+  apirl_status st = check_subset(p, subset, nsubsets);
+  if (st) return st;
+  if (!h_counts_subset || !d_counts_stage || !h_x_out) return fail(APIRL_ERR_INVALID, "null buffer");
+  const int64_t nb = apirl_projector_num_bins(p, subset, nsubsets);
+  const size_t esz = counts_dtype == APIRL_U16 ? 2 : 4;
+  DEVICE_SCOPE(p->device);
+  cudaStream_t s = (cudaStream_t)stream;
+  CK(cudaMemcpyAsync(d_counts_stage, h_counts_subset, nb * esz, cudaMemcpyHostToDevice, s));
+  double* d_lik = p->d_scalars;
+  st = apirl_em_pass(p, d_counts_stage, counts_dtype, 1, nullptr, d_x, d_bp, d_sens, nullptr, thr_value, ge, subset,
+                     nsubsets, h_lik ? d_lik : nullptr, stream);
+  if (st) return st;
+  const int64_t nv = (int64_t)p->g.nx * p->g.ny * p->g.nz;
+  CK(cudaMemcpyAsync(h_x_out, d_x, nv * sizeof(float), cudaMemcpyDeviceToHost, s));
+  if (h_lik) CK(cudaMemcpyAsync(h_lik, d_lik, sizeof(double), cudaMemcpyDeviceToHost, s));
+  CK(cudaStreamSynchronize(s));
+  return APIRL_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,245 @@
+// Whole reconstructions with host buffers: the MLEM / OSEM drivers of the
+// reference (recon/src/Mlem2d.cpp, MlemSinogram3d.cpp, OsemSinogram3d.cpp)
+// on device-resident state.  Each EM pass is captured once as a CUDA graph
+// (fused projection/ratio/backprojection kernel, likelihood sum, pixel update)
+// and replayed every iteration.
+#include <cuda_runtime.h>
+#include <cstdarg>
+#include <cstdio>
+#include <string>
+#include <vector>
+#include "internal.h"
+#include "../../include/apirl_b200.h"
+
+using apirl::SubsetSel;
+
+namespace {
+
+// Small RAII set for device buffers, graphs and the stream of one driver call.
+struct Res {
+  std::vector<void*> bufs;
+  std::vector<cudaGraphExec_t> execs;
+  std::vector<cudaGraph_t> graphs;
+  cudaStream_t st = nullptr;
+  apirl_projector* p = nullptr;
+  ~Res() {
+    if (st) cudaStreamSynchronize(st);
+    for (auto e : execs) cudaGraphExecDestroy(e);
+    for (auto g : graphs) cudaGraphDestroy(g);
+    for (void* b : bufs) cudaFree(b);
+    if (st) cudaStreamDestroy(st);
+    if (p) apirl_projector_destroy(p);
+  }
+  template <typename T> cudaError_t alloc(T** ptr, size_t n) {
+    cudaError_t e = cudaMalloc((void**)ptr, n * sizeof(T));
+    if (e == cudaSuccess) bufs.push_back(*ptr);
+    return e;
+  }
+};
+
+apirl_status set_err(apirl_status code, const char* what, cudaError_t e) {
+  char buf[256];
+  snprintf(buf, sizeof buf, "%s: %s", what, e == cudaSuccess ? "invalid argument" : cudaGetErrorString(e));
+  return apirl_internal_fail(code, buf);
+}
+
+#define DK(call)                                                                                \
+  do {                                                                                          \
+    cudaError_t e_ = (call);                                                                    \
+    if (e_ != cudaSuccess)                                                                      \
+      return set_err(e_ == cudaErrorMemoryAllocation ? APIRL_ERR_OOM : APIRL_ERR_CUDA, #call, e_); \
+  } while (0)
+#define DS(call)                          \
+  do {                                    \
+    apirl_status s_ = (call);             \
+    if (s_ != APIRL_OK) return s_;        \
+  } while (0)
+
+// One EM pass (fused kernel + update) recorded into a graph on `st`.
+apirl_status capture_pass(Res& r, apirl_projector* p, const float* d_meas, const float* d_add, float* d_x, float* d_bp,
+                          const float* d_sens, const float* d_thr, float thr, int ge, int subset, int nsub,
+                          double* d_lik_slot) {
+  cudaGraph_t g = nullptr;
+  DK(cudaStreamBeginCapture(r.st, cudaStreamCaptureModeThreadLocal));
+  apirl_status s = apirl_em_pass(p, d_meas, APIRL_F32, 0, d_add, d_x, d_bp, d_sens, d_thr, thr, ge, subset, nsub,
+                                 d_lik_slot, r.st);
+  cudaError_t e = cudaStreamEndCapture(r.st, &g);
+  if (s != APIRL_OK) { if (g) cudaGraphDestroy(g); return s; }
+  DK(e);
+  r.graphs.push_back(g);
+  cudaGraphExec_t ex = nullptr;
+  DK(cudaGraphInstantiate(&ex, g, 0));
+  r.execs.push_back(ex);
+  return APIRL_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+apirl_status apirl_osem_3d(const apirl_image_geom* img, const apirl_sino3d_geom* sino, const float* h_meas,
+                           const float* h_mult, const float* h_add, const float* h_init, int iters, int nsubsets,
+                           int device, float* h_out, double* h_lik, float* h_sens0) {
+  if (!h_meas || !h_init || !h_out || iters < 0 || nsubsets <= 0)
+    return set_err(APIRL_ERR_INVALID, "apirl_osem_3d arguments", cudaSuccess);
+  Res r;
+  DS(apirl_projector_create_3d(img, sino, device, &r.p));
+  int prev = 0;
+  cudaGetDevice(&prev);
+  DK(cudaSetDevice(device));
+  struct Restore { int d; ~Restore() { cudaSetDevice(d); } } restore{prev};
+  apirl_projector* p = r.p;
+  if (nsubsets > sino->n_proj) return set_err(APIRL_ERR_INVALID, "more subsets than angles", cudaSuccess);
+  DK(cudaStreamCreateWithFlags(&r.st, cudaStreamNonBlocking));
+  const int64_t nb = apirl_projector_num_bins(p, -1, 1);
+  const int64_t nv = (int64_t)img->nx * img->ny * img->nz;
+  float *d_meas, *d_mult = nullptr, *d_add = nullptr, *d_x, *d_bp, *d_sens;
+  double* d_lik;
+  DK(r.alloc(&d_meas, nb));
+  if (h_mult) DK(r.alloc(&d_mult, nb));
+  if (h_add) DK(r.alloc(&d_add, nb));
+  DK(r.alloc(&d_x, nv));
+  DK(r.alloc(&d_bp, nv));
+  DK(r.alloc(&d_sens, nv * nsubsets));
+  DK(r.alloc(&d_lik, (size_t)iters * nsubsets + 1 + nsubsets));
+  double* d_slot = d_lik + (size_t)iters * nsubsets + 1;
+  DK(cudaMemcpyAsync(d_meas, h_meas, nb * sizeof(float), cudaMemcpyHostToDevice, r.st));
+  if (h_mult) DK(cudaMemcpyAsync(d_mult, h_mult, nb * sizeof(float), cudaMemcpyHostToDevice, r.st));
+  if (h_add) DK(cudaMemcpyAsync(d_add, h_add, nb * sizeof(float), cudaMemcpyHostToDevice, r.st));
+  DK(cudaMemcpyAsync(d_x, h_init, nv * sizeof(float), cudaMemcpyHostToDevice, r.st));
+  DK(cudaMemsetAsync(d_bp, 0, nv * sizeof(float), r.st));
+  DK(cudaMemsetAsync(d_sens, 0, nv * nsubsets * sizeof(float), r.st));
+  // Per-subset sensitivity: A_s^T (mult or 1), then forcePositive
+  // (OsemSinogram3d.cpp:101-116, :327-346).
+  for (int s = 0; s < nsubsets; s++) {
+    SubsetSel ss;
+    ss.subset = s; ss.nsub = nsubsets; ss.nk = apirl::subset_nproj(sino->n_proj, s, nsubsets);
+    DK(apirl::launch_backproject(p->g, p->t, ss, d_mult, d_mult ? 1 : 2, nullptr, 0, d_sens + nv * s, r.st));
+    DK(apirl::launch_force_positive(nv, d_sens + nv * s, r.st));
+  }
+  for (int s = 0; s < nsubsets; s++)
+    DS(capture_pass(r, p, d_meas, d_add, d_x, d_bp, d_sens + nv * s, nullptr, 0.f, 1, s, nsubsets, d_slot + s));
+  for (int t = 0; t < iters; t++)
+    for (int s = 0; s < nsubsets; s++) {
+      DK(cudaGraphLaunch(r.execs[s], r.st));
+      DK(cudaMemcpyAsync(d_lik + (size_t)t * nsubsets + s, d_slot + s, sizeof(double), cudaMemcpyDeviceToDevice,
+                         r.st));
+    }
+  // Final likelihood on the whole-sinogram projection of the result (:291-293).
+  SubsetSel all;
+  all.subset = -1; all.nsub = 1; all.nk = sino->n_proj;
+  DK(apirl::launch_em_pass(p->g, p->t, all, d_meas, APIRL_F32, 0, d_add, d_x, d_bp, 0, 0, p->d_partials,
+                           d_lik + (size_t)iters * nsubsets, r.st));
+  DK(cudaMemcpyAsync(h_out, d_x, nv * sizeof(float), cudaMemcpyDeviceToHost, r.st));
+  if (h_lik) DK(cudaMemcpyAsync(h_lik, d_lik, ((size_t)iters * nsubsets + 1) * sizeof(double), cudaMemcpyDeviceToHost, r.st));
+  if (h_sens0) DK(cudaMemcpyAsync(h_sens0, d_sens, nv * sizeof(float), cudaMemcpyDeviceToHost, r.st));
+  DK(cudaStreamSynchronize(r.st));
+  return APIRL_OK;
+}
+
+apirl_status apirl_mlem_3d(const apirl_image_geom* img, const apirl_sino3d_geom* sino, const float* h_meas,
+                           const float* h_mult, const float* h_add, const float* h_init, int iters, int device,
+                           float* h_out, double* h_lik, float* h_sens) {
+  if (!h_meas || !h_init || !h_out || iters < 0) return set_err(APIRL_ERR_INVALID, "apirl_mlem_3d arguments", cudaSuccess);
+  Res r;
+  DS(apirl_projector_create_3d(img, sino, device, &r.p));
+  int prev = 0;
+  cudaGetDevice(&prev);
+  DK(cudaSetDevice(device));
+  struct Restore { int d; ~Restore() { cudaSetDevice(d); } } restore{prev};
+  apirl_projector* p = r.p;
+  DK(cudaStreamCreateWithFlags(&r.st, cudaStreamNonBlocking));
+  const int64_t nb = apirl_projector_num_bins(p, -1, 1);
+  const int64_t nv = (int64_t)img->nx * img->ny * img->nz;
+  float *d_meas, *d_mult = nullptr, *d_add = nullptr, *d_x, *d_bp, *d_sens, *d_thr;
+  double* d_lik;
+  DK(r.alloc(&d_meas, nb));
+  if (h_mult) DK(r.alloc(&d_mult, nb));
+  if (h_add) DK(r.alloc(&d_add, nb));
+  DK(r.alloc(&d_x, nv));
+  DK(r.alloc(&d_bp, nv));
+  DK(r.alloc(&d_sens, nv));
+  DK(r.alloc(&d_thr, 1));
+  DK(r.alloc(&d_lik, (size_t)iters + 2));
+  DK(cudaMemcpyAsync(d_meas, h_meas, nb * sizeof(float), cudaMemcpyHostToDevice, r.st));
+  if (h_mult) DK(cudaMemcpyAsync(d_mult, h_mult, nb * sizeof(float), cudaMemcpyHostToDevice, r.st));
+  if (h_add) DK(cudaMemcpyAsync(d_add, h_add, nb * sizeof(float), cudaMemcpyHostToDevice, r.st));
+  DK(cudaMemcpyAsync(d_x, h_init, nv * sizeof(float), cudaMemcpyHostToDevice, r.st));
+  DK(cudaMemsetAsync(d_bp, 0, nv * sizeof(float), r.st));
+  DK(cudaMemsetAsync(d_sens, 0, nv * sizeof(float), r.st));
+  SubsetSel all;
+  all.subset = -1; all.nsub = 1; all.nk = sino->n_proj;
+  DK(apirl::launch_backproject(p->g, p->t, all, d_mult, d_mult ? 1 : 2, nullptr, 0, d_sens, r.st));
+  DS(apirl_mlem_threshold(nv, d_sens, d_thr, r.st));
+  double* d_slot = d_lik + iters + 1;
+  DS(capture_pass(r, p, d_meas, d_add, d_x, d_bp, d_sens, d_thr, 0.f, 1, -1, 1, d_slot));
+  for (int t = 0; t < iters; t++) {
+    DK(cudaGraphLaunch(r.execs[0], r.st));
+    DK(cudaMemcpyAsync(d_lik + t, d_slot, sizeof(double), cudaMemcpyDeviceToDevice, r.st));
+  }
+  DK(apirl::launch_em_pass(p->g, p->t, all, d_meas, APIRL_F32, 0, d_add, d_x, d_bp, 0, 0, p->d_partials,
+                           d_lik + iters, r.st));
+  DK(cudaMemcpyAsync(h_out, d_x, nv * sizeof(float), cudaMemcpyDeviceToHost, r.st));
+  if (h_lik) DK(cudaMemcpyAsync(h_lik, d_lik, ((size_t)iters + 1) * sizeof(double), cudaMemcpyDeviceToHost, r.st));
+  if (h_sens) DK(cudaMemcpyAsync(h_sens, d_sens, nv * sizeof(float), cudaMemcpyDeviceToHost, r.st));
+  DK(cudaStreamSynchronize(r.st));
+  return APIRL_OK;
+}
+
+apirl_status apirl_mlem_2d(const apirl_image_geom* img, const apirl_sino2d_geom* sino, const float* h_meas,
+                           const float* h_mult, const float* h_add, const float* h_init, int iters, int device,
+                           float* h_out, double* h_lik, float* h_sens) {
+  if (!h_meas || !h_init || !h_out || iters < 0) return set_err(APIRL_ERR_INVALID, "apirl_mlem_2d arguments", cudaSuccess);
+  Res r;
+  DS(apirl_projector_create_2d(img, sino, device, &r.p));
+  int prev = 0;
+  cudaGetDevice(&prev);
+  DK(cudaSetDevice(device));
+  struct Restore { int d; ~Restore() { cudaSetDevice(d); } } restore{prev};
+  apirl_projector* p = r.p;
+  DK(cudaStreamCreateWithFlags(&r.st, cudaStreamNonBlocking));
+  const int64_t nb = apirl_projector_num_bins(p, -1, 1);
+  const int64_t nv = (int64_t)img->nx * img->ny * img->nz;
+  float *d_meas, *d_mult = nullptr, *d_add = nullptr, *d_x, *d_xprev, *d_bp, *d_sens, *d_thr;
+  double* d_lik;
+  DK(r.alloc(&d_meas, nb));
+  if (h_mult) DK(r.alloc(&d_mult, nb));
+  if (h_add) DK(r.alloc(&d_add, nb));
+  DK(r.alloc(&d_x, nv));
+  DK(r.alloc(&d_xprev, nv));
+  DK(r.alloc(&d_bp, nv));
+  DK(r.alloc(&d_sens, nv));
+  DK(r.alloc(&d_thr, 1));
+  DK(r.alloc(&d_lik, (size_t)iters + 2));
+  DK(cudaMemcpyAsync(d_meas, h_meas, nb * sizeof(float), cudaMemcpyHostToDevice, r.st));
+  if (h_mult) DK(cudaMemcpyAsync(d_mult, h_mult, nb * sizeof(float), cudaMemcpyHostToDevice, r.st));
+  if (h_add) DK(cudaMemcpyAsync(d_add, h_add, nb * sizeof(float), cudaMemcpyHostToDevice, r.st));
+  DK(cudaMemcpyAsync(d_x, h_init, nv * sizeof(float), cudaMemcpyHostToDevice, r.st));
+  DK(cudaMemsetAsync(d_bp, 0, nv * sizeof(float), r.st));
+  DK(cudaMemsetAsync(d_sens, 0, nv * sizeof(float), r.st));
+  SubsetSel all;
+  all.subset = -1; all.nsub = 1; all.nk = sino->n_proj;
+  DK(apirl::launch_backproject(p->g, p->t, all, d_mult, d_mult ? 1 : 2, nullptr, 0, d_sens, r.st));
+  DS(apirl_mlem_threshold(nv, d_sens, d_thr, r.st));
+  double* d_slot = d_lik + iters + 1;
+  DS(capture_pass(r, p, d_meas, d_add, d_x, d_bp, d_sens, d_thr, 0.f, 0, -1, 1, d_slot));
+  for (int t = 0; t < iters; t++) {
+    if (t == iters - 1) DK(cudaMemcpyAsync(d_xprev, d_x, nv * sizeof(float), cudaMemcpyDeviceToDevice, r.st));
+    DK(cudaGraphLaunch(r.execs[0], r.st));
+    DK(cudaMemcpyAsync(d_lik + t, d_slot, sizeof(double), cudaMemcpyDeviceToDevice, r.st));
+  }
+  // Mlem2d.cpp:228 evaluates the last value on the ratio sinogram of the last
+  // iteration: recompute that ratio from the image before the last update.
+  if (iters > 0)
+    DK(apirl::launch_em_pass(p->g, p->t, all, d_meas, APIRL_F32, 0, d_add, d_xprev, d_bp, 0, 2, p->d_partials,
+                             d_lik + iters, r.st));
+  else
+    DK(cudaMemsetAsync(d_lik, 0, sizeof(double), r.st));
+  DK(cudaMemcpyAsync(h_out, d_x, nv * sizeof(float), cudaMemcpyDeviceToHost, r.st));
+  if (h_lik) DK(cudaMemcpyAsync(h_lik, d_lik, ((size_t)iters + 1) * sizeof(double), cudaMemcpyDeviceToHost, r.st));
+  if (h_sens) DK(cudaMemcpyAsync(h_sens, d_sens, nv * sizeof(float), cudaMemcpyDeviceToHost, r.st));
+  DK(cudaStreamSynchronize(r.st));
+  return APIRL_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,113 @@
+// Host-side geometry tables, computed once per projector with the reference's
+// own float expressions so that the device walk sees bit-identical LOR end
+// points (no device transcendental enters a result):
+//   r_j   = RInc/2 + j*RInc - rFov, RInc = (2*rFov)/nR
+//   phi_i = i * (180/nProj) degrees     (Sinogram2DinCylindrical3Dpet.cpp:46-63)
+//   P1 = (r cos + sin aux, r sin - cos aux), P2 = (r cos - sin aux, r sin + cos aux),
+//   aux = sqrt(R^2 - r^2)               (Sinogram2DinCylindrical3Dpet.cpp:216-266)
+//   ring z_i = zInc/2 + i*zInc, zInc = axialFov/nRings, ring pairs per segment,
+//   end-point z = mean of the first and last pair (Sinogram3D.cpp:358-464,
+//   SiddonProjector.cpp:357-360, :392-396).
+// Built with g++ -O2 -ffp-contract=off, like the reference's own CPU build.
+#include <cmath>
+#include <vector>
+#include "internal.h"
+
+namespace apirl {
+
+namespace {
+const float kDegToRad = 0.01745329251994329576f;  // DEG_TO_RAD, utils/inc/Geometry.h:10
+
+void r_and_angles(int n_proj, int n_r, float r_fov, std::vector<float>& r, std::vector<float>& ang) {
+  const float rinc = (2 * r_fov) / (float)n_r;
+  const float phinc = (float)180 / (float)n_proj;
+  r.resize(n_r);
+  ang.resize(n_proj);
+  for (int j = 0; j < n_r; j++) r[j] = rinc / 2 + (float)j * rinc - r_fov;
+  for (int i = 0; i < n_proj; i++) ang[i] = (float)i * phinc;
+}
+
+void lor_table(int n_proj, int n_r, float r_scanner, const std::vector<float>& r, const std::vector<float>& ang,
+               std::vector<float>& lor) {
+  lor.resize((size_t)n_proj * n_r * 4);
+  for (int a = 0; a < n_proj; a++) {
+    const float phi = ang[a] * kDegToRad;
+    const float c = std::cos(phi);
+    const float s = std::sin(phi);
+    for (int l = 0; l < n_r; l++) {
+      const float rv = r[l];
+      const float aux = std::sqrt(r_scanner * r_scanner - rv * rv);
+      float* o = &lor[((size_t)a * n_r + l) * 4];
+      o[0] = rv * c + s * aux;
+      o[1] = rv * s - c * aux;
+      o[2] = rv * c - s * aux;
+      o[3] = rv * s + c * aux;
+    }
+  }
+}
+}  // namespace
+
+ImgGeom make_img_geom(int nx, int ny, int nz, float dx, float dy, float dz) {
+  ImgGeom g;
+  g.nx = nx; g.ny = ny; g.nz = nz;
+  g.dx = dx; g.dy = dy; g.dz = dz;
+  g.rfov = (dx * (float)nx) / 2;
+  g.offz = dz / 2;
+  return g;
+}
+
+int subset_nproj(int n_proj, int subset, int nsub) {
+  if (subset < 0) return n_proj;
+  int n = (int)std::floor((float)n_proj / (float)nsub);
+  if ((n_proj % nsub) > subset) n++;
+  return n;
+}
+
+void build_tables_2d(int n_proj, int n_r, float r_fov, float r_scanner, HostTables& t) {
+  std::vector<float> r, ang;
+  r_and_angles(n_proj, n_r, r_fov, r, ang);
+  lor_table(n_proj, n_r, r_scanner, r, ang, t.lor);
+  t.ok.resize(n_r);
+  for (int l = 0; l < n_r; l++) t.ok[l] = (r[l] > r_fov) ? 0 : 1;
+  t.z.assign(2, 0.f);
+  t.n_sinos = 1;
+}
+
+bool build_tables_3d(int n_proj, int n_r, int n_rings, float r_fov, float axial_fov, float r_scanner, int n_seg,
+                     const int* min_rd, const int* max_rd, HostTables& t) {
+  std::vector<float> r, ang;
+  r_and_angles(n_proj, n_r, r_fov, r, ang);
+  lor_table(n_proj, n_r, r_scanner, r, ang, t.lor);
+  t.ok.assign(n_r, 1);
+  const float zinc = axial_fov / (float)n_rings;
+  std::vector<float> ringz(n_rings);
+  for (int i = 0; i < n_rings; i++) ringz[i] = zinc / 2 + (float)i * zinc;
+  const float rw = axial_fov / (float)n_rings;
+  const float dz = rw / (float)1;
+  t.z.clear();
+  for (int sg = 0; sg < n_seg; sg++) {
+    for (int z1 = 0; z1 < 2 * n_rings; z1++) {
+      int cnt = 0;
+      float f1 = 0, l1 = 0, f2 = 0, l2 = 0;
+      int z1a = z1;
+      for (int z2 = 0; z2 < n_rings; z2++) {
+        if ((z1a - z2) <= max_rd[sg] && (z1a - z2) >= min_rd[sg] && z1a >= 0 && z2 >= 0 && z1a < n_rings &&
+            z2 < n_rings) {
+          if (cnt == 0) { f1 = ringz[z1a]; f2 = ringz[z2]; }
+          l1 = ringz[z1a]; l2 = ringz[z2];
+          cnt++;
+        }
+        z1a = z1a - 1;
+      }
+      if (cnt > 0) {
+        const float za = (f1 + l1) / 2, zb = (f2 + l2) / 2;
+        t.z.push_back(za - rw / 2 + dz / 2 + (float)0 * dz);
+        t.z.push_back(zb - rw / 2 + dz / 2 + (float)0 * dz);
+      }
+    }
+  }
+  t.n_sinos = (int)(t.z.size() / 2);
+  return t.n_sinos > 0;
+}
+
+}  // namespace apirl

@@ -1,0 +1,87 @@
+// Internal interface between the C ABI (capi.cu), the kernels (kernels.cu) and
+// the host-side geometry builder (host_geometry.cpp).
+#pragma once
+#include <cuda_runtime.h>
+#include <cstdint>
+#include <vector>
+#include "geom_types.h"
+
+namespace apirl {
+
+// Device-resident geometry of one sinogram.
+struct LorTable {
+  const float4* lor;    // [n_proj][n_r] = (p1x, p1y, p2x, p2y)
+  const float2* z;      // 3D: [n_sinos] = (z1, z2) end-point z; 2D: unused
+  const uint8_t* ok;    // 2D: [n_r] 1 when r <= sinogram rFov (getPointsFromLor); 3D: unused
+  int n_proj, n_r, n_sinos;
+  int is3d;
+};
+
+struct SubsetSel {
+  int subset;  // < 0: all angles
+  int nsub;
+  int nk;      // angles in this subset
+};
+
+// Host-side tables built with the reference's float expressions.
+struct HostTables {
+  std::vector<float> lor;   // n_proj * n_r * 4
+  std::vector<float> z;     // n_sinos * 2
+  std::vector<uint8_t> ok;  // n_r
+  int n_sinos = 1;
+};
+void build_tables_2d(int n_proj, int n_r, float r_fov, float r_scanner, HostTables& t);
+bool build_tables_3d(int n_proj, int n_r, int n_rings, float r_fov, float axial_fov, float r_scanner, int n_seg,
+                     const int* min_rd, const int* max_rd, HostTables& t);
+ImgGeom make_img_geom(int nx, int ny, int nz, float dx, float dy, float dz);
+
+int subset_nproj(int n_proj, int subset, int nsub);
+
+// Launchers (kernels.cu).  All return cudaGetLastError() after the launch.
+cudaError_t launch_project(const ImgGeom& g, const LorTable& t, SubsetSel s, const float* img, float* out,
+                           cudaStream_t st);
+// vin_mode: 0 = subset sinogram, 1 = whole sinogram read at the subset's angles, 2 = all ones.
+cudaError_t launch_backproject(const ImgGeom& g, const LorTable& t, SubsetSel s, const float* vin, int vin_mode,
+                               const float* vest, int divide, float* img, cudaStream_t st);
+cudaError_t launch_count_steps(const ImgGeom& g, const LorTable& t, SubsetSel s, int32_t* steps, cudaStream_t st);
+
+// Fused EM pass.  partials: >= em_pass_blocks() doubles of scratch.
+int64_t em_pass_blocks(const LorTable& t, SubsetSel s);
+// lik_mode: 0 = over e != 0, 1 = over e > 0, 2 = over ratio > 0.  back = 0: no backprojection.
+cudaError_t launch_em_pass(const ImgGeom& g, const LorTable& t, SubsetSel s, const void* counts, int counts_dtype,
+                           int counts_packed, const float* add, const float* x, float* bp, int back, int lik_mode,
+                           double* partials, double* lik, cudaStream_t st);
+
+cudaError_t launch_inverse_divide(int64_t n, const float* meas, float* est, cudaStream_t st);
+cudaError_t launch_add_bins(int64_t n, const float* add, float* est, cudaStream_t st);
+cudaError_t launch_likelihood(int64_t n, const float* est, const float* meas, int gt0, double* partials,
+                              int64_t n_partials, double* out, cudaStream_t st);
+int64_t likelihood_blocks(int64_t n);
+cudaError_t launch_threshold(int64_t n, const float* sens, unsigned* minmax_scratch, float* thr, cudaStream_t st);
+cudaError_t launch_update(int64_t n, float* x, float* bp, const float* sens, const float* thr_ptr, float thr_value,
+                          int ge, int zero_bp, cudaStream_t st);
+cudaError_t launch_force_positive(int64_t n, float* x, cudaStream_t st);
+cudaError_t launch_fill(int64_t n, float* x, float v, cudaStream_t st);
+
+}  // namespace apirl
+
+typedef int apirl_status;
+
+// Projector object behind the opaque apirl_projector handle.
+struct apirl_projector {
+  int device = 0;
+  int is3d = 0;
+  apirl::ImgGeom g{};
+  apirl::HostTables host;
+  float4* d_lor = nullptr;
+  float2* d_z = nullptr;
+  uint8_t* d_ok = nullptr;
+  apirl::LorTable t{};
+  double* d_partials = nullptr;  // per-block likelihood partials, enough for a whole-sinogram pass
+  int64_t n_partials = 0;
+  unsigned* d_minmax = nullptr;  // threshold reduction keys
+  double* d_scalars = nullptr;   // 8 doubles of per-projector scratch (likelihood of host passes)
+};
+
+// Records `msg` as the calling thread's last error and returns `code`.
+apirl_status apirl_internal_fail(apirl_status code, const char* msg);

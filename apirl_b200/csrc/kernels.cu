@@ -1,0 +1,455 @@
+// CUDA kernels for sm_100a: Siddon projection, backprojection, the fused EM
+// pass and the bin-wise / pixel-wise steps around them.
+//
+// Layout in HBM
+//   image        float [z][y][x]
+//   LOR table    float4 [angle][r] (p1x, p1y, p2x, p2y), built on the host
+//   ring z       float2 [sinogram] (z1, z2)
+//   sinogram     [sinogram][angle][r]; subset sinograms [sinogram][k][r]
+//
+// Thread mapping: one thread per sinogram bin, consecutive threads on
+// consecutive r of the same (sinogram, angle), so that the bin loads and stores
+// coalesce and a warp walks 32 near-parallel rays through neighbouring voxels.
+#include <cuda_runtime.h>
+#include <cstdint>
+#include <cfloat>
+#include "internal.h"
+#include "siddon.cuh"
+#include "../../include/apirl_b200.h"
+
+namespace apirl {
+
+namespace {
+
+constexpr int kBlock = 256;
+
+struct BinPos {
+  int g, k, l, a;  // sinogram, subset angle, r, full angle
+};
+
+__device__ __forceinline__ BinPos decode(int64_t b, const LorTable& t, const SubsetSel& s) {
+  BinPos p;
+  const int64_t per = (int64_t)s.nk * t.n_r;
+  p.g = (int)(b / per);
+  const int rem = (int)(b - (int64_t)p.g * per);
+  p.k = rem / t.n_r;
+  p.l = rem - p.k * t.n_r;
+  p.a = s.subset < 0 ? p.k : s.subset + s.nsub * p.k;
+  return p;
+}
+
+template <typename CT> __device__ __forceinline__ float load_count(const CT* p, int64_t i);
+template <> __device__ __forceinline__ float load_count<float>(const float* p, int64_t i) { return __ldg(p + i); }
+template <> __device__ __forceinline__ float load_count<uint32_t>(const uint32_t* p, int64_t i) {
+  return (float)__ldg(p + i);
+}
+template <> __device__ __forceinline__ float load_count<uint16_t>(const uint16_t* p, int64_t i) {
+  return (float)__ldg(p + i);
+}
+
+// Forward projection of one bin (3D), masked gather of the image.
+__device__ __forceinline__ float ray_sum3(const ImgGeom& g, const float4 L, const float2 z, const float* __restrict__ img,
+                                          Walk3& w) {
+  siddon3_setup(L.x, L.y, z.x, A_SUB(L.z, L.x), A_SUB(L.w, L.y), A_SUB(z.y, z.x), g, w);
+  float acc = 0.f;
+  siddon3_walk(w, g, [&](bool inb, int idx, float seg) {
+    if (inb) acc = A_ADD(acc, A_MUL(seg, __ldg(img + idx)));
+  });
+  return acc;
+}
+
+__device__ __forceinline__ float ray_sum2(const ImgGeom& g, const float4 L, const float* __restrict__ img, Walk2& w) {
+  siddon2_setup(L.x, L.y, A_SUB(L.z, L.x), A_SUB(L.w, L.y), g, w);
+  float acc = 0.f;
+  siddon2_walk(w, g, [&](bool inb, int idx, float seg) {
+    if (inb) acc = A_ADD(acc, A_MUL(seg, __ldg(img + idx)));
+  });
+  return acc;
+}
+
+__device__ __forceinline__ double block_sum(double v) {
+  __shared__ double red[kBlock / 32];
+  #pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  if (lane == 0) red[wid] = v;
+  __syncthreads();
+  double s = 0.0;
+  if (wid == 0) {
+    s = lane < (int)(blockDim.x >> 5) ? red[lane] : 0.0;
+    #pragma unroll
+    for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
+  }
+  return s;  // valid in thread 0
+}
+
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(kBlock) k_project3(ImgGeom g, LorTable t, SubsetSel s,
+                                                     const float* __restrict__ img, float* __restrict__ out,
+                                                     int64_t total) {
+  const int64_t b = (int64_t)blockIdx.x * kBlock + threadIdx.x;
+  if (b >= total) return;
+  const BinPos p = decode(b, t, s);
+  Walk3 w;
+  out[b] = ray_sum3(g, t.lor[(int64_t)p.a * t.n_r + p.l], t.z[p.g], img, w);
+}
+
+__global__ void __launch_bounds__(kBlock) k_project2(ImgGeom g, LorTable t, SubsetSel s,
+                                                     const float* __restrict__ img, float* __restrict__ out,
+                                                     int64_t total) {
+  const int64_t b = (int64_t)blockIdx.x * kBlock + threadIdx.x;
+  if (b >= total) return;
+  const BinPos p = decode(b, t, s);
+  if (!t.ok[p.l]) return;  // getPointsFromLor false: the bin is not written (SiddonProjector.cpp:166-173)
+  Walk2 w;
+  out[b] = ray_sum2(g, t.lor[(int64_t)p.a * t.n_r + p.l], img, w);
+}
+
+// divide == 0: Backproject, value = seg * v over bins with v != 0.
+// divide == 1: DivideAndBackproject with the 3D zero rules (SiddonProjector.cpp:669-683).
+// vin_mode: 0 = vin is a subset sinogram, 1 = vin is the whole sinogram (read at
+// this subset's angles), 2 = every bin is 1 (sensitivity of ones).
+__device__ __forceinline__ float load_bin(const float* __restrict__ v, int vin_mode, int64_t b, const BinPos& p,
+                                          const LorTable& t) {
+  if (vin_mode == 2) return 1.f;
+  if (vin_mode == 1) return __ldg(v + ((int64_t)p.g * t.n_proj + p.a) * t.n_r + p.l);
+  return __ldg(v + b);
+}
+
+__global__ void __launch_bounds__(kBlock) k_backproject3(ImgGeom g, LorTable t, SubsetSel s,
+                                                         const float* __restrict__ vin, int vin_mode,
+                                                         const float* __restrict__ vest, int divide,
+                                                         float* __restrict__ img, int64_t total) {
+  const int64_t b = (int64_t)blockIdx.x * kBlock + threadIdx.x;
+  if (b >= total) return;
+  const BinPos p = decode(b, t, s);
+  const float v = load_bin(vin, vin_mode, b, p, t);
+  if (v == 0.f) return;
+  const float e = divide ? vest[b] : 0.f;
+  const float4 L = t.lor[(int64_t)p.a * t.n_r + p.l];
+  const float2 z = t.z[p.g];
+  Walk3 w;
+  siddon3_setup(L.x, L.y, z.x, A_SUB(L.z, L.x), A_SUB(L.w, L.y), A_SUB(z.y, z.x), g, w);
+  siddon3_walk(w, g, [&](bool inb, int idx, float seg) {
+    if (!inb) return;
+    float val = A_MUL(seg, v);
+    if (divide && e != 0.f) val = A_DIV(val, e);
+    atomicAdd(img + idx, val);
+  });
+}
+
+// divide == 0: Backproject over every bin (SiddonProjector.cpp:34-87).
+// divide == 1: DivideAndBackproject, only bins with e != 0 and m != 0 (:110).
+__global__ void __launch_bounds__(kBlock) k_backproject2(ImgGeom g, LorTable t, SubsetSel s,
+                                                         const float* __restrict__ vin, int vin_mode,
+                                                         const float* __restrict__ vest, int divide,
+                                                         float* __restrict__ img, int64_t total) {
+  const int64_t b = (int64_t)blockIdx.x * kBlock + threadIdx.x;
+  if (b >= total) return;
+  const BinPos p = decode(b, t, s);
+  const float v = load_bin(vin, vin_mode, b, p, t);
+  const float e = divide ? vest[b] : 1.f;
+  if (divide && !(e != 0.f && v != 0.f)) return;
+  if (v == 0.f) return;  // adding seg * 0 leaves every voxel unchanged
+  if (!t.ok[p.l]) return;
+  const float4 L = t.lor[(int64_t)p.a * t.n_r + p.l];
+  Walk2 w;
+  siddon2_setup(L.x, L.y, A_SUB(L.z, L.x), A_SUB(L.w, L.y), g, w);
+  siddon2_walk(w, g, [&](bool inb, int idx, float seg) {
+    if (!inb) return;
+    float val = A_MUL(seg, v);
+    if (divide) val = A_DIV(val, e);
+    atomicAdd(img + idx, val);
+  });
+}
+
+__global__ void __launch_bounds__(kBlock) k_count_steps(ImgGeom g, LorTable t, SubsetSel s, int32_t* steps,
+                                                        int64_t total) {
+  const int64_t b = (int64_t)blockIdx.x * kBlock + threadIdx.x;
+  if (b >= total) return;
+  const BinPos p = decode(b, t, s);
+  const float4 L = t.lor[(int64_t)p.a * t.n_r + p.l];
+  if (t.is3d) {
+    const float2 z = t.z[p.g];
+    Walk3 w;
+    siddon3_setup(L.x, L.y, z.x, A_SUB(L.z, L.x), A_SUB(L.w, L.y), A_SUB(z.y, z.x), g, w);
+    steps[b] = w.n;
+  } else {
+    Walk2 w;
+    w.n = 0;
+    if (t.ok[p.l]) siddon2_setup(L.x, L.y, A_SUB(L.z, L.x), A_SUB(L.w, L.y), g, w);
+    steps[b] = w.n;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Fused EM pass: project, add, likelihood term, ratio, backproject.
+// lik_mode: 0 = term over e != 0 (3D), 1 = over e > 0 (2D), 2 = over the ratio
+// r > 0 (the final 2D value, Mlem2d.cpp:228).  back = 0 skips the backprojection.
+template <typename CT, bool IS3D>
+__global__ void __launch_bounds__(kBlock) k_em_pass(ImgGeom g, LorTable t, SubsetSel s, const CT* __restrict__ counts,
+                                                    int counts_packed, const float* __restrict__ add,
+                                                    const float* __restrict__ x, float* __restrict__ bp, int back,
+                                                    int lik_mode, double* __restrict__ partials, int64_t total) {
+  const int64_t b = (int64_t)blockIdx.x * kBlock + threadIdx.x;
+  double term = 0.0;
+  if (b < total) {
+    const BinPos p = decode(b, t, s);
+    const int64_t row = counts_packed ? ((int64_t)p.g * s.nk + p.k) : ((int64_t)p.g * t.n_proj + p.a);
+    const int64_t ci = row * t.n_r + p.l;
+    const float m = load_count<CT>(counts, ci);
+    const float4 L = t.lor[(int64_t)p.a * t.n_r + p.l];
+    if (IS3D) {
+      Walk3 w;
+      float e = ray_sum3(g, L, t.z[p.g], x, w);
+      if (add) e = A_ADD(e, __ldg(add + ci));
+      const float r = (m != 0.f && e != 0.f) ? A_DIV(m, e) : 0.f;
+      if (lik_mode == 2) { if (r > 0.f) term = (double)m * log((double)r) - (double)r; }
+      else if (lik_mode == 1 ? (e > 0.f) : (e != 0.f)) term = (double)m * log((double)e) - (double)e;
+      if (back && r != 0.f)
+        siddon3_walk(w, g, [&](bool inb, int idx, float seg) {
+          if (inb) atomicAdd(bp + idx, A_MUL(seg, r));
+        });
+    } else {
+      Walk2 w;
+      const bool ray = t.ok[p.l] != 0;
+      float e = 0.f;
+      if (ray) e = ray_sum2(g, L, x, w);
+      if (add) e = A_ADD(e, __ldg(add + ci));
+      const float r = (m != 0.f && e != 0.f) ? A_DIV(m, e) : 0.f;
+      if (lik_mode == 2) { if (r > 0.f) term = (double)m * log((double)r) - (double)r; }
+      else if (lik_mode == 1 ? (e > 0.f) : (e != 0.f)) term = (double)m * log((double)e) - (double)e;
+      if (back && ray && r != 0.f)
+        siddon2_walk(w, g, [&](bool inb, int idx, float seg) {
+          if (inb) atomicAdd(bp + idx, A_MUL(seg, r));
+        });
+    }
+  }
+  const double bs = block_sum(term);
+  if (threadIdx.x == 0) partials[blockIdx.x] = bs;
+}
+
+// Deterministic final sum of per-block partials (one block).
+__global__ void k_sum_partials(const double* __restrict__ partials, int64_t n, double* __restrict__ out) {
+  double v = 0.0;
+  for (int64_t i = threadIdx.x; i < n; i += blockDim.x) v += partials[i];
+  const double s = block_sum(v);
+  if (threadIdx.x == 0) *out = s;
+}
+
+// ---------------------------------------------------------------------------
+__global__ void k_inverse_divide(int64_t n, const float* __restrict__ meas, float* __restrict__ est) {
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+    const float num = meas[i], den = est[i];
+    est[i] = (num != 0.f && den != 0.f) ? A_DIV(num, den) : 0.f;
+  }
+}
+
+__global__ void k_add_bins(int64_t n, const float* __restrict__ add, float* __restrict__ est) {
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+    est[i] = A_ADD(est[i], add[i]);
+}
+
+__global__ void __launch_bounds__(kBlock) k_likelihood(int64_t n, const float* __restrict__ est,
+                                                       const float* __restrict__ meas, int gt0,
+                                                       double* __restrict__ partials) {
+  double v = 0.0;
+  for (int64_t i = (int64_t)blockIdx.x * kBlock + threadIdx.x; i < n; i += (int64_t)gridDim.x * kBlock) {
+    const float e = est[i];
+    if (gt0 ? (e > 0.f) : (e != 0.f)) v += (double)meas[i] * log((double)e) - (double)e;
+  }
+  const double s = block_sum(v);
+  if (threadIdx.x == 0) partials[blockIdx.x] = s;
+}
+
+__device__ __forceinline__ unsigned fkey(float f) {
+  const unsigned u = __float_as_uint(f);
+  return (u & 0x80000000u) ? ~u : (u | 0x80000000u);
+}
+__device__ __forceinline__ float fkey_inv(unsigned k) {
+  return __uint_as_float((k & 0x80000000u) ? (k & 0x7fffffffu) : ~k);
+}
+
+__global__ void k_minmax_init(const float* __restrict__ sens, unsigned* mm) {
+  mm[0] = fkey(FLT_MAX);
+  mm[1] = fkey(sens[0]);
+}
+
+// Minimum over non-zero values and maximum over all values.
+__global__ void __launch_bounds__(kBlock) k_minmax(int64_t n, const float* __restrict__ v, unsigned* mm) {
+  float mn = FLT_MAX, mx = -FLT_MAX;
+  for (int64_t i = (int64_t)blockIdx.x * kBlock + threadIdx.x; i < n; i += (int64_t)gridDim.x * kBlock) {
+    const float f = v[i];
+    if (f != 0.f && f < mn) mn = f;
+    if (f > mx) mx = f;
+  }
+  #pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    mn = fminf(mn, __shfl_down_sync(0xffffffffu, mn, o));
+    mx = fmaxf(mx, __shfl_down_sync(0xffffffffu, mx, o));
+  }
+  if ((threadIdx.x & 31) == 0) {
+    atomicMin(mm, fkey(mn));
+    atomicMax(mm + 1, fkey(mx));
+  }
+}
+
+__global__ void k_threshold(const unsigned* mm, float* thr) {
+  const float mn = fkey_inv(mm[0]), mx = fkey_inv(mm[1]);
+  *thr = A_ADD(mn, A_MUL(A_SUB(mx, mn), 0.0001f));
+}
+
+__global__ void k_update(int64_t n, float* __restrict__ x, float* __restrict__ bp, const float* __restrict__ sens,
+                         const float* __restrict__ thr_ptr, float thr_value, int ge, int zero_bp, int vec4) {
+  const float thr = thr_ptr ? *thr_ptr : thr_value;
+  const int64_t n4 = vec4 ? (n >> 2) : 0;
+  float4* x4 = reinterpret_cast<float4*>(x);
+  float4* b4 = reinterpret_cast<float4*>(bp);
+  const float4* s4 = reinterpret_cast<const float4*>(sens);
+  const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n4; i += stride) {
+    float4 xv = x4[i], bv = b4[i], sv = __ldg(s4 + i);
+    float* xs = &xv.x; const float* bs = &bv.x; const float* ss = &sv.x;
+    #pragma unroll
+    for (int c = 0; c < 4; c++) {
+      const bool okv = ge ? (ss[c] >= thr) : (ss[c] > thr);
+      xs[c] = okv ? A_DIV(A_MUL(xs[c], bs[c]), ss[c]) : 0.f;
+    }
+    x4[i] = xv;
+    if (zero_bp) b4[i] = make_float4(0.f, 0.f, 0.f, 0.f);
+  }
+  for (int64_t i = (n4 << 2) + (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
+    const bool okv = ge ? (sens[i] >= thr) : (sens[i] > thr);
+    x[i] = okv ? A_DIV(A_MUL(x[i], bp[i]), sens[i]) : 0.f;
+    if (zero_bp) bp[i] = 0.f;
+  }
+}
+
+__global__ void k_force_positive(int64_t n, float* __restrict__ x) {
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+    if (x[i] < 0.f) x[i] = 0.f;
+}
+
+__global__ void k_fill(int64_t n, float* __restrict__ x, float v) {
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+    x[i] = v;
+}
+
+inline unsigned grid_for(int64_t total) { return (unsigned)((total + kBlock - 1) / kBlock); }
+inline unsigned stream_grid(int64_t n) {
+  int64_t g = (n + kBlock - 1) / kBlock;
+  const int64_t cap = 148 * 16;  // a few waves over the 148 SMs; the loops stride
+  return (unsigned)(g < 1 ? 1 : (g > cap ? cap : g));
+}
+
+}  // namespace
+
+int64_t em_pass_blocks(const LorTable& t, SubsetSel s) {
+  return ((int64_t)t.n_sinos * s.nk * t.n_r + kBlock - 1) / kBlock;
+}
+int64_t likelihood_blocks(int64_t n) { return stream_grid(n); }
+
+cudaError_t launch_project(const ImgGeom& g, const LorTable& t, SubsetSel s, const float* img, float* out,
+                           cudaStream_t st) {
+  const int64_t total = (int64_t)t.n_sinos * s.nk * t.n_r;
+  if (total == 0) return cudaSuccess;
+  if (t.is3d) k_project3<<<grid_for(total), kBlock, 0, st>>>(g, t, s, img, out, total);
+  else k_project2<<<grid_for(total), kBlock, 0, st>>>(g, t, s, img, out, total);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_backproject(const ImgGeom& g, const LorTable& t, SubsetSel s, const float* vin, int vin_mode,
+                               const float* vest, int divide, float* img, cudaStream_t st) {
+  const int64_t total = (int64_t)t.n_sinos * s.nk * t.n_r;
+  if (total == 0) return cudaSuccess;
+  if (t.is3d) k_backproject3<<<grid_for(total), kBlock, 0, st>>>(g, t, s, vin, vin_mode, vest, divide, img, total);
+  else k_backproject2<<<grid_for(total), kBlock, 0, st>>>(g, t, s, vin, vin_mode, vest, divide, img, total);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_count_steps(const ImgGeom& g, const LorTable& t, SubsetSel s, int32_t* steps, cudaStream_t st) {
+  const int64_t total = (int64_t)t.n_sinos * s.nk * t.n_r;
+  if (total == 0) return cudaSuccess;
+  k_count_steps<<<grid_for(total), kBlock, 0, st>>>(g, t, s, steps, total);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_em_pass(const ImgGeom& g, const LorTable& t, SubsetSel s, const void* counts, int counts_dtype,
+                           int counts_packed, const float* add, const float* x, float* bp, int back, int lik_mode,
+                           double* partials, double* lik, cudaStream_t st) {
+  const int64_t total = (int64_t)t.n_sinos * s.nk * t.n_r;
+  const unsigned grid = grid_for(total);
+  if (total == 0) return cudaSuccess;
+#define APIRL_EM(CT)                                                                                          \
+  do {                                                                                                        \
+    if (t.is3d)                                                                                               \
+      k_em_pass<CT, true><<<grid, kBlock, 0, st>>>(g, t, s, (const CT*)counts, counts_packed, add, x, bp,     \
+                                                   back, lik_mode, partials, total);                          \
+    else                                                                                                      \
+      k_em_pass<CT, false><<<grid, kBlock, 0, st>>>(g, t, s, (const CT*)counts, counts_packed, add, x, bp,    \
+                                                    back, lik_mode, partials, total);                         \
+  } while (0)
+  switch (counts_dtype) {
+    case APIRL_F32: APIRL_EM(float); break;
+    case APIRL_U32: APIRL_EM(uint32_t); break;
+    case APIRL_U16: APIRL_EM(uint16_t); break;
+    default: return cudaErrorInvalidValue;
+  }
+#undef APIRL_EM
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess || !lik) return e;
+  k_sum_partials<<<1, kBlock, 0, st>>>(partials, grid, lik);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_inverse_divide(int64_t n, const float* meas, float* est, cudaStream_t st) {
+  if (n == 0) return cudaSuccess;
+  k_inverse_divide<<<stream_grid(n), kBlock, 0, st>>>(n, meas, est);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_add_bins(int64_t n, const float* add, float* est, cudaStream_t st) {
+  if (n == 0) return cudaSuccess;
+  k_add_bins<<<stream_grid(n), kBlock, 0, st>>>(n, add, est);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_likelihood(int64_t n, const float* est, const float* meas, int gt0, double* partials,
+                              int64_t n_partials, double* out, cudaStream_t st) {
+  const unsigned grid = stream_grid(n);
+  if ((int64_t)grid > n_partials) return cudaErrorInvalidValue;
+  k_likelihood<<<grid, kBlock, 0, st>>>(n, est, meas, gt0, partials);
+  k_sum_partials<<<1, kBlock, 0, st>>>(partials, grid, out);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_threshold(int64_t n, const float* sens, unsigned* mm, float* thr, cudaStream_t st) {
+  if (n == 0) return cudaErrorInvalidValue;
+  k_minmax_init<<<1, 1, 0, st>>>(sens, mm);
+  k_minmax<<<stream_grid(n), kBlock, 0, st>>>(n, sens, mm);
+  k_threshold<<<1, 1, 0, st>>>(mm, thr);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_update(int64_t n, float* x, float* bp, const float* sens, const float* thr_ptr, float thr_value,
+                          int ge, int zero_bp, cudaStream_t st) {
+  if (n == 0) return cudaSuccess;
+  const int vec4 = ((reinterpret_cast<uintptr_t>(x) | reinterpret_cast<uintptr_t>(bp) |
+                     reinterpret_cast<uintptr_t>(sens)) & 15u) == 0;
+  k_update<<<stream_grid((n + 3) / 4), kBlock, 0, st>>>(n, x, bp, sens, thr_ptr, thr_value, ge, zero_bp, vec4);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_force_positive(int64_t n, float* x, cudaStream_t st) {
+  if (n == 0) return cudaSuccess;
+  k_force_positive<<<stream_grid(n), kBlock, 0, st>>>(n, x);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_fill(int64_t n, float* x, float v, cudaStream_t st) {
+  if (n == 0) return cudaSuccess;
+  k_fill<<<stream_grid(n), kBlock, 0, st>>>(n, x, v);
+  return cudaGetLastError();
+}
+
+}  // namespace apirl

@@ -1,0 +1,169 @@
+// Device-side Siddon ray walk for sm_100a.
+//
+// The walk restates the reference's serial Siddon (recon/src/Siddon.cpp:13-344
+// for 3D, :358-643 for 2D) with the same float operations in the same order.
+// Every add, multiply, divide and square root that feeds a weight or a voxel
+// index is written with the round-to-nearest intrinsics (__fadd_rn, ...), which
+// the compiler never contracts into FMAs, so each segment (voxel, length) is
+// bit-identical to the reference compiled for x86 without FMA.  Instead of
+// materialising a malloc'd segment list per LOR (Siddon.cpp:222) the walk hands
+// each segment to a visitor in registers.
+#pragma once
+#include <cuda_runtime.h>
+#include <cfloat>
+#include <cstdint>
+#include "geom_types.h"
+
+namespace apirl {
+
+#define A_ADD(a, b) __fadd_rn((a), (b))
+#define A_SUB(a, b) __fsub_rn((a), (b))
+#define A_MUL(a, b) __fmul_rn((a), (b))
+#define A_DIV(a, b) __fdiv_rn((a), (b))
+
+__device__ __forceinline__ float fmin_ref(float a, float b) { return (b < a) ? b : a; }  // std::min
+__device__ __forceinline__ float fmax_ref(float a, float b) { return (a < b) ? b : a; }  // std::max
+
+// Walk state after the set-up of one LOR.  `n` is the number of segments the
+// reference records, |di| + |dj| + |dk| (Siddon.cpp:220).
+struct Walk3 {
+  float ax, ay, az, axu, ayu, azu, ac, L;
+  int i, j, k, iinc, jinc, kinc, n;
+};
+
+__device__ __forceinline__ void siddon3_setup(float p0x, float p0y, float p0z, float vx, float vy, float vz,
+                                              const ImgGeom& g, Walk3& w) {
+  const float rFov = g.rfov;
+  float amin, amax;
+  if (vx == 0.f) {
+    float a1 = A_DIV(A_SUB(-rFov, p0y), vy), a2 = A_DIV(A_SUB(rFov, p0y), vy);
+    if (a1 < a2) { amin = a1; amax = a2; } else { amin = a2; amax = a1; }
+  } else if (vy == 0.f) {
+    float a1 = A_DIV(A_SUB(-rFov, p0x), vx), a2 = A_DIV(A_SUB(rFov, p0x), vx);
+    if (a1 < a2) { amin = a1; amax = a2; } else { amin = a2; amax = a1; }
+  } else {
+    float ax1 = A_DIV(A_SUB(-rFov, p0x), vx), ay1 = A_DIV(A_SUB(-rFov, p0y), vy);
+    float ax2 = A_DIV(A_SUB(rFov, p0x), vx), ay2 = A_DIV(A_SUB(rFov, p0y), vy);
+    amin = fmax_ref(fmin_ref(ax1, ax2), fmin_ref(ay1, ay2));
+    amax = fmin_ref(fmax_ref(ax1, ax2), fmax_ref(ay1, ay2));
+  }
+  if (amin < 0.f || amin > 1.f) amin = 0.f;
+  if (amax > 1.f || amax < 0.f) amax = 1.f;
+  const float x1 = A_ADD(p0x, A_MUL(vx, amin)), y1 = A_ADD(p0y, A_MUL(vy, amin)), z1 = A_ADD(p0z, A_MUL(vz, amin));
+  const float x2 = A_ADD(p0x, A_MUL(vx, amax)), y2 = A_ADD(p0y, A_MUL(vy, amax)), z2 = A_ADD(p0z, A_MUL(vz, amax));
+  const int imin = (int)floorf(A_DIV(A_ADD(x1, rFov), g.dx)), jmin = (int)floorf(A_DIV(A_ADD(y1, rFov), g.dy));
+  const int kmin = (int)floorf(A_DIV(A_SUB(z1, g.offz), g.dz));
+  const int imax = (int)floorf(A_DIV(A_ADD(x2, rFov), g.dx)), jmax = (int)floorf(A_DIV(A_ADD(y2, rFov), g.dy));
+  const int kmax = (int)floorf(A_DIV(A_SUB(z2, g.offz), g.dz));
+  w.n = abs(imax - imin) + abs(jmax - jmin) + abs(kmax - kmin);
+  w.iinc = vx > 0.f ? 1 : (vx < 0.f ? -1 : 0);
+  w.jinc = vy > 0.f ? 1 : (vy < 0.f ? -1 : 0);
+  w.kinc = vz > 0.f ? 1 : (vz < 0.f ? -1 : 0);
+  const float ex = A_SUB(A_ADD(p0x, vx), p0x), ey = A_SUB(A_ADD(p0y, vy), p0y), ez = A_SUB(A_ADD(p0z, vz), p0z);
+  w.L = __fsqrt_rn(A_ADD(A_ADD(A_MUL(ex, ex), A_MUL(ey, ey)), A_MUL(ez, ez)));
+  w.axu = fabsf(A_DIV(g.dx, vx));
+  w.ayu = fabsf(A_DIV(g.dy, vy));
+  w.azu = fabsf(A_DIV(g.dz, vz));
+  w.ax = vx > 0.f ? A_DIV(A_SUB(A_ADD(-rFov, A_MUL((float)(imin + w.iinc), g.dx)), p0x), vx)
+       : (vx < 0.f ? A_DIV(A_SUB(A_ADD(-rFov, A_MUL((float)imin, g.dx)), p0x), vx) : FLT_MAX);
+  w.ay = vy > 0.f ? A_DIV(A_SUB(A_ADD(-rFov, A_MUL((float)(jmin + w.jinc), g.dy)), p0y), vy)
+       : (vy < 0.f ? A_DIV(A_SUB(A_ADD(-rFov, A_MUL((float)jmin, g.dy)), p0y), vy) : FLT_MAX);
+  w.az = vz > 0.f ? A_DIV(A_SUB(A_ADD(g.offz, A_MUL((float)(kmin + w.kinc), g.dz)), p0z), vz)
+       : (vz < 0.f ? A_DIV(A_SUB(A_ADD(g.offz, A_MUL((float)kmin, g.dz)), p0z), vz) : FLT_MAX);
+  w.ac = amin;
+  w.i = imin; w.j = jmin; w.k = kmin;
+}
+
+// Visits the n recorded segments in order: visit(inb, linear_index, length).
+// `inb` is the full six-sided bounds test; linear_index = (k*ny + j)*nx + i is
+// only meaningful when inb is true.  Record-then-advance as in Siddon.cpp:310-340.
+template <class V>
+__device__ __forceinline__ void siddon3_walk(Walk3 w, const ImgGeom& g, V&& visit) {
+  const int sx = w.iinc, sy = w.jinc * g.nx, sz = w.kinc * g.nx * g.ny;
+  int idx = (w.k * g.ny + w.j) * g.nx + w.i;
+  for (int m = 0; m < w.n; m++) {
+    const bool cx = (w.ax <= w.ay) && (w.ax <= w.az);
+    const bool cy = !cx && (w.ay <= w.ax) && (w.ay <= w.az);
+    const float an = cx ? w.ax : (cy ? w.ay : w.az);
+    const float seg = A_MUL(A_SUB(an, w.ac), w.L);
+    const bool inb = ((unsigned)w.i < (unsigned)g.nx) & ((unsigned)w.j < (unsigned)g.ny) &
+                     ((unsigned)w.k < (unsigned)g.nz);
+    visit(inb, idx, seg);
+    w.ac = an;
+    if (cx) { w.i += w.iinc; idx += sx; w.ax = A_ADD(w.ax, w.axu); }
+    else if (cy) { w.j += w.jinc; idx += sy; w.ay = A_ADD(w.ay, w.ayu); }
+    else { w.k += w.kinc; idx += sz; w.az = A_ADD(w.az, w.azu); }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// 2D (Siddon.cpp:358-643).  Differences from 3D: early exit when both end
+// indices are outside on one side (:515-519), negative first crossings clamp
+// to alpha_min (:596-606), and the weight is multiplied by `factor` (1 here).
+struct Walk2 {
+  float ax, ay, axu, ayu, ac, L;
+  int i, j, iinc, jinc, n;
+};
+
+__device__ __forceinline__ void siddon2_setup(float p0x, float p0y, float vx, float vy, const ImgGeom& g, Walk2& w) {
+  const float rFov = g.rfov;
+  float amin, amax;
+  if (vx == 0.f) {
+    float a1 = A_DIV(A_SUB(-rFov, p0y), vy), a2 = A_DIV(A_SUB(rFov, p0y), vy);
+    if (a1 < a2) { amin = a1; amax = a2; } else { amin = a2; amax = a1; }
+  } else if (vy == 0.f) {
+    float a1 = A_DIV(A_SUB(-rFov, p0x), vx), a2 = A_DIV(A_SUB(rFov, p0x), vx);
+    if (a1 < a2) { amin = a1; amax = a2; } else { amin = a2; amax = a1; }
+  } else {
+    float ax1 = A_DIV(A_SUB(-rFov, p0x), vx), ay1 = A_DIV(A_SUB(-rFov, p0y), vy);
+    float ax2 = A_DIV(A_SUB(rFov, p0x), vx), ay2 = A_DIV(A_SUB(rFov, p0y), vy);
+    amin = fmax_ref(fmin_ref(ax1, ax2), fmin_ref(ay1, ay2));
+    amax = fmin_ref(fmax_ref(ax1, ax2), fmax_ref(ay1, ay2));
+  }
+  if (amin < 0.f || amin > 1.f) amin = 0.f;
+  if (amax > 1.f || amax < 0.f) amax = 1.f;
+  const float x1 = A_ADD(p0x, A_MUL(vx, amin)), y1 = A_ADD(p0y, A_MUL(vy, amin));
+  const float x2 = A_ADD(p0x, A_MUL(vx, amax)), y2 = A_ADD(p0y, A_MUL(vy, amax));
+  const int imin = (int)floorf(A_DIV(A_ADD(x1, rFov), g.dx)), jmin = (int)floorf(A_DIV(A_ADD(y1, rFov), g.dy));
+  const int imax = (int)floorf(A_DIV(A_ADD(x2, rFov), g.dx)), jmax = (int)floorf(A_DIV(A_ADD(y2, rFov), g.dy));
+  if ((imin < 0 && imax < 0) || (jmin < 0 && jmax < 0) || (imin >= g.nx && imax >= g.nx) ||
+      (jmin >= g.ny && jmax >= g.ny)) {
+    w.n = 0;
+    return;
+  }
+  w.n = abs(imax - imin) + abs(jmax - jmin);
+  w.iinc = vx > 0.f ? 1 : (vx < 0.f ? -1 : 0);
+  w.jinc = vy > 0.f ? 1 : (vy < 0.f ? -1 : 0);
+  const float ex = A_SUB(A_ADD(p0x, vx), p0x), ey = A_SUB(A_ADD(p0y, vy), p0y);
+  w.L = __fsqrt_rn(A_ADD(A_MUL(ex, ex), A_MUL(ey, ey)));
+  w.axu = fabsf(A_DIV(g.dx, vx));
+  w.ayu = fabsf(A_DIV(g.dy, vy));
+  float ax = vx > 0.f ? A_DIV(A_SUB(A_ADD(-rFov, A_MUL((float)(imin + w.iinc), g.dx)), p0x), vx)
+           : (vx < 0.f ? A_DIV(A_SUB(A_ADD(-rFov, A_MUL((float)imin, g.dx)), p0x), vx) : FLT_MAX);
+  if (ax < 0.f) ax = amin;
+  float ay = vy > 0.f ? A_DIV(A_SUB(A_ADD(-rFov, A_MUL((float)(jmin + w.jinc), g.dy)), p0y), vy)
+           : (vy < 0.f ? A_DIV(A_SUB(A_ADD(-rFov, A_MUL((float)jmin, g.dy)), p0y), vy) : FLT_MAX);
+  if (ay < 0.f) ay = amin;
+  w.ax = ax; w.ay = ay;
+  w.ac = amin;
+  w.i = imin; w.j = jmin;
+}
+
+template <class V>
+__device__ __forceinline__ void siddon2_walk(Walk2 w, const ImgGeom& g, V&& visit) {
+  const int sy = w.jinc * g.nx;
+  int idx = w.j * g.nx + w.i;
+  for (int m = 0; m < w.n; m++) {
+    const bool cx = (w.ax <= w.ay);
+    const float an = cx ? w.ax : w.ay;
+    // ((alpha - alpha_c) * L) * factor with factor = 1: the product by 1 is exact.
+    const float seg = A_MUL(A_SUB(an, w.ac), w.L);
+    const bool inb = ((unsigned)w.i < (unsigned)g.nx) & ((unsigned)w.j < (unsigned)g.ny);
+    visit(inb, idx, seg);
+    w.ac = an;
+    if (cx) { w.i += w.iinc; idx += w.iinc; w.ax = A_ADD(w.ax, w.axu); }
+    else { w.j += w.jinc; idx += sy; w.ay = A_ADD(w.ay, w.ayu); }
+  }
+}
+
+}  // namespace apirl

@@ -1,0 +1,246 @@
+"""Python front end over the C ABI.
+
+``SiddonProjector`` mirrors the reference's ``SiddonProjector`` /
+``CuSiddonProjector`` operations (Project, Backproject, DivideAndBackproject;
+recon/inc/SiddonProjector.h:25-68) on device-resident torch tensors, plus the
+fused EM pass.  ``osem_3d`` / ``mlem_3d`` / ``mlem_2d`` mirror the
+``OsemSinogram3d`` / ``MlemSinogram3d`` / ``Mlem2d`` drivers on host arrays.
+torch provides device memory and streams only; every operation runs in the
+CUDA library.
+"""
+import ctypes
+
+import numpy as np
+
+from . import _lib
+from ._lib import check, ImageGeomC, Sino2DGeomC, Sino3DGeomC
+from .geometry import ImageGeom, Sino2DGeom, Sino3DGeom
+
+
+def _img_c(ig):
+    return ImageGeomC(ig.nx, ig.ny, ig.nz, ig.dx, ig.dy, ig.dz)
+
+
+def _sino3d_c(sg):
+    mn = (ctypes.c_int * sg.n_segments)(*sg.min_rd)
+    mx = (ctypes.c_int * sg.n_segments)(*sg.max_rd)
+    c = Sino3DGeomC(sg.n_proj, sg.n_r, sg.n_rings, sg.n_segments, sg.r_fov, sg.axial_fov, sg.r_scanner,
+                    ctypes.cast(mn, ctypes.POINTER(ctypes.c_int)), ctypes.cast(mx, ctypes.POINTER(ctypes.c_int)))
+    c._keep = (mn, mx)
+    return c
+
+
+def _sino2d_c(sg):
+    return Sino2DGeomC(sg.n_proj, sg.n_r, sg.r_fov, sg.r_scanner)
+
+
+def _ptr(t):
+    if t is None:
+        return None
+    return ctypes.c_void_p(t.data_ptr())
+
+
+def _stream(stream=None):
+    import torch
+    s = stream if stream is not None else torch.cuda.current_stream()
+    return ctypes.c_void_p(s.cuda_stream)
+
+
+_DT = {"float32": _lib.APIRL_F32, "uint32": _lib.APIRL_U32, "uint16": _lib.APIRL_U16}
+
+
+def _counts_dtype(t):
+    name = str(t.dtype).replace("torch.", "")
+    if name not in _DT:
+        raise TypeError(f"counts must be float32, uint32 or uint16, not {t.dtype}")
+    return _DT[name]
+
+
+class SiddonProjector:
+    """Siddon projector bound to one image geometry and one sinogram geometry."""
+
+    def __init__(self, image_geom: ImageGeom, sino_geom, device=0):
+        self.lib = _lib.load()
+        self.image_geom = image_geom
+        self.sino_geom = sino_geom
+        self.device = device
+        h = ctypes.c_void_p()
+        ig = _img_c(image_geom)
+        if isinstance(sino_geom, Sino3DGeom):
+            self._sc = _sino3d_c(sino_geom)
+            check(self.lib.apirl_projector_create_3d(ctypes.byref(ig), ctypes.byref(self._sc), device,
+                                                     ctypes.byref(h)))
+            self.is3d = True
+        elif isinstance(sino_geom, Sino2DGeom):
+            self._sc = _sino2d_c(sino_geom)
+            check(self.lib.apirl_projector_create_2d(ctypes.byref(ig), ctypes.byref(self._sc), device,
+                                                     ctypes.byref(h)))
+            self.is3d = False
+        else:
+            raise TypeError("sino_geom must be Sino2DGeom or Sino3DGeom")
+        self.h = h
+
+    def close(self):
+        if self.h:
+            self.lib.apirl_projector_destroy(self.h)
+            self.h = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    # ---- sizes / tables ------------------------------------------------
+    def num_bins(self, subset=-1, nsubsets=1):
+        return int(self.lib.apirl_projector_num_bins(self.h, subset, nsubsets))
+
+    @property
+    def num_sinograms(self):
+        return int(self.lib.apirl_projector_num_sinograms(self.h))
+
+    def tables(self):
+        sg = self.sino_geom
+        lor = np.zeros((sg.n_proj, sg.n_r, 4), np.float32)
+        z = np.zeros((self.num_sinograms, 2), np.float32) if self.is3d else None
+        check(self.lib.apirl_projector_tables(self.h, lor.ctypes.data_as(ctypes.c_void_p),
+                                              None if z is None else z.ctypes.data_as(ctypes.c_void_p)))
+        return lor, z
+
+    def count_steps(self, subset=-1, nsubsets=1, stream=None):
+        import torch
+        out = torch.empty(self.num_bins(subset, nsubsets), dtype=torch.int32, device=f"cuda:{self.device}")
+        check(self.lib.apirl_count_steps(self.h, subset, nsubsets, _ptr(out), _stream(stream)))
+        return out
+
+    # ---- projector operations (device tensors) ------------------------
+    def project(self, image, sino, subset=-1, nsubsets=1, stream=None):
+        """sino = A image (3D: sino is overwritten; 2D: bins with r > rFov untouched)."""
+        check(self.lib.apirl_project(self.h, _ptr(image), _ptr(sino), subset, nsubsets, _stream(stream)))
+        return sino
+
+    def backproject(self, sino, image, subset=-1, nsubsets=1, stream=None):
+        """image += A^T sino."""
+        check(self.lib.apirl_backproject(self.h, _ptr(sino), _ptr(image), subset, nsubsets, _stream(stream)))
+        return image
+
+    def divide_and_backproject(self, meas, est, image, subset=-1, nsubsets=1, stream=None):
+        """image += A^T (meas / est) with the reference's zero rules."""
+        check(self.lib.apirl_divide_and_backproject(self.h, _ptr(meas), _ptr(est), _ptr(image), subset, nsubsets,
+                                                    _stream(stream)))
+        return image
+
+    def em_pass(self, counts, x, bp, sens, subset=-1, nsubsets=1, add=None, thr=None, thr_value=0.0, ge=True,
+                counts_packed=False, lik=None, stream=None):
+        """One fused EM pass (OSEM sub-iteration / MLEM iteration); x is updated in place."""
+        check(self.lib.apirl_em_pass(self.h, _ptr(counts), _counts_dtype(counts), int(counts_packed), _ptr(add),
+                                     _ptr(x), _ptr(bp), _ptr(sens), _ptr(thr), float(thr_value), int(ge), subset,
+                                     nsubsets, _ptr(lik), _stream(stream)))
+        return x
+
+    def em_project_backproject(self, counts, x, bp, subset=-1, nsubsets=1, add=None, counts_packed=False, lik=None,
+                               stream=None):
+        """The fused kernel of em_pass alone (bp += A^T (m / (A x + add))); x is not updated."""
+        check(self.lib.apirl_em_project_backproject(self.h, _ptr(counts), _counts_dtype(counts), int(counts_packed),
+                                                    _ptr(add), _ptr(x), _ptr(bp), subset, nsubsets, _ptr(lik),
+                                                    _stream(stream)))
+        return bp
+
+    def em_pass_host(self, h_counts_subset, stage, x, bp, sens, subset, nsubsets, h_x_out, h_lik=None,
+                     thr_value=0.0, ge=True, stream=None):
+        """em_pass from host counts (packed subset, numpy) to a host image; blocks until done."""
+        dt = {"float32": _lib.APIRL_F32, "uint32": _lib.APIRL_U32, "uint16": _lib.APIRL_U16}[str(h_counts_subset.dtype)]
+        check(self.lib.apirl_em_pass_host(self.h, ctypes.c_void_p(h_counts_subset.ctypes.data), dt, _ptr(stage),
+                                          _ptr(x), _ptr(bp), _ptr(sens), float(thr_value), int(ge), subset, nsubsets,
+                                          ctypes.c_void_p(h_x_out.ctypes.data),
+                                          None if h_lik is None else ctypes.c_void_p(h_lik.ctypes.data),
+                                          _stream(stream)))
+        return h_x_out
+
+
+# ---- bin-wise / pixel-wise steps (device tensors) -------------------------
+def inverse_divide(meas, est, stream=None):
+    lib = _lib.load()
+    check(lib.apirl_inverse_divide(est.numel(), _ptr(meas), _ptr(est), _stream(stream)))
+    return est
+
+
+def add_bins(add, est, stream=None):
+    lib = _lib.load()
+    check(lib.apirl_add_bins(est.numel(), _ptr(add), _ptr(est), _stream(stream)))
+    return est
+
+
+def likelihood(est, meas, gt0=False, stream=None):
+    import torch
+    lib = _lib.load()
+    out = torch.zeros(1, dtype=torch.float64, device=est.device)
+    check(lib.apirl_likelihood(est.numel(), _ptr(est), _ptr(meas), int(gt0), _ptr(out), _stream(stream)))
+    return out
+
+
+def mlem_threshold(sens, stream=None):
+    import torch
+    lib = _lib.load()
+    out = torch.zeros(1, dtype=torch.float32, device=sens.device)
+    check(lib.apirl_mlem_threshold(sens.numel(), _ptr(sens), _ptr(out), _stream(stream)))
+    return out
+
+
+def update_pixels(x, bp, sens, thr=None, thr_value=0.0, ge=True, zero_bp=False, stream=None):
+    lib = _lib.load()
+    check(lib.apirl_update_pixels(x.numel(), _ptr(x), _ptr(bp), _ptr(sens), _ptr(thr), float(thr_value), int(ge),
+                                  int(zero_bp), _stream(stream)))
+    return x
+
+
+def force_positive(x, stream=None):
+    lib = _lib.load()
+    check(lib.apirl_force_positive(x.numel(), _ptr(x), _stream(stream)))
+    return x
+
+
+# ---- whole reconstructions (host arrays) ----------------------------------
+def _np_ptr(a):
+    return None if a is None else a.ctypes.data_as(ctypes.c_void_p)
+
+
+def _f32(a):
+    return None if a is None else np.ascontiguousarray(a, dtype=np.float32)
+
+
+def osem_3d(image_geom, sino_geom, meas, init, iters, nsubsets, mult=None, add=None, device=0):
+    """OsemSinogram3d::Reconstruct on the GPU.  Returns (image, likelihood[iters*nsubsets+1], sens of subset 0)."""
+    lib = _lib.load()
+    meas, init, mult, add = _f32(meas), _f32(init), _f32(mult), _f32(add)
+    out = np.zeros(image_geom.n_voxels, np.float32)
+    lik = np.zeros(iters * nsubsets + 1, np.float64)
+    sens0 = np.zeros(image_geom.n_voxels, np.float32)
+    ig, sc = _img_c(image_geom), _sino3d_c(sino_geom)
+    check(lib.apirl_osem_3d(ctypes.byref(ig), ctypes.byref(sc), _np_ptr(meas), _np_ptr(mult), _np_ptr(add),
+                            _np_ptr(init), iters, nsubsets, device, _np_ptr(out), _np_ptr(lik), _np_ptr(sens0)))
+    return out, lik, sens0
+
+
+def mlem_3d(image_geom, sino_geom, meas, init, iters, mult=None, add=None, device=0):
+    lib = _lib.load()
+    meas, init, mult, add = _f32(meas), _f32(init), _f32(mult), _f32(add)
+    out = np.zeros(image_geom.n_voxels, np.float32)
+    lik = np.zeros(iters + 1, np.float64)
+    sens = np.zeros(image_geom.n_voxels, np.float32)
+    ig, sc = _img_c(image_geom), _sino3d_c(sino_geom)
+    check(lib.apirl_mlem_3d(ctypes.byref(ig), ctypes.byref(sc), _np_ptr(meas), _np_ptr(mult), _np_ptr(add),
+                            _np_ptr(init), iters, device, _np_ptr(out), _np_ptr(lik), _np_ptr(sens)))
+    return out, lik, sens
+
+
+def mlem_2d(image_geom, sino_geom, meas, init, iters, mult=None, add=None, device=0):
+    lib = _lib.load()
+    meas, init, mult, add = _f32(meas), _f32(init), _f32(mult), _f32(add)
+    out = np.zeros(image_geom.n_voxels, np.float32)
+    lik = np.zeros(iters + 1, np.float64)
+    sens = np.zeros(image_geom.n_voxels, np.float32)
+    ig, sc = _img_c(image_geom), _sino2d_c(sino_geom)
+    check(lib.apirl_mlem_2d(ctypes.byref(ig), ctypes.byref(sc), _np_ptr(meas), _np_ptr(mult), _np_ptr(add),
+                            _np_ptr(init), iters, device, _np_ptr(out), _np_ptr(lik), _np_ptr(sens)))
+    return out, lik, sens

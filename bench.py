@@ -1,0 +1,426 @@
+"""Benchmark: 3D OSEM sub-iterations per second on the full 3D workload.
+
+Workload (one "step" = one OSEM sub-iteration): image 256x256x81 (2.08 x 2.08 x
+2.03 mm), 41 rings, span-1 sinograms of all ring pairs with |ring difference|
+<= 20 (1261 sinograms of 336 r x 336 angles, 142,361,856 bins), 21 subsets of
+16 angles; water cylinder with 6 hot spheres, attenuation factors in the
+sensitivity, 5e8 Poisson counts stored as uint32.  Steps cycle through the
+21 subsets as an OSEM iteration does.
+
+Arms
+  default            the CUDA path (fused projection/ratio/backprojection kernel
+                     + pixel update), counts and images resident in HBM.
+  --impl reference   the reference APIRL CPU code (oracle/_ref, compiled from the
+                     reference sources) on the host cores, or the oracle
+                     restatement where the reference was not built; each step is
+                     one sub-iteration restricted to a sample of segments.
+
+Multi-GPU: the job does not exchange data between GPUs; each rank runs its own
+replica of the reconstruction and `value` sums the ranks' sub-iterations over
+the slowest rank's time.
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "OSEM subiters/s (256²×81)"
+UNIT = "subiter/s"
+NSUB = 21
+TOTAL_COUNTS = 5e8
+L2_FLUSH_BYTES = 256 << 20
+WORKLOAD = ("3D OSEM 256x256x81 image, 41 rings span-1 |rd|<=20: 1261 sinograms x 336 angles x 336 r, "
+            "21 subsets, attenuation in sensitivity, 5e8 counts uint32")
+
+
+def peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            p = json.load(f)
+        return float(p["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+# ---------------------------------------------------------------------------
+class ClockSampler:
+    """nvidia-smi clock / throttle samples taken while the timed region runs."""
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.gpu = gpu_index
+        self.proc = None
+        self.path = os.path.join("/tmp", f"apirl_clocks_{os.getpid()}.csv")
+
+    def start(self):
+        try:
+            self.f = open(self.path, "w")
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={self.Q}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=self.f, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        self.f.close()
+        sm, smax, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in open(self.path):
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                smax.append(float(parts[2]))
+            except ValueError:
+                continue
+            for n, v in zip(names, parts[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(n)
+        os.unlink(self.path)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(smax) if smax else None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+# ---------------------------------------------------------------------------
+def setup_workload(dev, log):
+    """Builds the resident state of the 3D OSEM job on `dev` (outside timing)."""
+    import torch
+    import apirl_b200 as ap
+    from apirl_b200 import workloads
+
+    ig, sg = workloads.c2_geometry()
+    P = ap.SiddonProjector(ig, sg, device=dev.index)
+    nb = P.num_bins()
+    lor, z = P.tables()
+    t0 = time.time()
+    phantom = torch.from_numpy(workloads.cylinder_phantom_3d(ig, seed=2)).to(dev)
+    chords = workloads.cylinder_chords(lor, z)                      # FP64 on the host
+    atten = torch.from_numpy(np.exp(-workloads.MU_WATER_PER_MM * chords).astype(np.float32).reshape(-1)).to(dev)
+    del chords
+    expected = torch.empty(nb, dtype=torch.float32, device=dev)
+    P.project(phantom, expected)
+    expected.mul_(atten)
+    expected.mul_(TOTAL_COUNTS / float(expected.double().sum().item()))
+    gen = torch.Generator(device=dev).manual_seed(0)
+    counts = torch.poisson(expected, generator=gen).to(torch.int32).view(torch.uint32)
+    del expected
+    nv = ig.n_voxels
+    sens = torch.zeros((NSUB, nv), dtype=torch.float32, device=dev)
+    for s in range(NSUB):
+        # OsemSinogram3d::computeSensitivity with the multiplicative term:
+        # sens_s = A_s^T (attenuation of subset s), then forcePositive.
+        a_s = atten.view(sg.n_sinos, sg.n_proj, sg.n_r)[:, s::NSUB, :].contiguous().view(-1)
+        P.backproject(a_s, sens[s], s, NSUB)
+        ap.force_positive(sens[s])
+    x = torch.ones(nv, dtype=torch.float32, device=dev)
+    bp = torch.zeros(nv, dtype=torch.float32, device=dev)
+    # Siddon segments per subset (all bins: forward; bins with counts: backward).
+    fwd, bwd = [], []
+    cv = counts.view(torch.int32).view(sg.n_sinos, sg.n_proj, sg.n_r)
+    for s in range(NSUB):
+        st = P.count_steps(s, NSUB).view(sg.n_sinos, -1, sg.n_r).long()
+        fwd.append(int(st.sum().item()))
+        bwd.append(int(st[cv[:, s::NSUB, :] != 0].sum().item()))
+    torch.cuda.synchronize(dev)
+    log(f"setup {time.time() - t0:.1f} s: {nb} bins, counts {int(counts.view(torch.int32).sum().item())}, "
+        f"fwd segments/subset {statistics.mean(fwd):.4g}, bwd {statistics.mean(bwd):.4g}")
+    return dict(P=P, ig=ig, sg=sg, counts=counts, sens=sens, x=x, bp=bp, fwd=fwd, bwd=bwd, atten=atten)
+
+
+def step_bytes(w, s):
+    """Algorithmic HBM bytes of one sub-iteration: fp32 voxel read per forward
+    segment, read-modify-write per backward segment, the uint32 count per bin
+    (fused kernel), and 20 B per voxel for the update (x r/w, bp r, sens r, bp clear)."""
+    nbins = w["sg"].n_sinos * w["sg"].subset_nproj(s, NSUB) * w["sg"].n_r
+    kern = 4 * w["fwd"][s] + 8 * w["bwd"][s] + 4 * nbins
+    return kern, kern + 20 * w["ig"].n_voxels
+
+
+def run_gpu(args):
+    import torch
+    import torch.distributed as dist
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        torch.cuda.set_device(local)
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    dev = torch.device(f"cuda:{local}")
+    torch.cuda.set_device(dev)
+    log = (lambda m: print(f"[bench] {m}", file=sys.stderr, flush=True)) if rank == 0 else (lambda m: None)
+
+    import apirl_b200 as ap
+    ap.load_library()
+    w = setup_workload(dev, log)
+    P, counts, sens, x, bp = w["P"], w["counts"], w["sens"], w["x"], w["bp"]
+    stream = torch.cuda.Stream(device=dev)
+    flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.float32, device=dev)
+    lik = torch.zeros(1, dtype=torch.float64, device=dev)
+
+    def step(s, evs=None):
+        if evs:
+            evs[0].record(stream)
+        P.em_project_backproject(counts, x, bp, s, NSUB, lik=lik, stream=stream)
+        if evs:
+            evs[1].record(stream)
+        ap.update_pixels(x, bp, sens[s], thr_value=0.0, ge=True, zero_bp=True, stream=stream)
+        if evs:
+            evs[2].record(stream)
+
+    with torch.cuda.stream(stream):
+        for i in range(args.warmup):
+            step(i % NSUB)
+        torch.cuda.synchronize(dev)
+        if world > 1:
+            dist.barrier()
+        torch.cuda.synchronize(dev)
+        clocks = ClockSampler(local)
+        clocks.start()
+        evs = [[torch.cuda.Event(enable_timing=True) for _ in range(3)] for _ in range(args.steps)]
+        subs = [(args.warmup + i) % NSUB for i in range(args.steps)]
+        for i in range(args.steps):
+            flush.zero_()                      # L2 flush between timed steps, outside the events
+            step(subs[i], evs[i])
+        torch.cuda.synchronize(dev)
+        if world > 1:
+            dist.barrier()
+        clock = clocks.stop()
+    step_ms = [evs[i][0].elapsed_time(evs[i][2]) for i in range(args.steps)]
+    kern_ms = [evs[i][0].elapsed_time(evs[i][1]) for i in range(args.steps)]
+    total_ms = sum(step_ms)
+    if world > 1:
+        t = torch.tensor([total_ms], dtype=torch.float64, device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        total_ms = float(t.item())
+    value = args.steps * world / (total_ms / 1e3)
+
+    kb = [step_bytes(w, s) for s in subs]
+    kern_bytes = statistics.mean(k for k, _ in kb)
+    kern_s = statistics.mean(kern_ms) / 1e3
+    peak, peak_kind = peaks()
+    achieved = kern_bytes / kern_s / 1e9
+    gsteps = sum(w["fwd"][s] + w["bwd"][s] for s in subs) / (total_ms / 1e3) / 1e9 * world
+
+    # End-to-end through the C ABI with host buffers: the sub-iteration's packed
+    # counts go host->device from pinned memory, the updated image and the
+    # likelihood come back, every step.
+    e2e = None
+    if rank == 0 or world > 1:
+        sg = w["sg"]
+        import torch as _t
+        cv = counts.view(_t.int32).view(sg.n_sinos, sg.n_proj, sg.n_r)
+        host_counts = [cv[:, s::NSUB, :].contiguous().view(-1).cpu().pin_memory().numpy().view(np.uint32)
+                       for s in range(NSUB)]
+        stage = _t.empty(host_counts[0].size, dtype=_t.int32, device=dev)
+        h_x = _t.empty(w["ig"].n_voxels, dtype=_t.float32).pin_memory().numpy()
+        h_lik = np.zeros(1, np.float64)
+        for i in range(min(args.warmup, 3)):
+            P.em_pass_host(host_counts[i % NSUB], stage, x, bp, sens[i % NSUB], i % NSUB, NSUB, h_x, h_lik,
+                           stream=stream)
+        ev = [_t.cuda.Event(enable_timing=True) for _ in range(2)]
+        torch.cuda.synchronize(dev)
+        e_ms = 0.0
+        for i in range(args.steps):
+            s = (args.warmup + i) % NSUB
+            ev[0].record(stream)
+            P.em_pass_host(host_counts[s], stage, x, bp, sens[s], s, NSUB, h_x, h_lik, stream=stream)
+            ev[1].record(stream)
+            ev[1].synchronize()
+            e_ms += ev[0].elapsed_time(ev[1])
+        if world > 1:
+            t = torch.tensor([e_ms], dtype=torch.float64, device=dev)
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            e_ms = float(t.item())
+        e2e = {"value": args.steps * world / (e_ms / 1e3), "unit": UNIT,
+               "h2d_bytes_per_step": int(host_counts[0].nbytes), "d2h_bytes_per_step": int(h_x.nbytes + 8),
+               "api": "apirl_em_pass_host (C ABI, pinned host counts in, host image + likelihood out)"}
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        cpu = cpu_baseline(w, log, budget_s=args.cpu_seconds)
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded phantom, Poisson counts)",
+            "config": {"workload": WORKLOAD, "subsets": NSUB, "counts_dtype": "uint32",
+                       "l2": "flushed between timed steps (256 MB write outside the timed events)",
+                       "parallelism": f"replicas x{world}"},
+            "siddon_gsteps_per_s": gsteps,
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": achieved / peak, "traffic": args.traffic_bytes,
+                         "kernel": "k_em_pass (fused projection / ratio / backprojection)",
+                         "algorithmic_bytes_per_launch": kern_bytes, "kernel_ms": kern_s * 1e3,
+                         "peak_source": f"{peak_kind} hbm_gbs"},
+            "e2e": e2e,
+            "cpu_baseline": cpu,
+            "gpu_launches": 3 * args.steps,
+            "clocks": clock,
+        }
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+# ---------------------------------------------------------------------------
+# CPU side: the reference APIRL code on a sample of the same sub-iteration.
+SAMPLE_SEGMENTS = [0, 7, -7, 14, -14]
+
+
+def _sample_geometry(sg):
+    from apirl_b200.geometry import Sino3DGeom
+    return Sino3DGeom(sg.n_proj, sg.n_r, sg.n_rings, sg.r_fov, sg.axial_fov, sg.r_scanner,
+                      list(SAMPLE_SEGMENTS), list(SAMPLE_SEGMENTS))
+
+
+def _sample_counts(sg, counts_full):
+    """Counts of the sampled segments, in the sample sinogram's layout."""
+    off, parts = 0, {}
+    for rd, n in zip(sg.min_rd, sg.sinos_per_segment):
+        parts[rd] = (off, n)
+        off += n
+    per = sg.n_proj * sg.n_r
+    chunks = [counts_full[parts[rd][0] * per:(parts[rd][0] + parts[rd][1]) * per] for rd in SAMPLE_SEGMENTS]
+    return np.concatenate(chunks).astype(np.float32)
+
+
+class CpuSample:
+    """One sub-iteration (subset 0 of 21) of the reference code restricted to
+    the segments SAMPLE_SEGMENTS; `fraction` is the sample's share of the full
+    sub-iteration's Siddon segments, so subiter/s = fraction / seconds."""
+
+    def __init__(self, counts, log):
+        """counts: the sampled segments' counts in the sample sinogram's layout."""
+        sys.path.insert(0, os.path.join(ROOT, "tests"))
+        from oracle_lib import RefHarness, Oracle, REF_SO
+        from apirl_b200 import workloads
+        self.ig, self.sg = workloads.c2_geometry()
+        self.sample = _sample_geometry(self.sg)
+        counts = np.ascontiguousarray(counts, np.float32)
+        oracle = Oracle()
+        full_steps = oracle.count_steps_3d(self.sg, self.ig, 0, NSUB)
+        samp_steps = oracle.count_steps_3d(self.sample, self.ig, 0, NSUB)
+        self.fraction = samp_steps / full_steps
+        self.cores = os.cpu_count() or 1
+        if os.path.exists(REF_SO):
+            self.kind = "reference"
+            self.R = RefHarness()
+            self.R.set_threads(self.cores)
+            self.h = self.R.sino3d(self.sample, counts)
+        else:
+            self.kind = "port"
+            self.R = None
+            self.oracle = oracle
+            self.counts = counts
+        self.x = np.ones(self.ig.n_voxels, np.float32)
+        self.sens = np.ones(self.ig.n_voxels, np.float32)
+        log(f"cpu sample: segments {SAMPLE_SEGMENTS}, {self.sample.n_sinos} sinograms, "
+            f"{self.fraction:.4f} of a sub-iteration's segments, kind {self.kind}, {self.cores} threads")
+
+    def run(self):
+        t0 = time.perf_counter()
+        if self.R is not None:
+            self.R.osem_subiteration(self.h, self.ig, 0, NSUB, self.x, self.sens)
+        else:
+            o, sg, ig = self.oracle, self.sample, self.ig
+            est = o.project_3d(sg, ig, self.x, 0, NSUB)
+            m = self.counts.reshape(sg.n_sinos, sg.n_proj, sg.n_r)[:, 0::NSUB, :].reshape(-1)
+            ratio = o.inverse_divide(m, est)
+            bp = o.backproject_3d(sg, ig, ratio, 0, NSUB)
+            self.x = o.update(self.x, bp, self.sens, np.float32(0), True)
+        return time.perf_counter() - t0
+
+    def describe(self):
+        return (f"OSEM sub-iteration 0/21 of the full workload restricted to segments {SAMPLE_SEGMENTS} "
+                f"({self.sample.n_sinos} of 1261 sinograms, {self.fraction:.4f} of the sub-iteration's Siddon "
+                f"segments); value scaled to whole sub-iterations")
+
+
+def cpu_baseline(w, log, budget_s=15.0):
+    counts_full = w["counts"].view(__import__("torch").int32).cpu().numpy()
+    cs = CpuSample(_sample_counts(w["sg"], counts_full), log)
+    times = [cs.run()]
+    while sum(times) < budget_s and len(times) < 20:
+        times.append(cs.run())
+    sec = statistics.median(times)
+    return {"value": cs.fraction / sec, "unit": UNIT, "cores": cs.cores, "kind": cs.kind,
+            "sample": cs.describe() + f"; median of {len(times)} runs, {sec:.2f} s each"}
+
+
+def run_reference(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    log = lambda m: print(f"[bench-ref] {m}", file=sys.stderr, flush=True)
+    from apirl_b200 import workloads
+    ig, sg = workloads.c2_geometry()
+    # Counts of the same phantom for the sampled segments, generated on the host
+    # (this arm does not touch the GPU): expected values from the oracle's
+    # projection, scaled to the full job's mean of 5e8 / 142,361,856 per bin.
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    from oracle_lib import Oracle
+    o = Oracle()
+    sample = _sample_geometry(sg)
+    lam = o.project_3d(sample, ig, workloads.cylinder_phantom_3d(ig, seed=2)).astype(np.float64)
+    lam *= (TOTAL_COUNTS / float(sg.n_bins)) * lam.size / max(float(lam.sum()), 1.0)
+    counts = np.random.default_rng(0).poisson(lam).astype(np.float32)
+    cs = CpuSample(counts, log)
+    for _ in range(args.warmup):
+        cs.run()
+    times = [cs.run() for _ in range(args.steps)]
+    total = sum(times)
+    value = args.steps * cs.fraction / total
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": 0, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": total / args.steps / cs.fraction * 1e3, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded phantom, Poisson counts)",
+        "config": {"workload": WORKLOAD, "subsets": NSUB, "parallelism": f"{cs.cores} host threads (OpenMP)"},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": cs.cores, "kind": cs.kind, "sample": cs.describe()},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    ap_ = argparse.ArgumentParser(description=__doc__.split("\n")[0])
+    ap_.add_argument("--gpus", type=int, default=1)
+    ap_.add_argument("--steps", type=int, default=42)
+    ap_.add_argument("--warmup", type=int, default=5)
+    ap_.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap_.add_argument("--no-cpu-baseline", action="store_true")
+    ap_.add_argument("--cpu-seconds", type=float, default=15.0)
+    ap_.add_argument("--traffic-bytes", type=float, default=None,
+                     help="DRAM bytes per fused-kernel launch from an ncu capture, reported as roofline.traffic")
+    args = ap_.parse_args()
+    if args.warmup < 3 and args.impl != "reference":
+        args.warmup = 3
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_gpu(args)
+
+
+if __name__ == "__main__":
+    main()

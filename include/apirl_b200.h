@@ -1,0 +1,205 @@
+/*
+ * apirl_b200 -- B200-native Siddon projector / backprojector and the MLEM /
+ * OSEM update around it, as a C ABI.
+ *
+ * Every entry point replaces one operation of the reference APIRL CPU path;
+ * the reference interface each one stands in for is cited beside it
+ * (paths are relative to the APIRL source tree).
+ *
+ * Conventions
+ *  - Status codes: APIRL_OK (0) or one of the APIRL_ERR_* values; the message
+ *    of the last failure on the calling thread is apirl_last_error().  Nothing
+ *    here calls exit() (the reference's checkCudaErrors does).
+ *  - Pointers named d_* are device pointers on the projector's device; h_*
+ *    are host pointers.  `stream` is a cudaStream_t passed as void* (NULL =
+ *    the legacy default stream).  Device-pointer calls are asynchronous.
+ *  - Images are float32 [z][y][x] (Image::pixels, data/inc/Images.h:166).
+ *    2D sinograms are float32 [angle][r]; 3D sinograms are
+ *    [segment][sinogram][angle][r] with the segment's sinograms in the order
+ *    Sinogram3D::readFromInterfile builds them (data/src/Sinogram3D.cpp:396-464).
+ *  - Subsets: `subset` in [0, nsubsets) selects angles subset, subset+nsubsets,
+ *    ... (Sinogram3DCylindricalPet::getSubset, data/src/Sinogram3DCylindricalPet.cpp:164-197);
+ *    subset < 0 means all angles.  A subset sinogram is laid out
+ *    [sinogram][subset angle][r] and has apirl_projector_num_bins() bins.
+ *  - Voxel indices of Siddon segments are checked against all image bounds.
+ *    (The reference checks only one side in its Project: SiddonProjector.cpp:178, :417.)
+ */
+#ifndef APIRL_B200_H
+#define APIRL_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef int apirl_status;
+enum {
+  APIRL_OK = 0,
+  APIRL_ERR_INVALID = 1,       /* bad geometry, size, pointer or argument */
+  APIRL_ERR_CUDA = 2,          /* a CUDA runtime call failed */
+  APIRL_ERR_OOM = 3,           /* device allocation failed */
+  APIRL_ERR_NOT_SUPPORTED = 4, /* option not available on this path */
+  APIRL_ERR_ABORTED = 5        /* cancelled or timed out */
+};
+
+/* Element type of a measured-counts sinogram. */
+enum { APIRL_F32 = 0, APIRL_U32 = 1, APIRL_U16 = 2 };
+
+/* SizeImage (data/inc/Images.h:53-61). */
+typedef struct apirl_image_geom {
+  int nx, ny, nz;
+  float dx, dy, dz; /* voxel size in mm */
+} apirl_image_geom;
+
+/* Sinogram2DinCylindrical3Dpet(nProj, nR, rFov_mm, rScanner_mm)
+ * (data/src/Sinogram2DinCylindrical3Dpet.cpp:29-64). */
+typedef struct apirl_sino2d_geom {
+  int n_proj, n_r;
+  float r_fov, r_scanner; /* mm */
+} apirl_sino2d_geom;
+
+/* Sinogram3DCylindricalPet(header, rFov_mm, zFov_mm, rScanner_mm) with the
+ * header's segment table (data/src/Sinogram3D.cpp:106-471). */
+typedef struct apirl_sino3d_geom {
+  int n_proj, n_r, n_rings, n_segments;
+  float r_fov, axial_fov, r_scanner; /* mm */
+  const int* min_ring_diff;          /* n_segments entries */
+  const int* max_ring_diff;          /* n_segments entries */
+} apirl_sino3d_geom;
+
+typedef struct apirl_projector apirl_projector;
+
+const char* apirl_last_error(void);
+const char* apirl_version(void);
+
+/* ---- host-only geometry (no device needed) -------------------------------
+ * The LOR end-point table [angle][r][p1x,p1y,p2x,p2y] built with the
+ * reference's float expressions: r and angle tables of
+ * Sinogram2DinCylindrical3Dpet (data/src/Sinogram2DinCylindrical3Dpet.cpp:46-63)
+ * and getPointsFromLor (:216-266). */
+apirl_status apirl_lor_table(int n_proj, int n_r, float r_fov, float r_scanner, float* h_lor);
+/* Number of sinograms of a 3D geometry and, when h_z is not NULL, their
+ * end-point z ([sinogram][z1,z2]) as SiddonProjector::Project sets them
+ * (recon/src/SiddonProjector.cpp:357-360, :392-396 over the ring pairs of
+ * data/src/Sinogram3D.cpp:396-464). */
+int apirl_sino3d_ring_z(const apirl_sino3d_geom* sino, float* h_z);
+
+/* ---- projector set-up ---------------------------------------------------
+ * SiddonProjector(1, 1) bound to one image and one sinogram geometry
+ * (recon/inc/SiddonProjector.h:43-47).  Builds the LOR end-point table on the
+ * host with the reference's float expressions
+ * (Sinogram2DinCylindrical3Dpet::getPointsFromLor, .cpp:216-266) and keeps it,
+ * the per-sinogram ring z and scratch space resident on `device`. */
+apirl_status apirl_projector_create_2d(const apirl_image_geom* img, const apirl_sino2d_geom* sino, int device,
+                                       apirl_projector** out);
+apirl_status apirl_projector_create_3d(const apirl_image_geom* img, const apirl_sino3d_geom* sino, int device,
+                                       apirl_projector** out);
+void apirl_projector_destroy(apirl_projector* p);
+/* Bins of one subset (subset < 0: whole sinogram). */
+int64_t apirl_projector_num_bins(const apirl_projector* p, int subset, int nsubsets);
+int apirl_projector_num_sinograms(const apirl_projector* p);
+/* Copies the host-built LOR table ([angle][r][p1x,p1y,p2x,p2y]) and, for 3D,
+ * the per-sinogram end-point z ([sinogram][z1,z2]); either may be NULL. */
+apirl_status apirl_projector_tables(const apirl_projector* p, float* h_lor, float* h_z);
+/* Number of Siddon segments of every bin of a subset, written to d_steps (int32). */
+apirl_status apirl_count_steps(apirl_projector* p, int subset, int nsubsets, int32_t* d_steps, void* stream);
+
+/* ---- projector operations (device pointers) ------------------------------ */
+/* SiddonProjector::Project: d_sino = A d_image (recon/src/SiddonProjector.cpp:322-441
+ * for 3D, :146-193 for 2D; 2D bins whose r exceeds the sinogram rFov are left
+ * untouched, as the reference leaves them). */
+apirl_status apirl_project(apirl_projector* p, const float* d_image, float* d_sino, int subset, int nsubsets,
+                           void* stream);
+/* SiddonProjector::Backproject: d_image += A^T d_sino (:444-568 for 3D, :34-87
+ * for 2D).  Accumulates into d_image, as the reference does. */
+apirl_status apirl_backproject(apirl_projector* p, const float* d_sino, float* d_image, int subset, int nsubsets,
+                               void* stream);
+/* SiddonProjector::DivideAndBackproject: d_image += A^T (d_meas / d_est)
+ * (:571-704 for 3D, :90-144 for 2D, with each reference's zero rules). */
+apirl_status apirl_divide_and_backproject(apirl_projector* p, const float* d_meas, const float* d_est,
+                                          float* d_image, int subset, int nsubsets, void* stream);
+
+/* ---- bin-wise and pixel-wise steps --------------------------------------- */
+/* Sinogram3D::inverseDivideBinToBin: d_est = (m != 0 && e != 0) ? m / e : 0
+ * (data/src/Sinogram3D.cpp:830-855, Sinogram2D.cpp:245-266). */
+apirl_status apirl_inverse_divide(int64_t n, const float* d_meas, float* d_est, void* stream);
+/* Sinogram3D::addBinToBin: d_est += d_add (data/src/Sinogram3D.cpp:857-873). */
+apirl_status apirl_add_bins(int64_t n, const float* d_add, float* d_est, void* stream);
+/* Sinogram{2D,3D}::getLikelihoodValue: sum of m*log(e) - e over bins with
+ * e > 0 (gt0 = 1, 2D: Sinogram2D.cpp:565-581) or e != 0 (gt0 = 0, 3D:
+ * Sinogram3D.cpp:584-606), accumulated in FP64 and written to *d_out (device double). */
+apirl_status apirl_likelihood(int64_t n, const float* d_est, const float* d_meas, int gt0, double* d_out,
+                              void* stream);
+/* Mlem::updateUpdateThreshold: min over non-zero pixels + 1e-4 (max - min)
+ * (recon/src/Mlem.cpp:39-43, data/src/Images.cpp:397-433), written to *d_thr. */
+apirl_status apirl_mlem_threshold(int64_t n, const float* d_sens, float* d_thr, void* stream);
+/* EM pixel update: x = (sens >= thr | sens > thr) ? x * bp / sens : 0
+ * (recon/src/MlemSinogram3d.cpp:228-242 and OsemSinogram3d.cpp:217-237 use >=,
+ * Mlem2d.cpp:171-185 uses >).  thr is *d_thr when d_thr is not NULL, else
+ * thr_value.  With zero_bp != 0 the kernel also clears d_bp for the next pass. */
+apirl_status apirl_update_pixels(int64_t n, float* d_x, float* d_bp, const float* d_sens, const float* d_thr,
+                                 float thr_value, int ge, int zero_bp, void* stream);
+/* Image::forcePositive (data/src/Images.cpp:383-395). */
+apirl_status apirl_force_positive(int64_t n, float* d_x, void* stream);
+
+/* ---- fused EM pass --------------------------------------------------------
+ * One OSEM sub-iteration of OsemSinogram3d::Reconstruct
+ * (recon/src/OsemSinogram3d.cpp:159-237) -- or one MLEM iteration of
+ * Mlem2d::Reconstruct (recon/src/Mlem2d.cpp:146-185) for a 2D projector -- in
+ * two kernels: per bin, project the ray through d_x, add d_add, add the
+ * likelihood term, form the ratio m / e and backproject it into d_bp; then
+ * update d_x with d_sens and clear d_bp.  No estimated sinogram is stored.
+ *   d_counts : measured sinogram, element type counts_dtype; counts_packed = 0
+ *              means the whole sinogram (angles indexed as in the full
+ *              sinogram), 1 means the subset sinogram only.
+ *   d_add    : additive term laid out like d_counts (float), or NULL.
+ *   d_bp     : zero on entry, zero again on return.
+ *   d_lik    : receives the FP64 likelihood of this pass (device double), or NULL.
+ *   thr/ge   : as for apirl_update_pixels (d_thr may be NULL).
+ */
+apirl_status apirl_em_pass(apirl_projector* p, const void* d_counts, int counts_dtype, int counts_packed,
+                           const float* d_add, float* d_x, float* d_bp, const float* d_sens, const float* d_thr,
+                           float thr_value, int ge, int subset, int nsubsets, double* d_lik, void* stream);
+
+/* The first kernel of apirl_em_pass alone: project, add, likelihood, ratio and
+ * backprojection into d_bp, without the pixel update (d_x is only read). */
+apirl_status apirl_em_project_backproject(apirl_projector* p, const void* d_counts, int counts_dtype,
+                                          int counts_packed, const float* d_add, const float* d_x, float* d_bp,
+                                          int subset, int nsubsets, double* d_lik, void* stream);
+
+/* The same pass with HOST inputs and outputs: copies this pass's subset
+ * counts (packed, from pinned or pageable host memory) to the device, runs
+ * apirl_em_pass on the projector's resident image / sensitivity buffers, and
+ * copies the updated image and the likelihood back.  d_x, d_bp, d_sens are
+ * device buffers the caller keeps resident between passes. */
+apirl_status apirl_em_pass_host(apirl_projector* p, const void* h_counts_subset, int counts_dtype, void* d_counts_stage,
+                                float* d_x, float* d_bp, const float* d_sens, float thr_value, int ge, int subset,
+                                int nsubsets, float* h_x_out, double* h_lik, void* stream);
+
+/* ---- whole reconstructions (host buffers) --------------------------------
+ * OsemSinogram3d::Reconstruct (recon/src/OsemSinogram3d.cpp:36-325): per-subset
+ * sensitivity = A_s^T (h_mult or 1), forcePositive, threshold 0 with >=, then
+ * iters x nsubsets fused passes, each captured once as a CUDA graph and
+ * replayed.  h_lik receives iters*nsubsets+1 values (the last one for the
+ * whole-sinogram projection of the result).  h_mult / h_add may be NULL. */
+apirl_status apirl_osem_3d(const apirl_image_geom* img, const apirl_sino3d_geom* sino, const float* h_meas,
+                           const float* h_mult, const float* h_add, const float* h_init, int iters, int nsubsets,
+                           int device, float* h_out, double* h_lik, float* h_sens0);
+/* MlemSinogram3d::Reconstruct (recon/src/MlemSinogram3d.cpp:89-310): threshold
+ * from the sensitivity image, >= update; h_lik gets iters+1 values. */
+apirl_status apirl_mlem_3d(const apirl_image_geom* img, const apirl_sino3d_geom* sino, const float* h_meas,
+                           const float* h_mult, const float* h_add, const float* h_init, int iters, int device,
+                           float* h_out, double* h_lik, float* h_sens);
+/* Mlem2d::Reconstruct (recon/src/Mlem2d.cpp:60-278): > update; h_lik gets
+ * iters+1 values, the last evaluated on the ratio sinogram as the reference
+ * does (Mlem2d.cpp:228). */
+apirl_status apirl_mlem_2d(const apirl_image_geom* img, const apirl_sino2d_geom* sino, const float* h_meas,
+                           const float* h_mult, const float* h_add, const float* h_init, int iters, int device,
+                           float* h_out, double* h_lik, float* h_sens);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* APIRL_B200_H */

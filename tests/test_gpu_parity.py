@@ -1,0 +1,326 @@
+"""Parity of the CUDA path with the oracle (and, through the golden fixtures,
+with the reference APIRL code).  Every call goes through the C ABI.
+
+Tolerances
+  forward projection ..... bit-exact (same float operations, same order)
+  backprojection ......... rel L2 <= 1e-5 (fp32 atomics accumulate in another order)
+  adjoint <Ax,y> vs <x,A^T y> ... rel <= 1e-6 (FP64 dot products of fp32 results)
+  reconstructions ........ rel L2 <= 1e-4 after the stated iterations
+  likelihood (FP64) ...... rel <= 1e-9 against the oracle's FP64 sum of the GPU estimates
+"""
+import hashlib
+import json
+import os
+
+import numpy as np
+import pytest
+
+torch = pytest.importorskip("torch")
+pytestmark = pytest.mark.gpu
+
+import apirl_b200 as ap  # noqa: E402
+from apirl_b200 import workloads  # noqa: E402
+from apirl_b200.geometry import ImageGeom, Sino2DGeom, Sino3DGeom  # noqa: E402
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+G = np.load(os.path.join(HERE, "golden", "golden_small.npz"))
+with open(os.path.join(HERE, "golden", "golden_c2.json")) as f:
+    C2 = json.load(f)
+DEV = torch.device("cuda:0")
+
+
+def sha(a):
+    return hashlib.sha256(np.ascontiguousarray(a).tobytes()).hexdigest()
+
+
+def t(a, dtype=None):
+    return torch.from_numpy(np.ascontiguousarray(a if dtype is None else a.astype(dtype))).to(DEV)
+
+
+def rel(a, b):
+    a = np.asarray(a, np.float64)
+    b = np.asarray(b, np.float64)
+    return float(np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-300))
+
+
+def bits_equal(a, b):
+    return np.array_equal(np.ascontiguousarray(a, np.float32).view(np.uint32),
+                          np.ascontiguousarray(b, np.float32).view(np.uint32))
+
+
+def small_3d():
+    return ImageGeom(48, 48, 9, 2.08, 2.08, 2.03), Sino3DGeom.span1(25, 48, 5, 72.0, 5 * 4.054, 150.0, 3)
+
+
+@pytest.fixture(scope="module", autouse=True)
+def _gpu():
+    if not torch.cuda.is_available():
+        pytest.skip("no CUDA device")
+    ap.load_library()
+
+
+# ---------------------------------------------------------------------------
+def test_tables_equal_reference():
+    ig, sg = workloads.c1_geometry()
+    P = ap.SiddonProjector(ig, sg)
+    lor, _ = P.tables()
+    assert bits_equal(lor, G["lor_c1"])
+
+
+def test_2d_project_bit_exact_vs_reference():
+    ig, sg = workloads.c1_geometry()
+    P = ap.SiddonProjector(ig, sg)
+    out = torch.zeros(sg.n_bins, dtype=torch.float32, device=DEV)
+    P.project(t(G["c1_phantom"]), out)
+    torch.cuda.synchronize()
+    assert bits_equal(out.cpu().numpy(), G["c1_project"])
+
+
+def test_2d_backproject_vs_reference():
+    ig, sg = workloads.c1_geometry()
+    P = ap.SiddonProjector(ig, sg)
+    img = torch.zeros(ig.n_voxels, dtype=torch.float32, device=DEV)
+    P.backproject(torch.ones(sg.n_bins, dtype=torch.float32, device=DEV), img)
+    assert rel(img.cpu().numpy(), G["c1_backproject_ones"]) <= 1e-5
+
+
+def test_2d_divide_and_backproject(oracle):
+    ig, sg = workloads.c1_geometry()
+    rng = np.random.default_rng(3)
+    m = rng.poisson(5, sg.n_bins).astype(np.float32)
+    e = rng.random(sg.n_bins, dtype=np.float32)
+    e[::5] = 0
+    P = ap.SiddonProjector(ig, sg)
+    img = torch.zeros(ig.n_voxels, dtype=torch.float32, device=DEV)
+    P.divide_and_backproject(t(m), t(e), img)
+    assert rel(img.cpu().numpy(), oracle.divide_and_backproject_2d(sg, ig, m, e)) <= 1e-5
+
+
+@pytest.mark.parametrize("sub,ns", [(-1, 1), (0, 4), (3, 4), (2, 5)])
+def test_3d_project_bit_exact_backproject_close_vs_reference(sub, ns):
+    ig, sg = small_3d()
+    P = ap.SiddonProjector(ig, sg)
+    key = f"s3_project_{sub}_{ns}".replace("-", "m")
+    out = torch.zeros(P.num_bins(sub, ns), dtype=torch.float32, device=DEV)
+    P.project(t(G["s3_image"]), out, sub, ns)
+    assert bits_equal(out.cpu().numpy(), G[key])
+    img = torch.zeros(ig.n_voxels, dtype=torch.float32, device=DEV)
+    P.backproject(t(G[key.replace("project", "bpvalues")]), img, sub, ns)
+    assert rel(img.cpu().numpy(), G[key.replace("project", "backproject")]) <= 1e-5
+
+
+def test_3d_divide_and_backproject(oracle):
+    ig, sg = small_3d()
+    rng = np.random.default_rng(5)
+    nb = sg.subset_bins(1, 3)
+    m = rng.poisson(3, nb).astype(np.float32)
+    e = rng.random(nb, dtype=np.float32)
+    e[::4] = 0
+    P = ap.SiddonProjector(ig, sg)
+    img = torch.zeros(ig.n_voxels, dtype=torch.float32, device=DEV)
+    P.divide_and_backproject(t(m), t(e), img, 1, 3)
+    assert rel(img.cpu().numpy(), oracle.divide_and_backproject_3d(sg, ig, m, e, 1, 3)) <= 1e-5
+
+
+@pytest.mark.parametrize("which", ["2d", "3d"])
+def test_adjoint_identity(which):
+    if which == "2d":
+        ig, sg = workloads.c1_geometry()
+        sg = Sino2DGeom(sg.n_proj, sg.n_r, 130.0, sg.r_scanner)  # every ray valid and inside
+    else:
+        ig, sg = small_3d()
+    P = ap.SiddonProjector(ig, sg)
+    rng = np.random.default_rng(11)
+    x = rng.random(ig.n_voxels, dtype=np.float32)
+    y = rng.random(P.num_bins(), dtype=np.float32)
+    ax = torch.zeros(P.num_bins(), dtype=torch.float32, device=DEV)
+    P.project(t(x), ax)
+    aty = torch.zeros(ig.n_voxels, dtype=torch.float32, device=DEV)
+    P.backproject(t(y), aty)
+    lhs = float(np.dot(ax.cpu().numpy().astype(np.float64), y.astype(np.float64)))
+    rhs = float(np.dot(x.astype(np.float64), aty.cpu().numpy().astype(np.float64)))
+    assert abs(lhs - rhs) / abs(rhs) <= 1e-6
+
+
+# ---------------------------------------------------------------------------
+def _oracle_osem_pass(oracle, sg, ig, x, meas_full, sens, subset, ns):
+    meas_sub = meas_full.reshape(sg.n_sinos, sg.n_proj, sg.n_r)[:, subset::ns, :].reshape(-1) if subset >= 0 \
+        else meas_full
+    est = oracle.project_3d(sg, ig, x, subset, ns)
+    est64 = est.astype(np.float64)
+    nz = est != 0
+    lik = float(np.sum(meas_sub[nz].astype(np.float64) * np.log(est64[nz]) - est64[nz]))
+    ratio = oracle.inverse_divide(meas_sub, est)
+    bp = oracle.backproject_3d(sg, ig, ratio, subset, ns, threads=1)
+    return oracle.update(x, bp, sens, np.float32(0), True), lik, meas_sub
+
+
+@pytest.mark.parametrize("dtype", ["float32", "uint32", "uint16"])
+def test_em_pass_vs_oracle(oracle, dtype):
+    ig, sg = small_3d()
+    rng = np.random.default_rng(21)
+    x0 = (rng.random(ig.n_voxels, dtype=np.float32) + 0.5).astype(np.float32)
+    meas = rng.poisson(oracle.project_3d(sg, ig, x0) * 2).astype(np.float32)
+    sens = (rng.random(ig.n_voxels, dtype=np.float32) + 1).astype(np.float32)
+    subset, ns = 2, 5
+    want_x, want_lik, meas_sub = _oracle_osem_pass(oracle, sg, ig, x0, meas, sens, subset, ns)
+    P = ap.SiddonProjector(ig, sg)
+    for packed in (False, True):
+        x = t(x0)
+        bp = torch.zeros(ig.n_voxels, dtype=torch.float32, device=DEV)
+        lik = torch.zeros(1, dtype=torch.float64, device=DEV)
+        counts = t((meas_sub if packed else meas).astype(dtype))
+        P.em_pass(counts, x, bp, t(sens), subset, ns, lik=lik, counts_packed=packed)
+        torch.cuda.synchronize()
+        assert rel(x.cpu().numpy(), want_x) <= 1e-5
+        assert float(bp.abs().max()) == 0.0  # cleared for the next pass
+        assert abs(lik.item() - want_lik) <= 1e-9 * abs(want_lik)
+
+
+def test_em_pass_host_matches_device(oracle):
+    ig, sg = small_3d()
+    rng = np.random.default_rng(22)
+    x0 = (rng.random(ig.n_voxels, dtype=np.float32) + 0.5).astype(np.float32)
+    meas = rng.poisson(oracle.project_3d(sg, ig, x0) * 2).astype(np.uint32)
+    sens = np.ones(ig.n_voxels, np.float32)
+    subset, ns = 1, 4
+    want_x, want_lik, meas_sub = _oracle_osem_pass(oracle, sg, ig, x0, meas.astype(np.float32), sens, subset, ns)
+    P = ap.SiddonProjector(ig, sg)
+    import ctypes
+    from apirl_b200 import _lib
+    x = t(x0)
+    bp = torch.zeros(ig.n_voxels, dtype=torch.float32, device=DEV)
+    stage = torch.zeros(meas_sub.size, dtype=torch.int32, device=DEV)
+    h_counts = np.ascontiguousarray(meas_sub.astype(np.uint32))
+    h_x = np.zeros(ig.n_voxels, np.float32)
+    h_lik = np.zeros(1, np.float64)
+    st = t(sens)
+    _lib.check(P.lib.apirl_em_pass_host(P.h, h_counts.ctypes.data_as(ctypes.c_void_p), _lib.APIRL_U32,
+                                        ctypes.c_void_p(stage.data_ptr()), ctypes.c_void_p(x.data_ptr()),
+                                        ctypes.c_void_p(bp.data_ptr()), ctypes.c_void_p(st.data_ptr()), 0.0, 1,
+                                        subset, ns, h_x.ctypes.data_as(ctypes.c_void_p),
+                                        h_lik.ctypes.data_as(ctypes.c_void_p), None))
+    assert rel(h_x, want_x) <= 1e-5
+    assert abs(h_lik[0] - want_lik) <= 1e-9 * abs(want_lik)
+
+
+def test_update_threshold_and_force_positive(oracle):
+    rng = np.random.default_rng(4)
+    n = 1001
+    sens = rng.random(n, dtype=np.float32)
+    sens[::7] = 0
+    sens[3] = -0.5
+    x = rng.random(n, dtype=np.float32)
+    bp = rng.random(n, dtype=np.float32)
+    thr = ap.mlem_threshold(t(sens))
+    assert thr.item() == oracle.mlem_threshold(sens)
+    for ge in (True, False):
+        xt, bpt = t(x), t(bp)
+        ap.update_pixels(xt, bpt, t(sens), thr=thr, ge=ge, zero_bp=True)
+        torch.cuda.synchronize()
+        assert bits_equal(xt.cpu().numpy(), oracle.update(x, bp, sens, np.float32(thr.item()), ge))
+        assert float(bpt.abs().max()) == 0.0
+    s2 = t(sens)
+    ap.force_positive(s2)
+    assert s2.min().item() >= 0
+    e = t(x)
+    ap.inverse_divide(t(bp), e)
+    assert bits_equal(e.cpu().numpy(), oracle.inverse_divide(bp, x))
+    lik = ap.likelihood(t(x), t(bp))
+    want = float(np.sum(bp.astype(np.float64) * np.log(x.astype(np.float64)) - x.astype(np.float64)))
+    assert abs(lik.item() - want) <= 1e-12 * abs(want)
+
+
+# ---------------------------------------------------------------------------
+def test_osem_driver_vs_reference_and_oracle(oracle):
+    ig, sg = small_3d()
+    init = np.ones(ig.n_voxels, np.float32)
+    img, lik, sens0 = ap.osem_3d(ig, sg, G["s3_meas"], init, 2, 4)
+    assert rel(sens0, G["s3_osem_sens0"]) <= 1e-5
+    assert rel(img, G["s3_osem"]) <= 1e-4
+    # likelihood: reference accumulates in float, we in FP64
+    assert np.allclose(lik, G["s3_osem_lik"].astype(np.float64), rtol=1e-5)
+    o64, lik64, _ = oracle.osem_3d(sg, ig, init, G["s3_meas"], 2, 4, dtype=np.float64)
+    assert rel(img, o64) <= 1e-4
+
+
+def test_mlem2d_driver_60_iterations_vs_reference():
+    ig, sg = workloads.c1_geometry()
+    init = np.ones(ig.n_voxels, np.float32)
+    img, lik, sens = ap.mlem_2d(ig, sg, G["c1_meas"], init, 60)
+    assert rel(sens, G["c1_sens"]) <= 1e-5
+    assert rel(img, G["c1_mlem60"]) <= 1e-4
+    assert np.allclose(lik, G["c1_mlem60_lik"].astype(np.float64), rtol=1e-4)
+
+
+def test_mlem3d_driver_vs_oracle(oracle):
+    ig, sg = small_3d()
+    init = np.ones(ig.n_voxels, np.float32)
+    img, lik, sens = ap.mlem_3d(ig, sg, G["s3_meas"], init, 3)
+    # oracle MLEM 3D = OSEM with one subset and the MLEM threshold
+    x = init.copy()
+    sens_o = oracle.backproject_3d(sg, ig, np.ones(sg.n_bins, np.float32), threads=1)
+    assert rel(sens, sens_o) <= 1e-5
+    thr = oracle.mlem_threshold(sens_o)
+    for _ in range(3):
+        est = oracle.project_3d(sg, ig, x)
+        bp = oracle.backproject_3d(sg, ig, oracle.inverse_divide(G["s3_meas"], est), threads=1)
+        x = oracle.update(x, bp, sens_o, thr, True)
+    assert rel(img, x) <= 1e-4
+
+
+# ---------------------------------------------------------------------------
+@pytest.mark.slow
+def test_c2_full_size_projection_bytes_equal_reference():
+    """Subset 0 of 21 at full size: the GPU projection of the cylinder phantom
+    has exactly the reference's bytes (SHA-256 recorded from the reference)."""
+    ig, sg = workloads.c2_geometry()
+    P = ap.SiddonProjector(ig, sg)
+    ph = t(workloads.cylinder_phantom_3d(ig, seed=2))
+    out = torch.empty(P.num_bins(0, 21), dtype=torch.float32, device=DEV)
+    P.project(ph, out, 0, 21)
+    assert sha(out.cpu().numpy()) == C2["project_phantom_subset0_of21_sha256"]
+    P.project(torch.ones(ig.n_voxels, dtype=torch.float32, device=DEV), out, 0, 21)
+    assert sha(out.cpu().numpy()) == C2["project_ones_subset0_of21_sha256"]
+    steps = P.count_steps(0, 21)
+    assert int(steps.sum().item()) == 2144070812  # Siddon segments of subset 0
+
+
+@pytest.mark.slow
+def test_c2_full_size_backprojection_vs_oracle(oracle):
+    ig, sg = workloads.c2_geometry()
+    P = ap.SiddonProjector(ig, sg)
+    rng = np.random.default_rng(9)
+    v = rng.random(P.num_bins(5, 21), dtype=np.float32)
+    v[rng.random(v.size) < 0.3] = 0
+    img = torch.zeros(ig.n_voxels, dtype=torch.float32, device=DEV)
+    P.backproject(t(v), img, 5, 21)
+    assert rel(img.cpu().numpy(), oracle.backproject_3d(sg, ig, v, 5, 21)) <= 1e-5
+
+
+@pytest.mark.slow
+def test_c2_em_pass_properties():
+    """Full-size fused pass: the image update is invariant to the counts' storage
+    type, and a pass with measured = A x leaves x unchanged where sens = A^T 1."""
+    ig, sg = workloads.c2_geometry()
+    P = ap.SiddonProjector(ig, sg)
+    x0 = t(workloads.cylinder_phantom_3d(ig, seed=2) + 0.5)
+    ns, s = 21, 4
+    est = torch.empty(P.num_bins(s, ns), dtype=torch.float32, device=DEV)
+    P.project(x0, est, s, ns)
+    sens = torch.zeros(ig.n_voxels, dtype=torch.float32, device=DEV)
+    P.backproject(torch.ones_like(est), sens, s, ns)
+    x = x0.clone()
+    bp = torch.zeros_like(x)
+    P.em_pass(est, x, bp, sens, s, ns, counts_packed=True)
+    hit = sens > 0
+    # m == A x makes every ratio 1, so bp == sens and x is unchanged up to rounding
+    assert float(((x - x0).abs()[hit] / x0[hit]).max()) <= 1e-4
+    c = torch.poisson(est * 2.0, generator=torch.Generator(device=DEV).manual_seed(0))
+    xs = []
+    for cc in (c, c.to(torch.int32).view(torch.uint32), c.to(torch.int32).to(torch.int16).view(torch.uint16)):
+        xi = x0.clone()
+        bp.zero_()
+        P.em_pass(cc, xi, bp, sens, s, ns, counts_packed=True)
+        xs.append(xi.cpu().numpy())
+    assert rel(xs[0], xs[1]) <= 1e-5 and rel(xs[0], xs[2]) <= 1e-5
