@@ -1,0 +1,223 @@
+// The reference's .par-driven commands on the GPU path: MLEM, OSEM, project
+// and backproject (cmd/src/MLEM.cpp, OSEM.cpp, project.cpp, backproject.cpp).
+// One source; the command is chosen at build time with -DAPIRL_COMMAND=<name>
+// (the binary's name).  Each takes one argument, a parameter file ending in
+// .par whose first line is "<COMMAND> Parameters :=".
+//
+// Keys read (as in the reference):
+//   MLEM/OSEM  input type, input file, initial estimate, output filename prefix,
+//              number of iterations, number of subsets (OSEM), forwardprojector,
+//              backprojector, sensitivity filename, save estimates at iteration
+//              intervals, save estimated projections and backprojected image,
+//              multiplicative sinogram, additive sinogram, cylindrical pet radius
+//              (in mm), radius fov (in mm), axial fov (in mm), gpu id
+//   project    input file, output type, projector, output filename, output
+//              projection, number of subsets, subset index (+ scanner keys)
+//   backproject input type, input file, backprojector, output image, output
+//              filename, number of subsets, subset index (+ scanner keys)
+#include <chrono>
+#include <cstdio>
+#include <cstdlib>
+#include <iostream>
+#include <memory>
+#include <string>
+
+#include "apirl_host.h"
+
+using namespace apirl;
+
+#ifndef APIRL_COMMAND
+#define APIRL_COMMAND "OSEM"
+#endif
+
+namespace {
+
+const char* kCmd = APIRL_COMMAND;
+std::string g_par;
+std::string g_section;
+
+bool key(const char* k, std::string* v, bool required = true) {
+  int e = parametersFile_read(g_par.c_str(), g_section.c_str(), k, v);
+  if (e == 0) return true;
+  if (e == 2 && !required) return false;
+  std::cerr << "Error " << e << " reading \"" << k << "\" from " << g_par << std::endl;
+  exit(1);
+}
+
+float fkey(const char* k, float def) {
+  std::string v;
+  return key(k, &v, false) ? (float)atof(v.c_str()) : def;
+}
+
+int ikey(const char* k, int def) {
+  std::string v;
+  return key(k, &v, false) ? atoi(v.c_str()) : def;
+}
+
+struct Scanner {
+  float rScanner, rFov, zFov;
+};
+
+Scanner scanner(const Image* img) {
+  Scanner s;
+  s.rScanner = fkey("cylindrical pet radius (in mm)", 443.f);
+  s.rFov = fkey("radius fov (in mm)", img ? img->getFovRadio() : 0.f);
+  s.zFov = fkey("axial fov (in mm)", img ? img->getFovHeight() : 0.f);
+  return s;
+}
+
+std::unique_ptr<CuSiddonProjector> siddon(const std::string& name) {
+  if (name != "Siddon" && name != "CuSiddon") {
+    std::cerr << "Only the Siddon projector is available on this path (got \"" << name << "\")" << std::endl;
+    exit(1);
+  }
+  int ns = ikey("siddon number of samples on the detector", 1);
+  int nas = ikey("siddon number of axial samples on the detector", 1);
+  if (ns != 1 || nas != 1) {
+    std::cerr << "Only one LOR per bin is implemented (siddon number of samples = 1)" << std::endl;
+    exit(1);
+  }
+  return std::unique_ptr<CuSiddonProjector>(new CuSiddonProjector(1, 1, ikey("gpu id", 0)));
+}
+
+int recon(bool osem) {
+  std::string type, input, init, prefix, v;
+  key("input type", &type);
+  key("input file", &input);
+  key("initial estimate", &init);
+  key("output filename prefix", &prefix);
+  int iters = ikey("number of iterations", 1);
+  int subsets = osem ? ikey("number of subsets", 1) : 1;
+  std::string fwdName = "Siddon", backName = "Siddon";
+  key("forwardprojector", &fwdName, false);
+  key("backprojector", &backName, false);
+  Image x0;
+  if (!x0.readFromInterfile(init.c_str())) {
+    std::cerr << "Error reading the initial estimate: " << x0.getError() << std::endl;
+    return 1;
+  }
+  auto fwd = siddon(fwdName);
+  auto back = siddon(backName);
+  Scanner sc = scanner(&x0);
+  std::string mult, add;
+  bool hasMult = key("multiplicative sinogram", &mult, false);
+  bool hasAdd = key("additive sinogram", &add, false);
+  std::unique_ptr<Mlem> m;
+  std::unique_ptr<Sinogram2D> s2;
+  std::unique_ptr<Sinogram3D> s3;
+  if (type == "Sinogram2D") {
+    s2.reset(new Sinogram2DinCylindrical3Dpet(input.c_str(), sc.rFov, sc.rScanner));
+    if (s2->getNumR() <= 1) { std::cerr << "Error reading " << input << ": " << s2->getError() << std::endl; return 1; }
+    if (osem) { std::cerr << "OSEM needs a Sinogram3D input" << std::endl; return 1; }
+    m.reset(new Mlem2d(s2.get(), &x0, "", prefix, iters, 0, false, false, fwd.get(), back.get()));
+    // The reference's Mlem2d forces the sinogram rFov to the image's; an
+    // explicit "radius fov (in mm)" restores the sinogram's own bin pitch.
+    std::string rf;
+    if (key("radius fov (in mm)", &rf, false)) s2->setRadioFov_mm((float)atof(rf.c_str()));
+  } else if (type == "Sinogram3D") {
+    s3.reset(new Sinogram3DCylindricalPet(input.c_str(), sc.rFov, sc.zFov, sc.rScanner));
+    if (s3->getNumSinograms() <= 0 || s3->getBinCount() <= 1) {
+      std::cerr << "Error reading " << input << ": " << s3->getError() << std::endl;
+      return 1;
+    }
+    if (osem)
+      m.reset(new OsemSinogram3d(s3.get(), &x0, "", prefix, iters, 0, false, false, fwd.get(), back.get(), subsets));
+    else
+      m.reset(new MlemSinogram3d(s3.get(), &x0, "", prefix, iters, 0, false, false, fwd.get(), back.get()));
+  } else {
+    std::cerr << "input type " << type << " is not supported on this path (Sinogram2D, Sinogram3D)" << std::endl;
+    return 1;
+  }
+  if (hasMult && !m->setMultiplicativeProjection(mult)) { std::cerr << "Error reading " << mult << std::endl; return 1; }
+  if (hasAdd && !m->setAdditiveProjection(add)) { std::cerr << "Error reading " << add << std::endl; return 1; }
+  auto t0 = std::chrono::steady_clock::now();
+  if (!m->Reconstruct()) { std::cerr << "Reconstruction failed: " << m->getError() << std::endl; return 1; }
+  double s = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+  std::cout << kCmd << ": " << iters << " iterations in " << s << " s, output " << prefix << "_final.h33" << std::endl;
+  return 0;
+}
+
+int project() {
+  std::string input, type, proj, out, tmpl;
+  key("input file", &input);
+  key("output type", &type);
+  key("projector", &proj);
+  key("output filename", &out);
+  key("output projection", &tmpl);
+  int nsub = ikey("number of subsets", 0), subset = ikey("subset index", -1);
+  Image img;
+  if (!img.readFromInterfile(input.c_str())) { std::cerr << img.getError() << std::endl; return 1; }
+  auto p = siddon(proj);
+  Scanner sc = scanner(&img);
+  auto t0 = std::chrono::steady_clock::now();
+  if (type == "Sinogram2D") {
+    Sinogram2DinCylindrical3Dpet s(tmpl.c_str(), sc.rFov, sc.rScanner);
+    s.FillConstant(0);
+    if (!p->Project(&img, &s)) { std::cerr << p->getError() << std::endl; return 1; }
+    s.writeInterfile(out.c_str());
+  } else if (type == "Sinogram3D") {
+    Sinogram3DCylindricalPet full(tmpl.c_str(), sc.rFov, sc.zFov, sc.rScanner);
+    std::unique_ptr<Sinogram3D> s(nsub > 0 && subset >= 0 ? full.getSubset(subset, nsub) : full.Copy());
+    if (!p->Project(&img, s.get())) { std::cerr << p->getError() << std::endl; return 1; }
+    s->writeInterfile(out.c_str());
+  } else {
+    std::cerr << "output type " << type << " is not supported on this path" << std::endl;
+    return 1;
+  }
+  double sec = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+  std::cout << "project: " << sec << " s" << std::endl;
+  return 0;
+}
+
+int backproject() {
+  std::string type, input, proj, outImg, out;
+  key("input type", &type);
+  key("input file", &input);
+  key("backprojector", &proj);
+  key("output image", &outImg);
+  key("output filename", &out);
+  int nsub = ikey("number of subsets", 0), subset = ikey("subset index", -1);
+  Image img;
+  if (!img.readFromInterfile(outImg.c_str())) { std::cerr << img.getError() << std::endl; return 1; }
+  img.fillConstant(0);
+  auto p = siddon(proj);
+  Scanner sc = scanner(&img);
+  auto t0 = std::chrono::steady_clock::now();
+  if (type == "Sinogram2D") {
+    Sinogram2DinCylindrical3Dpet s(input.c_str(), sc.rFov, sc.rScanner);
+    if (!p->Backproject(&s, &img)) { std::cerr << p->getError() << std::endl; return 1; }
+  } else if (type == "Sinogram3D") {
+    Sinogram3DCylindricalPet full(input.c_str(), sc.rFov, sc.zFov, sc.rScanner);
+    std::unique_ptr<Sinogram3D> s(nsub > 0 && subset >= 0 ? full.getSubset(subset, nsub) : full.Copy());
+    if (!p->Backproject(s.get(), &img)) { std::cerr << p->getError() << std::endl; return 1; }
+  } else {
+    std::cerr << "input type " << type << " is not supported on this path" << std::endl;
+    return 1;
+  }
+  img.writeInterfile(out.c_str());
+  double sec = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+  std::cout << "backproject: " << sec << " s" << std::endl;
+  return 0;
+}
+
+}  // namespace
+
+int main(int argc, char** argv) {
+  if (argc != 2) {
+    std::cerr << "usage: " << kCmd << " parameters.par" << std::endl;
+    return -1;
+  }
+  g_par = argv[1];
+  if (g_par.size() < 4 || g_par.compare(g_par.size() - 4, 4, ".par") != 0) {
+    std::cerr << "The parameter file must have the .par extension" << std::endl;
+    return -1;
+  }
+  std::string cmd = kCmd;
+  g_section = cmd == "project" ? "Projection" : (cmd == "backproject" ? "Backproject" : cmd);
+  if (cmd == "MLEM") return recon(false);
+  if (cmd == "OSEM") return recon(true);
+  if (cmd == "project") return project();
+  if (cmd == "backproject") return backproject();
+  std::cerr << "unknown command " << cmd << std::endl;
+  return -1;
+}

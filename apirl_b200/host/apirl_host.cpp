@@ -1,0 +1,686 @@
+// Implementation of the C++ host layer (apirl_host.h) over the C ABI.
+#include "apirl_host.h"
+
+#include <cuda_runtime.h>
+
+#include <chrono>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <fstream>
+#include <limits>
+#include <sstream>
+
+namespace apirl {
+
+namespace {
+
+std::string trim(const std::string& s) {
+  size_t a = s.find_first_not_of(" \t\r\n"), b = s.find_last_not_of(" \t\r\n");
+  return a == std::string::npos ? std::string() : s.substr(a, b - a + 1);
+}
+
+// Splits "key := value"; the key keeps a leading '!'.
+bool split_line(const std::string& line, std::string* key, std::string* value) {
+  size_t p = line.find(":=");
+  if (p == std::string::npos) return false;
+  *key = trim(line.substr(0, p));
+  *value = trim(line.substr(p + 2));
+  return true;
+}
+
+std::string dir_of(const std::string& path) {
+  size_t p = path.find_last_of('/');
+  return p == std::string::npos ? std::string() : path.substr(0, p + 1);
+}
+
+std::string base_of(const std::string& path) {
+  size_t p = path.find_last_of('/');
+  return p == std::string::npos ? path : path.substr(p + 1);
+}
+
+// Resolves a data-file name relative to its header (Sinogram3D.cpp:117-141).
+std::string data_path(const std::string& header, const std::string& name) {
+  if (name.find('/') != std::string::npos && name[0] == '/') return name;
+  return dir_of(header) + name;
+}
+
+std::vector<int> parse_list(const std::string& v) {
+  std::vector<int> out;
+  size_t a = v.find('{'), b = v.rfind('}');
+  std::string body = (a != std::string::npos && b != std::string::npos && b > a) ? v.substr(a + 1, b - a - 1) : v;
+  std::stringstream ss(body);
+  std::string tok;
+  while (std::getline(ss, tok, ',')) {
+    tok = trim(tok);
+    if (!tok.empty()) out.push_back(atoi(tok.c_str()));
+  }
+  return out;
+}
+
+bool read_floats(const std::string& path, float* dst, size_t n, std::string* err) {
+  FILE* f = fopen(path.c_str(), "rb");
+  if (!f) { *err = "cannot open data file " + path; return false; }
+  size_t got = fread(dst, sizeof(float), n, f);
+  fclose(f);
+  if (got != n) { *err = "data file " + path + " is shorter than its header says"; return false; }
+  return true;
+}
+
+bool write_floats(const std::string& path, const float* src, size_t n) {
+  FILE* f = fopen(path.c_str(), "wb");
+  if (!f) return false;
+  size_t put = fwrite(src, sizeof(float), n, f);
+  fclose(f);
+  return put == n;
+}
+
+double now_ms() {
+  return std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now().time_since_epoch()).count();
+}
+
+}  // namespace
+
+// ---- key readers -------------------------------------------------------------
+int interfile_read(const char* header, const char* key, std::string* value) {
+  std::ifstream in(header);
+  if (!in) return 3;
+  std::string line;
+  if (!std::getline(in, line) || line.compare(0, 10, "!INTERFILE") != 0) return 4;
+  int count = 0;
+  while (std::getline(in, line)) {
+    if (!line.empty() && line[0] == ';') continue;
+    std::string k, v;
+    if (!split_line(line, &k, &v)) continue;
+    if (k.compare(0, 17, "!END OF INTERFILE") == 0) break;
+    if (k == key) { *value = v; count++; }
+  }
+  if (count == 0) return 2;
+  return count > 1 ? 1 : 0;
+}
+
+int parametersFile_read(const char* file, const char* command, const char* key, std::string* value) {
+  std::ifstream in(file);
+  if (!in) return 3;
+  std::string line;
+  if (!std::getline(in, line)) return 4;
+  std::string first = std::string(command) + " Parameters :=";
+  if (line.compare(0, first.size(), first) != 0) return 5;
+  int count = 0;
+  while (std::getline(in, line)) {
+    std::string l = trim(line);
+    if (l.empty() || l[0] == ';') continue;
+    std::string k, v;
+    if (!split_line(l, &k, &v)) continue;
+    if (k == "END") break;
+    if (k == key) { *value = v; count++; }
+  }
+  if (count == 0) return 2;
+  return count > 1 ? 1 : 0;
+}
+
+// ---- Image -------------------------------------------------------------------
+Image::Image() { SizeImage s{2, 1, 1, 1, 1.f, 1.f, 1.f}; init(s); }
+Image::Image(SizeImage s) { init(s); }
+Image::Image(Image* c) : size(c->size), pixels(c->pixels), fovRadio_mm(c->fovRadio_mm), fovHeight_mm(c->fovHeight_mm) {}
+Image::Image(const std::string& header) {
+  SizeImage s{2, 1, 1, 1, 1.f, 1.f, 1.f};
+  init(s);
+  readFromInterfile(header.c_str());
+}
+
+void Image::init(SizeImage s) {
+  size = s;
+  if (size.nDimensions == 2) size.nPixelsZ = 1;  // Images.cpp:40-44
+  pixels.assign((size_t)size.nPixelsX * size.nPixelsY * size.nPixelsZ, 0.f);
+  fovHeight_mm = size.sizePixelZ_mm * size.nPixelsZ;          // Images.cpp:54
+  fovRadio_mm = (size.sizePixelX_mm * size.nPixelsX) / 2;     // Images.cpp:55
+}
+
+void Image::fillConstant(float v) { std::fill(pixels.begin(), pixels.end(), v); }
+
+int Image::forcePositive() {
+  int n = 0;
+  for (float& p : pixels) if (p < 0) { p = 0; n++; }
+  return n;
+}
+
+float Image::getMinValue() const {
+  float mn = std::numeric_limits<float>::max();
+  for (float p : pixels) if (p != 0 && p < mn) mn = p;
+  return mn;
+}
+
+float Image::getMaxValue() const {
+  float mx = pixels.empty() ? 0.f : pixels[0];
+  for (float p : pixels) if (p > mx) mx = p;
+  return mx;
+}
+
+apirl_image_geom Image::geom() const {
+  return apirl_image_geom{size.nPixelsX, size.nPixelsY, size.nPixelsZ, size.sizePixelX_mm, size.sizePixelY_mm,
+                          size.sizePixelZ_mm};
+}
+
+// Interfile image: the keys medcon writes for a 3D float image
+// (data/medcon/m-intf.c MdcWriteIntfHeader): matrix size / scaling factor per
+// axis, short float, 4 bytes per pixel, little endian.
+bool Image::readFromInterfile(const char* header) {
+  std::string v;
+  int nx = 0, ny = 0, nz = 1;
+  float dx = 1, dy = 1, dz = 1;
+  int e = interfile_read(header, "!matrix size [1]", &v);
+  if (e == 3 || e == 4) { strError = std::string("cannot read interfile header ") + header; return false; }
+  if (e) { strError = "missing !matrix size [1]"; return false; }
+  nx = atoi(v.c_str());
+  if (interfile_read(header, "!matrix size [2]", &v)) { strError = "missing !matrix size [2]"; return false; }
+  ny = atoi(v.c_str());
+  if (!interfile_read(header, "!matrix size [3]", &v)) nz = atoi(v.c_str());
+  else if (!interfile_read(header, "!number of slices", &v)) nz = atoi(v.c_str());
+  else if (!interfile_read(header, "!total number of images", &v)) nz = atoi(v.c_str());
+  if (!interfile_read(header, "scaling factor (mm/pixel) [1]", &v)) dx = (float)atof(v.c_str());
+  if (!interfile_read(header, "scaling factor (mm/pixel) [2]", &v)) dy = (float)atof(v.c_str());
+  if (!interfile_read(header, "scaling factor (mm/pixel) [3]", &v)) dz = (float)atof(v.c_str());
+  if (!interfile_read(header, "!number format", &v) && v != "short float" && v != "float") {
+    strError = "only float images are supported (number format " + v + ")";
+    return false;
+  }
+  std::string dataName;
+  if (interfile_read(header, "!name of data file", &dataName)) { strError = "missing !name of data file"; return false; }
+  if (nx <= 0 || ny <= 0 || nz <= 0) { strError = "bad image size in header"; return false; }
+  SizeImage s{nz > 1 ? 3 : 2, nx, ny, nz, dx, dy, dz};
+  init(s);
+  if (nz == 1) { size.nPixelsZ = 1; size.sizePixelZ_mm = dz; fovHeight_mm = dz; }
+  return read_floats(data_path(header, dataName), pixels.data(), pixels.size(), &strError);
+}
+
+bool Image::writeInterfile(const char* path) const {
+  std::string hdr = std::string(path) + ".h33", dat = std::string(path) + ".i33";
+  std::ofstream f(hdr);
+  if (!f) { strError = "cannot create " + hdr; return false; }
+  f << "!INTERFILE :=\r\n!imaging modality := nucmed\r\n!originating system := apirl_b200\r\n"
+    << "!version of keys := 3.3\r\n!name of data file := " << base_of(dat) << "\r\n"
+    << "!GENERAL IMAGE DATA :=\r\n!type of data := Tomographic\r\nimagedata byte order := LITTLEENDIAN\r\n"
+    << "number of dimensions := 3\r\n"
+    << "!matrix size [1] := " << size.nPixelsX << "\r\nmatrix axis label [1] := x\r\n"
+    << "scaling factor (mm/pixel) [1] := " << size.sizePixelX_mm << "\r\n"
+    << "!matrix size [2] := " << size.nPixelsY << "\r\nmatrix axis label [2] := y\r\n"
+    << "scaling factor (mm/pixel) [2] := " << size.sizePixelY_mm << "\r\n"
+    << "!matrix size [3] := " << size.nPixelsZ << "\r\nmatrix axis label [3] := z\r\n"
+    << "scaling factor (mm/pixel) [3] := " << size.sizePixelZ_mm << "\r\n"
+    << "!number format := short float\r\n!number of bytes per pixel := 4\r\n"
+    << "!number of slices := " << size.nPixelsZ << "\r\n!END OF INTERFILE :=\r\n";
+  f.close();
+  if (!write_floats(dat, pixels.data(), pixels.size())) { strError = "cannot write " + dat; return false; }
+  return true;
+}
+
+// ---- Sinogram2D --------------------------------------------------------------
+Sinogram2D::Sinogram2D(int nProj, int nR, float rFov, float rScanner)
+    : numProj(nProj), numR(nR), radioFov_mm(rFov), radioScanner_mm(rScanner), bins((size_t)nProj * nR, 0.f) {}
+
+bool Sinogram2D::FillConstant(float v) { std::fill(bins.begin(), bins.end(), v); return true; }
+
+void Sinogram2D::inverseDivideBinToBin(const Sinogram2D* m) {
+  for (size_t i = 0; i < bins.size(); i++) {
+    float num = m->bins[i], den = bins[i];
+    bins[i] = (num != 0 && den != 0) ? num / den : 0.f;
+  }
+}
+void Sinogram2D::addBinToBin(const Sinogram2D* a) { for (size_t i = 0; i < bins.size(); i++) bins[i] = bins[i] + a->bins[i]; }
+void Sinogram2D::multiplyBinToBin(const Sinogram2D* a) { for (size_t i = 0; i < bins.size(); i++) bins[i] = bins[i] * a->bins[i]; }
+
+float Sinogram2D::getLikelihoodValue(const Sinogram2D* ref) const {
+  double l = 0;
+  for (size_t i = 0; i < bins.size(); i++)
+    if (bins[i] > 0) l += (double)ref->bins[i] * std::log((double)bins[i]) - (double)bins[i];
+  return (float)l;
+}
+
+// 2D sinogram interfile: matrix size [1] = r, [2] = angles (Sinogram2D.cpp:415-517).
+bool Sinogram2D::readFromInterfile(const char* header) {
+  std::string v, dataName;
+  if (interfile_read(header, "!matrix size [1]", &v)) { strError = "missing !matrix size [1]"; return false; }
+  int nr = atoi(v.c_str());
+  if (interfile_read(header, "!matrix size [2]", &v)) { strError = "missing !matrix size [2]"; return false; }
+  int np = atoi(v.c_str());
+  if (interfile_read(header, "!name of data file", &dataName)) { strError = "missing !name of data file"; return false; }
+  numR = nr; numProj = np;
+  bins.assign((size_t)nr * np, 0.f);
+  return read_floats(data_path(header, dataName), bins.data(), bins.size(), &strError);
+}
+
+bool Sinogram2D::writeInterfile(const char* path) const {
+  std::string hdr = std::string(path) + ".h33", dat = std::string(path) + ".i33";
+  std::ofstream f(hdr);
+  if (!f) return false;
+  f << "!INTERFILE :=\r\n!imaging modality := nucmed\r\n!originating system := apirl_b200\r\n"
+    << "!version of keys := 3.3\r\n!name of data file := " << base_of(dat) << "\r\n"
+    << "!GENERAL IMAGE DATA :=\r\n!type of data := Tomographic\r\n!total number of images := 1\r\n"
+    << "imagedata byte order := LITTLEENDIAN\r\n!matrix size [1] := " << numR << "\r\n!matrix size [2] := "
+    << numProj << "\r\n!number format := short float\r\n!number of bytes per pixel := 4\r\n"
+    << "!number of projections := 1\r\n!extent of rotation := 180\r\n!END OF INTERFILE :=\r\n";
+  f.close();
+  return write_floats(dat, bins.data(), bins.size());
+}
+
+Sinogram2DinCylindrical3Dpet::Sinogram2DinCylindrical3Dpet(const char* header, float rFov, float rScanner)
+    : Sinogram2D(1, 1, rFov, rScanner) {
+  readFromInterfile(header);
+}
+
+// ---- Sinogram3D --------------------------------------------------------------
+Sinogram3D::Sinogram3D(int nProj, int nR, int nRings, float rFov, float axialFov, float rScanner,
+                       const std::vector<int>& mn, const std::vector<int>& mx)
+    : numProj(nProj), numProjSubset(nProj), numR(nR), numRings(nRings), numSinos(0), radioFov_mm(rFov),
+      axialFov_mm(axialFov), radioScanner_mm(rScanner), minRD(mn), maxRD(mx) {
+  apirl_sino3d_geom g = geom();
+  numSinos = std::max(0, apirl_sino3d_ring_z(&g, nullptr));
+  // Sinograms per segment, enumerated as Sinogram3D::readFromInterfile does.
+  sinosPerSegment.clear();
+  for (size_t s = 0; s < minRD.size(); s++) {
+    int n = 0;
+    for (int z1 = 0; z1 < 2 * numRings; z1++) {
+      bool hit = false;
+      int z1a = z1;
+      for (int z2 = 0; z2 < numRings; z2++, z1a--)
+        if (z1a - z2 <= maxRD[s] && z1a - z2 >= minRD[s] && z1a >= 0 && z1a < numRings) hit = true;
+      n += hit;
+    }
+    sinosPerSegment.push_back(n);
+  }
+  bins.assign((size_t)numSinos * numProj * numR, 0.f);
+}
+
+apirl_sino3d_geom Sinogram3D::geom() const {
+  return apirl_sino3d_geom{numProj, numR, numRings, (int)minRD.size(), radioFov_mm, axialFov_mm, radioScanner_mm,
+                           minRD.data(), maxRD.data()};
+}
+
+bool Sinogram3D::FillConstant(float v) { std::fill(bins.begin(), bins.end(), v); return true; }
+
+void Sinogram3D::inverseDivideBinToBin(const Sinogram3D* m) {
+  for (size_t i = 0; i < bins.size(); i++) {
+    float num = m->bins[i], den = bins[i];
+    bins[i] = (num != 0 && den != 0) ? num / den : 0.f;
+  }
+}
+void Sinogram3D::addBinToBin(const Sinogram3D* a) { for (size_t i = 0; i < bins.size(); i++) bins[i] = bins[i] + a->bins[i]; }
+void Sinogram3D::multiplyBinToBin(const Sinogram3D* a) { for (size_t i = 0; i < bins.size(); i++) bins[i] = bins[i] * a->bins[i]; }
+
+float Sinogram3D::getLikelihoodValue(const Sinogram3D* ref) const {
+  double l = 0;
+  for (size_t i = 0; i < bins.size(); i++)
+    if (bins[i] != 0) l += (double)ref->bins[i] * std::log((double)bins[i]) - (double)bins[i];
+  return (float)l;
+}
+
+Sinogram3D* Sinogram3D::getSubset(int s, int S) const {
+  Sinogram3D* o = new Sinogram3D(*this);
+  int nk = (int)std::floor((float)numProj / (float)S);
+  if ((numProj % S) > s) nk++;
+  o->numProjSubset = nk;
+  o->subset = s;
+  o->nsubsets = S;
+  o->bins.assign((size_t)numSinos * nk * numR, 0.f);
+  for (int g = 0; g < numSinos; g++)
+    for (int k = 0; k < nk; k++)
+      memcpy(&o->bins[((size_t)g * nk + k) * numR], &bins[((size_t)g * numProj + s + S * k) * numR],
+             sizeof(float) * numR);
+  return o;
+}
+
+// 3D sinogram interfile with the keys Sinogram3D::writeInterfile writes and
+// readFromInterfile reads (data/src/Sinogram3D.cpp:106-471, :609-748).
+bool Sinogram3D::readFromInterfile(const char* header) {
+  std::string v, dataName;
+  if (interfile_read(header, "!name of data file", &dataName)) { strError = "missing !name of data file"; return false; }
+  if (interfile_read(header, "number of dimensions", &v) || atoi(v.c_str()) != 4) {
+    strError = "a 3D sinogram has four dimensions";
+    return false;
+  }
+  if (interfile_read(header, "!matrix size [4]", &v)) { strError = "missing !matrix size [4]"; return false; }
+  int nseg = atoi(v.c_str());
+  std::vector<int> nsin, mn, mx;
+  if (interfile_read(header, "!matrix size [3]", &v)) { strError = "missing !matrix size [3]"; return false; }
+  nsin = parse_list(v);
+  if (interfile_read(header, "minimum ring difference per segment", &v)) { strError = "missing minimum ring difference"; return false; }
+  mn = parse_list(v);
+  if (interfile_read(header, "maximum ring difference per segment", &v)) { strError = "missing maximum ring difference"; return false; }
+  mx = parse_list(v);
+  if ((int)nsin.size() != nseg || (int)mn.size() != nseg || (int)mx.size() != nseg) {
+    strError = "segment lists do not match the number of segments";
+    return false;
+  }
+  if (interfile_read(header, "!matrix size [2]", &v)) { strError = "missing !matrix size [2]"; return false; }
+  int np = atoi(v.c_str());
+  if (interfile_read(header, "!matrix size [1]", &v)) { strError = "missing !matrix size [1]"; return false; }
+  int nr = atoi(v.c_str());
+  int rings = interfile_read(header, "number of rings", &v) ? (nsin[0] + 1) / 2 : atoi(v.c_str());
+  Sinogram3D fresh(np, nr, rings, radioFov_mm, axialFov_mm, radioScanner_mm, mn, mx);
+  for (int s = 0; s < nseg; s++)
+    if (fresh.sinosPerSegment[s] != nsin[s]) {
+      strError = "sinograms per segment do not match the ring differences";
+      return false;
+    }
+  *this = fresh;
+  return read_floats(data_path(header, dataName), bins.data(), bins.size(), &strError);
+}
+
+bool Sinogram3D::writeInterfile(const char* path) const {
+  std::string hdr = std::string(path) + ".h33", dat = std::string(path) + ".i33";
+  std::ofstream f(hdr);
+  if (!f) return false;
+  const char* e = "\r\n";
+  f << "!INTERFILE :=" << e << "!imaging modality := nucmed" << e << "!originating system := apirl_b200" << e
+    << "!version of keys := 3.3" << e << "!name of data file := " << base_of(dat) << e
+    << "!GENERAL IMAGE DATA :=" << e << "!type of data := PET" << e << "!imagedata byte order := LITTLEENDIAN" << e
+    << "!number format := short float" << e << "!number of bytes per pixel := 4" << e
+    << "number of dimensions := 4" << e << "matrix axis label [4] := segment" << e
+    << "!matrix size [4] := " << minRD.size() << e << "matrix axis label [2] := view" << e
+    << "!matrix size [2] := " << numProjSubset << e << "matrix axis label [1] := tangential coordinate" << e
+    << "!matrix size [1] := " << numR << e << "matrix axis label [3] := axial coordinate" << e
+    << "!matrix size [3] := {";
+  for (size_t i = 0; i < sinosPerSegment.size(); i++) f << (i ? "," : "") << sinosPerSegment[i];
+  f << "}" << e << "minimum ring difference per segment := {";
+  for (size_t i = 0; i < minRD.size(); i++) f << (i ? "," : "") << minRD[i];
+  f << "}" << e << "maximum ring difference per segment := {";
+  for (size_t i = 0; i < maxRD.size(); i++) f << (i ? "," : "") << maxRD[i];
+  f << "}" << e << "number of rings := " << numRings << e << "!END OF INTERFILE :=" << e;
+  f.close();
+  return write_floats(dat, bins.data(), bins.size());
+}
+
+Sinogram3DCylindricalPet::Sinogram3DCylindricalPet(const char* header, float rFov, float zFov, float rScanner)
+    : Sinogram3D(1, 1, 1, rFov, zFov, rScanner, {0}, {0}) {
+  readFromInterfile(header);
+}
+
+// ---- CuSiddonProjector ---------------------------------------------------------
+struct CuSiddonProjector::State {
+  apirl_projector* p = nullptr;
+  bool is3d = false;
+  apirl_image_geom ig{};
+  std::vector<int> mn, mx;
+  int np = 0, nr = 0, rings = 0;
+  float rfov = 0, afov = 0, rsc = 0;
+  float *d_img = nullptr, *d_a = nullptr, *d_b = nullptr;
+  size_t nimg = 0, nsino = 0;
+  cudaStream_t stream = nullptr;
+};
+
+CuSiddonProjector::CuSiddonProjector(int nSamples, int nAxialSamples, int gpuId) : st(new State), device(gpuId) {
+  if (nSamples != 1 || nAxialSamples != 1)
+    strError = "only one LOR per bin (numSamplesOnDetector = numAxialSamplesOnDetector = 1) is implemented";
+}
+
+CuSiddonProjector::~CuSiddonProjector() {
+  if (st->p) apirl_projector_destroy(st->p);
+  int prev = 0;
+  cudaGetDevice(&prev);
+  cudaSetDevice(device);
+  cudaFree(st->d_img);
+  cudaFree(st->d_a);
+  cudaFree(st->d_b);
+  if (st->stream) cudaStreamDestroy(st->stream);
+  cudaSetDevice(prev);
+  delete st;
+}
+
+static bool same_img(const apirl_image_geom& a, const apirl_image_geom& b) {
+  return a.nx == b.nx && a.ny == b.ny && a.nz == b.nz && a.dx == b.dx && a.dy == b.dy && a.dz == b.dz;
+}
+
+bool CuSiddonProjector::prepare2d(const Image* img, const Sinogram2D* s) {
+  apirl_image_geom ig = img->geom();
+  apirl_sino2d_geom sg = s->geom();
+  if (st->p && !st->is3d && same_img(ig, st->ig) && st->np == sg.n_proj && st->nr == sg.n_r && st->rfov == sg.r_fov &&
+      st->rsc == sg.r_scanner)
+    return true;
+  if (st->p) apirl_projector_destroy(st->p);
+  st->p = nullptr;
+  if (apirl_projector_create_2d(&ig, &sg, device, &st->p) != APIRL_OK) { strError = apirl_last_error(); return false; }
+  st->is3d = false; st->ig = ig; st->np = sg.n_proj; st->nr = sg.n_r; st->rfov = sg.r_fov; st->rsc = sg.r_scanner;
+  return true;
+}
+
+bool CuSiddonProjector::prepare3d(const Image* img, const Sinogram3D* s) {
+  apirl_image_geom ig = img->geom();
+  if (st->p && st->is3d && same_img(ig, st->ig) && st->np == s->getNumProjFull() && st->nr == s->getNumR() &&
+      st->rings == s->getNumRings() && st->rfov == s->getRadioFov_mm() && st->afov == s->getAxialFoV_mm() &&
+      st->rsc == s->getRadioScanner_mm() && st->mn == s->minRingDiff() && st->mx == s->maxRingDiff())
+    return true;
+  if (st->p) apirl_projector_destroy(st->p);
+  st->p = nullptr;
+  apirl_sino3d_geom sg = s->geom();
+  if (apirl_projector_create_3d(&ig, &sg, device, &st->p) != APIRL_OK) { strError = apirl_last_error(); return false; }
+  st->is3d = true; st->ig = ig; st->np = s->getNumProjFull(); st->nr = s->getNumR(); st->rings = s->getNumRings();
+  st->rfov = s->getRadioFov_mm(); st->afov = s->getAxialFoV_mm(); st->rsc = s->getRadioScanner_mm();
+  st->mn = s->minRingDiff(); st->mx = s->maxRingDiff();
+  return true;
+}
+
+// op: 0 project (a = unused, out_sino written), 1 backproject (a), 2 divide-and-backproject (a / b).
+bool CuSiddonProjector::run(int op, Image* img, const float* a, const float* b, float* out_sino, size_t nbins,
+                            int subset, int nsub) {
+  int prev = 0;
+  cudaGetDevice(&prev);
+  struct Restore { int d; ~Restore() { cudaSetDevice(d); } } restore{prev};
+  if (cudaSetDevice(device) != cudaSuccess) { strError = "cudaSetDevice failed"; return false; }
+  if (!st->stream && cudaStreamCreateWithFlags(&st->stream, cudaStreamNonBlocking) != cudaSuccess) {
+    strError = "cudaStreamCreate failed";
+    return false;
+  }
+  const size_t nv = (size_t)img->getPixelCount();
+  auto grow = [&](float** p, size_t* have, size_t n) {
+    if (*have >= n) return true;
+    cudaFree(*p);
+    *p = nullptr;
+    if (cudaMalloc(p, n * sizeof(float)) != cudaSuccess) return false;
+    *have = n;
+    return true;
+  };
+  size_t dummy = st->nsino;
+  if (!grow(&st->d_img, &st->nimg, nv) || !grow(&st->d_a, &dummy, nbins)) { strError = "device allocation failed"; return false; }
+  if (op == 2) {
+    size_t have_b = st->d_b ? st->nsino : 0;
+    if (!grow(&st->d_b, &have_b, nbins)) { strError = "device allocation failed"; return false; }
+  }
+  st->nsino = std::max(st->nsino, nbins);
+  cudaStream_t s = st->stream;
+  apirl_status rc;
+  if (op == 0) {
+    cudaMemcpyAsync(st->d_img, img->getPixelsPtr(), nv * sizeof(float), cudaMemcpyHostToDevice, s);
+    // 2D bins with r > rFov keep their values (SiddonProjector.cpp:166-173).
+    cudaMemcpyAsync(st->d_a, out_sino, nbins * sizeof(float), cudaMemcpyHostToDevice, s);
+    rc = apirl_project(st->p, st->d_img, st->d_a, subset, nsub, s);
+    if (rc == APIRL_OK) cudaMemcpyAsync(out_sino, st->d_a, nbins * sizeof(float), cudaMemcpyDeviceToHost, s);
+  } else {
+    cudaMemcpyAsync(st->d_img, img->getPixelsPtr(), nv * sizeof(float), cudaMemcpyHostToDevice, s);
+    cudaMemcpyAsync(st->d_a, a, nbins * sizeof(float), cudaMemcpyHostToDevice, s);
+    if (op == 2) cudaMemcpyAsync(st->d_b, b, nbins * sizeof(float), cudaMemcpyHostToDevice, s);
+    rc = op == 1 ? apirl_backproject(st->p, st->d_a, st->d_img, subset, nsub, s)
+                 : apirl_divide_and_backproject(st->p, st->d_a, st->d_b, st->d_img, subset, nsub, s);
+    if (rc == APIRL_OK) cudaMemcpyAsync(img->getPixelsPtr(), st->d_img, nv * sizeof(float), cudaMemcpyDeviceToHost, s);
+  }
+  if (rc != APIRL_OK) { strError = apirl_last_error(); cudaStreamSynchronize(s); return false; }
+  if (cudaStreamSynchronize(s) != cudaSuccess) { strError = cudaGetErrorString(cudaGetLastError()); return false; }
+  return true;
+}
+
+bool CuSiddonProjector::Project(Image* img, Sinogram2D* s) {
+  return prepare2d(img, s) && run(0, img, nullptr, nullptr, s->getSinogramPtr(), (size_t)s->getNumProj() * s->getNumR(), -1, 1);
+}
+bool CuSiddonProjector::Backproject(Sinogram2D* s, Image* img) {
+  return prepare2d(img, s) && run(1, img, s->getSinogramPtr(), nullptr, nullptr, (size_t)s->getNumProj() * s->getNumR(), -1, 1);
+}
+bool CuSiddonProjector::DivideAndBackproject(Sinogram2D* in, Sinogram2D* est, Image* img) {
+  return prepare2d(img, in) &&
+         run(2, img, in->getSinogramPtr(), est->getSinogramPtr(), nullptr, (size_t)in->getNumProj() * in->getNumR(), -1, 1);
+}
+bool CuSiddonProjector::Project(Image* img, Sinogram3D* s) {
+  return prepare3d(img, s) &&
+         run(0, img, nullptr, nullptr, s->getSinogramPtr(), (size_t)s->getBinCount(), s->subsetIndex(), s->subsetCount());
+}
+bool CuSiddonProjector::Backproject(Sinogram3D* s, Image* img) {
+  return prepare3d(img, s) &&
+         run(1, img, s->getSinogramPtr(), nullptr, nullptr, (size_t)s->getBinCount(), s->subsetIndex(), s->subsetCount());
+}
+bool CuSiddonProjector::DivideAndBackproject(Sinogram3D* in, Sinogram3D* est, Image* img) {
+  return prepare3d(img, in) && run(2, img, in->getSinogramPtr(), est->getSinogramPtr(), nullptr,
+                                   (size_t)in->getBinCount(), in->subsetIndex(), in->subsetCount());
+}
+
+// ---- Mlem ----------------------------------------------------------------------
+Mlem::Mlem(Image* init, std::string path, std::string prefix, int iters, int saveInterval, bool saveInter,
+           bool sensFromFile, Projector* fwd, Projector* back)
+    : initialEstimate(init), pathSalida(path), outputFilenamePrefix(prefix), numIterations(iters),
+      saveIterationInterval(saveInterval), saveIntermediate(saveInter), sensitivityImageFromFile(sensFromFile),
+      forwardprojector(fwd), backprojector(back) {
+  reconstructionImage = new Image(init->getSize());
+  sensitivityImage = new Image(init->getSize());
+}
+
+Mlem::~Mlem() {
+  delete reconstructionImage;
+  delete sensitivityImage;
+}
+
+// <prefix>.log with the key/value lines and rows of numbers of Logger
+// (data/inc/Logger.h:93-148), wall-clock times instead of clock().
+void Mlem::writeLog(const std::string& type, const std::string& input, double totalMs,
+                    const std::vector<double>& iterMs) const {
+  std::ofstream f(outputFilenamePrefix + ".log");
+  if (!f) return;
+  f << "######## " << type << " Reconstruction #########\n";
+  f << "Name: " << outputFilenamePrefix << "\nType: " << type << "\nIterations: " << numIterations << "\n";
+  f << "Input Projections: " << input << "\n";
+  SizeImage s = initialEstimate->getSize();
+  f << "Image Size: " << s.nPixelsX << "[x] x " << s.nPixelsY << "[y] x " << s.nPixelsZ << "[z]\n";
+  f << "Device: GPU (apirl_b200)\n_______RESULTADOS DE RECONSTRUCCION_______\n";
+  f << "Tiempo Total de Reconstrucción: " << totalMs << "\n";
+  f << "Tiempos de Reconstrucción por Iteración [mseg]\n";
+  for (double t : iterMs) f << t << "\t";
+  f << "\nLikelihood por Iteración:\n";
+  f.precision(12);
+  for (double l : likelihood) f << l << "\t";
+  f << "\n";
+}
+
+// ---- Mlem2d --------------------------------------------------------------------
+Mlem2d::Mlem2d(Sinogram2D* in, Image* init, std::string path, std::string prefix, int iters, int saveInterval,
+               bool saveInter, bool sensFromFile, Projector* fwd, Projector* back)
+    : Mlem(init, path, prefix, iters, saveInterval, saveInter, sensFromFile, fwd, back), inputProjection(in) {
+  inputProjection->setRadioFov_mm(init->getFovRadio());  // Mlem2d.cpp:12
+}
+
+Mlem2d::~Mlem2d() { delete multiplicative; delete additive; }
+
+bool Mlem2d::setMultiplicativeProjection(const std::string& fn) {
+  delete multiplicative;
+  multiplicative = inputProjection->Copy();
+  return multiplicative->readFromInterfile(fn.c_str());
+}
+bool Mlem2d::setMultiplicativeProjection(Sinogram2D* s) { delete multiplicative; multiplicative = s->Copy(); return true; }
+bool Mlem2d::setAdditiveProjection(const std::string& fn) {
+  delete additive;
+  additive = inputProjection->Copy();
+  return additive->readFromInterfile(fn.c_str());
+}
+bool Mlem2d::setAdditiveProjection(Sinogram2D* s) { delete additive; additive = s->Copy(); return true; }
+
+bool Mlem2d::Reconstruct() {
+  double t0 = now_ms();
+  if (!dynamic_cast<CuSiddonProjector*>(forwardprojector) || !dynamic_cast<CuSiddonProjector*>(backprojector)) {
+    strError = "Mlem2d runs on the GPU and needs CuSiddonProjector as forward and back projector";
+    return false;
+  }
+  int dev = static_cast<CuSiddonProjector*>(forwardprojector)->gpuId();
+  apirl_image_geom ig = initialEstimate->geom();
+  apirl_sino2d_geom sg = inputProjection->geom();
+  likelihood.assign(numIterations + 1, 0.0);
+  apirl_status rc = apirl_mlem_2d(&ig, &sg, inputProjection->getSinogramPtr(),
+                                  multiplicative ? multiplicative->getSinogramPtr() : nullptr,
+                                  additive ? additive->getSinogramPtr() : nullptr, initialEstimate->getPixelsPtr(),
+                                  numIterations, dev, reconstructionImage->getPixelsPtr(), likelihood.data(),
+                                  sensitivityImage->getPixelsPtr());
+  if (rc != APIRL_OK) { strError = apirl_last_error(); return false; }
+  double t1 = now_ms();
+  sensitivityImage->writeInterfile((outputFilenamePrefix + "_sensitivity").c_str());
+  reconstructionImage->writeInterfile((outputFilenamePrefix + "_final").c_str());
+  writeLog("ML-EM", "2D Sinogram", t1 - t0, {});
+  return true;
+}
+
+// ---- MlemSinogram3d / OsemSinogram3d -------------------------------------------
+MlemSinogram3d::MlemSinogram3d(Sinogram3D* in, Image* init, std::string path, std::string prefix, int iters,
+                               int saveInterval, bool saveInter, bool sensFromFile, Projector* fwd, Projector* back)
+    : Mlem(init, path, prefix, iters, saveInterval, saveInter, sensFromFile, fwd, back),
+      inputProjection(in->Copy()) {}
+
+MlemSinogram3d::~MlemSinogram3d() { delete inputProjection; delete multiplicative; delete additive; }
+
+bool MlemSinogram3d::setMultiplicativeProjection(const std::string& fn) {
+  delete multiplicative;
+  multiplicative = inputProjection->Copy();
+  return multiplicative->readFromInterfile(fn.c_str());
+}
+bool MlemSinogram3d::setMultiplicativeProjection(Sinogram3D* s) { delete multiplicative; multiplicative = s->Copy(); return true; }
+bool MlemSinogram3d::setAdditiveProjection(const std::string& fn) {
+  delete additive;
+  additive = inputProjection->Copy();
+  return additive->readFromInterfile(fn.c_str());
+}
+bool MlemSinogram3d::setAdditiveProjection(Sinogram3D* s) { delete additive; additive = s->Copy(); return true; }
+
+bool MlemSinogram3d::deviceResident() const {
+  return dynamic_cast<CuSiddonProjector*>(forwardprojector) && dynamic_cast<CuSiddonProjector*>(backprojector);
+}
+
+bool MlemSinogram3d::Reconstruct() {
+  if (!deviceResident()) { strError = "MlemSinogram3d runs on the GPU and needs CuSiddonProjector"; return false; }
+  double t0 = now_ms();
+  int dev = static_cast<CuSiddonProjector*>(forwardprojector)->gpuId();
+  apirl_image_geom ig = initialEstimate->geom();
+  apirl_sino3d_geom sg = inputProjection->geom();
+  likelihood.assign(numIterations + 1, 0.0);
+  apirl_status rc = apirl_mlem_3d(&ig, &sg, inputProjection->getSinogramPtr(),
+                                  multiplicative ? multiplicative->getSinogramPtr() : nullptr,
+                                  additive ? additive->getSinogramPtr() : nullptr, initialEstimate->getPixelsPtr(),
+                                  numIterations, dev, reconstructionImage->getPixelsPtr(), likelihood.data(),
+                                  sensitivityImage->getPixelsPtr());
+  if (rc != APIRL_OK) { strError = apirl_last_error(); return false; }
+  double t1 = now_ms();
+  sensitivityImage->writeInterfile((outputFilenamePrefix + "_sensitivity").c_str());
+  reconstructionImage->writeInterfile((outputFilenamePrefix + "_final").c_str());
+  writeLog("ML-EM", "Sinogram3D", t1 - t0, {});
+  return true;
+}
+
+OsemSinogram3d::OsemSinogram3d(Sinogram3D* in, Image* init, std::string path, std::string prefix, int iters,
+                               int saveInterval, bool saveInter, bool sensFromFile, Projector* fwd, Projector* back,
+                               int nsub)
+    : MlemSinogram3d(in, init, path, prefix, iters, saveInterval, saveInter, sensFromFile, fwd, back),
+      numSubsets(nsub) {}
+
+bool OsemSinogram3d::Reconstruct() {
+  if (!deviceResident()) { strError = "OsemSinogram3d runs on the GPU and needs CuSiddonProjector"; return false; }
+  double t0 = now_ms();
+  int dev = static_cast<CuSiddonProjector*>(forwardprojector)->gpuId();
+  apirl_image_geom ig = initialEstimate->geom();
+  apirl_sino3d_geom sg = inputProjection->geom();
+  likelihood.assign((size_t)numIterations * numSubsets + 1, 0.0);
+  apirl_status rc = apirl_osem_3d(&ig, &sg, inputProjection->getSinogramPtr(),
+                                  multiplicative ? multiplicative->getSinogramPtr() : nullptr,
+                                  additive ? additive->getSinogramPtr() : nullptr, initialEstimate->getPixelsPtr(),
+                                  numIterations, numSubsets, dev, reconstructionImage->getPixelsPtr(),
+                                  likelihood.data(), sensitivityImage->getPixelsPtr());
+  if (rc != APIRL_OK) { strError = apirl_last_error(); return false; }
+  double t1 = now_ms();
+  sensitivityImage->writeInterfile((outputFilenamePrefix + "_sensitivity_subset_0").c_str());
+  reconstructionImage->writeInterfile((outputFilenamePrefix + "_final").c_str());
+  writeLog("OSEM", "Sinogram3D", t1 - t0, {});
+  return true;
+}
+
+}  // namespace apirl

@@ -313,6 +313,40 @@ int ref_mlem_2d(int nx, int ny, float dx, float dy, const float* init,
   return 0;
 }
 
+// ---- interfile output of the reference (format fixtures) -------------------
+int ref_sino3d_write(void* hv, const char* path_no_ext) {
+  return ((Sino3DHandle*)hv)->sino->writeInterfile(std::string(path_no_ext)) ? 0 : 1;
+}
+
+int ref_image_write(int nx, int ny, int nz, float dx, float dy, float dz, const float* px, const char* path_no_ext) {
+  Image* im = make_image(nx, ny, nz, dx, dy, dz, px);
+  int rc = im->writeInterfile((char*)path_no_ext) ? 0 : 1;
+  delete im;
+  return rc;
+}
+
+// Image::readFromInterfile (medcon); dims = {nx, ny, nz}, pix = {dx, dy, dz}.
+int ref_image_read(const char* header, int* dims, float* pix, float* out, long cap) {
+  Image* im = new Image();
+  if (!im->readFromInterfile((char*)header)) { delete im; return 1; }
+  SizeImage s = im->getSize();
+  dims[0] = s.nPixelsX; dims[1] = s.nPixelsY; dims[2] = s.nPixelsZ;
+  pix[0] = s.sizePixelX_mm; pix[1] = s.sizePixelY_mm; pix[2] = s.sizePixelZ_mm;
+  long n = (long)s.nPixelsX * s.nPixelsY * s.nPixelsZ;
+  if (out && n <= cap) memcpy(out, im->getPixelsPtr(), sizeof(float) * n);
+  return 0;
+}
+
+// Sinogram3DCylindricalPet(header, ...) reading; returns bins copied.
+long ref_sino3d_read(const char* header, float rFov, float zFov, float rScanner, float* out, long cap,
+                     int* nseg_out) {
+  Sinogram3DCylindricalPet* s = new Sinogram3DCylindricalPet((char*)header, rFov, zFov, rScanner);
+  long n = s->getBinCount();
+  *nseg_out = s->getNumSegments();
+  if (out && n <= cap) copy_out(s, out);
+  return n;
+}
+
 // ---- 3D -------------------------------------------------------------------
 void* ref_sino3d_create(const char* tmpdir, int nProj, int nR, int nRings, float rFov, float axialFov,
                         float rScanner, int nSeg, const int* nSinos, const int* minRD, const int* maxRD,

@@ -96,6 +96,21 @@ def main():
     R.set_threads(os.cpu_count() or 1)
     np.savez_compressed(os.path.join(HERE, "golden_small.npz"), **out)
 
+    # ---- interfile files written by the reference's own writers ---------------
+    iodir = os.path.join(HERE, "ref_io")
+    os.makedirs(iodir, exist_ok=True)
+    sgio = Sino3DGeom(8, 6, 3, 20.0, 12.0, 60.0, [0, 1, -1], [0, 1, -1])
+    vals = (np.arange(sgio.n_bins, dtype=np.float32) * 0.5 - 7).astype(np.float32)
+    hio = R.sino3d(sgio, vals)
+    R.write_sino3d(hio, os.path.join(iodir, "sino3d"))
+    igio = ImageGeom(8, 6, 3, 2.5, 2.0, 3.25)
+    R.write_image(igio, (np.arange(igio.n_voxels, dtype=np.float32) * 0.25 + 1).astype(np.float32),
+                  os.path.join(iodir, "image"))
+    # medcon writes the data file's absolute path; keep the fixture relocatable.
+    hp = os.path.join(iodir, "image.h33")
+    txt = open(hp, "rb").read().replace(os.path.join(iodir, "image.i33").encode(), b"image.i33")
+    open(hp, "wb").write(txt)
+
     # ---- full 3D OSEM geometry ----------------------------------------------
     ig, sg = workloads.c2_geometry()
     lor = R.lor_points_2d(sg.n_proj, sg.n_r, sg.r_fov, sg.r_scanner)

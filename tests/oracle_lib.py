@@ -236,6 +236,11 @@ class RefHarness:
         L.ref_backproject_3d.argtypes = [_vp, _i, _i, _i, _i, _i, _f, _f, _f, _vp, _vp]
         L.ref_osem_3d_subiteration.argtypes = [_vp, _i, _i, _i, _i, _i, _f, _f, _f, _vp, _vp, _vp]
         L.ref_osem_3d.argtypes = [_vp, _i, _i, _i, _f, _f, _f, _vp, _i, _i, ctypes.c_char_p, _vp, _vp, _vp]
+        L.ref_sino3d_write.argtypes = [_vp, ctypes.c_char_p]
+        L.ref_image_write.argtypes = [_i, _i, _i, _f, _f, _f, _vp, ctypes.c_char_p]
+        L.ref_image_read.argtypes = [ctypes.c_char_p, _vp, _vp, _vp, _l]
+        L.ref_sino3d_read.argtypes = [ctypes.c_char_p, _f, _f, _f, _vp, _l, _vp]
+        L.ref_sino3d_read.restype = _l
         self._tmp = tempfile.mkdtemp(prefix="apirl_ref_")
 
     def set_threads(self, n):
@@ -311,6 +316,27 @@ class RefHarness:
         lik = np.zeros(1, np.float32)
         self.L.ref_osem_3d_subiteration(h, subset, nsub, *_img_args(ig), _p(x), _p(sens), _p(lik))
         return float(lik[0])
+
+    def write_sino3d(self, h, path_no_ext):
+        assert self.L.ref_sino3d_write(h, path_no_ext.encode()) == 0
+
+    def write_image(self, ig, px, path_no_ext):
+        px = np.ascontiguousarray(px, np.float32)
+        assert self.L.ref_image_write(*_img_args(ig), _p(px), path_no_ext.encode()) == 0
+
+    def read_image(self, header, cap=1 << 24):
+        dims = np.zeros(3, np.int32)
+        pix = np.zeros(3, np.float32)
+        out = np.zeros(cap, np.float32)
+        if self.L.ref_image_read(header.encode(), _p(dims), _p(pix), _p(out), cap) != 0:
+            raise RuntimeError("reference could not read " + header)
+        return dims, pix, out[:int(np.prod(dims))]
+
+    def read_sino3d(self, header, sg, cap=1 << 26):
+        out = np.zeros(cap, np.float32)
+        nseg = np.zeros(1, np.int32)
+        n = self.L.ref_sino3d_read(header.encode(), sg.r_fov, sg.axial_fov, sg.r_scanner, _p(out), cap, _p(nseg))
+        return out[:n], int(nseg[0])
 
     def osem_3d(self, h, ig, init, iters, nsub):
         init = np.ascontiguousarray(init, np.float32)
