@@ -17,6 +17,9 @@ APIRL_ERR_OOM = 3
 APIRL_ERR_NOT_SUPPORTED = 4
 APIRL_ERR_ABORTED = 5
 
+APIRL_ALPHA_F32 = 0
+APIRL_ALPHA_F64 = 1
+
 APIRL_F32 = 0
 APIRL_U32 = 1
 APIRL_U16 = 2
@@ -56,6 +59,7 @@ SIGNATURES = {
     "apirl_projector_num_bins": (_i64, [_vp, _i, _i]),
     "apirl_projector_num_sinograms": (_i, [_vp]),
     "apirl_projector_tables": (_i, [_vp, _vp, _vp]),
+    "apirl_projector_set_alpha_precision": (_i, [_vp, _i]),
     "apirl_count_steps": (_i, [_vp, _i, _i, _vp, _vp]),
     "apirl_project": (_i, [_vp, _vp, _vp, _i, _i, _vp]),
     "apirl_backproject": (_i, [_vp, _vp, _vp, _i, _i, _vp]),

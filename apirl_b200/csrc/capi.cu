@@ -198,6 +198,12 @@ apirl_status apirl_projector_create_3d(const apirl_image_geom* img, const apirl_
   p->t.n_r = sino->n_r;
   p->t.n_sinos = p->host.n_sinos;
   p->t.is3d = 1;
+  p->n_rings = sino->n_rings;
+  p->r_fov = sino->r_fov;
+  p->axial_fov = sino->axial_fov;
+  p->r_scanner = sino->r_scanner;
+  p->min_rd.assign(sino->min_ring_diff, sino->min_ring_diff + sino->n_segments);
+  p->max_rd.assign(sino->max_ring_diff, sino->max_ring_diff + sino->n_segments);
   if ((int64_t)p->t.n_sinos * p->t.n_proj * p->t.n_r >= ((int64_t)1 << 40)) {
     delete p;
     return fail(APIRL_ERR_INVALID, "sinogram too large");
@@ -216,6 +222,8 @@ void apirl_projector_destroy(apirl_projector* p) {
   cudaFree(p->d_partials);
   cudaFree(p->d_minmax);
   cudaFree(p->d_scalars);
+  cudaFree(p->d_lor64);
+  cudaFree(p->d_z64);
   delete p;
 }
 
@@ -234,6 +242,32 @@ apirl_status apirl_projector_tables(const apirl_projector* p, float* h_lor, floa
   return APIRL_OK;
 }
 
+apirl_status apirl_projector_set_alpha_precision(apirl_projector* p, int mode) {
+  if (!p) return fail(APIRL_ERR_INVALID, "null projector");
+  if (mode != APIRL_ALPHA_F32 && mode != APIRL_ALPHA_F64) return fail(APIRL_ERR_INVALID, "unknown alpha mode %d", mode);
+  if (mode == APIRL_ALPHA_F64 && !p->is3d)
+    return fail(APIRL_ERR_NOT_SUPPORTED, "the FP64-alpha walk is implemented for 3D projectors");
+  DEVICE_SCOPE(p->device);
+  if (mode == APIRL_ALPHA_F64 && !p->d_lor64) {
+    std::vector<double> lor, z;
+    apirl::build_tables_3d_f64(p->t.n_proj, p->t.n_r, p->n_rings, p->r_fov, p->axial_fov, p->r_scanner,
+                               (int)p->min_rd.size(), p->min_rd.data(), p->max_rd.data(), lor, z);
+    CK(cudaMalloc(&p->d_lor64, lor.size() * sizeof(double)));
+    CK(cudaMemcpy(p->d_lor64, lor.data(), lor.size() * sizeof(double), cudaMemcpyHostToDevice));
+    CK(cudaMalloc(&p->d_z64, z.size() * sizeof(double)));
+    CK(cudaMemcpy(p->d_z64, z.data(), z.size() * sizeof(double), cudaMemcpyHostToDevice));
+    p->pg.lor = p->d_lor64;
+    p->pg.z = p->d_z64;
+    p->pg.nx = p->g.nx; p->pg.ny = p->g.ny; p->pg.nz = p->g.nz;
+    p->pg.dx = p->g.dx; p->pg.dy = p->g.dy; p->pg.dz = p->g.dz;
+    p->pg.rfov = ((double)p->g.dx * p->g.nx) / 2;
+    p->pg.offz = (double)p->g.dz / 2;
+  }
+  p->alpha_mode = mode;
+  p->pg.enabled = mode == APIRL_ALPHA_F64;
+  return APIRL_OK;
+}
+
 apirl_status apirl_count_steps(apirl_projector* p, int subset, int nsubsets, int32_t* d_steps, void* stream) {
   apirl_status st = check_subset(p, subset, nsubsets);
   if (st) return st;
@@ -249,7 +283,8 @@ apirl_status apirl_project(apirl_projector* p, const float* d_image, float* d_si
   if (st) return st;
   if (!d_image || !d_sino) return fail(APIRL_ERR_INVALID, "null image or sinogram");
   DEVICE_SCOPE(p->device);
-  CK(apirl::launch_project(p->g, p->t, make_subset(p, subset, nsubsets), d_image, d_sino, (cudaStream_t)stream));
+  CK(apirl::launch_project(p->g, p->t, make_subset(p, subset, nsubsets), d_image, d_sino, (cudaStream_t)stream,
+                           p->pg));
   return APIRL_OK;
 }
 
@@ -260,7 +295,7 @@ apirl_status apirl_backproject(apirl_projector* p, const float* d_sino, float* d
   if (!d_image || !d_sino) return fail(APIRL_ERR_INVALID, "null image or sinogram");
   DEVICE_SCOPE(p->device);
   CK(apirl::launch_backproject(p->g, p->t, make_subset(p, subset, nsubsets), d_sino, 0, nullptr, 0, d_image,
-                               (cudaStream_t)stream));
+                               (cudaStream_t)stream, p->pg));
   return APIRL_OK;
 }
 
@@ -271,7 +306,7 @@ apirl_status apirl_divide_and_backproject(apirl_projector* p, const float* d_mea
   if (!d_image || !d_meas || !d_est) return fail(APIRL_ERR_INVALID, "null image or sinogram");
   DEVICE_SCOPE(p->device);
   CK(apirl::launch_backproject(p->g, p->t, make_subset(p, subset, nsubsets), d_meas, 0, d_est, 1, d_image,
-                               (cudaStream_t)stream));
+                               (cudaStream_t)stream, p->pg));
   return APIRL_OK;
 }
 
@@ -335,7 +370,7 @@ apirl_status apirl_em_pass(apirl_projector* p, const void* d_counts, int counts_
   cudaStream_t s = (cudaStream_t)stream;
   SubsetSel ss = make_subset(p, subset, nsubsets);
   CK(apirl::launch_em_pass(p->g, p->t, ss, d_counts, counts_dtype, counts_packed, d_add, d_x, d_bp, 1,
-                           p->is3d ? 0 : 1, p->d_partials, d_lik, s));
+                           p->is3d ? 0 : 1, p->d_partials, d_lik, s, p->pg));
   const int64_t nv = (int64_t)p->g.nx * p->g.ny * p->g.nz;
   CK(apirl::launch_update(nv, d_x, d_bp, d_sens, d_thr, thr_value, ge, 1, s));
   return APIRL_OK;
@@ -351,7 +386,8 @@ apirl_status apirl_em_project_backproject(apirl_projector* p, const void* d_coun
     return fail(APIRL_ERR_INVALID, "unknown counts dtype %d", counts_dtype);
   DEVICE_SCOPE(p->device);
   CK(apirl::launch_em_pass(p->g, p->t, make_subset(p, subset, nsubsets), d_counts, counts_dtype, counts_packed,
-                           d_add, d_x, d_bp, 1, p->is3d ? 0 : 1, p->d_partials, d_lik, (cudaStream_t)stream));
+                           d_add, d_x, d_bp, 1, p->is3d ? 0 : 1, p->d_partials, d_lik, (cudaStream_t)stream,
+                           p->pg));
   return APIRL_OK;
 }
 

@@ -114,7 +114,7 @@ apirl_status apirl_osem_3d(const apirl_image_geom* img, const apirl_sino3d_geom*
   for (int s = 0; s < nsubsets; s++) {
     SubsetSel ss;
     ss.subset = s; ss.nsub = nsubsets; ss.nk = apirl::subset_nproj(sino->n_proj, s, nsubsets);
-    DK(apirl::launch_backproject(p->g, p->t, ss, d_mult, d_mult ? 1 : 2, nullptr, 0, d_sens + nv * s, r.st));
+    DK(apirl::launch_backproject(p->g, p->t, ss, d_mult, d_mult ? 1 : 2, nullptr, 0, d_sens + nv * s, r.st, p->pg));
     DK(apirl::launch_force_positive(nv, d_sens + nv * s, r.st));
   }
   for (int s = 0; s < nsubsets; s++)

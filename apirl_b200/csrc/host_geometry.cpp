@@ -110,4 +110,44 @@ bool build_tables_3d(int n_proj, int n_r, int n_rings, float r_fov, float axial_
   return t.n_sinos > 0;
 }
 
+void build_tables_3d_f64(int n_proj, int n_r, int n_rings, float r_fov, float axial_fov, float r_scanner, int n_seg,
+                         const int* min_rd, const int* max_rd, std::vector<double>& lor, std::vector<double>& z) {
+  const double rf = r_fov, R = r_scanner, afov = axial_fov;
+  const double rinc = (2.0 * rf) / n_r, phinc = 180.0 / n_proj;
+  lor.resize((size_t)n_proj * n_r * 4);
+  for (int a = 0; a < n_proj; a++) {
+    const double phi = (a * phinc) * 0.017453292519943295769;
+    const double c = std::cos(phi), s = std::sin(phi);
+    for (int l = 0; l < n_r; l++) {
+      const double rv = rinc / 2 + l * rinc - rf;
+      const double aux = std::sqrt(R * R - rv * rv);
+      double* o = &lor[((size_t)a * n_r + l) * 4];
+      o[0] = rv * c + s * aux;
+      o[1] = rv * s - c * aux;
+      o[2] = rv * c - s * aux;
+      o[3] = rv * s + c * aux;
+    }
+  }
+  const double zinc = afov / n_rings;
+  z.clear();
+  for (int sg = 0; sg < n_seg; sg++)
+    for (int z1 = 0; z1 < 2 * n_rings; z1++) {
+      int cnt = 0;
+      double f1 = 0, l1 = 0, f2 = 0, l2 = 0;
+      int z1a = z1;
+      for (int z2 = 0; z2 < n_rings; z2++, z1a--) {
+        if ((z1a - z2) <= max_rd[sg] && (z1a - z2) >= min_rd[sg] && z1a >= 0 && z1a < n_rings) {
+          const double za = zinc / 2 + z1a * zinc, zb = zinc / 2 + z2 * zinc;
+          if (cnt == 0) { f1 = za; f2 = zb; }
+          l1 = za; l2 = zb;
+          cnt++;
+        }
+      }
+      if (cnt > 0) {
+        z.push_back((f1 + l1) / 2);
+        z.push_back((f2 + l2) / 2);
+      }
+    }
+}
+
 }  // namespace apirl

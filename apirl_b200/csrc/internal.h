@@ -17,6 +17,15 @@ struct LorTable {
   int is3d;
 };
 
+// Double-precision geometry for the FP64-alpha precision mode (3D only).
+struct PreciseGeom {
+  const double4* lor = nullptr;  // [n_proj][n_r]
+  const double2* z = nullptr;    // [n_sinos]
+  int nx = 0, ny = 0, nz = 0;
+  double dx = 0, dy = 0, dz = 0, rfov = 0, offz = 0;
+  int enabled = 0;
+};
+
 struct SubsetSel {
   int subset;  // < 0: all angles
   int nsub;
@@ -30,6 +39,9 @@ struct HostTables {
   std::vector<uint8_t> ok;  // n_r
   int n_sinos = 1;
 };
+// The same tables in double precision (double trigonometry), for FP64-alpha.
+void build_tables_3d_f64(int n_proj, int n_r, int n_rings, float r_fov, float axial_fov, float r_scanner, int n_seg,
+                         const int* min_rd, const int* max_rd, std::vector<double>& lor, std::vector<double>& z);
 void build_tables_2d(int n_proj, int n_r, float r_fov, float r_scanner, HostTables& t);
 bool build_tables_3d(int n_proj, int n_r, int n_rings, float r_fov, float axial_fov, float r_scanner, int n_seg,
                      const int* min_rd, const int* max_rd, HostTables& t);
@@ -38,11 +50,13 @@ ImgGeom make_img_geom(int nx, int ny, int nz, float dx, float dy, float dz);
 int subset_nproj(int n_proj, int subset, int nsub);
 
 // Launchers (kernels.cu).  All return cudaGetLastError() after the launch.
+// pg.enabled selects the FP64-alpha walk (3D only).
 cudaError_t launch_project(const ImgGeom& g, const LorTable& t, SubsetSel s, const float* img, float* out,
-                           cudaStream_t st);
+                           cudaStream_t st, const PreciseGeom& pg = PreciseGeom());
 // vin_mode: 0 = subset sinogram, 1 = whole sinogram read at the subset's angles, 2 = all ones.
 cudaError_t launch_backproject(const ImgGeom& g, const LorTable& t, SubsetSel s, const float* vin, int vin_mode,
-                               const float* vest, int divide, float* img, cudaStream_t st);
+                               const float* vest, int divide, float* img, cudaStream_t st,
+                               const PreciseGeom& pg = PreciseGeom());
 cudaError_t launch_count_steps(const ImgGeom& g, const LorTable& t, SubsetSel s, int32_t* steps, cudaStream_t st);
 
 // Fused EM pass.  partials: >= em_pass_blocks() doubles of scratch.
@@ -50,7 +64,7 @@ int64_t em_pass_blocks(const LorTable& t, SubsetSel s);
 // lik_mode: 0 = over e != 0, 1 = over e > 0, 2 = over ratio > 0.  back = 0: no backprojection.
 cudaError_t launch_em_pass(const ImgGeom& g, const LorTable& t, SubsetSel s, const void* counts, int counts_dtype,
                            int counts_packed, const float* add, const float* x, float* bp, int back, int lik_mode,
-                           double* partials, double* lik, cudaStream_t st);
+                           double* partials, double* lik, cudaStream_t st, const PreciseGeom& pg = PreciseGeom());
 
 cudaError_t launch_inverse_divide(int64_t n, const float* meas, float* est, cudaStream_t st);
 cudaError_t launch_add_bins(int64_t n, const float* add, float* est, cudaStream_t st);
@@ -81,6 +95,13 @@ struct apirl_projector {
   int64_t n_partials = 0;
   unsigned* d_minmax = nullptr;  // threshold reduction keys
   double* d_scalars = nullptr;   // 8 doubles of per-projector scratch (likelihood of host passes)
+  int alpha_mode = 0;            // APIRL_ALPHA_F32 (reference arithmetic) or APIRL_ALPHA_F64
+  double4* d_lor64 = nullptr;    // FP64-alpha tables, built on first use
+  double2* d_z64 = nullptr;
+  apirl::PreciseGeom pg;
+  int n_rings = 0;               // 3D geometry as given, for building the FP64 tables
+  float r_fov = 0, axial_fov = 0, r_scanner = 0;
+  std::vector<int> min_rd, max_rd;
 };
 
 // Records `msg` as the calling thread's last error and returns `code`.

@@ -58,6 +58,24 @@ __device__ __forceinline__ float ray_sum3(const ImgGeom& g, const float4 L, cons
   return acc;
 }
 
+__device__ __forceinline__ ImgGeomD geom_d(const PreciseGeom& pg) {
+  ImgGeomD g;
+  g.nx = pg.nx; g.ny = pg.ny; g.nz = pg.nz;
+  g.dx = pg.dx; g.dy = pg.dy; g.dz = pg.dz; g.rfov = pg.rfov; g.offz = pg.offz;
+  return g;
+}
+
+// FP64-alpha forward projection of one bin.
+__device__ __forceinline__ float ray_sum3d(const ImgGeomD& g, const double4 L, const double2 z,
+                                           const float* __restrict__ img, Walk3D& w) {
+  siddon3d_setup(L.x, L.y, z.x, L.z - L.x, L.w - L.y, z.y - z.x, g, w);
+  float acc = 0.f;
+  siddon3d_walk(w, g, [&](bool inb, int idx, float seg) {
+    if (inb) acc = A_ADD(acc, A_MUL(seg, __ldg(img + idx)));
+  });
+  return acc;
+}
+
 __device__ __forceinline__ float ray_sum2(const ImgGeom& g, const float4 L, const float* __restrict__ img, Walk2& w) {
   siddon2_setup(L.x, L.y, A_SUB(L.z, L.x), A_SUB(L.w, L.y), g, w);
   float acc = 0.f;
@@ -84,14 +102,20 @@ __device__ __forceinline__ double block_sum(double v) {
 }
 
 // ---------------------------------------------------------------------------
-__global__ void __launch_bounds__(kBlock) k_project3(ImgGeom g, LorTable t, SubsetSel s,
+template <bool F64A>
+__global__ void __launch_bounds__(kBlock) k_project3(ImgGeom g, LorTable t, SubsetSel s, PreciseGeom pg,
                                                      const float* __restrict__ img, float* __restrict__ out,
                                                      int64_t total) {
   const int64_t b = (int64_t)blockIdx.x * kBlock + threadIdx.x;
   if (b >= total) return;
   const BinPos p = decode(b, t, s);
-  Walk3 w;
-  out[b] = ray_sum3(g, t.lor[(int64_t)p.a * t.n_r + p.l], t.z[p.g], img, w);
+  if (F64A) {
+    Walk3D w;
+    out[b] = ray_sum3d(geom_d(pg), pg.lor[(int64_t)p.a * t.n_r + p.l], pg.z[p.g], img, w);
+  } else {
+    Walk3 w;
+    out[b] = ray_sum3(g, t.lor[(int64_t)p.a * t.n_r + p.l], t.z[p.g], img, w);
+  }
 }
 
 __global__ void __launch_bounds__(kBlock) k_project2(ImgGeom g, LorTable t, SubsetSel s,
@@ -116,7 +140,8 @@ __device__ __forceinline__ float load_bin(const float* __restrict__ v, int vin_m
   return __ldg(v + b);
 }
 
-__global__ void __launch_bounds__(kBlock) k_backproject3(ImgGeom g, LorTable t, SubsetSel s,
+template <bool F64A>
+__global__ void __launch_bounds__(kBlock) k_backproject3(ImgGeom g, LorTable t, SubsetSel s, PreciseGeom pg,
                                                          const float* __restrict__ vin, int vin_mode,
                                                          const float* __restrict__ vest, int divide,
                                                          float* __restrict__ img, int64_t total) {
@@ -126,16 +151,26 @@ __global__ void __launch_bounds__(kBlock) k_backproject3(ImgGeom g, LorTable t, 
   const float v = load_bin(vin, vin_mode, b, p, t);
   if (v == 0.f) return;
   const float e = divide ? vest[b] : 0.f;
-  const float4 L = t.lor[(int64_t)p.a * t.n_r + p.l];
-  const float2 z = t.z[p.g];
-  Walk3 w;
-  siddon3_setup(L.x, L.y, z.x, A_SUB(L.z, L.x), A_SUB(L.w, L.y), A_SUB(z.y, z.x), g, w);
-  siddon3_walk(w, g, [&](bool inb, int idx, float seg) {
+  auto scatter = [&](bool inb, int idx, float seg) {
     if (!inb) return;
     float val = A_MUL(seg, v);
     if (divide && e != 0.f) val = A_DIV(val, e);
     atomicAdd(img + idx, val);
-  });
+  };
+  if (F64A) {
+    const ImgGeomD gd = geom_d(pg);
+    const double4 L = pg.lor[(int64_t)p.a * t.n_r + p.l];
+    const double2 z = pg.z[p.g];
+    Walk3D w;
+    siddon3d_setup(L.x, L.y, z.x, L.z - L.x, L.w - L.y, z.y - z.x, gd, w);
+    siddon3d_walk(w, gd, scatter);
+  } else {
+    const float4 L = t.lor[(int64_t)p.a * t.n_r + p.l];
+    const float2 z = t.z[p.g];
+    Walk3 w;
+    siddon3_setup(L.x, L.y, z.x, A_SUB(L.z, L.x), A_SUB(L.w, L.y), A_SUB(z.y, z.x), g, w);
+    siddon3_walk(w, g, scatter);
+  }
 }
 
 // divide == 0: Backproject over every bin (SiddonProjector.cpp:34-87).
@@ -186,8 +221,9 @@ __global__ void __launch_bounds__(kBlock) k_count_steps(ImgGeom g, LorTable t, S
 // Fused EM pass: project, add, likelihood term, ratio, backproject.
 // lik_mode: 0 = term over e != 0 (3D), 1 = over e > 0 (2D), 2 = over the ratio
 // r > 0 (the final 2D value, Mlem2d.cpp:228).  back = 0 skips the backprojection.
-template <typename CT, bool IS3D>
-__global__ void __launch_bounds__(kBlock) k_em_pass(ImgGeom g, LorTable t, SubsetSel s, const CT* __restrict__ counts,
+template <typename CT, bool IS3D, bool F64A>
+__global__ void __launch_bounds__(kBlock) k_em_pass(ImgGeom g, LorTable t, SubsetSel s, PreciseGeom pg,
+                                                    const CT* __restrict__ counts,
                                                     int counts_packed, const float* __restrict__ add,
                                                     const float* __restrict__ x, float* __restrict__ bp, int back,
                                                     int lik_mode, double* __restrict__ partials, int64_t total) {
@@ -199,7 +235,19 @@ __global__ void __launch_bounds__(kBlock) k_em_pass(ImgGeom g, LorTable t, Subse
     const int64_t ci = row * t.n_r + p.l;
     const float m = load_count<CT>(counts, ci);
     const float4 L = t.lor[(int64_t)p.a * t.n_r + p.l];
-    if (IS3D) {
+    if (IS3D && F64A) {
+      const ImgGeomD gd = geom_d(pg);
+      Walk3D w;
+      float e = ray_sum3d(gd, pg.lor[(int64_t)p.a * t.n_r + p.l], pg.z[p.g], x, w);
+      if (add) e = A_ADD(e, __ldg(add + ci));
+      const float r = (m != 0.f && e != 0.f) ? A_DIV(m, e) : 0.f;
+      if (lik_mode == 2) { if (r > 0.f) term = (double)m * log((double)r) - (double)r; }
+      else if (lik_mode == 1 ? (e > 0.f) : (e != 0.f)) term = (double)m * log((double)e) - (double)e;
+      if (back && r != 0.f)
+        siddon3d_walk(w, gd, [&](bool inb, int idx, float seg) {
+          if (inb) atomicAdd(bp + idx, A_MUL(seg, r));
+        });
+    } else if (IS3D) {
       Walk3 w;
       float e = ray_sum3(g, L, t.z[p.g], x, w);
       if (add) e = A_ADD(e, __ldg(add + ci));
@@ -350,19 +398,23 @@ int64_t em_pass_blocks(const LorTable& t, SubsetSel s) {
 int64_t likelihood_blocks(int64_t n) { return stream_grid(n); }
 
 cudaError_t launch_project(const ImgGeom& g, const LorTable& t, SubsetSel s, const float* img, float* out,
-                           cudaStream_t st) {
+                           cudaStream_t st, const PreciseGeom& pg) {
   const int64_t total = (int64_t)t.n_sinos * s.nk * t.n_r;
   if (total == 0) return cudaSuccess;
-  if (t.is3d) k_project3<<<grid_for(total), kBlock, 0, st>>>(g, t, s, img, out, total);
+  if (t.is3d && pg.enabled) k_project3<true><<<grid_for(total), kBlock, 0, st>>>(g, t, s, pg, img, out, total);
+  else if (t.is3d) k_project3<false><<<grid_for(total), kBlock, 0, st>>>(g, t, s, pg, img, out, total);
   else k_project2<<<grid_for(total), kBlock, 0, st>>>(g, t, s, img, out, total);
   return cudaGetLastError();
 }
 
 cudaError_t launch_backproject(const ImgGeom& g, const LorTable& t, SubsetSel s, const float* vin, int vin_mode,
-                               const float* vest, int divide, float* img, cudaStream_t st) {
+                               const float* vest, int divide, float* img, cudaStream_t st, const PreciseGeom& pg) {
   const int64_t total = (int64_t)t.n_sinos * s.nk * t.n_r;
   if (total == 0) return cudaSuccess;
-  if (t.is3d) k_backproject3<<<grid_for(total), kBlock, 0, st>>>(g, t, s, vin, vin_mode, vest, divide, img, total);
+  if (t.is3d && pg.enabled)
+    k_backproject3<true><<<grid_for(total), kBlock, 0, st>>>(g, t, s, pg, vin, vin_mode, vest, divide, img, total);
+  else if (t.is3d)
+    k_backproject3<false><<<grid_for(total), kBlock, 0, st>>>(g, t, s, pg, vin, vin_mode, vest, divide, img, total);
   else k_backproject2<<<grid_for(total), kBlock, 0, st>>>(g, t, s, vin, vin_mode, vest, divide, img, total);
   return cudaGetLastError();
 }
@@ -376,18 +428,21 @@ cudaError_t launch_count_steps(const ImgGeom& g, const LorTable& t, SubsetSel s,
 
 cudaError_t launch_em_pass(const ImgGeom& g, const LorTable& t, SubsetSel s, const void* counts, int counts_dtype,
                            int counts_packed, const float* add, const float* x, float* bp, int back, int lik_mode,
-                           double* partials, double* lik, cudaStream_t st) {
+                           double* partials, double* lik, cudaStream_t st, const PreciseGeom& pg) {
   const int64_t total = (int64_t)t.n_sinos * s.nk * t.n_r;
   const unsigned grid = grid_for(total);
   if (total == 0) return cudaSuccess;
 #define APIRL_EM(CT)                                                                                          \
   do {                                                                                                        \
-    if (t.is3d)                                                                                               \
-      k_em_pass<CT, true><<<grid, kBlock, 0, st>>>(g, t, s, (const CT*)counts, counts_packed, add, x, bp,     \
-                                                   back, lik_mode, partials, total);                          \
+    if (t.is3d && pg.enabled)                                                                                 \
+      k_em_pass<CT, true, true><<<grid, kBlock, 0, st>>>(g, t, s, pg, (const CT*)counts, counts_packed, add, x, \
+                                                         bp, back, lik_mode, partials, total);                \
+    else if (t.is3d)                                                                                          \
+      k_em_pass<CT, true, false><<<grid, kBlock, 0, st>>>(g, t, s, pg, (const CT*)counts, counts_packed, add,   \
+                                                          x, bp, back, lik_mode, partials, total);            \
     else                                                                                                      \
-      k_em_pass<CT, false><<<grid, kBlock, 0, st>>>(g, t, s, (const CT*)counts, counts_packed, add, x, bp,    \
-                                                    back, lik_mode, partials, total);                         \
+      k_em_pass<CT, false, false><<<grid, kBlock, 0, st>>>(g, t, s, pg, (const CT*)counts, counts_packed, add,  \
+                                                           x, bp, back, lik_mode, partials, total);           \
   } while (0)
   switch (counts_dtype) {
     case APIRL_F32: APIRL_EM(float); break;

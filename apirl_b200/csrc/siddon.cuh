@@ -167,3 +167,91 @@ __device__ __forceinline__ void siddon2_walk(Walk2 w, const ImgGeom& g, V&& visi
 }
 
 }  // namespace apirl
+
+// ---------------------------------------------------------------------------
+// FP64-alpha variant (precision mode, not the reference's arithmetic): ray
+// entry/exit, first crossings and the running crossing parameters are kept in
+// double so that long oblique rays cannot misorder voxel crossings; each
+// segment length is rounded to float once.  End points come from a double
+// table built with double trigonometry.
+namespace apirl {
+
+struct ImgGeomD {
+  int nx, ny, nz;
+  double dx, dy, dz, rfov, offz;
+};
+
+struct Walk3D {
+  double ax, ay, az, axu, ayu, azu, ac, L;
+  int i, j, k, iinc, jinc, kinc, n;
+};
+
+__device__ __forceinline__ double dmin_ref(double a, double b) { return (b < a) ? b : a; }
+__device__ __forceinline__ double dmax_ref(double a, double b) { return (a < b) ? b : a; }
+
+__device__ __forceinline__ void siddon3d_setup(double p0x, double p0y, double p0z, double vx, double vy, double vz,
+                                               const ImgGeomD& g, Walk3D& w) {
+  const double rFov = g.rfov;
+  double amin, amax;
+  if (vx == 0.0) {
+    double a1 = __ddiv_rn(-rFov - p0y, vy), a2 = __ddiv_rn(rFov - p0y, vy);
+    if (a1 < a2) { amin = a1; amax = a2; } else { amin = a2; amax = a1; }
+  } else if (vy == 0.0) {
+    double a1 = __ddiv_rn(-rFov - p0x, vx), a2 = __ddiv_rn(rFov - p0x, vx);
+    if (a1 < a2) { amin = a1; amax = a2; } else { amin = a2; amax = a1; }
+  } else {
+    double ax1 = __ddiv_rn(-rFov - p0x, vx), ay1 = __ddiv_rn(-rFov - p0y, vy);
+    double ax2 = __ddiv_rn(rFov - p0x, vx), ay2 = __ddiv_rn(rFov - p0y, vy);
+    amin = dmax_ref(dmin_ref(ax1, ax2), dmin_ref(ay1, ay2));
+    amax = dmin_ref(dmax_ref(ax1, ax2), dmax_ref(ay1, ay2));
+  }
+  if (amin < 0.0 || amin > 1.0) amin = 0.0;
+  if (amax > 1.0 || amax < 0.0) amax = 1.0;
+  const double x1 = __dadd_rn(p0x, __dmul_rn(vx, amin)), y1 = __dadd_rn(p0y, __dmul_rn(vy, amin));
+  const double z1 = __dadd_rn(p0z, __dmul_rn(vz, amin));
+  const double x2 = __dadd_rn(p0x, __dmul_rn(vx, amax)), y2 = __dadd_rn(p0y, __dmul_rn(vy, amax));
+  const double z2 = __dadd_rn(p0z, __dmul_rn(vz, amax));
+  const int imin = (int)floor(__ddiv_rn(x1 + rFov, g.dx)), jmin = (int)floor(__ddiv_rn(y1 + rFov, g.dy));
+  const int kmin = (int)floor(__ddiv_rn(z1 - g.offz, g.dz));
+  const int imax = (int)floor(__ddiv_rn(x2 + rFov, g.dx)), jmax = (int)floor(__ddiv_rn(y2 + rFov, g.dy));
+  const int kmax = (int)floor(__ddiv_rn(z2 - g.offz, g.dz));
+  w.n = abs(imax - imin) + abs(jmax - jmin) + abs(kmax - kmin);
+  w.iinc = vx > 0.0 ? 1 : (vx < 0.0 ? -1 : 0);
+  w.jinc = vy > 0.0 ? 1 : (vy < 0.0 ? -1 : 0);
+  w.kinc = vz > 0.0 ? 1 : (vz < 0.0 ? -1 : 0);
+  const double ex = (p0x + vx) - p0x, ey = (p0y + vy) - p0y, ez = (p0z + vz) - p0z;
+  w.L = __dsqrt_rn(__dadd_rn(__dadd_rn(__dmul_rn(ex, ex), __dmul_rn(ey, ey)), __dmul_rn(ez, ez)));
+  w.axu = fabs(__ddiv_rn(g.dx, vx));
+  w.ayu = fabs(__ddiv_rn(g.dy, vy));
+  w.azu = fabs(__ddiv_rn(g.dz, vz));
+  const double big = 1.7976931348623157e308;
+  w.ax = vx > 0.0 ? __ddiv_rn(-rFov + (double)(imin + w.iinc) * g.dx - p0x, vx)
+       : (vx < 0.0 ? __ddiv_rn(-rFov + (double)imin * g.dx - p0x, vx) : big);
+  w.ay = vy > 0.0 ? __ddiv_rn(-rFov + (double)(jmin + w.jinc) * g.dy - p0y, vy)
+       : (vy < 0.0 ? __ddiv_rn(-rFov + (double)jmin * g.dy - p0y, vy) : big);
+  w.az = vz > 0.0 ? __ddiv_rn(g.offz + (double)(kmin + w.kinc) * g.dz - p0z, vz)
+       : (vz < 0.0 ? __ddiv_rn(g.offz + (double)kmin * g.dz - p0z, vz) : big);
+  w.ac = amin;
+  w.i = imin; w.j = jmin; w.k = kmin;
+}
+
+template <class V>
+__device__ __forceinline__ void siddon3d_walk(Walk3D w, const ImgGeomD& g, V&& visit) {
+  const int sx = w.iinc, sy = w.jinc * g.nx, sz = w.kinc * g.nx * g.ny;
+  int idx = (w.k * g.ny + w.j) * g.nx + w.i;
+  for (int m = 0; m < w.n; m++) {
+    const bool cx = (w.ax <= w.ay) && (w.ax <= w.az);
+    const bool cy = !cx && (w.ay <= w.ax) && (w.ay <= w.az);
+    const double an = cx ? w.ax : (cy ? w.ay : w.az);
+    const float seg = (float)__dmul_rn(an - w.ac, w.L);
+    const bool inb = ((unsigned)w.i < (unsigned)g.nx) & ((unsigned)w.j < (unsigned)g.ny) &
+                     ((unsigned)w.k < (unsigned)g.nz);
+    visit(inb, idx, seg);
+    w.ac = an;
+    if (cx) { w.i += w.iinc; idx += sx; w.ax += w.axu; }
+    else if (cy) { w.j += w.jinc; idx += sy; w.ay += w.ayu; }
+    else { w.k += w.kinc; idx += sz; w.az += w.azu; }
+  }
+}
+
+}  // namespace apirl

@@ -107,6 +107,10 @@ class SiddonProjector:
                                               None if z is None else z.ctypes.data_as(ctypes.c_void_p)))
         return lor, z
 
+    def set_alpha_precision(self, fp64):
+        """fp64=False: the reference's float walk (default); True: FP64 alphas (precision study)."""
+        check(self.lib.apirl_projector_set_alpha_precision(self.h, _lib.APIRL_ALPHA_F64 if fp64 else _lib.APIRL_ALPHA_F32))
+
     def count_steps(self, subset=-1, nsubsets=1, stream=None):
         import torch
         out = torch.empty(self.num_bins(subset, nsubsets), dtype=torch.int32, device=f"cuda:{self.device}")

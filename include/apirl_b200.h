@@ -47,6 +47,9 @@ enum {
 /* Element type of a measured-counts sinogram. */
 enum { APIRL_F32 = 0, APIRL_U32 = 1, APIRL_U16 = 2 };
 
+/* Arithmetic of the Siddon walk (apirl_projector_set_alpha_precision). */
+enum { APIRL_ALPHA_F32 = 0, APIRL_ALPHA_F64 = 1 };
+
 /* SizeImage (data/inc/Images.h:53-61). */
 typedef struct apirl_image_geom {
   int nx, ny, nz;
@@ -103,6 +106,13 @@ int apirl_projector_num_sinograms(const apirl_projector* p);
 /* Copies the host-built LOR table ([angle][r][p1x,p1y,p2x,p2y]) and, for 3D,
  * the per-sinogram end-point z ([sinogram][z1,z2]); either may be NULL. */
 apirl_status apirl_projector_tables(const apirl_projector* p, float* h_lor, float* h_z);
+/* Precision study mode (3D projectors).  APIRL_ALPHA_F32 (default) is the
+ * reference's float arithmetic, bit-identical to Siddon.cpp.  APIRL_ALPHA_F64
+ * computes LOR end points (double trigonometry), entry/exit alphas, first
+ * crossings and the running crossing parameters in FP64 and rounds each
+ * segment length to float; projection and accumulation stay FP32.  No
+ * counterpart in the reference, whose walk is float only. */
+apirl_status apirl_projector_set_alpha_precision(apirl_projector* p, int mode);
 /* Number of Siddon segments of every bin of a subset, written to d_steps (int32). */
 apirl_status apirl_count_steps(apirl_projector* p, int subset, int nsubsets, int32_t* d_steps, void* stream);
 
