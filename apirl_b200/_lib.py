@@ -45,6 +45,11 @@ class Sino3DGeomC(ctypes.Structure):
                 ("min_ring_diff", ctypes.POINTER(_i)), ("max_ring_diff", ctypes.POINTER(_i))]
 
 
+class JobDescC(ctypes.Structure):
+    _fields_ = [("img", ImageGeomC), ("sino", Sino3DGeomC), ("h_counts", _vp), ("counts_dtype", _i),
+                ("h_mult", _vp), ("h_add", _vp), ("h_init", _vp), ("iters", _i), ("nsubsets", _i)]
+
+
 # name -> (restype, argtypes)
 SIGNATURES = {
     "apirl_last_error": (ctypes.c_char_p, []),
@@ -77,6 +82,12 @@ SIGNATURES = {
                            _i, _vp, _vp, _vp]),
     "apirl_mlem_3d": (_i, [ctypes.POINTER(ImageGeomC), ctypes.POINTER(Sino3DGeomC), _vp, _vp, _vp, _vp, _i, _i,
                            _vp, _vp, _vp]),
+    "apirl_job_footprint": (_i64, [ctypes.POINTER(JobDescC)]),
+    "apirl_batch_create": (_i, [_i, _i64, ctypes.POINTER(_vp)]),
+    "apirl_batch_destroy": (None, [_vp]),
+    "apirl_batch_submit": (_i, [_vp, ctypes.POINTER(JobDescC), ctypes.POINTER(_i64)]),
+    "apirl_batch_step": (_i, [_vp, ctypes.POINTER(_i), ctypes.POINTER(_i)]),
+    "apirl_batch_result": (_i, [_vp, _i64, _vp, _vp, ctypes.POINTER(_i)]),
     "apirl_mlem_2d": (_i, [ctypes.POINTER(ImageGeomC), ctypes.POINTER(Sino2DGeomC), _vp, _vp, _vp, _vp, _i, _i,
                            _vp, _vp, _vp]),
 }

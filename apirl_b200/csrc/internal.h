@@ -77,6 +77,50 @@ cudaError_t launch_update(int64_t n, float* x, float* bp, const float* sens, con
 cudaError_t launch_force_positive(int64_t n, float* x, cudaStream_t st);
 cudaError_t launch_fill(int64_t n, float* x, float v, cudaStream_t st);
 
+// ---- batched passes over many independent jobs --------------------------------
+// Each job's bins (voxels) occupy a range of whole 256-thread blocks of one
+// launch, so a block never straddles two jobs.
+struct EmJob {
+  ImgGeom g;
+  LorTable t;
+  SubsetSel s;
+  const void* counts;    // whole sinogram, [sinogram][angle][r]
+  const float* add;      // same layout or null
+  const float* x;
+  float* bp;
+  double* lik;           // output slot of this pass's likelihood
+  int64_t blk_begin;     // first block of this job in the launch
+  int64_t nbins;
+  int counts_dtype;
+  int back;
+  int lik_mode;
+};
+struct UpdJob {
+  float* x;
+  float* bp;
+  const float* sens;
+  int64_t blk_begin;     // first block (each block covers 1024 voxels)
+  int64_t nvox;
+  float thr;
+  int ge;
+};
+struct SensJob {
+  ImgGeom g;
+  LorTable t;            // whole sinogram; subset of angle a is a % nsub
+  const float* mult;     // null: ones
+  float* sens;           // nsub images of nvox
+  int64_t blk_begin;
+  int64_t nbins;
+  int64_t nvox;
+  int nsub;
+};
+constexpr int kBatchBinsPerBlock = 256;
+constexpr int kBatchVoxPerBlock = 1024;
+cudaError_t launch_em_batch(const EmJob* d_jobs, const EmJob* h_jobs, int njobs, int64_t nblocks, double* partials,
+                            cudaStream_t st);
+cudaError_t launch_update_batch(const UpdJob* d_jobs, int njobs, int64_t nblocks, cudaStream_t st);
+cudaError_t launch_sens_batch(const SensJob* d_jobs, int njobs, int64_t nblocks, cudaStream_t st);
+
 }  // namespace apirl
 
 typedef int apirl_status;

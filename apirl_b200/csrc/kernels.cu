@@ -383,6 +383,105 @@ __global__ void k_fill(int64_t n, float* __restrict__ x, float v) {
     x[i] = v;
 }
 
+
+// ---------------------------------------------------------------------------
+// Batched passes: many independent jobs in one launch.
+__device__ __forceinline__ float load_count_any(const void* p, int dtype, int64_t i) {
+  if (dtype == APIRL_U32) return (float)__ldg((const uint32_t*)p + i);
+  if (dtype == APIRL_U16) return (float)__ldg((const uint16_t*)p + i);
+  return __ldg((const float*)p + i);
+}
+
+template <typename J>
+__device__ __forceinline__ int find_job(const J* __restrict__ jobs, int njobs, int64_t blk) {
+  int lo = 0, hi = njobs - 1;
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (jobs[mid].blk_begin <= blk) lo = mid; else hi = mid - 1;
+  }
+  return lo;
+}
+
+__global__ void __launch_bounds__(kBlock) k_em_batch(const EmJob* __restrict__ jobs, int njobs,
+                                                     double* __restrict__ partials) {
+  __shared__ int sj;
+  if (threadIdx.x == 0) sj = find_job(jobs, njobs, blockIdx.x);
+  __syncthreads();
+  const EmJob& J = jobs[sj];
+  const int64_t b = ((int64_t)blockIdx.x - J.blk_begin) * kBlock + threadIdx.x;
+  double term = 0.0;
+  if (b < J.nbins) {
+    const BinPos p = decode(b, J.t, J.s);
+    const int64_t ci = ((int64_t)p.g * J.t.n_proj + p.a) * J.t.n_r + p.l;
+    const float m = load_count_any(J.counts, J.counts_dtype, ci);
+    Walk3 w;
+    float e = ray_sum3(J.g, J.t.lor[(int64_t)p.a * J.t.n_r + p.l], J.t.z[p.g], J.x, w);
+    if (J.add) e = A_ADD(e, __ldg(J.add + ci));
+    const float r = (m != 0.f && e != 0.f) ? A_DIV(m, e) : 0.f;
+    if (J.lik_mode == 1 ? (e > 0.f) : (e != 0.f)) term = (double)m * log((double)e) - (double)e;
+    if (J.back && r != 0.f) {
+      float* bp = J.bp;
+      siddon3_walk(w, J.g, [&](bool inb, int idx, float seg) {
+        if (inb) atomicAdd(bp + idx, A_MUL(seg, r));
+      });
+    }
+  }
+  const double bs = block_sum(term);
+  if (threadIdx.x == 0) partials[blockIdx.x] = bs;
+}
+
+// One block per job: deterministic sum of the job's block partials.
+__global__ void k_sum_batch(const EmJob* __restrict__ jobs, const double* __restrict__ partials) {
+  const EmJob& J = jobs[blockIdx.x];
+  const int64_t nb = (J.nbins + kBlock - 1) / kBlock;
+  double v = 0.0;
+  for (int64_t i = threadIdx.x; i < nb; i += blockDim.x) v += partials[J.blk_begin + i];
+  const double s = block_sum(v);
+  if (threadIdx.x == 0 && J.lik) *J.lik = s;
+}
+
+__global__ void __launch_bounds__(kBlock) k_update_batch(const UpdJob* __restrict__ jobs, int njobs) {
+  __shared__ int sj;
+  if (threadIdx.x == 0) sj = find_job(jobs, njobs, blockIdx.x);
+  __syncthreads();
+  const UpdJob& J = jobs[sj];
+  const int64_t base = ((int64_t)blockIdx.x - J.blk_begin) * kBatchVoxPerBlock;
+  #pragma unroll
+  for (int c = 0; c < kBatchVoxPerBlock / kBlock; c++) {
+    const int64_t i = base + c * kBlock + threadIdx.x;
+    if (i < J.nvox) {
+      const float sv = J.sens[i];
+      const bool okv = J.ge ? (sv >= J.thr) : (sv > J.thr);
+      J.x[i] = okv ? A_DIV(A_MUL(J.x[i], J.bp[i]), sv) : 0.f;
+      J.bp[i] = 0.f;
+    }
+  }
+}
+
+// Sensitivity of every subset of a job in one pass over its whole sinogram:
+// bin (g, a, l) belongs to subset a % nsub.  forcePositive is a separate pass.
+__global__ void __launch_bounds__(kBlock) k_sens_batch(const SensJob* __restrict__ jobs, int njobs) {
+  __shared__ int sj;
+  if (threadIdx.x == 0) sj = find_job(jobs, njobs, blockIdx.x);
+  __syncthreads();
+  const SensJob& J = jobs[sj];
+  const int64_t b = ((int64_t)blockIdx.x - J.blk_begin) * kBlock + threadIdx.x;
+  if (b >= J.nbins) return;
+  SubsetSel all;
+  all.subset = -1; all.nsub = 1; all.nk = J.t.n_proj;
+  const BinPos p = decode(b, J.t, all);
+  const float v = J.mult ? __ldg(J.mult + b) : 1.f;
+  if (v == 0.f) return;
+  float* sens = J.sens + (int64_t)(p.a % J.nsub) * J.nvox;
+  const float4 L = J.t.lor[(int64_t)p.a * J.t.n_r + p.l];
+  const float2 z = J.t.z[p.g];
+  Walk3 w;
+  siddon3_setup(L.x, L.y, z.x, A_SUB(L.z, L.x), A_SUB(L.w, L.y), A_SUB(z.y, z.x), J.g, w);
+  siddon3_walk(w, J.g, [&](bool inb, int idx, float seg) {
+    if (inb) atomicAdd(sens + idx, A_MUL(seg, v));
+  });
+}
+
 inline unsigned grid_for(int64_t total) { return (unsigned)((total + kBlock - 1) / kBlock); }
 inline unsigned stream_grid(int64_t n) {
   int64_t g = (n + kBlock - 1) / kBlock;
@@ -504,6 +603,29 @@ cudaError_t launch_force_positive(int64_t n, float* x, cudaStream_t st) {
 cudaError_t launch_fill(int64_t n, float* x, float v, cudaStream_t st) {
   if (n == 0) return cudaSuccess;
   k_fill<<<stream_grid(n), kBlock, 0, st>>>(n, x, v);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_em_batch(const EmJob* d_jobs, const EmJob* h_jobs, int njobs, int64_t nblocks, double* partials,
+                            cudaStream_t st) {
+  (void)h_jobs;
+  if (njobs == 0 || nblocks == 0) return cudaSuccess;
+  k_em_batch<<<(unsigned)nblocks, kBlock, 0, st>>>(d_jobs, njobs, partials);
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return e;
+  k_sum_batch<<<njobs, kBlock, 0, st>>>(d_jobs, partials);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_update_batch(const UpdJob* d_jobs, int njobs, int64_t nblocks, cudaStream_t st) {
+  if (njobs == 0 || nblocks == 0) return cudaSuccess;
+  k_update_batch<<<(unsigned)nblocks, kBlock, 0, st>>>(d_jobs, njobs);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_sens_batch(const SensJob* d_jobs, int njobs, int64_t nblocks, cudaStream_t st) {
+  if (njobs == 0 || nblocks == 0) return cudaSuccess;
+  k_sens_batch<<<(unsigned)nblocks, kBlock, 0, st>>>(d_jobs, njobs);
   return cudaGetLastError();
 }
 

@@ -104,3 +104,48 @@ def poisson_counts(expected, total, seed=0):
     lam = expected.astype(np.float64) * (total / float(expected.sum()))
     rng = np.random.default_rng(seed)
     return rng.poisson(lam).astype(np.uint32)
+
+
+# ---------------------------------------------------------------------------
+# Batched / served jobs: images drawn from {64^2, 128^2, 256^2} x {1, 41, 81}
+# slices, radial bins = angles = round(1.3 N) at the voxel pitch, span 1 with
+# max ring difference floor(Z/4), (Z+1)/2 rings of pitch 2 dz, random disc +
+# sphere phantoms, total counts log-uniform in [1e5, 1e8], 2-4 iterations of
+# 7-21 subsets.
+def job_geometry(n, z, dxy=2.08, dz=2.03, r_scanner=443.0):
+    ig = ImageGeom(n, n, z, dxy, dxy, dz)
+    nr = int(round(1.3 * n))
+    rings = (z + 1) // 2
+    sg = Sino3DGeom.span1(nr, nr, rings, nr * dxy / 2.0, rings * 2 * dz, r_scanner, z // 4)
+    return ig, sg
+
+
+def random_phantom(ig, rng):
+    x, y, z = voxel_centres(ig)
+    Y, X = np.meshgrid(y, x, indexing="ij")
+    w = ig.nx * ig.dx
+    rad = w * rng.uniform(0.3, 0.45)
+    img = np.repeat(((X ** 2 + Y ** 2) < rad ** 2)[None], ig.nz, axis=0).astype(np.float32)
+    Z = z[:, None, None]
+    for _ in range(int(rng.integers(1, 4))):
+        r = 0.8 * rad * math.sqrt(rng.random())
+        th = 2 * math.pi * rng.random()
+        cz = z[0] + (z[-1] - z[0]) * rng.random()
+        sr = rng.uniform(5.0, 10.0)
+        m = (X[None] - r * math.cos(th)) ** 2 + (Y[None] - r * math.sin(th)) ** 2 + (Z - cz) ** 2 < sr ** 2
+        img[m] = 4.0
+    return img.reshape(-1)
+
+
+def mixed_job_specs(n_jobs, seed=4, sizes=(64, 128, 256), slices=(1, 41, 81), iters=(2, 4), subsets=(7, 21),
+                    counts=(1e5, 1e8)):
+    """Seeded list of dicts: n, z, iters, nsubsets, total counts, phantom seed."""
+    rng = np.random.default_rng(seed)
+    specs = []
+    for i in range(n_jobs):
+        specs.append(dict(n=int(rng.choice(sizes)), z=int(rng.choice(slices)),
+                          iters=int(rng.integers(iters[0], iters[1] + 1)),
+                          nsubsets=int(rng.integers(subsets[0], subsets[1] + 1)),
+                          counts=float(10 ** rng.uniform(math.log10(counts[0]), math.log10(counts[1]))),
+                          seed=int(rng.integers(1 << 30))))
+    return specs

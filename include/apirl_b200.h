@@ -209,6 +209,41 @@ apirl_status apirl_mlem_2d(const apirl_image_geom* img, const apirl_sino2d_geom*
                            const float* h_mult, const float* h_add, const float* h_init, int iters, int device,
                            float* h_out, double* h_lik, float* h_sens);
 
+/* ---- batched and served reconstructions ---------------------------------
+ * Many independent 3D OSEM jobs (OsemSinogram3d::Reconstruct each,
+ * recon/src/OsemSinogram3d.cpp:36-325) of different geometries advance
+ * together: every apirl_batch_step runs one pass of every active job in one
+ * launch of the fused kernel and one of the pixel update.  Jobs are admitted
+ * in submission order while their device footprint fits the budget, with
+ * smaller jobs allowed past one that does not fit; finished jobs release their
+ * memory at once.  No counterpart in the reference, which reconstructs one
+ * sinogram per process. */
+typedef struct apirl_batch apirl_batch;
+typedef struct apirl_job_desc {
+  apirl_image_geom img;
+  apirl_sino3d_geom sino;  /* ring-difference arrays are copied by submit */
+  const void* h_counts;    /* whole sinogram, element type counts_dtype */
+  int counts_dtype;
+  const float* h_mult;     /* multiplicative sinogram (sensitivity only) or NULL */
+  const float* h_add;      /* additive sinogram or NULL */
+  const float* h_init;     /* initial image or NULL (ones) */
+  int iters, nsubsets;
+} apirl_job_desc;
+/* Device bytes a job holds while active. */
+int64_t apirl_job_footprint(const apirl_job_desc* job);
+apirl_status apirl_batch_create(int device, int64_t hbm_budget_bytes, apirl_batch** out);
+void apirl_batch_destroy(apirl_batch* b);
+/* Copies the job's host data and queues it; job ids start at 0. */
+apirl_status apirl_batch_submit(apirl_batch* b, const apirl_job_desc* job, int64_t* job_id);
+/* Admits what fits, computes the sensitivity images of newly admitted jobs,
+ * runs one pass of every active job, retires finished jobs; returns when the
+ * step is done on the device.  Counts after the step go to *n_active,
+ * *n_queued (either may be NULL). */
+apirl_status apirl_batch_step(apirl_batch* b, int* n_active, int* n_queued);
+/* *done = 1 and the outputs are filled (image, iters*nsubsets+1 likelihood
+ * values) once the job has finished; the job is forgotten afterwards. */
+apirl_status apirl_batch_result(apirl_batch* b, int64_t job_id, float* h_out, double* h_lik, int* done);
+
 #ifdef __cplusplus
 }
 #endif
