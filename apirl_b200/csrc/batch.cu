@@ -41,9 +41,9 @@ struct Job {
   apirl_image_geom img;
   apirl_sino3d_geom sino;
   std::vector<int> mn, mx;
-  std::vector<uint8_t> counts;
+  const void* h_counts = nullptr;  // caller's arrays, read at admission
+  const float *h_mult = nullptr, *h_add = nullptr, *h_init = nullptr;
   int dtype;
-  std::vector<float> mult, add, init;
   int iters, nsub;
   int64_t nbins = 0, nvox = 0, footprint = 0;
   Stage stage = Stage::Queued;
@@ -103,30 +103,25 @@ apirl_status admit(apirl_batch* b, Job& j) {
   if (s != APIRL_OK) return s;
   const size_t cb = (size_t)j.nbins * count_elem_size(j.dtype);
   BK(cudaMalloc(&j.d_counts, cb));
-  BK(cudaMemcpyAsync(j.d_counts, j.counts.data(), cb, cudaMemcpyHostToDevice, b->st));
-  if (!j.mult.empty()) {
+  BK(cudaMemcpyAsync(j.d_counts, j.h_counts, cb, cudaMemcpyHostToDevice, b->st));
+  if (j.h_mult) {
     BK(cudaMalloc(&j.d_mult, j.nbins * sizeof(float)));
-    BK(cudaMemcpyAsync(j.d_mult, j.mult.data(), j.nbins * sizeof(float), cudaMemcpyHostToDevice, b->st));
+    BK(cudaMemcpyAsync(j.d_mult, j.h_mult, j.nbins * sizeof(float), cudaMemcpyHostToDevice, b->st));
   }
-  if (!j.add.empty()) {
+  if (j.h_add) {
     BK(cudaMalloc(&j.d_add, j.nbins * sizeof(float)));
-    BK(cudaMemcpyAsync(j.d_add, j.add.data(), j.nbins * sizeof(float), cudaMemcpyHostToDevice, b->st));
+    BK(cudaMemcpyAsync(j.d_add, j.h_add, j.nbins * sizeof(float), cudaMemcpyHostToDevice, b->st));
   }
   BK(cudaMalloc(&j.d_x, j.nvox * sizeof(float)));
   BK(cudaMalloc(&j.d_bp, j.nvox * sizeof(float)));
   BK(cudaMalloc(&j.d_sens, j.nvox * j.nsub * sizeof(float)));
   BK(cudaMalloc(&j.d_lik, ((size_t)j.iters * j.nsub + 1) * sizeof(double)));
-  if (!j.init.empty())
-    BK(cudaMemcpyAsync(j.d_x, j.init.data(), j.nvox * sizeof(float), cudaMemcpyHostToDevice, b->st));
+  if (j.h_init)
+    BK(cudaMemcpyAsync(j.d_x, j.h_init, j.nvox * sizeof(float), cudaMemcpyHostToDevice, b->st));
   else
     BK(apirl::launch_fill(j.nvox, j.d_x, 1.f, b->st));
   BK(cudaMemsetAsync(j.d_bp, 0, j.nvox * sizeof(float), b->st));
   BK(cudaMemsetAsync(j.d_sens, 0, j.nvox * j.nsub * sizeof(float), b->st));
-  // Host copies are no longer needed.
-  std::vector<uint8_t>().swap(j.counts);
-  std::vector<float>().swap(j.mult);
-  std::vector<float>().swap(j.add);
-  std::vector<float>().swap(j.init);
   j.stage = Stage::Sens;
   b->used += j.footprint;
   return APIRL_OK;
@@ -213,11 +208,10 @@ apirl_status apirl_batch_submit(apirl_batch* b, const apirl_job_desc* d, int64_t
   j->nbins = (int64_t)nsinos * d->sino.n_proj * d->sino.n_r;
   j->nvox = (int64_t)d->img.nx * d->img.ny * d->img.nz;
   j->dtype = d->counts_dtype;
-  const uint8_t* c = (const uint8_t*)d->h_counts;
-  j->counts.assign(c, c + j->nbins * count_elem_size(d->counts_dtype));
-  if (d->h_mult) j->mult.assign(d->h_mult, d->h_mult + j->nbins);
-  if (d->h_add) j->add.assign(d->h_add, d->h_add + j->nbins);
-  if (d->h_init) j->init.assign(d->h_init, d->h_init + j->nvox);
+  j->h_counts = d->h_counts;
+  j->h_mult = d->h_mult;
+  j->h_add = d->h_add;
+  j->h_init = d->h_init;
   j->iters = d->iters;
   j->nsub = d->nsubsets;
   j->footprint = footprint_of(d->img, d->sino, d->counts_dtype, d->h_mult, d->h_add, d->nsubsets, j->nbins);

@@ -100,13 +100,18 @@ class ClockSampler:
 
 
 # ---------------------------------------------------------------------------
-def setup_workload(dev, log):
-    """Builds the resident state of the 3D OSEM job on `dev` (outside timing)."""
+def setup_workload(dev, log, max_ring_diff=None):
+    """Builds the resident state of the 3D OSEM job on `dev` (outside timing).
+    max_ring_diff < 20 keeps only the segments |rd| <= max_ring_diff (a smaller
+    case of the same kernels, used for profiler captures)."""
     import torch
     import apirl_b200 as ap
     from apirl_b200 import workloads
+    from apirl_b200.geometry import Sino3DGeom
 
     ig, sg = workloads.c2_geometry()
+    if max_ring_diff is not None and max_ring_diff < 20:
+        sg = Sino3DGeom.span1(sg.n_proj, sg.n_r, sg.n_rings, sg.r_fov, sg.axial_fov, sg.r_scanner, max_ring_diff)
     P = ap.SiddonProjector(ig, sg, device=dev.index)
     nb = P.num_bins()
     lor, z = P.tables()
@@ -171,7 +176,7 @@ def run_gpu(args):
 
     import apirl_b200 as ap
     ap.load_library()
-    w = setup_workload(dev, log)
+    w = setup_workload(dev, log, args.max_ring_diff)
     P, counts, sens, x, bp = w["P"], w["counts"], w["sens"], w["x"], w["bp"]
     stream = torch.cuda.Stream(device=dev)
     flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.float32, device=dev)
@@ -264,7 +269,9 @@ def run_gpu(args):
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded phantom, Poisson counts)",
-            "config": {"workload": WORKLOAD, "subsets": NSUB, "counts_dtype": "uint32",
+            "config": {"workload": WORKLOAD if args.max_ring_diff is None else
+                       WORKLOAD + f" (profiling case: segments |rd| <= {args.max_ring_diff} only)",
+                       "subsets": NSUB, "counts_dtype": "uint32",
                        "l2": "flushed between timed steps (256 MB write outside the timed events)",
                        "parallelism": f"replicas x{world}"},
             "siddon_gsteps_per_s": gsteps,
@@ -403,6 +410,88 @@ def run_reference(args):
     print(json.dumps(line), flush=True)
 
 
+# ---------------------------------------------------------------------------
+# Batched and served forms (not the headline): many OSEM jobs of mixed size.
+def _make_jobs(specs, dev, log, c2_every=0):
+    import torch
+    import apirl_b200 as ap
+    from apirl_b200 import workloads
+    from apirl_b200.batch import Job
+    jobs = []
+    for i, s in enumerate(specs):
+        if c2_every and i % c2_every == c2_every - 1:
+            ig, sg = workloads.c2_geometry()
+            x = workloads.cylinder_phantom_3d(ig, seed=2)
+        else:
+            ig, sg = workloads.job_geometry(s["n"], s["z"])
+            x = workloads.random_phantom(ig, np.random.default_rng(s["seed"]))
+        P = ap.SiddonProjector(ig, sg, device=dev.index)
+        est = torch.empty(P.num_bins(), dtype=torch.float32, device=dev)
+        P.project(torch.from_numpy(x).to(dev), est)
+        est.mul_(s["counts"] / float(est.double().sum().item()))
+        g = torch.Generator(device=dev).manual_seed(s["seed"])
+        counts = torch.poisson(est, generator=g).to(torch.int32).cpu().numpy().view(np.uint32)
+        P.close()
+        jobs.append(Job(ig, sg, counts, s["iters"], s["nsubsets"], tag=dict(s, geometry=(ig.nx, ig.nz, sg.n_sinos))))
+    torch.cuda.synchronize(dev)
+    log(f"made {len(jobs)} jobs, {sum(j.counts.size for j in jobs) / 1e6:.0f} M bins")
+    return jobs
+
+
+def _plain(jobs, dev):
+    import apirl_b200 as ap
+    t0 = time.perf_counter()
+    outs = []
+    for j in jobs:
+        img, lik, _ = ap.osem_3d(j.image_geom, j.sino_geom, j.counts.astype(np.float32),
+                                 np.ones(j.image_geom.n_voxels, np.float32), j.iters, j.nsubsets, device=dev.index)
+        outs.append(img)
+    return outs, time.perf_counter() - t0
+
+
+def run_batched(args, served=False):
+    import torch
+    from apirl_b200 import workloads
+    from apirl_b200.batch import Batch, serve
+    dev = torch.device("cuda:0")
+    log = lambda m: print(f"[bench] {m}", file=sys.stderr, flush=True)
+    n = args.jobs
+    specs = workloads.mixed_job_specs(n, seed=5 if served else 4)
+    jobs = _make_jobs(specs, dev, log, c2_every=10 if served else 0)
+    budget = int(args.budget_gb * (1 << 30))
+    # plain form: one job at a time through the single-job driver
+    ref, t_plain = _plain(jobs, dev)
+    if served:
+        arrivals = np.cumsum(np.random.default_rng(5).exponential(1.0 / args.rate, len(jobs)))
+        res, lat, makespan = serve(jobs, arrivals, budget_bytes=budget)
+        t_new = makespan - float(arrivals[0])
+    else:
+        b = Batch(0, budget_bytes=budget)
+        t0 = time.perf_counter()
+        res = b.run_all(jobs)
+        t_new = time.perf_counter() - t0
+        b.close()
+        lat = None
+    errs = [float(np.linalg.norm(r[0].astype(np.float64) - p) / np.linalg.norm(p.astype(np.float64)))
+            for r, p in zip(res, ref)]
+    line = {
+        "metric": "served OSEM reconstructions/hour" if served else "batched OSEM reconstructions/hour",
+        "value": len(jobs) / t_new * 3600, "unit": "recon/h", "n_gpus": 1, "higher_is_better": True,
+        "plain_value": len(jobs) / t_plain * 3600, "speedup_vs_plain": t_plain / t_new,
+        "max_rel_l2_vs_plain": max(errs), "dtype": "f32", "data": "synthetic (seeded phantoms, Poisson counts)",
+        "config": {"workload": ("Poisson arrivals at %.0f jobs/s of " % args.rate if served else "") +
+                   f"{len(jobs)} mixed OSEM jobs: images {{64,128,256}}^2 x {{1,41,81}} slices, 1.3N r/angles, "
+                   "span 1, 2-4 iterations x 7-21 subsets, 1e5-1e8 counts uint32" +
+                   ("; every 10th job the full 256x256x81 / 1261x336x336 geometry" if served else ""),
+                   "budget_gb": args.budget_gb},
+    }
+    if served:
+        line["p50_latency_s"] = float(np.percentile(lat, 50))
+        line["p99_latency_s"] = float(np.percentile(lat, 99))
+        line["makespan_s"] = float(t_new)
+    print(json.dumps(line), flush=True)
+
+
 def main():
     ap_ = argparse.ArgumentParser(description=__doc__.split("\n")[0])
     ap_.add_argument("--gpus", type=int, default=1)
@@ -411,6 +500,12 @@ def main():
     ap_.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap_.add_argument("--no-cpu-baseline", action="store_true")
     ap_.add_argument("--cpu-seconds", type=float, default=15.0)
+    ap_.add_argument("--workload", default="osem3d", choices=["osem3d", "batched", "served"])
+    ap_.add_argument("--max-ring-diff", type=int, default=None,
+                     help="profiling: keep segments |rd| <= this (smaller case of the same kernels)")
+    ap_.add_argument("--jobs", type=int, default=64)
+    ap_.add_argument("--rate", type=float, default=20.0, help="served: mean arrivals per second")
+    ap_.add_argument("--budget-gb", type=float, default=96.0)
     ap_.add_argument("--traffic-bytes", type=float, default=None,
                      help="DRAM bytes per fused-kernel launch from an ncu capture, reported as roofline.traffic")
     args = ap_.parse_args()
@@ -418,6 +513,8 @@ def main():
         args.warmup = 3
     if args.impl == "reference":
         run_reference(args)
+    elif args.workload in ("batched", "served"):
+        run_batched(args, served=args.workload == "served")
     else:
         run_gpu(args)
 

@@ -233,7 +233,9 @@ typedef struct apirl_job_desc {
 int64_t apirl_job_footprint(const apirl_job_desc* job);
 apirl_status apirl_batch_create(int device, int64_t hbm_budget_bytes, apirl_batch** out);
 void apirl_batch_destroy(apirl_batch* b);
-/* Copies the job's host data and queues it; job ids start at 0. */
+/* Queues a job; job ids start at 0.  The host arrays are read when the job
+ * is admitted (copied to the device), so they must stay valid until then
+ * (at the latest until apirl_batch_result reports it done). */
 apirl_status apirl_batch_submit(apirl_batch* b, const apirl_job_desc* job, int64_t* job_id);
 /* Admits what fits, computes the sensitivity images of newly admitted jobs,
  * runs one pass of every active job, retires finished jobs; returns when the

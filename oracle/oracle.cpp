@@ -555,6 +555,34 @@ int or_siddon3d_f32(float p1x, float p1y, float p1z, float p2x, float p2y, float
   return n;
 }
 
+int or_siddon3d_f64(double p1x, double p1y, double p1z, double p2x, double p2y, double p2z, int nx, int ny, int nz,
+                    float dx, float dy, float dz, int* ijk, double* w, int cap) {
+  ImgG<double> g = make_img<double>(nx, ny, nz, dx, dy, dz);
+  int c = 0;
+  int n = siddon3d<double>(p1x, p1y, p1z, p2x - p1x, p2y - p1y, p2z - p1z, g, [&](int i, int j, int k, double ww) {
+    if (c < cap) { ijk[3 * c] = i; ijk[3 * c + 1] = j; ijk[3 * c + 2] = k; w[c] = ww; }
+    c++;
+  });
+  return n;
+}
+
+int or_lor_points_2d_f64(int nProj, int nR, float rFov, float rScanner, double* out4) {
+  Sino2DG<double> s = make_sino2d<double>(nProj, nR, rFov, rScanner);
+  for (int a = 0; a < nProj; a++)
+    for (int l = 0; l < nR; l++) {
+      Lor<double> L = lor_points<double>(s.r[l], s.ang[a], s.rScanner);
+      double* o = out4 + ((long)a * nR + l) * 4;
+      o[0] = L.p1x; o[1] = L.p1y; o[2] = L.p2x; o[3] = L.p2y;
+    }
+  return 0;
+}
+
+int or_sino3d_z_f64(const or_sino3d* d, double* z1, double* z2) {
+  Sino3DG<double> s = mk<double>(d);
+  for (int g = 0; g < s.nSinos; g++) sino_z(s, g, z1[g], z2[g]);
+  return s.nSinos;
+}
+
 #define OR_FWD3(SUF, T)                                                                                      \
   int or_project_3d_##SUF(const or_sino3d* d, int subset, int nsub, int nx, int ny, int nz, float dx,       \
                           float dy, float dz, const T* img, T* out, int threads) {                          \
