@@ -17,6 +17,9 @@ APIRL_ERR_OOM = 3
 APIRL_ERR_NOT_SUPPORTED = 4
 APIRL_ERR_ABORTED = 5
 
+APIRL_OPT_DUAL_LAYOUT = 1
+APIRL_OPT_KERNEL_TIMING = 2
+
 APIRL_ALPHA_F32 = 0
 APIRL_ALPHA_F64 = 1
 
@@ -65,10 +68,13 @@ SIGNATURES = {
     "apirl_projector_num_sinograms": (_i, [_vp]),
     "apirl_projector_tables": (_i, [_vp, _vp, _vp]),
     "apirl_projector_set_alpha_precision": (_i, [_vp, _i]),
+    "apirl_projector_set_option": (_i, [_vp, _i, _i]),
+    "apirl_projector_kernel_ms": (_i, [_vp, ctypes.POINTER(ctypes.c_double)]),
     "apirl_count_steps": (_i, [_vp, _i, _i, _vp, _vp]),
     "apirl_project": (_i, [_vp, _vp, _vp, _i, _i, _vp]),
     "apirl_backproject": (_i, [_vp, _vp, _vp, _i, _i, _vp]),
     "apirl_divide_and_backproject": (_i, [_vp, _vp, _vp, _vp, _i, _i, _vp]),
+    "apirl_generate_acf": (_i, [_vp, _vp, _vp, _i, _i, _vp]),
     "apirl_inverse_divide": (_i, [_i64, _vp, _vp, _vp]),
     "apirl_add_bins": (_i, [_i64, _vp, _vp, _vp]),
     "apirl_likelihood": (_i, [_i64, _vp, _vp, _i, _vp, _vp]),

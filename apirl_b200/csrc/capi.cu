@@ -224,6 +224,10 @@ void apirl_projector_destroy(apirl_projector* p) {
   cudaFree(p->d_scalars);
   cudaFree(p->d_lor64);
   cudaFree(p->d_z64);
+  cudaFree(p->d_xT);
+  cudaFree(p->d_bpT);
+  if (p->ev0) cudaEventDestroy(p->ev0);
+  if (p->ev1) cudaEventDestroy(p->ev1);
   delete p;
 }
 
@@ -310,6 +314,20 @@ apirl_status apirl_divide_and_backproject(apirl_projector* p, const float* d_mea
   return APIRL_OK;
 }
 
+apirl_status apirl_generate_acf(apirl_projector* p, const float* d_mu, float* d_acf, int subset, int nsubsets,
+                                void* stream) {
+  apirl_status st = check_subset(p, subset, nsubsets);
+  if (st) return st;
+  if (!d_mu || !d_acf) return fail(APIRL_ERR_INVALID, "null image or sinogram");
+  DEVICE_SCOPE(p->device);
+  SubsetSel ss = make_subset(p, subset, nsubsets);
+  const int64_t nb = (int64_t)p->t.n_sinos * ss.nk * p->t.n_r;
+  if (!p->is3d) CK(cudaMemsetAsync(d_acf, 0, nb * sizeof(float), (cudaStream_t)stream));
+  CK(apirl::launch_project(p->g, p->t, ss, d_mu, d_acf, (cudaStream_t)stream, p->pg));
+  CK(apirl::launch_exp_nonzero(nb, d_acf, (cudaStream_t)stream));
+  return APIRL_OK;
+}
+
 apirl_status apirl_inverse_divide(int64_t n, const float* d_meas, float* d_est, void* stream) {
   if (n < 0 || (n > 0 && (!d_meas || !d_est))) return fail(APIRL_ERR_INVALID, "bad arguments");
   CK(apirl::launch_inverse_divide(n, d_meas, d_est, (cudaStream_t)stream));
@@ -358,20 +376,71 @@ apirl_status apirl_force_positive(int64_t n, float* d_x, void* stream) {
   return APIRL_OK;
 }
 
+namespace {
+
+bool use_dual(const apirl_projector* p) { return p->is3d && p->dual_layout && !p->pg.enabled; }
+
+apirl_status ensure_dual(apirl_projector* p, cudaStream_t s) {
+  if (p->d_xT) return APIRL_OK;
+  const int64_t nv = (int64_t)p->g.nx * p->g.ny * p->g.nz;
+  CK(cudaMalloc(&p->d_xT, nv * sizeof(float)));
+  CK(cudaMalloc(&p->d_bpT, nv * sizeof(float)));
+  CK(cudaMemsetAsync(p->d_bpT, 0, nv * sizeof(float), s));
+  return APIRL_OK;
+}
+
+// The fused kernel, bracketed by timing events when enabled.
+apirl_status fused(apirl_projector* p, SubsetSel ss, const void* d_counts, int dtype, int packed, const float* d_add,
+                   const float* d_x, float* d_bp, bool dual, double* d_lik, cudaStream_t s) {
+  if (p->timing) {
+    if (!p->ev0) {
+      CK(cudaEventCreate(&p->ev0));
+      CK(cudaEventCreate(&p->ev1));
+    }
+    CK(cudaEventRecord(p->ev0, s));
+  }
+  CK(apirl::launch_em_pass(p->g, p->t, ss, d_counts, dtype, packed, d_add, d_x, d_bp, 1, p->is3d ? 0 : 1,
+                           p->d_partials, d_lik, s, p->pg, dual ? p->d_xT : nullptr, dual ? p->d_bpT : nullptr));
+  if (p->timing) {
+    CK(cudaEventRecord(p->ev1, s));
+    p->timed = 1;
+  }
+  return APIRL_OK;
+}
+
+apirl_status check_em(apirl_projector* p, const void* d_counts, int dtype, const float* d_x, const float* d_bp,
+                      int subset, int nsubsets) {
+  apirl_status st = check_subset(p, subset, nsubsets);
+  if (st) return st;
+  if (!d_counts || !d_x || !d_bp) return fail(APIRL_ERR_INVALID, "null buffer");
+  if (dtype != APIRL_F32 && dtype != APIRL_U32 && dtype != APIRL_U16)
+    return fail(APIRL_ERR_INVALID, "unknown counts dtype %d", dtype);
+  return APIRL_OK;
+}
+
+}  // namespace
+
 apirl_status apirl_em_pass(apirl_projector* p, const void* d_counts, int counts_dtype, int counts_packed,
                            const float* d_add, float* d_x, float* d_bp, const float* d_sens, const float* d_thr,
                            float thr_value, int ge, int subset, int nsubsets, double* d_lik, void* stream) {
-  apirl_status st = check_subset(p, subset, nsubsets);
+  apirl_status st = check_em(p, d_counts, counts_dtype, d_x, d_bp, subset, nsubsets);
   if (st) return st;
-  if (!d_counts || !d_x || !d_bp || !d_sens) return fail(APIRL_ERR_INVALID, "null buffer");
-  if (counts_dtype != APIRL_F32 && counts_dtype != APIRL_U32 && counts_dtype != APIRL_U16)
-    return fail(APIRL_ERR_INVALID, "unknown counts dtype %d", counts_dtype);
+  if (!d_sens) return fail(APIRL_ERR_INVALID, "null sensitivity");
   DEVICE_SCOPE(p->device);
   cudaStream_t s = (cudaStream_t)stream;
   SubsetSel ss = make_subset(p, subset, nsubsets);
-  CK(apirl::launch_em_pass(p->g, p->t, ss, d_counts, counts_dtype, counts_packed, d_add, d_x, d_bp, 1,
-                           p->is3d ? 0 : 1, p->d_partials, d_lik, s, p->pg));
   const int64_t nv = (int64_t)p->g.nx * p->g.ny * p->g.nz;
+  if (use_dual(p)) {
+    st = ensure_dual(p, s);
+    if (st) return st;
+    CK(apirl::launch_transpose_xy(p->g.nx, p->g.ny, p->g.nz, d_x, p->d_xT, s));
+    st = fused(p, ss, d_counts, counts_dtype, counts_packed, d_add, d_x, d_bp, true, d_lik, s);
+    if (st) return st;
+    CK(apirl::launch_update_dual(p->g.nx, p->g.ny, p->g.nz, d_x, d_bp, p->d_bpT, d_sens, d_thr, thr_value, ge, s));
+    return APIRL_OK;
+  }
+  st = fused(p, ss, d_counts, counts_dtype, counts_packed, d_add, d_x, d_bp, false, d_lik, s);
+  if (st) return st;
   CK(apirl::launch_update(nv, d_x, d_bp, d_sens, d_thr, thr_value, ge, 1, s));
   return APIRL_OK;
 }
@@ -379,15 +448,40 @@ apirl_status apirl_em_pass(apirl_projector* p, const void* d_counts, int counts_
 apirl_status apirl_em_project_backproject(apirl_projector* p, const void* d_counts, int counts_dtype,
                                           int counts_packed, const float* d_add, const float* d_x, float* d_bp,
                                           int subset, int nsubsets, double* d_lik, void* stream) {
-  apirl_status st = check_subset(p, subset, nsubsets);
+  apirl_status st = check_em(p, d_counts, counts_dtype, d_x, d_bp, subset, nsubsets);
   if (st) return st;
-  if (!d_counts || !d_x || !d_bp) return fail(APIRL_ERR_INVALID, "null buffer");
-  if (counts_dtype != APIRL_F32 && counts_dtype != APIRL_U32 && counts_dtype != APIRL_U16)
-    return fail(APIRL_ERR_INVALID, "unknown counts dtype %d", counts_dtype);
   DEVICE_SCOPE(p->device);
-  CK(apirl::launch_em_pass(p->g, p->t, make_subset(p, subset, nsubsets), d_counts, counts_dtype, counts_packed,
-                           d_add, d_x, d_bp, 1, p->is3d ? 0 : 1, p->d_partials, d_lik, (cudaStream_t)stream,
-                           p->pg));
+  cudaStream_t s = (cudaStream_t)stream;
+  SubsetSel ss = make_subset(p, subset, nsubsets);
+  if (use_dual(p)) {
+    st = ensure_dual(p, s);
+    if (st) return st;
+    CK(apirl::launch_transpose_xy(p->g.nx, p->g.ny, p->g.nz, d_x, p->d_xT, s));
+    st = fused(p, ss, d_counts, counts_dtype, counts_packed, d_add, d_x, d_bp, true, d_lik, s);
+    if (st) return st;
+    CK(apirl::launch_merge_transposed(p->g.nx, p->g.ny, p->g.nz, d_bp, p->d_bpT, s));
+    return APIRL_OK;
+  }
+  return fused(p, ss, d_counts, counts_dtype, counts_packed, d_add, d_x, d_bp, false, d_lik, s);
+}
+
+apirl_status apirl_projector_set_option(apirl_projector* p, int option, int value) {
+  if (!p) return fail(APIRL_ERR_INVALID, "null projector");
+  switch (option) {
+    case APIRL_OPT_DUAL_LAYOUT: p->dual_layout = value != 0; return APIRL_OK;
+    case APIRL_OPT_KERNEL_TIMING: p->timing = value != 0; p->timed = 0; return APIRL_OK;
+    default: return fail(APIRL_ERR_INVALID, "unknown option %d", option);
+  }
+}
+
+apirl_status apirl_projector_kernel_ms(apirl_projector* p, double* ms) {
+  if (!p || !ms) return fail(APIRL_ERR_INVALID, "bad arguments");
+  if (!p->timed) return fail(APIRL_ERR_INVALID, "no timed pass recorded (enable APIRL_OPT_KERNEL_TIMING)");
+  DEVICE_SCOPE(p->device);
+  CK(cudaEventSynchronize(p->ev1));
+  float f = 0.f;
+  CK(cudaEventElapsedTime(&f, p->ev0, p->ev1));
+  *ms = f;
   return APIRL_OK;
 }
 

@@ -64,7 +64,14 @@ int64_t em_pass_blocks(const LorTable& t, SubsetSel s);
 // lik_mode: 0 = over e != 0, 1 = over e > 0, 2 = over ratio > 0.  back = 0: no backprojection.
 cudaError_t launch_em_pass(const ImgGeom& g, const LorTable& t, SubsetSel s, const void* counts, int counts_dtype,
                            int counts_packed, const float* add, const float* x, float* bp, int back, int lik_mode,
-                           double* partials, double* lik, cudaStream_t st, const PreciseGeom& pg = PreciseGeom());
+                           double* partials, double* lik, cudaStream_t st, const PreciseGeom& pg = PreciseGeom(),
+                           const float* xT = nullptr, float* bpT = nullptr);
+// Transposed-layout helpers for the fused pass (3D): [z][y][x] -> [z][x][y], and
+// the update that merges the two backprojection buffers.
+cudaError_t launch_transpose_xy(int nx, int ny, int nz, const float* in, float* out, cudaStream_t st);
+cudaError_t launch_merge_transposed(int nx, int ny, int nz, float* bpA, float* bpT, cudaStream_t st);
+cudaError_t launch_update_dual(int nx, int ny, int nz, float* x, float* bpA, float* bpT, const float* sens,
+                               const float* thr_ptr, float thr_value, int ge, cudaStream_t st);
 
 cudaError_t launch_inverse_divide(int64_t n, const float* meas, float* est, cudaStream_t st);
 cudaError_t launch_add_bins(int64_t n, const float* add, float* est, cudaStream_t st);
@@ -76,6 +83,7 @@ cudaError_t launch_update(int64_t n, float* x, float* bp, const float* sens, con
                           int ge, int zero_bp, cudaStream_t st);
 cudaError_t launch_force_positive(int64_t n, float* x, cudaStream_t st);
 cudaError_t launch_fill(int64_t n, float* x, float v, cudaStream_t st);
+cudaError_t launch_exp_nonzero(int64_t n, float* v, cudaStream_t st);
 
 // ---- batched passes over many independent jobs --------------------------------
 // Each job's bins (voxels) occupy a range of whole 256-thread blocks of one
@@ -143,6 +151,12 @@ struct apirl_projector {
   double4* d_lor64 = nullptr;    // FP64-alpha tables, built on first use
   double2* d_z64 = nullptr;
   apirl::PreciseGeom pg;
+  int dual_layout = 1;           // fused 3D pass gathers / scatters x-running rays in a transposed copy
+  float* d_xT = nullptr;         // [z][x][y] copies for the dual layout, allocated on first use
+  float* d_bpT = nullptr;        // kept zero between passes
+  int timing = 0;                // record CUDA events around the fused kernel
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  int timed = 0;                 // an event pair has been recorded
   int n_rings = 0;               // 3D geometry as given, for building the FP64 tables
   float r_fov = 0, axial_fov = 0, r_scanner = 0;
   std::vector<int> min_rd, max_rd;

@@ -221,11 +221,16 @@ __global__ void __launch_bounds__(kBlock) k_count_steps(ImgGeom g, LorTable t, S
 // Fused EM pass: project, add, likelihood term, ratio, backproject.
 // lik_mode: 0 = term over e != 0 (3D), 1 = over e > 0 (2D), 2 = over the ratio
 // r > 0 (the final 2D value, Mlem2d.cpp:228).  back = 0 skips the backprojection.
+// xT / bpT (both or neither): the image and backprojection stored transposed,
+// [z][x][y].  Rays running mostly along x read and scatter there, so that the
+// 32 near-parallel rays of a warp, which lie side by side along y, touch
+// contiguous addresses; rays mostly along y use the [z][y][x] buffers.
 template <typename CT, bool IS3D, bool F64A>
 __global__ void __launch_bounds__(kBlock) k_em_pass(ImgGeom g, LorTable t, SubsetSel s, PreciseGeom pg,
                                                     const CT* __restrict__ counts,
                                                     int counts_packed, const float* __restrict__ add,
-                                                    const float* __restrict__ x, float* __restrict__ bp, int back,
+                                                    const float* __restrict__ x, float* __restrict__ bp,
+                                                    const float* __restrict__ xT, float* __restrict__ bpT, int back,
                                                     int lik_mode, double* __restrict__ partials, int64_t total) {
   const int64_t b = (int64_t)blockIdx.x * kBlock + threadIdx.x;
   double term = 0.0;
@@ -248,15 +253,25 @@ __global__ void __launch_bounds__(kBlock) k_em_pass(ImgGeom g, LorTable t, Subse
           if (inb) atomicAdd(bp + idx, A_MUL(seg, r));
         });
     } else if (IS3D) {
+      const float2 z = t.z[p.g];
+      const float vx = A_SUB(L.z, L.x), vy = A_SUB(L.w, L.y);
+      const bool tr = xT != nullptr && fabsf(vx) >= fabsf(vy);
+      const float* __restrict__ xs = tr ? xT : x;
+      float* __restrict__ bs = tr ? bpT : bp;
+      const int ux = tr ? g.ny : 1, uy = tr ? 1 : g.nx;
       Walk3 w;
-      float e = ray_sum3(g, L, t.z[p.g], x, w);
+      siddon3_setup(L.x, L.y, z.x, vx, vy, A_SUB(z.y, z.x), g, w);
+      float e = 0.f;
+      siddon3_walk_s(w, g, ux, uy, [&](bool inb, int idx, float seg) {
+        if (inb) e = A_ADD(e, A_MUL(seg, __ldg(xs + idx)));
+      });
       if (add) e = A_ADD(e, __ldg(add + ci));
       const float r = (m != 0.f && e != 0.f) ? A_DIV(m, e) : 0.f;
       if (lik_mode == 2) { if (r > 0.f) term = (double)m * log((double)r) - (double)r; }
       else if (lik_mode == 1 ? (e > 0.f) : (e != 0.f)) term = (double)m * log((double)e) - (double)e;
       if (back && r != 0.f)
-        siddon3_walk(w, g, [&](bool inb, int idx, float seg) {
-          if (inb) atomicAdd(bp + idx, A_MUL(seg, r));
+        siddon3_walk_s(w, g, ux, uy, [&](bool inb, int idx, float seg) {
+          if (inb) atomicAdd(bs + idx, A_MUL(seg, r));
         });
     } else {
       Walk2 w;
@@ -378,6 +393,14 @@ __global__ void k_force_positive(int64_t n, float* __restrict__ x) {
     if (x[i] < 0.f) x[i] = 0.f;
 }
 
+// generateACFs (cmd/src/generateACFs.cpp:303-318): exp of every non-zero bin, 1 elsewhere.
+__global__ void k_exp_nonzero(int64_t n, float* __restrict__ v) {
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+    const float a = v[i];
+    v[i] = a != 0.f ? expf(a) : 1.f;
+  }
+}
+
 __global__ void k_fill(int64_t n, float* __restrict__ x, float v) {
   for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
     x[i] = v;
@@ -482,6 +505,81 @@ __global__ void __launch_bounds__(kBlock) k_sens_batch(const SensJob* __restrict
   });
 }
 
+// [z][y][x] -> [z][x][y] through 32x32 shared-memory tiles.
+__global__ void __launch_bounds__(256) k_transpose_xy(int nx, int ny, const float* __restrict__ in,
+                                                      float* __restrict__ out) {
+  __shared__ float tile[32][33];
+  const int z = blockIdx.z;
+  const int x0 = blockIdx.x * 32, y0 = blockIdx.y * 32;
+  const int64_t base = (int64_t)z * nx * ny;
+  for (int r = threadIdx.y; r < 32; r += 8) {
+    const int y = y0 + r, x = x0 + threadIdx.x;
+    if (x < nx && y < ny) tile[r][threadIdx.x] = in[base + (int64_t)y * nx + x];
+  }
+  __syncthreads();
+  for (int r = threadIdx.y; r < 32; r += 8) {
+    const int x = x0 + r, y = y0 + threadIdx.x;
+    if (x < nx && y < ny) out[base + (int64_t)x * ny + y] = tile[threadIdx.x][r];
+  }
+}
+
+// EM update with the backprojection held in two layouts: bp = bpA + (bpT)^T;
+// x = (sens >= thr | > thr) ? x * bp / sens : 0; both bp buffers cleared.
+__global__ void __launch_bounds__(256) k_update_dual(int nx, int ny, float* __restrict__ x, float* __restrict__ bpA,
+                                                     float* __restrict__ bpT, const float* __restrict__ sens,
+                                                     const float* __restrict__ thr_ptr, float thr_value, int ge) {
+  __shared__ float tile[32][33];
+  const float thr = thr_ptr ? *thr_ptr : thr_value;
+  const int z = blockIdx.z;
+  const int x0 = blockIdx.x * 32, y0 = blockIdx.y * 32;
+  const int64_t base = (int64_t)z * nx * ny;
+  for (int r = threadIdx.y; r < 32; r += 8) {  // read the transposed tile along y
+    const int xx = x0 + r, yy = y0 + threadIdx.x;
+    if (xx < nx && yy < ny) {
+      const int64_t i = base + (int64_t)xx * ny + yy;
+      tile[threadIdx.x][r] = bpT[i];
+      bpT[i] = 0.f;
+    }
+  }
+  __syncthreads();
+  for (int r = threadIdx.y; r < 32; r += 8) {
+    const int yy = y0 + r, xx = x0 + threadIdx.x;
+    if (xx < nx && yy < ny) {
+      const int64_t i = base + (int64_t)yy * nx + xx;
+      const float b = A_ADD(bpA[i], tile[r][threadIdx.x]);
+      const float sv = sens[i];
+      const bool okv = ge ? (sv >= thr) : (sv > thr);
+      x[i] = okv ? A_DIV(A_MUL(x[i], b), sv) : 0.f;
+      bpA[i] = 0.f;
+    }
+  }
+}
+
+// bpA += (bpT)^T, bpT cleared.
+__global__ void __launch_bounds__(256) k_merge_transposed(int nx, int ny, float* __restrict__ bpA,
+                                                          float* __restrict__ bpT) {
+  __shared__ float tile[32][33];
+  const int z = blockIdx.z;
+  const int x0 = blockIdx.x * 32, y0 = blockIdx.y * 32;
+  const int64_t base = (int64_t)z * nx * ny;
+  for (int r = threadIdx.y; r < 32; r += 8) {
+    const int xx = x0 + r, yy = y0 + threadIdx.x;
+    if (xx < nx && yy < ny) {
+      const int64_t i = base + (int64_t)xx * ny + yy;
+      tile[threadIdx.x][r] = bpT[i];
+      bpT[i] = 0.f;
+    }
+  }
+  __syncthreads();
+  for (int r = threadIdx.y; r < 32; r += 8) {
+    const int yy = y0 + r, xx = x0 + threadIdx.x;
+    if (xx < nx && yy < ny) {
+      const int64_t i = base + (int64_t)yy * nx + xx;
+      bpA[i] = A_ADD(bpA[i], tile[r][threadIdx.x]);
+    }
+  }
+}
+
 inline unsigned grid_for(int64_t total) { return (unsigned)((total + kBlock - 1) / kBlock); }
 inline unsigned stream_grid(int64_t n) {
   int64_t g = (n + kBlock - 1) / kBlock;
@@ -527,7 +625,8 @@ cudaError_t launch_count_steps(const ImgGeom& g, const LorTable& t, SubsetSel s,
 
 cudaError_t launch_em_pass(const ImgGeom& g, const LorTable& t, SubsetSel s, const void* counts, int counts_dtype,
                            int counts_packed, const float* add, const float* x, float* bp, int back, int lik_mode,
-                           double* partials, double* lik, cudaStream_t st, const PreciseGeom& pg) {
+                           double* partials, double* lik, cudaStream_t st, const PreciseGeom& pg, const float* xT,
+                           float* bpT) {
   const int64_t total = (int64_t)t.n_sinos * s.nk * t.n_r;
   const unsigned grid = grid_for(total);
   if (total == 0) return cudaSuccess;
@@ -535,13 +634,14 @@ cudaError_t launch_em_pass(const ImgGeom& g, const LorTable& t, SubsetSel s, con
   do {                                                                                                        \
     if (t.is3d && pg.enabled)                                                                                 \
       k_em_pass<CT, true, true><<<grid, kBlock, 0, st>>>(g, t, s, pg, (const CT*)counts, counts_packed, add, x, \
-                                                         bp, back, lik_mode, partials, total);                \
+                                                         bp, nullptr, nullptr, back, lik_mode, partials, total); \
     else if (t.is3d)                                                                                          \
       k_em_pass<CT, true, false><<<grid, kBlock, 0, st>>>(g, t, s, pg, (const CT*)counts, counts_packed, add,   \
-                                                          x, bp, back, lik_mode, partials, total);            \
+                                                          x, bp, xT, bpT, back, lik_mode, partials, total);   \
     else                                                                                                      \
       k_em_pass<CT, false, false><<<grid, kBlock, 0, st>>>(g, t, s, pg, (const CT*)counts, counts_packed, add,  \
-                                                           x, bp, back, lik_mode, partials, total);           \
+                                                           x, bp, nullptr, nullptr, back, lik_mode, partials, \
+                                                           total);                                            \
   } while (0)
   switch (counts_dtype) {
     case APIRL_F32: APIRL_EM(float); break;
@@ -597,6 +697,31 @@ cudaError_t launch_update(int64_t n, float* x, float* bp, const float* sens, con
 cudaError_t launch_force_positive(int64_t n, float* x, cudaStream_t st) {
   if (n == 0) return cudaSuccess;
   k_force_positive<<<stream_grid(n), kBlock, 0, st>>>(n, x);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_transpose_xy(int nx, int ny, int nz, const float* in, float* out, cudaStream_t st) {
+  dim3 grid((nx + 31) / 32, (ny + 31) / 32, nz), block(32, 8);
+  k_transpose_xy<<<grid, block, 0, st>>>(nx, ny, in, out);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_update_dual(int nx, int ny, int nz, float* x, float* bpA, float* bpT, const float* sens,
+                               const float* thr_ptr, float thr_value, int ge, cudaStream_t st) {
+  dim3 grid((nx + 31) / 32, (ny + 31) / 32, nz), block(32, 8);
+  k_update_dual<<<grid, block, 0, st>>>(nx, ny, x, bpA, bpT, sens, thr_ptr, thr_value, ge);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_merge_transposed(int nx, int ny, int nz, float* bpA, float* bpT, cudaStream_t st) {
+  dim3 grid((nx + 31) / 32, (ny + 31) / 32, nz), block(32, 8);
+  k_merge_transposed<<<grid, block, 0, st>>>(nx, ny, bpA, bpT);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_exp_nonzero(int64_t n, float* v, cudaStream_t st) {
+  if (n == 0) return cudaSuccess;
+  k_exp_nonzero<<<stream_grid(n), kBlock, 0, st>>>(n, v);
   return cudaGetLastError();
 }
 

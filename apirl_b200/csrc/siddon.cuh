@@ -78,6 +78,30 @@ __device__ __forceinline__ void siddon3_setup(float p0x, float p0y, float p0z, f
 // `inb` is the full six-sided bounds test; linear_index = (k*ny + j)*nx + i is
 // only meaningful when inb is true.  Record-then-advance as in Siddon.cpp:310-340.
 template <class V>
+__device__ __forceinline__ void siddon3_walk(Walk3 w, const ImgGeom& g, V&& visit);
+
+// The same walk over an image stored with unit strides ux (x) and uy (y):
+// [z][y][x] is ux = 1, uy = nx; the transposed [z][x][y] is ux = ny, uy = 1.
+template <class V>
+__device__ __forceinline__ void siddon3_walk_s(Walk3 w, const ImgGeom& g, int ux, int uy, V&& visit) {
+  const int sx = w.iinc * ux, sy = w.jinc * uy, sz = w.kinc * g.nx * g.ny;
+  int idx = w.k * (g.nx * g.ny) + w.j * uy + w.i * ux;
+  for (int m = 0; m < w.n; m++) {
+    const bool cx = (w.ax <= w.ay) && (w.ax <= w.az);
+    const bool cy = !cx && (w.ay <= w.ax) && (w.ay <= w.az);
+    const float an = cx ? w.ax : (cy ? w.ay : w.az);
+    const float seg = A_MUL(A_SUB(an, w.ac), w.L);
+    const bool inb = ((unsigned)w.i < (unsigned)g.nx) & ((unsigned)w.j < (unsigned)g.ny) &
+                     ((unsigned)w.k < (unsigned)g.nz);
+    visit(inb, idx, seg);
+    w.ac = an;
+    if (cx) { w.i += w.iinc; idx += sx; w.ax = A_ADD(w.ax, w.axu); }
+    else if (cy) { w.j += w.jinc; idx += sy; w.ay = A_ADD(w.ay, w.ayu); }
+    else { w.k += w.kinc; idx += sz; w.az = A_ADD(w.az, w.azu); }
+  }
+}
+
+template <class V>
 __device__ __forceinline__ void siddon3_walk(Walk3 w, const ImgGeom& g, V&& visit) {
   const int sx = w.iinc, sy = w.jinc * g.nx, sz = w.kinc * g.nx * g.ny;
   int idx = (w.k * g.ny + w.j) * g.nx + w.i;

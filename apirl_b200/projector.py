@@ -111,6 +111,15 @@ class SiddonProjector:
         """fp64=False: the reference's float walk (default); True: FP64 alphas (precision study)."""
         check(self.lib.apirl_projector_set_alpha_precision(self.h, _lib.APIRL_ALPHA_F64 if fp64 else _lib.APIRL_ALPHA_F32))
 
+    def set_option(self, option, value):
+        check(self.lib.apirl_projector_set_option(self.h, int(option), int(value)))
+
+    def last_kernel_ms(self):
+        """CUDA-event duration of the last fused kernel (needs APIRL_OPT_KERNEL_TIMING)."""
+        ms = ctypes.c_double()
+        check(self.lib.apirl_projector_kernel_ms(self.h, ctypes.byref(ms)))
+        return ms.value
+
     def count_steps(self, subset=-1, nsubsets=1, stream=None):
         import torch
         out = torch.empty(self.num_bins(subset, nsubsets), dtype=torch.int32, device=f"cuda:{self.device}")
@@ -133,6 +142,11 @@ class SiddonProjector:
         check(self.lib.apirl_divide_and_backproject(self.h, _ptr(meas), _ptr(est), _ptr(image), subset, nsubsets,
                                                     _stream(stream)))
         return image
+
+    def generate_acf(self, mu, acf, subset=-1, nsubsets=1, stream=None):
+        """acf = exp(A mu) where A mu != 0, else 1 (generateACFs)."""
+        check(self.lib.apirl_generate_acf(self.h, _ptr(mu), _ptr(acf), subset, nsubsets, _stream(stream)))
+        return acf
 
     def em_pass(self, counts, x, bp, sens, subset=-1, nsubsets=1, add=None, thr=None, thr_value=0.0, ge=True,
                 counts_packed=False, lik=None, stream=None):

@@ -113,6 +113,17 @@ apirl_status apirl_projector_tables(const apirl_projector* p, float* h_lor, floa
  * segment length to float; projection and accumulation stay FP32.  No
  * counterpart in the reference, whose walk is float only. */
 apirl_status apirl_projector_set_alpha_precision(apirl_projector* p, int mode);
+/* Tuning and instrumentation options (no counterpart in the reference).
+ * APIRL_OPT_DUAL_LAYOUT (default 1): the fused 3D pass keeps a transposed
+ *   [z][x][y] copy of the image and of the backprojection (2 extra images on
+ *   the device) and walks rays running mostly along x in it, so that a warp's
+ *   32 neighbouring rays touch contiguous memory.  Results equal the 0 setting
+ *   up to the order of fp32 additions in the backprojection.
+ * APIRL_OPT_KERNEL_TIMING (default 0): record CUDA events around the fused
+ *   kernel of every pass; apirl_projector_kernel_ms returns the last one. */
+enum { APIRL_OPT_DUAL_LAYOUT = 1, APIRL_OPT_KERNEL_TIMING = 2 };
+apirl_status apirl_projector_set_option(apirl_projector* p, int option, int value);
+apirl_status apirl_projector_kernel_ms(apirl_projector* p, double* ms);
 /* Number of Siddon segments of every bin of a subset, written to d_steps (int32). */
 apirl_status apirl_count_steps(apirl_projector* p, int subset, int nsubsets, int32_t* d_steps, void* stream);
 
@@ -130,6 +141,13 @@ apirl_status apirl_backproject(apirl_projector* p, const float* d_sino, float* d
  * (:571-704 for 3D, :90-144 for 2D, with each reference's zero rules). */
 apirl_status apirl_divide_and_backproject(apirl_projector* p, const float* d_meas, const float* d_est,
                                           float* d_image, int subset, int nsubsets, void* stream);
+
+/* generateACFs (cmd/src/generateACFs.cpp:292-330): project an attenuation map
+ * (1/mm) and take exp of every non-zero bin, 1 elsewhere: the attenuation
+ * correction factors.  Their reciprocals are the multiplicative sinogram of
+ * the EM drivers.  exp is CUDA's expf (within 2 ulp of the host's). */
+apirl_status apirl_generate_acf(apirl_projector* p, const float* d_mu, float* d_acf, int subset, int nsubsets,
+                                void* stream);
 
 /* ---- bin-wise and pixel-wise steps --------------------------------------- */
 /* Sinogram3D::inverseDivideBinToBin: d_est = (m != 0 && e != 0) ? m / e : 0
