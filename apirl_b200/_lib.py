@@ -19,6 +19,7 @@ APIRL_ERR_ABORTED = 5
 
 APIRL_OPT_DUAL_LAYOUT = 1
 APIRL_OPT_KERNEL_TIMING = 2
+APIRL_OPT_EM_BLOCK = 3
 
 APIRL_ALPHA_F32 = 0
 APIRL_ALPHA_F64 = 1
@@ -70,6 +71,7 @@ SIGNATURES = {
     "apirl_projector_set_alpha_precision": (_i, [_vp, _i]),
     "apirl_projector_set_option": (_i, [_vp, _i, _i]),
     "apirl_projector_kernel_ms": (_i, [_vp, ctypes.POINTER(ctypes.c_double)]),
+    "apirl_projector_autotune": (_i, [_vp, _vp, _i, _vp, _i, _i, _i, ctypes.POINTER(_i), _vp]),
     "apirl_count_steps": (_i, [_vp, _i, _i, _vp, _vp]),
     "apirl_project": (_i, [_vp, _vp, _vp, _i, _i, _vp]),
     "apirl_backproject": (_i, [_vp, _vp, _vp, _i, _i, _vp]),

@@ -34,6 +34,9 @@ apirl_status bfail(apirl_status code, const char* what, cudaError_t e = cudaSucc
 
 size_t count_elem_size(int dtype) { return dtype == APIRL_U16 ? 2 : 4; }
 
+// Passes with at least this many bins get a launch of their own.
+constexpr int64_t kOwnLaunchBins = 1 << 20;
+
 enum class Stage { Queued, Sens, Passes, Final, Done };
 
 struct Job {
@@ -62,7 +65,7 @@ int64_t footprint_of(const apirl_image_geom& img, const apirl_sino3d_geom& sino,
   int64_t b = nbins * (int64_t)count_elem_size(dtype);
   if (mult) b += nbins * 4;
   if (add) b += nbins * 4;
-  b += nv * 4 * (2 + nsub);                               // x, bp, sens per subset
+  b += nv * 4 * (4 + nsub);                               // x, bp, their transposed copies, sens per subset
   b += (int64_t)sino.n_proj * sino.n_r * 16;              // LOR table
   b += ((nbins + 255) / 256) * 8 + 4096;                  // partials, small tables
   return b;
@@ -238,11 +241,16 @@ apirl_status apirl_batch_step(apirl_batch* b, int* n_active, int* n_queued) {
       ++it;
     }
   }
-  std::vector<Job*> sens, passes, finals;
+  std::vector<Job*> sens, passes, finals, big;
   for (auto& j : b->active) {
     if (j->stage == Stage::Sens) sens.push_back(j.get());
-    else if (j->stage == Stage::Passes) passes.push_back(j.get());
-    else if (j->stage == Stage::Final) finals.push_back(j.get());
+    else if (j->stage == Stage::Passes) {
+      // Jobs whose pass fills the GPU on its own run through the single-job
+      // fused pass (transposed-copy walk, tuned block size); the rest share
+      // one launch.
+      if (apirl_projector_num_bins(j->p, j->pass % j->nsub, j->nsub) >= kOwnLaunchBins) big.push_back(j.get());
+      else passes.push_back(j.get());
+    } else if (j->stage == Stage::Final) finals.push_back(j.get());
   }
   const int njob_max = (int)b->active.size() + 1;
   int64_t em_blocks = 0, upd_blocks = 0, sens_blocks = 0;
@@ -296,6 +304,13 @@ apirl_status apirl_batch_step(apirl_batch* b, int* n_active, int* n_queued) {
     BK(cudaMemcpyAsync(b->d_em, b->h_em, ne * sizeof(EmJob), cudaMemcpyHostToDevice, b->st));
     BK(apirl::launch_em_batch(b->d_em, b->h_em, ne, em_blocks, b->d_partials, b->st));
   }
+  for (Job* j : big) {
+    const int sub = j->pass % j->nsub;
+    apirl_status es = apirl_em_pass(j->p, j->d_counts, j->dtype, 0, j->d_add, j->d_x, j->d_bp,
+                                    j->d_sens + (int64_t)sub * j->nvox, nullptr, 0.f, 1, sub, j->nsub,
+                                    j->d_lik + j->pass, b->st);
+    if (es != APIRL_OK) return es;
+  }
   if (nu) {
     BK(cudaMemcpyAsync(b->d_upd, b->h_upd, nu * sizeof(UpdJob), cudaMemcpyHostToDevice, b->st));
     BK(apirl::launch_update_batch(b->d_upd, nu, upd_blocks, b->st));
@@ -304,6 +319,7 @@ apirl_status apirl_batch_step(apirl_batch* b, int* n_active, int* n_queued) {
   // 4. advance and retire.
   for (Job* j : sens) j->stage = j->iters * j->nsub > 0 ? Stage::Passes : Stage::Final;
   for (Job* j : passes) if (++j->pass == j->iters * j->nsub) j->stage = Stage::Final;
+  for (Job* j : big) if (++j->pass == j->iters * j->nsub) j->stage = Stage::Final;
   for (Job* j : finals) {
     j->out.resize(j->nvox);
     j->lik.resize((size_t)j->iters * j->nsub + 1);

@@ -62,9 +62,12 @@ struct DeviceScope {
   }
 };
 
+// Also clears a launch error left by an earlier, unrelated call, so that the
+// cudaGetLastError() after each of our launches reports that launch only.
 #define DEVICE_SCOPE(dev)                                                   \
   DeviceScope scope_(dev);                                                  \
-  if (scope_.err != cudaSuccess) return cuda_fail(scope_.err, "cudaSetDevice")
+  if (scope_.err != cudaSuccess) return cuda_fail(scope_.err, "cudaSetDevice"); \
+  (void)cudaGetLastError()
 
 bool valid_img(const apirl_image_geom* g) {
   return g && g->nx > 0 && g->ny > 0 && g->nz > 0 && g->dx > 0 && g->dy > 0 && g->dz > 0 &&
@@ -113,6 +116,14 @@ apirl_status finish_create(apirl_projector* p, apirl_projector** out) {
   CK(cudaMalloc(&p->d_partials, p->n_partials * sizeof(double)));
   CK(cudaMalloc(&p->d_minmax, 2 * sizeof(unsigned)));
   CK(cudaMalloc(&p->d_scalars, 8 * sizeof(double)));
+  if (p->is3d && p->dual_layout) {
+    // transposed image / backprojection of the fused pass, allocated here so
+    // that no pass allocates (passes may be captured into CUDA graphs)
+    const int64_t nv = (int64_t)p->g.nx * p->g.ny * p->g.nz;
+    CK(cudaMalloc(&p->d_xT, nv * sizeof(float)));
+    CK(cudaMalloc(&p->d_bpT, nv * sizeof(float)));
+    CK(cudaMemset(p->d_bpT, 0, nv * sizeof(float)));
+  }
   *out = p;
   return APIRL_OK;
 }
@@ -330,12 +341,14 @@ apirl_status apirl_generate_acf(apirl_projector* p, const float* d_mu, float* d_
 
 apirl_status apirl_inverse_divide(int64_t n, const float* d_meas, float* d_est, void* stream) {
   if (n < 0 || (n > 0 && (!d_meas || !d_est))) return fail(APIRL_ERR_INVALID, "bad arguments");
+  (void)cudaGetLastError();  // clear an unrelated earlier launch error
   CK(apirl::launch_inverse_divide(n, d_meas, d_est, (cudaStream_t)stream));
   return APIRL_OK;
 }
 
 apirl_status apirl_add_bins(int64_t n, const float* d_add, float* d_est, void* stream) {
   if (n < 0 || (n > 0 && (!d_add || !d_est))) return fail(APIRL_ERR_INVALID, "bad arguments");
+  (void)cudaGetLastError();  // clear an unrelated earlier launch error
   CK(apirl::launch_add_bins(n, d_add, d_est, (cudaStream_t)stream));
   return APIRL_OK;
 }
@@ -343,6 +356,7 @@ apirl_status apirl_add_bins(int64_t n, const float* d_add, float* d_est, void* s
 apirl_status apirl_likelihood(int64_t n, const float* d_est, const float* d_meas, int gt0, double* d_out,
                               void* stream) {
   if (n <= 0 || !d_est || !d_meas || !d_out) return fail(APIRL_ERR_INVALID, "bad arguments");
+  (void)cudaGetLastError();  // clear an unrelated earlier launch error
   // The per-block partials live in a small allocation owned by this call path.
   const int64_t nb = apirl::likelihood_blocks(n);
   double* part = nullptr;
@@ -355,6 +369,7 @@ apirl_status apirl_likelihood(int64_t n, const float* d_est, const float* d_meas
 
 apirl_status apirl_mlem_threshold(int64_t n, const float* d_sens, float* d_thr, void* stream) {
   if (n <= 0 || !d_sens || !d_thr) return fail(APIRL_ERR_INVALID, "bad arguments");
+  (void)cudaGetLastError();  // clear an unrelated earlier launch error
   unsigned* mm = nullptr;
   CK(cudaMallocAsync(&mm, 2 * sizeof(unsigned), (cudaStream_t)stream));
   cudaError_t e = apirl::launch_threshold(n, d_sens, mm, d_thr, (cudaStream_t)stream);
@@ -366,27 +381,24 @@ apirl_status apirl_mlem_threshold(int64_t n, const float* d_sens, float* d_thr, 
 apirl_status apirl_update_pixels(int64_t n, float* d_x, float* d_bp, const float* d_sens, const float* d_thr,
                                  float thr_value, int ge, int zero_bp, void* stream) {
   if (n < 0 || (n > 0 && (!d_x || !d_bp || !d_sens))) return fail(APIRL_ERR_INVALID, "bad arguments");
+  (void)cudaGetLastError();  // clear an unrelated earlier launch error
   CK(apirl::launch_update(n, d_x, d_bp, d_sens, d_thr, thr_value, ge, zero_bp, (cudaStream_t)stream));
   return APIRL_OK;
 }
 
 apirl_status apirl_force_positive(int64_t n, float* d_x, void* stream) {
   if (n < 0 || (n > 0 && !d_x)) return fail(APIRL_ERR_INVALID, "bad arguments");
+  (void)cudaGetLastError();  // clear an unrelated earlier launch error
   CK(apirl::launch_force_positive(n, d_x, (cudaStream_t)stream));
   return APIRL_OK;
 }
 
 namespace {
 
-bool use_dual(const apirl_projector* p) { return p->is3d && p->dual_layout && !p->pg.enabled; }
+bool use_dual(const apirl_projector* p) { return p->is3d && p->dual_layout && !p->pg.enabled && p->d_xT; }
 
-apirl_status ensure_dual(apirl_projector* p, cudaStream_t s) {
-  if (p->d_xT) return APIRL_OK;
-  const int64_t nv = (int64_t)p->g.nx * p->g.ny * p->g.nz;
-  CK(cudaMalloc(&p->d_xT, nv * sizeof(float)));
-  CK(cudaMalloc(&p->d_bpT, nv * sizeof(float)));
-  CK(cudaMemsetAsync(p->d_bpT, 0, nv * sizeof(float), s));
-  return APIRL_OK;
+apirl_status ensure_dual(apirl_projector* p, cudaStream_t) {
+  return p->d_xT ? APIRL_OK : fail(APIRL_ERR_INVALID, "dual-layout buffers missing");
 }
 
 // The fused kernel, bracketed by timing events when enabled.
@@ -400,7 +412,8 @@ apirl_status fused(apirl_projector* p, SubsetSel ss, const void* d_counts, int d
     CK(cudaEventRecord(p->ev0, s));
   }
   CK(apirl::launch_em_pass(p->g, p->t, ss, d_counts, dtype, packed, d_add, d_x, d_bp, 1, p->is3d ? 0 : 1,
-                           p->d_partials, d_lik, s, p->pg, dual ? p->d_xT : nullptr, dual ? p->d_bpT : nullptr));
+                           p->d_partials, d_lik, s, p->pg, dual ? p->d_xT : nullptr, dual ? p->d_bpT : nullptr,
+                           p->em_block));
   if (p->timing) {
     CK(cudaEventRecord(p->ev1, s));
     p->timed = 1;
@@ -468,10 +481,66 @@ apirl_status apirl_em_project_backproject(apirl_projector* p, const void* d_coun
 apirl_status apirl_projector_set_option(apirl_projector* p, int option, int value) {
   if (!p) return fail(APIRL_ERR_INVALID, "null projector");
   switch (option) {
-    case APIRL_OPT_DUAL_LAYOUT: p->dual_layout = value != 0; return APIRL_OK;
+    case APIRL_OPT_DUAL_LAYOUT: {
+      p->dual_layout = value != 0;
+      if (p->dual_layout && p->is3d && !p->d_xT) {
+        DEVICE_SCOPE(p->device);
+        const int64_t nv = (int64_t)p->g.nx * p->g.ny * p->g.nz;
+        CK(cudaMalloc(&p->d_xT, nv * sizeof(float)));
+        CK(cudaMalloc(&p->d_bpT, nv * sizeof(float)));
+        CK(cudaMemset(p->d_bpT, 0, nv * sizeof(float)));
+      }
+      return APIRL_OK;
+    }
     case APIRL_OPT_KERNEL_TIMING: p->timing = value != 0; p->timed = 0; return APIRL_OK;
+    case APIRL_OPT_EM_BLOCK:
+      if (value < 32 || value > 256 || value % 32) return fail(APIRL_ERR_INVALID, "block size must be 32..256, x32");
+      p->em_block = value;
+      return APIRL_OK;
     default: return fail(APIRL_ERR_INVALID, "unknown option %d", option);
   }
+}
+
+apirl_status apirl_projector_autotune(apirl_projector* p, const void* d_counts, int counts_dtype, const float* d_x,
+                                     int subset, int nsubsets, int repeats, int* best_block, void* stream) {
+  apirl_status st = check_em(p, d_counts, counts_dtype, d_x, d_x, subset, nsubsets);
+  if (st) return st;
+  DEVICE_SCOPE(p->device);
+  cudaStream_t s = (cudaStream_t)stream;
+  const int64_t nv = (int64_t)p->g.nx * p->g.ny * p->g.nz;
+  float* bp = nullptr;
+  CK(cudaMalloc(&bp, nv * sizeof(float)));
+  cudaEvent_t a = nullptr, b = nullptr;
+  cudaEventCreate(&a);
+  cudaEventCreate(&b);
+  const int cands[] = {64, 96, 128, 192, 256};
+  const int saved_timing = p->timing;
+  p->timing = 0;
+  float best = 1e30f;
+  int best_b = p->em_block;
+  if (repeats < 1) repeats = 1;
+  for (int c : cands) {
+    p->em_block = c;
+    CK(cudaMemsetAsync(bp, 0, nv * sizeof(float), s));
+    st = apirl_em_project_backproject(p, d_counts, counts_dtype, 0, nullptr, d_x, bp, subset, nsubsets, nullptr, s);
+    if (st) break;
+    cudaEventRecord(a, s);
+    for (int r = 0; r < repeats && !st; r++)
+      st = apirl_em_project_backproject(p, d_counts, counts_dtype, 0, nullptr, d_x, bp, subset, nsubsets, nullptr, s);
+    cudaEventRecord(b, s);
+    cudaEventSynchronize(b);
+    float ms = 0;
+    cudaEventElapsedTime(&ms, a, b);
+    if (ms < best) { best = ms; best_b = c; }
+  }
+  p->timing = saved_timing;
+  p->em_block = best_b;
+  cudaEventDestroy(a);
+  cudaEventDestroy(b);
+  cudaFree(bp);
+  if (st) return st;
+  if (best_block) *best_block = best_b;
+  return APIRL_OK;
 }
 
 apirl_status apirl_projector_kernel_ms(apirl_projector* p, double* ms) {

@@ -65,7 +65,7 @@ int64_t em_pass_blocks(const LorTable& t, SubsetSel s);
 cudaError_t launch_em_pass(const ImgGeom& g, const LorTable& t, SubsetSel s, const void* counts, int counts_dtype,
                            int counts_packed, const float* add, const float* x, float* bp, int back, int lik_mode,
                            double* partials, double* lik, cudaStream_t st, const PreciseGeom& pg = PreciseGeom(),
-                           const float* xT = nullptr, float* bpT = nullptr);
+                           const float* xT = nullptr, float* bpT = nullptr, int block = 0);
 // Transposed-layout helpers for the fused pass (3D): [z][y][x] -> [z][x][y], and
 // the update that merges the two backprojection buffers.
 cudaError_t launch_transpose_xy(int nx, int ny, int nz, const float* in, float* out, cudaStream_t st);
@@ -155,6 +155,7 @@ struct apirl_projector {
   float* d_xT = nullptr;         // [z][x][y] copies for the dual layout, allocated on first use
   float* d_bpT = nullptr;        // kept zero between passes
   int timing = 0;                // record CUDA events around the fused kernel
+  int em_block = 128;            // threads per block of the fused kernel (APIRL_OPT_EM_BLOCK / autotune)
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
   int timed = 0;                 // an event pair has been recorded
   int n_rings = 0;               // 3D geometry as given, for building the FP64 tables

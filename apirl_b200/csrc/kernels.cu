@@ -22,6 +22,11 @@ namespace apirl {
 namespace {
 
 constexpr int kBlock = 256;
+// Minimum resident 256-thread blocks per SM for the fused kernel (register cap).
+#ifndef APIRL_EM_MIN_BLOCKS
+#define APIRL_EM_MIN_BLOCKS 5
+#endif
+constexpr int kEmMinBlocks = APIRL_EM_MIN_BLOCKS;
 
 struct BinPos {
   int g, k, l, a;  // sinogram, subset angle, r, full angle
@@ -106,7 +111,7 @@ template <bool F64A>
 __global__ void __launch_bounds__(kBlock) k_project3(ImgGeom g, LorTable t, SubsetSel s, PreciseGeom pg,
                                                      const float* __restrict__ img, float* __restrict__ out,
                                                      int64_t total) {
-  const int64_t b = (int64_t)blockIdx.x * kBlock + threadIdx.x;
+  const int64_t b = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (b >= total) return;
   const BinPos p = decode(b, t, s);
   if (F64A) {
@@ -121,7 +126,7 @@ __global__ void __launch_bounds__(kBlock) k_project3(ImgGeom g, LorTable t, Subs
 __global__ void __launch_bounds__(kBlock) k_project2(ImgGeom g, LorTable t, SubsetSel s,
                                                      const float* __restrict__ img, float* __restrict__ out,
                                                      int64_t total) {
-  const int64_t b = (int64_t)blockIdx.x * kBlock + threadIdx.x;
+  const int64_t b = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (b >= total) return;
   const BinPos p = decode(b, t, s);
   if (!t.ok[p.l]) return;  // getPointsFromLor false: the bin is not written (SiddonProjector.cpp:166-173)
@@ -145,7 +150,7 @@ __global__ void __launch_bounds__(kBlock) k_backproject3(ImgGeom g, LorTable t, 
                                                          const float* __restrict__ vin, int vin_mode,
                                                          const float* __restrict__ vest, int divide,
                                                          float* __restrict__ img, int64_t total) {
-  const int64_t b = (int64_t)blockIdx.x * kBlock + threadIdx.x;
+  const int64_t b = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (b >= total) return;
   const BinPos p = decode(b, t, s);
   const float v = load_bin(vin, vin_mode, b, p, t);
@@ -179,7 +184,7 @@ __global__ void __launch_bounds__(kBlock) k_backproject2(ImgGeom g, LorTable t, 
                                                          const float* __restrict__ vin, int vin_mode,
                                                          const float* __restrict__ vest, int divide,
                                                          float* __restrict__ img, int64_t total) {
-  const int64_t b = (int64_t)blockIdx.x * kBlock + threadIdx.x;
+  const int64_t b = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (b >= total) return;
   const BinPos p = decode(b, t, s);
   const float v = load_bin(vin, vin_mode, b, p, t);
@@ -200,7 +205,7 @@ __global__ void __launch_bounds__(kBlock) k_backproject2(ImgGeom g, LorTable t, 
 
 __global__ void __launch_bounds__(kBlock) k_count_steps(ImgGeom g, LorTable t, SubsetSel s, int32_t* steps,
                                                         int64_t total) {
-  const int64_t b = (int64_t)blockIdx.x * kBlock + threadIdx.x;
+  const int64_t b = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (b >= total) return;
   const BinPos p = decode(b, t, s);
   const float4 L = t.lor[(int64_t)p.a * t.n_r + p.l];
@@ -226,13 +231,13 @@ __global__ void __launch_bounds__(kBlock) k_count_steps(ImgGeom g, LorTable t, S
 // 32 near-parallel rays of a warp, which lie side by side along y, touch
 // contiguous addresses; rays mostly along y use the [z][y][x] buffers.
 template <typename CT, bool IS3D, bool F64A>
-__global__ void __launch_bounds__(kBlock) k_em_pass(ImgGeom g, LorTable t, SubsetSel s, PreciseGeom pg,
+__global__ void __launch_bounds__(kBlock, kEmMinBlocks) k_em_pass(ImgGeom g, LorTable t, SubsetSel s, PreciseGeom pg,
                                                     const CT* __restrict__ counts,
                                                     int counts_packed, const float* __restrict__ add,
                                                     const float* __restrict__ x, float* __restrict__ bp,
                                                     const float* __restrict__ xT, float* __restrict__ bpT, int back,
                                                     int lik_mode, double* __restrict__ partials, int64_t total) {
-  const int64_t b = (int64_t)blockIdx.x * kBlock + threadIdx.x;
+  const int64_t b = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   double term = 0.0;
   if (b < total) {
     const BinPos p = decode(b, t, s);
@@ -261,10 +266,7 @@ __global__ void __launch_bounds__(kBlock) k_em_pass(ImgGeom g, LorTable t, Subse
       const int ux = tr ? g.ny : 1, uy = tr ? 1 : g.nx;
       Walk3 w;
       siddon3_setup(L.x, L.y, z.x, vx, vy, A_SUB(z.y, z.x), g, w);
-      float e = 0.f;
-      siddon3_walk_s(w, g, ux, uy, [&](bool inb, int idx, float seg) {
-        if (inb) e = A_ADD(e, A_MUL(seg, __ldg(xs + idx)));
-      });
+      float e = siddon3_gather2(w, g, ux, uy, xs);
       if (add) e = A_ADD(e, __ldg(add + ci));
       const float r = (m != 0.f && e != 0.f) ? A_DIV(m, e) : 0.f;
       if (lik_mode == 2) { if (r > 0.f) term = (double)m * log((double)r) - (double)r; }
@@ -288,8 +290,11 @@ __global__ void __launch_bounds__(kBlock) k_em_pass(ImgGeom g, LorTable t, Subse
         });
     }
   }
-  const double bs = block_sum(term);
-  if (threadIdx.x == 0) partials[blockIdx.x] = bs;
+  // Warp-level partial, no block barrier: warps whose rays are short retire
+  // without waiting for the block's longest ray.
+  #pragma unroll
+  for (int o = 16; o > 0; o >>= 1) term += __shfl_down_sync(0xffffffffu, term, o);
+  if ((threadIdx.x & 31) == 0) partials[((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5] = term;
 }
 
 // Deterministic final sum of per-block partials (one block).
@@ -317,7 +322,7 @@ __global__ void __launch_bounds__(kBlock) k_likelihood(int64_t n, const float* _
                                                        const float* __restrict__ meas, int gt0,
                                                        double* __restrict__ partials) {
   double v = 0.0;
-  for (int64_t i = (int64_t)blockIdx.x * kBlock + threadIdx.x; i < n; i += (int64_t)gridDim.x * kBlock) {
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
     const float e = est[i];
     if (gt0 ? (e > 0.f) : (e != 0.f)) v += (double)meas[i] * log((double)e) - (double)e;
   }
@@ -341,7 +346,7 @@ __global__ void k_minmax_init(const float* __restrict__ sens, unsigned* mm) {
 // Minimum over non-zero values and maximum over all values.
 __global__ void __launch_bounds__(kBlock) k_minmax(int64_t n, const float* __restrict__ v, unsigned* mm) {
   float mn = FLT_MAX, mx = -FLT_MAX;
-  for (int64_t i = (int64_t)blockIdx.x * kBlock + threadIdx.x; i < n; i += (int64_t)gridDim.x * kBlock) {
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
     const float f = v[i];
     if (f != 0.f && f < mn) mn = f;
     if (f > mx) mx = f;
@@ -590,7 +595,8 @@ inline unsigned stream_grid(int64_t n) {
 }  // namespace
 
 int64_t em_pass_blocks(const LorTable& t, SubsetSel s) {
-  return ((int64_t)t.n_sinos * s.nk * t.n_r + kBlock - 1) / kBlock;
+  // one likelihood partial per warp of the largest block size
+  return ((int64_t)t.n_sinos * s.nk * t.n_r + kBlock - 1) / kBlock * (kBlock / 32);
 }
 int64_t likelihood_blocks(int64_t n) { return stream_grid(n); }
 
@@ -626,23 +632,32 @@ cudaError_t launch_count_steps(const ImgGeom& g, const LorTable& t, SubsetSel s,
 cudaError_t launch_em_pass(const ImgGeom& g, const LorTable& t, SubsetSel s, const void* counts, int counts_dtype,
                            int counts_packed, const float* add, const float* x, float* bp, int back, int lik_mode,
                            double* partials, double* lik, cudaStream_t st, const PreciseGeom& pg, const float* xT,
-                           float* bpT) {
+                           float* bpT, int block) {
   const int64_t total = (int64_t)t.n_sinos * s.nk * t.n_r;
-  const unsigned grid = grid_for(total);
+  if (block < 32 || block > kBlock || block % 32) block = kBlock;
+  const unsigned grid = (unsigned)((total + block - 1) / block);
   if (total == 0) return cudaSuccess;
 #define APIRL_EM(CT)                                                                                          \
   do {                                                                                                        \
     if (t.is3d && pg.enabled)                                                                                 \
-      k_em_pass<CT, true, true><<<grid, kBlock, 0, st>>>(g, t, s, pg, (const CT*)counts, counts_packed, add, x, \
+      k_em_pass<CT, true, true><<<grid, block, 0, st>>>(g, t, s, pg, (const CT*)counts, counts_packed, add, x, \
                                                          bp, nullptr, nullptr, back, lik_mode, partials, total); \
     else if (t.is3d)                                                                                          \
-      k_em_pass<CT, true, false><<<grid, kBlock, 0, st>>>(g, t, s, pg, (const CT*)counts, counts_packed, add,   \
+      k_em_pass<CT, true, false><<<grid, block, 0, st>>>(g, t, s, pg, (const CT*)counts, counts_packed, add,   \
                                                           x, bp, xT, bpT, back, lik_mode, partials, total);   \
     else                                                                                                      \
-      k_em_pass<CT, false, false><<<grid, kBlock, 0, st>>>(g, t, s, pg, (const CT*)counts, counts_packed, add,  \
+      k_em_pass<CT, false, false><<<grid, block, 0, st>>>(g, t, s, pg, (const CT*)counts, counts_packed, add,  \
                                                            x, bp, nullptr, nullptr, back, lik_mode, partials, \
                                                            total);                                            \
   } while (0)
+  static bool carveout_set = false;  // prefer L1 over shared memory: the kernel uses none
+  if (!carveout_set) {
+    cudaFuncSetAttribute(k_em_pass<float, true, false>, cudaFuncAttributePreferredSharedMemoryCarveout, 0);
+    cudaFuncSetAttribute(k_em_pass<uint32_t, true, false>, cudaFuncAttributePreferredSharedMemoryCarveout, 0);
+    cudaFuncSetAttribute(k_em_pass<uint16_t, true, false>, cudaFuncAttributePreferredSharedMemoryCarveout, 0);
+    (void)cudaGetLastError();
+    carveout_set = true;
+  }
   switch (counts_dtype) {
     case APIRL_F32: APIRL_EM(float); break;
     case APIRL_U32: APIRL_EM(uint32_t); break;
@@ -652,7 +667,7 @@ cudaError_t launch_em_pass(const ImgGeom& g, const LorTable& t, SubsetSel s, con
 #undef APIRL_EM
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess || !lik) return e;
-  k_sum_partials<<<1, kBlock, 0, st>>>(partials, grid, lik);
+  k_sum_partials<<<1, kBlock, 0, st>>>(partials, (int64_t)grid * (block / 32), lik);
   return cudaGetLastError();
 }
 

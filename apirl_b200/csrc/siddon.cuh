@@ -87,8 +87,11 @@ __device__ __forceinline__ void siddon3_walk_s(Walk3 w, const ImgGeom& g, int ux
   const int sx = w.iinc * ux, sy = w.jinc * uy, sz = w.kinc * g.nx * g.ny;
   int idx = w.k * (g.nx * g.ny) + w.j * uy + w.i * ux;
   for (int m = 0; m < w.n; m++) {
-    const bool cx = (w.ax <= w.ay) && (w.ax <= w.az);
-    const bool cy = !cx && (w.ay <= w.ax) && (w.ay <= w.az);
+    // The reference's test is (ax<=ay && ax<=az) / (ay<=ax && ay<=az) / else;
+    // the crossing parameters are never NaN (finite, FLT_MAX or +inf), and
+    // then "not x and ay <= az" selects exactly the same branch.
+    const bool cx = (w.ax <= w.ay) & (w.ax <= w.az);
+    const bool cy = !cx & (w.ay <= w.az);
     const float an = cx ? w.ax : (cy ? w.ay : w.az);
     const float seg = A_MUL(A_SUB(an, w.ac), w.L);
     const bool inb = ((unsigned)w.i < (unsigned)g.nx) & ((unsigned)w.j < (unsigned)g.ny) &
@@ -99,6 +102,49 @@ __device__ __forceinline__ void siddon3_walk_s(Walk3 w, const ImgGeom& g, int ux
     else if (cy) { w.j += w.jinc; idx += sy; w.ay = A_ADD(w.ay, w.ayu); }
     else { w.k += w.kinc; idx += sz; w.az = A_ADD(w.az, w.azu); }
   }
+}
+
+// Forward gather sum over the walk, two segments per iteration: both voxel
+// loads are issued before either product is added, doubling the loads in
+// flight per thread.  The additions keep the walk order, so the sum is
+// bit-identical to siddon3_walk_s with acc += seg * img[idx].
+__device__ __forceinline__ float siddon3_gather2(Walk3 w, const ImgGeom& g, int ux, int uy,
+                                                 const float* __restrict__ img) {
+  const int sx = w.iinc * ux, sy = w.jinc * uy, sz = w.kinc * g.nx * g.ny;
+  int idx = w.k * (g.nx * g.ny) + w.j * uy + w.i * ux;
+  float acc = 0.f;
+  auto advance = [&](int& id, float& seg, bool& inb) {
+    const bool cx = (w.ax <= w.ay) & (w.ax <= w.az);
+    const bool cy = !cx & (w.ay <= w.az);
+    const float an = cx ? w.ax : (cy ? w.ay : w.az);
+    seg = A_MUL(A_SUB(an, w.ac), w.L);
+    inb = ((unsigned)w.i < (unsigned)g.nx) & ((unsigned)w.j < (unsigned)g.ny) & ((unsigned)w.k < (unsigned)g.nz);
+    id = idx;
+    w.ac = an;
+    if (cx) { w.i += w.iinc; idx += sx; w.ax = A_ADD(w.ax, w.axu); }
+    else if (cy) { w.j += w.jinc; idx += sy; w.ay = A_ADD(w.ay, w.ayu); }
+    else { w.k += w.kinc; idx += sz; w.az = A_ADD(w.az, w.azu); }
+  };
+  int m = 0;
+  for (; m + 1 < w.n; m += 2) {
+    int ia, ib;
+    float sa, sb;
+    bool ka, kb;
+    advance(ia, sa, ka);
+    advance(ib, sb, kb);
+    const float va = ka ? __ldg(img + ia) : 0.f;
+    const float vb = kb ? __ldg(img + ib) : 0.f;
+    if (ka) acc = A_ADD(acc, A_MUL(sa, va));
+    if (kb) acc = A_ADD(acc, A_MUL(sb, vb));
+  }
+  if (m < w.n) {
+    int ia;
+    float sa;
+    bool ka;
+    advance(ia, sa, ka);
+    if (ka) acc = A_ADD(acc, A_MUL(sa, __ldg(img + ia)));
+  }
+  return acc;
 }
 
 template <class V>

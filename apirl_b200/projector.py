@@ -114,6 +114,13 @@ class SiddonProjector:
     def set_option(self, option, value):
         check(self.lib.apirl_projector_set_option(self.h, int(option), int(value)))
 
+    def autotune(self, counts, x, subset=0, nsubsets=1, repeats=2, stream=None):
+        """Picks the fused kernel's block size by timing the candidates; returns it."""
+        best = ctypes.c_int()
+        check(self.lib.apirl_projector_autotune(self.h, _ptr(counts), _counts_dtype(counts), _ptr(x), subset, nsubsets,
+                                                repeats, ctypes.byref(best), _stream(stream)))
+        return best.value
+
     def last_kernel_ms(self):
         """CUDA-event duration of the last fused kernel (needs APIRL_OPT_KERNEL_TIMING)."""
         ms = ctypes.c_double()

@@ -196,6 +196,11 @@ def run_gpu(args):
     lik = torch.zeros(1, dtype=torch.float64, device=dev)
 
     from apirl_b200 import _lib as _l
+    # autotuner: fused-kernel block size, timed on this job's own data (outside the timed region)
+    best_block = P.autotune(counts, x, 0, NSUB, repeats=2, stream=stream)
+    bp.zero_()
+    torch.cuda.synchronize(dev)
+    log(f"autotuned fused-kernel block size: {best_block}")
     P.set_option(_l.APIRL_OPT_KERNEL_TIMING, 1)
 
     def step(s, evs=None):
@@ -279,7 +284,7 @@ def run_gpu(args):
             "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded phantom, Poisson counts)",
             "config": {"workload": WORKLOAD if args.max_ring_diff is None else
                        WORKLOAD + f" (profiling case: segments |rd| <= {args.max_ring_diff} only)",
-                       "subsets": NSUB, "counts_dtype": "uint32",
+                       "subsets": NSUB, "counts_dtype": "uint32", "em_block": best_block,
                        "l2": "flushed between timed steps (256 MB write outside the timed events)",
                        "parallelism": f"replicas x{world}"},
             "siddon_gsteps_per_s": gsteps,

@@ -120,10 +120,17 @@ apirl_status apirl_projector_set_alpha_precision(apirl_projector* p, int mode);
  *   32 neighbouring rays touch contiguous memory.  Results equal the 0 setting
  *   up to the order of fp32 additions in the backprojection.
  * APIRL_OPT_KERNEL_TIMING (default 0): record CUDA events around the fused
- *   kernel of every pass; apirl_projector_kernel_ms returns the last one. */
-enum { APIRL_OPT_DUAL_LAYOUT = 1, APIRL_OPT_KERNEL_TIMING = 2 };
+ *   kernel of every pass; apirl_projector_kernel_ms returns the last one.
+ * APIRL_OPT_EM_BLOCK (default 128): threads per block of the fused kernel
+ *   (32..256, a multiple of 32). */
+enum { APIRL_OPT_DUAL_LAYOUT = 1, APIRL_OPT_KERNEL_TIMING = 2, APIRL_OPT_EM_BLOCK = 3 };
 apirl_status apirl_projector_set_option(apirl_projector* p, int option, int value);
 apirl_status apirl_projector_kernel_ms(apirl_projector* p, double* ms);
+/* Autotuner: times the fused kernel (apirl_em_project_backproject, `repeats`
+ * runs each, on the caller's counts and image) for block sizes 64..256 and
+ * keeps the fastest; its size goes to *best_block.  Allocates one scratch image. */
+apirl_status apirl_projector_autotune(apirl_projector* p, const void* d_counts, int counts_dtype, const float* d_x,
+                                     int subset, int nsubsets, int repeats, int* best_block, void* stream);
 /* Number of Siddon segments of every bin of a subset, written to d_steps (int32). */
 apirl_status apirl_count_steps(apirl_projector* p, int subset, int nsubsets, int32_t* d_steps, void* stream);
 

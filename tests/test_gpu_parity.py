@@ -165,7 +165,9 @@ def test_em_pass_vs_oracle(oracle, dtype):
     subset, ns = 2, 5
     want_x, want_lik, meas_sub = _oracle_osem_pass(oracle, sg, ig, x0, meas, sens, subset, ns)
     P = ap.SiddonProjector(ig, sg)
-    for packed in (False, True):
+    from apirl_b200 import _lib
+    for packed, block in ((False, 128), (True, 128), (False, 64), (True, 256), (False, 96)):
+        P.set_option(_lib.APIRL_OPT_EM_BLOCK, block)
         x = t(x0)
         bp = torch.zeros(ig.n_voxels, dtype=torch.float32, device=DEV)
         lik = torch.zeros(1, dtype=torch.float64, device=DEV)
