@@ -80,6 +80,7 @@ SIGNATURES = {
     "apirl_inverse_divide": (_i, [_i64, _vp, _vp, _vp]),
     "apirl_add_bins": (_i, [_i64, _vp, _vp, _vp]),
     "apirl_likelihood": (_i, [_i64, _vp, _vp, _i, _vp, _vp]),
+    "apirl_likelihood_noalloc": (_i, [_i64, _vp, _vp, _i, _vp, _vp]),
     "apirl_mlem_threshold": (_i, [_i64, _vp, _vp, _vp]),
     "apirl_update_pixels": (_i, [_i64, _vp, _vp, _vp, _vp, _f, _i, _i, _vp]),
     "apirl_force_positive": (_i, [_i64, _vp, _vp]),

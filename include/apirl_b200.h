@@ -167,6 +167,17 @@ apirl_status apirl_add_bins(int64_t n, const float* d_add, float* d_est, void* s
  * Sinogram3D.cpp:584-606), accumulated in FP64 and written to *d_out (device double). */
 apirl_status apirl_likelihood(int64_t n, const float* d_est, const float* d_meas, int gt0, double* d_out,
                               void* stream);
+/* apirl_likelihood without any device allocation.  No counterpart in the
+ * reference.  For callers that cannot call cudaMalloc: their device memory is
+ * owned by another allocator, or an allocation would stall or fail where they
+ * run.  Its scratch is one static device array of 65,536 FP64 partials
+ * (512 KiB), so n is limited to APIRL_LIKELIHOOD_NOALLOC_MAX_BINS (larger n:
+ * APIRL_ERR_INVALID).  Runs on the calling thread's current device; the first
+ * call on a device looks up the array's address there, so make it before any
+ * stream capture.  Calls share the array: calls that overlap on the GPU race. */
+#define APIRL_LIKELIHOOD_NOALLOC_MAX_BINS ((int64_t)65536 * 4096)
+apirl_status apirl_likelihood_noalloc(int64_t n, const float* d_est, const float* d_meas, int gt0, double* d_out,
+                                      void* stream);
 /* Mlem::updateUpdateThreshold: min over non-zero pixels + 1e-4 (max - min)
  * (recon/src/Mlem.cpp:39-43, data/src/Images.cpp:397-433), written to *d_thr. */
 apirl_status apirl_mlem_threshold(int64_t n, const float* d_sens, float* d_thr, void* stream);
