@@ -6,6 +6,8 @@
 #include <cstring>
 #include <string>
 #include <vector>
+#include <climits>
+
 #include "internal.h"
 #include "../../include/apirl_b200.h"
 
@@ -98,6 +100,29 @@ apirl_status check_subset(const apirl_projector* p, int subset, int nsub) {
   return APIRL_OK;
 }
 
+// The padded two-layout buffers of the fused 3D pass, allocated with the
+// projector so that no pass allocates (passes may be captured into CUDA
+// graphs).  Volumes whose padded size does not fit a 32-bit index keep the
+// single unpadded layout.
+apirl_status alloc_pad(apirl_projector* p) {
+  if (p->pad.pA) return APIRL_OK;
+  const int64_t pv = (int64_t)(p->g.nx + 2 * apirl::kPad) * (p->g.ny + 2 * apirl::kPad) * (p->g.nz + 2 * apirl::kPad);
+  if (pv > INT_MAX) return APIRL_OK;
+  float* b[4] = {nullptr, nullptr, nullptr, nullptr};
+  for (int i = 0; i < 4; i++) {
+    if (cudaMalloc(&b[i], pv * sizeof(float)) != cudaSuccess || cudaMemset(b[i], 0, pv * sizeof(float)) != cudaSuccess) {
+      for (int k = 0; k <= i; k++) cudaFree(b[k]);
+      return cuda_fail(cudaGetLastError(), "padded layout buffers");
+    }
+  }
+  p->pad.pA = b[0];
+  p->pad.pT = b[1];
+  p->pad.bA = b[2];
+  p->pad.bT = b[3];
+  p->pad.lim = (unsigned)pv;
+  return APIRL_OK;
+}
+
 apirl_status finish_create(apirl_projector* p, apirl_projector** out) {
   const size_t nl = p->host.lor.size() / 4;
   CK(cudaMalloc(&p->d_lor, nl * sizeof(float4)));
@@ -117,12 +142,8 @@ apirl_status finish_create(apirl_projector* p, apirl_projector** out) {
   CK(cudaMalloc(&p->d_minmax, 2 * sizeof(unsigned)));
   CK(cudaMalloc(&p->d_scalars, 8 * sizeof(double)));
   if (p->is3d && p->dual_layout) {
-    // transposed image / backprojection of the fused pass, allocated here so
-    // that no pass allocates (passes may be captured into CUDA graphs)
-    const int64_t nv = (int64_t)p->g.nx * p->g.ny * p->g.nz;
-    CK(cudaMalloc(&p->d_xT, nv * sizeof(float)));
-    CK(cudaMalloc(&p->d_bpT, nv * sizeof(float)));
-    CK(cudaMemset(p->d_bpT, 0, nv * sizeof(float)));
+    const apirl_status st = alloc_pad(p);
+    if (st) return st;
   }
   *out = p;
   return APIRL_OK;
@@ -235,8 +256,10 @@ void apirl_projector_destroy(apirl_projector* p) {
   cudaFree(p->d_scalars);
   cudaFree(p->d_lor64);
   cudaFree(p->d_z64);
-  cudaFree(p->d_xT);
-  cudaFree(p->d_bpT);
+  cudaFree(p->pad.pA);
+  cudaFree(p->pad.pT);
+  cudaFree(p->pad.bA);
+  cudaFree(p->pad.bT);
   if (p->ev0) cudaEventDestroy(p->ev0);
   if (p->ev1) cudaEventDestroy(p->ev1);
   delete p;
@@ -395,11 +418,7 @@ apirl_status apirl_force_positive(int64_t n, float* d_x, void* stream) {
 
 namespace {
 
-bool use_dual(const apirl_projector* p) { return p->is3d && p->dual_layout && !p->pg.enabled && p->d_xT; }
-
-apirl_status ensure_dual(apirl_projector* p, cudaStream_t) {
-  return p->d_xT ? APIRL_OK : fail(APIRL_ERR_INVALID, "dual-layout buffers missing");
-}
+bool use_dual(const apirl_projector* p) { return p->is3d && p->dual_layout && !p->pg.enabled && p->pad.pA; }
 
 // The fused kernel, bracketed by timing events when enabled.
 apirl_status fused(apirl_projector* p, SubsetSel ss, const void* d_counts, int dtype, int packed, const float* d_add,
@@ -412,8 +431,7 @@ apirl_status fused(apirl_projector* p, SubsetSel ss, const void* d_counts, int d
     CK(cudaEventRecord(p->ev0, s));
   }
   CK(apirl::launch_em_pass(p->g, p->t, ss, d_counts, dtype, packed, d_add, d_x, d_bp, 1, p->is3d ? 0 : 1,
-                           p->d_partials, d_lik, s, p->pg, dual ? p->d_xT : nullptr, dual ? p->d_bpT : nullptr,
-                           p->em_block));
+                           p->d_partials, d_lik, s, p->pg, dual ? p->pad : apirl::PadBuffers(), p->em_block));
   if (p->timing) {
     CK(cudaEventRecord(p->ev1, s));
     p->timed = 1;
@@ -444,12 +462,10 @@ apirl_status apirl_em_pass(apirl_projector* p, const void* d_counts, int counts_
   SubsetSel ss = make_subset(p, subset, nsubsets);
   const int64_t nv = (int64_t)p->g.nx * p->g.ny * p->g.nz;
   if (use_dual(p)) {
-    st = ensure_dual(p, s);
-    if (st) return st;
-    CK(apirl::launch_transpose_xy(p->g.nx, p->g.ny, p->g.nz, d_x, p->d_xT, s));
+    CK(apirl::launch_pad_copy(p->g, d_x, p->pad, s));
     st = fused(p, ss, d_counts, counts_dtype, counts_packed, d_add, d_x, d_bp, true, d_lik, s);
     if (st) return st;
-    CK(apirl::launch_update_dual(p->g.nx, p->g.ny, p->g.nz, d_x, d_bp, p->d_bpT, d_sens, d_thr, thr_value, ge, s));
+    CK(apirl::launch_pad_reduce(p->g, p->pad, 0, d_x, nullptr, d_sens, d_thr, thr_value, ge, s));
     return APIRL_OK;
   }
   st = fused(p, ss, d_counts, counts_dtype, counts_packed, d_add, d_x, d_bp, false, d_lik, s);
@@ -467,12 +483,10 @@ apirl_status apirl_em_project_backproject(apirl_projector* p, const void* d_coun
   cudaStream_t s = (cudaStream_t)stream;
   SubsetSel ss = make_subset(p, subset, nsubsets);
   if (use_dual(p)) {
-    st = ensure_dual(p, s);
-    if (st) return st;
-    CK(apirl::launch_transpose_xy(p->g.nx, p->g.ny, p->g.nz, d_x, p->d_xT, s));
+    CK(apirl::launch_pad_copy(p->g, d_x, p->pad, s));
     st = fused(p, ss, d_counts, counts_dtype, counts_packed, d_add, d_x, d_bp, true, d_lik, s);
     if (st) return st;
-    CK(apirl::launch_merge_transposed(p->g.nx, p->g.ny, p->g.nz, d_bp, p->d_bpT, s));
+    CK(apirl::launch_pad_reduce(p->g, p->pad, 1, nullptr, d_bp, nullptr, nullptr, 0.f, 0, s));
     return APIRL_OK;
   }
   return fused(p, ss, d_counts, counts_dtype, counts_packed, d_add, d_x, d_bp, false, d_lik, s);
@@ -483,12 +497,9 @@ apirl_status apirl_projector_set_option(apirl_projector* p, int option, int valu
   switch (option) {
     case APIRL_OPT_DUAL_LAYOUT: {
       p->dual_layout = value != 0;
-      if (p->dual_layout && p->is3d && !p->d_xT) {
+      if (p->dual_layout && p->is3d) {
         DEVICE_SCOPE(p->device);
-        const int64_t nv = (int64_t)p->g.nx * p->g.ny * p->g.nz;
-        CK(cudaMalloc(&p->d_xT, nv * sizeof(float)));
-        CK(cudaMalloc(&p->d_bpT, nv * sizeof(float)));
-        CK(cudaMemset(p->d_bpT, 0, nv * sizeof(float)));
+        return alloc_pad(p);
       }
       return APIRL_OK;
     }

@@ -11,4 +11,7 @@ struct ImgGeom {
   float rfov, offz;
 };
 
+// Border width, in voxels, of the padded image layouts of the fused 3D pass.
+constexpr int kPad = 2;
+
 }  // namespace apirl

@@ -61,18 +61,25 @@ cudaError_t launch_count_steps(const ImgGeom& g, const LorTable& t, SubsetSel s,
 
 // Fused EM pass.  partials: >= em_pass_blocks() doubles of scratch.
 int64_t em_pass_blocks(const LorTable& t, SubsetSel s);
+// Padded two-layout buffers of the fused 3D pass: the image as [z][y][x] (pA)
+// and [z][x][y] (pT), and the backprojection likewise (bA, bT), each with a
+// kPad (2) voxel zero border; lim = voxels of one padded buffer.
+struct PadBuffers {
+  float* pA = nullptr;
+  float* pT = nullptr;
+  float* bA = nullptr;
+  float* bT = nullptr;
+  unsigned lim = 0;
+};
 // lik_mode: 0 = over e != 0, 1 = over e > 0, 2 = over ratio > 0.  back = 0: no backprojection.
 cudaError_t launch_em_pass(const ImgGeom& g, const LorTable& t, SubsetSel s, const void* counts, int counts_dtype,
                            int counts_packed, const float* add, const float* x, float* bp, int back, int lik_mode,
                            double* partials, double* lik, cudaStream_t st, const PreciseGeom& pg = PreciseGeom(),
-                           const float* xT = nullptr, float* bpT = nullptr, int block = 0);
-// Transposed-layout helpers for the fused pass (3D): [z][y][x] -> [z][x][y], and
-// the update that merges the two backprojection buffers.
-cudaError_t launch_transpose_xy(int nx, int ny, int nz, const float* in, float* out, cudaStream_t st);
-cudaError_t launch_merge_transposed(int nx, int ny, int nz, float* bpA, float* bpT, cudaStream_t st);
-cudaError_t launch_update_dual(int nx, int ny, int nz, float* x, float* bpA, float* bpT, const float* sens,
-                               const float* thr_ptr, float thr_value, int ge, cudaStream_t st);
-
+                           const PadBuffers& pad = PadBuffers(), int block = 0);
+cudaError_t launch_pad_copy(const ImgGeom& g, const float* x, const PadBuffers& pad, cudaStream_t st);
+// mode 0: EM update of x from bA + bT (threshold rule); mode 1: bp += bA + bT.  Clears bA, bT.
+cudaError_t launch_pad_reduce(const ImgGeom& g, const PadBuffers& pad, int mode, float* x, float* bp,
+                              const float* sens, const float* thr_ptr, float thr_value, int ge, cudaStream_t st);
 cudaError_t launch_inverse_divide(int64_t n, const float* meas, float* est, cudaStream_t st);
 cudaError_t launch_add_bins(int64_t n, const float* add, float* est, cudaStream_t st);
 cudaError_t launch_likelihood(int64_t n, const float* est, const float* meas, int gt0, double* partials,
@@ -152,8 +159,7 @@ struct apirl_projector {
   double2* d_z64 = nullptr;
   apirl::PreciseGeom pg;
   int dual_layout = 1;           // fused 3D pass gathers / scatters x-running rays in a transposed copy
-  float* d_xT = nullptr;         // [z][x][y] copies for the dual layout, allocated on first use
-  float* d_bpT = nullptr;        // kept zero between passes
+  apirl::PadBuffers pad;         // padded two-layout copies of the fused pass (3D), interiors of bA/bT zero
   int timing = 0;                // record CUDA events around the fused kernel
   int em_block = 128;            // threads per block of the fused kernel (APIRL_OPT_EM_BLOCK / autotune)
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;

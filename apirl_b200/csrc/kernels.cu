@@ -24,7 +24,7 @@ namespace {
 constexpr int kBlock = 256;
 // Minimum resident 256-thread blocks per SM for the fused kernel (register cap).
 #ifndef APIRL_EM_MIN_BLOCKS
-#define APIRL_EM_MIN_BLOCKS 5
+#define APIRL_EM_MIN_BLOCKS 4
 #endif
 constexpr int kEmMinBlocks = APIRL_EM_MIN_BLOCKS;
 
@@ -226,16 +226,15 @@ __global__ void __launch_bounds__(kBlock) k_count_steps(ImgGeom g, LorTable t, S
 // Fused EM pass: project, add, likelihood term, ratio, backproject.
 // lik_mode: 0 = term over e != 0 (3D), 1 = over e > 0 (2D), 2 = over the ratio
 // r > 0 (the final 2D value, Mlem2d.cpp:228).  back = 0 skips the backprojection.
-// xT / bpT (both or neither): the image and backprojection stored transposed,
-// [z][x][y].  Rays running mostly along x read and scatter there, so that the
-// 32 near-parallel rays of a warp, which lie side by side along y, touch
-// contiguous addresses; rays mostly along y use the [z][y][x] buffers.
+// pad.pA set (3D): the pass reads the image from the padded two-layout copies
+// and scatters into the padded backprojection pair (see PadBuffers); else it
+// uses x and bp directly.
 template <typename CT, bool IS3D, bool F64A>
 __global__ void __launch_bounds__(kBlock, kEmMinBlocks) k_em_pass(ImgGeom g, LorTable t, SubsetSel s, PreciseGeom pg,
                                                     const CT* __restrict__ counts,
                                                     int counts_packed, const float* __restrict__ add,
                                                     const float* __restrict__ x, float* __restrict__ bp,
-                                                    const float* __restrict__ xT, float* __restrict__ bpT, int back,
+                                                    PadBuffers pad, int back,
                                                     int lik_mode, double* __restrict__ partials, int64_t total) {
   const int64_t b = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   double term = 0.0;
@@ -257,23 +256,33 @@ __global__ void __launch_bounds__(kBlock, kEmMinBlocks) k_em_pass(ImgGeom g, Lor
         siddon3d_walk(w, gd, [&](bool inb, int idx, float seg) {
           if (inb) atomicAdd(bp + idx, A_MUL(seg, r));
         });
-    } else if (IS3D) {
+    } else if (IS3D && pad.pA) {
+      // Two padded layouts: rays running mostly along x use the transposed
+      // copy, so that a warp's neighbouring rays touch contiguous addresses.
       const float2 z = t.z[p.g];
       const float vx = A_SUB(L.z, L.x), vy = A_SUB(L.w, L.y);
-      const bool tr = xT != nullptr && fabsf(vx) >= fabsf(vy);
-      const float* __restrict__ xs = tr ? xT : x;
-      float* __restrict__ bs = tr ? bpT : bp;
-      const int ux = tr ? g.ny : 1, uy = tr ? 1 : g.nx;
+      const bool tr = fabsf(vx) >= fabsf(vy);
+      const int px = g.nx + 2 * kPad, py = g.ny + 2 * kPad;
+      const int uz = px * py;
+      const int ux = tr ? py : 1, uy = tr ? 1 : px;
       Walk3 w;
       siddon3_setup(L.x, L.y, z.x, vx, vy, A_SUB(z.y, z.x), g, w);
-      float e = siddon3_gather2(w, g, ux, uy, xs);
+      float e = siddon3_gather_pad(w, g, ux, uy, uz, pad.lim, tr ? pad.pT : pad.pA);
+      if (add) e = A_ADD(e, __ldg(add + ci));
+      const float r = (m != 0.f && e != 0.f) ? A_DIV(m, e) : 0.f;
+      if (lik_mode == 2) { if (r > 0.f) term = (double)m * log((double)r) - (double)r; }
+      else if (lik_mode == 1 ? (e > 0.f) : (e != 0.f)) term = (double)m * log((double)e) - (double)e;
+      if (back && r != 0.f) siddon3_scatter_pad(w, g, ux, uy, uz, pad.lim, r, tr ? pad.bT : pad.bA);
+    } else if (IS3D) {
+      Walk3 w;
+      float e = ray_sum3(g, L, t.z[p.g], x, w);
       if (add) e = A_ADD(e, __ldg(add + ci));
       const float r = (m != 0.f && e != 0.f) ? A_DIV(m, e) : 0.f;
       if (lik_mode == 2) { if (r > 0.f) term = (double)m * log((double)r) - (double)r; }
       else if (lik_mode == 1 ? (e > 0.f) : (e != 0.f)) term = (double)m * log((double)e) - (double)e;
       if (back && r != 0.f)
-        siddon3_walk_s(w, g, ux, uy, [&](bool inb, int idx, float seg) {
-          if (inb) atomicAdd(bs + idx, A_MUL(seg, r));
+        siddon3_walk(w, g, [&](bool inb, int idx, float seg) {
+          if (inb) atomicAdd(bp + idx, A_MUL(seg, r));
         });
     } else {
       Walk2 w;
@@ -510,77 +519,73 @@ __global__ void __launch_bounds__(kBlock) k_sens_batch(const SensJob* __restrict
   });
 }
 
-// [z][y][x] -> [z][x][y] through 32x32 shared-memory tiles.
-__global__ void __launch_bounds__(256) k_transpose_xy(int nx, int ny, const float* __restrict__ in,
-                                                      float* __restrict__ out) {
+// ---- padded two-layout copies of the fused pass ------------------------------
+// A: [z][y][x] and T: [z][x][y], both with a kPad-voxel border on every side.
+struct PadDims {
+  int nx, ny, nz;
+  __device__ __forceinline__ int64_t a(int x, int y, int z) const {
+    return ((int64_t)(z + kPad) * (ny + 2 * kPad) + (y + kPad)) * (nx + 2 * kPad) + (x + kPad);
+  }
+  __device__ __forceinline__ int64_t t(int x, int y, int z) const {
+    return ((int64_t)(z + kPad) * (nx + 2 * kPad) + (x + kPad)) * (ny + 2 * kPad) + (y + kPad);
+  }
+};
+
+// x ([z][y][x], unpadded) -> interiors of pA and pT (32x32 tiles per slice).
+__global__ void __launch_bounds__(256) k_pad_copy(PadDims d, const float* __restrict__ x, float* __restrict__ pA,
+                                                  float* __restrict__ pT) {
   __shared__ float tile[32][33];
-  const int z = blockIdx.z;
-  const int x0 = blockIdx.x * 32, y0 = blockIdx.y * 32;
-  const int64_t base = (int64_t)z * nx * ny;
+  const int z = blockIdx.z, x0 = blockIdx.x * 32, y0 = blockIdx.y * 32;
+  const int64_t base = (int64_t)z * d.nx * d.ny;
   for (int r = threadIdx.y; r < 32; r += 8) {
-    const int y = y0 + r, x = x0 + threadIdx.x;
-    if (x < nx && y < ny) tile[r][threadIdx.x] = in[base + (int64_t)y * nx + x];
+    const int yy = y0 + r, xx = x0 + threadIdx.x;
+    if (xx < d.nx && yy < d.ny) {
+      const float v = x[base + (int64_t)yy * d.nx + xx];
+      tile[r][threadIdx.x] = v;
+      pA[d.a(xx, yy, z)] = v;
+    }
   }
   __syncthreads();
   for (int r = threadIdx.y; r < 32; r += 8) {
-    const int x = x0 + r, y = y0 + threadIdx.x;
-    if (x < nx && y < ny) out[base + (int64_t)x * ny + y] = tile[threadIdx.x][r];
+    const int xx = x0 + r, yy = y0 + threadIdx.x;
+    if (xx < d.nx && yy < d.ny) pT[d.t(xx, yy, z)] = tile[threadIdx.x][r];
   }
 }
 
-// EM update with the backprojection held in two layouts: bp = bpA + (bpT)^T;
-// x = (sens >= thr | > thr) ? x * bp / sens : 0; both bp buffers cleared.
-__global__ void __launch_bounds__(256) k_update_dual(int nx, int ny, float* __restrict__ x, float* __restrict__ bpA,
-                                                     float* __restrict__ bpT, const float* __restrict__ sens,
-                                                     const float* __restrict__ thr_ptr, float thr_value, int ge) {
+// Sum of the two padded backprojections at every interior voxel, [z][y][x]
+// order, interiors cleared.  mode 0: EM update of x (threshold rule ge/gt);
+// mode 1: bp += sum.
+__global__ void __launch_bounds__(256) k_pad_reduce(PadDims d, float* __restrict__ bA, float* __restrict__ bT,
+                                                    int mode, float* __restrict__ x, float* __restrict__ bp,
+                                                    const float* __restrict__ sens, const float* __restrict__ thr_ptr,
+                                                    float thr_value, int ge) {
   __shared__ float tile[32][33];
-  const float thr = thr_ptr ? *thr_ptr : thr_value;
-  const int z = blockIdx.z;
-  const int x0 = blockIdx.x * 32, y0 = blockIdx.y * 32;
-  const int64_t base = (int64_t)z * nx * ny;
-  for (int r = threadIdx.y; r < 32; r += 8) {  // read the transposed tile along y
+  const int z = blockIdx.z, x0 = blockIdx.x * 32, y0 = blockIdx.y * 32;
+  const int64_t base = (int64_t)z * d.nx * d.ny;
+  for (int r = threadIdx.y; r < 32; r += 8) {  // transposed buffer, read along y
     const int xx = x0 + r, yy = y0 + threadIdx.x;
-    if (xx < nx && yy < ny) {
-      const int64_t i = base + (int64_t)xx * ny + yy;
-      tile[threadIdx.x][r] = bpT[i];
-      bpT[i] = 0.f;
+    if (xx < d.nx && yy < d.ny) {
+      const int64_t i = d.t(xx, yy, z);
+      tile[threadIdx.x][r] = bT[i];
+      bT[i] = 0.f;
     }
   }
   __syncthreads();
+  const float thr = (mode == 0 && thr_ptr) ? *thr_ptr : thr_value;
   for (int r = threadIdx.y; r < 32; r += 8) {
     const int yy = y0 + r, xx = x0 + threadIdx.x;
-    if (xx < nx && yy < ny) {
-      const int64_t i = base + (int64_t)yy * nx + xx;
-      const float b = A_ADD(bpA[i], tile[r][threadIdx.x]);
-      const float sv = sens[i];
-      const bool okv = ge ? (sv >= thr) : (sv > thr);
-      x[i] = okv ? A_DIV(A_MUL(x[i], b), sv) : 0.f;
-      bpA[i] = 0.f;
-    }
-  }
-}
-
-// bpA += (bpT)^T, bpT cleared.
-__global__ void __launch_bounds__(256) k_merge_transposed(int nx, int ny, float* __restrict__ bpA,
-                                                          float* __restrict__ bpT) {
-  __shared__ float tile[32][33];
-  const int z = blockIdx.z;
-  const int x0 = blockIdx.x * 32, y0 = blockIdx.y * 32;
-  const int64_t base = (int64_t)z * nx * ny;
-  for (int r = threadIdx.y; r < 32; r += 8) {
-    const int xx = x0 + r, yy = y0 + threadIdx.x;
-    if (xx < nx && yy < ny) {
-      const int64_t i = base + (int64_t)xx * ny + yy;
-      tile[threadIdx.x][r] = bpT[i];
-      bpT[i] = 0.f;
-    }
-  }
-  __syncthreads();
-  for (int r = threadIdx.y; r < 32; r += 8) {
-    const int yy = y0 + r, xx = x0 + threadIdx.x;
-    if (xx < nx && yy < ny) {
-      const int64_t i = base + (int64_t)yy * nx + xx;
-      bpA[i] = A_ADD(bpA[i], tile[r][threadIdx.x]);
+    if (xx < d.nx && yy < d.ny) {
+      const int64_t ia = d.a(xx, yy, z);
+      const float b = A_ADD(bA[ia], tile[r][threadIdx.x]);
+      bA[ia] = 0.f;
+      const int64_t i = base + (int64_t)yy * d.nx + xx;
+      if (mode == 0) {
+        const float sv = sens[i];
+        const bool okv = ge ? (sv >= thr) : (sv > thr);
+        x[i] = okv ? A_DIV(A_MUL(x[i], b), sv) : 0.f;
+      } else {
+        bp[i] = A_ADD(bp[i], b);
+      }
     }
   }
 }
@@ -631,8 +636,8 @@ cudaError_t launch_count_steps(const ImgGeom& g, const LorTable& t, SubsetSel s,
 
 cudaError_t launch_em_pass(const ImgGeom& g, const LorTable& t, SubsetSel s, const void* counts, int counts_dtype,
                            int counts_packed, const float* add, const float* x, float* bp, int back, int lik_mode,
-                           double* partials, double* lik, cudaStream_t st, const PreciseGeom& pg, const float* xT,
-                           float* bpT, int block) {
+                           double* partials, double* lik, cudaStream_t st, const PreciseGeom& pg,
+                           const PadBuffers& pad, int block) {
   const int64_t total = (int64_t)t.n_sinos * s.nk * t.n_r;
   if (block < 32 || block > kBlock || block % 32) block = kBlock;
   const unsigned grid = (unsigned)((total + block - 1) / block);
@@ -641,13 +646,13 @@ cudaError_t launch_em_pass(const ImgGeom& g, const LorTable& t, SubsetSel s, con
   do {                                                                                                        \
     if (t.is3d && pg.enabled)                                                                                 \
       k_em_pass<CT, true, true><<<grid, block, 0, st>>>(g, t, s, pg, (const CT*)counts, counts_packed, add, x, \
-                                                         bp, nullptr, nullptr, back, lik_mode, partials, total); \
+                                                         bp, PadBuffers(), back, lik_mode, partials, total);   \
     else if (t.is3d)                                                                                          \
       k_em_pass<CT, true, false><<<grid, block, 0, st>>>(g, t, s, pg, (const CT*)counts, counts_packed, add,   \
-                                                          x, bp, xT, bpT, back, lik_mode, partials, total);   \
+                                                          x, bp, pad, back, lik_mode, partials, total);       \
     else                                                                                                      \
       k_em_pass<CT, false, false><<<grid, block, 0, st>>>(g, t, s, pg, (const CT*)counts, counts_packed, add,  \
-                                                           x, bp, nullptr, nullptr, back, lik_mode, partials, \
+                                                           x, bp, PadBuffers(), back, lik_mode, partials,     \
                                                            total);                                            \
   } while (0)
   static bool carveout_set = false;  // prefer L1 over shared memory: the kernel uses none
@@ -715,22 +720,18 @@ cudaError_t launch_force_positive(int64_t n, float* x, cudaStream_t st) {
   return cudaGetLastError();
 }
 
-cudaError_t launch_transpose_xy(int nx, int ny, int nz, const float* in, float* out, cudaStream_t st) {
-  dim3 grid((nx + 31) / 32, (ny + 31) / 32, nz), block(32, 8);
-  k_transpose_xy<<<grid, block, 0, st>>>(nx, ny, in, out);
+cudaError_t launch_pad_copy(const ImgGeom& g, const float* x, const PadBuffers& pad, cudaStream_t st) {
+  dim3 grid((g.nx + 31) / 32, (g.ny + 31) / 32, g.nz), block(32, 8);
+  PadDims d{g.nx, g.ny, g.nz};
+  k_pad_copy<<<grid, block, 0, st>>>(d, x, pad.pA, pad.pT);
   return cudaGetLastError();
 }
 
-cudaError_t launch_update_dual(int nx, int ny, int nz, float* x, float* bpA, float* bpT, const float* sens,
-                               const float* thr_ptr, float thr_value, int ge, cudaStream_t st) {
-  dim3 grid((nx + 31) / 32, (ny + 31) / 32, nz), block(32, 8);
-  k_update_dual<<<grid, block, 0, st>>>(nx, ny, x, bpA, bpT, sens, thr_ptr, thr_value, ge);
-  return cudaGetLastError();
-}
-
-cudaError_t launch_merge_transposed(int nx, int ny, int nz, float* bpA, float* bpT, cudaStream_t st) {
-  dim3 grid((nx + 31) / 32, (ny + 31) / 32, nz), block(32, 8);
-  k_merge_transposed<<<grid, block, 0, st>>>(nx, ny, bpA, bpT);
+cudaError_t launch_pad_reduce(const ImgGeom& g, const PadBuffers& pad, int mode, float* x, float* bp,
+                              const float* sens, const float* thr_ptr, float thr_value, int ge, cudaStream_t st) {
+  dim3 grid((g.nx + 31) / 32, (g.ny + 31) / 32, g.nz), block(32, 8);
+  PadDims d{g.nx, g.ny, g.nz};
+  k_pad_reduce<<<grid, block, 0, st>>>(d, pad.bA, pad.bT, mode, x, bp, sens, thr_ptr, thr_value, ge);
   return cudaGetLastError();
 }
 

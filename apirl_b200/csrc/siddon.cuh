@@ -29,6 +29,9 @@ __device__ __forceinline__ float fmax_ref(float a, float b) { return (a < b) ? b
 struct Walk3 {
   float ax, ay, az, axu, ayu, azu, ac, L;
   int i, j, k, iinc, jinc, kinc, n;
+  // 1 when the entry and exit voxel indices lie in [-1, n] on every axis
+  // (see siddon3_gather_pad).
+  int guarded;
 };
 
 __device__ __forceinline__ void siddon3_setup(float p0x, float p0y, float p0z, float vx, float vy, float vz,
@@ -56,6 +59,10 @@ __device__ __forceinline__ void siddon3_setup(float p0x, float p0y, float p0z, f
   const int imax = (int)floorf(A_DIV(A_ADD(x2, rFov), g.dx)), jmax = (int)floorf(A_DIV(A_ADD(y2, rFov), g.dy));
   const int kmax = (int)floorf(A_DIV(A_SUB(z2, g.offz), g.dz));
   w.n = abs(imax - imin) + abs(jmax - jmin) + abs(kmax - kmin);
+  // Recorded indices run monotonically from the entry index towards the exit
+  // index on each axis, so their range is bounded by the two.
+  w.guarded = (min(imin, imax) >= -1) & (max(imin, imax) <= g.nx) & (min(jmin, jmax) >= -1) &
+              (max(jmin, jmax) <= g.ny) & (min(kmin, kmax) >= -1) & (max(kmin, kmax) <= g.nz);
   w.iinc = vx > 0.f ? 1 : (vx < 0.f ? -1 : 0);
   w.jinc = vy > 0.f ? 1 : (vy < 0.f ? -1 : 0);
   w.kinc = vz > 0.f ? 1 : (vz < 0.f ? -1 : 0);
@@ -145,6 +152,103 @@ __device__ __forceinline__ float siddon3_gather2(Walk3 w, const ImgGeom& g, int 
     if (ka) acc = A_ADD(acc, A_MUL(sa, __ldg(img + ia)));
   }
   return acc;
+}
+
+// Walks over an image padded with a kPad-voxel zero border on every side
+// (padded sizes n+2 kPad; unit strides ux, uy, uz of the padded layout; `lim`
+// = number of padded voxels).  When w.guarded the entry and exit indices lie
+// in [-1, n]; recorded indices run between them, and float ties at the exit
+// can add at most one crossing per axis beyond it (the crossing parameters'
+// rounding error is orders below one crossing step), so the walk stays in
+// [-2, n+1], inside the border: a border segment reads a zero (the sum is
+// unchanged; the reference skips it) or scatters into the border, which
+// nothing reads.  The three per-axis bounds tests become one test of the
+// linear index against the padded volume, kept as a memory-safety net.
+// Otherwise the reference's bounds test is applied.
+__device__ __forceinline__ float siddon3_gather_pad(Walk3 w, const ImgGeom& g, int ux, int uy, int uz, unsigned lim,
+                                                    const float* __restrict__ img) {
+  const int sx = w.iinc * ux, sy = w.jinc * uy, sz = w.kinc * uz;
+  int idx = (w.k + kPad) * uz + (w.j + kPad) * uy + (w.i + kPad) * ux;
+  float acc = 0.f;
+  if (w.guarded) {
+    int m = 0;
+    for (; m + 1 < w.n; m += 2) {
+      bool cx = (w.ax <= w.ay) & (w.ax <= w.az);
+      bool cy = !cx & (w.ay <= w.az);
+      float an = cx ? w.ax : (cy ? w.ay : w.az);
+      const float sa = A_MUL(A_SUB(an, w.ac), w.L);
+      const int ia = idx;
+      w.ac = an;
+      if (cx) { idx += sx; w.ax = A_ADD(w.ax, w.axu); }
+      else if (cy) { idx += sy; w.ay = A_ADD(w.ay, w.ayu); }
+      else { idx += sz; w.az = A_ADD(w.az, w.azu); }
+      cx = (w.ax <= w.ay) & (w.ax <= w.az);
+      cy = !cx & (w.ay <= w.az);
+      an = cx ? w.ax : (cy ? w.ay : w.az);
+      const float sb = A_MUL(A_SUB(an, w.ac), w.L);
+      const int ib = idx;
+      w.ac = an;
+      if (cx) { idx += sx; w.ax = A_ADD(w.ax, w.axu); }
+      else if (cy) { idx += sy; w.ay = A_ADD(w.ay, w.ayu); }
+      else { idx += sz; w.az = A_ADD(w.az, w.azu); }
+      const float va = (unsigned)ia < lim ? __ldg(img + ia) : 0.f;
+      const float vb = (unsigned)ib < lim ? __ldg(img + ib) : 0.f;
+      acc = A_ADD(acc, A_MUL(sa, va));
+      acc = A_ADD(acc, A_MUL(sb, vb));
+    }
+    if (m < w.n) {
+      const bool cx = (w.ax <= w.ay) & (w.ax <= w.az);
+      const bool cy = !cx & (w.ay <= w.az);
+      const float an = cx ? w.ax : (cy ? w.ay : w.az);
+      const float v = (unsigned)idx < lim ? __ldg(img + idx) : 0.f;
+      acc = A_ADD(acc, A_MUL(A_MUL(A_SUB(an, w.ac), w.L), v));
+    }
+    return acc;
+  }
+  for (int m = 0; m < w.n; m++) {
+    const bool cx = (w.ax <= w.ay) & (w.ax <= w.az);
+    const bool cy = !cx & (w.ay <= w.az);
+    const float an = cx ? w.ax : (cy ? w.ay : w.az);
+    const float seg = A_MUL(A_SUB(an, w.ac), w.L);
+    if (((unsigned)w.i < (unsigned)g.nx) & ((unsigned)w.j < (unsigned)g.ny) & ((unsigned)w.k < (unsigned)g.nz))
+      acc = A_ADD(acc, A_MUL(seg, __ldg(img + idx)));
+    w.ac = an;
+    if (cx) { w.i += w.iinc; idx += sx; w.ax = A_ADD(w.ax, w.axu); }
+    else if (cy) { w.j += w.jinc; idx += sy; w.ay = A_ADD(w.ay, w.ayu); }
+    else { w.k += w.kinc; idx += sz; w.az = A_ADD(w.az, w.azu); }
+  }
+  return acc;
+}
+
+__device__ __forceinline__ void siddon3_scatter_pad(Walk3 w, const ImgGeom& g, int ux, int uy, int uz, unsigned lim,
+                                                    float r, float* __restrict__ img) {
+  const int sx = w.iinc * ux, sy = w.jinc * uy, sz = w.kinc * uz;
+  int idx = (w.k + kPad) * uz + (w.j + kPad) * uy + (w.i + kPad) * ux;
+  if (w.guarded) {
+    for (int m = 0; m < w.n; m++) {
+      const bool cx = (w.ax <= w.ay) & (w.ax <= w.az);
+      const bool cy = !cx & (w.ay <= w.az);
+      const float an = cx ? w.ax : (cy ? w.ay : w.az);
+      if ((unsigned)idx < lim) atomicAdd(img + idx, A_MUL(A_MUL(A_SUB(an, w.ac), w.L), r));
+      w.ac = an;
+      if (cx) { idx += sx; w.ax = A_ADD(w.ax, w.axu); }
+      else if (cy) { idx += sy; w.ay = A_ADD(w.ay, w.ayu); }
+      else { idx += sz; w.az = A_ADD(w.az, w.azu); }
+    }
+    return;
+  }
+  for (int m = 0; m < w.n; m++) {
+    const bool cx = (w.ax <= w.ay) & (w.ax <= w.az);
+    const bool cy = !cx & (w.ay <= w.az);
+    const float an = cx ? w.ax : (cy ? w.ay : w.az);
+    const float seg = A_MUL(A_SUB(an, w.ac), w.L);
+    if (((unsigned)w.i < (unsigned)g.nx) & ((unsigned)w.j < (unsigned)g.ny) & ((unsigned)w.k < (unsigned)g.nz))
+      atomicAdd(img + idx, A_MUL(seg, r));
+    w.ac = an;
+    if (cx) { w.i += w.iinc; idx += sx; w.ax = A_ADD(w.ax, w.axu); }
+    else if (cy) { w.j += w.jinc; idx += sy; w.ay = A_ADD(w.ay, w.ayu); }
+    else { w.k += w.kinc; idx += sz; w.az = A_ADD(w.az, w.azu); }
+  }
 }
 
 template <class V>

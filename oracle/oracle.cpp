@@ -19,6 +19,10 @@
 //   2D DivideAndBackproject ... recon/src/SiddonProjector.cpp:90-144
 //   3D Project / Backproject .. recon/src/SiddonProjector.cpp:322-441 / 444-568
 //   3D DivideAndBackproject ... recon/src/SiddonProjector.cpp:571-704
+//   sampled LORs (numSamplesOnDetector, numAxialSamplesOnDetector,
+//   useMultipleLorsPerBin) ..... recon/src/SiddonProjector.cpp:346-397, 466-510,
+//                               626-652; data/src/Sinogram2DinCylindrical3Dpet.cpp:283-299,
+//                               data/src/Sinogram2D.cpp:172-187 (getDeltaR)
 //   LOR end points ............ data/src/Sinogram2DinCylindrical3Dpet.cpp:216-266
 //   r / angle tables .......... data/src/Sinogram2DinCylindrical3Dpet.cpp:46-63
 //   ring z, ring pairs ........ data/src/Sinogram3D.cpp:358-464
@@ -216,6 +220,7 @@ template <typename T> struct Sino3DG {
   T rFov, axialFov, rScanner;
   std::vector<T> r, ang;
   std::vector<T> z1, z2;  // averaged end-point z per sinogram, before the ring-width shift
+  std::vector<std::vector<T>> zl1, zl2;  // z of every ring pair of each sinogram (getAxialValue{1,2}FromList)
   T ringWidth;
 };
 
@@ -244,6 +249,8 @@ Sino3DG<T> make_sino3d(int nProj, int nR, int nRings, float rFov, float axialFov
       if (!l1.empty()) {
         s.z1.push_back((l1.front() + l1.back()) / 2);
         s.z2.push_back((l2.front() + l2.back()) / 2);
+        s.zl1.push_back(l1);
+        s.zl2.push_back(l2);
       }
     }
   }
@@ -267,14 +274,71 @@ template <typename T> inline void sino_z(const Sino3DG<T>& s, int g, T& za, T& z
   zb = s.z2[g] - rw / 2 + dz / 2 + (T)0 * dz;
 }
 
+// Rays per bin of the 3D projectors.  ns = numSamplesOnDetector, nas =
+// numAxialSamplesOnDetector (SiddonProjector(int, int), SiddonProjector.cpp:28-32),
+// multi = useMultipleLorsPerBin (Projector.h:54-60).
+struct Sampling {
+  int ns = 1, nas = 1, multi = 0;
+};
+
+// Sinogram2D::getDeltaR (data/src/Sinogram2D.cpp:172-187).
+template <typename T> inline T delta_r(const Sino3DG<T>& s, int l) {
+  if (l > 0 && l < s.nR - 1) return (s.r[l + 1] - s.r[l - 1]) / 2;
+  if (l == 0) return s.r[1] - s.r[0];
+  return s.r[s.nR - 1] - s.r[s.nR - 2];
+}
+
+// Calls f(L, za, zb) for every ray of bin (sinogram g, angle a, r l), in the
+// reference's loop order: ring pair m, radial sample o, axial sample p
+// (SiddonProjector.cpp:346-397).  `dab` selects DivideAndBackproject's rule for
+// when the oversampled end points are used ((ns == 1 && nas == 1) fails,
+// :628); Project and Backproject use them when ns != 1 (:374, :486).
+// Without useMultipleLorsPerBin the end-point z is overwritten by the mean
+// ring-pair z shifted to axial sample p (:390-396).
+template <typename T, typename F>
+void for_rays(const Sino3DG<T>& s, int g, int a, int l, const Sampling& sm, bool dab, F&& f) {
+  const int numZ = sm.multi ? (int)s.zl1[g].size() : 1;
+  const T rw = s.ringWidth;
+  const T dzo = rw / (T)sm.nas;
+  const bool over = dab ? !(sm.ns == 1 && sm.nas == 1) : (sm.ns != 1);
+  for (int m = 0; m < numZ; m++)
+    for (int o = 0; o < sm.ns; o++)
+      for (int p = 0; p < sm.nas; p++) {
+        Lor<T> L;
+        T za, zb;
+        if (!over) {
+          // getPointsFromLor (Sinogram2DinCylindrical3Dpet.cpp:216-229)
+          L = lor_points<T>(s.r[l], s.ang[a], s.rScanner);
+          za = s.zl1[g][m];
+          zb = s.zl2[g][m];
+        } else {
+          // getPointsFromOverSampledLor (:283-299)
+          const T inc = delta_r(s, l);
+          const T dZ = rw / (T)sm.nas;
+          const T r = s.r[l] - (inc / 2) + inc / (T)sm.ns * (T)o + (inc / (T)(2 * sm.ns));
+          L = lor_points<T>(r, s.ang[a], s.rScanner);
+          za = s.zl1[g][m] - rw / 2 + dZ / 2 + (T)p * dZ;
+          zb = s.zl2[g][m] - rw / 2 + dZ / 2 + (T)p * dZ;
+        }
+        if (!sm.multi) {
+          za = s.z1[g] - rw / 2 + dzo / 2 + (T)p * dzo;
+          zb = s.z2[g] - rw / 2 + dzo / 2 + (T)p * dzo;
+        }
+        f(L, za, zb);
+      }
+}
+
 inline bool inb(const int i, const int j, const int k, int nx, int ny, int nz) {
   return i >= 0 && j >= 0 && k >= 0 && i < nx && j < ny && k < nz;
 }
 
 // ---------------------------------------------------------------------------
 // 3D projector.  Bins are laid out [sinogram][subset angle][r].
+// Each bin accumulates the gathers of all its rays into one sum, in ray order
+// (incrementSinogramBin on a zero-filled bin, SiddonProjector.cpp:339,419-420).
 template <typename T>
-void project3d(const Sino3DG<T>& s, int subset, int nsub, const ImgG<T>& g, const T* img, T* out, int threads) {
+void project3d(const Sino3DG<T>& s, int subset, int nsub, const ImgG<T>& g, const T* img, T* out, int threads,
+               const Sampling& sm = Sampling()) {
   const int nk = subset_nproj(s.nProj, subset, nsub);
   const long per = (long)nk * s.nR;
   const long total = per * s.nSinos;
@@ -283,11 +347,11 @@ void project3d(const Sino3DG<T>& s, int subset, int nsub, const ImgG<T>& g, cons
     int gsino = (int)(b / per);
     int k = (int)((b % per) / s.nR), l = (int)(b % s.nR);
     int a = subset_angle(k, subset, nsub);
-    Lor<T> L = lor_points<T>(s.r[l], s.ang[a], s.rScanner);
-    T za, zb; sino_z(s, gsino, za, zb);
     T acc = 0;
-    siddon3d<T>(L.p1x, L.p1y, za, L.p2x - L.p1x, L.p2y - L.p1y, zb - za, g, [&](int i, int j, int kk, T w) {
-      if (inb(i, j, kk, g.nx, g.ny, g.nz)) acc += w * (T)1 * img[((long)kk * g.ny + j) * g.nx + i];
+    for_rays(s, gsino, a, l, sm, false, [&](const Lor<T>& L, T za, T zb) {
+      siddon3d<T>(L.p1x, L.p1y, za, L.p2x - L.p1x, L.p2y - L.p1y, zb - za, g, [&](int i, int j, int kk, T w) {
+        if (inb(i, j, kk, g.nx, g.ny, g.nz)) acc += w * (T)1 * img[((long)kk * g.ny + j) * g.nx + i];
+      });
     });
     out[b] = acc;
   }
@@ -297,7 +361,7 @@ void project3d(const Sino3DG<T>& s, int subset, int nsub, const ImgG<T>& g, cons
 // mode 1: DivideAndBackproject (in != 0: est != 0 ? w*in/est : w*in)
 template <typename T>
 void backproject3d(const Sino3DG<T>& s, int subset, int nsub, const ImgG<T>& g, const T* vin, const T* vest,
-                   T* img, int threads, int mode) {
+                   T* img, int threads, int mode, const Sampling& sm = Sampling()) {
   const int nk = subset_nproj(s.nProj, subset, nsub);
   const long per = (long)nk * s.nR;
   const long total = per * s.nSinos;
@@ -317,14 +381,14 @@ void backproject3d(const Sino3DG<T>& s, int subset, int nsub, const ImgG<T>& g, 
       int gsino = (int)(b / per);
       int k = (int)((b % per) / s.nR), l = (int)(b % s.nR);
       int a = subset_angle(k, subset, nsub);
-      Lor<T> L = lor_points<T>(s.r[l], s.ang[a], s.rScanner);
-      T za, zb; sino_z(s, gsino, za, zb);
-      siddon3d<T>(L.p1x, L.p1y, za, L.p2x - L.p1x, L.p2y - L.p1y, zb - za, g, [&](int i, int j, int kk, T w) {
-        if (!inb(i, j, kk, g.nx, g.ny, g.nz)) return;
-        T v;
-        if (mode == 0) v = w * (T)1 * m;
-        else v = est != 0 ? w * (T)1 * m / est : w * (T)1 * m;
-        dst[((long)kk * g.ny + j) * g.nx + i] += v;
+      for_rays(s, gsino, a, l, sm, mode == 1, [&](const Lor<T>& L, T za, T zb) {
+        siddon3d<T>(L.p1x, L.p1y, za, L.p2x - L.p1x, L.p2y - L.p1y, zb - za, g, [&](int i, int j, int kk, T w) {
+          if (!inb(i, j, kk, g.nx, g.ny, g.nz)) return;
+          T v;
+          if (mode == 0) v = w * (T)1 * m;
+          else v = est != 0 ? w * (T)1 * m / est : w * (T)1 * m;
+          dst[((long)kk * g.ny + j) * g.nx + i] += v;
+        });
       });
     }
   }
@@ -646,6 +710,25 @@ int or_sino3d_z_f64(const or_sino3d* d, double* z1, double* z2) {
 
 OR_FWD3(f32, float)
 OR_FWD3(f64, double)
+
+// Sampled-LOR projectors: ns radial and nas axial samples per bin, multi =
+// one ray per ring pair of the bin (useMultipleLorsPerBin).  mode 0 =
+// Project, 1 = Backproject, 2 = DivideAndBackproject (vest used).
+#define OR_SAMPLED3(SUF, T)                                                                                  \
+  int or_sampled_3d_##SUF(const or_sino3d* d, int ns, int nas, int multi, int mode, int subset, int nsub,   \
+                          int nx, int ny, int nz, float dx, float dy, float dz, const T* in, const T* vest, \
+                          T* out, int threads) {                                                            \
+    if (ns < 1 || nas < 1 || d->nR < 2) return -1;                                                           \
+    Sino3DG<T> s = mk<T>(d);                                                                                 \
+    Sampling sm;                                                                                             \
+    sm.ns = ns; sm.nas = nas; sm.multi = multi != 0;                                                         \
+    ImgG<T> g = make_img<T>(nx, ny, nz, dx, dy, dz);                                                         \
+    if (mode == 0) project3d<T>(s, subset, nsub, g, in, out, threads, sm);                                   \
+    else backproject3d<T>(s, subset, nsub, g, in, mode == 2 ? vest : nullptr, out, threads, mode == 2 ? 1 : 0, sm); \
+    return 0;                                                                                                \
+  }
+OR_SAMPLED3(f32, float)
+OR_SAMPLED3(f64, double)
 
 // Number of recorded Siddon segments per bin of a 3D subset (the step count
 // used for the Gsteps/s figure).

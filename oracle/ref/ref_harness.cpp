@@ -154,6 +154,102 @@ class MaskedSiddonProjector : public Projector {
   bool DivideAndBackproject(Sinogram3D* a, Sinogram3D* b, Image* out) { return ref->DivideAndBackproject(a, b, out); }
 };
 
+// The 3D loops of SiddonProjector::Project and ::DivideAndBackproject with
+// several rays per bin (recon/src/SiddonProjector.cpp:322-441, :571-704):
+// the reference's own getPointsFromLor / getPointsFromOverSampledLor and
+// Siddon(), the loop order and the ray-selection rules unchanged, and a full
+// bounds mask on the voxel index (the reference checks only the upper bounds
+// at :417 and :666).
+struct SampledMasked {
+  int ns, nas, multi;
+
+  // Calls f(LOR) for every ray of bin (k, l) of sinogram s2.
+  template <class F>
+  void rays(Sinogram3D* sino, Sinogram2DinCylindrical3Dpet* s2, int k, int l, bool dab, F&& f) const {
+    float ringWidth_mm = sino->getAxialFoV_mm() / sino->getNumRings();
+    float deltaZ_oversampling = ringWidth_mm / nas;
+    int numZ = multi ? s2->getNumZ() : 1;
+    float z1_mm = 0, z2_mm = 0;
+    if (!multi) {
+      z1_mm = (s2->getAxialValue1FromList(0) + s2->getAxialValue1FromList(s2->getNumZ() - 1)) / 2;
+      z2_mm = (s2->getAxialValue2FromList(0) + s2->getAxialValue2FromList(s2->getNumZ() - 1)) / 2;
+    }
+    const bool plain = dab ? (ns == 1 && nas == 1) : (ns == 1);
+    for (int m = 0; m < numZ; m++)
+      for (int o = 0; o < ns; o++)
+        for (int p = 0; p < nas; p++) {
+          Point3D P1, P2; float geom; int ok;
+          if (plain) ok = s2->getPointsFromLor(k, l, m, &P1, &P2, &geom);
+          else ok = s2->getPointsFromOverSampledLor(k, l, o, ns, m, ringWidth_mm, p, nas, &P1, &P2, &geom);
+          if (!multi) {
+            P1.Z = z1_mm - ringWidth_mm / 2 + deltaZ_oversampling / 2 + p * deltaZ_oversampling;
+            P2.Z = z2_mm - ringWidth_mm / 2 + deltaZ_oversampling / 2 + p * deltaZ_oversampling;
+          }
+          if (!ok) continue;
+          Line3D LOR;
+          LOR.P0 = P1; LOR.Vx = P2.X - P1.X; LOR.Vy = P2.Y - P1.Y; LOR.Vz = P2.Z - P1.Z;
+          f(LOR, geom);
+        }
+  }
+
+  void project(Image* im, Sinogram3D* out) const {
+    SizeImage sz = im->getSize();
+    float* px = im->getPixelsPtr();
+    out->FillConstant(0.0);
+    for (int i = 0; i < out->getNumSegments(); i++)
+      for (int j = 0; j < out->getSegment(i)->getNumSinograms(); j++) {
+        Sinogram2DinCylindrical3Dpet* s2 = out->getSegment(i)->getSinogram2D(j);
+        #pragma omp parallel for schedule(dynamic, 1)
+        for (int k = 0; k < s2->getNumProj(); k++)
+          for (int l = 0; l < s2->getNumR(); l++)
+            rays(out, s2, k, l, false, [&](Line3D& LOR, float geom) {
+              SiddonSegment* w = NULL; int n = 0;
+              Siddon(LOR, im, &w, &n, 1);
+              if (n <= 0) return;
+              for (int q = 0; q < n; q++)
+                if (w[q].IndexX >= 0 && w[q].IndexY >= 0 && w[q].IndexZ >= 0 && w[q].IndexX < sz.nPixelsX &&
+                    w[q].IndexY < sz.nPixelsY && w[q].IndexZ < sz.nPixelsZ)
+                  s2->incrementSinogramBin(k, l, w[q].Segment * geom *
+                      px[w[q].IndexZ * (sz.nPixelsX * sz.nPixelsY) + w[q].IndexY * sz.nPixelsX + w[q].IndexX]);
+              free(w);
+            });
+      }
+  }
+
+  void divide_and_backproject(Sinogram3D* in, Sinogram3D* est, Image* im) const {
+    SizeImage sz = im->getSize();
+    float* px = im->getPixelsPtr();
+    for (int i = 0; i < in->getNumSegments(); i++) {
+      #pragma omp parallel for schedule(dynamic, 1)
+      for (int j = 0; j < in->getSegment(i)->getNumSinograms(); j++) {
+        Sinogram2DinCylindrical3Dpet* s2 = in->getSegment(i)->getSinogram2D(j);
+        Sinogram2D* e2 = est->getSegment(i)->getSinogram2D(j);
+        for (int k = 0; k < s2->getNumProj(); k++)
+          for (int l = 0; l < s2->getNumR(); l++) {
+            const float m = s2->getSinogramBin(k, l), e = e2->getSinogramBin(k, l);
+            if (m == 0) continue;
+            rays(in, s2, k, l, true, [&](Line3D& LOR, float geom) {
+              SiddonSegment* w = NULL; int n = 0;
+              Siddon(LOR, im, &w, &n, 1);
+              for (int q = 0; q < n; q++) {
+                if (!(w[q].IndexX >= 0 && w[q].IndexY >= 0 && w[q].IndexZ >= 0 && w[q].IndexX < sz.nPixelsX &&
+                      w[q].IndexY < sz.nPixelsY && w[q].IndexZ < sz.nPixelsZ))
+                  continue;
+                float v;
+                if (e != 0) v = w[q].Segment * geom * m / e;
+                else if (m != 0) v = w[q].Segment * geom * m;
+                else v = 0;
+                #pragma omp atomic
+                px[w[q].IndexZ * (sz.nPixelsX * sz.nPixelsY) + w[q].IndexY * sz.nPixelsX + w[q].IndexX] += v;
+              }
+              if (n != 0) free(w);
+            });
+          }
+      }
+    }
+  }
+};
+
 std::string write_sino3d_header(const char* dir, int nProj, int nR, int nRings, int nSeg,
                                 const int* nSinos, const int* minRD, const int* maxRD,
                                 const float* data) {
@@ -408,6 +504,41 @@ int ref_backproject_3d(void* hv, int subset, int nsubsets, int nx, int ny, int n
   SiddonProjector sp(1, 1);
   sp.Backproject(s, im);
   memcpy(img_inout, im->getPixelsPtr(), sizeof(float) * (size_t)nx * ny * nz);
+  delete im;
+  return 0;
+}
+
+// Several rays per bin: ns radial and nas axial samples (SiddonProjector(ns,
+// nas)), multi = setMultipleLorsPerBin(true).  mode 0: masked Project into
+// `out` (subset sinogram layout); 1: the reference's own
+// SiddonProjector::Backproject of `in`, accumulated into `out` (image);
+// 2: masked DivideAndBackproject of in / vest, accumulated into `out`.
+int ref_sampled_3d(void* hv, int ns, int nas, int multi, int mode, int subset, int nsubsets, int nx, int ny, int nz,
+                   float dx, float dy, float dz, const float* in, const float* vest, float* out) {
+  Sinogram3DCylindricalPet* full = ((Sino3DHandle*)hv)->sino;
+  Sinogram3D* s = subset >= 0 ? full->getSubset(subset, nsubsets) : full->getSubset(0, 1);
+  SampledMasked sm{ns, nas, multi};
+  if (mode == 0) {
+    Image* im = make_image(nx, ny, nz, dx, dy, dz, in);
+    sm.project(im, s);
+    copy_out(s, out);
+    delete im;
+    return 0;
+  }
+  copy_in(s, in);
+  Image* im = make_image(nx, ny, nz, dx, dy, dz, out);
+  if (mode == 1) {
+    SiddonProjector sp(ns, nas);
+    // SiddonProjector derives privately from Projector (SiddonProjector.h:25);
+    // the reference's callers reach the base with a C-style cast too.
+    ((Projector*)&sp)->setMultipleLorsPerBin(multi != 0);
+    sp.Backproject(s, im);
+  } else {
+    Sinogram3D* e = subset >= 0 ? full->getSubset(subset, nsubsets) : full->getSubset(0, 1);
+    copy_in(e, vest);
+    sm.divide_and_backproject(s, e, im);
+  }
+  memcpy(out, im->getPixelsPtr(), sizeof(float) * (size_t)nx * ny * nz);
   delete im;
   return 0;
 }
