@@ -23,6 +23,7 @@ APIRL_OPT_EM_BLOCK = 3
 
 APIRL_ALPHA_F32 = 0
 APIRL_ALPHA_F64 = 1
+APIRL_MAX_SAMPLES = 64
 
 APIRL_F32 = 0
 APIRL_U32 = 1
@@ -47,6 +48,11 @@ class Sino3DGeomC(ctypes.Structure):
     _fields_ = [("n_proj", _i), ("n_r", _i), ("n_rings", _i), ("n_segments", _i),
                 ("r_fov", _f), ("axial_fov", _f), ("r_scanner", _f),
                 ("min_ring_diff", ctypes.POINTER(_i)), ("max_ring_diff", ctypes.POINTER(_i))]
+
+
+class SamplingC(ctypes.Structure):
+    """apirl_sampling: rays per bin (numSamplesOnDetector, numAxialSamplesOnDetector, useMultipleLorsPerBin)."""
+    _fields_ = [("n_samples", _i), ("n_axial_samples", _i), ("multiple_lors_per_bin", _i)]
 
 
 class JobDescC(ctypes.Structure):
@@ -88,9 +94,10 @@ SIGNATURES = {
     "apirl_em_project_backproject": (_i, [_vp, _vp, _i, _i, _vp, _vp, _vp, _i, _i, _vp, _vp]),
     "apirl_em_pass_host": (_i, [_vp, _vp, _i, _vp, _vp, _vp, _vp, _f, _i, _i, _i, _vp, _vp, _vp]),
     "apirl_osem_3d": (_i, [ctypes.POINTER(ImageGeomC), ctypes.POINTER(Sino3DGeomC), _vp, _vp, _vp, _vp, _i, _i,
-                           _i, _vp, _vp, _vp]),
+                           _i, _vp, _vp, _vp, ctypes.POINTER(SamplingC)]),
     "apirl_mlem_3d": (_i, [ctypes.POINTER(ImageGeomC), ctypes.POINTER(Sino3DGeomC), _vp, _vp, _vp, _vp, _i, _i,
-                           _vp, _vp, _vp]),
+                           _vp, _vp, _vp, ctypes.POINTER(SamplingC)]),
+    "apirl_projector_set_sampling": (_i, [_vp, _i, _i, _i]),
     "apirl_job_footprint": (_i64, [ctypes.POINTER(JobDescC)]),
     "apirl_batch_create": (_i, [_i, _i64, ctypes.POINTER(_vp)]),
     "apirl_batch_destroy": (None, [_vp]),

@@ -256,6 +256,11 @@ void apirl_projector_destroy(apirl_projector* p) {
   cudaFree(p->d_scalars);
   cudaFree(p->d_lor64);
   cudaFree(p->d_z64);
+  for (int k = 0; k < 2; k++) {
+    cudaFree(p->d_lor_s[k]);
+    cudaFree(p->d_zs[k]);
+    cudaFree(p->d_zoff[k]);
+  }
   cudaFree(p->pad.pA);
   cudaFree(p->pad.pT);
   cudaFree(p->pad.bA);
@@ -285,6 +290,8 @@ apirl_status apirl_projector_set_alpha_precision(apirl_projector* p, int mode) {
   if (mode != APIRL_ALPHA_F32 && mode != APIRL_ALPHA_F64) return fail(APIRL_ERR_INVALID, "unknown alpha mode %d", mode);
   if (mode == APIRL_ALPHA_F64 && !p->is3d)
     return fail(APIRL_ERR_NOT_SUPPORTED, "the FP64-alpha walk is implemented for 3D projectors");
+  if (mode == APIRL_ALPHA_F64 && p->t.lor_s)
+    return fail(APIRL_ERR_NOT_SUPPORTED, "the FP64-alpha walk takes one ray per bin (sampling is set)");
   DEVICE_SCOPE(p->device);
   if (mode == APIRL_ALPHA_F64 && !p->d_lor64) {
     std::vector<double> lor, z;
@@ -303,6 +310,62 @@ apirl_status apirl_projector_set_alpha_precision(apirl_projector* p, int mode) {
   }
   p->alpha_mode = mode;
   p->pg.enabled = mode == APIRL_ALPHA_F64;
+  return APIRL_OK;
+}
+
+apirl_status apirl_projector_set_sampling(apirl_projector* p, int n_samples, int n_axial_samples,
+                                         int multiple_lors_per_bin) {
+  if (!p) return fail(APIRL_ERR_INVALID, "null projector");
+  if (n_samples < 1 || n_axial_samples < 1 || n_samples > APIRL_MAX_SAMPLES || n_axial_samples > APIRL_MAX_SAMPLES)
+    return fail(APIRL_ERR_INVALID, "samples per bin must be 1..%d (got %d radial, %d axial)", APIRL_MAX_SAMPLES,
+                n_samples, n_axial_samples);
+  const bool plain = n_samples == 1 && n_axial_samples == 1 && !multiple_lors_per_bin;
+  if (!p->is3d && !plain)
+    return fail(APIRL_ERR_NOT_SUPPORTED, "2D projectors take one ray per bin (the reference's 2D loops ignore "
+                                         "the sample counts)");
+  if (!plain && p->alpha_mode == APIRL_ALPHA_F64)
+    return fail(APIRL_ERR_NOT_SUPPORTED, "sampling is not combined with the FP64-alpha walk");
+  if (!plain && p->t.n_r < 2 && (n_samples > 1 || n_axial_samples > 1))
+    return fail(APIRL_ERR_INVALID, "oversampling needs at least 2 radial bins (getDeltaR)");
+  DEVICE_SCOPE(p->device);
+  // Drop any previous sampled tables.
+  for (int k = 0; k < 2; k++) {
+    cudaFree(p->d_lor_s[k]);
+    cudaFree(p->d_zs[k]);
+    cudaFree(p->d_zoff[k]);
+    p->d_lor_s[k] = nullptr;
+    p->d_zs[k] = nullptr;
+    p->d_zoff[k] = nullptr;
+  }
+  p->t.lor_s = nullptr; p->t.zs = nullptr; p->t.zoff = nullptr; p->t.n_rs = 1; p->t.n_as = 1;
+  p->t_dab = p->t;
+  p->n_samples = 1; p->n_axial_samples = 1; p->multi_lors = 0;
+  if (plain) return APIRL_OK;
+  LorTable* dst[2] = {&p->t, &p->t_dab};
+  for (int k = 0; k < 2; k++) {
+    apirl::RayTables rt;
+    if (!apirl::build_rays_3d(p->t.n_proj, p->t.n_r, p->n_rings, p->r_fov, p->axial_fov, p->r_scanner,
+                              (int)p->min_rd.size(), p->min_rd.data(), p->max_rd.data(), n_samples, n_axial_samples,
+                              multiple_lors_per_bin != 0, k == 1, rt))
+      return fail(APIRL_ERR_INVALID, "a sampled ray end point is not finite (sample outside the scanner radius)");
+    if ((int)rt.zoff.size() != p->t.n_sinos + 1) return fail(APIRL_ERR_INVALID, "ring-pair table mismatch");
+    CK(cudaMalloc(&p->d_lor_s[k], rt.lor.size() * sizeof(float)));
+    CK(cudaMemcpy(p->d_lor_s[k], rt.lor.data(), rt.lor.size() * sizeof(float), cudaMemcpyHostToDevice));
+    CK(cudaMalloc(&p->d_zs[k], rt.zs.size() * sizeof(float)));
+    CK(cudaMemcpy(p->d_zs[k], rt.zs.data(), rt.zs.size() * sizeof(float), cudaMemcpyHostToDevice));
+    CK(cudaMalloc(&p->d_zoff[k], rt.zoff.size() * sizeof(int)));
+    CK(cudaMemcpy(p->d_zoff[k], rt.zoff.data(), rt.zoff.size() * sizeof(int), cudaMemcpyHostToDevice));
+  }
+  for (int k = 0; k < 2; k++) {
+    dst[k]->lor_s = p->d_lor_s[k];
+    dst[k]->zs = p->d_zs[k];
+    dst[k]->zoff = p->d_zoff[k];
+    dst[k]->n_rs = n_samples;
+    dst[k]->n_as = n_axial_samples;
+  }
+  p->n_samples = n_samples;
+  p->n_axial_samples = n_axial_samples;
+  p->multi_lors = multiple_lors_per_bin != 0;
   return APIRL_OK;
 }
 
@@ -343,8 +406,8 @@ apirl_status apirl_divide_and_backproject(apirl_projector* p, const float* d_mea
   if (st) return st;
   if (!d_image || !d_meas || !d_est) return fail(APIRL_ERR_INVALID, "null image or sinogram");
   DEVICE_SCOPE(p->device);
-  CK(apirl::launch_backproject(p->g, p->t, make_subset(p, subset, nsubsets), d_meas, 0, d_est, 1, d_image,
-                               (cudaStream_t)stream, p->pg));
+  CK(apirl::launch_backproject(p->g, p->t_dab.lor_s ? p->t_dab : p->t, make_subset(p, subset, nsubsets), d_meas, 0,
+                               d_est, 1, d_image, (cudaStream_t)stream, p->pg));
   return APIRL_OK;
 }
 
@@ -418,7 +481,9 @@ apirl_status apirl_force_positive(int64_t n, float* d_x, void* stream) {
 
 namespace {
 
-bool use_dual(const apirl_projector* p) { return p->is3d && p->dual_layout && !p->pg.enabled && p->pad.pA; }
+bool use_dual(const apirl_projector* p) {
+  return p->is3d && p->dual_layout && !p->pg.enabled && p->pad.pA && !p->t.lor_s;
+}
 
 // The fused kernel, bracketed by timing events when enabled.
 apirl_status fused(apirl_projector* p, SubsetSel ss, const void* d_counts, int dtype, int packed, const float* d_add,

@@ -79,11 +79,14 @@ extern "C" {
 
 apirl_status apirl_osem_3d(const apirl_image_geom* img, const apirl_sino3d_geom* sino, const float* h_meas,
                            const float* h_mult, const float* h_add, const float* h_init, int iters, int nsubsets,
-                           int device, float* h_out, double* h_lik, float* h_sens0) {
+                           int device, float* h_out, double* h_lik, float* h_sens0, const apirl_sampling* sampling) {
   if (!h_meas || !h_init || !h_out || iters < 0 || nsubsets <= 0)
     return set_err(APIRL_ERR_INVALID, "apirl_osem_3d arguments", cudaSuccess);
   Res r;
   DS(apirl_projector_create_3d(img, sino, device, &r.p));
+  if (sampling)
+    DS(apirl_projector_set_sampling(r.p, sampling->n_samples, sampling->n_axial_samples,
+                                    sampling->multiple_lors_per_bin));
   int prev = 0;
   cudaGetDevice(&prev);
   DK(cudaSetDevice(device));
@@ -139,10 +142,13 @@ apirl_status apirl_osem_3d(const apirl_image_geom* img, const apirl_sino3d_geom*
 
 apirl_status apirl_mlem_3d(const apirl_image_geom* img, const apirl_sino3d_geom* sino, const float* h_meas,
                            const float* h_mult, const float* h_add, const float* h_init, int iters, int device,
-                           float* h_out, double* h_lik, float* h_sens) {
+                           float* h_out, double* h_lik, float* h_sens, const apirl_sampling* sampling) {
   if (!h_meas || !h_init || !h_out || iters < 0) return set_err(APIRL_ERR_INVALID, "apirl_mlem_3d arguments", cudaSuccess);
   Res r;
   DS(apirl_projector_create_3d(img, sino, device, &r.p));
+  if (sampling)
+    DS(apirl_projector_set_sampling(r.p, sampling->n_samples, sampling->n_axial_samples,
+                                    sampling->multiple_lors_per_bin));
   int prev = 0;
   cudaGetDevice(&prev);
   DK(cudaSetDevice(device));

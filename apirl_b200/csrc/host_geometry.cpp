@@ -110,6 +110,90 @@ bool build_tables_3d(int n_proj, int n_r, int n_rings, float r_fov, float axial_
   return t.n_sinos > 0;
 }
 
+bool build_rays_3d(int n_proj, int n_r, int n_rings, float r_fov, float axial_fov, float r_scanner, int n_seg,
+                   const int* min_rd, const int* max_rd, int ns, int nas, int multi, bool dab, RayTables& t) {
+  std::vector<float> r, ang;
+  r_and_angles(n_proj, n_r, r_fov, r, ang);
+  // End points: getPointsFromLor, or getPointsFromOverSampledLor with the
+  // radial sample o (Sinogram2DinCylindrical3Dpet.cpp:216-229, :283-299) and
+  // getDeltaR (data/src/Sinogram2D.cpp:172-187).
+  const bool over = dab ? !(ns == 1 && nas == 1) : (ns != 1);
+  t.n_rs = ns;
+  t.n_as = nas;
+  t.lor.resize((size_t)n_proj * n_r * ns * 4);
+  bool finite = true;
+  for (int a = 0; a < n_proj; a++) {
+    const float phi = ang[a] * kDegToRad;
+    const float c = std::cos(phi);
+    const float s = std::sin(phi);
+    for (int l = 0; l < n_r; l++) {
+      float inc = 0;
+      if (over) {
+        if (l > 0 && l < n_r - 1) inc = (r[l + 1] - r[l - 1]) / 2;
+        else if (l == 0) inc = r[1] - r[0];
+        else inc = r[n_r - 1] - r[n_r - 2];
+      }
+      for (int o = 0; o < ns; o++) {
+        const float rv = over ? r[l] - (inc / 2) + inc / (float)ns * (float)o + (inc / (float)(2 * ns)) : r[l];
+        const float aux = std::sqrt(r_scanner * r_scanner - rv * rv);
+        float* q = &t.lor[(((size_t)a * n_r + l) * ns + o) * 4];
+        q[0] = rv * c + s * aux;
+        q[1] = rv * s - c * aux;
+        q[2] = rv * c - s * aux;
+        q[3] = rv * s + c * aux;
+        finite = finite && std::isfinite(q[0]) && std::isfinite(q[1]) && std::isfinite(q[2]) && std::isfinite(q[3]);
+      }
+    }
+  }
+  // End-point z per (ring pair m, axial sample q): the pair's ring z, or with
+  // oversampling that z shifted to sample q; without useMultipleLorsPerBin the
+  // mean pair z shifted to sample q (SiddonProjector.cpp:357-360, :390-396).
+  const float zinc = axial_fov / (float)n_rings;
+  std::vector<float> ringz(n_rings);
+  for (int i = 0; i < n_rings; i++) ringz[i] = zinc / 2 + (float)i * zinc;
+  const float rw = axial_fov / (float)n_rings;
+  const float dzo = rw / (float)nas;
+  t.zs.clear();
+  t.zoff.assign(1, 0);
+  for (int sg = 0; sg < n_seg; sg++) {
+    for (int z1 = 0; z1 < 2 * n_rings; z1++) {
+      std::vector<float> l1, l2;
+      int z1a = z1;
+      for (int z2 = 0; z2 < n_rings; z2++) {
+        if ((z1a - z2) <= max_rd[sg] && (z1a - z2) >= min_rd[sg] && z1a >= 0 && z2 >= 0 && z1a < n_rings &&
+            z2 < n_rings) {
+          l1.push_back(ringz[z1a]);
+          l2.push_back(ringz[z2]);
+        }
+        z1a = z1a - 1;
+      }
+      if (l1.empty()) continue;
+      const float m1 = (l1.front() + l1.back()) / 2, m2 = (l2.front() + l2.back()) / 2;
+      const int num_z = multi ? (int)l1.size() : 1;
+      for (int m = 0; m < num_z; m++)
+        for (int q = 0; q < nas; q++) {
+          float za, zb;
+          if (!multi) {
+            za = m1 - rw / 2 + dzo / 2 + (float)q * dzo;
+            zb = m2 - rw / 2 + dzo / 2 + (float)q * dzo;
+          } else if (!over) {
+            za = l1[m];
+            zb = l2[m];
+          } else {
+            const float dz = rw / (float)nas;
+            za = l1[m] - rw / 2 + dz / 2 + (float)q * dz;
+            zb = l2[m] - rw / 2 + dz / 2 + (float)q * dz;
+          }
+          finite = finite && std::isfinite(za) && std::isfinite(zb);
+          t.zs.push_back(za);
+          t.zs.push_back(zb);
+        }
+      t.zoff.push_back((int)(t.zs.size() / 2));
+    }
+  }
+  return finite;
+}
+
 void build_tables_3d_f64(int n_proj, int n_r, int n_rings, float r_fov, float axial_fov, float r_scanner, int n_seg,
                          const int* min_rd, const int* max_rd, std::vector<double>& lor, std::vector<double>& z) {
   const double rf = r_fov, R = r_scanner, afov = axial_fov;

@@ -15,6 +15,21 @@ struct LorTable {
   const uint8_t* ok;    // 2D: [n_r] 1 when r <= sinogram rFov (getPointsFromLor); 3D: unused
   int n_proj, n_r, n_sinos;
   int is3d;
+  // Several rays per bin (3D; set when lor_s is not null): a bin is the sum
+  // over its rays, in the order ring pair m, radial sample o, axial sample q,
+  // with end points lor_s[(a * n_r + l) * n_rs + o] and zs[zoff[g] + m * n_as + q].
+  const float4* lor_s = nullptr;
+  const float2* zs = nullptr;
+  const int* zoff = nullptr;  // [n_sinos + 1]
+  int n_rs = 1, n_as = 1;
+};
+
+// Host tables of the sampled rays of every bin.
+struct RayTables {
+  std::vector<float> lor;  // n_proj * n_r * n_rs * 4
+  std::vector<float> zs;   // 2 per (sinogram, ring pair, axial sample)
+  std::vector<int> zoff;   // n_sinos + 1
+  int n_rs = 1, n_as = 1;
 };
 
 // Double-precision geometry for the FP64-alpha precision mode (3D only).
@@ -45,6 +60,12 @@ void build_tables_3d_f64(int n_proj, int n_r, int n_rings, float r_fov, float ax
 void build_tables_2d(int n_proj, int n_r, float r_fov, float r_scanner, HostTables& t);
 bool build_tables_3d(int n_proj, int n_r, int n_rings, float r_fov, float axial_fov, float r_scanner, int n_seg,
                      const int* min_rd, const int* max_rd, HostTables& t);
+// Rays of every bin for SiddonProjector(ns, nas) with useMultipleLorsPerBin =
+// multi (recon/src/SiddonProjector.cpp:346-397).  dab: DivideAndBackproject's
+// rule for when the oversampled end points are used (:628).  Returns false
+// when a ray end point is not finite (a sample outside the scanner radius).
+bool build_rays_3d(int n_proj, int n_r, int n_rings, float r_fov, float axial_fov, float r_scanner, int n_seg,
+                   const int* min_rd, const int* max_rd, int ns, int nas, int multi, bool dab, RayTables& t);
 ImgGeom make_img_geom(int nx, int ny, int nz, float dx, float dy, float dz);
 
 int subset_nproj(int n_proj, int subset, int nsub);
@@ -167,6 +188,13 @@ struct apirl_projector {
   int n_rings = 0;               // 3D geometry as given, for building the FP64 tables
   float r_fov = 0, axial_fov = 0, r_scanner = 0;
   std::vector<int> min_rd, max_rd;
+  // Sampled rays (apirl_projector_set_sampling): t carries the rays of
+  // Project / Backproject, t_dab those of DivideAndBackproject.
+  int n_samples = 1, n_axial_samples = 1, multi_lors = 0;
+  apirl::LorTable t_dab{};
+  float4* d_lor_s[2] = {nullptr, nullptr};
+  float2* d_zs[2] = {nullptr, nullptr};
+  int* d_zoff[2] = {nullptr, nullptr};
 };
 
 // Records `msg` as the calling thread's last error and returns `code`.

@@ -63,6 +63,49 @@ __device__ __forceinline__ float ray_sum3(const ImgGeom& g, const float4 L, cons
   return acc;
 }
 
+// Calls f(L, z) for every ray of bin p of a sampled table, in the reference's
+// loop order: ring pair, radial sample, axial sample (SiddonProjector.cpp:346-397).
+template <class F>
+__device__ __forceinline__ void for_rays(const LorTable& t, const BinPos& p, F&& f) {
+  const int z0 = __ldg(t.zoff + p.g), nz = __ldg(t.zoff + p.g + 1) - z0;
+  const float4* lr = t.lor_s + ((int64_t)p.a * t.n_r + p.l) * t.n_rs;
+  for (int mz = 0; mz < nz; mz += t.n_as)
+    for (int o = 0; o < t.n_rs; o++) {
+      const float4 L = __ldg(lr + o);
+      for (int q = 0; q < t.n_as; q++) f(L, __ldg(t.zs + z0 + mz + q));
+    }
+}
+
+// Forward projection of one bin over all its rays: one running sum, as the
+// reference increments the zero-filled bin ray after ray (SiddonProjector.cpp:339,419).
+__device__ __forceinline__ float rays_sum3(const ImgGeom& g, const LorTable& t, const BinPos& p,
+                                           const float* __restrict__ img) {
+  float acc = 0.f;
+  for_rays(t, p, [&](const float4 L, const float2 z) {
+    Walk3 w;
+    siddon3_setup(L.x, L.y, z.x, A_SUB(L.z, L.x), A_SUB(L.w, L.y), A_SUB(z.y, z.x), g, w);
+    siddon3_walk(w, g, [&](bool inb, int idx, float seg) {
+      if (inb) acc = A_ADD(acc, A_MUL(seg, __ldg(img + idx)));
+    });
+  });
+  return acc;
+}
+
+// Scatter of v * segment along every ray of bin p (optionally divided by e).
+__device__ __forceinline__ void rays_scatter3(const ImgGeom& g, const LorTable& t, const BinPos& p, float v,
+                                              bool divide, float e, float* __restrict__ img) {
+  for_rays(t, p, [&](const float4 L, const float2 z) {
+    Walk3 w;
+    siddon3_setup(L.x, L.y, z.x, A_SUB(L.z, L.x), A_SUB(L.w, L.y), A_SUB(z.y, z.x), g, w);
+    siddon3_walk(w, g, [&](bool inb, int idx, float seg) {
+      if (!inb) return;
+      float val = A_MUL(seg, v);
+      if (divide) val = A_DIV(val, e);
+      atomicAdd(img + idx, val);
+    });
+  });
+}
+
 __device__ __forceinline__ ImgGeomD geom_d(const PreciseGeom& pg) {
   ImgGeomD g;
   g.nx = pg.nx; g.ny = pg.ny; g.nz = pg.nz;
@@ -117,6 +160,8 @@ __global__ void __launch_bounds__(kBlock) k_project3(ImgGeom g, LorTable t, Subs
   if (F64A) {
     Walk3D w;
     out[b] = ray_sum3d(geom_d(pg), pg.lor[(int64_t)p.a * t.n_r + p.l], pg.z[p.g], img, w);
+  } else if (t.lor_s) {
+    out[b] = rays_sum3(g, t, p, img);
   } else {
     Walk3 w;
     out[b] = ray_sum3(g, t.lor[(int64_t)p.a * t.n_r + p.l], t.z[p.g], img, w);
@@ -156,6 +201,10 @@ __global__ void __launch_bounds__(kBlock) k_backproject3(ImgGeom g, LorTable t, 
   const float v = load_bin(vin, vin_mode, b, p, t);
   if (v == 0.f) return;
   const float e = divide ? vest[b] : 0.f;
+  if (!F64A && t.lor_s) {
+    rays_scatter3(g, t, p, v, divide && e != 0.f, e, img);
+    return;
+  }
   auto scatter = [&](bool inb, int idx, float seg) {
     if (!inb) return;
     float val = A_MUL(seg, v);
@@ -208,6 +257,16 @@ __global__ void __launch_bounds__(kBlock) k_count_steps(ImgGeom g, LorTable t, S
   const int64_t b = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (b >= total) return;
   const BinPos p = decode(b, t, s);
+  if (t.is3d && t.lor_s) {
+    int n = 0;
+    for_rays(t, p, [&](const float4 L, const float2 z) {
+      Walk3 w;
+      siddon3_setup(L.x, L.y, z.x, A_SUB(L.z, L.x), A_SUB(L.w, L.y), A_SUB(z.y, z.x), g, w);
+      n += w.n;
+    });
+    steps[b] = n;
+    return;
+  }
   const float4 L = t.lor[(int64_t)p.a * t.n_r + p.l];
   if (t.is3d) {
     const float2 z = t.z[p.g];
@@ -301,6 +360,34 @@ __global__ void __launch_bounds__(kBlock, kEmMinBlocks) k_em_pass(ImgGeom g, Lor
   }
   // Warp-level partial, no block barrier: warps whose rays are short retire
   // without waiting for the block's longest ray.
+  #pragma unroll
+  for (int o = 16; o > 0; o >>= 1) term += __shfl_down_sync(0xffffffffu, term, o);
+  if ((threadIdx.x & 31) == 0) partials[((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5] = term;
+}
+
+// The fused pass for sampled tables (several rays per bin, 3D): the bin's
+// estimate is the running sum over its rays, the ratio is scattered along
+// every ray.  Single [z][y][x] layout, bounds-tested walks.
+template <typename CT>
+__global__ void __launch_bounds__(kBlock) k_em_pass_rays(ImgGeom g, LorTable t, SubsetSel s,
+                                                         const CT* __restrict__ counts, int counts_packed,
+                                                         const float* __restrict__ add, const float* __restrict__ x,
+                                                         float* __restrict__ bp, int back, int lik_mode,
+                                                         double* __restrict__ partials, int64_t total) {
+  const int64_t b = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  double term = 0.0;
+  if (b < total) {
+    const BinPos p = decode(b, t, s);
+    const int64_t row = counts_packed ? ((int64_t)p.g * s.nk + p.k) : ((int64_t)p.g * t.n_proj + p.a);
+    const int64_t ci = row * t.n_r + p.l;
+    const float m = load_count<CT>(counts, ci);
+    float e = rays_sum3(g, t, p, x);
+    if (add) e = A_ADD(e, __ldg(add + ci));
+    const float r = (m != 0.f && e != 0.f) ? A_DIV(m, e) : 0.f;
+    if (lik_mode == 2) { if (r > 0.f) term = (double)m * log((double)r) - (double)r; }
+    else if (lik_mode == 1 ? (e > 0.f) : (e != 0.f)) term = (double)m * log((double)e) - (double)e;
+    if (back && r != 0.f) rays_scatter3(g, t, p, r, false, 0.f, bp);
+  }
   #pragma unroll
   for (int o = 16; o > 0; o >>= 1) term += __shfl_down_sync(0xffffffffu, term, o);
   if ((threadIdx.x & 31) == 0) partials[((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5] = term;
@@ -644,7 +731,10 @@ cudaError_t launch_em_pass(const ImgGeom& g, const LorTable& t, SubsetSel s, con
   if (total == 0) return cudaSuccess;
 #define APIRL_EM(CT)                                                                                          \
   do {                                                                                                        \
-    if (t.is3d && pg.enabled)                                                                                 \
+    if (t.is3d && t.lor_s)                                                                                    \
+      k_em_pass_rays<CT><<<grid, block, 0, st>>>(g, t, s, (const CT*)counts, counts_packed, add, x, bp, back,  \
+                                                 lik_mode, partials, total);                                  \
+    else if (t.is3d && pg.enabled)                                                                            \
       k_em_pass<CT, true, true><<<grid, block, 0, st>>>(g, t, s, pg, (const CT*)counts, counts_packed, add, x, \
                                                          bp, PadBuffers(), back, lik_mode, partials, total);   \
     else if (t.is3d)                                                                                          \

@@ -94,6 +94,23 @@ class Sino3DGeom:
             rds += [d, -d]
         return cls(n_proj, n_r, n_rings, r_fov, axial_fov, r_scanner, rds, list(rds))
 
+    @classmethod
+    def span(cls, n_proj, n_r, n_rings, r_fov, axial_fov, r_scanner, span, max_ring_diff):
+        """Axially compressed sinogram of odd span S: segment 0 covers ring
+        differences -(S-1)/2..(S-1)/2, then +1, -1, +2, -2, ... each the next S
+        differences, up to max_ring_diff; several ring pairs share a sinogram."""
+        if span < 1 or span % 2 == 0:
+            raise ValueError("span must be odd")
+        h = (span - 1) // 2
+        mn, mx = [-h], [h]
+        lo = h + 1
+        while lo <= max_ring_diff:
+            hi = min(lo + span - 1, max_ring_diff)
+            mn += [lo, -hi]
+            mx += [hi, -lo]
+            lo = hi + 1
+        return cls(n_proj, n_r, n_rings, r_fov, axial_fov, r_scanner, mn, mx)
+
     @property
     def n_segments(self):
         return len(self.min_rd)

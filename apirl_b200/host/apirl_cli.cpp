@@ -71,13 +71,15 @@ std::unique_ptr<CuSiddonProjector> siddon(const std::string& name) {
     std::cerr << "Only the Siddon projector is available on this path (got \"" << name << "\")" << std::endl;
     exit(1);
   }
+  // getSiddonProjectorParameters (data/src/readParameters.cpp:162-203); an
+  // absent key means one sample.
   int ns = ikey("siddon number of samples on the detector", 1);
   int nas = ikey("siddon number of axial samples on the detector", 1);
-  if (ns != 1 || nas != 1) {
-    std::cerr << "Only one LOR per bin is implemented (siddon number of samples = 1)" << std::endl;
+  if (ns < 1 || nas < 1 || ns > APIRL_MAX_SAMPLES || nas > APIRL_MAX_SAMPLES) {
+    std::cerr << "siddon number of samples must be 1.." << APIRL_MAX_SAMPLES << std::endl;
     exit(1);
   }
-  return std::unique_ptr<CuSiddonProjector>(new CuSiddonProjector(1, 1, ikey("gpu id", 0)));
+  return std::unique_ptr<CuSiddonProjector>(new CuSiddonProjector(ns, nas, ikey("gpu id", 0)));
 }
 
 int recon(bool osem) {

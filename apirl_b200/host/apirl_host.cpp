@@ -407,12 +407,11 @@ struct CuSiddonProjector::State {
   float *d_img = nullptr, *d_a = nullptr, *d_b = nullptr;
   size_t nimg = 0, nsino = 0;
   cudaStream_t stream = nullptr;
+  int ns = 1, nas = 1, multi = 0;  // sampling applied to p
 };
 
-CuSiddonProjector::CuSiddonProjector(int nSamples, int nAxialSamples, int gpuId) : st(new State), device(gpuId) {
-  if (nSamples != 1 || nAxialSamples != 1)
-    strError = "only one LOR per bin (numSamplesOnDetector = numAxialSamplesOnDetector = 1) is implemented";
-}
+CuSiddonProjector::CuSiddonProjector(int nSamples, int nAxialSamples, int gpuId)
+    : st(new State), device(gpuId), numSamplesOnDetector(nSamples), numAxialSamplesOnDetector(nAxialSamples) {}
 
 CuSiddonProjector::~CuSiddonProjector() {
   if (st->p) apirl_projector_destroy(st->p);
@@ -446,17 +445,28 @@ bool CuSiddonProjector::prepare2d(const Image* img, const Sinogram2D* s) {
 
 bool CuSiddonProjector::prepare3d(const Image* img, const Sinogram3D* s) {
   apirl_image_geom ig = img->geom();
-  if (st->p && st->is3d && same_img(ig, st->ig) && st->np == s->getNumProjFull() && st->nr == s->getNumR() &&
-      st->rings == s->getNumRings() && st->rfov == s->getRadioFov_mm() && st->afov == s->getAxialFoV_mm() &&
-      st->rsc == s->getRadioScanner_mm() && st->mn == s->minRingDiff() && st->mx == s->maxRingDiff())
-    return true;
-  if (st->p) apirl_projector_destroy(st->p);
-  st->p = nullptr;
-  apirl_sino3d_geom sg = s->geom();
-  if (apirl_projector_create_3d(&ig, &sg, device, &st->p) != APIRL_OK) { strError = apirl_last_error(); return false; }
-  st->is3d = true; st->ig = ig; st->np = s->getNumProjFull(); st->nr = s->getNumR(); st->rings = s->getNumRings();
-  st->rfov = s->getRadioFov_mm(); st->afov = s->getAxialFoV_mm(); st->rsc = s->getRadioScanner_mm();
-  st->mn = s->minRingDiff(); st->mx = s->maxRingDiff();
+  if (!(st->p && st->is3d && same_img(ig, st->ig) && st->np == s->getNumProjFull() && st->nr == s->getNumR() &&
+        st->rings == s->getNumRings() && st->rfov == s->getRadioFov_mm() && st->afov == s->getAxialFoV_mm() &&
+        st->rsc == s->getRadioScanner_mm() && st->mn == s->minRingDiff() && st->mx == s->maxRingDiff())) {
+    if (st->p) apirl_projector_destroy(st->p);
+    st->p = nullptr;
+    apirl_sino3d_geom sg = s->geom();
+    if (apirl_projector_create_3d(&ig, &sg, device, &st->p) != APIRL_OK) { strError = apirl_last_error(); return false; }
+    st->is3d = true; st->ig = ig; st->np = s->getNumProjFull(); st->nr = s->getNumR(); st->rings = s->getNumRings();
+    st->rfov = s->getRadioFov_mm(); st->afov = s->getAxialFoV_mm(); st->rsc = s->getRadioScanner_mm();
+    st->mn = s->minRingDiff(); st->mx = s->maxRingDiff();
+    st->ns = 1; st->nas = 1; st->multi = 0;
+  }
+  // Rays per bin: the constructor's sample counts and the current
+  // useMultipleLorsPerBin flag, which callers may change between calls.
+  const int multi = useMultipleLorsPerBin ? 1 : 0;
+  if (st->ns != numSamplesOnDetector || st->nas != numAxialSamplesOnDetector || st->multi != multi) {
+    if (apirl_projector_set_sampling(st->p, numSamplesOnDetector, numAxialSamplesOnDetector, multi) != APIRL_OK) {
+      strError = apirl_last_error();
+      return false;
+    }
+    st->ns = numSamplesOnDetector; st->nas = numAxialSamplesOnDetector; st->multi = multi;
+  }
   return true;
 }
 
@@ -637,6 +647,20 @@ bool MlemSinogram3d::deviceResident() const {
   return dynamic_cast<CuSiddonProjector*>(forwardprojector) && dynamic_cast<CuSiddonProjector*>(backprojector);
 }
 
+// The fused GPU pass walks one set of rays for the projection and the
+// backprojection, so both projectors must sample alike.
+bool MlemSinogram3d::sameSampling(apirl_sampling* out) {
+  const apirl_sampling f = static_cast<CuSiddonProjector*>(forwardprojector)->sampling();
+  const apirl_sampling b = static_cast<CuSiddonProjector*>(backprojector)->sampling();
+  if (f.n_samples != b.n_samples || f.n_axial_samples != b.n_axial_samples ||
+      f.multiple_lors_per_bin != b.multiple_lors_per_bin) {
+    strError = "forward and back projectors must use the same samples per bin";
+    return false;
+  }
+  *out = f;
+  return true;
+}
+
 bool MlemSinogram3d::Reconstruct() {
   if (!deviceResident()) { strError = "MlemSinogram3d runs on the GPU and needs CuSiddonProjector"; return false; }
   double t0 = now_ms();
@@ -644,11 +668,13 @@ bool MlemSinogram3d::Reconstruct() {
   apirl_image_geom ig = initialEstimate->geom();
   apirl_sino3d_geom sg = inputProjection->geom();
   likelihood.assign(numIterations + 1, 0.0);
+  apirl_sampling sm;
+  if (!sameSampling(&sm)) return false;
   apirl_status rc = apirl_mlem_3d(&ig, &sg, inputProjection->getSinogramPtr(),
                                   multiplicative ? multiplicative->getSinogramPtr() : nullptr,
                                   additive ? additive->getSinogramPtr() : nullptr, initialEstimate->getPixelsPtr(),
                                   numIterations, dev, reconstructionImage->getPixelsPtr(), likelihood.data(),
-                                  sensitivityImage->getPixelsPtr());
+                                  sensitivityImage->getPixelsPtr(), &sm);
   if (rc != APIRL_OK) { strError = apirl_last_error(); return false; }
   double t1 = now_ms();
   sensitivityImage->writeInterfile((outputFilenamePrefix + "_sensitivity").c_str());
@@ -670,11 +696,13 @@ bool OsemSinogram3d::Reconstruct() {
   apirl_image_geom ig = initialEstimate->geom();
   apirl_sino3d_geom sg = inputProjection->geom();
   likelihood.assign((size_t)numIterations * numSubsets + 1, 0.0);
+  apirl_sampling sm;
+  if (!sameSampling(&sm)) return false;
   apirl_status rc = apirl_osem_3d(&ig, &sg, inputProjection->getSinogramPtr(),
                                   multiplicative ? multiplicative->getSinogramPtr() : nullptr,
                                   additive ? additive->getSinogramPtr() : nullptr, initialEstimate->getPixelsPtr(),
                                   numIterations, numSubsets, dev, reconstructionImage->getPixelsPtr(),
-                                  likelihood.data(), sensitivityImage->getPixelsPtr());
+                                  likelihood.data(), sensitivityImage->getPixelsPtr(), &sm);
   if (rc != APIRL_OK) { strError = apirl_last_error(); return false; }
   double t1 = now_ms();
   sensitivityImage->writeInterfile((outputFilenamePrefix + "_sensitivity_subset_0").c_str());

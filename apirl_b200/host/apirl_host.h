@@ -190,11 +190,14 @@ class CuSiddonProjector : public Projector {
   bool Backproject(Sinogram3D* projection, Image* image) override;
   bool DivideAndBackproject(Sinogram3D* in, Sinogram3D* est, Image* out) override;
   int gpuId() const { return device; }
+  // The rays per bin this projector walks (SiddonProjector.h:43-47, Projector.h:54).
+  apirl_sampling sampling() const { return {numSamplesOnDetector, numAxialSamplesOnDetector, useMultipleLorsPerBin}; }
 
  private:
   struct State;
   State* st;
   int device;
+  int numSamplesOnDetector, numAxialSamplesOnDetector;
   bool prepare2d(const Image* img, const Sinogram2D* s);
   bool prepare3d(const Image* img, const Sinogram3D* s);
   bool run(int op, Image* img, const float* a, const float* b, float* out_sino, size_t nbins, int subset, int nsub);
@@ -268,6 +271,7 @@ class MlemSinogram3d : public Mlem {
 
  protected:
   bool deviceResident() const;
+  bool sameSampling(apirl_sampling* out);
   Sinogram3D* inputProjection;
   Sinogram3D* multiplicative = nullptr;
   Sinogram3D* additive = nullptr;

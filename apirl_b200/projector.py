@@ -111,6 +111,11 @@ class SiddonProjector:
         """fp64=False: the reference's float walk (default); True: FP64 alphas (precision study)."""
         check(self.lib.apirl_projector_set_alpha_precision(self.h, _lib.APIRL_ALPHA_F64 if fp64 else _lib.APIRL_ALPHA_F32))
 
+    def set_sampling(self, n_samples=1, n_axial_samples=1, multiple_lors_per_bin=False):
+        """Rays per bin: SiddonProjector(nSamples, nAxialSamples) and setMultipleLorsPerBin (3D)."""
+        check(self.lib.apirl_projector_set_sampling(self.h, int(n_samples), int(n_axial_samples),
+                                                    int(bool(multiple_lors_per_bin))))
+
     def set_option(self, option, value):
         check(self.lib.apirl_projector_set_option(self.h, int(option), int(value)))
 
@@ -234,7 +239,15 @@ def _f32(a):
     return None if a is None else np.ascontiguousarray(a, dtype=np.float32)
 
 
-def osem_3d(image_geom, sino_geom, meas, init, iters, nsubsets, mult=None, add=None, device=0):
+def _sampling_c(sampling):
+    """sampling: None (one ray per bin) or (n_samples, n_axial_samples, multiple_lors_per_bin)."""
+    if sampling is None:
+        return None
+    ns, nas, multi = sampling
+    return ctypes.byref(_lib.SamplingC(int(ns), int(nas), int(bool(multi))))
+
+
+def osem_3d(image_geom, sino_geom, meas, init, iters, nsubsets, mult=None, add=None, device=0, sampling=None):
     """OsemSinogram3d::Reconstruct on the GPU.  Returns (image, likelihood[iters*nsubsets+1], sens of subset 0)."""
     lib = _lib.load()
     meas, init, mult, add = _f32(meas), _f32(init), _f32(mult), _f32(add)
@@ -243,11 +256,12 @@ def osem_3d(image_geom, sino_geom, meas, init, iters, nsubsets, mult=None, add=N
     sens0 = np.zeros(image_geom.n_voxels, np.float32)
     ig, sc = _img_c(image_geom), _sino3d_c(sino_geom)
     check(lib.apirl_osem_3d(ctypes.byref(ig), ctypes.byref(sc), _np_ptr(meas), _np_ptr(mult), _np_ptr(add),
-                            _np_ptr(init), iters, nsubsets, device, _np_ptr(out), _np_ptr(lik), _np_ptr(sens0)))
+                            _np_ptr(init), iters, nsubsets, device, _np_ptr(out), _np_ptr(lik), _np_ptr(sens0),
+                            _sampling_c(sampling)))
     return out, lik, sens0
 
 
-def mlem_3d(image_geom, sino_geom, meas, init, iters, mult=None, add=None, device=0):
+def mlem_3d(image_geom, sino_geom, meas, init, iters, mult=None, add=None, device=0, sampling=None):
     lib = _lib.load()
     meas, init, mult, add = _f32(meas), _f32(init), _f32(mult), _f32(add)
     out = np.zeros(image_geom.n_voxels, np.float32)
@@ -255,7 +269,8 @@ def mlem_3d(image_geom, sino_geom, meas, init, iters, mult=None, add=None, devic
     sens = np.zeros(image_geom.n_voxels, np.float32)
     ig, sc = _img_c(image_geom), _sino3d_c(sino_geom)
     check(lib.apirl_mlem_3d(ctypes.byref(ig), ctypes.byref(sc), _np_ptr(meas), _np_ptr(mult), _np_ptr(add),
-                            _np_ptr(init), iters, device, _np_ptr(out), _np_ptr(lik), _np_ptr(sens)))
+                            _np_ptr(init), iters, device, _np_ptr(out), _np_ptr(lik), _np_ptr(sens),
+                            _sampling_c(sampling)))
     return out, lik, sens
 
 

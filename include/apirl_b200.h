@@ -113,6 +113,23 @@ apirl_status apirl_projector_tables(const apirl_projector* p, float* h_lor, floa
  * segment length to float; projection and accumulation stay FP32.  No
  * counterpart in the reference, whose walk is float only. */
 apirl_status apirl_projector_set_alpha_precision(apirl_projector* p, int mode);
+/* Several rays per bin (3D projectors):
+ * SiddonProjector(nSamplesOnDetector, nAxialSamplesOnDetector)
+ * (recon/src/SiddonProjector.cpp:16-32) and
+ * Projector::setMultipleLorsPerBin (recon/inc/Projector.h:54-60).  Every bin
+ * becomes the sum over multiple_lors_per_bin ? (its ring pairs) : 1 x
+ * n_samples radial x n_axial_samples axial rays, in the reference's loop order
+ * (SiddonProjector.cpp:346-397): radial samples through
+ * getPointsFromOverSampledLor (data/src/Sinogram2DinCylindrical3Dpet.cpp:283-299)
+ * at r - dR/2 + (o + 1/2) dR / n_samples, axial samples spread over the ring
+ * width.  Project and Backproject use the oversampled end points when
+ * n_samples != 1, DivideAndBackproject unless both counts are 1 (:628), as the
+ * reference does.  (1, 1, 0) restores one ray per bin.  Sampled projectors run
+ * the fused pass on one unpadded layout; the FP64-alpha mode and the batch
+ * engine take one ray per bin. */
+#define APIRL_MAX_SAMPLES 64
+apirl_status apirl_projector_set_sampling(apirl_projector* p, int n_samples, int n_axial_samples,
+                                         int multiple_lors_per_bin);
 /* Tuning and instrumentation options (no counterpart in the reference).
  * APIRL_OPT_DUAL_LAYOUT (default 1): the fused 3D pass keeps a transposed
  *   [z][x][y] copy of the image and of the backprojection (2 extra images on
@@ -229,15 +246,22 @@ apirl_status apirl_em_pass_host(apirl_projector* p, const void* h_counts_subset,
  * sensitivity = A_s^T (h_mult or 1), forcePositive, threshold 0 with >=, then
  * iters x nsubsets fused passes, each captured once as a CUDA graph and
  * replayed.  h_lik receives iters*nsubsets+1 values (the last one for the
- * whole-sinogram projection of the result).  h_mult / h_add may be NULL. */
+ * whole-sinogram projection of the result).  h_mult / h_add may be NULL.
+ * sampling: the projector's rays per bin (apirl_projector_set_sampling), or
+ * NULL for one ray per bin. */
+typedef struct {
+  int n_samples;             /* numSamplesOnDetector */
+  int n_axial_samples;       /* numAxialSamplesOnDetector */
+  int multiple_lors_per_bin; /* useMultipleLorsPerBin */
+} apirl_sampling;
 apirl_status apirl_osem_3d(const apirl_image_geom* img, const apirl_sino3d_geom* sino, const float* h_meas,
                            const float* h_mult, const float* h_add, const float* h_init, int iters, int nsubsets,
-                           int device, float* h_out, double* h_lik, float* h_sens0);
+                           int device, float* h_out, double* h_lik, float* h_sens0, const apirl_sampling* sampling);
 /* MlemSinogram3d::Reconstruct (recon/src/MlemSinogram3d.cpp:89-310): threshold
  * from the sensitivity image, >= update; h_lik gets iters+1 values. */
 apirl_status apirl_mlem_3d(const apirl_image_geom* img, const apirl_sino3d_geom* sino, const float* h_meas,
                            const float* h_mult, const float* h_add, const float* h_init, int iters, int device,
-                           float* h_out, double* h_lik, float* h_sens);
+                           float* h_out, double* h_lik, float* h_sens, const apirl_sampling* sampling);
 /* Mlem2d::Reconstruct (recon/src/Mlem2d.cpp:60-278): > update; h_lik gets
  * iters+1 values, the last evaluated on the ratio sinogram as the reference
  * does (Mlem2d.cpp:228). */

@@ -75,6 +75,9 @@ class Oracle:
             getattr(L, f"or_mlem_threshold_{suf}").argtypes = [_l, _vp]
             getattr(L, f"or_mlem_threshold_{suf}").restype = T
             getattr(L, f"or_update_{suf}").argtypes = [_l, _vp, _vp, _vp, T, _i]
+        for suf in ("f32", "f64"):
+            getattr(L, f"or_sampled_3d_{suf}").argtypes = [_vp, _i, _i, _i, _i, _i, _i, _i, _i, _i, _f, _f, _f,
+                                                           _vp, _vp, _vp, _i]
         L.or_lor_points_2d.argtypes = [_i, _i, _f, _f, _vp]
         L.or_sino3d_z.argtypes = [_vp, _vp, _vp]
         L.or_siddon3d_f32.argtypes = [_f, _f, _f, _f, _f, _f, _i, _i, _i, _f, _f, _f, _vp, _vp, _i]
@@ -139,6 +142,21 @@ class Oracle:
         getattr(self.L, f"or_divide_and_backproject_3d_{self._suf(dt)}")(
             ctypes.byref(s), subset, nsub, *_img_args(ig), _p(vin), _p(vest), _p(img), threads or self.threads)
         return img
+
+    def sampled_3d(self, sg, ig, mode, ns, nas, multi, vin, vest=None, subset=-1, nsub=1, dtype=np.float32,
+                   threads=None):
+        """Projectors with several rays per bin.  mode 0: Project (vin = image),
+        1: Backproject, 2: DivideAndBackproject (vin / vest sinograms)."""
+        dt = np.dtype(dtype)
+        vin = np.ascontiguousarray(vin, dtype=dt)
+        vest = None if vest is None else np.ascontiguousarray(vest, dtype=dt)
+        out = np.zeros(sg.subset_bins(subset, nsub) if mode == 0 else ig.n_voxels, dt)
+        s = _sino3d_struct(sg)
+        rc = getattr(self.L, f"or_sampled_3d_{self._suf(dt)}")(
+            ctypes.byref(s), ns, nas, int(multi), mode, subset, nsub, *_img_args(ig), _p(vin), _p(vest), _p(out),
+            threads or self.threads)
+        assert rc == 0
+        return out
 
     def osem_3d(self, sg, ig, init, meas, iters, nsub, mult=None, add=None, dtype=np.float32, threads=None):
         dt = np.dtype(dtype)
@@ -241,6 +259,7 @@ class RefHarness:
         L.ref_image_read.argtypes = [ctypes.c_char_p, _vp, _vp, _vp, _l]
         L.ref_sino3d_read.argtypes = [ctypes.c_char_p, _f, _f, _f, _vp, _l, _vp]
         L.ref_sino3d_read.restype = _l
+        L.ref_sampled_3d.argtypes = [_vp, _i, _i, _i, _i, _i, _i, _i, _i, _i, _f, _f, _f, _vp, _vp, _vp]
         self._tmp = tempfile.mkdtemp(prefix="apirl_ref_")
 
     def set_threads(self, n):
@@ -311,6 +330,14 @@ class RefHarness:
         img = np.zeros(ig.n_voxels, np.float32)
         self.L.ref_backproject_3d(h, subset, nsub, *_img_args(ig), _p(values), _p(img))
         return img
+
+    def sampled_3d(self, h, sg, ig, mode, ns, nas, multi, vin, vest=None, subset=-1, nsub=1):
+        vin = np.ascontiguousarray(vin, np.float32)
+        vest = None if vest is None else np.ascontiguousarray(vest, np.float32)
+        out = np.zeros(sg.subset_bins(subset, nsub) if mode == 0 else ig.n_voxels, np.float32)
+        assert self.L.ref_sampled_3d(h, ns, nas, int(multi), mode, subset, nsub, *_img_args(ig), _p(vin), _p(vest),
+                                     _p(out)) == 0
+        return out
 
     def osem_subiteration(self, h, ig, subset, nsub, x, sens):
         lik = np.zeros(1, np.float32)
