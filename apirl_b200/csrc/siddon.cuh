@@ -162,8 +162,9 @@ __device__ __forceinline__ float siddon3_gather2(Walk3 w, const ImgGeom& g, int 
 // rounding error is orders below one crossing step), so the walk stays in
 // [-2, n+1], inside the border: a border segment reads a zero (the sum is
 // unchanged; the reference skips it) or scatters into the border, which
-// nothing reads.  The three per-axis bounds tests become one test of the
-// linear index against the padded volume, kept as a memory-safety net.
+// nothing reads.  The three per-axis bounds tests become one clamp of the
+// linear index to the padded volume's last voxel (a border voxel), kept as a
+// memory-safety net.
 // Otherwise the reference's bounds test is applied.
 __device__ __forceinline__ float siddon3_gather_pad(Walk3 w, const ImgGeom& g, int ux, int uy, int uz, unsigned lim,
                                                     const float* __restrict__ img) {
@@ -191,8 +192,8 @@ __device__ __forceinline__ float siddon3_gather_pad(Walk3 w, const ImgGeom& g, i
       if (cx) { idx += sx; w.ax = A_ADD(w.ax, w.axu); }
       else if (cy) { idx += sy; w.ay = A_ADD(w.ay, w.ayu); }
       else { idx += sz; w.az = A_ADD(w.az, w.azu); }
-      const float va = (unsigned)ia < lim ? __ldg(img + ia) : 0.f;
-      const float vb = (unsigned)ib < lim ? __ldg(img + ib) : 0.f;
+      const float va = __ldg(img + min((unsigned)ia, lim - 1u));
+      const float vb = __ldg(img + min((unsigned)ib, lim - 1u));
       acc = A_ADD(acc, A_MUL(sa, va));
       acc = A_ADD(acc, A_MUL(sb, vb));
     }
@@ -200,7 +201,7 @@ __device__ __forceinline__ float siddon3_gather_pad(Walk3 w, const ImgGeom& g, i
       const bool cx = (w.ax <= w.ay) & (w.ax <= w.az);
       const bool cy = !cx & (w.ay <= w.az);
       const float an = cx ? w.ax : (cy ? w.ay : w.az);
-      const float v = (unsigned)idx < lim ? __ldg(img + idx) : 0.f;
+      const float v = __ldg(img + min((unsigned)idx, lim - 1u));
       acc = A_ADD(acc, A_MUL(A_MUL(A_SUB(an, w.ac), w.L), v));
     }
     return acc;
@@ -229,7 +230,7 @@ __device__ __forceinline__ void siddon3_scatter_pad(Walk3 w, const ImgGeom& g, i
       const bool cx = (w.ax <= w.ay) & (w.ax <= w.az);
       const bool cy = !cx & (w.ay <= w.az);
       const float an = cx ? w.ax : (cy ? w.ay : w.az);
-      if ((unsigned)idx < lim) atomicAdd(img + idx, A_MUL(A_MUL(A_SUB(an, w.ac), w.L), r));
+      atomicAdd(img + min((unsigned)idx, lim - 1u), A_MUL(A_MUL(A_SUB(an, w.ac), w.L), r));
       w.ac = an;
       if (cx) { idx += sx; w.ax = A_ADD(w.ax, w.axu); }
       else if (cy) { idx += sy; w.ay = A_ADD(w.ay, w.ayu); }

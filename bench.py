@@ -37,6 +37,10 @@ UNIT = "subiter/s"
 NSUB = 21
 TOTAL_COUNTS = 5e8
 L2_FLUSH_BYTES = 256 << 20
+# DRAM bytes (read + write) per k_em_pass launch of the full workload, mean of
+# three launches captured with ncu --metrics dram__bytes_read.sum,
+# dram__bytes_write.sum (one pass; profiles/k_em_pass_osem3d_256x256x81.md).
+FULL_TRAFFIC_BYTES = 2.180e8
 WORKLOAD = ("3D OSEM 256x256x81 image, 41 rings span-1 |rd|<=20: 1261 sinograms x 336 angles x 336 r, "
             "21 subsets, attenuation in sensitivity, 5e8 counts uint32")
 
@@ -289,7 +293,9 @@ def run_gpu(args):
                        "parallelism": f"replicas x{world}"},
             "siddon_gsteps_per_s": gsteps,
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                         "frac": achieved / peak, "traffic": args.traffic_bytes,
+                         "frac": achieved / peak,
+                         "traffic": args.traffic_bytes if args.traffic_bytes is not None else
+                         (FULL_TRAFFIC_BYTES if args.max_ring_diff is None else None),
                          "kernel": "k_em_pass (fused projection / ratio / backprojection)",
                          "timing": "CUDA events recorded by the library around the kernel, same stream",
                          "algorithmic_bytes_per_launch": kern_bytes, "kernel_ms": kern_s * 1e3,
@@ -521,7 +527,8 @@ def main():
     ap_.add_argument("--rate", type=float, default=20.0, help="served: mean arrivals per second")
     ap_.add_argument("--budget-gb", type=float, default=96.0)
     ap_.add_argument("--traffic-bytes", type=float, default=None,
-                     help="DRAM bytes per fused-kernel launch from an ncu capture, reported as roofline.traffic")
+                     help="DRAM bytes per fused-kernel launch from an ncu capture, reported as roofline.traffic "
+                          f"(default for the full workload: {FULL_TRAFFIC_BYTES:.3g})")
     args = ap_.parse_args()
     if args.warmup < 3 and args.impl != "reference":
         args.warmup = 3
