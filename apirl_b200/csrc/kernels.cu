@@ -24,9 +24,14 @@ namespace {
 constexpr int kBlock = 256;
 // Minimum resident 256-thread blocks per SM for the fused kernel (register cap).
 #ifndef APIRL_EM_MIN_BLOCKS
-#define APIRL_EM_MIN_BLOCKS 4
+#define APIRL_EM_MIN_BLOCKS 5
 #endif
 constexpr int kEmMinBlocks = APIRL_EM_MIN_BLOCKS;
+// 1: the fused 3D pass sets the walk up a second time for the backprojection
+// (fewer live registers during the forward walk).
+#ifndef APIRL_EM_RESETUP
+#define APIRL_EM_RESETUP 1
+#endif
 
 struct BinPos {
   int g, k, l, a;  // sinogram, subset angle, r, full angle
@@ -331,7 +336,19 @@ __global__ void __launch_bounds__(kBlock, kEmMinBlocks) k_em_pass(ImgGeom g, Lor
       const float r = (m != 0.f && e != 0.f) ? A_DIV(m, e) : 0.f;
       if (lik_mode == 2) { if (r > 0.f) term = (double)m * log((double)r) - (double)r; }
       else if (lik_mode == 1 ? (e > 0.f) : (e != 0.f)) term = (double)m * log((double)e) - (double)e;
+#if APIRL_EM_RESETUP
+      // The walk is set up again from the tables for the backprojection
+      // instead of keeping the set-up state live through the forward walk.
+      if (back && r != 0.f) {
+        const float4 L2 = __ldcg(t.lor + (int64_t)p.a * t.n_r + p.l);
+        const float2 z2 = __ldcg(t.z + p.g);
+        Walk3 w2;
+        siddon3_setup(L2.x, L2.y, z2.x, A_SUB(L2.z, L2.x), A_SUB(L2.w, L2.y), A_SUB(z2.y, z2.x), g, w2);
+        siddon3_scatter_pad(w2, g, ux, uy, uz, pad.lim, r, tr ? pad.bT : pad.bA);
+      }
+#else
       if (back && r != 0.f) siddon3_scatter_pad(w, g, ux, uy, uz, pad.lim, r, tr ? pad.bT : pad.bA);
+#endif
     } else if (IS3D) {
       Walk3 w;
       float e = ray_sum3(g, L, t.z[p.g], x, w);

@@ -99,6 +99,26 @@ def cylinder_chords(lor, z, radius=100.0):
     return chord_xy[None] * scale
 
 
+# Expected counts per unit of attenuated projection of the 3D workload:
+# 5e8 / 1.7491305e9, the sum of (A x_phantom) * attenuation over all
+# 142,361,856 bins, so that the job holds 5e8 expected counts.  A constant, so
+# that any set of sinograms can be drawn again on its own.
+C2_COUNTS_PER_UNIT = np.float32(5e8 / 1749130543.7612033)
+
+
+def c2_counts(expected, sino_index, n_per_sino, seed=0):
+    """Poisson counts (uint32) of the 3D workload.  expected: float32
+    (A x_phantom) * attenuation of the listed sinograms, [len(sino_index) *
+    n_per_sino]; sino_index: each sinogram's index in the whole sinogram.
+    Sinogram g draws from numpy's default_rng([seed, g]), so a sample of
+    sinograms gets the same counts as in the whole job."""
+    lam = np.asarray(expected, np.float32).reshape(len(sino_index), n_per_sino) * C2_COUNTS_PER_UNIT
+    out = np.empty(lam.shape, np.uint32)
+    for i, g in enumerate(sino_index):
+        out[i] = np.random.default_rng([seed, int(g)]).poisson(lam[i])
+    return out.reshape(-1)
+
+
 def poisson_counts(expected, total, seed=0):
     """Scale `expected` to sum `total` and draw Poisson counts (uint32), numpy."""
     lam = expected.astype(np.float64) * (total / float(expected.sum()))

@@ -104,7 +104,7 @@ class ClockSampler:
 
 
 # ---------------------------------------------------------------------------
-def setup_workload(dev, log, max_ring_diff=None):
+def setup_workload(dev, log, max_ring_diff=None, alpha="f32"):
     """Builds the resident state of the 3D OSEM job on `dev` (outside timing).
     max_ring_diff < 20 keeps only the segments |rd| <= max_ring_diff (a smaller
     case of the same kernels, used for profiler captures)."""
@@ -117,6 +117,8 @@ def setup_workload(dev, log, max_ring_diff=None):
     if max_ring_diff is not None and max_ring_diff < 20:
         sg = Sino3DGeom.span1(sg.n_proj, sg.n_r, sg.n_rings, sg.r_fov, sg.axial_fov, sg.r_scanner, max_ring_diff)
     P = ap.SiddonProjector(ig, sg, device=dev.index)
+    if alpha == "f64":
+        P.set_alpha_precision(True)  # precision-study mode: FP64 walk geometry
     nb = P.num_bins()
     lor, z = P.tables()
     t0 = time.time()
@@ -127,9 +129,10 @@ def setup_workload(dev, log, max_ring_diff=None):
     expected = torch.empty(nb, dtype=torch.float32, device=dev)
     P.project(phantom, expected)
     expected.mul_(atten)
-    expected.mul_(TOTAL_COUNTS / float(expected.double().sum().item()))
-    gen = torch.Generator(device=dev).manual_seed(0)
-    counts = torch.poisson(expected, generator=gen).to(torch.int32).view(torch.uint32)
+    # Poisson draws per sinogram on the host (seeded by sinogram index), so
+    # that the CPU reference arm can draw its sample's counts identically.
+    counts = torch.from_numpy(workloads.c2_counts(expected.cpu().numpy(), range(sg.n_sinos),
+                                                  sg.n_proj * sg.n_r).view(np.int32)).to(dev).view(torch.uint32)
     del expected
     nv = ig.n_voxels
     sens = torch.zeros((NSUB, nv), dtype=torch.float32, device=dev)
@@ -193,7 +196,7 @@ def run_gpu(args):
 
     import apirl_b200 as ap
     ap.load_library()
-    w = setup_workload(dev, log, args.max_ring_diff)
+    w = setup_workload(dev, log, args.max_ring_diff, args.alpha)
     P, counts, sens, x, bp = w["P"], w["counts"], w["sens"], w["x"], w["bp"]
     stream = torch.cuda.Stream(device=dev)
     flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.float32, device=dev)
@@ -279,7 +282,7 @@ def run_gpu(args):
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        cpu = cpu_baseline(w, log, budget_s=args.cpu_seconds)
+        cpu = cpu_baseline(w, log, budget_s=args.cpu_seconds, threads=args.cpu_threads)
 
     if rank == 0:
         line = {
@@ -289,6 +292,7 @@ def run_gpu(args):
             "config": {"workload": WORKLOAD if args.max_ring_diff is None else
                        WORKLOAD + f" (profiling case: segments |rd| <= {args.max_ring_diff} only)",
                        "subsets": NSUB, "counts_dtype": "uint32", "em_block": best_block,
+                       "alpha": args.alpha,
                        "l2": "flushed between timed steps (256 MB write outside the timed events)",
                        "parallelism": f"replicas x{world}"},
             "siddon_gsteps_per_s": gsteps,
@@ -322,15 +326,20 @@ def _sample_geometry(sg):
                       list(SAMPLE_SEGMENTS), list(SAMPLE_SEGMENTS))
 
 
-def _sample_counts(sg, counts_full):
-    """Counts of the sampled segments, in the sample sinogram's layout."""
+def _sample_sinograms(sg):
+    """Indices, in the whole sinogram, of the sampled segments' sinograms."""
     off, parts = 0, {}
     for rd, n in zip(sg.min_rd, sg.sinos_per_segment):
         parts[rd] = (off, n)
         off += n
+    return [g for rd in SAMPLE_SEGMENTS for g in range(parts[rd][0], parts[rd][0] + parts[rd][1])]
+
+
+def _sample_counts(sg, counts_full):
+    """Counts of the sampled segments, in the sample sinogram's layout."""
     per = sg.n_proj * sg.n_r
-    chunks = [counts_full[parts[rd][0] * per:(parts[rd][0] + parts[rd][1]) * per] for rd in SAMPLE_SEGMENTS]
-    return np.concatenate(chunks).astype(np.float32)
+    idx = _sample_sinograms(sg)
+    return counts_full.reshape(sg.n_sinos, per)[idx].reshape(-1).astype(np.float32)
 
 
 class CpuSample:
@@ -338,8 +347,9 @@ class CpuSample:
     the segments SAMPLE_SEGMENTS; `fraction` is the sample's share of the full
     sub-iteration's Siddon segments, so subiter/s = fraction / seconds."""
 
-    def __init__(self, counts, log):
-        """counts: the sampled segments' counts in the sample sinogram's layout."""
+    def __init__(self, counts, log, threads=None):
+        """counts: the sampled segments' counts in the sample sinogram's layout;
+        threads: host threads for the reference's OpenMP loops (default: all)."""
         sys.path.insert(0, os.path.join(ROOT, "tests"))
         from oracle_lib import RefHarness, Oracle, REF_SO
         from apirl_b200 import workloads
@@ -350,7 +360,7 @@ class CpuSample:
         full_steps = oracle.count_steps_3d(self.sg, self.ig, 0, NSUB)
         samp_steps = oracle.count_steps_3d(self.sample, self.ig, 0, NSUB)
         self.fraction = samp_steps / full_steps
-        self.cores = os.cpu_count() or 1
+        self.cores = threads or os.cpu_count() or 1
         if os.path.exists(REF_SO):
             self.kind = "reference"
             self.R = RefHarness()
@@ -372,10 +382,10 @@ class CpuSample:
             self.R.osem_subiteration(self.h, self.ig, 0, NSUB, self.x, self.sens)
         else:
             o, sg, ig = self.oracle, self.sample, self.ig
-            est = o.project_3d(sg, ig, self.x, 0, NSUB)
+            est = o.project_3d(sg, ig, self.x, 0, NSUB, threads=self.cores)
             m = self.counts.reshape(sg.n_sinos, sg.n_proj, sg.n_r)[:, 0::NSUB, :].reshape(-1)
             ratio = o.inverse_divide(m, est)
-            bp = o.backproject_3d(sg, ig, ratio, 0, NSUB)
+            bp = o.backproject_3d(sg, ig, ratio, 0, NSUB, threads=self.cores)
             self.x = o.update(self.x, bp, self.sens, np.float32(0), True)
         return time.perf_counter() - t0
 
@@ -385,9 +395,9 @@ class CpuSample:
                 f"segments); value scaled to whole sub-iterations")
 
 
-def cpu_baseline(w, log, budget_s=15.0):
+def cpu_baseline(w, log, budget_s=15.0, threads=None):
     counts_full = w["counts"].view(__import__("torch").int32).cpu().numpy()
-    cs = CpuSample(_sample_counts(w["sg"], counts_full), log)
+    cs = CpuSample(_sample_counts(w["sg"], counts_full), log, threads)
     times = [cs.run()]
     while sum(times) < budget_s and len(times) < 20:
         times.append(cs.run())
@@ -403,17 +413,21 @@ def run_reference(args):
     log = lambda m: print(f"[bench-ref] {m}", file=sys.stderr, flush=True)
     from apirl_b200 import workloads
     ig, sg = workloads.c2_geometry()
-    # Counts of the same phantom for the sampled segments, generated on the host
-    # (this arm does not touch the GPU): expected values from the oracle's
-    # projection, scaled to the full job's mean of 5e8 / 142,361,856 per bin.
+    # The sampled segments' counts, drawn on the host exactly as the GPU arm
+    # draws them (this arm does not touch the GPU): the oracle's projection of
+    # the phantom (bit-identical to the GPU's), the same attenuation factors,
+    # the same per-sinogram seeds.
     sys.path.insert(0, os.path.join(ROOT, "tests"))
     from oracle_lib import Oracle
     o = Oracle()
     sample = _sample_geometry(sg)
-    lam = o.project_3d(sample, ig, workloads.cylinder_phantom_3d(ig, seed=2)).astype(np.float64)
-    lam *= (TOTAL_COUNTS / float(sg.n_bins)) * lam.size / max(float(lam.sum()), 1.0)
-    counts = np.random.default_rng(0).poisson(lam).astype(np.float32)
-    cs = CpuSample(counts, log)
+    proj = o.project_3d(sample, ig, workloads.cylinder_phantom_3d(ig, seed=2))
+    lor = o.lor_points_2d(sample.n_proj, sample.n_r, sample.r_fov, sample.r_scanner)
+    z1, z2 = o.sino3d_z(sample)
+    chords = workloads.cylinder_chords(lor, np.stack([z1, z2], 1).astype(np.float32))
+    atten = np.exp(-workloads.MU_WATER_PER_MM * chords).astype(np.float32).reshape(-1)
+    counts = workloads.c2_counts(proj * atten, _sample_sinograms(sg), sg.n_proj * sg.n_r).astype(np.float32)
+    cs = CpuSample(counts, log, args.cpu_threads)
     for _ in range(args.warmup):
         cs.run()
     times = [cs.run() for _ in range(args.steps)]
@@ -520,6 +534,10 @@ def main():
     ap_.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap_.add_argument("--no-cpu-baseline", action="store_true")
     ap_.add_argument("--cpu-seconds", type=float, default=15.0)
+    ap_.add_argument("--alpha", default="f32", choices=["f32", "f64"],
+                     help="walk geometry: f32 = the reference's float arithmetic (headline); f64 = precision mode")
+    ap_.add_argument("--cpu-threads", type=int, default=None,
+                     help="host threads of the CPU baseline / reference arm (default: all)")
     ap_.add_argument("--workload", default="osem3d", choices=["osem3d", "batched", "served"])
     ap_.add_argument("--max-ring-diff", type=int, default=None,
                      help="profiling: keep segments |rd| <= this (smaller case of the same kernels)")

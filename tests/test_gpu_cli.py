@@ -131,6 +131,45 @@ def test_osem_command(case):
     assert os.path.exists(d / "rec.log")
 
 
+def test_project_command_with_samples(case):
+    """`siddon number of samples on the detector` (getSiddonProjectorParameters,
+    data/src/readParameters.cpp:162-203) reaches the projector."""
+    d, ig, sg, x, meas, P, est = case
+    keys = {"input file": "x.h33", "output type": "Sinogram3D", "projector": "Siddon",
+            "output filename": "proj_s", "output projection": "meas.h33",
+            "siddon number of samples on the detector": 2,
+            "siddon number of axial samples on the detector": 3}
+    keys.update({"cylindrical pet radius (in mm)": sg.r_scanner, "radius fov (in mm)": sg.r_fov,
+                 "axial fov (in mm)": sg.axial_fov})
+    with open(d / "proj_s.par", "w") as f:
+        f.write("Projection Parameters :=\n" + "".join(f"{k} := {v}\n" for k, v in keys.items()) + "END :=\n")
+    run("project", str(d / "proj_s.par"), d)
+    got = read_data(str(d / "proj_s"), sg.n_bins)
+    Ps = ap.SiddonProjector(ig, sg)
+    Ps.set_sampling(2, 3, False)
+    want = torch.zeros(sg.n_bins, dtype=torch.float32, device=DEV)
+    Ps.project(torch.from_numpy(x).to(DEV), want)
+    want = want.cpu().numpy()
+    assert np.array_equal(got.view(np.uint32), want.view(np.uint32))
+    assert not np.array_equal(got.view(np.uint32), est.view(np.uint32))
+
+
+def test_osem_command_with_samples(case):
+    d, ig, sg, x, meas, P, est = case
+    keys = {"input type": "Sinogram3D", "input file": "meas.h33", "initial estimate": "ones.h33",
+            "output filename prefix": "rec_s", "number of iterations": 1, "number of subsets": 3,
+            "forwardprojector": "Siddon", "backprojector": "Siddon",
+            "siddon number of samples on the detector": 2}
+    keys.update({"cylindrical pet radius (in mm)": sg.r_scanner, "radius fov (in mm)": sg.r_fov,
+                 "axial fov (in mm)": sg.axial_fov})
+    with open(d / "osem_s.par", "w") as f:
+        f.write("OSEM Parameters :=\n" + "".join(f"{k} := {v}\n" for k, v in keys.items()) + "END :=\n")
+    run("OSEM", str(d / "osem_s.par"), d)
+    got = read_data(str(d / "rec_s_final"), ig.n_voxels)
+    want, _, _ = ap.osem_3d(ig, sg, meas, np.ones(ig.n_voxels, np.float32), 1, 3, sampling=(2, 1, False))
+    assert np.linalg.norm(got - want) / np.linalg.norm(want) <= 1e-5
+
+
 def test_mlem2d_command(tmp_path):
     ig = ImageGeom(64, 64, 1, 2.08, 2.08, 1.0)
     sg = Sino2DGeom(60, 80, 83.2, 300.0)
