@@ -65,7 +65,9 @@ int64_t footprint_of(const apirl_image_geom& img, const apirl_sino3d_geom& sino,
   int64_t b = nbins * (int64_t)count_elem_size(dtype);
   if (mult) b += nbins * 4;
   if (add) b += nbins * 4;
-  b += nv * 4 * (4 + nsub);                               // x, bp, their transposed copies, sens per subset
+  const int64_t pv = (int64_t)(img.nx + 2 * apirl::kPad) * (img.ny + 2 * apirl::kPad) * (img.nz + 2 * apirl::kPad);
+  b += nv * 4 * (2 + nsub);                               // x, bp, sens per subset
+  b += pv * 4 * 4;                                        // padded two-layout image and backprojection copies
   b += (int64_t)sino.n_proj * sino.n_r * 16;              // LOR table
   b += ((nbins + 255) / 256) * 8 + 4096;                  // partials, small tables
   return b;
@@ -246,7 +248,7 @@ apirl_status apirl_batch_step(apirl_batch* b, int* n_active, int* n_queued) {
     if (j->stage == Stage::Sens) sens.push_back(j.get());
     else if (j->stage == Stage::Passes) {
       // Jobs whose pass fills the GPU on its own run through the single-job
-      // fused pass (transposed-copy walk, tuned block size); the rest share
+      // fused pass (padded two-layout walk, tuned block size); the rest share
       // one launch.
       if (apirl_projector_num_bins(j->p, j->pass % j->nsub, j->nsub) >= kOwnLaunchBins) big.push_back(j.get());
       else passes.push_back(j.get());

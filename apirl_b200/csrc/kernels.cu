@@ -22,6 +22,7 @@ namespace apirl {
 namespace {
 
 constexpr int kBlock = 256;
+constexpr int kSumLevel2 = 296;  // first-level blocks of the two-level partial sum (2 per SM)
 // Minimum resident 256-thread blocks per SM for the fused kernel (register cap).
 #ifndef APIRL_EM_MIN_BLOCKS
 #define APIRL_EM_MIN_BLOCKS 5
@@ -418,6 +419,19 @@ __global__ void k_sum_partials(const double* __restrict__ partials, int64_t n, d
   if (threadIdx.x == 0) *out = s;
 }
 
+// First level of the two-level sum of many partials: block b sums its
+// contiguous chunk in a fixed order (deterministic), out2[b] = chunk sum.
+__global__ void __launch_bounds__(kBlock) k_sum_chunks(const double* __restrict__ partials, int64_t n,
+                                                       double* __restrict__ out2) {
+  const int64_t chunk = (n + gridDim.x - 1) / gridDim.x;
+  const int64_t lo = (int64_t)blockIdx.x * chunk;
+  const int64_t hi = lo + chunk < n ? lo + chunk : n;
+  double v = 0.0;
+  for (int64_t i = lo + threadIdx.x; i < hi; i += blockDim.x) v += partials[i];
+  const double s = block_sum(v);
+  if (threadIdx.x == 0) out2[blockIdx.x] = s;
+}
+
 // ---------------------------------------------------------------------------
 __global__ void k_inverse_divide(int64_t n, const float* __restrict__ meas, float* __restrict__ est) {
   for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
@@ -695,6 +709,19 @@ __global__ void __launch_bounds__(256) k_pad_reduce(PadDims d, float* __restrict
 }
 
 inline unsigned grid_for(int64_t total) { return (unsigned)((total + kBlock - 1) / kBlock); }
+
+// Deterministic sum of n partials into *out.  Above kSumLevel2 * 64 partials
+// the sum runs in two levels (kSumLevel2 blocks, then one), the second level's
+// kSumLevel2 values stored right after partials[n - 1].
+cudaError_t launch_sum(double* partials, int64_t n, double* out, cudaStream_t st) {
+  if (n > (int64_t)kSumLevel2 * 64) {
+    k_sum_chunks<<<kSumLevel2, kBlock, 0, st>>>(partials, n, partials + n);
+    k_sum_partials<<<1, kBlock, 0, st>>>(partials + n, kSumLevel2, out);
+  } else {
+    k_sum_partials<<<1, kBlock, 0, st>>>(partials, n, out);
+  }
+  return cudaGetLastError();
+}
 inline unsigned stream_grid(int64_t n) {
   int64_t g = (n + kBlock - 1) / kBlock;
   const int64_t cap = 148 * 16;  // a few waves over the 148 SMs; the loops stride
@@ -704,8 +731,10 @@ inline unsigned stream_grid(int64_t n) {
 }  // namespace
 
 int64_t em_pass_blocks(const LorTable& t, SubsetSel s) {
-  // one likelihood partial per warp of the largest block size
-  return ((int64_t)t.n_sinos * s.nk * t.n_r + kBlock - 1) / kBlock * (kBlock / 32);
+  // One likelihood partial per warp for any block size of 32..256 threads
+  // (ceil(total / b) * b / 32 <= total / 32 + 8), then the second level of
+  // the sum right after the last partial.
+  return ((int64_t)t.n_sinos * s.nk * t.n_r + 31) / 32 + 8 + kSumLevel2;
 }
 int64_t likelihood_blocks(int64_t n) { return stream_grid(n); }
 
@@ -779,8 +808,7 @@ cudaError_t launch_em_pass(const ImgGeom& g, const LorTable& t, SubsetSel s, con
 #undef APIRL_EM
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess || !lik) return e;
-  k_sum_partials<<<1, kBlock, 0, st>>>(partials, (int64_t)grid * (block / 32), lik);
-  return cudaGetLastError();
+  return launch_sum(partials, (int64_t)grid * (block / 32), lik, st);
 }
 
 cudaError_t launch_inverse_divide(int64_t n, const float* meas, float* est, cudaStream_t st) {

@@ -131,11 +131,13 @@ apirl_status apirl_projector_set_alpha_precision(apirl_projector* p, int mode);
 apirl_status apirl_projector_set_sampling(apirl_projector* p, int n_samples, int n_axial_samples,
                                          int multiple_lors_per_bin);
 /* Tuning and instrumentation options (no counterpart in the reference).
- * APIRL_OPT_DUAL_LAYOUT (default 1): the fused 3D pass keeps a transposed
- *   [z][x][y] copy of the image and of the backprojection (2 extra images on
- *   the device) and walks rays running mostly along x in it, so that a warp's
- *   32 neighbouring rays touch contiguous memory.  Results equal the 0 setting
- *   up to the order of fp32 additions in the backprojection.
+ * APIRL_OPT_DUAL_LAYOUT (default 1): the fused 3D pass keeps the image and
+ *   the backprojection in two padded layouts, [z][y][x] and [z][x][y], each
+ *   with a 2-voxel zero border (4 extra images on the device), and walks rays
+ *   running mostly along x in the [z][x][y] one, so that a warp's 32
+ *   neighbouring rays touch contiguous memory; rays that stay within the
+ *   border skip the per-step bounds tests.  Results equal the 0 setting up to
+ *   the order of fp32 additions in the backprojection.
  * APIRL_OPT_KERNEL_TIMING (default 0): record CUDA events around the fused
  *   kernel of every pass; apirl_projector_kernel_ms returns the last one.
  * APIRL_OPT_EM_BLOCK (default 128): threads per block of the fused kernel
