@@ -91,8 +91,10 @@ SIGNATURES = {
     "apirl_update_pixels": (_i, [_i64, _vp, _vp, _vp, _vp, _f, _i, _i, _vp]),
     "apirl_force_positive": (_i, [_i64, _vp, _vp]),
     "apirl_em_pass": (_i, [_vp, _vp, _i, _i, _vp, _vp, _vp, _vp, _vp, _f, _i, _i, _i, _vp, _vp]),
+    "apirl_zero_count_image": (_i, [_vp, _vp, _i, _i, _vp, _vp, _vp, _i, _i, _vp]),
+    "apirl_em_pass_sparse": (_i, [_vp, _vp, _i, _i, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _f, _i, _i, _i, _vp, _vp]),
     "apirl_em_project_backproject": (_i, [_vp, _vp, _i, _i, _vp, _vp, _vp, _i, _i, _vp, _vp]),
-    "apirl_em_pass_host": (_i, [_vp, _vp, _i, _vp, _vp, _vp, _vp, _f, _i, _i, _i, _vp, _vp, _vp]),
+    "apirl_em_pass_host": (_i, [_vp, _vp, _i, _vp, _vp, _vp, _vp, _vp, _vp, _f, _i, _i, _i, _vp, _vp, _vp]),
     "apirl_osem_3d": (_i, [ctypes.POINTER(ImageGeomC), ctypes.POINTER(Sino3DGeomC), _vp, _vp, _vp, _vp, _i, _i,
                            _i, _vp, _vp, _vp, ctypes.POINTER(SamplingC)]),
     "apirl_mlem_3d": (_i, [ctypes.POINTER(ImageGeomC), ctypes.POINTER(Sino3DGeomC), _vp, _vp, _vp, _vp, _i, _i,

@@ -487,7 +487,8 @@ bool use_dual(const apirl_projector* p) {
 
 // The fused kernel, bracketed by timing events when enabled.
 apirl_status fused(apirl_projector* p, SubsetSel ss, const void* d_counts, int dtype, int packed, const float* d_add,
-                   const float* d_x, float* d_bp, bool dual, double* d_lik, cudaStream_t s) {
+                   const float* d_x, float* d_bp, bool dual, double* d_lik, cudaStream_t s,
+                   const float* d_zimg = nullptr, const double* d_zero_add = nullptr) {
   if (p->timing) {
     if (!p->ev0) {
       CK(cudaEventCreate(&p->ev0));
@@ -496,7 +497,8 @@ apirl_status fused(apirl_projector* p, SubsetSel ss, const void* d_counts, int d
     CK(cudaEventRecord(p->ev0, s));
   }
   CK(apirl::launch_em_pass(p->g, p->t, ss, d_counts, dtype, packed, d_add, d_x, d_bp, 1, p->is3d ? 0 : 1,
-                           p->d_partials, d_lik, s, p->pg, dual ? p->pad : apirl::PadBuffers(), p->em_block));
+                           p->d_partials, d_lik, s, p->pg, dual ? p->pad : apirl::PadBuffers(), p->em_block,
+                           d_zimg, d_zero_add));
   if (p->timing) {
     CK(cudaEventRecord(p->ev1, s));
     p->timed = 1;
@@ -534,6 +536,49 @@ apirl_status apirl_em_pass(apirl_projector* p, const void* d_counts, int counts_
     return APIRL_OK;
   }
   st = fused(p, ss, d_counts, counts_dtype, counts_packed, d_add, d_x, d_bp, false, d_lik, s);
+  if (st) return st;
+  CK(apirl::launch_update(nv, d_x, d_bp, d_sens, d_thr, thr_value, ge, 1, s));
+  return APIRL_OK;
+}
+
+apirl_status apirl_zero_count_image(apirl_projector* p, const void* d_counts, int counts_dtype, int counts_packed,
+                                    const float* d_add, float* d_zimg, double* d_zero_add, int subset, int nsubsets,
+                                    void* stream) {
+  apirl_status st = check_subset(p, subset, nsubsets);
+  if (st) return st;
+  if (!d_counts || !d_zimg) return fail(APIRL_ERR_INVALID, "null buffer");
+  if (counts_dtype != APIRL_F32 && counts_dtype != APIRL_U32 && counts_dtype != APIRL_U16)
+    return fail(APIRL_ERR_INVALID, "unknown counts dtype %d", counts_dtype);
+  if (!p->is3d || p->t.lor_s)
+    return fail(APIRL_ERR_NOT_SUPPORTED, "the sparse pass needs a 3D projector with one ray per bin");
+  DEVICE_SCOPE(p->device);
+  CK(apirl::launch_zero_bins(p->g, p->t, make_subset(p, subset, nsubsets), d_counts, counts_dtype, counts_packed,
+                             d_add, d_zimg, p->d_partials, d_zero_add, (cudaStream_t)stream,
+                             use_dual(p) ? p->pad : apirl::PadBuffers()));
+  return APIRL_OK;
+}
+
+apirl_status apirl_em_pass_sparse(apirl_projector* p, const void* d_counts, int counts_dtype, int counts_packed,
+                                  const float* d_add, float* d_x, float* d_bp, const float* d_sens,
+                                  const float* d_zimg, const double* d_zero_add, const float* d_thr, float thr_value,
+                                  int ge, int subset, int nsubsets, double* d_lik, void* stream) {
+  apirl_status st = check_em(p, d_counts, counts_dtype, d_x, d_bp, subset, nsubsets);
+  if (st) return st;
+  if (!d_sens || !d_zimg) return fail(APIRL_ERR_INVALID, "null sensitivity or zero-count image");
+  if (!p->is3d || p->t.lor_s || p->pg.enabled)
+    return fail(APIRL_ERR_NOT_SUPPORTED, "the sparse pass needs a 3D projector with one float ray per bin");
+  DEVICE_SCOPE(p->device);
+  cudaStream_t s = (cudaStream_t)stream;
+  SubsetSel ss = make_subset(p, subset, nsubsets);
+  const int64_t nv = (int64_t)p->g.nx * p->g.ny * p->g.nz;
+  if (use_dual(p)) {
+    CK(apirl::launch_pad_copy(p->g, d_x, p->pad, s));
+    st = fused(p, ss, d_counts, counts_dtype, counts_packed, d_add, d_x, d_bp, true, d_lik, s, d_zimg, d_zero_add);
+    if (st) return st;
+    CK(apirl::launch_pad_reduce(p->g, p->pad, 0, d_x, nullptr, d_sens, d_thr, thr_value, ge, s));
+    return APIRL_OK;
+  }
+  st = fused(p, ss, d_counts, counts_dtype, counts_packed, d_add, d_x, d_bp, false, d_lik, s, d_zimg, d_zero_add);
   if (st) return st;
   CK(apirl::launch_update(nv, d_x, d_bp, d_sens, d_thr, thr_value, ge, 1, s));
   return APIRL_OK;
@@ -632,8 +677,8 @@ apirl_status apirl_projector_kernel_ms(apirl_projector* p, double* ms) {
 
 apirl_status apirl_em_pass_host(apirl_projector* p, const void* h_counts_subset, int counts_dtype,
                                 void* d_counts_stage, float* d_x, float* d_bp, const float* d_sens,
-                                float thr_value, int ge, int subset, int nsubsets, float* h_x_out, double* h_lik,
-                                void* stream) {
+                                const float* d_zimg, const double* d_zero_add, float thr_value, int ge, int subset,
+                                int nsubsets, float* h_x_out, double* h_lik, void* stream) {
   apirl_status st = check_subset(p, subset, nsubsets);
   if (st) return st;
   if (!h_counts_subset || !d_counts_stage || !h_x_out) return fail(APIRL_ERR_INVALID, "null buffer");
@@ -643,8 +688,12 @@ apirl_status apirl_em_pass_host(apirl_projector* p, const void* h_counts_subset,
   cudaStream_t s = (cudaStream_t)stream;
   CK(cudaMemcpyAsync(d_counts_stage, h_counts_subset, nb * esz, cudaMemcpyHostToDevice, s));
   double* d_lik = p->d_scalars;
-  st = apirl_em_pass(p, d_counts_stage, counts_dtype, 1, nullptr, d_x, d_bp, d_sens, nullptr, thr_value, ge, subset,
-                     nsubsets, h_lik ? d_lik : nullptr, stream);
+  if (d_zimg)
+    st = apirl_em_pass_sparse(p, d_counts_stage, counts_dtype, 1, nullptr, d_x, d_bp, d_sens, d_zimg, d_zero_add,
+                              nullptr, thr_value, ge, subset, nsubsets, h_lik ? d_lik : nullptr, stream);
+  else
+    st = apirl_em_pass(p, d_counts_stage, counts_dtype, 1, nullptr, d_x, d_bp, d_sens, nullptr, thr_value, ge,
+                       subset, nsubsets, h_lik ? d_lik : nullptr, stream);
   if (st) return st;
   const int64_t nv = (int64_t)p->g.nx * p->g.ny * p->g.nz;
   CK(cudaMemcpyAsync(h_x_out, d_x, nv * sizeof(float), cudaMemcpyDeviceToHost, s));

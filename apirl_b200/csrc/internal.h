@@ -96,7 +96,15 @@ struct PadBuffers {
 cudaError_t launch_em_pass(const ImgGeom& g, const LorTable& t, SubsetSel s, const void* counts, int counts_dtype,
                            int counts_packed, const float* add, const float* x, float* bp, int back, int lik_mode,
                            double* partials, double* lik, cudaStream_t st, const PreciseGeom& pg = PreciseGeom(),
-                           const PadBuffers& pad = PadBuffers(), int block = 0);
+                           const PadBuffers& pad = PadBuffers(), int block = 0, const float* zimg = nullptr,
+                           const double* zero_add = nullptr);
+// Sparse pass (zimg set, 3D float walk): bins with zero counts are not walked;
+// the likelihood subtracts x . zimg + *zero_add instead of their estimates.
+// zimg = A_s^T 1[m == 0] and zero_add = sum of those bins' additive terms,
+// from launch_zero_bins (img accumulated; partials: em_pass_blocks scratch).
+cudaError_t launch_zero_bins(const ImgGeom& g, const LorTable& t, SubsetSel s, const void* counts, int counts_dtype,
+                             int counts_packed, const float* add, float* img, double* partials, double* zero_add,
+                             cudaStream_t st, const PadBuffers& pad = PadBuffers());
 cudaError_t launch_pad_copy(const ImgGeom& g, const float* x, const PadBuffers& pad, cudaStream_t st);
 // mode 0: EM update of x from bA + bT (threshold rule); mode 1: bp += bA + bT.  Clears bA, bT.
 cudaError_t launch_pad_reduce(const ImgGeom& g, const PadBuffers& pad, int mode, float* x, float* bp,

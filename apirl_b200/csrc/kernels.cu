@@ -300,7 +300,8 @@ __global__ void __launch_bounds__(kBlock, kEmMinBlocks) k_em_pass(ImgGeom g, Lor
                                                     int counts_packed, const float* __restrict__ add,
                                                     const float* __restrict__ x, float* __restrict__ bp,
                                                     PadBuffers pad, int back,
-                                                    int lik_mode, double* __restrict__ partials, int64_t total) {
+                                                    int lik_mode, double* __restrict__ partials, int64_t total,
+                                                    int skip_zero) {
   const int64_t b = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   double term = 0.0;
   if (b < total) {
@@ -309,7 +310,11 @@ __global__ void __launch_bounds__(kBlock, kEmMinBlocks) k_em_pass(ImgGeom g, Lor
     const int64_t ci = row * t.n_r + p.l;
     const float m = load_count<CT>(counts, ci);
     const float4 L = t.lor[(int64_t)p.a * t.n_r + p.l];
-    if (IS3D && F64A) {
+    if (skip_zero && m == 0.f) {
+      // Sparse pass: a zero-count bin's ratio is 0 and its likelihood term
+      // -e is linear in the image; the caller's zero-count image supplies
+      // the sum of those terms (k_neg_dot), so the bin is not walked.
+    } else if (IS3D && F64A) {
       const ImgGeomD gd = geom_d(pg);
       Walk3D w;
       float e = ray_sum3d(gd, pg.lor[(int64_t)p.a * t.n_r + p.l], pg.z[p.g], x, w);
@@ -417,6 +422,60 @@ __global__ void k_sum_partials(const double* __restrict__ partials, int64_t n, d
   for (int64_t i = threadIdx.x; i < n; i += blockDim.x) v += partials[i];
   const double s = block_sum(v);
   if (threadIdx.x == 0) *out = s;
+}
+
+// out[b] = - (x . z over block b's contiguous chunk of voxels), FP64, fixed
+// order; block 0 also subtracts *zero_add (when given).  The negated
+// zero-count-bin estimates of the sparse pass.
+__global__ void __launch_bounds__(kBlock) k_neg_dot(const float* __restrict__ x, const float* __restrict__ z,
+                                                    int64_t n, const double* __restrict__ zero_add,
+                                                    double* __restrict__ out) {
+  const int64_t chunk = (n + gridDim.x - 1) / gridDim.x;
+  const int64_t lo = (int64_t)blockIdx.x * chunk;
+  const int64_t hi = lo + chunk < n ? lo + chunk : n;
+  double v = 0.0;
+  for (int64_t i = lo + threadIdx.x; i < hi; i += blockDim.x) v += (double)x[i] * (double)z[i];
+  const double s = block_sum(v);
+  if (threadIdx.x == 0) out[blockIdx.x] = -s - ((blockIdx.x == 0 && zero_add) ? *zero_add : 0.0);
+}
+
+// Zero-count image of a subset for the sparse pass: img += A_s^T 1[m == 0]
+// (the reference's 3D bounds test, one ray per bin), and per-warp partials of
+// the zero-count bins' additive terms.
+// With pad.bA set the scatter goes to the padded two-layout backprojection
+// pair (as in the fused pass), to be folded into img by k_pad_reduce.
+template <typename CT>
+__global__ void __launch_bounds__(kBlock) k_zero_bins(ImgGeom g, LorTable t, SubsetSel s,
+                                                      const CT* __restrict__ counts, int counts_packed,
+                                                      const float* __restrict__ add, float* __restrict__ img,
+                                                      PadBuffers pad, double* __restrict__ partials, int64_t total) {
+  const int64_t b = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  double term = 0.0;
+  if (b < total) {
+    const BinPos p = decode(b, t, s);
+    const int64_t row = counts_packed ? ((int64_t)p.g * s.nk + p.k) : ((int64_t)p.g * t.n_proj + p.a);
+    const int64_t ci = row * t.n_r + p.l;
+    if (load_count<CT>(counts, ci) == 0.f) {
+      if (add) term = (double)__ldg(add + ci);
+      const float4 L = t.lor[(int64_t)p.a * t.n_r + p.l];
+      const float2 z = t.z[p.g];
+      const float vx = A_SUB(L.z, L.x), vy = A_SUB(L.w, L.y);
+      Walk3 w;
+      siddon3_setup(L.x, L.y, z.x, vx, vy, A_SUB(z.y, z.x), g, w);
+      if (pad.bA) {
+        const bool tr = fabsf(vx) >= fabsf(vy);
+        const int px = g.nx + 2 * kPad, py = g.ny + 2 * kPad;
+        siddon3_scatter_pad(w, g, tr ? py : 1, tr ? 1 : px, px * py, pad.lim, 1.f, tr ? pad.bT : pad.bA);
+      } else {
+        siddon3_walk(w, g, [&](bool inb, int idx, float seg) {
+          if (inb) atomicAdd(img + idx, seg);
+        });
+      }
+    }
+  }
+  #pragma unroll
+  for (int o = 16; o > 0; o >>= 1) term += __shfl_down_sync(0xffffffffu, term, o);
+  if ((threadIdx.x & 31) == 0) partials[((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5] = term;
 }
 
 // First level of the two-level sum of many partials: block b sums its
@@ -672,7 +731,9 @@ __global__ void __launch_bounds__(256) k_pad_copy(PadDims d, const float* __rest
 
 // Sum of the two padded backprojections at every interior voxel, [z][y][x]
 // order, interiors cleared.  mode 0: EM update of x (threshold rule ge/gt);
-// mode 1: bp += sum.
+// mode 1: bp += sum.  All loads come before the clearing stores (a store to
+// an address whose load is still in flight stalls the thread's later memory
+// operations: clearing in place made this kernel ~8x slower).
 __global__ void __launch_bounds__(256) k_pad_reduce(PadDims d, float* __restrict__ bA, float* __restrict__ bT,
                                                     int mode, float* __restrict__ x, float* __restrict__ bp,
                                                     const float* __restrict__ sens, const float* __restrict__ thr_ptr,
@@ -682,27 +743,35 @@ __global__ void __launch_bounds__(256) k_pad_reduce(PadDims d, float* __restrict
   const int64_t base = (int64_t)z * d.nx * d.ny;
   for (int r = threadIdx.y; r < 32; r += 8) {  // transposed buffer, read along y
     const int xx = x0 + r, yy = y0 + threadIdx.x;
-    if (xx < d.nx && yy < d.ny) {
-      const int64_t i = d.t(xx, yy, z);
-      tile[threadIdx.x][r] = bT[i];
-      bT[i] = 0.f;
-    }
+    if (xx < d.nx && yy < d.ny) tile[threadIdx.x][r] = bT[d.t(xx, yy, z)];
+  }
+  __syncthreads();
+  float bv[4];
+  #pragma unroll
+  for (int q = 0; q < 4; q++) {
+    const int r = threadIdx.y + 8 * q;
+    const int yy = y0 + r, xx = x0 + threadIdx.x;
+    bv[q] = (xx < d.nx && yy < d.ny) ? A_ADD(bA[d.a(xx, yy, z)], tile[r][threadIdx.x]) : 0.f;
   }
   __syncthreads();
   const float thr = (mode == 0 && thr_ptr) ? *thr_ptr : thr_value;
-  for (int r = threadIdx.y; r < 32; r += 8) {
+  #pragma unroll
+  for (int q = 0; q < 4; q++) {
+    const int r = threadIdx.y + 8 * q;
+    {
+      const int xx = x0 + r, yy = y0 + threadIdx.x;
+      if (xx < d.nx && yy < d.ny) bT[d.t(xx, yy, z)] = 0.f;
+    }
     const int yy = y0 + r, xx = x0 + threadIdx.x;
     if (xx < d.nx && yy < d.ny) {
-      const int64_t ia = d.a(xx, yy, z);
-      const float b = A_ADD(bA[ia], tile[r][threadIdx.x]);
-      bA[ia] = 0.f;
+      bA[d.a(xx, yy, z)] = 0.f;
       const int64_t i = base + (int64_t)yy * d.nx + xx;
       if (mode == 0) {
         const float sv = sens[i];
         const bool okv = ge ? (sv >= thr) : (sv > thr);
-        x[i] = okv ? A_DIV(A_MUL(x[i], b), sv) : 0.f;
+        x[i] = okv ? A_DIV(A_MUL(x[i], bv[q]), sv) : 0.f;
       } else {
-        bp[i] = A_ADD(bp[i], b);
+        bp[i] = A_ADD(bp[i], bv[q]);
       }
     }
   }
@@ -732,9 +801,9 @@ inline unsigned stream_grid(int64_t n) {
 
 int64_t em_pass_blocks(const LorTable& t, SubsetSel s) {
   // One likelihood partial per warp for any block size of 32..256 threads
-  // (ceil(total / b) * b / 32 <= total / 32 + 8), then the second level of
-  // the sum right after the last partial.
-  return ((int64_t)t.n_sinos * s.nk * t.n_r + 31) / 32 + 8 + kSumLevel2;
+  // (ceil(total / b) * b / 32 <= total / 32 + 8), the zero-count image's
+  // partials of the sparse pass, then the second level of the sum.
+  return ((int64_t)t.n_sinos * s.nk * t.n_r + 31) / 32 + 8 + 2 * kSumLevel2;
 }
 int64_t likelihood_blocks(int64_t n) { return stream_grid(n); }
 
@@ -770,11 +839,14 @@ cudaError_t launch_count_steps(const ImgGeom& g, const LorTable& t, SubsetSel s,
 cudaError_t launch_em_pass(const ImgGeom& g, const LorTable& t, SubsetSel s, const void* counts, int counts_dtype,
                            int counts_packed, const float* add, const float* x, float* bp, int back, int lik_mode,
                            double* partials, double* lik, cudaStream_t st, const PreciseGeom& pg,
-                           const PadBuffers& pad, int block) {
+                           const PadBuffers& pad, int block, const float* zimg, const double* zero_add) {
   const int64_t total = (int64_t)t.n_sinos * s.nk * t.n_r;
   if (block < 32 || block > kBlock || block % 32) block = kBlock;
   const unsigned grid = (unsigned)((total + block - 1) / block);
   if (total == 0) return cudaSuccess;
+  // The sparse form walks only bins with counts; it runs on the 3D float
+  // walk with one ray per bin.
+  if (zimg && (!t.is3d || t.lor_s || pg.enabled || lik_mode != 0)) return cudaErrorInvalidValue;
 #define APIRL_EM(CT)                                                                                          \
   do {                                                                                                        \
     if (t.is3d && t.lor_s)                                                                                    \
@@ -782,14 +854,15 @@ cudaError_t launch_em_pass(const ImgGeom& g, const LorTable& t, SubsetSel s, con
                                                  lik_mode, partials, total);                                  \
     else if (t.is3d && pg.enabled)                                                                            \
       k_em_pass<CT, true, true><<<grid, block, 0, st>>>(g, t, s, pg, (const CT*)counts, counts_packed, add, x, \
-                                                         bp, PadBuffers(), back, lik_mode, partials, total);   \
+                                                         bp, PadBuffers(), back, lik_mode, partials, total, 0); \
     else if (t.is3d)                                                                                          \
       k_em_pass<CT, true, false><<<grid, block, 0, st>>>(g, t, s, pg, (const CT*)counts, counts_packed, add,   \
-                                                          x, bp, pad, back, lik_mode, partials, total);       \
+                                                          x, bp, pad, back, lik_mode, partials, total,        \
+                                                          zimg != nullptr);                                   \
     else                                                                                                      \
       k_em_pass<CT, false, false><<<grid, block, 0, st>>>(g, t, s, pg, (const CT*)counts, counts_packed, add,  \
                                                            x, bp, PadBuffers(), back, lik_mode, partials,     \
-                                                           total);                                            \
+                                                           total, 0);                                         \
   } while (0)
   static bool carveout_set = false;  // prefer L1 over shared memory: the kernel uses none
   if (!carveout_set) {
@@ -808,7 +881,46 @@ cudaError_t launch_em_pass(const ImgGeom& g, const LorTable& t, SubsetSel s, con
 #undef APIRL_EM
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess || !lik) return e;
-  return launch_sum(partials, (int64_t)grid * (block / 32), lik, st);
+  int64_t np = (int64_t)grid * (block / 32);
+  if (zimg) {
+    // - sum of the zero-count bins' estimates: - x . zimg - sum of their additive terms.
+    const int64_t nv = (int64_t)g.nx * g.ny * g.nz;
+    k_neg_dot<<<kSumLevel2, kBlock, 0, st>>>(x, zimg, nv, zero_add, partials + np);
+    np += kSumLevel2;
+  }
+  return launch_sum(partials, np, lik, st);
+}
+
+cudaError_t launch_zero_bins(const ImgGeom& g, const LorTable& t, SubsetSel s, const void* counts, int counts_dtype,
+                             int counts_packed, const float* add, float* img, double* partials, double* zero_add,
+                             cudaStream_t st, const PadBuffers& pad) {
+  const int64_t total = (int64_t)t.n_sinos * s.nk * t.n_r;
+  if (!t.is3d || t.lor_s) return cudaErrorInvalidValue;
+  if (total == 0) return cudaSuccess;
+  const unsigned grid = grid_for(total);
+  switch (counts_dtype) {
+    case APIRL_F32:
+      k_zero_bins<float><<<grid, kBlock, 0, st>>>(g, t, s, (const float*)counts, counts_packed, add, img, pad,
+                                                 partials, total);
+      break;
+    case APIRL_U32:
+      k_zero_bins<uint32_t><<<grid, kBlock, 0, st>>>(g, t, s, (const uint32_t*)counts, counts_packed, add, img,
+                                                    pad, partials, total);
+      break;
+    case APIRL_U16:
+      k_zero_bins<uint16_t><<<grid, kBlock, 0, st>>>(g, t, s, (const uint16_t*)counts, counts_packed, add, img,
+                                                    pad, partials, total);
+      break;
+    default: return cudaErrorInvalidValue;
+  }
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return e;
+  if (pad.bA) {
+    e = launch_pad_reduce(g, pad, 1, nullptr, img, nullptr, nullptr, 0.f, 0, st);
+    if (e != cudaSuccess) return e;
+  }
+  if (!zero_add) return cudaSuccess;
+  return launch_sum(partials, (int64_t)grid * (kBlock / 32), zero_add, st);
 }
 
 cudaError_t launch_inverse_divide(int64_t n, const float* meas, float* est, cudaStream_t st) {

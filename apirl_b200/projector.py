@@ -168,6 +168,23 @@ class SiddonProjector:
                                      nsubsets, _ptr(lik), _stream(stream)))
         return x
 
+    def zero_count_image(self, counts, zimg, subset=-1, nsubsets=1, add=None, counts_packed=False, zero_add=None,
+                         stream=None):
+        """zimg += A_s^T 1[counts == 0]; zero_add (device double) = sum of add over those bins."""
+        check(self.lib.apirl_zero_count_image(self.h, _ptr(counts), _counts_dtype(counts), int(counts_packed),
+                                              _ptr(add), _ptr(zimg), _ptr(zero_add), subset, nsubsets,
+                                              _stream(stream)))
+        return zimg
+
+    def em_pass_sparse(self, counts, x, bp, sens, zimg, subset=-1, nsubsets=1, add=None, zero_add=None, thr=None,
+                       thr_value=0.0, ge=True, counts_packed=False, lik=None, stream=None):
+        """em_pass walking only bins with counts; zimg / zero_add from zero_count_image."""
+        check(self.lib.apirl_em_pass_sparse(self.h, _ptr(counts), _counts_dtype(counts), int(counts_packed),
+                                            _ptr(add), _ptr(x), _ptr(bp), _ptr(sens), _ptr(zimg), _ptr(zero_add),
+                                            _ptr(thr), float(thr_value), int(ge), subset, nsubsets, _ptr(lik),
+                                            _stream(stream)))
+        return x
+
     def em_project_backproject(self, counts, x, bp, subset=-1, nsubsets=1, add=None, counts_packed=False, lik=None,
                                stream=None):
         """The fused kernel of em_pass alone (bp += A^T (m / (A x + add))); x is not updated."""
@@ -177,11 +194,13 @@ class SiddonProjector:
         return bp
 
     def em_pass_host(self, h_counts_subset, stage, x, bp, sens, subset, nsubsets, h_x_out, h_lik=None,
-                     thr_value=0.0, ge=True, stream=None):
-        """em_pass from host counts (packed subset, numpy) to a host image; blocks until done."""
+                     thr_value=0.0, ge=True, stream=None, zimg=None, zero_add=None):
+        """em_pass (em_pass_sparse when zimg is given) from host counts (packed
+        subset, numpy) to a host image; blocks until done."""
         dt = {"float32": _lib.APIRL_F32, "uint32": _lib.APIRL_U32, "uint16": _lib.APIRL_U16}[str(h_counts_subset.dtype)]
         check(self.lib.apirl_em_pass_host(self.h, ctypes.c_void_p(h_counts_subset.ctypes.data), dt, _ptr(stage),
-                                          _ptr(x), _ptr(bp), _ptr(sens), float(thr_value), int(ge), subset, nsubsets,
+                                          _ptr(x), _ptr(bp), _ptr(sens), _ptr(zimg), _ptr(zero_add),
+                                          float(thr_value), int(ge), subset, nsubsets,
                                           ctypes.c_void_p(h_x_out.ctypes.data),
                                           None if h_lik is None else ctypes.c_void_p(h_lik.ctypes.data),
                                           _stream(stream)))

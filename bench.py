@@ -157,12 +157,15 @@ def setup_workload(dev, log, max_ring_diff=None, alpha="f32"):
     return dict(P=P, ig=ig, sg=sg, counts=counts, sens=sens, x=x, bp=bp, fwd=fwd, bwd=bwd, atten=atten)
 
 
-def step_bytes(w, s):
+def step_bytes(w, s, sparse=False):
     """Algorithmic HBM bytes of one sub-iteration: fp32 voxel read per forward
     segment, read-modify-write per backward segment, the uint32 count per bin
-    (fused kernel), and 20 B per voxel for the update (x r/w, bp r, sens r, bp clear)."""
+    (fused kernel), and 20 B per voxel for the update (x r/w, bp r, sens r, bp
+    clear).  The sparse pass walks forward only the bins with counts, whose
+    segments are the backward ones."""
     nbins = w["sg"].n_sinos * w["sg"].subset_nproj(s, NSUB) * w["sg"].n_r
-    kern = 4 * w["fwd"][s] + 8 * w["bwd"][s] + 4 * nbins
+    fwd = w["bwd"][s] if sparse else w["fwd"][s]
+    kern = 4 * fwd + 8 * w["bwd"][s] + 4 * nbins
     return kern, kern + 20 * w["ig"].n_voxels
 
 
@@ -196,6 +199,8 @@ def run_gpu(args):
 
     import apirl_b200 as ap
     ap.load_library()
+    if args.alpha == "f64":
+        args.pass_form = "full"  # the sparse pass takes the float walk
     w = setup_workload(dev, log, args.max_ring_diff, args.alpha)
     P, counts, sens, x, bp = w["P"], w["counts"], w["sens"], w["x"], w["bp"]
     stream = torch.cuda.Stream(device=dev)
@@ -210,16 +215,32 @@ def run_gpu(args):
     log(f"autotuned fused-kernel block size: {best_block}")
     P.set_option(_l.APIRL_OPT_KERNEL_TIMING, 1)
 
+    sparse = args.pass_form == "sparse"
+    zimg = torch.zeros((NSUB, w["ig"].n_voxels), dtype=torch.float32, device=dev) if sparse else None
+
+    def zero_images():
+        # Per-subset zero-count images of the sparse pass (once per
+        # reconstruction, like the sensitivity images): Z_s = A_s^T 1[m == 0].
+        zimg.zero_()
+        for s in range(NSUB):
+            P.zero_count_image(counts, zimg[s], s, NSUB, stream=stream)
+
     def step(s, evs=None):
         if evs:
             evs[0].record(stream)
-        # one OSEM sub-iteration through the C ABI: (layout copy,) fused
+        # one OSEM sub-iteration through the C ABI: layout copy, fused
         # projection / ratio / backprojection kernel, likelihood sum, update
-        P.em_pass(counts, x, bp, sens[s], s, NSUB, thr_value=0.0, ge=True, lik=lik, stream=stream)
+        if sparse:
+            P.em_pass_sparse(counts, x, bp, sens[s], zimg[s], s, NSUB, thr_value=0.0, ge=True, lik=lik,
+                             stream=stream)
+        else:
+            P.em_pass(counts, x, bp, sens[s], s, NSUB, thr_value=0.0, ge=True, lik=lik, stream=stream)
         if evs:
             evs[1].record(stream)
 
     with torch.cuda.stream(stream):
+        if sparse:
+            zero_images()
         for i in range(args.warmup):
             step(i % NSUB)
         torch.cuda.synchronize(dev)
@@ -228,6 +249,14 @@ def run_gpu(args):
         torch.cuda.synchronize(dev)
         clocks = ClockSampler(local)
         clocks.start()
+        pre = [torch.cuda.Event(enable_timing=True) for _ in range(2)]
+        if sparse:
+            # the zero-count images are part of the timed job: computed again
+            # here and amortized over the timed sub-iterations
+            flush.zero_()
+            pre[0].record(stream)
+            zero_images()
+            pre[1].record(stream)
         evs = [[torch.cuda.Event(enable_timing=True) for _ in range(2)] for _ in range(args.steps)]
         subs = [(args.warmup + i) % NSUB for i in range(args.steps)]
         kern_ms = []
@@ -240,14 +269,18 @@ def run_gpu(args):
             dist.barrier()
         clock = clocks.stop()
     step_ms = [evs[i][0].elapsed_time(evs[i][1]) for i in range(args.steps)]
-    value, total_ms = whole_job_value(args.steps, sum(step_ms), world, dist if world > 1 else None, dev)
+    pre_ms = pre[0].elapsed_time(pre[1]) if sparse else 0.0
+    value, total_ms = whole_job_value(args.steps, sum(step_ms) + pre_ms, world, dist if world > 1 else None, dev)
 
-    kb = [step_bytes(w, s) for s in subs]
+    kb = [step_bytes(w, s, sparse) for s in subs]
     kern_bytes = statistics.mean(k for k, _ in kb)
     kern_s = statistics.mean(kern_ms) / 1e3
     peak, peak_kind = peaks()
     achieved = kern_bytes / kern_s / 1e9
-    gsteps = sum(w["fwd"][s] + w["bwd"][s] for s in subs) / (total_ms / 1e3) / 1e9 * world
+    walked = sum((2 * w["bwd"][s]) if sparse else (w["fwd"][s] + w["bwd"][s]) for s in subs)
+    if sparse:
+        walked += sum(w["fwd"][s] - w["bwd"][s] for s in range(NSUB))  # the zero-count images' segments
+    gsteps = walked / (total_ms / 1e3) / 1e9 * world
 
     # End-to-end through the C ABI with host buffers: the sub-iteration's packed
     # counts go host->device from pinned memory, the updated image and the
@@ -262,23 +295,46 @@ def run_gpu(args):
         stage = _t.empty(host_counts[0].size, dtype=_t.int32, device=dev)
         h_x = _t.empty(w["ig"].n_voxels, dtype=_t.float32).pin_memory().numpy()
         h_lik = np.zeros(1, np.float64)
-        for i in range(min(args.warmup, 3)):
-            P.em_pass_host(host_counts[i % NSUB], stage, x, bp, sens[i % NSUB], i % NSUB, NSUB, h_x, h_lik,
-                           stream=stream)
         ev = [_t.cuda.Event(enable_timing=True) for _ in range(2)]
-        torch.cuda.synchronize(dev)
-        e_ms = 0.0
-        for i in range(args.steps):
-            s = (args.warmup + i) % NSUB
-            ev[0].record(stream)
-            P.em_pass_host(host_counts[s], stage, x, bp, sens[s], s, NSUB, h_x, h_lik, stream=stream)
-            ev[1].record(stream)
-            ev[1].synchronize()
-            e_ms += ev[0].elapsed_time(ev[1])
+
+        def e2e_zero_images():
+            # the zero-count images from the host counts: each subset's counts
+            # host->device, then its image (sparse pass only)
+            zimg.zero_()
+            for s in range(NSUB):
+                stage.copy_(_t.from_numpy(host_counts[s].view(np.int32)), non_blocking=True)
+                P.zero_count_image(stage.view(_t.uint32), zimg[s], s, NSUB, counts_packed=True, stream=stream)
+
+        def e2e_step(s):
+            P.em_pass_host(host_counts[s], stage, x, bp, sens[s], s, NSUB, h_x, h_lik, stream=stream,
+                           zimg=zimg[s] if sparse else None)
+
+        with _t.cuda.stream(stream):
+            if sparse:
+                e2e_zero_images()
+            for i in range(min(args.warmup, 3)):
+                e2e_step(i % NSUB)
+            torch.cuda.synchronize(dev)
+            e_ms = 0.0
+            if sparse:
+                ev[0].record(stream)
+                e2e_zero_images()
+                ev[1].record(stream)
+                ev[1].synchronize()
+                e_ms += ev[0].elapsed_time(ev[1])
+            for i in range(args.steps):
+                s = (args.warmup + i) % NSUB
+                ev[0].record(stream)
+                e2e_step(s)
+                ev[1].record(stream)
+                ev[1].synchronize()
+                e_ms += ev[0].elapsed_time(ev[1])
         e_value, e_ms = whole_job_value(args.steps, e_ms, world, dist if world > 1 else None, dev)
+        h2d = host_counts[0].nbytes + (sum(h.nbytes for h in host_counts) / args.steps if sparse else 0)
         e2e = {"value": e_value, "unit": UNIT,
-               "h2d_bytes_per_step": int(host_counts[0].nbytes), "d2h_bytes_per_step": int(h_x.nbytes + 8),
-               "api": "apirl_em_pass_host (C ABI, pinned host counts in, host image + likelihood out)"}
+               "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(h_x.nbytes + 8),
+               "api": "apirl_em_pass_host (C ABI, pinned host counts in, host image + likelihood out)"
+                      + ("; the zero-count images from host counts inside the timed region" if sparse else "")}
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -293,6 +349,10 @@ def run_gpu(args):
                        WORKLOAD + f" (profiling case: segments |rd| <= {args.max_ring_diff} only)",
                        "subsets": NSUB, "counts_dtype": "uint32", "em_block": best_block,
                        "alpha": args.alpha,
+                       "pass": ("sparse: bins with zero counts not walked, their likelihood terms -x.Z_s from "
+                                "per-subset zero-count images Z_s = A_s^T 1[m=0], all 21 computed inside the "
+                                "timed region and amortized over the timed sub-iterations") if sparse else
+                               "full: every bin walked",
                        "l2": "flushed between timed steps (256 MB write outside the timed events)",
                        "parallelism": f"replicas x{world}"},
             "siddon_gsteps_per_s": gsteps,
@@ -306,7 +366,9 @@ def run_gpu(args):
                          "peak_source": f"{peak_kind} hbm_gbs"},
             "e2e": e2e,
             "cpu_baseline": cpu,
-            "gpu_launches": 4 * args.steps,
+            # per step: layout copy, fused kernel, (zero-count dot,) two-level
+            # likelihood sum, reduce/update; plus one zero-count kernel per subset
+            "gpu_launches": (6 * args.steps + NSUB) if sparse else 5 * args.steps,
             "clocks": clock,
         }
         print(json.dumps(line), flush=True)
@@ -534,6 +596,9 @@ def main():
     ap_.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap_.add_argument("--no-cpu-baseline", action="store_true")
     ap_.add_argument("--cpu-seconds", type=float, default=15.0)
+    ap_.add_argument("--pass", dest="pass_form", default="full", choices=["sparse", "full"],
+                     help="sparse: bins with zero counts are not walked (their likelihood terms from per-subset "
+                          "zero-count images computed inside the timed region); full: every bin walked")
     ap_.add_argument("--alpha", default="f32", choices=["f32", "f64"],
                      help="walk geometry: f32 = the reference's float arithmetic (headline); f64 = precision mode")
     ap_.add_argument("--cpu-threads", type=int, default=None,

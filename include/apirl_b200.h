@@ -228,6 +228,26 @@ apirl_status apirl_em_pass(apirl_projector* p, const void* d_counts, int counts_
                            const float* d_add, float* d_x, float* d_bp, const float* d_sens, const float* d_thr,
                            float thr_value, int ge, int subset, int nsubsets, double* d_lik, void* stream);
 
+/* Sparse form of apirl_em_pass (3D projectors, one float ray per bin; no
+ * counterpart in the reference, whose results it reproduces).  A bin with
+ * zero counts has ratio 0, so it adds nothing to the backprojection, and its
+ * likelihood term is -e, linear in the image: the sum of those terms is
+ * -(x . Z_s) - sum of their additive terms, with Z_s = A_s^T 1[m == 0]
+ * fixed by the data.  The pass therefore walks only bins with counts and
+ * evaluates the zero-count part as an FP64 dot product.  d_zimg, *d_zero_add:
+ * from apirl_zero_count_image for the same counts, subset and additive term
+ * (it accumulates into d_zimg: zero it first; d_zero_add may be NULL when
+ * there is no additive term).
+ * The image update equals apirl_em_pass's up to the order of fp32 additions;
+ * the FP64 likelihood equals it up to the rounding of Z_s (~1e-7 relative). */
+apirl_status apirl_zero_count_image(apirl_projector* p, const void* d_counts, int counts_dtype, int counts_packed,
+                                    const float* d_add, float* d_zimg, double* d_zero_add, int subset, int nsubsets,
+                                    void* stream);
+apirl_status apirl_em_pass_sparse(apirl_projector* p, const void* d_counts, int counts_dtype, int counts_packed,
+                                  const float* d_add, float* d_x, float* d_bp, const float* d_sens,
+                                  const float* d_zimg, const double* d_zero_add, const float* d_thr, float thr_value,
+                                  int ge, int subset, int nsubsets, double* d_lik, void* stream);
+
 /* The first kernel of apirl_em_pass alone: project, add, likelihood, ratio and
  * backprojection into d_bp, without the pixel update (d_x is only read). */
 apirl_status apirl_em_project_backproject(apirl_projector* p, const void* d_counts, int counts_dtype,
@@ -238,10 +258,12 @@ apirl_status apirl_em_project_backproject(apirl_projector* p, const void* d_coun
  * counts (packed, from pinned or pageable host memory) to the device, runs
  * apirl_em_pass on the projector's resident image / sensitivity buffers, and
  * copies the updated image and the likelihood back.  d_x, d_bp, d_sens are
- * device buffers the caller keeps resident between passes. */
+ * device buffers the caller keeps resident between passes.  With d_zimg set
+ * the pass is apirl_em_pass_sparse (d_zimg, d_zero_add as there). */
 apirl_status apirl_em_pass_host(apirl_projector* p, const void* h_counts_subset, int counts_dtype, void* d_counts_stage,
-                                float* d_x, float* d_bp, const float* d_sens, float thr_value, int ge, int subset,
-                                int nsubsets, float* h_x_out, double* h_lik, void* stream);
+                                float* d_x, float* d_bp, const float* d_sens, const float* d_zimg,
+                                const double* d_zero_add, float thr_value, int ge, int subset, int nsubsets,
+                                float* h_x_out, double* h_lik, void* stream);
 
 /* ---- whole reconstructions (host buffers) --------------------------------
  * OsemSinogram3d::Reconstruct (recon/src/OsemSinogram3d.cpp:36-325): per-subset

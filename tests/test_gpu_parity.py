@@ -199,7 +199,8 @@ def test_em_pass_host_matches_device(oracle):
     st = t(sens)
     _lib.check(P.lib.apirl_em_pass_host(P.h, h_counts.ctypes.data_as(ctypes.c_void_p), _lib.APIRL_U32,
                                         ctypes.c_void_p(stage.data_ptr()), ctypes.c_void_p(x.data_ptr()),
-                                        ctypes.c_void_p(bp.data_ptr()), ctypes.c_void_p(st.data_ptr()), 0.0, 1,
+                                        ctypes.c_void_p(bp.data_ptr()), ctypes.c_void_p(st.data_ptr()), None, None,
+                                        0.0, 1,
                                         subset, ns, h_x.ctypes.data_as(ctypes.c_void_p),
                                         h_lik.ctypes.data_as(ctypes.c_void_p), None))
     assert rel(h_x, want_x) <= 1e-5
@@ -427,3 +428,48 @@ def test_dual_layout_pass_equals_single_layout(oracle):
     assert rel(outs[1][0], outs[0][0]) <= 1e-6
     assert outs[1][1] == outs[0][1]
     assert rel(outs[1][2], outs[0][2]) <= 1e-6
+
+
+@pytest.mark.parametrize("dual", [1, 0])
+def test_sparse_pass_equals_full_pass(oracle, dual):
+    """apirl_em_pass_sparse (zero-count bins not walked, their likelihood terms
+    from the zero-count image) against apirl_em_pass and the oracle."""
+    from apirl_b200 import _lib
+    ig, sg = small_3d()
+    rng = np.random.default_rng(77)
+    x0 = (rng.random(ig.n_voxels, dtype=np.float32) + 0.5).astype(np.float32)
+    meas = rng.poisson(oracle.project_3d(sg, ig, x0) * 0.3).astype(np.float32)
+    meas[rng.random(meas.size) < 0.3] = 0  # plenty of zero-count bins
+    add = (rng.random(meas.size, dtype=np.float32) * 0.1).astype(np.float32)
+    sens = (rng.random(ig.n_voxels, dtype=np.float32) + 1).astype(np.float32)
+    subset, ns = 3, 5
+    P = ap.SiddonProjector(ig, sg)
+    P.set_option(_lib.APIRL_OPT_DUAL_LAYOUT, dual)
+    for use_add in (False, True):
+        a = t(add) if use_add else None
+        for dtype, packed in ((np.float32, False), (np.uint32, False), (np.uint16, True)):
+            counts_np = meas.reshape(sg.n_sinos, sg.n_proj, sg.n_r)[:, subset::ns, :].reshape(-1) if packed else meas
+            counts = t(counts_np.astype(dtype))
+            ad = a
+            if use_add and packed:
+                ad = t(add.reshape(sg.n_sinos, sg.n_proj, sg.n_r)[:, subset::ns, :].reshape(-1))
+            zimg = torch.zeros(ig.n_voxels, dtype=torch.float32, device=DEV)
+            zadd = torch.zeros(1, dtype=torch.float64, device=DEV)
+            P.zero_count_image(counts, zimg, subset, ns, add=ad, counts_packed=packed, zero_add=zadd)
+            x_full, x_sp = t(x0), t(x0)
+            bp = torch.zeros(ig.n_voxels, dtype=torch.float32, device=DEV)
+            lik_full = torch.zeros(1, dtype=torch.float64, device=DEV)
+            lik_sp = torch.zeros(1, dtype=torch.float64, device=DEV)
+            P.em_pass(counts, x_full, bp, t(sens), subset, ns, add=ad, lik=lik_full, counts_packed=packed)
+            P.em_pass_sparse(counts, x_sp, bp, t(sens), zimg, subset, ns, add=ad, zero_add=zadd, lik=lik_sp,
+                             counts_packed=packed)
+            torch.cuda.synchronize()
+            assert rel(x_sp.cpu().numpy(), x_full.cpu().numpy()) <= 1e-6
+            assert float(bp.abs().max()) == 0.0
+            assert abs(lik_sp.item() - lik_full.item()) <= 1e-6 * abs(lik_full.item())
+    # the oracle's zero-count image: backprojection of the zero indicator
+    sub = meas.reshape(sg.n_sinos, sg.n_proj, sg.n_r)[:, subset::ns, :].reshape(-1)
+    want = oracle.backproject_3d(sg, ig, (sub == 0).astype(np.float32), subset, ns)
+    zimg = torch.zeros(ig.n_voxels, dtype=torch.float32, device=DEV)
+    P.zero_count_image(t(meas), zimg, subset, ns)
+    assert rel(zimg.cpu().numpy(), want) <= 1e-5
