@@ -87,71 +87,24 @@ __device__ __forceinline__ void siddon3_setup(float p0x, float p0y, float p0z, f
 template <class V>
 __device__ __forceinline__ void siddon3_walk(Walk3 w, const ImgGeom& g, V&& visit);
 
-// The same walk over an image stored with unit strides ux (x) and uy (y):
-// [z][y][x] is ux = 1, uy = nx; the transposed [z][x][y] is ux = ny, uy = 1.
-template <class V>
-__device__ __forceinline__ void siddon3_walk_s(Walk3 w, const ImgGeom& g, int ux, int uy, V&& visit) {
-  const int sx = w.iinc * ux, sy = w.jinc * uy, sz = w.kinc * g.nx * g.ny;
-  int idx = w.k * (g.nx * g.ny) + w.j * uy + w.i * ux;
-  for (int m = 0; m < w.n; m++) {
-    // The reference's test is (ax<=ay && ax<=az) / (ay<=ax && ay<=az) / else;
-    // the crossing parameters are never NaN (finite, FLT_MAX or +inf), and
-    // then "not x and ay <= az" selects exactly the same branch.
-    const bool cx = (w.ax <= w.ay) & (w.ax <= w.az);
-    const bool cy = !cx & (w.ay <= w.az);
-    const float an = cx ? w.ax : (cy ? w.ay : w.az);
-    const float seg = A_MUL(A_SUB(an, w.ac), w.L);
-    const bool inb = ((unsigned)w.i < (unsigned)g.nx) & ((unsigned)w.j < (unsigned)g.ny) &
-                     ((unsigned)w.k < (unsigned)g.nz);
-    visit(inb, idx, seg);
-    w.ac = an;
-    if (cx) { w.i += w.iinc; idx += sx; w.ax = A_ADD(w.ax, w.axu); }
-    else if (cy) { w.j += w.jinc; idx += sy; w.ay = A_ADD(w.ay, w.ayu); }
-    else { w.k += w.kinc; idx += sz; w.az = A_ADD(w.az, w.azu); }
-  }
-}
-
-// Forward gather sum over the walk, two segments per iteration: both voxel
-// loads are issued before either product is added, doubling the loads in
-// flight per thread.  The additions keep the walk order, so the sum is
-// bit-identical to siddon3_walk_s with acc += seg * img[idx].
-__device__ __forceinline__ float siddon3_gather2(Walk3 w, const ImgGeom& g, int ux, int uy,
-                                                 const float* __restrict__ img) {
-  const int sx = w.iinc * ux, sy = w.jinc * uy, sz = w.kinc * g.nx * g.ny;
-  int idx = w.k * (g.nx * g.ny) + w.j * uy + w.i * ux;
-  float acc = 0.f;
-  auto advance = [&](int& id, float& seg, bool& inb) {
-    const bool cx = (w.ax <= w.ay) & (w.ax <= w.az);
-    const bool cy = !cx & (w.ay <= w.az);
-    const float an = cx ? w.ax : (cy ? w.ay : w.az);
-    seg = A_MUL(A_SUB(an, w.ac), w.L);
-    inb = ((unsigned)w.i < (unsigned)g.nx) & ((unsigned)w.j < (unsigned)g.ny) & ((unsigned)w.k < (unsigned)g.nz);
-    id = idx;
-    w.ac = an;
-    if (cx) { w.i += w.iinc; idx += sx; w.ax = A_ADD(w.ax, w.axu); }
-    else if (cy) { w.j += w.jinc; idx += sy; w.ay = A_ADD(w.ay, w.ayu); }
-    else { w.k += w.kinc; idx += sz; w.az = A_ADD(w.az, w.azu); }
-  };
-  int m = 0;
-  for (; m + 1 < w.n; m += 2) {
-    int ia, ib;
-    float sa, sb;
-    bool ka, kb;
-    advance(ia, sa, ka);
-    advance(ib, sb, kb);
-    const float va = ka ? __ldg(img + ia) : 0.f;
-    const float vb = kb ? __ldg(img + ib) : 0.f;
-    if (ka) acc = A_ADD(acc, A_MUL(sa, va));
-    if (kb) acc = A_ADD(acc, A_MUL(sb, vb));
-  }
-  if (m < w.n) {
-    int ia;
-    float sa;
-    bool ka;
-    advance(ia, sa, ka);
-    if (ka) acc = A_ADD(acc, A_MUL(sa, __ldg(img + ia)));
-  }
-  return acc;
+// The next crossing of a walk, min(ax, ay, az) with the reference's tie order
+// x, y, z (Siddon.cpp:317-339); cx / cy tell which axis it is.  The crossing
+// parameters are never NaN, so min-then-compare selects exactly the
+// reference's branch.
+#ifndef APIRL_SEL_MINMAX
+#define APIRL_SEL_MINMAX 1
+#endif
+__device__ __forceinline__ float next_crossing(const Walk3& w, bool& cx, bool& cy) {
+#if APIRL_SEL_MINMAX
+  const float an = fminf(fminf(w.ax, w.ay), w.az);
+  cx = w.ax == an;
+  cy = !cx & (w.ay == an);
+  return an;
+#else
+  cx = (w.ax <= w.ay) & (w.ax <= w.az);
+  cy = !cx & (w.ay <= w.az);
+  return cx ? w.ax : (cy ? w.ay : w.az);
+#endif
 }
 
 // Walks over an image padded with a kPad-voxel zero border on every side
@@ -174,18 +127,15 @@ __device__ __forceinline__ float siddon3_gather_pad(Walk3 w, const ImgGeom& g, i
   if (w.guarded) {
     int m = 0;
     for (; m + 1 < w.n; m += 2) {
-      bool cx = (w.ax <= w.ay) & (w.ax <= w.az);
-      bool cy = !cx & (w.ay <= w.az);
-      float an = cx ? w.ax : (cy ? w.ay : w.az);
+      bool cx, cy;
+      float an = next_crossing(w, cx, cy);
       const float sa = A_MUL(A_SUB(an, w.ac), w.L);
       const int ia = idx;
       w.ac = an;
       if (cx) { idx += sx; w.ax = A_ADD(w.ax, w.axu); }
       else if (cy) { idx += sy; w.ay = A_ADD(w.ay, w.ayu); }
       else { idx += sz; w.az = A_ADD(w.az, w.azu); }
-      cx = (w.ax <= w.ay) & (w.ax <= w.az);
-      cy = !cx & (w.ay <= w.az);
-      an = cx ? w.ax : (cy ? w.ay : w.az);
+      an = next_crossing(w, cx, cy);
       const float sb = A_MUL(A_SUB(an, w.ac), w.L);
       const int ib = idx;
       w.ac = an;
@@ -198,18 +148,16 @@ __device__ __forceinline__ float siddon3_gather_pad(Walk3 w, const ImgGeom& g, i
       acc = A_ADD(acc, A_MUL(sb, vb));
     }
     if (m < w.n) {
-      const bool cx = (w.ax <= w.ay) & (w.ax <= w.az);
-      const bool cy = !cx & (w.ay <= w.az);
-      const float an = cx ? w.ax : (cy ? w.ay : w.az);
+      bool cx, cy;
+      const float an = next_crossing(w, cx, cy);
       const float v = __ldg(img + min((unsigned)idx, lim - 1u));
       acc = A_ADD(acc, A_MUL(A_MUL(A_SUB(an, w.ac), w.L), v));
     }
     return acc;
   }
   for (int m = 0; m < w.n; m++) {
-    const bool cx = (w.ax <= w.ay) & (w.ax <= w.az);
-    const bool cy = !cx & (w.ay <= w.az);
-    const float an = cx ? w.ax : (cy ? w.ay : w.az);
+    bool cx, cy;
+    const float an = next_crossing(w, cx, cy);
     const float seg = A_MUL(A_SUB(an, w.ac), w.L);
     if (((unsigned)w.i < (unsigned)g.nx) & ((unsigned)w.j < (unsigned)g.ny) & ((unsigned)w.k < (unsigned)g.nz))
       acc = A_ADD(acc, A_MUL(seg, __ldg(img + idx)));
@@ -227,9 +175,8 @@ __device__ __forceinline__ void siddon3_scatter_pad(Walk3 w, const ImgGeom& g, i
   int idx = (w.k + kPad) * uz + (w.j + kPad) * uy + (w.i + kPad) * ux;
   if (w.guarded) {
     for (int m = 0; m < w.n; m++) {
-      const bool cx = (w.ax <= w.ay) & (w.ax <= w.az);
-      const bool cy = !cx & (w.ay <= w.az);
-      const float an = cx ? w.ax : (cy ? w.ay : w.az);
+      bool cx, cy;
+      const float an = next_crossing(w, cx, cy);
       atomicAdd(img + min((unsigned)idx, lim - 1u), A_MUL(A_MUL(A_SUB(an, w.ac), w.L), r));
       w.ac = an;
       if (cx) { idx += sx; w.ax = A_ADD(w.ax, w.axu); }
@@ -239,9 +186,8 @@ __device__ __forceinline__ void siddon3_scatter_pad(Walk3 w, const ImgGeom& g, i
     return;
   }
   for (int m = 0; m < w.n; m++) {
-    const bool cx = (w.ax <= w.ay) & (w.ax <= w.az);
-    const bool cy = !cx & (w.ay <= w.az);
-    const float an = cx ? w.ax : (cy ? w.ay : w.az);
+    bool cx, cy;
+    const float an = next_crossing(w, cx, cy);
     const float seg = A_MUL(A_SUB(an, w.ac), w.L);
     if (((unsigned)w.i < (unsigned)g.nx) & ((unsigned)w.j < (unsigned)g.ny) & ((unsigned)w.k < (unsigned)g.nz))
       atomicAdd(img + idx, A_MUL(seg, r));
@@ -257,9 +203,8 @@ __device__ __forceinline__ void siddon3_walk(Walk3 w, const ImgGeom& g, V&& visi
   const int sx = w.iinc, sy = w.jinc * g.nx, sz = w.kinc * g.nx * g.ny;
   int idx = (w.k * g.ny + w.j) * g.nx + w.i;
   for (int m = 0; m < w.n; m++) {
-    const bool cx = (w.ax <= w.ay) && (w.ax <= w.az);
-    const bool cy = !cx && (w.ay <= w.ax) && (w.ay <= w.az);
-    const float an = cx ? w.ax : (cy ? w.ay : w.az);
+    bool cx, cy;
+    const float an = next_crossing(w, cx, cy);
     const float seg = A_MUL(A_SUB(an, w.ac), w.L);
     const bool inb = ((unsigned)w.i < (unsigned)g.nx) & ((unsigned)w.j < (unsigned)g.ny) &
                      ((unsigned)w.k < (unsigned)g.nz);

@@ -473,3 +473,16 @@ def test_sparse_pass_equals_full_pass(oracle, dual):
     zimg = torch.zeros(ig.n_voxels, dtype=torch.float32, device=DEV)
     P.zero_count_image(t(meas), zimg, subset, ns)
     assert rel(zimg.cpu().numpy(), want) <= 1e-5
+
+
+def test_osem_driver_sparse_long_job_vs_oracle(oracle):
+    """Four iterations: the driver runs the sparse pass (zero-count images)."""
+    ig, sg = small_3d()
+    rng = np.random.default_rng(41)
+    truth = (rng.random(ig.n_voxels, dtype=np.float32) + 0.5).astype(np.float32)
+    meas = rng.poisson(oracle.project_3d(sg, ig, truth) * 0.5).astype(np.float32)
+    init = np.ones(ig.n_voxels, np.float32)
+    img, lik, _ = ap.osem_3d(ig, sg, meas, init, 4, 4)
+    want, want_lik, _ = oracle.osem_3d(sg, ig, init, meas, 4, 4)
+    assert rel(img, want) <= 1e-4
+    assert np.allclose(lik[:-1], want_lik[:-1].astype(np.float64), rtol=1e-5)
