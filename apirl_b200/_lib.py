@@ -23,6 +23,8 @@ APIRL_OPT_EM_BLOCK = 3
 
 APIRL_ALPHA_F32 = 0
 APIRL_ALPHA_F64 = 1
+APIRL_SCANNER_CYLINDRICAL = 0
+APIRL_SCANNER_MMR = 1
 APIRL_MAX_SAMPLES = 64
 
 APIRL_F32 = 0
@@ -47,7 +49,7 @@ class Sino2DGeomC(ctypes.Structure):
 class Sino3DGeomC(ctypes.Structure):
     _fields_ = [("n_proj", _i), ("n_r", _i), ("n_rings", _i), ("n_segments", _i),
                 ("r_fov", _f), ("axial_fov", _f), ("r_scanner", _f),
-                ("min_ring_diff", ctypes.POINTER(_i)), ("max_ring_diff", ctypes.POINTER(_i))]
+                ("min_ring_diff", ctypes.POINTER(_i)), ("max_ring_diff", ctypes.POINTER(_i)), ("scanner", _i)]
 
 
 class SamplingC(ctypes.Structure):
@@ -65,6 +67,9 @@ SIGNATURES = {
     "apirl_last_error": (ctypes.c_char_p, []),
     "apirl_version": (ctypes.c_char_p, []),
     "apirl_lor_table": (_i, [_i, _i, _f, _f, _vp]),
+    "apirl_mmr_lor_table": (_i, [_i, _i, _vp]),
+    "apirl_projector_create_3d_mmr": (_i, [ctypes.POINTER(ImageGeomC), _i, _i, _i, _i, _vp, _vp, _i,
+                                           ctypes.POINTER(_vp)]),
     "apirl_sino3d_ring_z": (_i, [ctypes.POINTER(Sino3DGeomC), _vp]),
     "apirl_projector_create_2d": (_i, [ctypes.POINTER(ImageGeomC), ctypes.POINTER(Sino2DGeomC), _i,
                                        ctypes.POINTER(_vp)]),

@@ -170,7 +170,8 @@ int apirl_sino3d_ring_z(const apirl_sino3d_geom* sino, float* h_z) {
     return -1;
   }
   HostTables t;
-  if (!apirl::build_tables_3d(1, 1, sino->n_rings, 1.f, sino->axial_fov, 2.f, sino->n_segments,
+  const float afov = sino->scanner == APIRL_SCANNER_MMR ? apirl::kMmrAxialFov : sino->axial_fov;
+  if (!apirl::build_tables_3d(1, 1, sino->n_rings, 1.f, afov, 2.f, sino->n_segments,
                               sino->min_ring_diff, sino->max_ring_diff, t))
     return 0;
   if (h_z) memcpy(h_z, t.z.data(), t.z.size() * sizeof(float));
@@ -201,10 +202,60 @@ apirl_status apirl_projector_create_2d(const apirl_image_geom* img, const apirl_
   return st;
 }
 
+apirl_status apirl_mmr_lor_table(int n_proj, int n_r, float* h_lor) {
+  if (n_proj < 2 || n_r <= 0 || !h_lor) return fail(APIRL_ERR_INVALID, "bad arguments");
+  std::vector<float> lor;
+  apirl::mmr_lor_table(n_proj, n_r, lor);
+  memcpy(h_lor, lor.data(), lor.size() * sizeof(float));
+  return APIRL_OK;
+}
+
+apirl_status apirl_projector_create_3d_mmr(const apirl_image_geom* img, int n_proj, int n_r, int n_rings,
+                                           int n_segments, const int* min_ring_diff, const int* max_ring_diff,
+                                           int device, apirl_projector** out) {
+  if (!out) return fail(APIRL_ERR_INVALID, "null output pointer");
+  *out = nullptr;
+  if (!valid_img(img)) return fail(APIRL_ERR_INVALID, "invalid image geometry");
+  if (n_proj < 2 || n_r <= 0 || n_rings <= 0 || n_segments <= 0 || !min_ring_diff || !max_ring_diff)
+    return fail(APIRL_ERR_INVALID, "invalid mMR sinogram geometry (need n_proj >= 2, n_r, n_rings, segments)");
+  if (!walk_bounded(img, apirl::kMmrRadius + apirl::kMmrDoi, apirl::kMmrAxialFov))
+    return fail(APIRL_ERR_INVALID, "voxels too small for the scanner size (walks above 1e5 segments)");
+  for (int i = 0; i < n_segments; i++)
+    if (min_ring_diff[i] > max_ring_diff[i])
+      return fail(APIRL_ERR_INVALID, "segment %d: minimum ring difference above maximum", i);
+  DEVICE_SCOPE(device);
+  apirl_projector* p = new apirl_projector;
+  p->device = device;
+  p->is3d = 1;
+  p->scanner = APIRL_SCANNER_MMR;
+  p->g = apirl::make_img_geom(img->nx, img->ny, img->nz, img->dx, img->dy, img->dz);
+  if (!apirl::build_tables_mmr(n_proj, n_r, n_rings, n_segments, min_ring_diff, max_ring_diff, p->host)) {
+    delete p;
+    return fail(APIRL_ERR_INVALID, "segment table yields no sinograms");
+  }
+  p->t.n_proj = n_proj;
+  p->t.n_r = n_r;
+  p->t.n_sinos = p->host.n_sinos;
+  p->t.is3d = 1;
+  p->n_rings = n_rings;
+  p->r_fov = apirl::kMmrRFov;
+  p->axial_fov = apirl::kMmrAxialFov;
+  p->r_scanner = apirl::kMmrRadius;
+  p->min_rd.assign(min_ring_diff, min_ring_diff + n_segments);
+  p->max_rd.assign(max_ring_diff, max_ring_diff + n_segments);
+  apirl_status st = finish_create(p, out);
+  if (st != APIRL_OK) { std::string m = g_err; apirl_projector_destroy(p); g_err = m; }
+  return st;
+}
+
 apirl_status apirl_projector_create_3d(const apirl_image_geom* img, const apirl_sino3d_geom* sino, int device,
                                        apirl_projector** out) {
   if (!out) return fail(APIRL_ERR_INVALID, "null output pointer");
   *out = nullptr;
+  if (sino && sino->scanner == APIRL_SCANNER_MMR)
+    return apirl_projector_create_3d_mmr(img, sino->n_proj, sino->n_r, sino->n_rings, sino->n_segments,
+                                         sino->min_ring_diff, sino->max_ring_diff, device, out);
+  if (sino && sino->scanner != APIRL_SCANNER_CYLINDRICAL) return fail(APIRL_ERR_INVALID, "unknown scanner %d", sino->scanner);
   if (!valid_img(img)) return fail(APIRL_ERR_INVALID, "invalid image geometry");
   if (!sino || sino->n_proj <= 0 || sino->n_r <= 0 || sino->n_rings <= 0 || sino->n_segments <= 0 ||
       !sino->min_ring_diff || !sino->max_ring_diff || !(sino->r_fov > 0) || !(sino->axial_fov > 0) ||
@@ -290,6 +341,8 @@ apirl_status apirl_projector_set_alpha_precision(apirl_projector* p, int mode) {
   if (mode != APIRL_ALPHA_F32 && mode != APIRL_ALPHA_F64) return fail(APIRL_ERR_INVALID, "unknown alpha mode %d", mode);
   if (mode == APIRL_ALPHA_F64 && !p->is3d)
     return fail(APIRL_ERR_NOT_SUPPORTED, "the FP64-alpha walk is implemented for 3D projectors");
+  if (mode == APIRL_ALPHA_F64 && p->scanner != APIRL_SCANNER_CYLINDRICAL)
+    return fail(APIRL_ERR_NOT_SUPPORTED, "the FP64-alpha tables are built for the cylindrical scanner");
   if (mode == APIRL_ALPHA_F64 && p->t.lor_s)
     return fail(APIRL_ERR_NOT_SUPPORTED, "the FP64-alpha walk takes one ray per bin (sampling is set)");
   DEVICE_SCOPE(p->device);
@@ -323,6 +376,8 @@ apirl_status apirl_projector_set_sampling(apirl_projector* p, int n_samples, int
   if (!p->is3d && !plain)
     return fail(APIRL_ERR_NOT_SUPPORTED, "2D projectors take one ray per bin (the reference's 2D loops ignore "
                                          "the sample counts)");
+  if (p->scanner != APIRL_SCANNER_CYLINDRICAL && !plain)
+    return fail(APIRL_ERR_NOT_SUPPORTED, "sampled rays are built for the cylindrical scanner");
   if (!plain && p->alpha_mode == APIRL_ALPHA_F64)
     return fail(APIRL_ERR_NOT_SUPPORTED, "sampling is not combined with the FP64-alpha walk");
   if (!plain && p->t.n_r < 2 && (n_samples > 1 || n_axial_samples > 1))

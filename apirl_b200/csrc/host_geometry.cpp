@@ -110,6 +110,55 @@ bool build_tables_3d(int n_proj, int n_r, int n_rings, float r_fov, float axial_
   return t.n_sinos > 0;
 }
 
+// Siemens Biograph mMR (data/src/Sinogram2DinSiemensMmr.cpp,
+// data/src/Sinogram3DSiemensMmr.cpp): arc-corrected r values with the mean
+// depth of interaction, angles i * 180 / nProj, odd r bins rotated back by
+// half an angular step, end points on the effective radius R + DOI.
+const float kMmrRadius = 656.0f / 2.0f;
+const float kMmrRFov = 594.0f / 2.0f;
+const float kMmrAxialFov = 260.0f;
+const float kMmrDoi = 9.6f;
+const float kMmrBin = 4.0891f / 2.0f;
+
+void mmr_lor_table(int n_proj, int n_r, std::vector<float>& lor) {
+  // Sinogram2DinSiemensMmr(nProj, nR) (:57-81): r values and angles.
+  const float bin = n_r == 344 ? kMmrBin : kMmrBin * 344 / n_r;
+  std::vector<float> r(n_r), ang(n_proj);
+  for (int j = 0; j < n_r; j++) {
+    const float lr = bin / 2 + (bin * ((float)j - (float)(n_r / 2)));
+    r[j] = (kMmrRadius + kMmrDoi * std::cos(lr / kMmrRadius)) * std::sin(lr / kMmrRadius);
+  }
+  const float phinc = (float)180 / (float)n_proj;
+  for (int i = 0; i < n_proj; i++) ang[i] = (float)i * phinc;
+  // getPointsFromLor, 3D form (:174-198).
+  const float step = ang[1] - ang[0];
+  const float reff = kMmrRadius + kMmrDoi;  // getEffectiveRadioScanner_mm (Sinogram2DinSiemensMmr.h:105)
+  lor.resize((size_t)n_proj * n_r * 4);
+  for (int a = 0; a < n_proj; a++)
+    for (int l = 0; l < n_r; l++) {
+      const float phi = (ang[a] - (float)(l % 2) * step / 2) * kDegToRad;
+      const float c = std::cos(phi), sn = std::sin(phi);
+      const float rv = r[l];
+      const float aux = std::sqrt(reff * reff - rv * rv);
+      float* o = &lor[((size_t)a * n_r + l) * 4];
+      o[0] = rv * c + sn * aux;
+      o[1] = rv * sn - c * aux;
+      o[2] = rv * c - sn * aux;
+      o[3] = rv * sn + c * aux;
+    }
+}
+
+bool build_tables_mmr(int n_proj, int n_r, int n_rings, int n_seg, const int* min_rd, const int* max_rd,
+                      HostTables& t) {
+  if (n_proj < 2) return false;
+  // Ring pairs and end-point z as for any cylindrical scanner, with the
+  // mMR's 260 mm axial field of view (ring width 260 / nRings).
+  if (!build_tables_3d(n_proj, n_r, n_rings, kMmrRFov, kMmrAxialFov, kMmrRadius, n_seg, min_rd, max_rd, t))
+    return false;
+  mmr_lor_table(n_proj, n_r, t.lor);
+  return true;
+}
+
 bool build_rays_3d(int n_proj, int n_r, int n_rings, float r_fov, float axial_fov, float r_scanner, int n_seg,
                    const int* min_rd, const int* max_rd, int ns, int nas, int multi, bool dab, RayTables& t) {
   std::vector<float> r, ang;

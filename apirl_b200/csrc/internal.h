@@ -66,6 +66,12 @@ bool build_tables_3d(int n_proj, int n_r, int n_rings, float r_fov, float axial_
 // when a ray end point is not finite (a sample outside the scanner radius).
 bool build_rays_3d(int n_proj, int n_r, int n_rings, float r_fov, float axial_fov, float r_scanner, int n_seg,
                    const int* min_rd, const int* max_rd, int ns, int nas, int multi, bool dab, RayTables& t);
+// Siemens mMR tables (LOR end points per data/src/Sinogram2DinSiemensMmr.cpp,
+// ring z for its 260 mm axial field of view); the LOR table alone for tests.
+bool build_tables_mmr(int n_proj, int n_r, int n_rings, int n_seg, const int* min_rd, const int* max_rd,
+                      HostTables& t);
+void mmr_lor_table(int n_proj, int n_r, std::vector<float>& lor);
+extern const float kMmrRadius, kMmrRFov, kMmrAxialFov, kMmrDoi;
 ImgGeom make_img_geom(int nx, int ny, int nz, float dx, float dy, float dz);
 
 int subset_nproj(int n_proj, int subset, int nsub);
@@ -198,6 +204,7 @@ struct apirl_projector {
   std::vector<int> min_rd, max_rd;
   // Sampled rays (apirl_projector_set_sampling): t carries the rays of
   // Project / Backproject, t_dab those of DivideAndBackproject.
+  int scanner = 0;               // APIRL_SCANNER_CYLINDRICAL or APIRL_SCANNER_MMR
   int n_samples = 1, n_axial_samples = 1, multi_lors = 0;
   apirl::LorTable t_dab{};
   float4* d_lor_s[2] = {nullptr, nullptr};

@@ -67,6 +67,7 @@ class Sino3DGeom:
     min_rd: List[int]
     max_rd: List[int]
     sinos_per_segment: List[int] = field(default_factory=list)
+    scanner: str = "cylindrical"   # or "mmr" (Siemens Biograph mMR geometry)
 
     def __post_init__(self):
         if not self.sinos_per_segment:
@@ -110,6 +111,15 @@ class Sino3DGeom:
             mx += [hi, -lo]
             lo = hi + 1
         return cls(n_proj, n_r, n_rings, r_fov, axial_fov, r_scanner, mn, mx)
+
+    @classmethod
+    def mmr(cls, n_proj=252, n_r=344, n_rings=64, span=11, max_ring_diff=60):
+        """Siemens Biograph mMR sinogram (Sinogram3DSiemensMmr): r_fov 297,
+        axial fov 260, radius 328 mm are the scanner's constants."""
+        g = cls.span(n_proj, n_r, n_rings, 297.0, 260.0, 328.0, span, max_ring_diff) if span > 1 else \
+            cls.span1(n_proj, n_r, n_rings, 297.0, 260.0, 328.0, max_ring_diff)
+        g.scanner = "mmr"
+        return g
 
     @property
     def n_segments(self):

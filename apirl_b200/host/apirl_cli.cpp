@@ -116,8 +116,12 @@ int recon(bool osem) {
     // explicit "radius fov (in mm)" restores the sinogram's own bin pitch.
     std::string rf;
     if (key("radius fov (in mm)", &rf, false)) s2->setRadioFov_mm((float)atof(rf.c_str()));
-  } else if (type == "Sinogram3D") {
-    s3.reset(new Sinogram3DCylindricalPet(input.c_str(), sc.rFov, sc.zFov, sc.rScanner));
+  } else if (type == "Sinogram3D" || type == "Sinogram3DSiemensMmr") {
+    // Sinogram3DSiemensMmr carries the mMR's fixed geometry (OSEM.cpp:416-425).
+    if (type == "Sinogram3D")
+      s3.reset(new Sinogram3DCylindricalPet(input.c_str(), sc.rFov, sc.zFov, sc.rScanner));
+    else
+      s3.reset(new Sinogram3DSiemensMmr(input.c_str()));
     if (s3->getNumSinograms() <= 0 || s3->getBinCount() <= 1) {
       std::cerr << "Error reading " << input << ": " << s3->getError() << std::endl;
       return 1;
@@ -127,7 +131,8 @@ int recon(bool osem) {
     else
       m.reset(new MlemSinogram3d(s3.get(), &x0, "", prefix, iters, 0, false, false, fwd.get(), back.get()));
   } else {
-    std::cerr << "input type " << type << " is not supported on this path (Sinogram2D, Sinogram3D)" << std::endl;
+    std::cerr << "input type " << type << " is not supported on this path (Sinogram2D, Sinogram3D, "
+              << "Sinogram3DSiemensMmr)" << std::endl;
     return 1;
   }
   if (hasMult && !m->setMultiplicativeProjection(mult)) { std::cerr << "Error reading " << mult << std::endl; return 1; }
@@ -157,9 +162,12 @@ int project() {
     s.FillConstant(0);
     if (!p->Project(&img, &s)) { std::cerr << p->getError() << std::endl; return 1; }
     s.writeInterfile(out.c_str());
-  } else if (type == "Sinogram3D") {
-    Sinogram3DCylindricalPet full(tmpl.c_str(), sc.rFov, sc.zFov, sc.rScanner);
-    std::unique_ptr<Sinogram3D> s(nsub > 0 && subset >= 0 ? full.getSubset(subset, nsub) : full.Copy());
+  } else if (type == "Sinogram3D" || type == "Sinogram3DSiemensMmr") {
+    std::unique_ptr<Sinogram3D> full(type == "Sinogram3D"
+                                         ? (Sinogram3D*)new Sinogram3DCylindricalPet(tmpl.c_str(), sc.rFov, sc.zFov,
+                                                                                     sc.rScanner)
+                                         : (Sinogram3D*)new Sinogram3DSiemensMmr(tmpl.c_str()));
+    std::unique_ptr<Sinogram3D> s(nsub > 0 && subset >= 0 ? full->getSubset(subset, nsub) : full->Copy());
     if (!p->Project(&img, s.get())) { std::cerr << p->getError() << std::endl; return 1; }
     s->writeInterfile(out.c_str());
   } else {
@@ -188,9 +196,12 @@ int backproject() {
   if (type == "Sinogram2D") {
     Sinogram2DinCylindrical3Dpet s(input.c_str(), sc.rFov, sc.rScanner);
     if (!p->Backproject(&s, &img)) { std::cerr << p->getError() << std::endl; return 1; }
-  } else if (type == "Sinogram3D") {
-    Sinogram3DCylindricalPet full(input.c_str(), sc.rFov, sc.zFov, sc.rScanner);
-    std::unique_ptr<Sinogram3D> s(nsub > 0 && subset >= 0 ? full.getSubset(subset, nsub) : full.Copy());
+  } else if (type == "Sinogram3D" || type == "Sinogram3DSiemensMmr") {
+    std::unique_ptr<Sinogram3D> full(type == "Sinogram3D"
+                                         ? (Sinogram3D*)new Sinogram3DCylindricalPet(input.c_str(), sc.rFov, sc.zFov,
+                                                                                     sc.rScanner)
+                                         : (Sinogram3D*)new Sinogram3DSiemensMmr(input.c_str()));
+    std::unique_ptr<Sinogram3D> s(nsub > 0 && subset >= 0 ? full->getSubset(subset, nsub) : full->Copy());
     if (!p->Backproject(s.get(), &img)) { std::cerr << p->getError() << std::endl; return 1; }
   } else {
     std::cerr << "input type " << type << " is not supported on this path" << std::endl;

@@ -294,7 +294,7 @@ Sinogram3D::Sinogram3D(int nProj, int nR, int nRings, float rFov, float axialFov
 
 apirl_sino3d_geom Sinogram3D::geom() const {
   return apirl_sino3d_geom{numProj, numR, numRings, (int)minRD.size(), radioFov_mm, axialFov_mm, radioScanner_mm,
-                           minRD.data(), maxRD.data()};
+                           minRD.data(), maxRD.data(), scanner()};
 }
 
 bool Sinogram3D::FillConstant(float v) { std::fill(bins.begin(), bins.end(), v); return true; }
@@ -316,7 +316,7 @@ float Sinogram3D::getLikelihoodValue(const Sinogram3D* ref) const {
 }
 
 Sinogram3D* Sinogram3D::getSubset(int s, int S) const {
-  Sinogram3D* o = new Sinogram3D(*this);
+  Sinogram3D* o = Copy();  // keeps the scanner type
   int nk = (int)std::floor((float)numProj / (float)S);
   if ((numProj % S) > s) nk++;
   o->numProjSubset = nk;
@@ -396,6 +396,13 @@ Sinogram3DCylindricalPet::Sinogram3DCylindricalPet(const char* header, float rFo
   readFromInterfile(header);
 }
 
+// Sinogram3DSiemensMmr(header) (data/src/Sinogram3DSiemensMmr.cpp): the mMR's
+// fixed field of view (594 mm / 260 mm) and radius (328 mm).
+Sinogram3DSiemensMmr::Sinogram3DSiemensMmr(const char* header)
+    : Sinogram3D(1, 1, 1, 594.0f / 2.0f, 260.0f, 656.0f / 2.0f, {0}, {0}) {
+  readFromInterfile(header);
+}
+
 // ---- CuSiddonProjector ---------------------------------------------------------
 struct CuSiddonProjector::State {
   apirl_projector* p = nullptr;
@@ -408,6 +415,7 @@ struct CuSiddonProjector::State {
   size_t nimg = 0, nsino = 0;
   cudaStream_t stream = nullptr;
   int ns = 1, nas = 1, multi = 0;  // sampling applied to p
+  int scanner = APIRL_SCANNER_CYLINDRICAL;
 };
 
 CuSiddonProjector::CuSiddonProjector(int nSamples, int nAxialSamples, int gpuId)
@@ -447,7 +455,8 @@ bool CuSiddonProjector::prepare3d(const Image* img, const Sinogram3D* s) {
   apirl_image_geom ig = img->geom();
   if (!(st->p && st->is3d && same_img(ig, st->ig) && st->np == s->getNumProjFull() && st->nr == s->getNumR() &&
         st->rings == s->getNumRings() && st->rfov == s->getRadioFov_mm() && st->afov == s->getAxialFoV_mm() &&
-        st->rsc == s->getRadioScanner_mm() && st->mn == s->minRingDiff() && st->mx == s->maxRingDiff())) {
+        st->rsc == s->getRadioScanner_mm() && st->mn == s->minRingDiff() && st->mx == s->maxRingDiff() &&
+        st->scanner == s->scanner())) {
     if (st->p) apirl_projector_destroy(st->p);
     st->p = nullptr;
     apirl_sino3d_geom sg = s->geom();
@@ -455,6 +464,7 @@ bool CuSiddonProjector::prepare3d(const Image* img, const Sinogram3D* s) {
     st->is3d = true; st->ig = ig; st->np = s->getNumProjFull(); st->nr = s->getNumR(); st->rings = s->getNumRings();
     st->rfov = s->getRadioFov_mm(); st->afov = s->getAxialFoV_mm(); st->rsc = s->getRadioScanner_mm();
     st->mn = s->minRingDiff(); st->mx = s->maxRingDiff();
+    st->scanner = s->scanner();
     st->ns = 1; st->nas = 1; st->multi = 0;
   }
   // Rays per bin: the constructor's sample counts and the current

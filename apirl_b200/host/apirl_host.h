@@ -140,6 +140,8 @@ class Sinogram3D {
   bool writeInterfile(const char* pathWithoutExtension) const;
   const char* getError() const { return strError.c_str(); }
   apirl_sino3d_geom geom() const;
+  // APIRL_SCANNER_CYLINDRICAL, or APIRL_SCANNER_MMR for Sinogram3DSiemensMmr.
+  virtual int scanner() const { return APIRL_SCANNER_CYLINDRICAL; }
 
  protected:
   int numProj, numProjSubset, numR, numRings, numSinos;
@@ -156,6 +158,15 @@ class Sinogram3DCylindricalPet : public Sinogram3D {
   // Sinogram3DCylindricalPet(header, rFov, zFov, rScanner) (Sinogram3DCylindricalPet.cpp:19-35).
   Sinogram3DCylindricalPet(const char* headerPath, float rFov_mm, float zFov_mm, float rScanner_mm);
   Sinogram3D* Copy() const override { return new Sinogram3DCylindricalPet(*this); }
+};
+
+// data/inc/Sinogram3DSiemensMmr.h: the Siemens Biograph mMR's sinograms.
+class Sinogram3DSiemensMmr : public Sinogram3D {
+ public:
+  using Sinogram3D::Sinogram3D;
+  explicit Sinogram3DSiemensMmr(const char* headerPath);
+  Sinogram3D* Copy() const override { return new Sinogram3DSiemensMmr(*this); }
+  int scanner() const override { return APIRL_SCANNER_MMR; }
 };
 
 // recon/inc/Projector.h:48-85.

@@ -25,7 +25,9 @@ def _sino3d_c(sg):
     mn = (ctypes.c_int * sg.n_segments)(*sg.min_rd)
     mx = (ctypes.c_int * sg.n_segments)(*sg.max_rd)
     c = Sino3DGeomC(sg.n_proj, sg.n_r, sg.n_rings, sg.n_segments, sg.r_fov, sg.axial_fov, sg.r_scanner,
-                    ctypes.cast(mn, ctypes.POINTER(ctypes.c_int)), ctypes.cast(mx, ctypes.POINTER(ctypes.c_int)))
+                    ctypes.cast(mn, ctypes.POINTER(ctypes.c_int)), ctypes.cast(mx, ctypes.POINTER(ctypes.c_int)),
+                    _lib.APIRL_SCANNER_MMR if getattr(sg, "scanner", "cylindrical") == "mmr"
+                    else _lib.APIRL_SCANNER_CYLINDRICAL)
     c._keep = (mn, mx)
     return c
 

@@ -64,12 +64,19 @@ typedef struct apirl_sino2d_geom {
 } apirl_sino2d_geom;
 
 /* Sinogram3DCylindricalPet(header, rFov_mm, zFov_mm, rScanner_mm) with the
- * header's segment table (data/src/Sinogram3D.cpp:106-471). */
+ * header's segment table (data/src/Sinogram3D.cpp:106-471).  scanner =
+ * APIRL_SCANNER_MMR selects Sinogram3DSiemensMmr instead, whose r_fov,
+ * axial_fov and r_scanner are the scanner's constants (the fields are then
+ * ignored); see apirl_projector_create_3d_mmr.  Zero-initialised structs are
+ * the cylindrical scanner. */
+#define APIRL_SCANNER_CYLINDRICAL 0
+#define APIRL_SCANNER_MMR 1
 typedef struct apirl_sino3d_geom {
   int n_proj, n_r, n_rings, n_segments;
   float r_fov, axial_fov, r_scanner; /* mm */
   const int* min_ring_diff;          /* n_segments entries */
   const int* max_ring_diff;          /* n_segments entries */
+  int scanner;                       /* APIRL_SCANNER_CYLINDRICAL (0) or APIRL_SCANNER_MMR */
 } apirl_sino3d_geom;
 
 typedef struct apirl_projector apirl_projector;
@@ -99,6 +106,23 @@ apirl_status apirl_projector_create_2d(const apirl_image_geom* img, const apirl_
                                        apirl_projector** out);
 apirl_status apirl_projector_create_3d(const apirl_image_geom* img, const apirl_sino3d_geom* sino, int device,
                                        apirl_projector** out);
+/* Siemens Biograph mMR (Sinogram3DSiemensMmr, data/src/Sinogram3DSiemensMmr.cpp;
+ * Sinogram2DinSiemensMmr, data/src/Sinogram2DinSiemensMmr.cpp:19-198): scanner
+ * radius 328 mm, mean depth of interaction 9.6 mm, 594 mm transaxial and
+ * 260 mm axial field of view.  r values are arc-corrected crystal positions
+ * (bin 4.0891/2 mm, scaled to 344 bins), angles i * 180 / n_proj, and odd r
+ * bins are rotated back by half an angular step; the end points lie on the
+ * effective radius 337.6 mm.  The angular step is the whole sinogram's for
+ * every subset (the reference's subset sinograms take it from their own
+ * angle list, i.e. n_subsets times larger).  Ring pairs and end-point z as for
+ * the cylindrical scanner with a 260 mm axial field of view.  Sampling and the
+ * FP64-alpha mode are not offered for this geometry.  Equivalent to
+ * apirl_projector_create_3d with scanner = APIRL_SCANNER_MMR. */
+apirl_status apirl_projector_create_3d_mmr(const apirl_image_geom* img, int n_proj, int n_r, int n_rings,
+                                           int n_segments, const int* min_ring_diff, const int* max_ring_diff,
+                                           int device, apirl_projector** out);
+/* The mMR LOR end-point table on the host ([angle][r][p1x,p1y,p2x,p2y]). */
+apirl_status apirl_mmr_lor_table(int n_proj, int n_r, float* h_lor);
 void apirl_projector_destroy(apirl_projector* p);
 /* Bins of one subset (subset < 0: whole sinogram). */
 int64_t apirl_projector_num_bins(const apirl_projector* p, int subset, int nsubsets);

@@ -571,6 +571,45 @@ int osem3d(const Sino3DG<T>& s, const ImgG<T>& g, const T* init, const T* meas, 
   return 0;
 }
 
+// 3D projector and backprojector over given geometry tables (any scanner):
+// lor = [nProj][nR] (p1x, p1y, p2x, p2y), z = [nSinos] (z1, z2), the end
+// points SiddonProjector::Project / Backproject hand to Siddon() (:392-400,
+// :500-520); loops as project3d / backproject3d (mode 0).
+template <typename T>
+void project3d_tab(int nSinos, int nProj, int nR, const float* lor, const float* z, int subset, int nsub,
+                   const ImgG<T>& g, const T* img, T* out, int threads) {
+  const int nk = subset_nproj(nProj, subset, nsub);
+  const long per = (long)nk * nR, total = per * nSinos;
+  #pragma omp parallel for schedule(dynamic, 256) num_threads(threads)
+  for (long b = 0; b < total; b++) {
+    const int gs = (int)(b / per), k = (int)((b % per) / nR), l = (int)(b % nR);
+    const float* L = lor + ((long)subset_angle(k, subset, nsub) * nR + l) * 4;
+    const T za = (T)z[2 * gs], zb = (T)z[2 * gs + 1];
+    T acc = 0;
+    siddon3d<T>((T)L[0], (T)L[1], za, (T)L[2] - (T)L[0], (T)L[3] - (T)L[1], zb - za, g, [&](int i, int j, int kk, T w) {
+      if (inb(i, j, kk, g.nx, g.ny, g.nz)) acc += w * (T)1 * img[((long)kk * g.ny + j) * g.nx + i];
+    });
+    out[b] = acc;
+  }
+}
+
+template <typename T>
+void backproject3d_tab(int nSinos, int nProj, int nR, const float* lor, const float* z, int subset, int nsub,
+                       const ImgG<T>& g, const T* vin, T* img) {
+  const int nk = subset_nproj(nProj, subset, nsub);
+  const long per = (long)nk * nR, total = per * nSinos;
+  for (long b = 0; b < total; b++) {
+    const T m = vin[b];
+    if (m == 0) continue;
+    const int gs = (int)(b / per), k = (int)((b % per) / nR), l = (int)(b % nR);
+    const float* L = lor + ((long)subset_angle(k, subset, nsub) * nR + l) * 4;
+    const T za = (T)z[2 * gs], zb = (T)z[2 * gs + 1];
+    siddon3d<T>((T)L[0], (T)L[1], za, (T)L[2] - (T)L[0], (T)L[3] - (T)L[1], zb - za, g, [&](int i, int j, int kk, T w) {
+      if (inb(i, j, kk, g.nx, g.ny, g.nz)) img[((long)kk * g.ny + j) * g.nx + i] += w * (T)1 * m;
+    });
+  }
+}
+
 struct S3 {
   int nProj, nR, nRings, nSeg;
   float rFov, axialFov, rScanner;
@@ -710,6 +749,23 @@ int or_sino3d_z_f64(const or_sino3d* d, double* z1, double* z2) {
 
 OR_FWD3(f32, float)
 OR_FWD3(f64, double)
+
+int or_project_3d_tables_f32(int nSinos, int nProj, int nR, const float* lor, const float* z, int subset, int nsub,
+                             int nx, int ny, int nz, float dx, float dy, float dz, const float* img, float* out,
+                             int threads) {
+  project3d_tab<float>(nSinos, nProj, nR, lor, z, subset, nsub, make_img<float>(nx, ny, nz, dx, dy, dz), img, out,
+                       threads);
+  return 0;
+}
+
+// Serial, in bin order (the reference's order with one thread).
+int or_backproject_3d_tables_f32(int nSinos, int nProj, int nR, const float* lor, const float* z, int subset,
+                                 int nsub, int nx, int ny, int nz, float dx, float dy, float dz, const float* vin,
+                                 float* img) {
+  backproject3d_tab<float>(nSinos, nProj, nR, lor, z, subset, nsub, make_img<float>(nx, ny, nz, dx, dy, dz), vin,
+                           img);
+  return 0;
+}
 
 // Sampled-LOR projectors: ns radial and nas axial samples per bin, multi =
 // one ray per ring pair of the bin (useMultipleLorsPerBin).  mode 0 =

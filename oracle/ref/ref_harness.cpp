@@ -48,6 +48,7 @@
 #include <Sinogram2DinCylindrical3Dpet.h>
 #include <Sinogram3D.h>
 #include <Sinogram3DCylindricalPet.h>
+#include <Sinogram3DSiemensMmr.h>
 #include <Mlem2d.h>
 
 namespace {
@@ -613,6 +614,71 @@ int ref_osem_3d(void* hv, int nx, int ny, int nz, float dx, float dy, float dz, 
   }
   memcpy(out_img, x.data(), sizeof(float) * n);
   if (out_sens0) memcpy(out_sens0, sens[0].data(), sizeof(float) * n);
+  return 0;
+}
+
+// ---- Siemens mMR ------------------------------------------------------------
+// Sinogram3DSiemensMmr read from an interfile header (the reference's own
+// constructor, data/src/Sinogram3DSiemensMmr.cpp); no subsets are taken of it
+// (getSubset copies nProj angles into a one-float buffer, :183).
+void* ref_mmr_sino3d_create(const char* tmpdir, int nProj, int nR, int nRings, int nSeg, const int* nSinos,
+                            const int* minRD, const int* maxRD, const float* data) {
+  std::string hdr = write_sino3d_header(tmpdir, nProj, nR, nRings, nSeg, nSinos, minRD, maxRD, data);
+  if (hdr.empty()) return NULL;
+  Sinogram3DSiemensMmr* s = new Sinogram3DSiemensMmr((char*)hdr.c_str());
+  if (s->getNumSegments() != nSeg) return NULL;
+  return s;
+}
+
+// LOR end points of every (angle, r) from the first 2D sinogram
+// (getPointsFromLor, Sinogram2DinSiemensMmr.cpp:174-198) and each sinogram's
+// end-point z as SiddonProjector::Project sets it (:357-360, :392-396).
+int ref_mmr_tables(void* hv, float* lor, float* z) {
+  Sinogram3D* s = (Sinogram3D*)hv;
+  Sinogram2DinCylindrical3Dpet* s0 = s->getSegment(0)->getSinogram2D(0);
+  for (int k = 0; k < s0->getNumProj(); k++)
+    for (int l = 0; l < s0->getNumR(); l++) {
+      Point3D P1, P2; float geom;
+      s0->getPointsFromLor(k, l, 0, &P1, &P2, &geom);
+      float* o = lor + ((size_t)k * s0->getNumR() + l) * 4;
+      o[0] = P1.X; o[1] = P1.Y; o[2] = P2.X; o[3] = P2.Y;
+    }
+  float ringWidth_mm = s->getAxialFoV_mm() / s->getNumRings();
+  float deltaZ = ringWidth_mm / 1;
+  int g = 0;
+  for (int i = 0; i < s->getNumSegments(); i++)
+    for (int j = 0; j < s->getSegment(i)->getNumSinograms(); j++, g++) {
+      Sinogram2DinCylindrical3Dpet* s2 = s->getSegment(i)->getSinogram2D(j);
+      float z1 = (s2->getAxialValue1FromList(0) + s2->getAxialValue1FromList(s2->getNumZ() - 1)) / 2;
+      float z2 = (s2->getAxialValue2FromList(0) + s2->getAxialValue2FromList(s2->getNumZ() - 1)) / 2;
+      int p = 0;
+      z[2 * g] = z1 - ringWidth_mm / 2 + deltaZ / 2 + p * deltaZ;
+      z[2 * g + 1] = z2 - ringWidth_mm / 2 + deltaZ / 2 + p * deltaZ;
+    }
+  return g;
+}
+
+// Whole-sinogram projection (masked loops of SiddonProjector::Project).
+int ref_mmr_project(void* hv, int nx, int ny, int nz, float dx, float dy, float dz, const float* img, float* out) {
+  Sinogram3D* s = (Sinogram3D*)hv;
+  Image* im = make_image(nx, ny, nz, dx, dy, dz, img);
+  MaskedSiddonProjector p;
+  p.Project(im, s);
+  copy_out(s, out);
+  delete im;
+  return 0;
+}
+
+// SiddonProjector::Backproject (unmodified) of `values`, accumulated into img_inout.
+int ref_mmr_backproject(void* hv, int nx, int ny, int nz, float dx, float dy, float dz, const float* values,
+                        float* img_inout) {
+  Sinogram3D* s = (Sinogram3D*)hv;
+  copy_in(s, values);
+  Image* im = make_image(nx, ny, nz, dx, dy, dz, img_inout);
+  SiddonProjector sp(1, 1);
+  sp.Backproject(s, im);
+  memcpy(img_inout, im->getPixelsPtr(), sizeof(float) * (size_t)nx * ny * nz);
+  delete im;
   return 0;
 }
 

@@ -78,6 +78,8 @@ class Oracle:
         for suf in ("f32", "f64"):
             getattr(L, f"or_sampled_3d_{suf}").argtypes = [_vp, _i, _i, _i, _i, _i, _i, _i, _i, _i, _f, _f, _f,
                                                            _vp, _vp, _vp, _i]
+        L.or_project_3d_tables_f32.argtypes = [_i, _i, _i, _vp, _vp, _i, _i, _i, _i, _i, _f, _f, _f, _vp, _vp, _i]
+        L.or_backproject_3d_tables_f32.argtypes = [_i, _i, _i, _vp, _vp, _i, _i, _i, _i, _i, _f, _f, _f, _vp, _vp]
         L.or_lor_points_2d.argtypes = [_i, _i, _f, _f, _vp]
         L.or_sino3d_z.argtypes = [_vp, _vp, _vp]
         L.or_siddon3d_f32.argtypes = [_f, _f, _f, _f, _f, _f, _i, _i, _i, _f, _f, _f, _vp, _vp, _i]
@@ -157,6 +159,28 @@ class Oracle:
             threads or self.threads)
         assert rc == 0
         return out
+
+    def project_3d_tables(self, lor, z, ig, img, subset=-1, nsub=1, threads=None):
+        """Projection over given tables: lor [n_proj, n_r, 4], z [n_sinos, 2] (float32)."""
+        lor = np.ascontiguousarray(lor, np.float32)
+        z = np.ascontiguousarray(z, np.float32)
+        n_proj, n_r = lor.shape[0], lor.shape[1]
+        n_sinos = z.shape[0]
+        img = np.ascontiguousarray(img, np.float32)
+        nk = len(range(subset, n_proj, nsub)) if subset >= 0 else n_proj
+        out = np.zeros(n_sinos * nk * n_r, np.float32)
+        self.L.or_project_3d_tables_f32(n_sinos, n_proj, n_r, _p(lor), _p(z), subset, nsub, *_img_args(ig), _p(img),
+                                        _p(out), threads or self.threads)
+        return out
+
+    def backproject_3d_tables(self, lor, z, ig, values, subset=-1, nsub=1):
+        lor = np.ascontiguousarray(lor, np.float32)
+        z = np.ascontiguousarray(z, np.float32)
+        values = np.ascontiguousarray(values, np.float32)
+        img = np.zeros(ig.n_voxels, np.float32)
+        self.L.or_backproject_3d_tables_f32(z.shape[0], lor.shape[0], lor.shape[1], _p(lor), _p(z), subset, nsub,
+                                            *_img_args(ig), _p(values), _p(img))
+        return img
 
     def osem_3d(self, sg, ig, init, meas, iters, nsub, mult=None, add=None, dtype=np.float32, threads=None):
         dt = np.dtype(dtype)
@@ -260,6 +284,11 @@ class RefHarness:
         L.ref_sino3d_read.argtypes = [ctypes.c_char_p, _f, _f, _f, _vp, _l, _vp]
         L.ref_sino3d_read.restype = _l
         L.ref_sampled_3d.argtypes = [_vp, _i, _i, _i, _i, _i, _i, _i, _i, _i, _f, _f, _f, _vp, _vp, _vp]
+        L.ref_mmr_sino3d_create.argtypes = [ctypes.c_char_p, _i, _i, _i, _i, _vp, _vp, _vp, _vp]
+        L.ref_mmr_sino3d_create.restype = _vp
+        L.ref_mmr_tables.argtypes = [_vp, _vp, _vp]
+        L.ref_mmr_project.argtypes = [_vp, _i, _i, _i, _f, _f, _f, _vp, _vp]
+        L.ref_mmr_backproject.argtypes = [_vp, _i, _i, _i, _f, _f, _f, _vp, _vp]
         self._tmp = tempfile.mkdtemp(prefix="apirl_ref_")
 
     def set_threads(self, n):
@@ -338,6 +367,37 @@ class RefHarness:
         assert self.L.ref_sampled_3d(h, ns, nas, int(multi), mode, subset, nsub, *_img_args(ig), _p(vin), _p(vest),
                                      _p(out)) == 0
         return out
+
+    # ---- Siemens mMR (whole sinogram only) ------------------------------------
+    def mmr_sino3d(self, sg, data=None):
+        d = tempfile.mkdtemp(dir=self._tmp)
+        nsin = np.ascontiguousarray(sg.sinos_per_segment, np.int32)
+        mn = np.ascontiguousarray(sg.min_rd, np.int32)
+        mx = np.ascontiguousarray(sg.max_rd, np.int32)
+        dat = None if data is None else np.ascontiguousarray(data, np.float32)
+        h = self.L.ref_mmr_sino3d_create(d.encode(), sg.n_proj, sg.n_r, sg.n_rings, len(mn), _p(nsin), _p(mn),
+                                         _p(mx), _p(dat))
+        if not h:
+            raise RuntimeError("reference failed to read the mMR sinogram header")
+        return h
+
+    def mmr_tables(self, h, sg):
+        lor = np.zeros((sg.n_proj, sg.n_r, 4), np.float32)
+        z = np.zeros((sg.n_sinos, 2), np.float32)
+        assert self.L.ref_mmr_tables(h, _p(lor), _p(z)) == sg.n_sinos
+        return lor, z
+
+    def mmr_project(self, h, sg, ig, img):
+        img = np.ascontiguousarray(img, np.float32)
+        out = np.zeros(sg.n_bins, np.float32)
+        self.L.ref_mmr_project(h, *_img_args(ig), _p(img), _p(out))
+        return out
+
+    def mmr_backproject(self, h, sg, ig, values):
+        values = np.ascontiguousarray(values, np.float32)
+        img = np.zeros(ig.n_voxels, np.float32)
+        self.L.ref_mmr_backproject(h, *_img_args(ig), _p(values), _p(img))
+        return img
 
     def osem_subiteration(self, h, ig, subset, nsub, x, sens):
         lik = np.zeros(1, np.float32)

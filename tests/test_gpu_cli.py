@@ -190,3 +190,29 @@ def test_mlem2d_command(tmp_path):
     got = read_data(str(tmp_path / "r2_final"), ig.n_voxels)
     want, _, _ = ap.mlem_2d(ig, sg, meas, np.ones(ig.n_voxels, np.float32), 5)
     assert np.linalg.norm(got - want) / np.linalg.norm(want) <= 1e-5
+
+
+def test_osem_command_mmr(tmp_path):
+    """input type := Sinogram3DSiemensMmr (cmd/src/OSEM.cpp:416-425)."""
+    d = tmp_path
+    sg = Sino3DGeom.mmr(36, 86, 8, 3, 4)
+    ig = ImageGeom(72, 72, 16, 8.35, 8.35, 16.25)
+    rng = np.random.default_rng(8)
+    x = (rng.random(ig.n_voxels, dtype=np.float32) + 0.5).astype(np.float32)
+    P = ap.SiddonProjector(ig, sg)
+    est = torch.zeros(sg.n_bins, dtype=torch.float32, device=DEV)
+    P.project(torch.from_numpy(x).to(DEV), est)
+    meas = rng.poisson(est.cpu().numpy() * 0.2).astype(np.float32)
+    write_image(str(d / "ones"), ig, np.ones(ig.n_voxels, np.float32))
+    write_sino3d(str(d / "meas"), sg, meas)
+    keys = {"input type": "Sinogram3DSiemensMmr", "input file": "meas.h33", "initial estimate": "ones.h33",
+            "output filename prefix": "rec", "number of iterations": 2, "number of subsets": 4,
+            "forwardprojector": "Siddon", "backprojector": "Siddon"}
+    with open(d / "osem.par", "w") as f:
+        f.write("OSEM Parameters :=\n" + "".join(f"{k} := {v}\n" for k, v in keys.items()) + "END :=\n")
+    run("OSEM", str(d / "osem.par"), d)
+    got = read_data(str(d / "rec_final"), ig.n_voxels)
+    want, _, _ = ap.osem_3d(ig, sg, meas, np.ones(ig.n_voxels, np.float32), 2, 4)
+    ok = np.isfinite(want)
+    assert np.array_equal(np.isfinite(got), ok)
+    assert np.linalg.norm(got[ok] - want[ok]) / np.linalg.norm(want[ok]) <= 1e-5
