@@ -196,7 +196,9 @@ def test_osem_command_mmr(tmp_path):
     """input type := Sinogram3DSiemensMmr (cmd/src/OSEM.cpp:416-425)."""
     d = tmp_path
     sg = Sino3DGeom.mmr(36, 86, 8, 3, 4)
-    ig = ImageGeom(72, 72, 16, 8.35, 8.35, 16.25)
+    # every voxel crossed by rays of every subset (no zero sensitivity, which
+    # with the reference's threshold 0 and >= would give NaN)
+    ig = ImageGeom(48, 48, 14, 8.35, 8.35, 16.25)
     rng = np.random.default_rng(8)
     x = (rng.random(ig.n_voxels, dtype=np.float32) + 0.5).astype(np.float32)
     P = ap.SiddonProjector(ig, sg)
@@ -213,6 +215,5 @@ def test_osem_command_mmr(tmp_path):
     run("OSEM", str(d / "osem.par"), d)
     got = read_data(str(d / "rec_final"), ig.n_voxels)
     want, _, _ = ap.osem_3d(ig, sg, meas, np.ones(ig.n_voxels, np.float32), 2, 4)
-    ok = np.isfinite(want)
-    assert np.array_equal(np.isfinite(got), ok)
-    assert np.linalg.norm(got[ok] - want[ok]) / np.linalg.norm(want[ok]) <= 1e-5
+    assert np.all(np.isfinite(want))
+    assert np.linalg.norm(got - want) / np.linalg.norm(want) <= 1e-5
