@@ -105,6 +105,7 @@ SIGNATURES = {
     "apirl_mlem_3d": (_i, [ctypes.POINTER(ImageGeomC), ctypes.POINTER(Sino3DGeomC), _vp, _vp, _vp, _vp, _i, _i,
                            _vp, _vp, _vp, ctypes.POINTER(SamplingC)]),
     "apirl_projector_set_sampling": (_i, [_vp, _i, _i, _i]),
+    "apirl_projector_set_shard": (_i, [_vp, _i, _i]),
     "apirl_job_footprint": (_i64, [ctypes.POINTER(JobDescC)]),
     "apirl_batch_create": (_i, [_i, _i64, ctypes.POINTER(_vp)]),
     "apirl_batch_destroy": (None, [_vp]),

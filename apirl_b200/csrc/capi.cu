@@ -327,7 +327,7 @@ int64_t apirl_projector_num_bins(const apirl_projector* p, int subset, int nsubs
   return (int64_t)p->t.n_sinos * s.nk * p->t.n_r;
 }
 
-int apirl_projector_num_sinograms(const apirl_projector* p) { return p ? p->t.n_sinos : -1; }
+int apirl_projector_num_sinograms(const apirl_projector* p) { return p ? p->host.n_sinos : -1; }
 
 apirl_status apirl_projector_tables(const apirl_projector* p, float* h_lor, float* h_z) {
   if (!p) return fail(APIRL_ERR_INVALID, "null projector");
@@ -421,6 +421,18 @@ apirl_status apirl_projector_set_sampling(apirl_projector* p, int n_samples, int
   p->n_samples = n_samples;
   p->n_axial_samples = n_axial_samples;
   p->multi_lors = multiple_lors_per_bin != 0;
+  return APIRL_OK;
+}
+
+apirl_status apirl_projector_set_shard(apirl_projector* p, int first_sinogram, int n_sinograms) {
+  if (!p) return fail(APIRL_ERR_INVALID, "null projector");
+  const int total = p->host.n_sinos;
+  if (first_sinogram < 0 || n_sinograms < 1 || first_sinogram + n_sinograms > total)
+    return fail(APIRL_ERR_INVALID, "shard %d + %d outside the %d sinograms", first_sinogram, n_sinograms, total);
+  p->t.g0 = first_sinogram;
+  p->t.n_sinos = n_sinograms;
+  p->t_dab.g0 = first_sinogram;
+  p->t_dab.n_sinos = n_sinograms;
   return APIRL_OK;
 }
 

@@ -13,8 +13,11 @@ struct LorTable {
   const float4* lor;    // [n_proj][n_r] = (p1x, p1y, p2x, p2y)
   const float2* z;      // 3D: [n_sinos] = (z1, z2) end-point z; 2D: unused
   const uint8_t* ok;    // 2D: [n_r] 1 when r <= sinogram rFov (getPointsFromLor); 3D: unused
-  int n_proj, n_r, n_sinos;
+  int n_proj, n_r, n_sinos;  // n_sinos: sinograms of the shard the kernels cover
   int is3d;
+  // First sinogram of the shard (apirl_projector_set_shard): bins cover
+  // sinograms g0 .. g0 + n_sinos - 1 of the whole sinogram.
+  int g0 = 0;
   // Several rays per bin (3D; set when lor_s is not null): a bin is the sum
   // over its rays, in the order ring pair m, radial sample o, axial sample q,
   // with end points lor_s[(a * n_r + l) * n_rs + o] and zs[zoff[g] + m * n_as + q].

@@ -41,8 +41,9 @@ struct BinPos {
 __device__ __forceinline__ BinPos decode(int64_t b, const LorTable& t, const SubsetSel& s) {
   BinPos p;
   const int64_t per = (int64_t)s.nk * t.n_r;
-  p.g = (int)(b / per);
-  const int rem = (int)(b - (int64_t)p.g * per);
+  const int gl = (int)(b / per);  // sinogram within the shard
+  const int rem = (int)(b - (int64_t)gl * per);
+  p.g = t.g0 + gl;
   p.k = rem / t.n_r;
   p.l = rem - p.k * t.n_r;
   p.a = s.subset < 0 ? p.k : s.subset + s.nsub * p.k;
@@ -306,7 +307,7 @@ __global__ void __launch_bounds__(kBlock, kEmMinBlocks) k_em_pass(ImgGeom g, Lor
   double term = 0.0;
   if (b < total) {
     const BinPos p = decode(b, t, s);
-    const int64_t row = counts_packed ? ((int64_t)p.g * s.nk + p.k) : ((int64_t)p.g * t.n_proj + p.a);
+    const int64_t row = counts_packed ? ((int64_t)(p.g - t.g0) * s.nk + p.k) : ((int64_t)p.g * t.n_proj + p.a);
     const int64_t ci = row * t.n_r + p.l;
     const float m = load_count<CT>(counts, ci);
     const float4 L = t.lor[(int64_t)p.a * t.n_r + p.l];
@@ -401,7 +402,7 @@ __global__ void __launch_bounds__(kBlock) k_em_pass_rays(ImgGeom g, LorTable t, 
   double term = 0.0;
   if (b < total) {
     const BinPos p = decode(b, t, s);
-    const int64_t row = counts_packed ? ((int64_t)p.g * s.nk + p.k) : ((int64_t)p.g * t.n_proj + p.a);
+    const int64_t row = counts_packed ? ((int64_t)(p.g - t.g0) * s.nk + p.k) : ((int64_t)p.g * t.n_proj + p.a);
     const int64_t ci = row * t.n_r + p.l;
     const float m = load_count<CT>(counts, ci);
     float e = rays_sum3(g, t, p, x);
@@ -453,7 +454,7 @@ __global__ void __launch_bounds__(kBlock) k_zero_bins(ImgGeom g, LorTable t, Sub
   double term = 0.0;
   if (b < total) {
     const BinPos p = decode(b, t, s);
-    const int64_t row = counts_packed ? ((int64_t)p.g * s.nk + p.k) : ((int64_t)p.g * t.n_proj + p.a);
+    const int64_t row = counts_packed ? ((int64_t)(p.g - t.g0) * s.nk + p.k) : ((int64_t)p.g * t.n_proj + p.a);
     const int64_t ci = row * t.n_r + p.l;
     if (load_count<CT>(counts, ci) == 0.f) {
       if (add) term = (double)__ldg(add + ci);

@@ -118,6 +118,10 @@ class SiddonProjector:
         check(self.lib.apirl_projector_set_sampling(self.h, int(n_samples), int(n_axial_samples),
                                                     int(bool(multiple_lors_per_bin))))
 
+    def set_shard(self, first_sinogram, n_sinograms):
+        """Restrict every operation to sinograms [first, first + n) of the whole sinogram."""
+        check(self.lib.apirl_projector_set_shard(self.h, int(first_sinogram), int(n_sinograms)))
+
     def set_option(self, option, value):
         check(self.lib.apirl_projector_set_option(self.h, int(option), int(value)))
 

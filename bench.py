@@ -182,6 +182,92 @@ def whole_job_value(steps, local_ms, world, dist=None, device=None):
     return steps * world / (total_ms / 1e3), total_ms
 
 
+def run_sharded(args):
+    """--shard: ONE reconstruction split over the ranks by LOR shards
+    (apirl_b200.sharded): each sub-iteration is the fused pass over the rank's
+    sinograms, an NCCL all-reduce of the backprojection image and of the
+    likelihood, and the pixel update.  value = the job's sub-iterations over
+    the slowest rank's time (strong scaling)."""
+    import datetime
+    import torch
+    import torch.distributed as dist
+    from apirl_b200.sharded import shard_ranges, ShardedOsem, GpuShard
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    if world > 1:
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    dev = torch.device(f"cuda:{local}")
+    log = (lambda m: print(f"[bench] {m}", file=sys.stderr, flush=True)) if rank == 0 else (lambda m: None)
+    import apirl_b200 as ap
+    from apirl_b200 import _lib as _l
+    ap.load_library()
+    w = setup_workload(dev, log)
+    ig, sg = w["ig"], w["sg"]
+    first, n = shard_ranges(sg.n_sinos, world)[rank]
+    backend = GpuShard(ig, sg, w["counts"], NSUB, first, n, device=local, mult=w["atten"])
+    backend.P.set_option(_l.APIRL_OPT_KERNEL_TIMING, 1)
+    job = ShardedOsem(backend, NSUB, dist if world > 1 else None)
+    job.compute_sensitivity()
+    # algorithmic bytes of the fused kernel on this rank's shard, per subset
+    cv = w["counts"].view(torch.int32).view(sg.n_sinos, sg.n_proj, sg.n_r)[first:first + n]
+    shard_bytes = []
+    for s_ in range(NSUB):
+        st = backend.P.count_steps(s_, NSUB).view(n, -1, sg.n_r).long()
+        fwd, bwd = int(st.sum().item()), int(st[cv[:, s_::NSUB, :] != 0].sum().item())
+        shard_bytes.append(4 * fwd + 8 * bwd + 4 * st.numel())
+    x = torch.ones(ig.n_voxels, dtype=torch.float32, device=dev)
+    flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.float32, device=dev)
+    for i in range(args.warmup):
+        job.subiteration(x, i % NSUB)
+    torch.cuda.synchronize(dev)
+    if world > 1:
+        dist.barrier()
+    clocks = ClockSampler(local)
+    clocks.start()
+    evs = [[torch.cuda.Event(enable_timing=True) for _ in range(2)] for _ in range(args.steps)]
+    kern = []
+    for i in range(args.steps):
+        flush.zero_()
+        evs[i][0].record()
+        job.subiteration(x, (args.warmup + i) % NSUB)
+        evs[i][1].record()
+        kern.append(backend.P.last_kernel_ms())
+    torch.cuda.synchronize(dev)
+    if world > 1:
+        dist.barrier()
+    clock = clocks.stop()
+    local_ms = sum(e[0].elapsed_time(e[1]) for e in evs)
+    t = torch.tensor([local_ms], dtype=torch.float64, device=dev)
+    if world > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    total_ms = float(t.item())
+    value = args.steps / (total_ms / 1e3)
+    if rank == 0:
+        peak, peak_kind = peaks()
+        subs = [(args.warmup + i) % NSUB for i in range(args.steps)]
+        achieved = statistics.mean(shard_bytes[s_] for s_ in subs) / (statistics.mean(kern) / 1e3) / 1e9
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True,
+            "scaling": "strong", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded phantom, Poisson counts)",
+            "config": {"workload": WORKLOAD, "subsets": NSUB, "counts_dtype": "uint32",
+                       "parallelism": f"LOR shards x{world} (sinograms {first}..{first + n - 1} on rank 0), "
+                                      "NCCL all-reduce of the backprojection image and likelihood",
+                       "l2": "flushed between timed steps (256 MB write outside the timed events)"},
+            "roofline": {"bound": "hbm", "kernel": "k_em_pass on rank 0's shard",
+                         "kernel_ms": statistics.mean(kern), "peak": peak, "unit": "GB/s",
+                         "peak_source": f"{peak_kind} hbm_gbs",
+                         "achieved": achieved, "frac": achieved / peak, "traffic": None},
+            "e2e": None, "cpu_baseline": None, "gpu_launches": 5 * args.steps, "clocks": clock,
+        }
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
 def run_gpu(args):
     import torch
     import torch.distributed as dist
@@ -599,6 +685,8 @@ def main():
     ap_.add_argument("--pass", dest="pass_form", default="full", choices=["sparse", "full"],
                      help="sparse: bins with zero counts are not walked (their likelihood terms from per-subset "
                           "zero-count images computed inside the timed region); full: every bin walked")
+    ap_.add_argument("--shard", action="store_true",
+                     help="one job split over the ranks by LOR shards (strong scaling) instead of replicas")
     ap_.add_argument("--alpha", default="f32", choices=["f32", "f64"],
                      help="walk geometry: f32 = the reference's float arithmetic (headline); f64 = precision mode")
     ap_.add_argument("--cpu-threads", type=int, default=None,
@@ -617,6 +705,8 @@ def main():
         args.warmup = 3
     if args.impl == "reference":
         run_reference(args)
+    elif args.shard:
+        run_sharded(args)
     elif args.workload in ("batched", "served"):
         run_batched(args, served=args.workload == "served")
     else:

@@ -124,8 +124,10 @@ apirl_status apirl_projector_create_3d_mmr(const apirl_image_geom* img, int n_pr
 /* The mMR LOR end-point table on the host ([angle][r][p1x,p1y,p2x,p2y]). */
 apirl_status apirl_mmr_lor_table(int n_proj, int n_r, float* h_lor);
 void apirl_projector_destroy(apirl_projector* p);
-/* Bins of one subset (subset < 0: whole sinogram). */
+/* Bins of one subset (subset < 0: all angles) of the projector's sinograms
+ * (its shard, when one is set). */
 int64_t apirl_projector_num_bins(const apirl_projector* p, int subset, int nsubsets);
+/* Sinograms of the whole sinogram (independent of a shard). */
 int apirl_projector_num_sinograms(const apirl_projector* p);
 /* Copies the host-built LOR table ([angle][r][p1x,p1y,p2x,p2y]) and, for 3D,
  * the per-sinogram end-point z ([sinogram][z1,z2]); either may be NULL. */
@@ -154,6 +156,16 @@ apirl_status apirl_projector_set_alpha_precision(apirl_projector* p, int mode);
 #define APIRL_MAX_SAMPLES 64
 apirl_status apirl_projector_set_sampling(apirl_projector* p, int n_samples, int n_axial_samples,
                                          int multiple_lors_per_bin);
+/* Restricts the projector to the sinograms first .. first + n - 1 of the
+ * whole sinogram (a LOR shard, for splitting one reconstruction over several
+ * GPUs; no counterpart in the reference).  Every operation then covers the
+ * shard's bins only: subset and packed sinograms (projections, backprojection
+ * inputs, packed counts) hold the shard's sinograms, while whole-sinogram
+ * layouts (counts_packed = 0, d_add, multiplicative factors) stay indexed by
+ * the global sinogram.  Backprojections and the likelihood are then partial
+ * sums over the shard, to be summed over the shards (all-reduce) before the
+ * pixel update.  (0, all sinograms) restores the whole sinogram. */
+apirl_status apirl_projector_set_shard(apirl_projector* p, int first_sinogram, int n_sinograms);
 /* Tuning and instrumentation options (no counterpart in the reference).
  * APIRL_OPT_DUAL_LAYOUT (default 1): the fused 3D pass keeps the image and
  *   the backprojection in two padded layouts, [z][y][x] and [z][x][y], each

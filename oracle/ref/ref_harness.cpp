@@ -620,7 +620,7 @@ int ref_osem_3d(void* hv, int nx, int ny, int nz, float dx, float dy, float dz, 
 // ---- Siemens mMR ------------------------------------------------------------
 // Sinogram3DSiemensMmr read from an interfile header (the reference's own
 // constructor, data/src/Sinogram3DSiemensMmr.cpp); no subsets are taken of it
-// (getSubset copies nProj angles into a one-float buffer, :183).
+// (getSubset copies nProj angles into a one-float buffer, :184).
 void* ref_mmr_sino3d_create(const char* tmpdir, int nProj, int nR, int nRings, int nSeg, const int* nSinos,
                             const int* minRD, const int* maxRD, const float* data) {
   std::string hdr = write_sino3d_header(tmpdir, nProj, nR, nRings, nSeg, nSinos, minRD, maxRD, data);
