@@ -248,10 +248,13 @@ apirl_status apirl_force_positive(int64_t n, float* d_x, void* stream);
 /* ---- fused EM pass --------------------------------------------------------
  * One OSEM sub-iteration of OsemSinogram3d::Reconstruct
  * (recon/src/OsemSinogram3d.cpp:159-237) -- or one MLEM iteration of
- * Mlem2d::Reconstruct (recon/src/Mlem2d.cpp:146-185) for a 2D projector -- in
- * two kernels: per bin, project the ray through d_x, add d_add, add the
- * likelihood term, form the ratio m / e and backproject it into d_bp; then
- * update d_x with d_sens and clear d_bp.  No estimated sinogram is stored.
+ * Mlem2d::Reconstruct (recon/src/Mlem2d.cpp:146-185) for a 2D projector.
+ * One fused kernel does, per bin: project the ray through d_x, add d_add, add
+ * the likelihood term, form the ratio m / e and backproject it; a second
+ * kernel updates d_x with d_sens (3D projectors with the default layout also
+ * copy d_x into their padded layouts first and fold the backprojection back
+ * from them; the likelihood is a deterministic two-level FP64 sum).  No
+ * estimated sinogram is stored.
  *   d_counts : measured sinogram, element type counts_dtype; counts_packed = 0
  *              means the whole sinogram (angles indexed as in the full
  *              sinogram), 1 means the subset sinogram only.
