@@ -20,6 +20,7 @@ APIRL_ERR_ABORTED = 5
 APIRL_OPT_DUAL_LAYOUT = 1
 APIRL_OPT_KERNEL_TIMING = 2
 APIRL_OPT_EM_BLOCK = 3
+APIRL_OPT_PERSISTENT = 4
 
 APIRL_ALPHA_F32 = 0
 APIRL_ALPHA_F64 = 1

@@ -141,6 +141,7 @@ apirl_status finish_create(apirl_projector* p, apirl_projector** out) {
   CK(cudaMalloc(&p->d_partials, p->n_partials * sizeof(double)));
   CK(cudaMalloc(&p->d_minmax, 2 * sizeof(unsigned)));
   CK(cudaMalloc(&p->d_scalars, 8 * sizeof(double)));
+  CK(cudaMalloc(&p->d_chunk, sizeof(unsigned long long)));
   if (p->is3d && p->dual_layout) {
     const apirl_status st = alloc_pad(p);
     if (st) return st;
@@ -305,6 +306,7 @@ void apirl_projector_destroy(apirl_projector* p) {
   cudaFree(p->d_partials);
   cudaFree(p->d_minmax);
   cudaFree(p->d_scalars);
+  cudaFree(p->d_chunk);
   cudaFree(p->d_lor64);
   cudaFree(p->d_z64);
   for (int k = 0; k < 2; k++) {
@@ -565,7 +567,7 @@ apirl_status fused(apirl_projector* p, SubsetSel ss, const void* d_counts, int d
   }
   CK(apirl::launch_em_pass(p->g, p->t, ss, d_counts, dtype, packed, d_add, d_x, d_bp, 1, p->is3d ? 0 : 1,
                            p->d_partials, d_lik, s, p->pg, dual ? p->pad : apirl::PadBuffers(), p->em_block,
-                           d_zimg, d_zero_add));
+                           d_zimg, d_zero_add, p->persistent ? p->d_chunk : nullptr));
   if (p->timing) {
     CK(cudaEventRecord(p->ev1, s));
     p->timed = 1;
@@ -681,6 +683,7 @@ apirl_status apirl_projector_set_option(apirl_projector* p, int option, int valu
       return APIRL_OK;
     }
     case APIRL_OPT_KERNEL_TIMING: p->timing = value != 0; p->timed = 0; return APIRL_OK;
+    case APIRL_OPT_PERSISTENT: p->persistent = value != 0; return APIRL_OK;
     case APIRL_OPT_EM_BLOCK:
       if (value < 32 || value > 256 || value % 32) return fail(APIRL_ERR_INVALID, "block size must be 32..256, x32");
       p->em_block = value;

@@ -106,7 +106,7 @@ cudaError_t launch_em_pass(const ImgGeom& g, const LorTable& t, SubsetSel s, con
                            int counts_packed, const float* add, const float* x, float* bp, int back, int lik_mode,
                            double* partials, double* lik, cudaStream_t st, const PreciseGeom& pg = PreciseGeom(),
                            const PadBuffers& pad = PadBuffers(), int block = 0, const float* zimg = nullptr,
-                           const double* zero_add = nullptr);
+                           const double* zero_add = nullptr, unsigned long long* persist_counter = nullptr);
 // Sparse pass (zimg set, 3D float walk): bins with zero counts are not walked;
 // the likelihood subtracts x . zimg + *zero_add instead of their estimates.
 // zimg = A_s^T 1[m == 0] and zero_add = sum of those bins' additive terms,
@@ -200,6 +200,8 @@ struct apirl_projector {
   apirl::PadBuffers pad;         // padded two-layout copies of the fused pass (3D), interiors of bA/bT zero
   int timing = 0;                // record CUDA events around the fused kernel
   int em_block = 128;            // threads per block of the fused kernel (APIRL_OPT_EM_BLOCK / autotune)
+  int persistent = 1;            // APIRL_OPT_PERSISTENT: warps pull 32-bin chunks (padded 3D pass)
+  unsigned long long* d_chunk = nullptr;  // chunk counter of the persistent pass
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
   int timed = 0;                 // an event pair has been recorded
   int n_rings = 0;               // 3D geometry as given, for building the FP64 tables

@@ -417,6 +417,60 @@ __global__ void __launch_bounds__(kBlock) k_em_pass_rays(ImgGeom g, LorTable t, 
   if ((threadIdx.x & 31) == 0) partials[((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5] = term;
 }
 
+// The padded-layout fused pass as a persistent kernel: each warp takes the
+// next chunk of 32 consecutive bins from *chunk_counter until none are left,
+// so that warps never wait for the rest of their block and the SM keeps its
+// full complement of warps until the end of the pass.  The bins of a chunk
+// are those of one warp in k_em_pass, and the chunk's likelihood partial goes
+// to partials[chunk]: results are identical to k_em_pass's.
+template <typename CT>
+__global__ void __launch_bounds__(kBlock, kEmMinBlocks) k_em_pass_persist(
+    ImgGeom g, LorTable t, SubsetSel s, const CT* __restrict__ counts, int counts_packed,
+    const float* __restrict__ add, PadBuffers pad, int back, double* __restrict__ partials, int64_t total,
+    int skip_zero, unsigned long long* __restrict__ chunk_counter) {
+  const int lane = threadIdx.x & 31;
+  const int64_t nchunks = (total + 31) >> 5;
+  const int px = g.nx + 2 * kPad, py = g.ny + 2 * kPad;
+  const int uz = px * py;
+  for (;;) {
+    unsigned long long c = 0;
+    if (lane == 0) c = atomicAdd(chunk_counter, 1ULL);
+    c = __shfl_sync(0xffffffffu, c, 0);
+    if ((int64_t)c >= nchunks) break;
+    const int64_t b = (int64_t)c * 32 + lane;
+    double term = 0.0;
+    if (b < total) {
+      const BinPos p = decode(b, t, s);
+      const int64_t row = counts_packed ? ((int64_t)(p.g - t.g0) * s.nk + p.k) : ((int64_t)p.g * t.n_proj + p.a);
+      const int64_t ci = row * t.n_r + p.l;
+      const float m = load_count<CT>(counts, ci);
+      if (!(skip_zero && m == 0.f)) {
+        const float4 L = t.lor[(int64_t)p.a * t.n_r + p.l];
+        const float2 z = t.z[p.g];
+        const float vx = A_SUB(L.z, L.x), vy = A_SUB(L.w, L.y);
+        const bool tr = fabsf(vx) >= fabsf(vy);
+        const int ux = tr ? py : 1, uy = tr ? 1 : px;
+        Walk3 w;
+        siddon3_setup(L.x, L.y, z.x, vx, vy, A_SUB(z.y, z.x), g, w);
+        float e = siddon3_gather_pad(w, g, ux, uy, uz, pad.lim, tr ? pad.pT : pad.pA);
+        if (add) e = A_ADD(e, __ldg(add + ci));
+        const float r = (m != 0.f && e != 0.f) ? A_DIV(m, e) : 0.f;
+        if (e != 0.f) term = (double)m * log((double)e) - (double)e;
+        if (back && r != 0.f) {
+          const float4 L2 = __ldcg(t.lor + (int64_t)p.a * t.n_r + p.l);
+          const float2 z2 = __ldcg(t.z + p.g);
+          Walk3 w2;
+          siddon3_setup(L2.x, L2.y, z2.x, A_SUB(L2.z, L2.x), A_SUB(L2.w, L2.y), A_SUB(z2.y, z2.x), g, w2);
+          siddon3_scatter_pad(w2, g, ux, uy, uz, pad.lim, r, tr ? pad.bT : pad.bA);
+        }
+      }
+    }
+    #pragma unroll
+    for (int o = 16; o > 0; o >>= 1) term += __shfl_down_sync(0xffffffffu, term, o);
+    if (lane == 0) partials[c] = term;
+  }
+}
+
 // Deterministic final sum of per-block partials (one block).
 __global__ void k_sum_partials(const double* __restrict__ partials, int64_t n, double* __restrict__ out) {
   double v = 0.0;
@@ -840,7 +894,8 @@ cudaError_t launch_count_steps(const ImgGeom& g, const LorTable& t, SubsetSel s,
 cudaError_t launch_em_pass(const ImgGeom& g, const LorTable& t, SubsetSel s, const void* counts, int counts_dtype,
                            int counts_packed, const float* add, const float* x, float* bp, int back, int lik_mode,
                            double* partials, double* lik, cudaStream_t st, const PreciseGeom& pg,
-                           const PadBuffers& pad, int block, const float* zimg, const double* zero_add) {
+                           const PadBuffers& pad, int block, const float* zimg, const double* zero_add,
+                           unsigned long long* persist_counter) {
   const int64_t total = (int64_t)t.n_sinos * s.nk * t.n_r;
   if (block < 32 || block > kBlock || block % 32) block = kBlock;
   const unsigned grid = (unsigned)((total + block - 1) / block);
@@ -865,6 +920,54 @@ cudaError_t launch_em_pass(const ImgGeom& g, const LorTable& t, SubsetSel s, con
                                                            x, bp, PadBuffers(), back, lik_mode, partials,     \
                                                            total, 0);                                         \
   } while (0)
+  if (persist_counter && t.is3d && !t.lor_s && !pg.enabled && pad.pA && lik_mode == 0) {
+    // Persistent form: as many blocks as fit on the SMs at once.
+    static int resident[3] = {0, 0, 0};
+    const int ti = counts_dtype == APIRL_F32 ? 0 : (counts_dtype == APIRL_U32 ? 1 : 2);
+    if (!resident[ti]) {
+      int per_sm = 0, dev = 0, sms = 0;
+      cudaError_t oe = counts_dtype == APIRL_F32
+          ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_em_pass_persist<float>, block, 0)
+          : (counts_dtype == APIRL_U32
+                 ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_em_pass_persist<uint32_t>, block, 0)
+                 : cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_em_pass_persist<uint16_t>, block, 0));
+      if (oe != cudaSuccess) return oe;
+      cudaGetDevice(&dev);
+      cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+      resident[ti] = (per_sm < 1 ? 1 : per_sm) * sms;
+    }
+    const int64_t chunks = (total + 31) / 32;
+    const int64_t need = (chunks * 32 + block - 1) / block;
+    const unsigned pgrid = (unsigned)(need < resident[ti] ? need : resident[ti]);
+    cudaError_t me = cudaMemsetAsync(persist_counter, 0, sizeof(unsigned long long), st);
+    if (me != cudaSuccess) return me;
+    switch (counts_dtype) {
+      case APIRL_F32:
+        k_em_pass_persist<float><<<pgrid, block, 0, st>>>(g, t, s, (const float*)counts, counts_packed, add, pad,
+                                                          back, partials, total, zimg != nullptr, persist_counter);
+        break;
+      case APIRL_U32:
+        k_em_pass_persist<uint32_t><<<pgrid, block, 0, st>>>(g, t, s, (const uint32_t*)counts, counts_packed, add,
+                                                             pad, back, partials, total, zimg != nullptr,
+                                                             persist_counter);
+        break;
+      case APIRL_U16:
+        k_em_pass_persist<uint16_t><<<pgrid, block, 0, st>>>(g, t, s, (const uint16_t*)counts, counts_packed, add,
+                                                             pad, back, partials, total, zimg != nullptr,
+                                                             persist_counter);
+        break;
+      default: return cudaErrorInvalidValue;
+    }
+    cudaError_t pe = cudaGetLastError();
+    if (pe != cudaSuccess || !lik) return pe;
+    int64_t np = chunks;
+    if (zimg) {
+      const int64_t nv = (int64_t)g.nx * g.ny * g.nz;
+      k_neg_dot<<<kSumLevel2, kBlock, 0, st>>>(x, zimg, nv, zero_add, partials + np);
+      np += kSumLevel2;
+    }
+    return launch_sum(partials, np, lik, st);
+  }
   static bool carveout_set = false;  // prefer L1 over shared memory: the kernel uses none
   if (!carveout_set) {
     cudaFuncSetAttribute(k_em_pass<float, true, false>, cudaFuncAttributePreferredSharedMemoryCarveout, 0);
@@ -882,7 +985,9 @@ cudaError_t launch_em_pass(const ImgGeom& g, const LorTable& t, SubsetSel s, con
 #undef APIRL_EM
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess || !lik) return e;
-  int64_t np = (int64_t)grid * (block / 32);
+  // One partial per 32 bins, whatever the block size (warps past the last
+  // bin wrote zeros behind them): the same sum for every block size.
+  int64_t np = (total + 31) / 32;
   if (zimg) {
     // - sum of the zero-count bins' estimates: - x . zimg - sum of their additive terms.
     const int64_t nv = (int64_t)g.nx * g.ny * g.nz;

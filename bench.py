@@ -300,6 +300,7 @@ def run_gpu(args):
     torch.cuda.synchronize(dev)
     log(f"autotuned fused-kernel block size: {best_block}")
     P.set_option(_l.APIRL_OPT_KERNEL_TIMING, 1)
+    P.set_option(_l.APIRL_OPT_PERSISTENT, args.persistent)
 
     sparse = args.pass_form == "sparse"
     zimg = torch.zeros((NSUB, w["ig"].n_voxels), dtype=torch.float32, device=dev) if sparse else None
@@ -434,7 +435,7 @@ def run_gpu(args):
             "config": {"workload": WORKLOAD if args.max_ring_diff is None else
                        WORKLOAD + f" (profiling case: segments |rd| <= {args.max_ring_diff} only)",
                        "subsets": NSUB, "counts_dtype": "uint32", "em_block": best_block,
-                       "alpha": args.alpha,
+                       "alpha": args.alpha, "persistent": args.persistent,
                        "pass": ("sparse: bins with zero counts not walked, their likelihood terms -x.Z_s from "
                                 "per-subset zero-count images Z_s = A_s^T 1[m=0], all 21 computed inside the "
                                 "timed region and amortized over the timed sub-iterations") if sparse else
@@ -446,8 +447,10 @@ def run_gpu(args):
                          "frac": achieved / peak,
                          "traffic": args.traffic_bytes if args.traffic_bytes is not None else
                          (FULL_TRAFFIC_BYTES if args.max_ring_diff is None else None),
-                         "kernel": "k_em_pass (fused projection / ratio / backprojection)",
-                         "timing": "CUDA events recorded by the library around the kernel, same stream",
+                         "kernel": ("k_em_pass_persist" if args.persistent and args.alpha == "f32" else "k_em_pass")
+                                   + " (fused projection / ratio / backprojection)",
+                         "timing": "CUDA events recorded by the library on the launching stream around the fused "
+                                   "kernel and its two small likelihood-sum kernels",
                          "algorithmic_bytes_per_launch": kern_bytes, "kernel_ms": kern_s * 1e3,
                          "peak_source": f"{peak_kind} hbm_gbs"},
             "e2e": e2e,
@@ -685,6 +688,8 @@ def main():
     ap_.add_argument("--pass", dest="pass_form", default="full", choices=["sparse", "full"],
                      help="sparse: bins with zero counts are not walked (their likelihood terms from per-subset "
                           "zero-count images computed inside the timed region); full: every bin walked")
+    ap_.add_argument("--persistent", type=int, default=1, choices=[0, 1],
+                     help="1: the fused pass as a persistent kernel whose warps pull 32-bin chunks")
     ap_.add_argument("--shard", action="store_true",
                      help="one job split over the ranks by LOR shards (strong scaling) instead of replicas")
     ap_.add_argument("--alpha", default="f32", choices=["f32", "f64"],

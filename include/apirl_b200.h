@@ -177,8 +177,11 @@ apirl_status apirl_projector_set_shard(apirl_projector* p, int first_sinogram, i
  * APIRL_OPT_KERNEL_TIMING (default 0): record CUDA events around the fused
  *   kernel of every pass; apirl_projector_kernel_ms returns the last one.
  * APIRL_OPT_EM_BLOCK (default 128): threads per block of the fused kernel
- *   (32..256, a multiple of 32). */
-enum { APIRL_OPT_DUAL_LAYOUT = 1, APIRL_OPT_KERNEL_TIMING = 2, APIRL_OPT_EM_BLOCK = 3 };
+ *   (32..256, a multiple of 32).
+ * APIRL_OPT_PERSISTENT (default 1): the padded 3D pass runs as a persistent
+ *   kernel whose warps pull chunks of 32 bins from a counter (identical
+ *   results; the SMs keep their warps busy to the end of the pass). */
+enum { APIRL_OPT_DUAL_LAYOUT = 1, APIRL_OPT_KERNEL_TIMING = 2, APIRL_OPT_EM_BLOCK = 3, APIRL_OPT_PERSISTENT = 4 };
 apirl_status apirl_projector_set_option(apirl_projector* p, int option, int value);
 apirl_status apirl_projector_kernel_ms(apirl_projector* p, double* ms);
 /* Autotuner: times the fused kernel (apirl_em_project_backproject, `repeats`

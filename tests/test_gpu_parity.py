@@ -486,3 +486,29 @@ def test_osem_driver_sparse_long_job_vs_oracle(oracle):
     want, want_lik, _ = oracle.osem_3d(sg, ig, init, meas, 4, 4)
     assert rel(img, want) <= 1e-4
     assert np.allclose(lik[:-1], want_lik[:-1].astype(np.float64), rtol=1e-5)
+
+
+def test_persistent_pass_equals_plain_pass(oracle):
+    """APIRL_OPT_PERSISTENT: same bins per warp-chunk, same likelihood partials."""
+    from apirl_b200 import _lib
+    ig, sg = small_3d()
+    rng = np.random.default_rng(23)
+    x0 = (rng.random(ig.n_voxels, dtype=np.float32) + 0.5).astype(np.float32)
+    meas = rng.poisson(oracle.project_3d(sg, ig, x0) * 2).astype(np.uint32)
+    sens = (rng.random(ig.n_voxels, dtype=np.float32) + 1).astype(np.float32)
+    P = ap.SiddonProjector(ig, sg)
+    out = {}
+    for persistent in (0, 1):
+        P.set_option(_lib.APIRL_OPT_PERSISTENT, persistent)
+        for block in (64, 128, 256):
+            P.set_option(_lib.APIRL_OPT_EM_BLOCK, block)
+            x = t(x0)
+            bp = torch.zeros(ig.n_voxels, dtype=torch.float32, device=DEV)
+            lik = torch.zeros(1, dtype=torch.float64, device=DEV)
+            P.em_pass(t(meas), x, bp, t(sens), 3, 5, lik=lik)
+            torch.cuda.synchronize()
+            out[(persistent, block)] = (x.cpu().numpy(), lik.item())
+    ref_x, ref_lik = out[(0, 128)]
+    for k, (x, lik) in out.items():
+        assert rel(x, ref_x) <= 1e-6
+        assert lik == ref_lik  # per-chunk partials summed in the same order
