@@ -100,6 +100,7 @@ SIGNATURES = {
     "apirl_zero_count_image": (_i, [_vp, _vp, _i, _i, _vp, _vp, _vp, _i, _i, _vp]),
     "apirl_em_pass_sparse": (_i, [_vp, _vp, _i, _i, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _f, _i, _i, _i, _vp, _vp]),
     "apirl_em_project_backproject": (_i, [_vp, _vp, _i, _i, _vp, _vp, _vp, _i, _i, _vp, _vp]),
+    "apirl_stage_counts": (_i, [_vp, _vp, _i, _vp, _i, _i, _vp]),
     "apirl_em_pass_host": (_i, [_vp, _vp, _i, _vp, _vp, _vp, _vp, _vp, _vp, _f, _i, _i, _i, _vp, _vp, _vp]),
     "apirl_osem_3d": (_i, [ctypes.POINTER(ImageGeomC), ctypes.POINTER(Sino3DGeomC), _vp, _vp, _vp, _vp, _i, _i,
                            _i, _vp, _vp, _vp, ctypes.POINTER(SamplingC)]),

@@ -320,6 +320,10 @@ void apirl_projector_destroy(apirl_projector* p) {
   cudaFree(p->pad.bT);
   if (p->ev0) cudaEventDestroy(p->ev0);
   if (p->ev1) cudaEventDestroy(p->ev1);
+  if (p->copy_ready) cudaEventDestroy(p->copy_ready);
+  for (auto& e : p->staged)
+    if (e.done) cudaEventDestroy(e.done);
+  if (p->copy_stream) cudaStreamDestroy(p->copy_stream);
   delete p;
 }
 
@@ -745,18 +749,60 @@ apirl_status apirl_projector_kernel_ms(apirl_projector* p, double* ms) {
   return APIRL_OK;
 }
 
+apirl_status apirl_stage_counts(apirl_projector* p, const void* h_counts_subset, int counts_dtype, void* d_counts_stage,
+                                int subset, int nsubsets, void* stream) {
+  apirl_status st = check_subset(p, subset, nsubsets);
+  if (st) return st;
+  if (!h_counts_subset || !d_counts_stage) return fail(APIRL_ERR_INVALID, "null buffer");
+  if (counts_dtype != APIRL_F32 && counts_dtype != APIRL_U32 && counts_dtype != APIRL_U16)
+    return fail(APIRL_ERR_INVALID, "unknown counts dtype %d", counts_dtype);
+  const int64_t nb = apirl_projector_num_bins(p, subset, nsubsets);
+  const size_t esz = counts_dtype == APIRL_U16 ? 2 : 4;
+  DEVICE_SCOPE(p->device);
+  if (!p->copy_stream) {
+    CK(cudaStreamCreateWithFlags(&p->copy_stream, cudaStreamNonBlocking));
+    CK(cudaEventCreateWithFlags(&p->copy_ready, cudaEventDisableTiming));
+    for (auto& e : p->staged) CK(cudaEventCreateWithFlags(&e.done, cudaEventDisableTiming));
+  }
+  // A free slot, or the one staging the same device buffer (restaged).
+  apirl_projector::Staged* slot = nullptr;
+  for (auto& e : p->staged)
+    if (e.dev == d_counts_stage) slot = &e;
+  for (auto& e : p->staged)
+    if (!slot && !e.dev) slot = &e;
+  if (!slot) return fail(APIRL_ERR_INVALID, "more than 4 staged copies outstanding");
+  // The copy starts after the caller's stream's earlier work (which may still
+  // read d_counts_stage) and runs beside its later work.
+  CK(cudaEventRecord(p->copy_ready, (cudaStream_t)stream));
+  CK(cudaStreamWaitEvent(p->copy_stream, p->copy_ready, 0));
+  CK(cudaMemcpyAsync(d_counts_stage, h_counts_subset, nb * esz, cudaMemcpyHostToDevice, p->copy_stream));
+  CK(cudaEventRecord(slot->done, p->copy_stream));
+  slot->host = h_counts_subset;
+  slot->dev = d_counts_stage;
+  return APIRL_OK;
+}
+
 apirl_status apirl_em_pass_host(apirl_projector* p, const void* h_counts_subset, int counts_dtype,
                                 void* d_counts_stage, float* d_x, float* d_bp, const float* d_sens,
                                 const float* d_zimg, const double* d_zero_add, float thr_value, int ge, int subset,
                                 int nsubsets, float* h_x_out, double* h_lik, void* stream) {
   apirl_status st = check_subset(p, subset, nsubsets);
   if (st) return st;
-  if (!h_counts_subset || !d_counts_stage || !h_x_out) return fail(APIRL_ERR_INVALID, "null buffer");
+  if (!h_counts_subset || !d_counts_stage) return fail(APIRL_ERR_INVALID, "null buffer");
   const int64_t nb = apirl_projector_num_bins(p, subset, nsubsets);
   const size_t esz = counts_dtype == APIRL_U16 ? 2 : 4;
   DEVICE_SCOPE(p->device);
   cudaStream_t s = (cudaStream_t)stream;
-  CK(cudaMemcpyAsync(d_counts_stage, h_counts_subset, nb * esz, cudaMemcpyHostToDevice, s));
+  apirl_projector::Staged* slot = nullptr;
+  for (auto& e : p->staged)
+    if (e.dev == d_counts_stage && e.host == h_counts_subset) slot = &e;
+  if (slot) {
+    CK(cudaStreamWaitEvent(s, slot->done, 0));  // staged ahead by apirl_stage_counts
+    slot->dev = nullptr;
+    slot->host = nullptr;
+  } else {
+    CK(cudaMemcpyAsync(d_counts_stage, h_counts_subset, nb * esz, cudaMemcpyHostToDevice, s));
+  }
   double* d_lik = p->d_scalars;
   if (d_zimg)
     st = apirl_em_pass_sparse(p, d_counts_stage, counts_dtype, 1, nullptr, d_x, d_bp, d_sens, d_zimg, d_zero_add,
@@ -766,7 +812,7 @@ apirl_status apirl_em_pass_host(apirl_projector* p, const void* h_counts_subset,
                        subset, nsubsets, h_lik ? d_lik : nullptr, stream);
   if (st) return st;
   const int64_t nv = (int64_t)p->g.nx * p->g.ny * p->g.nz;
-  CK(cudaMemcpyAsync(h_x_out, d_x, nv * sizeof(float), cudaMemcpyDeviceToHost, s));
+  if (h_x_out) CK(cudaMemcpyAsync(h_x_out, d_x, nv * sizeof(float), cudaMemcpyDeviceToHost, s));
   if (h_lik) CK(cudaMemcpyAsync(h_lik, d_lik, sizeof(double), cudaMemcpyDeviceToHost, s));
   CK(cudaStreamSynchronize(s));
   return APIRL_OK;

@@ -203,6 +203,15 @@ struct apirl_projector {
   int persistent = 1;            // APIRL_OPT_PERSISTENT: warps pull 32-bin chunks (padded 3D pass)
   unsigned long long* d_chunk = nullptr;  // chunk counter of the persistent pass
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  // Counts staged ahead of apirl_em_pass_host (apirl_stage_counts): copied on
+  // copy_stream; each slot's event is recorded after its copy.
+  cudaStream_t copy_stream = nullptr;
+  cudaEvent_t copy_ready = nullptr;
+  struct Staged {
+    const void* host = nullptr;
+    void* dev = nullptr;
+    cudaEvent_t done = nullptr;
+  } staged[4];
   int timed = 0;                 // an event pair has been recorded
   int n_rings = 0;               // 3D geometry as given, for building the FP64 tables
   float r_fov = 0, axial_fov = 0, r_scanner = 0;

@@ -119,39 +119,47 @@ __device__ __forceinline__ float next_crossing(const Walk3& w, bool& cx, bool& c
 // linear index to the padded volume's last voxel (a border voxel), kept as a
 // memory-safety net.
 // Otherwise the reference's bounds test is applied.
+// Segments per iteration of the guarded gather: their voxel loads are all
+// issued before any product is added (the additions keep the walk order).
+#ifndef APIRL_GATHER_UNROLL
+#define APIRL_GATHER_UNROLL 6
+#endif
 __device__ __forceinline__ float siddon3_gather_pad(Walk3 w, const ImgGeom& g, int ux, int uy, int uz, unsigned lim,
                                                     const float* __restrict__ img) {
   const int sx = w.iinc * ux, sy = w.jinc * uy, sz = w.kinc * uz;
   int idx = (w.k + kPad) * uz + (w.j + kPad) * uy + (w.i + kPad) * ux;
   float acc = 0.f;
   if (w.guarded) {
+    constexpr int U = APIRL_GATHER_UNROLL;
     int m = 0;
-    for (; m + 1 < w.n; m += 2) {
-      bool cx, cy;
-      float an = next_crossing(w, cx, cy);
-      const float sa = A_MUL(A_SUB(an, w.ac), w.L);
-      const int ia = idx;
-      w.ac = an;
-      if (cx) { idx += sx; w.ax = A_ADD(w.ax, w.axu); }
-      else if (cy) { idx += sy; w.ay = A_ADD(w.ay, w.ayu); }
-      else { idx += sz; w.az = A_ADD(w.az, w.azu); }
-      an = next_crossing(w, cx, cy);
-      const float sb = A_MUL(A_SUB(an, w.ac), w.L);
-      const int ib = idx;
-      w.ac = an;
-      if (cx) { idx += sx; w.ax = A_ADD(w.ax, w.axu); }
-      else if (cy) { idx += sy; w.ay = A_ADD(w.ay, w.ayu); }
-      else { idx += sz; w.az = A_ADD(w.az, w.azu); }
-      const float va = __ldg(img + min((unsigned)ia, lim - 1u));
-      const float vb = __ldg(img + min((unsigned)ib, lim - 1u));
-      acc = A_ADD(acc, A_MUL(sa, va));
-      acc = A_ADD(acc, A_MUL(sb, vb));
+    for (; m + U <= w.n; m += U) {
+      int ia[U];
+      float sa[U], va[U];
+      #pragma unroll
+      for (int u = 0; u < U; u++) {
+        bool cx, cy;
+        const float an = next_crossing(w, cx, cy);
+        sa[u] = A_MUL(A_SUB(an, w.ac), w.L);
+        ia[u] = idx;
+        w.ac = an;
+        if (cx) { idx += sx; w.ax = A_ADD(w.ax, w.axu); }
+        else if (cy) { idx += sy; w.ay = A_ADD(w.ay, w.ayu); }
+        else { idx += sz; w.az = A_ADD(w.az, w.azu); }
+      }
+      #pragma unroll
+      for (int u = 0; u < U; u++) va[u] = __ldg(img + min((unsigned)ia[u], lim - 1u));
+      #pragma unroll
+      for (int u = 0; u < U; u++) acc = A_ADD(acc, A_MUL(sa[u], va[u]));
     }
-    if (m < w.n) {
+    for (; m < w.n; m++) {
       bool cx, cy;
       const float an = next_crossing(w, cx, cy);
       const float v = __ldg(img + min((unsigned)idx, lim - 1u));
       acc = A_ADD(acc, A_MUL(A_MUL(A_SUB(an, w.ac), w.L), v));
+      w.ac = an;
+      if (cx) { idx += sx; w.ax = A_ADD(w.ax, w.axu); }
+      else if (cy) { idx += sy; w.ay = A_ADD(w.ay, w.ayu); }
+      else { idx += sz; w.az = A_ADD(w.az, w.azu); }
     }
     return acc;
   }

@@ -199,6 +199,12 @@ class SiddonProjector:
                                                     _stream(stream)))
         return bp
 
+    def stage_counts(self, h_counts_subset, stage, subset, nsubsets, stream=None):
+        """Copy a pass's host counts to `stage` ahead of em_pass_host, beside the current work."""
+        dt = {"float32": _lib.APIRL_F32, "uint32": _lib.APIRL_U32, "uint16": _lib.APIRL_U16}[str(h_counts_subset.dtype)]
+        check(self.lib.apirl_stage_counts(self.h, ctypes.c_void_p(h_counts_subset.ctypes.data), dt, _ptr(stage),
+                                          subset, nsubsets, _stream(stream)))
+
     def em_pass_host(self, h_counts_subset, stage, x, bp, sens, subset, nsubsets, h_x_out, h_lik=None,
                      thr_value=0.0, ge=True, stream=None, zimg=None, zero_add=None):
         """em_pass (em_pass_sparse when zimg is given) from host counts (packed
@@ -207,7 +213,7 @@ class SiddonProjector:
         check(self.lib.apirl_em_pass_host(self.h, ctypes.c_void_p(h_counts_subset.ctypes.data), dt, _ptr(stage),
                                           _ptr(x), _ptr(bp), _ptr(sens), _ptr(zimg), _ptr(zero_add),
                                           float(thr_value), int(ge), subset, nsubsets,
-                                          ctypes.c_void_p(h_x_out.ctypes.data),
+                                          None if h_x_out is None else ctypes.c_void_p(h_x_out.ctypes.data),
                                           None if h_lik is None else ctypes.c_void_p(h_lik.ctypes.data),
                                           _stream(stream)))
         return h_x_out

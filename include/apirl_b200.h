@@ -301,11 +301,21 @@ apirl_status apirl_em_project_backproject(apirl_projector* p, const void* d_coun
  * apirl_em_pass on the projector's resident image / sensitivity buffers, and
  * copies the updated image and the likelihood back.  d_x, d_bp, d_sens are
  * device buffers the caller keeps resident between passes.  With d_zimg set
- * the pass is apirl_em_pass_sparse (d_zimg, d_zero_add as there). */
+ * the pass is apirl_em_pass_sparse (d_zimg, d_zero_add as there).  h_x_out
+ * or h_lik may be NULL (no copy back). */
 apirl_status apirl_em_pass_host(apirl_projector* p, const void* h_counts_subset, int counts_dtype, void* d_counts_stage,
                                 float* d_x, float* d_bp, const float* d_sens, const float* d_zimg,
                                 const double* d_zero_add, float thr_value, int ge, int subset, int nsubsets,
                                 float* h_x_out, double* h_lik, void* stream);
+
+/* Starts copying a pass's host counts into d_counts_stage on a copy stream of
+ * the projector, after the work already queued on `stream` and beside the
+ * work queued later, so that the copy for the next pass overlaps the current
+ * one.  The next apirl_em_pass_host with the same host pointer and stage
+ * waits for this copy instead of copying.  Use two stages, alternating (at
+ * most 4 staged copies outstanding per projector). */
+apirl_status apirl_stage_counts(apirl_projector* p, const void* h_counts_subset, int counts_dtype, void* d_counts_stage,
+                                int subset, int nsubsets, void* stream);
 
 /* ---- whole reconstructions (host buffers) --------------------------------
  * OsemSinogram3d::Reconstruct (recon/src/OsemSinogram3d.cpp:36-325): per-subset
