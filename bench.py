@@ -37,10 +37,10 @@ UNIT = "subiter/s"
 NSUB = 21
 TOTAL_COUNTS = 5e8
 L2_FLUSH_BYTES = 256 << 20
-# DRAM bytes (read + write) per k_em_pass launch of the full workload, mean of
-# three launches captured with ncu --metrics dram__bytes_read.sum,
+# DRAM bytes (read + write) per fused-kernel launch of the full workload,
+# mean of three launches captured with ncu --metrics dram__bytes_read.sum,
 # dram__bytes_write.sum (one pass; profiles/k_em_pass_osem3d_256x256x81.md).
-FULL_TRAFFIC_BYTES = 2.180e8
+FULL_TRAFFIC_BYTES = 2.208e8
 WORKLOAD = ("3D OSEM 256x256x81 image, 41 rings span-1 |rd|<=20: 1261 sinograms x 336 angles x 336 r, "
             "21 subsets, attenuation in sensitivity, 5e8 counts uint32")
 
