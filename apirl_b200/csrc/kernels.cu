@@ -13,6 +13,7 @@
 #include <cuda_runtime.h>
 #include <cstdint>
 #include <cfloat>
+#include <atomic>
 #include "internal.h"
 #include "siddon.cuh"
 #include "../../include/apirl_b200.h"
@@ -834,6 +835,23 @@ __global__ void __launch_bounds__(256) k_pad_reduce(PadDims d, float* __restrict
 
 inline unsigned grid_for(int64_t total) { return (unsigned)((total + kBlock - 1) / kBlock); }
 
+// The fused 3D kernels use no shared memory: give the SM's unified L1 /
+// shared storage to L1.  Set once per device (function attributes belong to
+// the device's context).
+void prefer_l1() {
+  static std::atomic<int> done[64];
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return;
+  if (done[dev].exchange(1)) return;
+  cudaFuncSetAttribute(k_em_pass<float, true, false>, cudaFuncAttributePreferredSharedMemoryCarveout, 0);
+  cudaFuncSetAttribute(k_em_pass<uint32_t, true, false>, cudaFuncAttributePreferredSharedMemoryCarveout, 0);
+  cudaFuncSetAttribute(k_em_pass<uint16_t, true, false>, cudaFuncAttributePreferredSharedMemoryCarveout, 0);
+  cudaFuncSetAttribute(k_em_pass_persist<float>, cudaFuncAttributePreferredSharedMemoryCarveout, 0);
+  cudaFuncSetAttribute(k_em_pass_persist<uint32_t>, cudaFuncAttributePreferredSharedMemoryCarveout, 0);
+  cudaFuncSetAttribute(k_em_pass_persist<uint16_t>, cudaFuncAttributePreferredSharedMemoryCarveout, 0);
+  (void)cudaGetLastError();
+}
+
 // Deterministic sum of n partials into *out.  Above kSumLevel2 * 64 partials
 // the sum runs in two levels (kSumLevel2 blocks, then one), the second level's
 // kSumLevel2 values stored right after partials[n - 1].
@@ -921,24 +939,22 @@ cudaError_t launch_em_pass(const ImgGeom& g, const LorTable& t, SubsetSel s, con
                                                            total, 0);                                         \
   } while (0)
   if (persist_counter && t.is3d && !t.lor_s && !pg.enabled && pad.pA && lik_mode == 0) {
-    // Persistent form: as many blocks as fit on the SMs at once.
-    static int resident[3] = {0, 0, 0};
-    const int ti = counts_dtype == APIRL_F32 ? 0 : (counts_dtype == APIRL_U32 ? 1 : 2);
-    if (!resident[ti]) {
-      int per_sm = 0, dev = 0, sms = 0;
-      cudaError_t oe = counts_dtype == APIRL_F32
-          ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_em_pass_persist<float>, block, 0)
-          : (counts_dtype == APIRL_U32
-                 ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_em_pass_persist<uint32_t>, block, 0)
-                 : cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_em_pass_persist<uint16_t>, block, 0));
-      if (oe != cudaSuccess) return oe;
-      cudaGetDevice(&dev);
-      cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-      resident[ti] = (per_sm < 1 ? 1 : per_sm) * sms;
-    }
+    prefer_l1();
+    // Persistent form: as many blocks of this size as fit on the current
+    // device's SMs at once (a host-side query of a few microseconds).
+    int per_sm = 0, dev = 0, sms = 0;
+    cudaError_t oe = counts_dtype == APIRL_F32
+        ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_em_pass_persist<float>, block, 0)
+        : (counts_dtype == APIRL_U32
+               ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_em_pass_persist<uint32_t>, block, 0)
+               : cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_em_pass_persist<uint16_t>, block, 0));
+    if (oe != cudaSuccess) return oe;
+    if ((oe = cudaGetDevice(&dev)) != cudaSuccess) return oe;
+    if ((oe = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev)) != cudaSuccess) return oe;
+    const int64_t resident = (int64_t)(per_sm < 1 ? 1 : per_sm) * sms;
     const int64_t chunks = (total + 31) / 32;
     const int64_t need = (chunks * 32 + block - 1) / block;
-    const unsigned pgrid = (unsigned)(need < resident[ti] ? need : resident[ti]);
+    const unsigned pgrid = (unsigned)(need < resident ? need : resident);
     cudaError_t me = cudaMemsetAsync(persist_counter, 0, sizeof(unsigned long long), st);
     if (me != cudaSuccess) return me;
     switch (counts_dtype) {
@@ -968,14 +984,7 @@ cudaError_t launch_em_pass(const ImgGeom& g, const LorTable& t, SubsetSel s, con
     }
     return launch_sum(partials, np, lik, st);
   }
-  static bool carveout_set = false;  // prefer L1 over shared memory: the kernel uses none
-  if (!carveout_set) {
-    cudaFuncSetAttribute(k_em_pass<float, true, false>, cudaFuncAttributePreferredSharedMemoryCarveout, 0);
-    cudaFuncSetAttribute(k_em_pass<uint32_t, true, false>, cudaFuncAttributePreferredSharedMemoryCarveout, 0);
-    cudaFuncSetAttribute(k_em_pass<uint16_t, true, false>, cudaFuncAttributePreferredSharedMemoryCarveout, 0);
-    (void)cudaGetLastError();
-    carveout_set = true;
-  }
+  prefer_l1();
   switch (counts_dtype) {
     case APIRL_F32: APIRL_EM(float); break;
     case APIRL_U32: APIRL_EM(uint32_t); break;

@@ -648,6 +648,49 @@ def _plain(jobs, dev):
     return outs, time.perf_counter() - t0
 
 
+def run_mlem2d(args):
+    """--workload mlem2d: the 2D configuration (128x128 image, 192x192
+    sinogram, disc phantom with 6 hot points, 1e6 counts, 60 MLEM iterations)
+    through the whole-reconstruction driver (host buffers in and out, one CUDA
+    graph per iteration), against the reference's Mlem2d on the host cores."""
+    import torch
+    import apirl_b200 as ap
+    from apirl_b200 import workloads
+    ap.load_library()
+    ig, sg = workloads.c1_geometry()
+    x = workloads.disc_phantom_2d(ig, seed=0)
+    P = ap.SiddonProjector(ig, sg)
+    est = torch.zeros(sg.n_bins, dtype=torch.float32, device="cuda:0")
+    P.project(torch.from_numpy(x).cuda(), est)
+    meas = workloads.poisson_counts(est.cpu().numpy(), 1e6, seed=0).astype(np.float32)
+    init = np.ones(ig.n_voxels, np.float32)
+    iters = 60
+    for _ in range(max(args.warmup, 1)):
+        ap.mlem_2d(ig, sg, meas, init, iters)
+    times = []
+    for _ in range(max(args.steps, 1)):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        ap.mlem_2d(ig, sg, meas, init, iters)
+        times.append(time.perf_counter() - t0)
+    gpu = iters / statistics.median(times)
+    cpu = None
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    from oracle_lib import RefHarness, REF_SO
+    if os.path.exists(REF_SO) and not args.no_cpu_baseline:
+        R = RefHarness()
+        cores = R.set_threads(args.cpu_threads or os.cpu_count() or 1)
+        t0 = time.perf_counter()
+        R.mlem_2d(sg, ig, init, meas, iters)
+        cpu = {"value": iters / (time.perf_counter() - t0), "unit": "iter/s", "cores": cores, "kind": "reference",
+               "sample": "the whole 60-iteration Mlem2d reconstruction"}
+    print(json.dumps({"metric": "2D MLEM iterations/s (128x128, 192x192 sinogram)", "value": gpu, "unit": "iter/s",
+                      "n_gpus": 1, "higher_is_better": True, "ms_per_reconstruction": 1e3 * statistics.median(times),
+                      "dtype": "f32", "data": "synthetic (disc phantom, 1e6 Poisson counts)",
+                      "config": {"workload": "2D MLEM 60 iterations, whole driver with host buffers (e2e)"},
+                      "cpu_baseline": cpu}), flush=True)
+
+
 def run_batched(args, served=False):
     import torch
     from apirl_b200 import workloads
@@ -710,7 +753,7 @@ def main():
                      help="walk geometry: f32 = the reference's float arithmetic (headline); f64 = precision mode")
     ap_.add_argument("--cpu-threads", type=int, default=None,
                      help="host threads of the CPU baseline / reference arm (default: all)")
-    ap_.add_argument("--workload", default="osem3d", choices=["osem3d", "batched", "served"])
+    ap_.add_argument("--workload", default="osem3d", choices=["osem3d", "batched", "served", "mlem2d"])
     ap_.add_argument("--max-ring-diff", type=int, default=None,
                      help="profiling: keep segments |rd| <= this (smaller case of the same kernels)")
     ap_.add_argument("--jobs", type=int, default=64)
@@ -726,6 +769,8 @@ def main():
         run_reference(args)
     elif args.shard:
         run_sharded(args)
+    elif args.workload == "mlem2d":
+        run_mlem2d(args)
     elif args.workload in ("batched", "served"):
         run_batched(args, served=args.workload == "served")
     else:
