@@ -98,5 +98,8 @@ def test_invalid_geometries_rejected():
         if sub >= 0:
             with pytest.raises(ap.ApirlError):
                 P.project(t(np.ones(ig.n_voxels, np.float32)), out, sub, ns)
-    with pytest.raises(ap.ApirlError):
-        P.set_shard(2, 4)
+    P.set_shard(2, 4)  # 9 sinograms: a valid shard
+    P.set_shard(0, 9)
+    for first, n in ((5, 5), (-1, 2), (0, 0)):
+        with pytest.raises(ap.ApirlError):
+            P.set_shard(first, n)
