@@ -680,9 +680,19 @@ def run_mlem2d(args):
     if os.path.exists(REF_SO) and not args.no_cpu_baseline:
         R = RefHarness()
         cores = R.set_threads(args.cpu_threads or os.cpu_count() or 1)
-        t0 = time.perf_counter()
-        R.mlem_2d(sg, ig, init, meas, iters)
-        cpu = {"value": iters / (time.perf_counter() - t0), "unit": "iter/s", "cores": cores, "kind": "reference",
+        # the reference prints its progress on stdout: send it to stderr, so
+        # that stdout carries only the JSON line
+        sys.stdout.flush()
+        saved = os.dup(1)
+        os.dup2(2, 1)
+        try:
+            t0 = time.perf_counter()
+            R.mlem_2d(sg, ig, init, meas, iters)
+            sec = time.perf_counter() - t0
+        finally:
+            os.dup2(saved, 1)
+            os.close(saved)
+        cpu = {"value": iters / sec, "unit": "iter/s", "cores": cores, "kind": "reference",
                "sample": "the whole 60-iteration Mlem2d reconstruction"}
     print(json.dumps({"metric": "2D MLEM iterations/s (128x128, 192x192 sinogram)", "value": gpu, "unit": "iter/s",
                       "n_gpus": 1, "higher_is_better": True, "ms_per_reconstruction": 1e3 * statistics.median(times),
