@@ -23,6 +23,11 @@
  *    [sinogram][subset angle][r] and has apirl_projector_num_bins() bins.
  *  - Voxel indices of Siddon segments are checked against all image bounds.
  *    (The reference checks only one side in its Project: SiddonProjector.cpp:178, :417.)
+ *  - A projector owns scratch buffers (likelihood partials, padded image
+ *    copies, the persistent pass's chunk counter): the calls made with one
+ *    projector must run one after another on the device (one stream, or
+ *    streams ordered by the caller).  Different projectors are independent;
+ *    calls on different projectors may come from different host threads.
  */
 #ifndef APIRL_B200_H
 #define APIRL_B200_H
