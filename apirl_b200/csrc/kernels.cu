@@ -53,17 +53,8 @@ __device__ __forceinline__ BinPos decode(int64_t b, const LorTable& t, const Sub
 
 template <typename CT> __device__ __forceinline__ float load_count(const CT* p, int64_t i);
 template <> __device__ __forceinline__ float load_count<float>(const float* p, int64_t i) { return __ldg(p + i); }
-// Counts are read once per pass: a streaming load keeps them from pushing the
-// image and backprojection out of L2 (APIRL_STREAM_COUNTS).
-#ifndef APIRL_STREAM_COUNTS
-#define APIRL_STREAM_COUNTS 0
-#endif
 template <> __device__ __forceinline__ float load_count<uint32_t>(const uint32_t* p, int64_t i) {
-#if APIRL_STREAM_COUNTS
-  return (float)__ldcs(p + i);
-#else
   return (float)__ldg(p + i);
-#endif
 }
 template <> __device__ __forceinline__ float load_count<uint16_t>(const uint16_t* p, int64_t i) {
   return (float)__ldg(p + i);

@@ -177,35 +177,12 @@ __device__ __forceinline__ float siddon3_gather_pad(Walk3 w, const ImgGeom& g, i
   return acc;
 }
 
-// Segments per iteration of the guarded scatter (loop unrolling only; the
-// atomic adds are issued in walk order).
-#ifndef APIRL_SCATTER_UNROLL
-#define APIRL_SCATTER_UNROLL 1
-#endif
 __device__ __forceinline__ void siddon3_scatter_pad(Walk3 w, const ImgGeom& g, int ux, int uy, int uz, unsigned lim,
                                                     float r, float* __restrict__ img) {
   const int sx = w.iinc * ux, sy = w.jinc * uy, sz = w.kinc * uz;
   int idx = (w.k + kPad) * uz + (w.j + kPad) * uy + (w.i + kPad) * ux;
   if (w.guarded) {
-#if APIRL_SCATTER_UNROLL > 1
-    constexpr int U = APIRL_SCATTER_UNROLL;
-    int m = 0;
-    for (; m + U <= w.n; m += U) {
-      #pragma unroll
-      for (int u = 0; u < U; u++) {
-        bool cx, cy;
-        const float an = next_crossing(w, cx, cy);
-        atomicAdd(img + min((unsigned)idx, lim - 1u), A_MUL(A_MUL(A_SUB(an, w.ac), w.L), r));
-        w.ac = an;
-        if (cx) { idx += sx; w.ax = A_ADD(w.ax, w.axu); }
-        else if (cy) { idx += sy; w.ay = A_ADD(w.ay, w.ayu); }
-        else { idx += sz; w.az = A_ADD(w.az, w.azu); }
-      }
-    }
-    for (; m < w.n; m++) {
-#else
     for (int m = 0; m < w.n; m++) {
-#endif
       bool cx, cy;
       const float an = next_crossing(w, cx, cy);
       atomicAdd(img + min((unsigned)idx, lim - 1u), A_MUL(A_MUL(A_SUB(an, w.ac), w.L), r));
