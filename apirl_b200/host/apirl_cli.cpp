@@ -1,5 +1,6 @@
-// The reference's .par-driven commands on the GPU path: MLEM, OSEM, project
-// and backproject (cmd/src/MLEM.cpp, OSEM.cpp, project.cpp, backproject.cpp).
+// The reference's .par-driven commands on the GPU path: MLEM, OSEM, project,
+// backproject and cuMLEM (cmd/src/MLEM.cpp, OSEM.cpp, project.cpp,
+// backproject.cpp, cmdGPU/src/cuMLEM.cpp).
 // One source; the command is chosen at build time with -DAPIRL_COMMAND=<name>
 // (the binary's name).  Each takes one argument, a parameter file ending in
 // .par whose first line is "<COMMAND> Parameters :=".
@@ -15,6 +16,13 @@
 //              projection, number of subsets, subset index (+ scanner keys)
 //   backproject input type, input file, backprojector, output image, output
 //              filename, number of subsets, subset index (+ scanner keys)
+//   cuMLEM     section "MLEM": input type (Sinogram3D, Sinogram3DSiemensMmr),
+//              input file, initial estimate, output filename prefix, number of
+//              iterations, forwardprojector and backprojector (CuSiddonProjector),
+//              projector / backprojector / pixel update block size ({x,y,z}),
+//              gpu id, number of subsets (OSEM, Sinogram3DSiemensMmr only, as in
+//              the reference), multiplicative sinogram, additive sinogram
+//              (+ scanner keys)
 #include <chrono>
 #include <cstdio>
 #include <cstdlib>
@@ -213,6 +221,100 @@ int backproject() {
   return 0;
 }
 
+// ProcessBlockSizeString (reconGPU/src/readCudaParameters.cpp:22-48): the
+// three numbers between the last '{' and the last '}', separated by spaces or
+// commas.
+bool block_size(const char* k, dim3* out) {
+  std::string v;
+  key(k, &v);
+  size_t a = v.rfind('{'), b = v.rfind('}');
+  if (a == std::string::npos || b == std::string::npos || b < a) {
+    std::cerr << "\"" << k << "\" must be {x,y,z}" << std::endl;
+    return false;
+  }
+  std::string body = v.substr(a + 1, b - a - 1);
+  for (char& c : body)
+    if (c == ',') c = ' ';
+  unsigned int x = 0, y = 0, z = 0;
+  if (sscanf(body.c_str(), "%u %u %u", &x, &y, &z) != 3) {
+    std::cerr << "\"" << k << "\" needs three elements" << std::endl;
+    return false;
+  }
+  *out = dim3(x, y, z);
+  return true;
+}
+
+// cmdGPU/src/cuMLEM.cpp:159-483.
+int cumlem() {
+  std::string type, input, init, prefix, fwdName, backName;
+  key("input type", &type);
+  key("input file", &input);
+  key("initial estimate", &init);
+  key("output filename prefix", &prefix);
+  std::string it;
+  key("number of iterations", &it);
+  const int iters = atoi(it.c_str());
+  key("forwardprojector", &fwdName);
+  key("backprojector", &backName);
+  dim3 bp, bb, bu;
+  if (!block_size("projector block size", &bp) || !block_size("backprojector block size", &bb) ||
+      !block_size("pixel update block size", &bu))
+    return -1;
+  int gpu = ikey("gpu id", 0);
+  int subsets = ikey("number of subsets", 0);
+  for (const std::string* n : {&fwdName, &backName})
+    if (*n != "CuSiddonProjector") {
+      std::cerr << "No existe el proyector " << *n << "." << std::endl;
+      return 1;
+    }
+  Image x0;
+  if (!x0.readFromInterfile(init.c_str())) {
+    std::cerr << "Error reading the initial estimate: " << x0.getError() << std::endl;
+    return -1;
+  }
+  CuSiddonProjector fwd, back;
+  std::unique_ptr<Sinogram3D> s3;
+  std::unique_ptr<CuMlemSinogram3d> m;
+  if (type == "Sinogram3D") {
+    Scanner sc = scanner(&x0);
+    s3.reset(new Sinogram3DCylindricalPet(input.c_str(), sc.rFov, sc.zFov, sc.rScanner));
+  } else if (type == "Sinogram3DSiemensMmr") {
+    s3.reset(new Sinogram3DSiemensMmr(input.c_str()));
+  } else {
+    std::cerr << "input type " << type << " is not supported (Sinogram3D, Sinogram3DSiemensMmr)" << std::endl;
+    return -1;
+  }
+  if (s3->getNumSinograms() <= 0 || s3->getBinCount() <= 1) {
+    std::cerr << "Error reading " << input << ": " << s3->getError() << std::endl;
+    return 1;
+  }
+  // The reference runs OSEM for mMR sinograms with a subset count only.
+  if (type == "Sinogram3DSiemensMmr" && subsets > 0)
+    m.reset(new CuOsemSinogram3d(s3.get(), &x0, "", prefix, iters, 0, false, false, &fwd, &back, subsets));
+  else
+    m.reset(new CuMlemSinogram3d(s3.get(), &x0, "", prefix, iters, 0, false, false, &fwd, &back));
+  std::string mult, add;
+  if (key("multiplicative sinogram", &mult, false) && !m->setMultiplicativeProjection(mult)) {
+    std::cerr << "Error reading " << mult << std::endl;
+    return 1;
+  }
+  if (key("additive sinogram", &add, false) && !m->setAdditiveProjection(add)) {
+    std::cerr << "Error reading " << add << std::endl;
+    return 1;
+  }
+  m->setBackprojectorKernelConfig(&bb);
+  m->setProjectorKernelConfig(&bp);
+  m->setUpdatePixelKernelConfig(&bu);
+  auto t0 = std::chrono::steady_clock::now();
+  if (!m->Reconstruct(SIDDON_PROJ_TEXT_CYLINDRICAL_SCANNER, gpu)) {
+    std::cerr << "Reconstruction failed: " << m->getError() << std::endl;
+    return 1;
+  }
+  double sec = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+  std::cout << kCmd << ": " << iters << " iterations in " << sec << " s, output " << prefix << "_final.h33" << std::endl;
+  return 0;
+}
+
 }  // namespace
 
 int main(int argc, char** argv) {
@@ -226,11 +328,12 @@ int main(int argc, char** argv) {
     return -1;
   }
   std::string cmd = kCmd;
-  g_section = cmd == "project" ? "Projection" : (cmd == "backproject" ? "Backproject" : cmd);
+  g_section = cmd == "project" ? "Projection" : (cmd == "backproject" ? "Backproject" : cmd == "cuMLEM" ? "MLEM" : cmd);
   if (cmd == "MLEM") return recon(false);
   if (cmd == "OSEM") return recon(true);
   if (cmd == "project") return project();
   if (cmd == "backproject") return backproject();
+  if (cmd == "cuMLEM") return cumlem();
   std::cerr << "unknown command " << cmd << std::endl;
   return -1;
 }

@@ -422,6 +422,12 @@ CuSiddonProjector::CuSiddonProjector(int nSamples, int nAxialSamples, int gpuId)
     : st(new State), device(gpuId), numSamplesOnDetector(nSamples), numAxialSamplesOnDetector(nAxialSamples) {}
 
 CuSiddonProjector::~CuSiddonProjector() {
+  release();
+  delete st;
+}
+
+// Frees the projector and buffers set up on `device`; the next call sets up again.
+void CuSiddonProjector::release() {
   if (st->p) apirl_projector_destroy(st->p);
   int prev = 0;
   cudaGetDevice(&prev);
@@ -431,7 +437,20 @@ CuSiddonProjector::~CuSiddonProjector() {
   cudaFree(st->d_b);
   if (st->stream) cudaStreamDestroy(st->stream);
   cudaSetDevice(prev);
-  delete st;
+  *st = State();
+}
+
+bool CuSiddonProjector::setGpuId(int id) {
+  int n = 0;
+  if (cudaGetDeviceCount(&n) != cudaSuccess || id < 0 || id >= n) {
+    strError = "no GPU with index " + std::to_string(id);
+    return false;
+  }
+  if (id != device) {
+    release();
+    device = id;
+  }
+  return true;
 }
 
 static bool same_img(const apirl_image_geom& a, const apirl_image_geom& b) {
@@ -549,6 +568,240 @@ bool CuSiddonProjector::Backproject(Sinogram3D* s, Image* img) {
 bool CuSiddonProjector::DivideAndBackproject(Sinogram3D* in, Sinogram3D* est, Image* img) {
   return prepare3d(img, in) && run(2, img, in->getSinogramPtr(), est->getSinogramPtr(), nullptr,
                                    (size_t)in->getBinCount(), in->subsetIndex(), in->subsetCount());
+}
+
+// Device-buffer calls (CuProjector).  op: 0 project d_a -> d_out (sinogram),
+// 1 backproject d_a into d_out (image), 2 divide d_a by d_b and backproject.
+bool CuSiddonProjector::runDevice(int op, const float* d_a, const float* d_b, float* d_out, Image* img,
+                                  Sinogram3D* s, bool copyResult) {
+  if (!img || !s || !d_a || !d_out || (op == 2 && !d_b)) {
+    strError = "null image, sinogram or device buffer";
+    return false;
+  }
+  int prev = 0;
+  cudaGetDevice(&prev);
+  struct Restore { int d; ~Restore() { cudaSetDevice(d); } } restore{prev};
+  if (cudaSetDevice(device) != cudaSuccess) { strError = "cudaSetDevice failed"; return false; }
+  if (!prepare3d(img, s)) return false;
+  cudaStream_t legacy = 0;
+  apirl_status rc;
+  if (op == 0)
+    rc = apirl_project(st->p, d_a, d_out, s->subsetIndex(), s->subsetCount(), legacy);
+  else if (op == 1)
+    rc = apirl_backproject(st->p, d_a, d_out, s->subsetIndex(), s->subsetCount(), legacy);
+  else
+    rc = apirl_divide_and_backproject(st->p, d_a, d_b, d_out, s->subsetIndex(), s->subsetCount(), legacy);
+  if (rc != APIRL_OK) { strError = apirl_last_error(); cudaStreamSynchronize(legacy); return false; }
+  if (copyResult) {
+    cudaError_t e = op == 0 ? cudaMemcpy(s->getSinogramPtr(), d_out, (size_t)s->getBinCount() * sizeof(float),
+                                         cudaMemcpyDeviceToHost)
+                            : cudaMemcpy(img->getPixelsPtr(), d_out, (size_t)img->getPixelCount() * sizeof(float),
+                                         cudaMemcpyDeviceToHost);
+    if (e != cudaSuccess) { strError = cudaGetErrorString(e); return false; }
+  }
+  cudaError_t e = cudaStreamSynchronize(legacy);
+  if (e != cudaSuccess) { strError = cudaGetErrorString(e); return false; }
+  return true;
+}
+
+bool CuSiddonProjector::Project(float* d_image, float* d_projection, float*, float*, Image* inputImage,
+                                Sinogram3D* outputSinogram, bool copyResult) {
+  return runDevice(0, d_image, nullptr, d_projection, inputImage, outputSinogram, copyResult);
+}
+bool CuSiddonProjector::Backproject(float* d_inputSinogram, float* d_outputImage, float*, float*,
+                                    Sinogram3D* inputSinogram, Image* outputImage, bool copyResult) {
+  return runDevice(1, d_inputSinogram, nullptr, d_outputImage, outputImage, inputSinogram, copyResult);
+}
+bool CuSiddonProjector::DivideAndBackproject(float* d_inputSinogram, float* d_estimatedSinogram,
+                                             float* d_outputImage, float*, float*, Sinogram3D* inputSinogram,
+                                             Image* outputImage, bool copyResult) {
+  return runDevice(2, d_inputSinogram, d_estimatedSinogram, d_outputImage, outputImage, inputSinogram, copyResult);
+}
+
+// ---- CuProjector / CuProjectorInterface ------------------------------------------
+CuProjector::CuProjector() : gridSize(1, 1, 1), blockSize(128, 1, 1) {}
+
+CuProjector::CuProjector(unsigned int bx, unsigned int by, unsigned int bz, unsigned int gx, unsigned int gy,
+                         unsigned int gz) {
+  setKernelConfig(bx, by, bz, gx, gy, gz);
+}
+
+void CuProjector::setKernelConfig(unsigned int bx, unsigned int by, unsigned int bz, unsigned int gx,
+                                  unsigned int gy, unsigned int gz) {
+  blockSize = dim3(bx, by, bz);
+  gridSize = dim3(gx, gy, gz);
+  threads_per_block = bx * by * bz;
+}
+
+CuProjectorInterface::CuProjectorInterface(CuProjector* p) : projector(p), blockSizeProjector(128, 1, 1) {}
+
+CuProjectorInterface::~CuProjectorInterface() { release(); }
+
+void CuProjectorInterface::release() {
+  if (bufDevice >= 0) {
+    int prev = 0;
+    cudaGetDevice(&prev);
+    cudaSetDevice(bufDevice);
+    cudaFree(d_image);
+    cudaFree(d_projection);
+    cudaFree(d_estimated);
+    cudaFree(d_ring1_mm);
+    cudaFree(d_ring2_mm);
+    cudaSetDevice(prev);
+  }
+  d_image = d_projection = d_estimated = d_ring1_mm = d_ring2_mm = nullptr;
+  nImage = nBins = nEstimated = nSinos = 0;
+  bufDevice = -1;
+}
+
+void CuProjectorInterface::setProjectorKernelConfig(unsigned int x, unsigned int y, unsigned int z,
+                                                    Sinogram3D* sinogram) {
+  blockSizeProjector = dim3(x, y, z);
+  const unsigned int per = (unsigned int)(sinogram->getNumProj() * sinogram->getNumR());
+  const unsigned int gx = x ? (per + x - 1) / x : 1;
+  if (projector) projector->setKernelConfig(x, y, z, gx, (unsigned int)sinogram->getNumSinograms(), 1);
+}
+
+void CuProjectorInterface::setProjectorKernelConfig(dim3 b, Sinogram3D* sinogram) {
+  setProjectorKernelConfig(b.x, b.y, b.z, sinogram);
+}
+
+bool CuProjectorInterface::setGpuId(int id) {
+  int n = 0;
+  if (cudaGetDeviceCount(&n) != cudaSuccess || id < 0 || id >= n) {
+    strError = "no GPU with index " + std::to_string(id);
+    return false;
+  }
+  gpuId = id;
+  return true;
+}
+
+bool CuProjectorInterface::Project(Image*, Sinogram2D*) {
+  strError = "CuProjectorInterface projects Sinogram3D only";
+  return false;
+}
+bool CuProjectorInterface::Backproject(Sinogram2D*, Image*) {
+  strError = "CuProjectorInterface backprojects Sinogram3D only";
+  return false;
+}
+bool CuProjectorInterface::DivideAndBackproject(Sinogram2D*, Sinogram2D*, Image*) {
+  strError = "CuProjectorInterface backprojects Sinogram3D only";
+  return false;
+}
+
+// Device buffers for `s` and `img` on gpuId (grown, never shrunk), the ring
+// arrays filled, the CuProjector on the same GPU and its launch shape set.
+bool CuProjectorInterface::prepare(Sinogram3D* s, Image* img, bool estimate) {
+  if (!projector || !s || !img) { strError = "null projector, image or sinogram"; return false; }
+  if (auto* sp = dynamic_cast<CuSiddonProjector*>(projector)) {
+    if (!sp->setGpuId(gpuId)) { strError = sp->getError(); return false; }
+  }
+  if (bufDevice != gpuId) release();
+  if (cudaSetDevice(gpuId) != cudaSuccess) { strError = "cudaSetDevice failed"; return false; }
+  bufDevice = gpuId;
+  auto grow = [](float** p, size_t* have, size_t n) {
+    if (*have >= n) return true;
+    cudaFree(*p);
+    *p = nullptr;
+    *have = 0;
+    if (cudaMalloc(p, n * sizeof(float)) != cudaSuccess) return false;
+    *have = n;
+    return true;
+  };
+  const size_t nsino = (size_t)s->getNumSinograms();
+  const bool newRings = nsino != nSinos || !d_ring1_mm;
+  if (!grow(&d_image, &nImage, (size_t)img->getPixelCount()) || !grow(&d_projection, &nBins, (size_t)s->getBinCount()) ||
+      (estimate && !grow(&d_estimated, &nEstimated, (size_t)s->getBinCount()))) {
+    strError = "device allocation failed";
+    return false;
+  }
+  // Axial end points per sinogram (the reference's d_ring1_mm / d_ring2_mm,
+  // CuProjectorInterface.cu:243-275), rebuilt on every call: the geometry
+  // may change between calls with the same sinogram count.
+  apirl_sino3d_geom g = s->geom();
+  std::vector<float> z((size_t)2 * nsino);
+  if (apirl_sino3d_ring_z(&g, z.data()) != (int)nsino) { strError = apirl_last_error(); return false; }
+  std::vector<float> z1(nsino), z2(nsino);
+  for (size_t i = 0; i < nsino; i++) { z1[i] = z[2 * i]; z2[i] = z[2 * i + 1]; }
+  if (newRings) {
+    cudaFree(d_ring1_mm);
+    cudaFree(d_ring2_mm);
+    d_ring1_mm = d_ring2_mm = nullptr;
+    nSinos = 0;
+    if (cudaMalloc(&d_ring1_mm, nsino * sizeof(float)) != cudaSuccess ||
+        cudaMalloc(&d_ring2_mm, nsino * sizeof(float)) != cudaSuccess) {
+      strError = "device allocation failed";
+      return false;
+    }
+    nSinos = nsino;
+  }
+  if (cudaMemcpy(d_ring1_mm, z1.data(), nsino * sizeof(float), cudaMemcpyHostToDevice) != cudaSuccess ||
+      cudaMemcpy(d_ring2_mm, z2.data(), nsino * sizeof(float), cudaMemcpyHostToDevice) != cudaSuccess) {
+    strError = "copy of the ring arrays failed";
+    return false;
+  }
+  setProjectorKernelConfig(blockSizeProjector, s);
+  return true;
+}
+
+namespace {
+const char* projector_error(CuProjector* p) {
+  auto* q = dynamic_cast<Projector*>(p);
+  return q && q->getError()[0] ? q->getError() : "the CuProjector call failed";
+}
+}  // namespace
+
+bool CuProjectorInterface::Project(Image* img, Sinogram3D* s) {
+  int prev = 0;
+  cudaGetDevice(&prev);
+  struct Restore { int d; ~Restore() { cudaSetDevice(d); } } restore{prev};
+  if (!prepare(s, img, false)) return false;
+  const size_t nb = (size_t)s->getBinCount();
+  if (cudaMemcpy(d_image, img->getPixelsPtr(), (size_t)img->getPixelCount() * sizeof(float),
+                 cudaMemcpyHostToDevice) != cudaSuccess ||
+      cudaMemset(d_projection, 0, nb * sizeof(float)) != cudaSuccess) {
+    strError = "copy to the device failed";
+    return false;
+  }
+  if (!projector->Project(d_image, d_projection, d_ring1_mm, d_ring2_mm, img, s, false)) {
+    strError = projector_error(projector);
+    return false;
+  }
+  if (cudaMemcpy(s->getSinogramPtr(), d_projection, nb * sizeof(float), cudaMemcpyDeviceToHost) != cudaSuccess) {
+    strError = "copy from the device failed";
+    return false;
+  }
+  return true;
+}
+
+bool CuProjectorInterface::Backproject(Sinogram3D* s, Image* img) { return DivideAndBackproject(s, nullptr, img); }
+
+bool CuProjectorInterface::DivideAndBackproject(Sinogram3D* s, Sinogram3D* est, Image* img) {
+  int prev = 0;
+  cudaGetDevice(&prev);
+  struct Restore { int d; ~Restore() { cudaSetDevice(d); } } restore{prev};
+  if (est && est->getBinCount() != (s ? s->getBinCount() : -1)) {
+    strError = "the estimated sinogram has another size";
+    return false;
+  }
+  if (!prepare(s, img, est != nullptr)) return false;
+  const size_t nb = (size_t)s->getBinCount(), nv = (size_t)img->getPixelCount();
+  if (cudaMemcpy(d_projection, s->getSinogramPtr(), nb * sizeof(float), cudaMemcpyHostToDevice) != cudaSuccess ||
+      (est && cudaMemcpy(d_estimated, est->getSinogramPtr(), nb * sizeof(float), cudaMemcpyHostToDevice) !=
+                  cudaSuccess) ||
+      cudaMemset(d_image, 0, nv * sizeof(float)) != cudaSuccess) {
+    strError = "copy to the device failed";
+    return false;
+  }
+  const bool ok = est ? projector->DivideAndBackproject(d_projection, d_estimated, d_image, d_ring1_mm, d_ring2_mm, s,
+                                                        img, false)
+                      : projector->Backproject(d_projection, d_image, d_ring1_mm, d_ring2_mm, s, img, false);
+  if (!ok) { strError = projector_error(projector); return false; }
+  if (cudaMemcpy(img->getPixelsPtr(), d_image, nv * sizeof(float), cudaMemcpyDeviceToHost) != cudaSuccess) {
+    strError = "copy from the device failed";
+    return false;
+  }
+  return true;
 }
 
 // ---- Mlem ----------------------------------------------------------------------
@@ -671,27 +924,45 @@ bool MlemSinogram3d::sameSampling(apirl_sampling* out) {
   return true;
 }
 
-bool MlemSinogram3d::Reconstruct() {
-  if (!deviceResident()) { strError = "MlemSinogram3d runs on the GPU and needs CuSiddonProjector"; return false; }
+bool MlemSinogram3d::reconstructOnDevice(int numSubsets) {
+  if (!deviceResident()) {
+    strError = "the reconstruction runs on the GPU and needs CuSiddonProjector as forward and back projector";
+    return false;
+  }
   double t0 = now_ms();
   int dev = static_cast<CuSiddonProjector*>(forwardprojector)->gpuId();
+  if (static_cast<CuSiddonProjector*>(backprojector)->gpuId() != dev) {
+    strError = "forward and back projectors must be on the same GPU";
+    return false;
+  }
   apirl_image_geom ig = initialEstimate->geom();
   apirl_sino3d_geom sg = inputProjection->geom();
-  likelihood.assign(numIterations + 1, 0.0);
   apirl_sampling sm;
   if (!sameSampling(&sm)) return false;
-  apirl_status rc = apirl_mlem_3d(&ig, &sg, inputProjection->getSinogramPtr(),
-                                  multiplicative ? multiplicative->getSinogramPtr() : nullptr,
-                                  additive ? additive->getSinogramPtr() : nullptr, initialEstimate->getPixelsPtr(),
-                                  numIterations, dev, reconstructionImage->getPixelsPtr(), likelihood.data(),
-                                  sensitivityImage->getPixelsPtr(), &sm);
+  const float* mult = multiplicative ? multiplicative->getSinogramPtr() : nullptr;
+  const float* add = additive ? additive->getSinogramPtr() : nullptr;
+  apirl_status rc;
+  if (numSubsets == 0) {
+    likelihood.assign(numIterations + 1, 0.0);
+    rc = apirl_mlem_3d(&ig, &sg, inputProjection->getSinogramPtr(), mult, add, initialEstimate->getPixelsPtr(),
+                       numIterations, dev, reconstructionImage->getPixelsPtr(), likelihood.data(),
+                       sensitivityImage->getPixelsPtr(), &sm);
+  } else {
+    likelihood.assign((size_t)numIterations * numSubsets + 1, 0.0);
+    rc = apirl_osem_3d(&ig, &sg, inputProjection->getSinogramPtr(), mult, add, initialEstimate->getPixelsPtr(),
+                       numIterations, numSubsets, dev, reconstructionImage->getPixelsPtr(), likelihood.data(),
+                       sensitivityImage->getPixelsPtr(), &sm);
+  }
   if (rc != APIRL_OK) { strError = apirl_last_error(); return false; }
   double t1 = now_ms();
-  sensitivityImage->writeInterfile((outputFilenamePrefix + "_sensitivity").c_str());
+  sensitivityImage->writeInterfile(
+      (outputFilenamePrefix + (numSubsets == 0 ? "_sensitivity" : "_sensitivity_subset_0")).c_str());
   reconstructionImage->writeInterfile((outputFilenamePrefix + "_final").c_str());
-  writeLog("ML-EM", "Sinogram3D", t1 - t0, {});
+  writeLog(numSubsets == 0 ? "ML-EM" : "OSEM", "Sinogram3D", t1 - t0, {});
   return true;
 }
+
+bool MlemSinogram3d::Reconstruct() { return reconstructOnDevice(0); }
 
 OsemSinogram3d::OsemSinogram3d(Sinogram3D* in, Image* init, std::string path, std::string prefix, int iters,
                                int saveInterval, bool saveInter, bool sensFromFile, Projector* fwd, Projector* back,
@@ -700,25 +971,47 @@ OsemSinogram3d::OsemSinogram3d(Sinogram3D* in, Image* init, std::string path, st
       numSubsets(nsub) {}
 
 bool OsemSinogram3d::Reconstruct() {
-  if (!deviceResident()) { strError = "OsemSinogram3d runs on the GPU and needs CuSiddonProjector"; return false; }
-  double t0 = now_ms();
-  int dev = static_cast<CuSiddonProjector*>(forwardprojector)->gpuId();
-  apirl_image_geom ig = initialEstimate->geom();
-  apirl_sino3d_geom sg = inputProjection->geom();
-  likelihood.assign((size_t)numIterations * numSubsets + 1, 0.0);
-  apirl_sampling sm;
-  if (!sameSampling(&sm)) return false;
-  apirl_status rc = apirl_osem_3d(&ig, &sg, inputProjection->getSinogramPtr(),
-                                  multiplicative ? multiplicative->getSinogramPtr() : nullptr,
-                                  additive ? additive->getSinogramPtr() : nullptr, initialEstimate->getPixelsPtr(),
-                                  numIterations, numSubsets, dev, reconstructionImage->getPixelsPtr(),
-                                  likelihood.data(), sensitivityImage->getPixelsPtr(), &sm);
-  if (rc != APIRL_OK) { strError = apirl_last_error(); return false; }
-  double t1 = now_ms();
-  sensitivityImage->writeInterfile((outputFilenamePrefix + "_sensitivity_subset_0").c_str());
-  reconstructionImage->writeInterfile((outputFilenamePrefix + "_final").c_str());
-  writeLog("OSEM", "Sinogram3D", t1 - t0, {});
-  return true;
+  if (numSubsets < 1) { strError = "number of subsets must be >= 1"; return false; }
+  return reconstructOnDevice(numSubsets);
+}
+
+// ---- CuMlemSinogram3d / CuOsemSinogram3d -----------------------------------------
+CuMlemSinogram3d::CuMlemSinogram3d(Sinogram3D* in, Image* init, std::string path, std::string prefix, int iters,
+                                   int saveInterval, bool saveInter, bool sensFromFile, CuProjector* fwd,
+                                   CuProjector* back)
+    : MlemSinogram3d(in, init, path, prefix, iters, saveInterval, saveInter, sensFromFile,
+                     dynamic_cast<Projector*>(fwd), dynamic_cast<Projector*>(back)) {}
+
+bool CuMlemSinogram3d::Reconstruct() { return reconstructOnDevice(0); }
+
+bool CuMlemSinogram3d::Reconstruct(TipoProyector tipoProy) {
+  if (!deviceResident()) { strError = "CuMlemSinogram3d needs CuSiddonProjector as forward and back projector"; return false; }
+  return Reconstruct(tipoProy, static_cast<CuSiddonProjector*>(forwardprojector)->gpuId());
+}
+
+bool CuMlemSinogram3d::Reconstruct(TipoProyector tipoProy, int indexGpu) {
+  if (tipoProy != SIDDON_CYLINDRICAL_SCANNER && tipoProy != SIDDON_PROJ_TEXT_CYLINDRICAL_SCANNER &&
+      tipoProy != SIDDON_BACKPROJ_SURF_CYLINDRICAL_SCANNER) {
+    strError = "only the cylindrical-scanner Siddon projector kinds are available";
+    return false;
+  }
+  if (!deviceResident()) { strError = "CuMlemSinogram3d needs CuSiddonProjector as forward and back projector"; return false; }
+  auto* f = static_cast<CuSiddonProjector*>(forwardprojector);
+  auto* b = static_cast<CuSiddonProjector*>(backprojector);
+  if (!f->setGpuId(indexGpu)) { strError = f->getError(); return false; }
+  if (!b->setGpuId(indexGpu)) { strError = b->getError(); return false; }
+  return Reconstruct();
+}
+
+CuOsemSinogram3d::CuOsemSinogram3d(Sinogram3D* in, Image* init, std::string path, std::string prefix, int iters,
+                                   int saveInterval, bool saveInter, bool sensFromFile, CuProjector* fwd,
+                                   CuProjector* back, int nsub)
+    : CuMlemSinogram3d(in, init, path, prefix, iters, saveInterval, saveInter, sensFromFile, fwd, back),
+      numSubsets(nsub) {}
+
+bool CuOsemSinogram3d::Reconstruct() {
+  if (numSubsets < 1) { strError = "number of subsets must be >= 1"; return false; }
+  return reconstructOnDevice(numSubsets);
 }
 
 }  // namespace apirl

@@ -10,7 +10,12 @@
 //   Projector ................... recon/inc/Projector.h:48-85
 //   CuSiddonProjector ........... recon/inc/SiddonProjector.h:25-68 (SiddonProjector)
 //                                 and reconGPU/inc/CuSiddonProjector.h:110-158
+//   CuProjector, TipoProyector .. reconGPU/inc/CuProjector.h:63-110,
+//                                 reconGPU/inc/CuSiddonProjector.h:101-106
+//   CuProjectorInterface ........ reconGPU/inc/CuProjectorInterface.h:53-172
 //   Mlem, Mlem2d, MlemSinogram3d, OsemSinogram3d .. recon/inc/Mlem*.h, OsemSinogram3d.h
+//   CuMlemSinogram3d, CuOsemSinogram3d .. reconGPU/inc/CuMlemSinogram3d.h:65-282,
+//                                 reconGPU/inc/CuOsemSinogram3d.h:66-146
 //
 // Everything is in namespace apirl; `using namespace apirl;` gives the
 // reference's spellings.  Compute runs on the GPU through the C ABI; these
@@ -19,6 +24,8 @@
 #include <cstdint>
 #include <string>
 #include <vector>
+
+#include <vector_types.h>  // dim3, as in the reference's GPU-side signatures
 
 #include "../../include/apirl_b200.h"
 
@@ -188,9 +195,57 @@ class Projector {
   std::string strError;
 };
 
-// The Siddon projector on the GPU, as a Projector: host images and sinograms
-// in and out, device buffers and geometry tables cached between calls.
-class CuSiddonProjector : public Projector {
+// reconGPU/inc/CuSiddonProjector.h:101-106.  Every cylindrical kind runs the
+// same exact Siddon walk here (the reference's texture kind sampled the image
+// with trilinear interpolation instead); SIDDON_HEXAGONAL_SCANNER is rejected.
+typedef enum {
+  SIDDON_CYLINDRICAL_SCANNER,
+  SIDDON_PROJ_TEXT_CYLINDRICAL_SCANNER,
+  SIDDON_BACKPROJ_SURF_CYLINDRICAL_SCANNER,
+  SIDDON_HEXAGONAL_SCANNER
+} TipoProyector;
+
+// reconGPU/inc/CuProjector.h:63-110: projection between device buffers.  An
+// image buffer holds the voxels [z][y][x]; a sinogram buffer holds the bins of
+// every sinogram of the Sinogram3D argument in its order, [sinogram][angle][r]
+// (the subset's angles only, for a sinogram made by getSubset).  d_ring1 and
+// d_ring2 hold one float per sinogram, the axial end points in mm; an
+// implementation may take them from the Sinogram3D instead.
+class CuProjector {
+ public:
+  CuProjector();
+  CuProjector(unsigned int numThreadsPerBlockX, unsigned int numThreadsPerBlockY, unsigned int numThreadsPerBlockZ,
+              unsigned int numBlocksX, unsigned int numBlocksY, unsigned int numBlocksZ);
+  virtual ~CuProjector() = default;
+  virtual bool Backproject(float* d_inputSinogram, float* d_outputImage, float* d_ring1, float* d_ring2,
+                           Sinogram3D* inputSinogram, Image* outputImage, bool copyResult) {
+    return false;
+  }
+  virtual bool DivideAndBackproject(float* d_inputSinogram, float* d_estimatedSinogram, float* d_outputImage,
+                                    float* d_ring1, float* d_ring2, Sinogram3D* inputSinogram, Image* outputImage,
+                                    bool copyResult) {
+    return false;
+  }
+  virtual bool Project(float* d_image, float* d_projection, float* d_ring1, float* d_ring2, Image* inputImage,
+                       Sinogram3D* outputSinogram, bool copyResult) {
+    return false;
+  }
+  virtual void initGpuMemory(Sinogram3D*) {}
+  void setKernelConfig(unsigned int numThreadsPerBlockX, unsigned int numThreadsPerBlockY,
+                       unsigned int numThreadsPerBlockZ, unsigned int numBlocksX, unsigned int numBlocksY,
+                       unsigned int numBlocksZ);
+  dim3 getBlockSize() const { return blockSize; }
+  dim3 getGridSize() const { return gridSize; }
+
+ protected:
+  unsigned int threads_per_block = 0;
+  dim3 gridSize, blockSize;
+};
+
+// The Siddon projector on the GPU.  As a Projector: host images and sinograms
+// in and out, device buffers and geometry tables cached between calls.  As a
+// CuProjector: the caller's device buffers in and out.
+class CuSiddonProjector : public Projector, public CuProjector {
  public:
   explicit CuSiddonProjector(int nSamplesOnDetector = 1, int nAxialSamplesOnDetector = 1, int gpuId = 0);
   ~CuSiddonProjector() override;
@@ -200,7 +255,29 @@ class CuSiddonProjector : public Projector {
   bool Project(Image* image, Sinogram3D* projection) override;
   bool Backproject(Sinogram3D* projection, Image* image) override;
   bool DivideAndBackproject(Sinogram3D* in, Sinogram3D* est, Image* out) override;
+  // reconGPU/inc/CuSiddonProjector.h:140-158, on device buffers of the
+  // projector's GPU.  Project overwrites d_projection; Backproject and
+  // DivideAndBackproject add into d_outputImage (the caller zeroes it first,
+  // as the reference's kernels expect) and leave the sinograms unchanged.
+  // copyResult also copies the result into the host object (outputSinogram's
+  // bins, outputImage's pixels).  The axial end points come from the
+  // Sinogram3D as SiddonProjector computes them, so d_ring1 and d_ring2 are
+  // not read and may be NULL.  The work runs on the legacy default stream and
+  // is finished when the call returns, like the reference's wrappers.
+  bool Project(float* d_image, float* d_projection, float* d_ring1, float* d_ring2, Image* inputImage,
+               Sinogram3D* outputSinogram, bool copyResult) override;
+  bool Backproject(float* d_inputSinogram, float* d_outputImage, float* d_ring1, float* d_ring2,
+                   Sinogram3D* inputSinogram, Image* outputImage, bool copyResult) override;
+  bool DivideAndBackproject(float* d_inputSinogram, float* d_estimatedSinogram, float* d_outputImage,
+                            float* d_ring1, float* d_ring2, Sinogram3D* inputSinogram, Image* outputImage,
+                            bool copyResult) override;
+  // reconGPU/src/CuSiddonProjector.cu:34-44.  Nothing is set up ahead: the
+  // geometry tables are built by the first call that also knows the image.
+  bool InitGpuMemory(Sinogram3D*) { return true; }
+  void initGpuMemory(Sinogram3D* s) override { InitGpuMemory(s); }
   int gpuId() const { return device; }
+  // Moves the projector to GPU `id`; what was set up on another GPU is freed.
+  bool setGpuId(int id);
   // The rays per bin this projector walks (SiddonProjector.h:43-47, Projector.h:54).
   apirl_sampling sampling() const { return {numSamplesOnDetector, numAxialSamplesOnDetector, useMultipleLorsPerBin}; }
 
@@ -212,6 +289,46 @@ class CuSiddonProjector : public Projector {
   bool prepare2d(const Image* img, const Sinogram2D* s);
   bool prepare3d(const Image* img, const Sinogram3D* s);
   bool run(int op, Image* img, const float* a, const float* b, float* out_sino, size_t nbins, int subset, int nsub);
+  bool runDevice(int op, const float* d_a, const float* d_b, float* d_out, Image* img, Sinogram3D* s,
+                 bool copyResult);
+  void release();
+};
+
+// reconGPU/inc/CuProjectorInterface.h:53-172: a CuProjector used as a
+// Projector, with host images and sinograms in and out and device buffers
+// kept between calls (the reference allocated and freed them per call).
+// Sinogram3D only: the Sinogram2D calls return false, as the reference's do.
+// Project overwrites the sinogram; Backproject and DivideAndBackproject
+// overwrite the image (the reference zeroes its device image first).  The
+// ring arrays given to the CuProjector are the per-sinogram axial end points,
+// apirl_sino3d_ring_z.  The CuProjector stays the caller's.
+class CuProjectorInterface : public Projector {
+ public:
+  explicit CuProjectorInterface(CuProjector* projector);
+  ~CuProjectorInterface() override;
+  // Block size as given; grid = (ceil(nProj * nR / x), number of sinograms, 1)
+  // (CuProjectorInterface.cu:152-172), passed to the CuProjector.
+  void setProjectorKernelConfig(unsigned int numThreadsPerBlockX, unsigned int numThreadsPerBlockY,
+                                unsigned int numThreadsPerBlockZ, Sinogram3D* sinogram);
+  void setProjectorKernelConfig(dim3 blockSize, Sinogram3D* sinogram);
+  void setProjectorBlockSizeConfig(dim3 blockSize) { blockSizeProjector = blockSize; }
+  bool setGpuId(int id);
+  bool Project(Image* image, Sinogram2D* projection) override;
+  bool Backproject(Sinogram2D* projection, Image* image) override;
+  bool DivideAndBackproject(Sinogram2D* in, Sinogram2D* est, Image* out) override;
+  bool Project(Image* image, Sinogram3D* projection) override;
+  bool Backproject(Sinogram3D* projection, Image* image) override;
+  bool DivideAndBackproject(Sinogram3D* in, Sinogram3D* est, Image* out) override;
+
+ private:
+  bool prepare(Sinogram3D* s, Image* img, bool estimate);
+  void release();
+  CuProjector* projector;
+  int gpuId = 0, bufDevice = -1;
+  dim3 blockSizeProjector;
+  float *d_image = nullptr, *d_projection = nullptr, *d_estimated = nullptr;
+  float *d_ring1_mm = nullptr, *d_ring2_mm = nullptr;
+  size_t nImage = 0, nBins = 0, nEstimated = 0, nSinos = 0;
 };
 
 // recon/inc/Mlem.h:82-297.
@@ -283,6 +400,8 @@ class MlemSinogram3d : public Mlem {
  protected:
   bool deviceResident() const;
   bool sameSampling(apirl_sampling* out);
+  // The fused device driver: ML-EM for numSubsets == 0, else OSEM.
+  bool reconstructOnDevice(int numSubsets);
   Sinogram3D* inputProjection;
   Sinogram3D* multiplicative = nullptr;
   Sinogram3D* additive = nullptr;
@@ -293,6 +412,52 @@ class OsemSinogram3d : public MlemSinogram3d {
   OsemSinogram3d(Sinogram3D* inputProjection, Image* initialEstimate, std::string pathSalida,
                  std::string outputPrefix, int numIterations, int saveIterationInterval, bool saveIntermediate,
                  bool sensitivityFromFile, Projector* forwardprojector, Projector* backprojector, int numSubsets);
+  bool Reconstruct() override;
+
+ private:
+  int numSubsets;
+};
+
+// reconGPU/inc/CuMlemSinogram3d.h:65-282: ML-EM with CuProjector pointers.
+// Both projectors must be CuSiddonProjector with the same rays per bin; the
+// iterations run in MlemSinogram3d's fused device driver.  The kernel
+// configuration setters keep the block sizes they are given (getters below)
+// and check nothing: launch shapes are the library's.
+class CuMlemSinogram3d : public MlemSinogram3d {
+ public:
+  CuMlemSinogram3d(Sinogram3D* inputProjection, Image* initialEstimate, std::string pathSalida,
+                   std::string outputPrefix, int numIterations, int saveIterationInterval, bool saveIntermediate,
+                   bool sensitivityFromFile, CuProjector* forwardprojector, CuProjector* backprojector);
+  void setProjectorKernelConfig(unsigned int x, unsigned int y, unsigned int z) { blockSizeProjector = dim3(x, y, z); }
+  void setBackprojectorKernelConfig(unsigned int x, unsigned int y, unsigned int z) {
+    blockSizeBackprojector = dim3(x, y, z);
+  }
+  void setUpdatePixelKernelConfig(unsigned int x, unsigned int y, unsigned int z) { blockSizeImageUpdate = dim3(x, y, z); }
+  void setProjectorKernelConfig(dim3* b) { blockSizeProjector = *b; }
+  void setBackprojectorKernelConfig(dim3* b) { blockSizeBackprojector = *b; }
+  void setUpdatePixelKernelConfig(dim3* b) { blockSizeImageUpdate = *b; }
+  dim3 getProjectorKernelConfig() const { return blockSizeProjector; }
+  dim3 getBackprojectorKernelConfig() const { return blockSizeBackprojector; }
+  dim3 getUpdatePixelKernelConfig() const { return blockSizeImageUpdate; }
+  // On the projectors' GPU.
+  bool Reconstruct() override;
+  virtual bool Reconstruct(TipoProyector tipoProy);
+  // Moves both projectors to GPU indexGpu first (CuMlemSinogram3d.cu:498).
+  virtual bool Reconstruct(TipoProyector tipoProy, int indexGpu);
+
+ protected:
+  dim3 blockSizeProjector{128, 1, 1}, blockSizeBackprojector{128, 1, 1}, blockSizeImageUpdate{512, 1, 1};
+};
+
+// reconGPU/inc/CuOsemSinogram3d.h:66-146: OSEM with CuProjector pointers, run
+// by OsemSinogram3d's device driver.
+class CuOsemSinogram3d : public CuMlemSinogram3d {
+ public:
+  CuOsemSinogram3d(Sinogram3D* inputProjection, Image* initialEstimate, std::string pathSalida,
+                   std::string outputPrefix, int numIterations, int saveIterationInterval, bool saveIntermediate,
+                   bool sensitivityFromFile, CuProjector* forwardprojector, CuProjector* backprojector,
+                   int numSubsets);
+  using CuMlemSinogram3d::Reconstruct;
   bool Reconstruct() override;
 
  private:
