@@ -142,6 +142,7 @@ apirl_status finish_create(apirl_projector* p, apirl_projector** out) {
   CK(cudaMalloc(&p->d_minmax, 2 * sizeof(unsigned)));
   CK(cudaMalloc(&p->d_scalars, 8 * sizeof(double)));
   CK(cudaMalloc(&p->d_chunk, sizeof(unsigned long long)));
+  if (p->is3d) CK(apirl::prepare_em_kernels(p->em_block));
   if (p->is3d && p->dual_layout) {
     const apirl_status st = alloc_pad(p);
     if (st) return st;
@@ -691,6 +692,10 @@ apirl_status apirl_projector_set_option(apirl_projector* p, int option, int valu
     case APIRL_OPT_EM_BLOCK:
       if (value < 32 || value > 256 || value % 32) return fail(APIRL_ERR_INVALID, "block size must be 32..256, x32");
       p->em_block = value;
+      if (p->is3d) {
+        DEVICE_SCOPE(p->device);
+        CK(apirl::prepare_em_kernels(value));
+      }
       return APIRL_OK;
     default: return fail(APIRL_ERR_INVALID, "unknown option %d", option);
   }
@@ -730,6 +735,10 @@ apirl_status apirl_projector_autotune(apirl_projector* p, const void* d_counts, 
   }
   p->timing = saved_timing;
   p->em_block = best_b;
+  if (!st) {
+    cudaError_t pe = apirl::prepare_em_kernels(best_b);
+    if (pe != cudaSuccess) st = fail(APIRL_ERR_CUDA, "prepare_em_kernels: %s", cudaGetErrorString(pe));
+  }
   cudaEventDestroy(a);
   cudaEventDestroy(b);
   cudaFree(bp);

@@ -107,6 +107,10 @@ cudaError_t launch_em_pass(const ImgGeom& g, const LorTable& t, SubsetSel s, con
                            double* partials, double* lik, cudaStream_t st, const PreciseGeom& pg = PreciseGeom(),
                            const PadBuffers& pad = PadBuffers(), int block = 0, const float* zimg = nullptr,
                            const double* zero_add = nullptr, unsigned long long* persist_counter = nullptr);
+// Fits the shared-memory carveout of the persistent fused kernels to `block`
+// threads per block (called outside graph capture, when a projector is made
+// or its block size changes).
+cudaError_t prepare_em_kernels(int block);
 // Sparse pass (zimg set, 3D float walk): bins with zero counts are not walked;
 // the likelihood subtracts x . zimg + *zero_add instead of their estimates.
 // zimg = A_s^T 1[m == 0] and zero_add = sum of those bins' additive terms,

@@ -14,6 +14,8 @@
 #include <cstdint>
 #include <cfloat>
 #include <atomic>
+#include <mutex>
+#include <vector>
 #include "internal.h"
 #include "siddon.cuh"
 #include "../../include/apirl_b200.h"
@@ -846,10 +848,50 @@ void prefer_l1() {
   cudaFuncSetAttribute(k_em_pass<float, true, false>, cudaFuncAttributePreferredSharedMemoryCarveout, 0);
   cudaFuncSetAttribute(k_em_pass<uint32_t, true, false>, cudaFuncAttributePreferredSharedMemoryCarveout, 0);
   cudaFuncSetAttribute(k_em_pass<uint16_t, true, false>, cudaFuncAttributePreferredSharedMemoryCarveout, 0);
-  cudaFuncSetAttribute(k_em_pass_persist<float>, cudaFuncAttributePreferredSharedMemoryCarveout, 0);
-  cudaFuncSetAttribute(k_em_pass_persist<uint32_t>, cudaFuncAttributePreferredSharedMemoryCarveout, 0);
-  cudaFuncSetAttribute(k_em_pass_persist<uint16_t>, cudaFuncAttributePreferredSharedMemoryCarveout, 0);
   (void)cudaGetLastError();
+}
+
+// The persistent kernel's carveout: the shared memory that its resident
+// blocks need (static, dynamic and the per-block reserve,
+// cudaDevAttrReservedSharedMemoryPerBlock), at as many blocks per SM as its
+// registers and threads allow, and all the rest for L1.  A preferred carveout
+// of 0 can leave room for fewer blocks' reserves than the registers allow
+// (with 128 threads per block, 10 blocks fit in the registers at 48 per
+// thread, 8 blocks' reserves in the smallest carveout), which costs warps.
+// Fitted again when the block size changes (the attribute is per function).
+std::mutex g_carve_mu;
+struct CarveFit {
+  const void* f;
+  int dev, block;
+};
+std::vector<CarveFit> g_carve;
+
+cudaError_t fit_carveout(const void* f, int block, size_t dyn_smem) {
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return e;
+  std::lock_guard<std::mutex> lock(g_carve_mu);
+  CarveFit* slot = nullptr;
+  for (CarveFit& c : g_carve)
+    if (c.f == f && c.dev == dev) slot = &c;
+  if (slot && slot->block == block) return cudaSuccess;
+  cudaFuncAttributes fa;
+  int per_sm = 0, reserved = 0, max_sm = 0;
+  if ((e = cudaFuncGetAttributes(&fa, f)) != cudaSuccess) return e;
+  if ((e = cudaDeviceGetAttribute(&reserved, cudaDevAttrReservedSharedMemoryPerBlock, dev)) != cudaSuccess) return e;
+  if ((e = cudaDeviceGetAttribute(&max_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, dev)) != cudaSuccess) return e;
+  // With every byte offered to shared memory, residency is set by the
+  // registers and threads alone.
+  if ((e = cudaFuncSetAttribute(f, cudaFuncAttributePreferredSharedMemoryCarveout, 100)) != cudaSuccess) return e;
+  if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, f, block, dyn_smem)) != cudaSuccess) return e;
+  if (max_sm <= 0) return cudaErrorInvalidValue;
+  const int64_t need = (int64_t)(per_sm < 1 ? 1 : per_sm) * ((int64_t)fa.sharedSizeBytes + (int64_t)dyn_smem + reserved);
+  int pct = (int)((need * 100 + max_sm - 1) / max_sm);
+  pct = pct < 1 ? 1 : (pct > 100 ? 100 : pct);
+  if ((e = cudaFuncSetAttribute(f, cudaFuncAttributePreferredSharedMemoryCarveout, pct)) != cudaSuccess) return e;
+  if (slot) slot->block = block;
+  else g_carve.push_back(CarveFit{f, dev, block});
+  return cudaSuccess;
 }
 
 // Deterministic sum of n partials into *out.  Above kSumLevel2 * 64 partials
@@ -871,6 +913,16 @@ inline unsigned stream_grid(int64_t n) {
 }
 
 }  // namespace
+
+cudaError_t prepare_em_kernels(int block) {
+  for (const void* f : {(const void*)k_em_pass_persist<float>, (const void*)k_em_pass_persist<uint32_t>,
+                        (const void*)k_em_pass_persist<uint16_t>}) {
+    cudaError_t e = fit_carveout(f, block, 0);
+    if (e != cudaSuccess) return e;
+  }
+  return cudaSuccess;
+}
+
 
 int64_t em_pass_blocks(const LorTable& t, SubsetSel s) {
   // One likelihood partial per warp for any block size of 32..256 threads
@@ -942,6 +994,15 @@ cudaError_t launch_em_pass(const ImgGeom& g, const LorTable& t, SubsetSel s, con
     prefer_l1();
     // Persistent form: as many blocks of this size as fit on the current
     // device's SMs at once (a host-side query of a few microseconds).
+    const void* pf = counts_dtype == APIRL_F32   ? (const void*)k_em_pass_persist<float>
+                     : counts_dtype == APIRL_U32 ? (const void*)k_em_pass_persist<uint32_t>
+                                                 : (const void*)k_em_pass_persist<uint16_t>;
+    // Fitted here unless the launch is being captured into a graph (the
+    // projector fits it ahead for its block size: prepare_em_kernels).
+    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+    cudaError_t fe = cudaStreamIsCapturing(st, &cs);
+    if (fe != cudaSuccess) return fe;
+    if (cs == cudaStreamCaptureStatusNone && (fe = fit_carveout(pf, block, 0)) != cudaSuccess) return fe;
     int per_sm = 0, dev = 0, sms = 0;
     cudaError_t oe = counts_dtype == APIRL_F32
         ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_em_pass_persist<float>, block, 0)

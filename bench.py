@@ -295,7 +295,11 @@ def run_gpu(args):
 
     from apirl_b200 import _lib as _l
     # autotuner: fused-kernel block size, timed on this job's own data (outside the timed region)
-    best_block = P.autotune(counts, x, 0, NSUB, repeats=2, stream=stream)
+    if args.em_block:
+        P.set_option(_l.APIRL_OPT_EM_BLOCK, args.em_block)
+        best_block = args.em_block
+    else:
+        best_block = P.autotune(counts, x, 0, NSUB, repeats=2, stream=stream)
     bp.zero_()
     torch.cuda.synchronize(dev)
     log(f"autotuned fused-kernel block size: {best_block}")
@@ -755,6 +759,8 @@ def main():
     ap_.add_argument("--pass", dest="pass_form", default="full", choices=["sparse", "full"],
                      help="sparse: bins with zero counts are not walked (their likelihood terms from per-subset "
                           "zero-count images computed inside the timed region); full: every bin walked")
+    ap_.add_argument("--em-block", type=int, default=0,
+                     help="threads per block of the fused kernel (0: autotuned on the job's own data)")
     ap_.add_argument("--persistent", type=int, default=1, choices=[0, 1],
                      help="1: the fused pass as a persistent kernel whose warps pull 32-bin chunks")
     ap_.add_argument("--shard", action="store_true",
