@@ -122,7 +122,7 @@ __device__ __forceinline__ float next_crossing(const Walk3& w, bool& cx, bool& c
 // Segments per iteration of the guarded gather: their voxel loads are all
 // issued before any product is added (the additions keep the walk order).
 #ifndef APIRL_GATHER_UNROLL
-#define APIRL_GATHER_UNROLL 6
+#define APIRL_GATHER_UNROLL 4
 #endif
 __device__ __forceinline__ float siddon3_gather_pad(Walk3 w, const ImgGeom& g, int ux, int uy, int uz, unsigned lim,
                                                     const float* __restrict__ img) {

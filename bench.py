@@ -38,9 +38,9 @@ NSUB = 21
 TOTAL_COUNTS = 5e8
 L2_FLUSH_BYTES = 256 << 20
 # DRAM bytes (read + write) per fused-kernel launch of the full workload,
-# mean of three launches captured with ncu --metrics dram__bytes_read.sum,
+# mean of the four timed launches captured with ncu --metrics dram__bytes_read.sum,
 # dram__bytes_write.sum (one pass; profiles/k_em_pass_osem3d_256x256x81.md).
-FULL_TRAFFIC_BYTES = 2.208e8
+FULL_TRAFFIC_BYTES = 2.603e8
 WORKLOAD = ("3D OSEM 256x256x81 image, 41 rings span-1 |rd|<=20: 1261 sinograms x 336 angles x 336 r, "
             "21 subsets, attenuation in sensitivity, 5e8 counts uint32")
 
