@@ -791,10 +791,15 @@ apirl_status apirl_stage_counts(apirl_projector* p, const void* h_counts_subset,
   return APIRL_OK;
 }
 
-apirl_status apirl_em_pass_host(apirl_projector* p, const void* h_counts_subset, int counts_dtype,
-                                void* d_counts_stage, float* d_x, float* d_bp, const float* d_sens,
-                                const float* d_zimg, const double* d_zero_add, float thr_value, int ge, int subset,
-                                int nsubsets, float* h_x_out, double* h_lik, void* stream) {
+}  // extern "C"
+
+namespace {
+// apirl_em_pass_host and apirl_em_pass_host_async; `wait`: synchronise the
+// stream before returning.
+apirl_status em_pass_host(apirl_projector* p, const void* h_counts_subset, int counts_dtype, void* d_counts_stage,
+                          float* d_x, float* d_bp, const float* d_sens, const float* d_zimg,
+                          const double* d_zero_add, float thr_value, int ge, int subset, int nsubsets,
+                          float* h_x_out, double* h_lik, void* stream, bool wait) {
   apirl_status st = check_subset(p, subset, nsubsets);
   if (st) return st;
   if (!h_counts_subset || !d_counts_stage) return fail(APIRL_ERR_INVALID, "null buffer");
@@ -823,8 +828,27 @@ apirl_status apirl_em_pass_host(apirl_projector* p, const void* h_counts_subset,
   const int64_t nv = (int64_t)p->g.nx * p->g.ny * p->g.nz;
   if (h_x_out) CK(cudaMemcpyAsync(h_x_out, d_x, nv * sizeof(float), cudaMemcpyDeviceToHost, s));
   if (h_lik) CK(cudaMemcpyAsync(h_lik, d_lik, sizeof(double), cudaMemcpyDeviceToHost, s));
-  CK(cudaStreamSynchronize(s));
+  if (wait) CK(cudaStreamSynchronize(s));
   return APIRL_OK;
+}
+}  // namespace
+
+extern "C" {
+
+apirl_status apirl_em_pass_host(apirl_projector* p, const void* h_counts_subset, int counts_dtype,
+                                void* d_counts_stage, float* d_x, float* d_bp, const float* d_sens,
+                                const float* d_zimg, const double* d_zero_add, float thr_value, int ge, int subset,
+                                int nsubsets, float* h_x_out, double* h_lik, void* stream) {
+  return em_pass_host(p, h_counts_subset, counts_dtype, d_counts_stage, d_x, d_bp, d_sens, d_zimg, d_zero_add,
+                      thr_value, ge, subset, nsubsets, h_x_out, h_lik, stream, true);
+}
+
+apirl_status apirl_em_pass_host_async(apirl_projector* p, const void* h_counts_subset, int counts_dtype,
+                                      void* d_counts_stage, float* d_x, float* d_bp, const float* d_sens,
+                                      const float* d_zimg, const double* d_zero_add, float thr_value, int ge,
+                                      int subset, int nsubsets, float* h_x_out, double* h_lik, void* stream) {
+  return em_pass_host(p, h_counts_subset, counts_dtype, d_counts_stage, d_x, d_bp, d_sens, d_zimg, d_zero_add,
+                      thr_value, ge, subset, nsubsets, h_x_out, h_lik, stream, false);
 }
 
 }  // extern "C"

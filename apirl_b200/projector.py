@@ -206,11 +206,14 @@ class SiddonProjector:
                                           subset, nsubsets, _stream(stream)))
 
     def em_pass_host(self, h_counts_subset, stage, x, bp, sens, subset, nsubsets, h_x_out, h_lik=None,
-                     thr_value=0.0, ge=True, stream=None, zimg=None, zero_add=None):
+                     thr_value=0.0, ge=True, stream=None, zimg=None, zero_add=None, wait=True):
         """em_pass (em_pass_sparse when zimg is given) from host counts (packed
-        subset, numpy) to a host image; blocks until done."""
+        subset, numpy) to a host image; blocks until done, or with wait=False
+        returns once queued (apirl_em_pass_host_async: h_x_out / h_lik, which
+        should be page-locked, are filled when the stream gets there)."""
         dt = {"float32": _lib.APIRL_F32, "uint32": _lib.APIRL_U32, "uint16": _lib.APIRL_U16}[str(h_counts_subset.dtype)]
-        check(self.lib.apirl_em_pass_host(self.h, ctypes.c_void_p(h_counts_subset.ctypes.data), dt, _ptr(stage),
+        fn = self.lib.apirl_em_pass_host if wait else self.lib.apirl_em_pass_host_async
+        check(fn(self.h, ctypes.c_void_p(h_counts_subset.ctypes.data), dt, _ptr(stage),
                                           _ptr(x), _ptr(bp), _ptr(sens), _ptr(zimg), _ptr(zero_add),
                                           float(thr_value), int(ge), subset, nsubsets,
                                           None if h_x_out is None else ctypes.c_void_p(h_x_out.ctypes.data),

@@ -87,7 +87,8 @@ class GpuShard:
     """The CUDA backend: a projector restricted to sinograms [first, first + n),
     the whole job's counts (and multiplicative term) resident on `device`."""
 
-    def __init__(self, image_geom, sino_geom, counts, nsubsets, first, n, device=0, mult=None, stream=None):
+    def __init__(self, image_geom, sino_geom, counts, nsubsets, first, n, device=0, mult=None, stream=None,
+                 ge=True):
         import torch
         from .projector import SiddonProjector
         self.torch = torch
@@ -100,6 +101,7 @@ class GpuShard:
         self.first, self.n = first, n
         self.nsub = nsubsets
         self.stream = stream
+        self.ge = ge                  # update where sens >= 0 (the reference's OSEM rule) or > 0
 
     def zeros_image(self):
         return self.torch.zeros(self.ig.n_voxels, dtype=self.torch.float32, device=self.dev)
@@ -126,4 +128,4 @@ class GpuShard:
 
     def update(self, x, bp, sens):
         from .projector import update_pixels
-        update_pixels(x, bp, sens, thr_value=0.0, ge=True, zero_bp=True, stream=self.stream)
+        update_pixels(x, bp, sens, thr_value=0.0, ge=self.ge, zero_bp=True, stream=self.stream)

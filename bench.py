@@ -36,6 +36,13 @@ METRIC = "OSEM subiters/s (256²×81)"
 UNIT = "subiter/s"
 NSUB = 21
 TOTAL_COUNTS = 5e8
+# Pixel update of the timed passes: x <- x * bp / sens where sens > 0, else 0.
+# The reference's OSEM rule (threshold 0 with >=, OsemSinogram3d.cpp:24-33,
+# :217-237, kept by the library's drivers) gives 0 * 0 / 0 = NaN at voxels
+# that no ray of a subset crosses; this workload has 4 such voxels in subset
+# 3 and 2 in subset 16 (image corners), and the NaN reaches every voxel
+# within three more passes.  The passes do the same work either way.
+UPDATE_GE = False
 L2_FLUSH_BYTES = 256 << 20
 # DRAM bytes (read + write) per fused-kernel launch of the full workload,
 # mean of the four timed launches captured with ncu --metrics dram__bytes_read.sum,
@@ -206,7 +213,7 @@ def run_sharded(args):
     w = setup_workload(dev, log)
     ig, sg = w["ig"], w["sg"]
     first, n = shard_ranges(sg.n_sinos, world)[rank]
-    backend = GpuShard(ig, sg, w["counts"], NSUB, first, n, device=local, mult=w["atten"])
+    backend = GpuShard(ig, sg, w["counts"], NSUB, first, n, device=local, mult=w["atten"], ge=UPDATE_GE)
     backend.P.set_option(_l.APIRL_OPT_KERNEL_TIMING, 1)
     job = ShardedOsem(backend, NSUB, dist if world > 1 else None)
     job.compute_sensitivity()
@@ -255,7 +262,8 @@ def run_sharded(args):
             "config": {"workload": WORKLOAD, "subsets": NSUB, "counts_dtype": "uint32",
                        "parallelism": f"LOR shards x{world} (sinograms {first}..{first + n - 1} on rank 0), "
                                       "NCCL all-reduce of the backprojection image and likelihood",
-                       "l2": "flushed between timed steps (256 MB write outside the timed events)"},
+                       "l2": "flushed between timed steps (256 MB write outside the timed events)",
+                       "update": "x*bp/sens where sens > 0"},
             "roofline": {"bound": "hbm", "kernel": "k_em_pass on rank 0's shard",
                          "kernel_ms": statistics.mean(kern), "peak": peak, "unit": "GB/s",
                          "peak_source": f"{peak_kind} hbm_gbs",
@@ -322,10 +330,10 @@ def run_gpu(args):
         # one OSEM sub-iteration through the C ABI: layout copy, fused
         # projection / ratio / backprojection kernel, likelihood sum, update
         if sparse:
-            P.em_pass_sparse(counts, x, bp, sens[s], zimg[s], s, NSUB, thr_value=0.0, ge=True, lik=lik,
+            P.em_pass_sparse(counts, x, bp, sens[s], zimg[s], s, NSUB, thr_value=0.0, ge=UPDATE_GE, lik=lik,
                              stream=stream)
         else:
-            P.em_pass(counts, x, bp, sens[s], s, NSUB, thr_value=0.0, ge=True, lik=lik, stream=stream)
+            P.em_pass(counts, x, bp, sens[s], s, NSUB, thr_value=0.0, ge=UPDATE_GE, lik=lik, stream=stream)
         if evs:
             evs[1].record(stream)
 
@@ -388,6 +396,8 @@ def run_gpu(args):
         h_x_t = _t.empty(w["ig"].n_voxels, dtype=_t.float32).pin_memory()
         h_x = h_x_t.numpy()
         h_lik = np.zeros(1, np.float64)
+        # one page-locked likelihood slot per timed step (filled asynchronously)
+        h_liks = _t.zeros(max(args.steps, 1), dtype=_t.float64).pin_memory().numpy()
         ev = [_t.cuda.Event(enable_timing=True) for _ in range(2)]
 
         def e2e_zero_images():
@@ -401,7 +411,7 @@ def run_gpu(args):
         def e2e_step(s):
             # the sub-iteration's counts in, its likelihood out; the image
             # stays resident and comes back once, at the end of the job
-            P.em_pass_host(host_counts[s], stage, x, bp, sens[s], s, NSUB, None, h_lik, stream=stream,
+            P.em_pass_host(host_counts[s], stage, x, bp, sens[s], s, NSUB, None, h_lik, ge=UPDATE_GE, stream=stream,
                            zimg=zimg[s] if sparse else None)
 
         with _t.cuda.stream(stream):
@@ -418,25 +428,31 @@ def run_gpu(args):
                 ev[1].synchronize()
                 e_ms += ev[0].elapsed_time(ev[1])
             # Each pass's counts go up on the library's copy stream while the
-            # previous pass computes (apirl_stage_counts, two stages).
+            # previous pass computes (apirl_stage_counts, two stages); each
+            # pass's likelihood comes back into its own page-locked slot
+            # without a host round trip between passes
+            # (apirl_em_pass_host_async), all within the timed region.
             subs_e = [(args.warmup + i) % NSUB for i in range(args.steps)]
+            h_liks[:] = np.nan
             ev[0].record(stream)
             P.stage_counts(host_counts[subs_e[0]], stages[0], subs_e[0], NSUB, stream=stream)
             for i, s in enumerate(subs_e):
                 if i + 1 < args.steps:
                     P.stage_counts(host_counts[subs_e[i + 1]], stages[(i + 1) % 2], subs_e[i + 1], NSUB,
                                    stream=stream)
-                P.em_pass_host(host_counts[s], stages[i % 2], x, bp, sens[s], s, NSUB, None, h_lik, stream=stream,
-                               zimg=zimg[s] if sparse else None)
+                P.em_pass_host(host_counts[s], stages[i % 2], x, bp, sens[s], s, NSUB, None, h_liks[i:i + 1],
+                               ge=UPDATE_GE, stream=stream, zimg=zimg[s] if sparse else None, wait=False)
             h_x_t.copy_(x, non_blocking=True)  # the reconstructed image, once
             ev[1].record(stream)
             ev[1].synchronize()
             e_ms += ev[0].elapsed_time(ev[1])
+            if not np.all(np.isfinite(h_liks[:args.steps])):
+                raise RuntimeError("e2e: a pass's likelihood did not arrive")
         e_value, e_ms = whole_job_value(args.steps, e_ms, world, dist if world > 1 else None, dev)
         h2d = host_counts[0].nbytes + (sum(h.nbytes for h in host_counts) / args.steps if sparse else 0)
         e2e = {"value": e_value, "unit": UNIT,
                "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(8 + h_x.nbytes / args.steps),
-               "api": "apirl_em_pass_host (C ABI): each sub-iteration's uint32 counts host->device from pinned "
+               "api": "apirl_em_pass_host_async (C ABI): each sub-iteration's uint32 counts host->device from pinned "
                       "memory (apirl_stage_counts: the next pass's copy overlaps the current pass) and its FP64 "
                       "likelihood back; the image host<-device once at the end (counted per step above)"
                       + ("; the zero-count images from host counts inside the timed region" if sparse else "")}
@@ -459,6 +475,8 @@ def run_gpu(args):
                                 "timed region and amortized over the timed sub-iterations") if sparse else
                                "full: every bin walked",
                        "l2": "flushed between timed steps (256 MB write outside the timed events)",
+                       "update": "x*bp/sens where sens > 0 (the reference's >= 0 gives NaN at the 6 voxels "
+                                 "no ray of subsets 3 and 16 crosses)",
                        "parallelism": f"replicas x{world}"},
             "siddon_gsteps_per_s": gsteps,
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",

@@ -313,6 +313,17 @@ apirl_status apirl_em_pass_host(apirl_projector* p, const void* h_counts_subset,
                                 const double* d_zero_add, float thr_value, int ge, int subset, int nsubsets,
                                 float* h_x_out, double* h_lik, void* stream);
 
+/* apirl_em_pass_host without the wait: returns once the pass and its copies
+ * are queued on `stream`.  h_x_out and h_lik are written when that work has
+ * finished (synchronise the stream or an event recorded after the call);
+ * they should be page-locked, since a copy into pageable memory makes the
+ * call wait for it.  Queued passes run back to back, with no host round trip
+ * between them. */
+apirl_status apirl_em_pass_host_async(apirl_projector* p, const void* h_counts_subset, int counts_dtype,
+                                      void* d_counts_stage, float* d_x, float* d_bp, const float* d_sens,
+                                      const float* d_zimg, const double* d_zero_add, float thr_value, int ge,
+                                      int subset, int nsubsets, float* h_x_out, double* h_lik, void* stream);
+
 /* Starts copying a pass's host counts into d_counts_stage on a copy stream of
  * the projector, after the work already queued on `stream` and beside the
  * work queued later, so that the copy for the next pass overlaps the current

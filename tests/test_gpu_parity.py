@@ -515,7 +515,9 @@ def test_persistent_pass_equals_plain_pass(oracle):
 
 
 def test_staged_counts_host_pass(oracle):
-    """apirl_stage_counts + apirl_em_pass_host equal the unstaged host pass."""
+    """apirl_stage_counts + apirl_em_pass_host, and the same passes queued
+    back to back with apirl_em_pass_host_async (likelihoods into page-locked
+    slots, read after one synchronisation), equal the unstaged host pass."""
     ig, sg = small_3d()
     rng = np.random.default_rng(24)
     x0 = (rng.random(ig.n_voxels, dtype=np.float32) + 0.5).astype(np.float32)
@@ -526,19 +528,19 @@ def test_staged_counts_host_pass(oracle):
     P = ap.SiddonProjector(ig, sg)
     stages = [torch.zeros(host[0].size, dtype=torch.int32, device=DEV) for _ in range(2)]
     res = []
-    for staged in (False, True):
+    for staged, wait in ((False, True), (True, True), (True, False)):
         x = t(x0)
         bp = torch.zeros(ig.n_voxels, dtype=torch.float32, device=DEV)
-        liks = []
+        slots = torch.full((ns,), float("nan"), dtype=torch.float64).pin_memory().numpy()
         if staged:
             P.stage_counts(host[0], stages[0], 0, ns)
         for s in range(ns):
             if staged and s + 1 < ns:
                 P.stage_counts(host[s + 1], stages[(s + 1) % 2], s + 1, ns)
-            h_lik = np.zeros(1, np.float64)
-            P.em_pass_host(host[s], stages[s % 2], x, bp, sens, s, ns, None, h_lik)
-            liks.append(h_lik[0])
-        res.append((x.cpu().numpy(), liks))
-    assert rel(res[1][0], res[0][0]) <= 1e-6
-    assert res[1][1][0] == res[0][1][0]  # later passes see images that differ in fp32 atomic order
-    assert np.allclose(res[1][1], res[0][1], rtol=1e-7)
+            P.em_pass_host(host[s], stages[s % 2], x, bp, sens, s, ns, None, slots[s:s + 1], wait=wait)
+        torch.cuda.synchronize()
+        res.append((x.cpu().numpy(), slots.copy()))
+    for x, liks in res[1:]:
+        assert rel(x, res[0][0]) <= 1e-6
+        assert liks[0] == res[0][1][0]  # later passes see images that differ in fp32 atomic order
+        assert np.allclose(liks, res[0][1], rtol=1e-7)
