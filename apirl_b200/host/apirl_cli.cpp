@@ -1,6 +1,6 @@
 // The reference's .par-driven commands on the GPU path: MLEM, OSEM, project,
-// backproject and cuMLEM (cmd/src/MLEM.cpp, OSEM.cpp, project.cpp,
-// backproject.cpp, cmdGPU/src/cuMLEM.cpp).
+// backproject, generateACFs and cuMLEM (cmd/src/MLEM.cpp, OSEM.cpp,
+// project.cpp, backproject.cpp, generateACFs.cpp, cmdGPU/src/cuMLEM.cpp).
 // One source; the command is chosen at build time with -DAPIRL_COMMAND=<name>
 // (the binary's name).  Each takes one argument, a parameter file ending in
 // .par whose first line is "<COMMAND> Parameters :=".
@@ -16,6 +16,10 @@
 //              projection, number of subsets, subset index (+ scanner keys)
 //   backproject input type, input file, backprojector, output image, output
 //              filename, number of subsets, subset index (+ scanner keys)
+//   generateACFs input file (attenuation map, 1/cm), output type (Sinogram2D,
+//              Sinogram3D, Sinogram3DSiemensMmr), output filename, output
+//              projection, projector (Siddon, CuSiddonProjector: + projector
+//              block size, gpu id) (+ scanner keys)
 //   cuMLEM     section "MLEM": input type (Sinogram3D, Sinogram3DSiemensMmr),
 //              input file, initial estimate, output filename prefix, number of
 //              iterations, forwardprojector and backprojector (CuSiddonProjector),
@@ -24,6 +28,7 @@
 //              the reference), multiplicative sinogram, additive sinogram
 //              (+ scanner keys)
 #include <chrono>
+#include <cmath>
 #include <cstdio>
 #include <cstdlib>
 #include <iostream>
@@ -221,6 +226,74 @@ int backproject() {
   return 0;
 }
 
+// Attenuation correction factors in place: exp of every non-zero bin, 1
+// elsewhere (generateACFs.cpp:306-320, :500-520), with the host's float exp
+// as the reference computes them.
+void to_acf(float* bins, size_t n) {
+  for (size_t i = 0; i < n; i++) bins[i] = bins[i] != 0.f ? std::exp(bins[i]) : 1.f;
+}
+
+bool block_size(const char* k, dim3* out);
+
+// cmd/src/generateACFs.cpp:180-560.
+int generate_acfs() {
+  std::string input, type, out, tmpl, proj;
+  key("input file", &input);
+  key("output type", &type);
+  key("output filename", &out);
+  key("output projection", &tmpl);
+  key("projector", &proj);
+  Image mu;
+  if (!mu.readFromInterfile(input.c_str())) {
+    std::cerr << "Error reading the attenuation map: " << mu.getError() << std::endl;
+    return -1;
+  }
+  // "CuSiddonProjector" reads its block size and GPU (generateACFs.cpp:254-271);
+  // every name runs the Siddon projector on the GPU here.
+  dim3 b;
+  if (proj == "CuSiddonProjector" && !block_size("projector block size", &b)) return -1;
+  CuSiddonProjector p(1, 1, ikey("gpu id", 0));
+  // 1/cm to 1/mm (generateACFs.cpp:275-285).
+  float* px = mu.getPixelsPtr();
+  for (int i = 0; i < mu.getPixelCount(); i++) px[i] = px[i] / 10;
+  Scanner sc = scanner(&mu);
+  auto t0 = std::chrono::steady_clock::now();
+  if (type == "Sinogram2D") {
+    Sinogram2DinCylindrical3Dpet s(tmpl.c_str(), sc.rFov, sc.rScanner);
+    if (s.getNumR() <= 1) { std::cerr << "Error reading " << tmpl << ": " << s.getError() << std::endl; return -1; }
+    s.FillConstant(0);
+    if (!p.Project(&mu, &s)) { std::cerr << p.getError() << std::endl; return 1; }
+    to_acf(s.getSinogramPtr(), (size_t)s.getNumProj() * s.getNumR());
+    s.writeInterfile(out.c_str());
+  } else if (type == "Sinogram3D" || type == "Sinogram3DSiemensMmr") {
+    std::unique_ptr<Sinogram3D> s(type == "Sinogram3D"
+                                      ? (Sinogram3D*)new Sinogram3DCylindricalPet(tmpl.c_str(), sc.rFov, sc.zFov,
+                                                                                  sc.rScanner)
+                                      : (Sinogram3D*)new Sinogram3DSiemensMmr(tmpl.c_str()));
+    if (s->getNumSinograms() <= 0 || s->getBinCount() <= 1) {
+      std::cerr << "Error reading " << tmpl << ": " << s->getError() << std::endl;
+      return -1;
+    }
+    std::unique_ptr<Sinogram3D> in(s->Copy());  // the template's own bins
+    if (!p.Project(&mu, s.get())) { std::cerr << p.getError() << std::endl; return 1; }
+    to_acf(s->getSinogramPtr(), (size_t)s->getBinCount());
+    s->writeInterfile(out.c_str());
+    // The template corrected with the factors, "<output>_attCorrected"
+    // (generateACFs.cpp:522-545).
+    float* a = in->getSinogramPtr();
+    const float* f = s->getSinogramPtr();
+    for (int i = 0; i < in->getBinCount(); i++) a[i] = a[i] * f[i];
+    in->writeInterfile((out + "_attCorrected").c_str());
+  } else {
+    std::cerr << "output type " << type << " is not supported (Sinogram2D, Sinogram3D, Sinogram3DSiemensMmr)"
+              << std::endl;
+    return -1;
+  }
+  double sec = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+  std::cout << "generateACFs: " << sec << " s" << std::endl;
+  return 0;
+}
+
 // ProcessBlockSizeString (reconGPU/src/readCudaParameters.cpp:22-48): the
 // three numbers between the last '{' and the last '}', separated by spaces or
 // commas.
@@ -329,6 +402,7 @@ int main(int argc, char** argv) {
   }
   std::string cmd = kCmd;
   g_section = cmd == "project" ? "Projection" : (cmd == "backproject" ? "Backproject" : cmd == "cuMLEM" ? "MLEM" : cmd);
+  if (cmd == "generateACFs") return generate_acfs();
   if (cmd == "MLEM") return recon(false);
   if (cmd == "OSEM") return recon(true);
   if (cmd == "project") return project();

@@ -268,3 +268,39 @@ def test_cumlem_command_mmr_subsets(tmp_path):
     want, _, _ = ap.osem_3d(ig, sg, meas, np.ones(ig.n_voxels, np.float32), 2, 4)
     assert np.all(np.isfinite(want))
     assert np.linalg.norm(got - want) / np.linalg.norm(want) <= 1e-5
+
+
+def _expf(v):
+    import ctypes
+    libm = ctypes.CDLL("libm.so.6")
+    libm.expf.restype = ctypes.c_float
+    libm.expf.argtypes = [ctypes.c_float]
+    return np.array([libm.expf(float(a)) for a in np.asarray(v, np.float32)], np.float32)
+
+
+def test_generate_acfs_command(case):
+    """generateACFs (cmd/src/generateACFs.cpp): the map in 1/cm is divided by
+    10, projected, and every non-zero bin becomes expf(bin), the others 1; the
+    template sinogram times the factors goes to <output>_attCorrected."""
+    d, ig, sg, x, meas, P, est = case
+    rng = np.random.default_rng(11)
+    mu_cm = (rng.random(ig.n_voxels, dtype=np.float32) * 0.096).astype(np.float32)
+    mu_cm[: ig.nx * ig.ny] = 0  # a slice of zeros: bins that miss the map keep 1
+    write_image(str(d / "mu"), ig, mu_cm)
+    keys = {"input file": "mu.h33", "output type": "Sinogram3D", "output filename": "acf",
+            "output projection": "meas.h33", "projector": "CuSiddonProjector",
+            "projector block size": "{128,1,1}", "gpu id": 0,
+            "cylindrical pet radius (in mm)": sg.r_scanner, "radius fov (in mm)": sg.r_fov,
+            "axial fov (in mm)": sg.axial_fov}
+    with open(d / "acf.par", "w") as f:
+        f.write("generateACFs Parameters :=\n" + "".join(f"{k} := {v}\n" for k, v in keys.items()) + "END :=\n")
+    run("generateACFs", str(d / "acf.par"), d)
+    got = read_data(str(d / "acf"), sg.n_bins)
+    proj = torch.zeros(sg.n_bins, dtype=torch.float32, device=DEV)
+    P.project(torch.from_numpy(mu_cm / np.float32(10)).to(DEV), proj)
+    proj = proj.cpu().numpy()
+    want = np.where(proj != 0, _expf(proj), np.float32(1)).astype(np.float32)
+    assert np.array_equal(got.view(np.uint32), want.view(np.uint32))
+    assert (got == 1).any() and (got > 1).any()
+    corrected = read_data(str(d / "acf_attCorrected"), sg.n_bins)
+    assert np.array_equal(corrected.view(np.uint32), (meas * want).astype(np.float32).view(np.uint32))
