@@ -26,12 +26,18 @@ namespace {
 
 constexpr int kBlock = 256;
 constexpr int kSumLevel2 = 296;  // first-level blocks of the two-level partial sum (2 per SM)
-// Minimum resident 256-thread blocks per SM for the fused kernel (register
-// cap): 6 gives 40 registers (16 B of spill in the persistent kernel, 48
-// warps per SM), measured 0.9 % faster than 5 (48 registers, 40 warps).
-#ifndef APIRL_EM_MIN_BLOCKS
-#define APIRL_EM_MIN_BLOCKS 6
+// Minimum resident 256-thread blocks per SM (register caps).  The
+// persistent fused kernel: 6 gives 40 registers (16 B of spill, 48 warps per
+// SM), measured 0.9 % faster than 5 (48 registers, 40 warps).  The other
+// fused kernels (2D, unpadded 3D, FP64 walk geometry): 5, i.e. 48 registers;
+// at 40 the FP64 form spills 184 B and runs at less than half the speed.
+#ifndef APIRL_PERSIST_MIN_BLOCKS
+#define APIRL_PERSIST_MIN_BLOCKS 6
 #endif
+#ifndef APIRL_EM_MIN_BLOCKS
+#define APIRL_EM_MIN_BLOCKS 5
+#endif
+constexpr int kPersistMinBlocks = APIRL_PERSIST_MIN_BLOCKS;
 constexpr int kEmMinBlocks = APIRL_EM_MIN_BLOCKS;
 // 1: the fused 3D pass sets the walk up a second time for the backprojection
 // (fewer live registers during the forward walk).
@@ -429,7 +435,7 @@ __global__ void __launch_bounds__(kBlock) k_em_pass_rays(ImgGeom g, LorTable t, 
 // are those of one warp in k_em_pass, and the chunk's likelihood partial goes
 // to partials[chunk]: results are identical to k_em_pass's.
 template <typename CT>
-__global__ void __launch_bounds__(kBlock, kEmMinBlocks) k_em_pass_persist(
+__global__ void __launch_bounds__(kBlock, kPersistMinBlocks) k_em_pass_persist(
     ImgGeom g, LorTable t, SubsetSel s, const CT* __restrict__ counts, int counts_packed,
     const float* __restrict__ add, PadBuffers pad, int back, double* __restrict__ partials, int64_t total,
     int skip_zero, unsigned long long* __restrict__ chunk_counter) {
