@@ -77,10 +77,21 @@ class ClockSampler:
         try:
             self.f = open(self.path, "w")
             self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={self.Q}",
-                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                          "--format=csv,noheader,nounits", "-lms", "50"],
                                          stdout=self.f, stderr=subprocess.DEVNULL)
         except Exception:
             self.proc = None
+            return
+        # nvidia-smi takes a moment to start: wait for its first sample, so
+        # that sampling runs through the whole timed region that follows.
+        deadline = time.time() + 5.0
+        while time.time() < deadline and self.proc.poll() is None:
+            try:
+                if os.path.getsize(self.path) > 0:
+                    break
+            except OSError:
+                pass
+            time.sleep(0.01)
 
     def stop(self):
         if self.proc is None:
@@ -769,7 +780,8 @@ def run_batched(args, served=False):
 def main():
     ap_ = argparse.ArgumentParser(description=__doc__.split("\n")[0])
     ap_.add_argument("--gpus", type=int, default=1)
-    ap_.add_argument("--steps", type=int, default=42)
+    ap_.add_argument("--steps", type=int, default=63,
+                     help="timed sub-iterations (63: the job's 3 iterations x 21 subsets)")
     ap_.add_argument("--warmup", type=int, default=5)
     ap_.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap_.add_argument("--no-cpu-baseline", action="store_true")
