@@ -99,9 +99,36 @@ apirl_status zero_images(Res& r, apirl_projector* p, const float* d_meas, const 
   return APIRL_OK;
 }
 
+// The calling thread's iteration hook (apirl_set_iteration_hook).
+struct IterationHook {
+  apirl_iteration_cb cb = nullptr;
+  int interval = 0;
+  void* user = nullptr;
+};
+thread_local IterationHook g_hook;
+
+// After iteration t: when the hook asks for it, the image comes to the host
+// (the stream's work so far finished) and goes to the callback.
+apirl_status iteration_done(Res& r, int t, const float* d_x, int64_t nv, std::vector<float>& h_tmp) {
+  if (!g_hook.cb || g_hook.interval <= 0 || t % g_hook.interval != 0) return APIRL_OK;
+  h_tmp.resize((size_t)nv);
+  DK(cudaMemcpyAsync(h_tmp.data(), d_x, nv * sizeof(float), cudaMemcpyDeviceToHost, r.st));
+  DK(cudaStreamSynchronize(r.st));
+  g_hook.cb(t, h_tmp.data(), nv, g_hook.user);
+  return APIRL_OK;
+}
+
 }  // namespace
 
 extern "C" {
+
+apirl_status apirl_set_iteration_hook(apirl_iteration_cb cb, int interval, void* user) {
+  if (interval < 0) return set_err(APIRL_ERR_INVALID, "iteration hook interval must be >= 0", cudaSuccess);
+  g_hook.cb = cb;
+  g_hook.interval = interval;
+  g_hook.user = user;
+  return APIRL_OK;
+}
 
 apirl_status apirl_osem_3d(const apirl_image_geom* img, const apirl_sino3d_geom* sino, const float* h_meas,
                            const float* h_mult, const float* h_add, const float* h_init, int iters, int nsubsets,
@@ -156,12 +183,15 @@ apirl_status apirl_osem_3d(const apirl_image_geom* img, const apirl_sino3d_geom*
   for (int s = 0; s < nsubsets; s++)
     DS(capture_pass(r, p, d_meas, d_add, d_x, d_bp, d_sens + nv * s, nullptr, 0.f, 1, s, nsubsets, d_slot + s,
                     d_zimg ? d_zimg + nv * s : nullptr, d_zadd ? d_zadd + s : nullptr));
-  for (int t = 0; t < iters; t++)
+  std::vector<float> h_tmp;
+  for (int t = 0; t < iters; t++) {
     for (int s = 0; s < nsubsets; s++) {
       DK(cudaGraphLaunch(r.execs[s], r.st));
       DK(cudaMemcpyAsync(d_lik + (size_t)t * nsubsets + s, d_slot + s, sizeof(double), cudaMemcpyDeviceToDevice,
                          r.st));
     }
+    DS(iteration_done(r, t, d_x, nv, h_tmp));
+  }
   // Final likelihood on the whole-sinogram projection of the result (:291-293).
   SubsetSel all;
   all.subset = -1; all.nsub = 1; all.nk = sino->n_proj;
@@ -220,9 +250,11 @@ apirl_status apirl_mlem_3d(const apirl_image_geom* img, const apirl_sino3d_geom*
     DS(zero_images(r, p, d_meas, d_add, 1, sino->n_proj, d_zimg, d_zadd));
   }
   DS(capture_pass(r, p, d_meas, d_add, d_x, d_bp, d_sens, d_thr, 0.f, 1, -1, 1, d_slot, d_zimg, d_zadd));
+  std::vector<float> h_tmp;
   for (int t = 0; t < iters; t++) {
     DK(cudaGraphLaunch(r.execs[0], r.st));
     DK(cudaMemcpyAsync(d_lik + t, d_slot, sizeof(double), cudaMemcpyDeviceToDevice, r.st));
+    DS(iteration_done(r, t, d_x, nv, h_tmp));
   }
   DK(apirl::launch_em_pass(p->g, p->t, all, d_meas, APIRL_F32, 0, d_add, d_x, d_bp, 0, 0, p->d_partials,
                            d_lik + iters, r.st));
@@ -270,10 +302,12 @@ apirl_status apirl_mlem_2d(const apirl_image_geom* img, const apirl_sino2d_geom*
   DS(apirl_mlem_threshold(nv, d_sens, d_thr, r.st));
   double* d_slot = d_lik + iters + 1;
   DS(capture_pass(r, p, d_meas, d_add, d_x, d_bp, d_sens, d_thr, 0.f, 0, -1, 1, d_slot));
+  std::vector<float> h_tmp;
   for (int t = 0; t < iters; t++) {
     if (t == iters - 1) DK(cudaMemcpyAsync(d_xprev, d_x, nv * sizeof(float), cudaMemcpyDeviceToDevice, r.st));
     DK(cudaGraphLaunch(r.execs[0], r.st));
     DK(cudaMemcpyAsync(d_lik + t, d_slot, sizeof(double), cudaMemcpyDeviceToDevice, r.st));
+    DS(iteration_done(r, t, d_x, nv, h_tmp));
   }
   // Mlem2d.cpp:228 evaluates the last value on the ratio sinogram of the last
   // iteration: recompute that ratio from the image before the last update.

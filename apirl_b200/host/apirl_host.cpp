@@ -79,6 +79,30 @@ double now_ms() {
   return std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now().time_since_epoch()).count();
 }
 
+// "<prefix>_iter_<t>" images at the save interval (OsemSinogram3d.cpp:266-276,
+// MlemSinogram3d.cpp:244-251, Mlem2d.cpp:187-198), written from the drivers'
+// iteration hook while a reconstruction runs.
+struct IterationSaver {
+  SizeImage size;
+  std::string prefix;
+  bool ok = true;
+  static void save(int t, const float* h_image, int64_t n, void* user) {
+    auto* self = static_cast<IterationSaver*>(user);
+    Image img(self->size);
+    if ((int64_t)img.getPixelCount() != n) { self->ok = false; return; }
+    std::memcpy(img.getPixelsPtr(), h_image, (size_t)n * sizeof(float));
+    self->ok = img.writeInterfile((self->prefix + "_iter_" + std::to_string(t)).c_str()) && self->ok;
+  }
+};
+
+// Installs the saver for the lifetime of one driver call (interval 0: none).
+struct HookScope {
+  HookScope(IterationSaver* saver, int interval) {
+    apirl_set_iteration_hook(interval > 0 ? &IterationSaver::save : nullptr, interval > 0 ? interval : 0, saver);
+  }
+  ~HookScope() { apirl_set_iteration_hook(nullptr, 0, nullptr); }
+};
+
 }  // namespace
 
 // ---- key readers -------------------------------------------------------------
@@ -872,12 +896,15 @@ bool Mlem2d::Reconstruct() {
   apirl_image_geom ig = initialEstimate->geom();
   apirl_sino2d_geom sg = inputProjection->geom();
   likelihood.assign(numIterations + 1, 0.0);
+  IterationSaver saver{initialEstimate->getSize(), outputFilenamePrefix};
+  HookScope hook(&saver, saveIterationInterval);
   apirl_status rc = apirl_mlem_2d(&ig, &sg, inputProjection->getSinogramPtr(),
                                   multiplicative ? multiplicative->getSinogramPtr() : nullptr,
                                   additive ? additive->getSinogramPtr() : nullptr, initialEstimate->getPixelsPtr(),
                                   numIterations, dev, reconstructionImage->getPixelsPtr(), likelihood.data(),
                                   sensitivityImage->getPixelsPtr());
   if (rc != APIRL_OK) { strError = apirl_last_error(); return false; }
+  if (!saver.ok) { strError = "writing an intermediate image failed"; return false; }
   double t1 = now_ms();
   sensitivityImage->writeInterfile((outputFilenamePrefix + "_sensitivity").c_str());
   reconstructionImage->writeInterfile((outputFilenamePrefix + "_final").c_str());
@@ -941,6 +968,8 @@ bool MlemSinogram3d::reconstructOnDevice(int numSubsets) {
   if (!sameSampling(&sm)) return false;
   const float* mult = multiplicative ? multiplicative->getSinogramPtr() : nullptr;
   const float* add = additive ? additive->getSinogramPtr() : nullptr;
+  IterationSaver saver{initialEstimate->getSize(), outputFilenamePrefix};
+  HookScope hook(&saver, saveIterationInterval);
   apirl_status rc;
   if (numSubsets == 0) {
     likelihood.assign(numIterations + 1, 0.0);
@@ -954,6 +983,7 @@ bool MlemSinogram3d::reconstructOnDevice(int numSubsets) {
                        sensitivityImage->getPixelsPtr(), &sm);
   }
   if (rc != APIRL_OK) { strError = apirl_last_error(); return false; }
+  if (!saver.ok) { strError = "writing an intermediate image failed"; return false; }
   double t1 = now_ms();
   sensitivityImage->writeInterfile(
       (outputFilenamePrefix + (numSubsets == 0 ? "_sensitivity" : "_sensitivity_subset_0")).c_str());

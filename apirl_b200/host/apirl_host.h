@@ -331,7 +331,11 @@ class CuProjectorInterface : public Projector {
   size_t nImage = 0, nBins = 0, nEstimated = 0, nSinos = 0;
 };
 
-// recon/inc/Mlem.h:82-297.
+// recon/inc/Mlem.h:82-297.  saveIterationInterval > 0 writes
+// "<prefix>_iter_<t>" after every iteration t with t % interval == 0, as the
+// reference does; saveIntermediate (the reference's estimated projections and
+// backprojected images at those iterations) is kept but not acted on: the
+// fused pass never forms them.
 class Mlem {
  public:
   Mlem(Image* initialEstimate, std::string pathSalida, std::string outputPrefix, int numIterations,

@@ -222,6 +222,30 @@ class SiddonProjector:
         return h_x_out
 
 
+# ---- iteration hook of the whole-reconstruction drivers -------------------
+_ITER_CB = ctypes.CFUNCTYPE(None, ctypes.c_int, ctypes.POINTER(ctypes.c_float), ctypes.c_int64, ctypes.c_void_p)
+_iter_hook = None  # the installed ctypes callback, kept alive while installed
+
+
+def set_iteration_hook(callback=None, interval=0):
+    """apirl_set_iteration_hook: osem_3d / mlem_3d / mlem_2d called afterwards
+    on this thread call callback(t, image) (numpy copy) after every iteration t
+    with t % interval == 0.  No arguments: remove it."""
+    global _iter_hook
+    lib = _lib.load()
+    if callback is None or interval <= 0:
+        check(lib.apirl_set_iteration_hook(None, 0, None))
+        _iter_hook = None
+        return
+
+    def trampoline(t, img, n, user):
+        callback(t, np.ctypeslib.as_array(img, shape=(n,)).copy())
+
+    cb = _ITER_CB(trampoline)
+    check(lib.apirl_set_iteration_hook(ctypes.cast(cb, ctypes.c_void_p), int(interval), None))
+    _iter_hook = cb
+
+
 # ---- bin-wise / pixel-wise steps (device tensors) -------------------------
 def inverse_divide(meas, est, stream=None):
     lib = _lib.load()

@@ -341,6 +341,14 @@ apirl_status apirl_stage_counts(apirl_projector* p, const void* h_counts_subset,
  * whole-sinogram projection of the result).  h_mult / h_add may be NULL.
  * sampling: the projector's rays per bin (apirl_projector_set_sampling), or
  * NULL for one ray per bin. */
+/* "save estimates at iteration intervals" (OsemSinogram3d.cpp:266-276,
+ * MlemSinogram3d.cpp:244-251, Mlem2d.cpp:187-198): the drivers below, when
+ * called afterwards on the same thread, hand the image after every iteration
+ * t (0-based) with t % interval == 0 to cb (h_image valid during the call).
+ * cb NULL or interval 0: no calls (the default). */
+typedef void (*apirl_iteration_cb)(int iteration, const float* h_image, int64_t n_voxels, void* user);
+apirl_status apirl_set_iteration_hook(apirl_iteration_cb cb, int interval, void* user);
+
 typedef struct {
   int n_samples;             /* numSamplesOnDetector */
   int n_axial_samples;       /* numAxialSamplesOnDetector */

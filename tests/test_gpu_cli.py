@@ -304,3 +304,45 @@ def test_generate_acfs_command(case):
     assert (got == 1).any() and (got > 1).any()
     corrected = read_data(str(d / "acf_attCorrected"), sg.n_bins)
     assert np.array_equal(corrected.view(np.uint32), (meas * want).astype(np.float32).view(np.uint32))
+
+
+def test_osem_command_saves_iterations(case):
+    """save estimates at iteration intervals (OsemSinogram3d.cpp:266-276):
+    <prefix>_iter_<t> after iterations t = 0, 2, ...; the last saved image
+    equals the final one."""
+    d, ig, sg, x, meas, P, est = case
+    keys = {"input type": "Sinogram3D", "input file": "meas.h33", "initial estimate": "ones.h33",
+            "output filename prefix": "rsave", "number of iterations": 3, "number of subsets": 3,
+            "forwardprojector": "Siddon", "backprojector": "Siddon", "save estimates at iteration intervals": 2}
+    keys.update({"cylindrical pet radius (in mm)": sg.r_scanner, "radius fov (in mm)": sg.r_fov,
+                 "axial fov (in mm)": sg.axial_fov})
+    with open(d / "osem_save.par", "w") as f:
+        f.write("OSEM Parameters :=\n" + "".join(f"{k} := {v}\n" for k, v in keys.items()) + "END :=\n")
+    run("OSEM", str(d / "osem_save.par"), d)
+    assert os.path.exists(d / "rsave_iter_0.h33") and os.path.exists(d / "rsave_iter_2.h33")
+    assert not os.path.exists(d / "rsave_iter_1.h33")
+    final = read_data(str(d / "rsave_final"), ig.n_voxels)
+    assert np.array_equal(read_data(str(d / "rsave_iter_2"), ig.n_voxels).view(np.uint32), final.view(np.uint32))
+    want1, _, _ = ap.osem_3d(ig, sg, meas, np.ones(ig.n_voxels, np.float32), 1, 3)
+    got1 = read_data(str(d / "rsave_iter_0"), ig.n_voxels)
+    assert np.linalg.norm(got1 - want1) / np.linalg.norm(want1) <= 1e-5
+
+
+def test_iteration_hook_c_abi(case):
+    """apirl_set_iteration_hook (apirl_b200.set_iteration_hook): the driver
+    hands the image after every interval-th iteration to the callback;
+    removed, it calls nothing."""
+    d, ig, sg, x, meas, P, est = case
+    seen = []
+    ap.set_iteration_hook(lambda t, img: seen.append((t, img)), 1)
+    try:
+        img, _, _ = ap.mlem_3d(ig, sg, meas, np.ones(ig.n_voxels, np.float32), 2)
+    finally:
+        ap.set_iteration_hook()
+    assert [t for t, _ in seen] == [0, 1]
+    assert np.array_equal(seen[1][1].view(np.uint32), img.view(np.uint32))
+    seen.clear()
+    ap.mlem_3d(ig, sg, meas, np.ones(ig.n_voxels, np.float32), 1)
+    assert seen == []
+    from apirl_b200 import _lib
+    assert _lib.load().apirl_set_iteration_hook(None, -1, None) != 0
