@@ -58,6 +58,11 @@ class SamplingC(ctypes.Structure):
     _fields_ = [("n_samples", _i), ("n_axial_samples", _i), ("multiple_lors_per_bin", _i)]
 
 
+class ReconOptionsC(ctypes.Structure):
+    """apirl_recon_options: rays per bin, given / returned sensitivity images."""
+    _fields_ = [("sampling", ctypes.POINTER(SamplingC)), ("h_sens_in", _vp), ("h_sens_out", _vp)]
+
+
 class JobDescC(ctypes.Structure):
     _fields_ = [("img", ImageGeomC), ("sino", Sino3DGeomC), ("h_counts", _vp), ("counts_dtype", _i),
                 ("h_mult", _vp), ("h_add", _vp), ("h_init", _vp), ("iters", _i), ("nsubsets", _i)]
@@ -108,6 +113,12 @@ SIGNATURES = {
                            _i, _vp, _vp, _vp, ctypes.POINTER(SamplingC)]),
     "apirl_mlem_3d": (_i, [ctypes.POINTER(ImageGeomC), ctypes.POINTER(Sino3DGeomC), _vp, _vp, _vp, _vp, _i, _i,
                            _vp, _vp, _vp, ctypes.POINTER(SamplingC)]),
+    "apirl_osem_3d_ex": (_i, [ctypes.POINTER(ImageGeomC), ctypes.POINTER(Sino3DGeomC), _vp, _vp, _vp, _vp, _i, _i,
+                              _i, _vp, _vp, ctypes.POINTER(ReconOptionsC)]),
+    "apirl_mlem_3d_ex": (_i, [ctypes.POINTER(ImageGeomC), ctypes.POINTER(Sino3DGeomC), _vp, _vp, _vp, _vp, _i, _i,
+                              _vp, _vp, ctypes.POINTER(ReconOptionsC)]),
+    "apirl_mlem_2d_ex": (_i, [ctypes.POINTER(ImageGeomC), ctypes.POINTER(Sino2DGeomC), _vp, _vp, _vp, _vp, _i, _i,
+                              _vp, _vp, ctypes.POINTER(ReconOptionsC)]),
     "apirl_projector_set_sampling": (_i, [_vp, _i, _i, _i]),
     "apirl_projector_set_shard": (_i, [_vp, _i, _i]),
     "apirl_job_footprint": (_i64, [ctypes.POINTER(JobDescC)]),

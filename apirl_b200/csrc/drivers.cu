@@ -130,9 +130,16 @@ apirl_status apirl_set_iteration_hook(apirl_iteration_cb cb, int interval, void*
   return APIRL_OK;
 }
 
-apirl_status apirl_osem_3d(const apirl_image_geom* img, const apirl_sino3d_geom* sino, const float* h_meas,
-                           const float* h_mult, const float* h_add, const float* h_init, int iters, int nsubsets,
-                           int device, float* h_out, double* h_lik, float* h_sens0, const apirl_sampling* sampling) {
+}  // extern "C"
+
+namespace {
+
+// h_sens_in: nsubsets given sensitivity images (or NULL: computed);
+// h_sens_out: receives the first n_sens_out of them.
+apirl_status osem_3d(const apirl_image_geom* img, const apirl_sino3d_geom* sino, const float* h_meas,
+                     const float* h_mult, const float* h_add, const float* h_init, int iters, int nsubsets,
+                     int device, float* h_out, double* h_lik, const float* h_sens_in, float* h_sens_out,
+                     int n_sens_out, const apirl_sampling* sampling) {
   if (!h_meas || !h_init || !h_out || iters < 0 || nsubsets <= 0)
     return set_err(APIRL_ERR_INVALID, "apirl_osem_3d arguments", cudaSuccess);
   Res r;
@@ -165,12 +172,17 @@ apirl_status apirl_osem_3d(const apirl_image_geom* img, const apirl_sino3d_geom*
   DK(cudaMemcpyAsync(d_x, h_init, nv * sizeof(float), cudaMemcpyHostToDevice, r.st));
   DK(cudaMemsetAsync(d_bp, 0, nv * sizeof(float), r.st));
   DK(cudaMemsetAsync(d_sens, 0, nv * nsubsets * sizeof(float), r.st));
-  // Per-subset sensitivity: A_s^T (mult or 1), then forcePositive
-  // (OsemSinogram3d.cpp:101-116, :327-346).
+  // Per-subset sensitivity: A_s^T (mult or 1), or the given images, then
+  // forcePositive (OsemSinogram3d.cpp:84-116, :327-346).
   for (int s = 0; s < nsubsets; s++) {
-    SubsetSel ss;
-    ss.subset = s; ss.nsub = nsubsets; ss.nk = apirl::subset_nproj(sino->n_proj, s, nsubsets);
-    DK(apirl::launch_backproject(p->g, p->t, ss, d_mult, d_mult ? 1 : 2, nullptr, 0, d_sens + nv * s, r.st, p->pg));
+    if (h_sens_in) {
+      DK(cudaMemcpyAsync(d_sens + nv * s, h_sens_in + nv * s, nv * sizeof(float), cudaMemcpyHostToDevice, r.st));
+    } else {
+      SubsetSel ss;
+      ss.subset = s; ss.nsub = nsubsets; ss.nk = apirl::subset_nproj(sino->n_proj, s, nsubsets);
+      DK(apirl::launch_backproject(p->g, p->t, ss, d_mult, d_mult ? 1 : 2, nullptr, 0, d_sens + nv * s, r.st,
+                                   p->pg));
+    }
     DK(apirl::launch_force_positive(nv, d_sens + nv * s, r.st));
   }
   float* d_zimg = nullptr;
@@ -199,14 +211,18 @@ apirl_status apirl_osem_3d(const apirl_image_geom* img, const apirl_sino3d_geom*
                            d_lik + (size_t)iters * nsubsets, r.st));
   DK(cudaMemcpyAsync(h_out, d_x, nv * sizeof(float), cudaMemcpyDeviceToHost, r.st));
   if (h_lik) DK(cudaMemcpyAsync(h_lik, d_lik, ((size_t)iters * nsubsets + 1) * sizeof(double), cudaMemcpyDeviceToHost, r.st));
-  if (h_sens0) DK(cudaMemcpyAsync(h_sens0, d_sens, nv * sizeof(float), cudaMemcpyDeviceToHost, r.st));
+  if (h_sens_out && n_sens_out > 0)
+    DK(cudaMemcpyAsync(h_sens_out, d_sens, nv * (n_sens_out < nsubsets ? n_sens_out : nsubsets) * sizeof(float),
+                       cudaMemcpyDeviceToHost, r.st));
   DK(cudaStreamSynchronize(r.st));
   return APIRL_OK;
 }
 
-apirl_status apirl_mlem_3d(const apirl_image_geom* img, const apirl_sino3d_geom* sino, const float* h_meas,
-                           const float* h_mult, const float* h_add, const float* h_init, int iters, int device,
-                           float* h_out, double* h_lik, float* h_sens, const apirl_sampling* sampling) {
+// h_sens_in: the given sensitivity image (or NULL: computed).
+apirl_status mlem_3d(const apirl_image_geom* img, const apirl_sino3d_geom* sino, const float* h_meas,
+                     const float* h_mult, const float* h_add, const float* h_init, int iters, int device,
+                     float* h_out, double* h_lik, const float* h_sens_in, float* h_sens,
+                     const apirl_sampling* sampling) {
   if (!h_meas || !h_init || !h_out || iters < 0) return set_err(APIRL_ERR_INVALID, "apirl_mlem_3d arguments", cudaSuccess);
   Res r;
   DS(apirl_projector_create_3d(img, sino, device, &r.p));
@@ -239,7 +255,11 @@ apirl_status apirl_mlem_3d(const apirl_image_geom* img, const apirl_sino3d_geom*
   DK(cudaMemsetAsync(d_sens, 0, nv * sizeof(float), r.st));
   SubsetSel all;
   all.subset = -1; all.nsub = 1; all.nk = sino->n_proj;
-  DK(apirl::launch_backproject(p->g, p->t, all, d_mult, d_mult ? 1 : 2, nullptr, 0, d_sens, r.st));
+  // Sensitivity A^T (mult or 1), or the given image (MlemSinogram3d.cpp:132-151).
+  if (h_sens_in)
+    DK(cudaMemcpyAsync(d_sens, h_sens_in, nv * sizeof(float), cudaMemcpyHostToDevice, r.st));
+  else
+    DK(apirl::launch_backproject(p->g, p->t, all, d_mult, d_mult ? 1 : 2, nullptr, 0, d_sens, r.st));
   DS(apirl_mlem_threshold(nv, d_sens, d_thr, r.st));
   double* d_slot = d_lik + iters + 1;
   float* d_zimg = nullptr;
@@ -265,9 +285,9 @@ apirl_status apirl_mlem_3d(const apirl_image_geom* img, const apirl_sino3d_geom*
   return APIRL_OK;
 }
 
-apirl_status apirl_mlem_2d(const apirl_image_geom* img, const apirl_sino2d_geom* sino, const float* h_meas,
-                           const float* h_mult, const float* h_add, const float* h_init, int iters, int device,
-                           float* h_out, double* h_lik, float* h_sens) {
+apirl_status mlem_2d(const apirl_image_geom* img, const apirl_sino2d_geom* sino, const float* h_meas,
+                     const float* h_mult, const float* h_add, const float* h_init, int iters, int device,
+                     float* h_out, double* h_lik, const float* h_sens_in, float* h_sens) {
   if (!h_meas || !h_init || !h_out || iters < 0) return set_err(APIRL_ERR_INVALID, "apirl_mlem_2d arguments", cudaSuccess);
   Res r;
   DS(apirl_projector_create_2d(img, sino, device, &r.p));
@@ -298,7 +318,11 @@ apirl_status apirl_mlem_2d(const apirl_image_geom* img, const apirl_sino2d_geom*
   DK(cudaMemsetAsync(d_sens, 0, nv * sizeof(float), r.st));
   SubsetSel all;
   all.subset = -1; all.nsub = 1; all.nk = sino->n_proj;
-  DK(apirl::launch_backproject(p->g, p->t, all, d_mult, d_mult ? 1 : 2, nullptr, 0, d_sens, r.st));
+  // Sensitivity A^T (mult or 1), or the given image (Mlem2d.cpp:95-112).
+  if (h_sens_in)
+    DK(cudaMemcpyAsync(d_sens, h_sens_in, nv * sizeof(float), cudaMemcpyHostToDevice, r.st));
+  else
+    DK(apirl::launch_backproject(p->g, p->t, all, d_mult, d_mult ? 1 : 2, nullptr, 0, d_sens, r.st));
   DS(apirl_mlem_threshold(nv, d_sens, d_thr, r.st));
   double* d_slot = d_lik + iters + 1;
   DS(capture_pass(r, p, d_meas, d_add, d_x, d_bp, d_sens, d_thr, 0.f, 0, -1, 1, d_slot));
@@ -321,6 +345,53 @@ apirl_status apirl_mlem_2d(const apirl_image_geom* img, const apirl_sino2d_geom*
   if (h_sens) DK(cudaMemcpyAsync(h_sens, d_sens, nv * sizeof(float), cudaMemcpyDeviceToHost, r.st));
   DK(cudaStreamSynchronize(r.st));
   return APIRL_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+apirl_status apirl_osem_3d(const apirl_image_geom* img, const apirl_sino3d_geom* sino, const float* h_meas,
+                           const float* h_mult, const float* h_add, const float* h_init, int iters, int nsubsets,
+                           int device, float* h_out, double* h_lik, float* h_sens0, const apirl_sampling* sampling) {
+  return osem_3d(img, sino, h_meas, h_mult, h_add, h_init, iters, nsubsets, device, h_out, h_lik, nullptr, h_sens0,
+                 1, sampling);
+}
+
+apirl_status apirl_osem_3d_ex(const apirl_image_geom* img, const apirl_sino3d_geom* sino, const float* h_meas,
+                              const float* h_mult, const float* h_add, const float* h_init, int iters, int nsubsets,
+                              int device, float* h_out, double* h_lik, const apirl_recon_options* opts) {
+  const apirl_recon_options o = opts ? *opts : apirl_recon_options{nullptr, nullptr, nullptr};
+  return osem_3d(img, sino, h_meas, h_mult, h_add, h_init, iters, nsubsets, device, h_out, h_lik, o.h_sens_in,
+                 o.h_sens_out, nsubsets, o.sampling);
+}
+
+apirl_status apirl_mlem_3d(const apirl_image_geom* img, const apirl_sino3d_geom* sino, const float* h_meas,
+                           const float* h_mult, const float* h_add, const float* h_init, int iters, int device,
+                           float* h_out, double* h_lik, float* h_sens, const apirl_sampling* sampling) {
+  return mlem_3d(img, sino, h_meas, h_mult, h_add, h_init, iters, device, h_out, h_lik, nullptr, h_sens, sampling);
+}
+
+apirl_status apirl_mlem_3d_ex(const apirl_image_geom* img, const apirl_sino3d_geom* sino, const float* h_meas,
+                              const float* h_mult, const float* h_add, const float* h_init, int iters, int device,
+                              float* h_out, double* h_lik, const apirl_recon_options* opts) {
+  const apirl_recon_options o = opts ? *opts : apirl_recon_options{nullptr, nullptr, nullptr};
+  return mlem_3d(img, sino, h_meas, h_mult, h_add, h_init, iters, device, h_out, h_lik, o.h_sens_in, o.h_sens_out,
+                 o.sampling);
+}
+
+apirl_status apirl_mlem_2d(const apirl_image_geom* img, const apirl_sino2d_geom* sino, const float* h_meas,
+                           const float* h_mult, const float* h_add, const float* h_init, int iters, int device,
+                           float* h_out, double* h_lik, float* h_sens) {
+  return mlem_2d(img, sino, h_meas, h_mult, h_add, h_init, iters, device, h_out, h_lik, nullptr, h_sens);
+}
+
+apirl_status apirl_mlem_2d_ex(const apirl_image_geom* img, const apirl_sino2d_geom* sino, const float* h_meas,
+                              const float* h_mult, const float* h_add, const float* h_init, int iters, int device,
+                              float* h_out, double* h_lik, const apirl_recon_options* opts) {
+  const apirl_recon_options o = opts ? *opts : apirl_recon_options{nullptr, nullptr, nullptr};
+  if (o.sampling) return set_err(APIRL_ERR_NOT_SUPPORTED, "2D reconstructions walk one ray per bin", cudaSuccess);
+  return mlem_2d(img, sino, h_meas, h_mult, h_add, h_init, iters, device, h_out, h_lik, o.h_sens_in, o.h_sens_out);
 }
 
 }  // extern "C"

@@ -106,7 +106,10 @@ int recon(bool osem) {
   std::string fwdName = "Siddon", backName = "Siddon";
   key("forwardprojector", &fwdName, false);
   key("backprojector", &backName, false);
-  // getSaveIntermidiateIntervals (data/src/readParameters.cpp:60-110).
+  // getSensitivityFromFile, getSaveIntermidiateIntervals
+  // (data/src/readParameters.cpp:25-110).
+  std::string sensName;
+  const bool sensFromFile = key("sensitivity filename", &sensName, false);
   const int saveInterval = ikey("save estimates at iteration intervals", 0);
   const bool saveInter = saveInterval > 0 && ikey("save estimated projections and backprojected image", 0) != 0;
   if (saveInter)
@@ -130,7 +133,8 @@ int recon(bool osem) {
     s2.reset(new Sinogram2DinCylindrical3Dpet(input.c_str(), sc.rFov, sc.rScanner));
     if (s2->getNumR() <= 1) { std::cerr << "Error reading " << input << ": " << s2->getError() << std::endl; return 1; }
     if (osem) { std::cerr << "OSEM needs a Sinogram3D input" << std::endl; return 1; }
-    m.reset(new Mlem2d(s2.get(), &x0, "", prefix, iters, saveInterval, saveInter, false, fwd.get(), back.get()));
+    m.reset(new Mlem2d(s2.get(), &x0, "", prefix, iters, saveInterval, saveInter, sensFromFile, fwd.get(),
+                       back.get()));
     // The reference's Mlem2d forces the sinogram rFov to the image's; an
     // explicit "radius fov (in mm)" restores the sinogram's own bin pitch.
     std::string rf;
@@ -146,16 +150,17 @@ int recon(bool osem) {
       return 1;
     }
     if (osem)
-      m.reset(new OsemSinogram3d(s3.get(), &x0, "", prefix, iters, saveInterval, saveInter, false, fwd.get(),
-                                 back.get(), subsets));
+      m.reset(new OsemSinogram3d(s3.get(), &x0, "", prefix, iters, saveInterval, saveInter, sensFromFile,
+                                 fwd.get(), back.get(), subsets));
     else
-      m.reset(new MlemSinogram3d(s3.get(), &x0, "", prefix, iters, saveInterval, saveInter, false, fwd.get(),
-                                 back.get()));
+      m.reset(new MlemSinogram3d(s3.get(), &x0, "", prefix, iters, saveInterval, saveInter, sensFromFile,
+                                 fwd.get(), back.get()));
   } else {
     std::cerr << "input type " << type << " is not supported on this path (Sinogram2D, Sinogram3D, "
               << "Sinogram3DSiemensMmr)" << std::endl;
     return 1;
   }
+  if (sensFromFile) m->setSensitivityFilename(sensName);
   if (hasMult && !m->setMultiplicativeProjection(mult)) { std::cerr << "Error reading " << mult << std::endl; return 1; }
   if (hasAdd && !m->setAdditiveProjection(add)) { std::cerr << "Error reading " << add << std::endl; return 1; }
   auto t0 = std::chrono::steady_clock::now();
@@ -344,6 +349,8 @@ int cumlem() {
   int gpu = ikey("gpu id", 0);
   int subsets = ikey("number of subsets", 0);
   const int saveInterval = ikey("save estimates at iteration intervals", 0);
+  std::string sensName;
+  const bool sensFromFile = key("sensitivity filename", &sensName, false);
   for (const std::string* n : {&fwdName, &backName})
     if (*n != "CuSiddonProjector") {
       std::cerr << "No existe el proyector " << *n << "." << std::endl;
@@ -372,10 +379,11 @@ int cumlem() {
   }
   // The reference runs OSEM for mMR sinograms with a subset count only.
   if (type == "Sinogram3DSiemensMmr" && subsets > 0)
-    m.reset(new CuOsemSinogram3d(s3.get(), &x0, "", prefix, iters, saveInterval, false, false, &fwd, &back,
+    m.reset(new CuOsemSinogram3d(s3.get(), &x0, "", prefix, iters, saveInterval, false, sensFromFile, &fwd, &back,
                                  subsets));
   else
-    m.reset(new CuMlemSinogram3d(s3.get(), &x0, "", prefix, iters, saveInterval, false, false, &fwd, &back));
+    m.reset(new CuMlemSinogram3d(s3.get(), &x0, "", prefix, iters, saveInterval, false, sensFromFile, &fwd, &back));
+  if (sensFromFile) m->setSensitivityFilename(sensName);
   std::string mult, add;
   if (key("multiplicative sinogram", &mult, false) && !m->setMultiplicativeProjection(mult)) {
     std::cerr << "Error reading " << mult << std::endl;

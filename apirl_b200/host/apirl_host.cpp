@@ -896,17 +896,27 @@ bool Mlem2d::Reconstruct() {
   apirl_image_geom ig = initialEstimate->geom();
   apirl_sino2d_geom sg = inputProjection->geom();
   likelihood.assign(numIterations + 1, 0.0);
+  // Mlem2d.cpp:95-112: the sensitivity image read from sensitivityFilename
+  // (sensitivityImageFromFile), or computed and written.
+  Image given;
+  if (sensitivityImageFromFile &&
+      (!given.readFromInterfile(sensitivityFilename.c_str()) ||
+       given.getPixelCount() != initialEstimate->getPixelCount())) {
+    strError = "reading the sensitivity image " + sensitivityFilename + " failed";
+    return false;
+  }
+  apirl_recon_options opts{nullptr, sensitivityImageFromFile ? given.getPixelsPtr() : nullptr,
+                           sensitivityImage->getPixelsPtr()};
   IterationSaver saver{initialEstimate->getSize(), outputFilenamePrefix};
   HookScope hook(&saver, saveIterationInterval);
-  apirl_status rc = apirl_mlem_2d(&ig, &sg, inputProjection->getSinogramPtr(),
-                                  multiplicative ? multiplicative->getSinogramPtr() : nullptr,
-                                  additive ? additive->getSinogramPtr() : nullptr, initialEstimate->getPixelsPtr(),
-                                  numIterations, dev, reconstructionImage->getPixelsPtr(), likelihood.data(),
-                                  sensitivityImage->getPixelsPtr());
+  apirl_status rc = apirl_mlem_2d_ex(&ig, &sg, inputProjection->getSinogramPtr(),
+                                     multiplicative ? multiplicative->getSinogramPtr() : nullptr,
+                                     additive ? additive->getSinogramPtr() : nullptr, initialEstimate->getPixelsPtr(),
+                                     numIterations, dev, reconstructionImage->getPixelsPtr(), likelihood.data(), &opts);
   if (rc != APIRL_OK) { strError = apirl_last_error(); return false; }
   if (!saver.ok) { strError = "writing an intermediate image failed"; return false; }
   double t1 = now_ms();
-  sensitivityImage->writeInterfile((outputFilenamePrefix + "_sensitivity").c_str());
+  if (!sensitivityImageFromFile) sensitivityImage->writeInterfile((outputFilenamePrefix + "_sensitivity").c_str());
   reconstructionImage->writeInterfile((outputFilenamePrefix + "_final").c_str());
   writeLog("ML-EM", "2D Sinogram", t1 - t0, {});
   return true;
@@ -968,25 +978,52 @@ bool MlemSinogram3d::reconstructOnDevice(int numSubsets) {
   if (!sameSampling(&sm)) return false;
   const float* mult = multiplicative ? multiplicative->getSinogramPtr() : nullptr;
   const float* add = additive ? additive->getSinogramPtr() : nullptr;
+  const int64_t nv = initialEstimate->getPixelCount();
+  const int nimg = numSubsets == 0 ? 1 : numSubsets;
+  // The sensitivity images: read (sensitivityImageFromFile; OSEM reads
+  // "<name>_subset_<s>.h33", OsemSinogram3d.cpp:84-96, ML-EM the named file,
+  // MlemSinogram3d.cpp:132-138) or computed by the driver and written.
+  std::vector<float> sens((size_t)nimg * nv);
+  if (sensitivityImageFromFile) {
+    for (int s = 0; s < nimg; s++) {
+      const std::string fn =
+          numSubsets == 0 ? sensitivityFilename : sensitivityFilename + "_subset_" + std::to_string(s) + ".h33";
+      Image im;
+      if (!im.readFromInterfile(fn.c_str()) || im.getPixelCount() != nv) {
+        strError = "reading the sensitivity image " + fn + " failed";
+        return false;
+      }
+      std::memcpy(sens.data() + (size_t)s * nv, im.getPixelsPtr(), (size_t)nv * sizeof(float));
+    }
+  }
+  apirl_recon_options opts{&sm, sensitivityImageFromFile ? sens.data() : nullptr,
+                           sensitivityImageFromFile ? nullptr : sens.data()};
   IterationSaver saver{initialEstimate->getSize(), outputFilenamePrefix};
   HookScope hook(&saver, saveIterationInterval);
   apirl_status rc;
   if (numSubsets == 0) {
     likelihood.assign(numIterations + 1, 0.0);
-    rc = apirl_mlem_3d(&ig, &sg, inputProjection->getSinogramPtr(), mult, add, initialEstimate->getPixelsPtr(),
-                       numIterations, dev, reconstructionImage->getPixelsPtr(), likelihood.data(),
-                       sensitivityImage->getPixelsPtr(), &sm);
+    rc = apirl_mlem_3d_ex(&ig, &sg, inputProjection->getSinogramPtr(), mult, add, initialEstimate->getPixelsPtr(),
+                          numIterations, dev, reconstructionImage->getPixelsPtr(), likelihood.data(), &opts);
   } else {
     likelihood.assign((size_t)numIterations * numSubsets + 1, 0.0);
-    rc = apirl_osem_3d(&ig, &sg, inputProjection->getSinogramPtr(), mult, add, initialEstimate->getPixelsPtr(),
-                       numIterations, numSubsets, dev, reconstructionImage->getPixelsPtr(), likelihood.data(),
-                       sensitivityImage->getPixelsPtr(), &sm);
+    rc = apirl_osem_3d_ex(&ig, &sg, inputProjection->getSinogramPtr(), mult, add, initialEstimate->getPixelsPtr(),
+                          numIterations, numSubsets, dev, reconstructionImage->getPixelsPtr(), likelihood.data(),
+                          &opts);
   }
   if (rc != APIRL_OK) { strError = apirl_last_error(); return false; }
   if (!saver.ok) { strError = "writing an intermediate image failed"; return false; }
   double t1 = now_ms();
-  sensitivityImage->writeInterfile(
-      (outputFilenamePrefix + (numSubsets == 0 ? "_sensitivity" : "_sensitivity_subset_0")).c_str());
+  std::memcpy(sensitivityImage->getPixelsPtr(), sens.data(), (size_t)nv * sizeof(float));
+  if (!sensitivityImageFromFile) {
+    for (int s = 0; s < nimg; s++) {
+      Image im(initialEstimate->getSize());
+      std::memcpy(im.getPixelsPtr(), sens.data() + (size_t)s * nv, (size_t)nv * sizeof(float));
+      im.writeInterfile(
+          (outputFilenamePrefix + (numSubsets == 0 ? "_sensitivity" : "_sensitivity_subset_" + std::to_string(s)))
+              .c_str());
+    }
+  }
   reconstructionImage->writeInterfile((outputFilenamePrefix + "_final").c_str());
   writeLog(numSubsets == 0 ? "ML-EM" : "OSEM", "Sinogram3D", t1 - t0, {});
   return true;

@@ -305,40 +305,71 @@ def _sampling_c(sampling):
     return ctypes.byref(_lib.SamplingC(int(ns), int(nas), int(bool(multi))))
 
 
-def osem_3d(image_geom, sino_geom, meas, init, iters, nsubsets, mult=None, add=None, device=0, sampling=None):
-    """OsemSinogram3d::Reconstruct on the GPU.  Returns (image, likelihood[iters*nsubsets+1], sens of subset 0)."""
+def _recon_opts(sampling, sens_in, sens_out):
+    """apirl_recon_options; the ctypes objects are returned with it so they stay alive."""
+    smp = None
+    if sampling is not None:
+        ns, nas, multi = sampling
+        smp = _lib.SamplingC(int(ns), int(nas), int(bool(multi)))
+    o = _lib.ReconOptionsC(ctypes.pointer(smp) if smp is not None else None,
+                           _np_ptr(sens_in) if sens_in is not None else None,
+                           _np_ptr(sens_out) if sens_out is not None else None)
+    return o, smp
+
+
+def osem_3d(image_geom, sino_geom, meas, init, iters, nsubsets, mult=None, add=None, device=0, sampling=None,
+            sens=None, all_sens=False):
+    """OsemSinogram3d::Reconstruct on the GPU.  Returns (image,
+    likelihood[iters*nsubsets+1], sensitivity): subset 0's image, or all
+    nsubsets images [subset, voxel] with all_sens.  sens: given sensitivity
+    images [subset, voxel] instead of A_s^T (mult or 1) (forcePositive applied)."""
     lib = _lib.load()
     meas, init, mult, add = _f32(meas), _f32(init), _f32(mult), _f32(add)
-    out = np.zeros(image_geom.n_voxels, np.float32)
+    nv = image_geom.n_voxels
+    out = np.zeros(nv, np.float32)
     lik = np.zeros(iters * nsubsets + 1, np.float64)
-    sens0 = np.zeros(image_geom.n_voxels, np.float32)
     ig, sc = _img_c(image_geom), _sino3d_c(sino_geom)
-    check(lib.apirl_osem_3d(ctypes.byref(ig), ctypes.byref(sc), _np_ptr(meas), _np_ptr(mult), _np_ptr(add),
-                            _np_ptr(init), iters, nsubsets, device, _np_ptr(out), _np_ptr(lik), _np_ptr(sens0),
-                            _sampling_c(sampling)))
-    return out, lik, sens0
+    if sens is None and not all_sens:
+        sens0 = np.zeros(nv, np.float32)
+        check(lib.apirl_osem_3d(ctypes.byref(ig), ctypes.byref(sc), _np_ptr(meas), _np_ptr(mult), _np_ptr(add),
+                                _np_ptr(init), iters, nsubsets, device, _np_ptr(out), _np_ptr(lik), _np_ptr(sens0),
+                                _sampling_c(sampling)))
+        return out, lik, sens0
+    sens_in = None if sens is None else np.ascontiguousarray(sens, np.float32).reshape(-1)
+    if sens_in is not None and sens_in.size != nsubsets * nv:
+        raise ValueError("sens must hold nsubsets images")
+    sens_out = np.zeros((nsubsets, nv), np.float32)
+    opts, _keep = _recon_opts(sampling, sens_in, sens_out)
+    check(lib.apirl_osem_3d_ex(ctypes.byref(ig), ctypes.byref(sc), _np_ptr(meas), _np_ptr(mult), _np_ptr(add),
+                               _np_ptr(init), iters, nsubsets, device, _np_ptr(out), _np_ptr(lik), ctypes.byref(opts)))
+    return out, lik, (sens_out if all_sens else sens_out[0].copy())
 
 
-def mlem_3d(image_geom, sino_geom, meas, init, iters, mult=None, add=None, device=0, sampling=None):
+def mlem_3d(image_geom, sino_geom, meas, init, iters, mult=None, add=None, device=0, sampling=None, sens=None):
+    """MlemSinogram3d::Reconstruct on the GPU; sens: a given sensitivity image."""
     lib = _lib.load()
     meas, init, mult, add = _f32(meas), _f32(init), _f32(mult), _f32(add)
     out = np.zeros(image_geom.n_voxels, np.float32)
     lik = np.zeros(iters + 1, np.float64)
-    sens = np.zeros(image_geom.n_voxels, np.float32)
+    sens_out = np.zeros(image_geom.n_voxels, np.float32)
     ig, sc = _img_c(image_geom), _sino3d_c(sino_geom)
-    check(lib.apirl_mlem_3d(ctypes.byref(ig), ctypes.byref(sc), _np_ptr(meas), _np_ptr(mult), _np_ptr(add),
-                            _np_ptr(init), iters, device, _np_ptr(out), _np_ptr(lik), _np_ptr(sens),
-                            _sampling_c(sampling)))
-    return out, lik, sens
+    sens_in = None if sens is None else np.ascontiguousarray(sens, np.float32).reshape(-1)
+    opts, _keep = _recon_opts(sampling, sens_in, sens_out)
+    check(lib.apirl_mlem_3d_ex(ctypes.byref(ig), ctypes.byref(sc), _np_ptr(meas), _np_ptr(mult), _np_ptr(add),
+                               _np_ptr(init), iters, device, _np_ptr(out), _np_ptr(lik), ctypes.byref(opts)))
+    return out, lik, sens_out
 
 
-def mlem_2d(image_geom, sino_geom, meas, init, iters, mult=None, add=None, device=0):
+def mlem_2d(image_geom, sino_geom, meas, init, iters, mult=None, add=None, device=0, sens=None):
+    """Mlem2d::Reconstruct on the GPU; sens: a given sensitivity image."""
     lib = _lib.load()
     meas, init, mult, add = _f32(meas), _f32(init), _f32(mult), _f32(add)
     out = np.zeros(image_geom.n_voxels, np.float32)
     lik = np.zeros(iters + 1, np.float64)
-    sens = np.zeros(image_geom.n_voxels, np.float32)
+    sens_out = np.zeros(image_geom.n_voxels, np.float32)
     ig, sc = _img_c(image_geom), _sino2d_c(sino_geom)
-    check(lib.apirl_mlem_2d(ctypes.byref(ig), ctypes.byref(sc), _np_ptr(meas), _np_ptr(mult), _np_ptr(add),
-                            _np_ptr(init), iters, device, _np_ptr(out), _np_ptr(lik), _np_ptr(sens)))
-    return out, lik, sens
+    sens_in = None if sens is None else np.ascontiguousarray(sens, np.float32).reshape(-1)
+    opts, _keep = _recon_opts(None, sens_in, sens_out)
+    check(lib.apirl_mlem_2d_ex(ctypes.byref(ig), ctypes.byref(sc), _np_ptr(meas), _np_ptr(mult), _np_ptr(add),
+                               _np_ptr(init), iters, device, _np_ptr(out), _np_ptr(lik), ctypes.byref(opts)))
+    return out, lik, sens_out

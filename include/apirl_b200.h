@@ -369,6 +369,29 @@ apirl_status apirl_mlem_2d(const apirl_image_geom* img, const apirl_sino2d_geom*
                            const float* h_mult, const float* h_add, const float* h_init, int iters, int device,
                            float* h_out, double* h_lik, float* h_sens);
 
+/* The same drivers with the sensitivity images given or returned whole
+ * (sensitivityImageFromFile / setSensitivityFilename, Mlem.h:85-119;
+ * OsemSinogram3d.cpp:84-116, MlemSinogram3d.cpp:132-151, Mlem2d.cpp:95-112).
+ * h_sens_in: OSEM, nsubsets images [subset][voxel], forcePositive applied as
+ * the reference does to the images it reads; ML-EM, one image used as is (the
+ * threshold is taken from it).  NULL: computed as A^T (mult or 1).
+ * h_sens_out: receives every sensitivity image (nsubsets for OSEM), may be
+ * NULL.  sampling: as above (NULL: one ray per bin; must be NULL in 2D). */
+typedef struct {
+  const apirl_sampling* sampling;
+  const float* h_sens_in;
+  float* h_sens_out;
+} apirl_recon_options;
+apirl_status apirl_osem_3d_ex(const apirl_image_geom* img, const apirl_sino3d_geom* sino, const float* h_meas,
+                              const float* h_mult, const float* h_add, const float* h_init, int iters, int nsubsets,
+                              int device, float* h_out, double* h_lik, const apirl_recon_options* opts);
+apirl_status apirl_mlem_3d_ex(const apirl_image_geom* img, const apirl_sino3d_geom* sino, const float* h_meas,
+                              const float* h_mult, const float* h_add, const float* h_init, int iters, int device,
+                              float* h_out, double* h_lik, const apirl_recon_options* opts);
+apirl_status apirl_mlem_2d_ex(const apirl_image_geom* img, const apirl_sino2d_geom* sino, const float* h_meas,
+                              const float* h_mult, const float* h_add, const float* h_init, int iters, int device,
+                              float* h_out, double* h_lik, const apirl_recon_options* opts);
+
 /* ---- batched and served reconstructions ---------------------------------
  * Many independent 3D OSEM jobs (OsemSinogram3d::Reconstruct each,
  * recon/src/OsemSinogram3d.cpp:36-325) of different geometries advance

@@ -346,3 +346,29 @@ def test_iteration_hook_c_abi(case):
     assert seen == []
     from apirl_b200 import _lib
     assert _lib.load().apirl_set_iteration_hook(None, -1, None) != 0
+
+
+def test_osem_command_sensitivity_from_file(case):
+    """sensitivity filename (OsemSinogram3d.cpp:84-116): every subset's
+    computed sensitivity is written as <prefix>_sensitivity_subset_<s>, and a
+    run given "<prefix>_sensitivity" reads them back instead of computing."""
+    d, ig, sg, x, meas, P, est = case
+    base = {"input type": "Sinogram3D", "input file": "meas.h33", "initial estimate": "ones.h33",
+            "number of iterations": 2, "number of subsets": 3, "forwardprojector": "Siddon",
+            "backprojector": "Siddon", "cylindrical pet radius (in mm)": sg.r_scanner,
+            "radius fov (in mm)": sg.r_fov, "axial fov (in mm)": sg.axial_fov}
+    for name, extra in (("sa", {}), ("sb", {"sensitivity filename": "sa_sensitivity"})):
+        keys = dict(base, **{"output filename prefix": name}, **extra)
+        with open(d / f"{name}.par", "w") as f:
+            f.write("OSEM Parameters :=\n" + "".join(f"{k} := {v}\n" for k, v in keys.items()) + "END :=\n")
+        run("OSEM", str(d / f"{name}.par"), d)
+    for s in range(3):
+        assert os.path.exists(d / f"sa_sensitivity_subset_{s}.h33")
+        assert not os.path.exists(d / f"sb_sensitivity_subset_{s}.h33")
+    _, _, sens_all = ap.osem_3d(ig, sg, meas, np.ones(ig.n_voxels, np.float32), 0, 3, all_sens=True)
+    for s in range(3):
+        got = read_data(str(d / f"sa_sensitivity_subset_{s}"), ig.n_voxels)
+        assert np.linalg.norm(got - sens_all[s]) / np.linalg.norm(sens_all[s]) <= 1e-6
+    a = read_data(str(d / "sa_final"), ig.n_voxels)
+    b = read_data(str(d / "sb_final"), ig.n_voxels)
+    assert np.linalg.norm(a - b) / np.linalg.norm(a) <= 1e-6

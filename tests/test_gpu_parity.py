@@ -544,3 +544,38 @@ def test_staged_counts_host_pass(oracle):
         assert rel(x, res[0][0]) <= 1e-6
         assert liks[0] == res[0][1][0]  # later passes see images that differ in fp32 atomic order
         assert np.allclose(liks, res[0][1], rtol=1e-7)
+
+
+def test_drivers_with_given_sensitivity(oracle):
+    """apirl_osem_3d_ex / apirl_mlem_3d_ex / apirl_mlem_2d_ex: every subset's
+    sensitivity comes back, and given back in place of the computed ones they
+    give the same reconstruction (the atomics' order aside); a given image
+    that differs changes it."""
+    ig, sg = small_3d()
+    rng = np.random.default_rng(31)
+    x0 = (rng.random(ig.n_voxels, dtype=np.float32) + 0.5).astype(np.float32)
+    meas = rng.poisson(oracle.project_3d(sg, ig, x0) * 2).astype(np.float32)
+    init = np.ones(ig.n_voxels, np.float32)
+    img, lik, sens_all = ap.osem_3d(ig, sg, meas, init, 2, 4, all_sens=True)
+    assert sens_all.shape == (4, ig.n_voxels)
+    _, _, sens0 = ap.osem_3d(ig, sg, meas, init, 0, 4)
+    assert rel(sens_all[0], sens0) <= 1e-6  # fp32 atomics: equal up to the order of additions
+    img2, lik2, back = ap.osem_3d(ig, sg, meas, init, 2, 4, sens=sens_all, all_sens=True)
+    assert np.array_equal(back.view(np.uint32), sens_all.view(np.uint32))
+    assert rel(img2, img) <= 1e-6 and lik2[0] == lik[0]
+    img3, _, _ = ap.osem_3d(ig, sg, meas, init, 2, 4, sens=sens_all * np.float32(2))
+    assert rel(img3, img) > 1e-3
+    m_img, m_lik, m_sens = ap.mlem_3d(ig, sg, meas, init, 2)
+    m_img2, m_lik2, _ = ap.mlem_3d(ig, sg, meas, init, 2, sens=m_sens)
+    assert rel(m_img2, m_img) <= 1e-6 and m_lik2[0] == m_lik[0]
+    ig2 = ImageGeom(32, 32, 1, 2.08, 2.08, 1.0)
+    sg2 = Sino2DGeom(40, 48, 49.92, 300.0)
+    x2 = (rng.random(ig2.n_voxels, dtype=np.float32) + 0.5).astype(np.float32)
+    P2 = ap.SiddonProjector(ig2, sg2)
+    est = torch.zeros(sg2.n_bins, dtype=torch.float32, device=DEV)
+    P2.project(t(x2), est)
+    meas2 = rng.poisson(est.cpu().numpy()).astype(np.float32)
+    a, _, s2 = ap.mlem_2d(ig2, sg2, meas2, np.ones(ig2.n_voxels, np.float32), 3)
+    b, _, _ = ap.mlem_2d(ig2, sg2, meas2, np.ones(ig2.n_voxels, np.float32), 3, sens=s2)
+    assert rel(b, a) <= 1e-6
+
