@@ -21,6 +21,9 @@ APIRL_OPT_DUAL_LAYOUT = 1
 APIRL_OPT_KERNEL_TIMING = 2
 APIRL_OPT_EM_BLOCK = 3
 APIRL_OPT_PERSISTENT = 4
+APIRL_OPT_SPARSE_IMAGE = 5
+APIRL_SPARSE_ZERO_COUNT = 0
+APIRL_SPARSE_GEOMETRY = 1
 
 APIRL_ALPHA_F32 = 0
 APIRL_ALPHA_F64 = 1
@@ -109,6 +112,7 @@ SIGNATURES = {
     "apirl_em_pass_host": (_i, [_vp, _vp, _i, _vp, _vp, _vp, _vp, _vp, _vp, _f, _i, _i, _i, _vp, _vp, _vp]),
     "apirl_em_pass_host_async": (_i, [_vp, _vp, _i, _vp, _vp, _vp, _vp, _vp, _vp, _f, _i, _i, _i, _vp, _vp, _vp]),
     "apirl_set_iteration_hook": (_i, [_vp, _i, _vp]),
+    "apirl_backproject_ones": (_i, [_vp, _vp, _i, _i, _vp]),
     "apirl_osem_3d": (_i, [ctypes.POINTER(ImageGeomC), ctypes.POINTER(Sino3DGeomC), _vp, _vp, _vp, _vp, _i, _i,
                            _i, _vp, _vp, _vp, ctypes.POINTER(SamplingC)]),
     "apirl_mlem_3d": (_i, [ctypes.POINTER(ImageGeomC), ctypes.POINTER(Sino3DGeomC), _vp, _vp, _vp, _vp, _i, _i,

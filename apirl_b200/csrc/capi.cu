@@ -474,6 +474,16 @@ apirl_status apirl_backproject(apirl_projector* p, const float* d_sino, float* d
   return APIRL_OK;
 }
 
+apirl_status apirl_backproject_ones(apirl_projector* p, float* d_image, int subset, int nsubsets, void* stream) {
+  apirl_status st = check_subset(p, subset, nsubsets);
+  if (st) return st;
+  if (!d_image) return fail(APIRL_ERR_INVALID, "null image");
+  DEVICE_SCOPE(p->device);
+  CK(apirl::launch_backproject(p->g, p->t, make_subset(p, subset, nsubsets), nullptr, 2, nullptr, 0, d_image,
+                               (cudaStream_t)stream, p->pg));
+  return APIRL_OK;
+}
+
 apirl_status apirl_divide_and_backproject(apirl_projector* p, const float* d_meas, const float* d_est,
                                           float* d_image, int subset, int nsubsets, void* stream) {
   apirl_status st = check_subset(p, subset, nsubsets);
@@ -572,7 +582,7 @@ apirl_status fused(apirl_projector* p, SubsetSel ss, const void* d_counts, int d
   }
   CK(apirl::launch_em_pass(p->g, p->t, ss, d_counts, dtype, packed, d_add, d_x, d_bp, 1, p->is3d ? 0 : 1,
                            p->d_partials, d_lik, s, p->pg, dual ? p->pad : apirl::PadBuffers(), p->em_block,
-                           d_zimg, d_zero_add, p->persistent ? p->d_chunk : nullptr));
+                           d_zimg, d_zero_add, p->persistent ? p->d_chunk : nullptr, p->sparse_image));
   if (p->timing) {
     CK(cudaEventRecord(p->ev1, s));
     p->timed = 1;
@@ -689,6 +699,11 @@ apirl_status apirl_projector_set_option(apirl_projector* p, int option, int valu
     }
     case APIRL_OPT_KERNEL_TIMING: p->timing = value != 0; p->timed = 0; return APIRL_OK;
     case APIRL_OPT_PERSISTENT: p->persistent = value != 0; return APIRL_OK;
+    case APIRL_OPT_SPARSE_IMAGE:
+      if (value != APIRL_SPARSE_ZERO_COUNT && value != APIRL_SPARSE_GEOMETRY)
+        return fail(APIRL_ERR_INVALID, "unknown sparse image kind %d", value);
+      p->sparse_image = value;
+      return APIRL_OK;
     case APIRL_OPT_EM_BLOCK:
       if (value < 32 || value > 256 || value % 32) return fail(APIRL_ERR_INVALID, "block size must be 32..256, x32");
       p->em_block = value;

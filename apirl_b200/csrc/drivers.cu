@@ -85,6 +85,14 @@ bool use_sparse(const apirl_projector* p, int passes_per_subset) {
   return passes_per_subset >= 4 && p->is3d && !p->t.lor_s && !p->pg.enabled;
 }
 
+// With neither a multiplicative nor an additive term, and sensitivities the
+// driver computed, each sensitivity image is A_s^T 1 = G_s, the geometry
+// image of the sparse pass (APIRL_SPARSE_GEOMETRY): the passes then walk only
+// bins with counts at no set-up cost, for any number of passes.
+bool use_geometry_sparse(const apirl_projector* p, const float* h_mult, const float* h_add, const float* h_sens_in) {
+  return !h_mult && !h_add && !h_sens_in && p->is3d && !p->t.lor_s && !p->pg.enabled;
+}
+
 // Zero-count images and their additive sums of `nsub` subsets of d_meas.
 apirl_status zero_images(Res& r, apirl_projector* p, const float* d_meas, const float* d_add, int nsub, int n_proj,
                          float* d_zimg, double* d_zero_add) {
@@ -187,7 +195,10 @@ apirl_status osem_3d(const apirl_image_geom* img, const apirl_sino3d_geom* sino,
   }
   float* d_zimg = nullptr;
   double* d_zadd = nullptr;
-  if (use_sparse(p, iters)) {
+  if (use_geometry_sparse(p, h_mult, h_add, h_sens_in)) {
+    DS(apirl_projector_set_option(p, APIRL_OPT_SPARSE_IMAGE, APIRL_SPARSE_GEOMETRY));
+    d_zimg = d_sens;
+  } else if (use_sparse(p, iters)) {
     DK(r.alloc(&d_zimg, nv * nsubsets));
     DK(r.alloc(&d_zadd, nsubsets));
     DS(zero_images(r, p, d_meas, d_add, nsubsets, sino->n_proj, d_zimg, d_zadd));
@@ -264,7 +275,10 @@ apirl_status mlem_3d(const apirl_image_geom* img, const apirl_sino3d_geom* sino,
   double* d_slot = d_lik + iters + 1;
   float* d_zimg = nullptr;
   double* d_zadd = nullptr;
-  if (use_sparse(p, iters)) {
+  if (use_geometry_sparse(p, h_mult, h_add, h_sens_in)) {
+    DS(apirl_projector_set_option(p, APIRL_OPT_SPARSE_IMAGE, APIRL_SPARSE_GEOMETRY));
+    d_zimg = d_sens;
+  } else if (use_sparse(p, iters)) {
     DK(r.alloc(&d_zimg, nv));
     DK(r.alloc(&d_zadd, 1));
     DS(zero_images(r, p, d_meas, d_add, 1, sino->n_proj, d_zimg, d_zadd));

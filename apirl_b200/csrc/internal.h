@@ -106,11 +106,14 @@ cudaError_t launch_em_pass(const ImgGeom& g, const LorTable& t, SubsetSel s, con
                            int counts_packed, const float* add, const float* x, float* bp, int back, int lik_mode,
                            double* partials, double* lik, cudaStream_t st, const PreciseGeom& pg = PreciseGeom(),
                            const PadBuffers& pad = PadBuffers(), int block = 0, const float* zimg = nullptr,
-                           const double* zero_add = nullptr, unsigned long long* persist_counter = nullptr);
+                           const double* zero_add = nullptr, unsigned long long* persist_counter = nullptr,
+                           int zimg_all_bins = 0);
 // Fits the shared-memory carveout of the persistent fused kernels to `block`
 // threads per block (called outside graph capture, when a projector is made
 // or its block size changes).
 cudaError_t prepare_em_kernels(int block);
+// zimg_all_bins: zimg is G_s = A_s^T 1 over all bins and zero_add the sum of
+// all bins' additive terms; walked bins then add m log e alone.
 // Sparse pass (zimg set, 3D float walk): bins with zero counts are not walked;
 // the likelihood subtracts x . zimg + *zero_add instead of their estimates.
 // zimg = A_s^T 1[m == 0] and zero_add = sum of those bins' additive terms,
@@ -206,6 +209,7 @@ struct apirl_projector {
   int em_block = 128;            // threads per block of the fused kernel (APIRL_OPT_EM_BLOCK / autotune)
   int persistent = 1;            // APIRL_OPT_PERSISTENT: warps pull 32-bin chunks (padded 3D pass)
   unsigned long long* d_chunk = nullptr;  // chunk counter of the persistent pass
+  int sparse_image = 0;          // APIRL_OPT_SPARSE_IMAGE: 0 = zero-count image Z_s, 1 = geometry image G_s
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
   // Counts staged ahead of apirl_em_pass_host (apirl_stage_counts): copied on
   // copy_stream; each slot's event is recorded after its copy.

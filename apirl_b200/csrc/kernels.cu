@@ -299,6 +299,16 @@ __global__ void __launch_bounds__(kBlock) k_count_steps(ImgGeom g, LorTable t, S
   }
 }
 
+// A walked bin's likelihood term (Sinogram3D::getLikelihoodValue,
+// data/src/Sinogram3D.cpp:584-606: m log e - e over e != 0).  skip_zero:
+// 0 = every bin walked; 1 = zero-count bins not walked, their -e supplied by
+// -x . Z_s (Z_s = A_s^T 1[m == 0]); 2 = zero-count bins not walked and the
+// -e of every bin supplied by -x . G_s - sum(add) (G_s = A_s^T 1, a
+// geometry image), so a walked bin adds m log e alone.
+__device__ __forceinline__ double lik_term(float m, float e, int skip_zero) {
+  return skip_zero == 2 ? (double)m * log((double)e) : (double)m * log((double)e) - (double)e;
+}
+
 // ---------------------------------------------------------------------------
 // Fused EM pass: project, add, likelihood term, ratio, backproject.
 // lik_mode: 0 = term over e != 0 (3D), 1 = over e > 0 (2D), 2 = over the ratio
@@ -324,8 +334,8 @@ __global__ void __launch_bounds__(kBlock, kEmMinBlocks) k_em_pass(ImgGeom g, Lor
     const float4 L = t.lor[(int64_t)p.a * t.n_r + p.l];
     if (skip_zero && m == 0.f) {
       // Sparse pass: a zero-count bin's ratio is 0 and its likelihood term
-      // -e is linear in the image; the caller's zero-count image supplies
-      // the sum of those terms (k_neg_dot), so the bin is not walked.
+      // -e is linear in the image; the caller's zero-count or geometry image
+      // supplies the sum of those terms (k_neg_dot), so the bin is not walked.
     } else if (IS3D && F64A) {
       const ImgGeomD gd = geom_d(pg);
       Walk3D w;
@@ -353,7 +363,7 @@ __global__ void __launch_bounds__(kBlock, kEmMinBlocks) k_em_pass(ImgGeom g, Lor
       if (add) e = A_ADD(e, __ldg(add + ci));
       const float r = (m != 0.f && e != 0.f) ? A_DIV(m, e) : 0.f;
       if (lik_mode == 2) { if (r > 0.f) term = (double)m * log((double)r) - (double)r; }
-      else if (lik_mode == 1 ? (e > 0.f) : (e != 0.f)) term = (double)m * log((double)e) - (double)e;
+      else if (lik_mode == 1 ? (e > 0.f) : (e != 0.f)) term = lik_term(m, e, skip_zero);
 #if APIRL_EM_RESETUP
       // The walk is set up again from the tables for the backprojection
       // instead of keeping the set-up state live through the forward walk.
@@ -373,7 +383,7 @@ __global__ void __launch_bounds__(kBlock, kEmMinBlocks) k_em_pass(ImgGeom g, Lor
       if (add) e = A_ADD(e, __ldg(add + ci));
       const float r = (m != 0.f && e != 0.f) ? A_DIV(m, e) : 0.f;
       if (lik_mode == 2) { if (r > 0.f) term = (double)m * log((double)r) - (double)r; }
-      else if (lik_mode == 1 ? (e > 0.f) : (e != 0.f)) term = (double)m * log((double)e) - (double)e;
+      else if (lik_mode == 1 ? (e > 0.f) : (e != 0.f)) term = lik_term(m, e, skip_zero);
       if (back && r != 0.f)
         siddon3_walk(w, g, [&](bool inb, int idx, float seg) {
           if (inb) atomicAdd(bp + idx, A_MUL(seg, r));
@@ -466,7 +476,7 @@ __global__ void __launch_bounds__(kBlock, kPersistMinBlocks) k_em_pass_persist(
         float e = siddon3_gather_pad(w, g, ux, uy, uz, pad.lim, tr ? pad.pT : pad.pA);
         if (add) e = A_ADD(e, __ldg(add + ci));
         const float r = (m != 0.f && e != 0.f) ? A_DIV(m, e) : 0.f;
-        if (e != 0.f) term = (double)m * log((double)e) - (double)e;
+        if (e != 0.f) term = lik_term(m, e, skip_zero);
         if (back && r != 0.f) {
           const float4 L2 = __ldcg(t.lor + (int64_t)p.a * t.n_r + p.l);
           const float2 z2 = __ldcg(t.z + p.g);
@@ -973,7 +983,8 @@ cudaError_t launch_em_pass(const ImgGeom& g, const LorTable& t, SubsetSel s, con
                            int counts_packed, const float* add, const float* x, float* bp, int back, int lik_mode,
                            double* partials, double* lik, cudaStream_t st, const PreciseGeom& pg,
                            const PadBuffers& pad, int block, const float* zimg, const double* zero_add,
-                           unsigned long long* persist_counter) {
+                           unsigned long long* persist_counter, int zimg_all_bins) {
+  const int skip = zimg ? (zimg_all_bins ? 2 : 1) : 0;
   const int64_t total = (int64_t)t.n_sinos * s.nk * t.n_r;
   if (block < 32 || block > kBlock || block % 32) block = kBlock;
   const unsigned grid = (unsigned)((total + block - 1) / block);
@@ -992,7 +1003,7 @@ cudaError_t launch_em_pass(const ImgGeom& g, const LorTable& t, SubsetSel s, con
     else if (t.is3d)                                                                                          \
       k_em_pass<CT, true, false><<<grid, block, 0, st>>>(g, t, s, pg, (const CT*)counts, counts_packed, add,   \
                                                           x, bp, pad, back, lik_mode, partials, total,        \
-                                                          zimg != nullptr);                                   \
+                                                          skip);                                   \
     else                                                                                                      \
       k_em_pass<CT, false, false><<<grid, block, 0, st>>>(g, t, s, pg, (const CT*)counts, counts_packed, add,  \
                                                            x, bp, PadBuffers(), back, lik_mode, partials,     \
@@ -1029,16 +1040,16 @@ cudaError_t launch_em_pass(const ImgGeom& g, const LorTable& t, SubsetSel s, con
     switch (counts_dtype) {
       case APIRL_F32:
         k_em_pass_persist<float><<<pgrid, block, 0, st>>>(g, t, s, (const float*)counts, counts_packed, add, pad,
-                                                          back, partials, total, zimg != nullptr, persist_counter);
+                                                          back, partials, total, skip, persist_counter);
         break;
       case APIRL_U32:
         k_em_pass_persist<uint32_t><<<pgrid, block, 0, st>>>(g, t, s, (const uint32_t*)counts, counts_packed, add,
-                                                             pad, back, partials, total, zimg != nullptr,
+                                                             pad, back, partials, total, skip,
                                                              persist_counter);
         break;
       case APIRL_U16:
         k_em_pass_persist<uint16_t><<<pgrid, block, 0, st>>>(g, t, s, (const uint16_t*)counts, counts_packed, add,
-                                                             pad, back, partials, total, zimg != nullptr,
+                                                             pad, back, partials, total, skip,
                                                              persist_counter);
         break;
       default: return cudaErrorInvalidValue;

@@ -150,6 +150,12 @@ class SiddonProjector:
         check(self.lib.apirl_project(self.h, _ptr(image), _ptr(sino), subset, nsubsets, _stream(stream)))
         return sino
 
+    def backproject_ones(self, image, subset=-1, nsubsets=1, stream=None):
+        """image += A_s^T 1 (the unweighted sensitivity; G_s of the sparse pass
+        with APIRL_SPARSE_GEOMETRY)."""
+        check(self.lib.apirl_backproject_ones(self.h, _ptr(image), subset, nsubsets, _stream(stream)))
+        return image
+
     def backproject(self, sino, image, subset=-1, nsubsets=1, stream=None):
         """image += A^T sino."""
         check(self.lib.apirl_backproject(self.h, _ptr(sino), _ptr(image), subset, nsubsets, _stream(stream)))

@@ -48,6 +48,8 @@ L2_FLUSH_BYTES = 256 << 20
 # mean of the four timed launches captured with ncu --metrics dram__bytes_read.sum,
 # dram__bytes_write.sum (one pass; profiles/k_em_pass_osem3d_256x256x81.md).
 FULL_TRAFFIC_BYTES = 2.603e8
+# The same for the nonzero pass (the default).
+NONZERO_TRAFFIC_BYTES = None
 WORKLOAD = ("3D OSEM 256x256x81 image, 41 rings span-1 |rd|<=20: 1261 sinograms x 336 angles x 336 r, "
             "21 subsets, attenuation in sensitivity, 5e8 counts uint32")
 
@@ -179,11 +181,12 @@ def step_bytes(w, s, sparse=False):
     """Algorithmic HBM bytes of one sub-iteration: fp32 voxel read per forward
     segment, read-modify-write per backward segment, the uint32 count per bin
     (fused kernel), and 20 B per voxel for the update (x r/w, bp r, sens r, bp
-    clear).  The sparse pass walks forward only the bins with counts, whose
-    segments are the backward ones."""
+    clear).  The sparse and nonzero passes walk forward only the bins with
+    counts, whose segments are the backward ones, and read x and the
+    per-subset image for the likelihood's dot product (8 B per voxel)."""
     nbins = w["sg"].n_sinos * w["sg"].subset_nproj(s, NSUB) * w["sg"].n_r
     fwd = w["bwd"][s] if sparse else w["fwd"][s]
-    kern = 4 * fwd + 8 * w["bwd"][s] + 4 * nbins
+    kern = 4 * fwd + 8 * w["bwd"][s] + 4 * nbins + (8 * w["ig"].n_voxels if sparse else 0)
     return kern, kern + 20 * w["ig"].n_voxels
 
 
@@ -326,7 +329,17 @@ def run_gpu(args):
     P.set_option(_l.APIRL_OPT_PERSISTENT, args.persistent)
 
     sparse = args.pass_form == "sparse"
-    zimg = torch.zeros((NSUB, w["ig"].n_voxels), dtype=torch.float32, device=dev) if sparse else None
+    nonzero = args.pass_form == "nonzero"
+    skipz = sparse or nonzero  # zero-count bins not walked
+    zimg = torch.zeros((NSUB, w["ig"].n_voxels), dtype=torch.float32, device=dev) if skipz else None
+    if nonzero:
+        # G_s = A_s^T 1 per subset: geometry alone (column sums of the subset's
+        # system matrix), made once per scanner geometry at set-up like the
+        # LOR tables and the sensitivity images.
+        P.set_option(_l.APIRL_OPT_SPARSE_IMAGE, _l.APIRL_SPARSE_GEOMETRY)
+        for s_ in range(NSUB):
+            P.backproject_ones(zimg[s_], s_, NSUB, stream=stream)
+        torch.cuda.synchronize(dev)
 
     def zero_images():
         # Per-subset zero-count images of the sparse pass (once per
@@ -340,7 +353,7 @@ def run_gpu(args):
             evs[0].record(stream)
         # one OSEM sub-iteration through the C ABI: layout copy, fused
         # projection / ratio / backprojection kernel, likelihood sum, update
-        if sparse:
+        if skipz:
             P.em_pass_sparse(counts, x, bp, sens[s], zimg[s], s, NSUB, thr_value=0.0, ge=UPDATE_GE, lik=lik,
                              stream=stream)
         else:
@@ -382,12 +395,12 @@ def run_gpu(args):
     pre_ms = pre[0].elapsed_time(pre[1]) if sparse else 0.0
     value, total_ms = whole_job_value(args.steps, sum(step_ms) + pre_ms, world, dist if world > 1 else None, dev)
 
-    kb = [step_bytes(w, s, sparse) for s in subs]
+    kb = [step_bytes(w, s, skipz) for s in subs]
     kern_bytes = statistics.mean(k for k, _ in kb)
     kern_s = statistics.mean(kern_ms) / 1e3
     peak, peak_kind = peaks()
     achieved = kern_bytes / kern_s / 1e9
-    walked = sum((2 * w["bwd"][s]) if sparse else (w["fwd"][s] + w["bwd"][s]) for s in subs)
+    walked = sum((2 * w["bwd"][s]) if skipz else (w["fwd"][s] + w["bwd"][s]) for s in subs)
     if sparse:
         walked += sum(w["fwd"][s] - w["bwd"][s] for s in range(NSUB))  # the zero-count images' segments
     gsteps = walked / (total_ms / 1e3) / 1e9 * world
@@ -423,7 +436,7 @@ def run_gpu(args):
             # the sub-iteration's counts in, its likelihood out; the image
             # stays resident and comes back once, at the end of the job
             P.em_pass_host(host_counts[s], stage, x, bp, sens[s], s, NSUB, None, h_lik, ge=UPDATE_GE, stream=stream,
-                           zimg=zimg[s] if sparse else None)
+                           zimg=zimg[s] if skipz else None)
 
         with _t.cuda.stream(stream):
             if sparse:
@@ -452,7 +465,7 @@ def run_gpu(args):
                     P.stage_counts(host_counts[subs_e[i + 1]], stages[(i + 1) % 2], subs_e[i + 1], NSUB,
                                    stream=stream)
                 P.em_pass_host(host_counts[s], stages[i % 2], x, bp, sens[s], s, NSUB, None, h_liks[i:i + 1],
-                               ge=UPDATE_GE, stream=stream, zimg=zimg[s] if sparse else None, wait=False)
+                               ge=UPDATE_GE, stream=stream, zimg=zimg[s] if skipz else None, wait=False)
             h_x_t.copy_(x, non_blocking=True)  # the reconstructed image, once
             ev[1].record(stream)
             ev[1].synchronize()
@@ -484,6 +497,9 @@ def run_gpu(args):
                        "pass": ("sparse: bins with zero counts not walked, their likelihood terms -x.Z_s from "
                                 "per-subset zero-count images Z_s = A_s^T 1[m=0], all 21 computed inside the "
                                 "timed region and amortized over the timed sub-iterations") if sparse else
+                               ("nonzero: bins with zero counts not walked; likelihood = sum over bins with counts "
+                                "of m log e - x.G_s, G_s = A_s^T 1 per subset (geometry only: made once per "
+                                "scanner geometry at set-up, like the LOR tables)") if nonzero else
                                "full: every bin walked",
                        "l2": "flushed between timed steps (256 MB write outside the timed events)",
                        "update": "x*bp/sens where sens > 0 (the reference's >= 0 gives NaN at the 6 voxels "
@@ -493,7 +509,8 @@ def run_gpu(args):
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak,
                          "traffic": args.traffic_bytes if args.traffic_bytes is not None else
-                         (FULL_TRAFFIC_BYTES if args.max_ring_diff is None else None),
+                         ({"full": FULL_TRAFFIC_BYTES, "nonzero": NONZERO_TRAFFIC_BYTES}.get(args.pass_form)
+                          if args.max_ring_diff is None else None),
                          "kernel": ("k_em_pass_persist" if args.persistent and args.alpha == "f32" else "k_em_pass")
                                    + " (fused projection / ratio / backprojection)",
                          "timing": "CUDA events recorded by the library on the launching stream around the fused "
@@ -504,7 +521,7 @@ def run_gpu(args):
             "cpu_baseline": cpu,
             # per step: layout copy, fused kernel, (zero-count dot,) two-level
             # likelihood sum, reduce/update; plus one zero-count kernel per subset
-            "gpu_launches": (6 * args.steps + NSUB) if sparse else 5 * args.steps,
+            "gpu_launches": (6 * args.steps + NSUB) if sparse else (6 * args.steps if nonzero else 5 * args.steps),
             "clocks": clock,
         }
         print(json.dumps(line), flush=True)
@@ -786,9 +803,10 @@ def main():
     ap_.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap_.add_argument("--no-cpu-baseline", action="store_true")
     ap_.add_argument("--cpu-seconds", type=float, default=15.0)
-    ap_.add_argument("--pass", dest="pass_form", default="full", choices=["sparse", "full"],
-                     help="sparse: bins with zero counts are not walked (their likelihood terms from per-subset "
-                          "zero-count images computed inside the timed region); full: every bin walked")
+    ap_.add_argument("--pass", dest="pass_form", default="nonzero", choices=["sparse", "nonzero", "full"],
+                     help="nonzero: bins with zero counts are not walked, the likelihood from per-subset geometry "
+                          "images A_s^T 1 made at set-up; sparse: the same walk, the likelihood from per-subset "
+                          "zero-count images computed inside the timed region; full: every bin walked")
     ap_.add_argument("--em-block", type=int, default=0,
                      help="threads per block of the fused kernel (0: autotuned on the job's own data)")
     ap_.add_argument("--persistent", type=int, default=1, choices=[0, 1],

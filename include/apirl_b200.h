@@ -185,8 +185,26 @@ apirl_status apirl_projector_set_shard(apirl_projector* p, int first_sinogram, i
  *   (32..256, a multiple of 32).
  * APIRL_OPT_PERSISTENT (default 1): the padded 3D pass runs as a persistent
  *   kernel whose warps pull chunks of 32 bins from a counter (identical
- *   results; the SMs keep their warps busy to the end of the pass). */
-enum { APIRL_OPT_DUAL_LAYOUT = 1, APIRL_OPT_KERNEL_TIMING = 2, APIRL_OPT_EM_BLOCK = 3, APIRL_OPT_PERSISTENT = 4 };
+ *   results; the SMs keep their warps busy to the end of the pass).
+ * APIRL_OPT_SPARSE_IMAGE (default APIRL_SPARSE_ZERO_COUNT): what the image
+ *   and the scalar given to the sparse pass (apirl_em_pass_sparse,
+ *   apirl_em_pass_host with d_zimg) hold.  APIRL_SPARSE_ZERO_COUNT: Z_s =
+ *   A_s^T 1[m == 0] and the sum of the zero-count bins' additive terms
+ *   (apirl_zero_count_image; it depends on the counts).
+ *   APIRL_SPARSE_GEOMETRY: G_s = A_s^T 1 over every bin of the subset (a
+ *   backprojection of ones, apirl_backproject_ones: the geometry alone, the
+ *   sensitivity image itself when there is no multiplicative term) and the
+ *   sum of every bin's additive term; the likelihood is then the sum over
+ *   bins with counts of m log e, minus x . G_s, minus that sum, which is
+ *   sum(m log e - e) over the bins with e != 0 as the reference defines it. */
+enum {
+  APIRL_OPT_DUAL_LAYOUT = 1,
+  APIRL_OPT_KERNEL_TIMING = 2,
+  APIRL_OPT_EM_BLOCK = 3,
+  APIRL_OPT_PERSISTENT = 4,
+  APIRL_OPT_SPARSE_IMAGE = 5
+};
+enum { APIRL_SPARSE_ZERO_COUNT = 0, APIRL_SPARSE_GEOMETRY = 1 };
 apirl_status apirl_projector_set_option(apirl_projector* p, int option, int value);
 apirl_status apirl_projector_kernel_ms(apirl_projector* p, double* ms);
 /* Autotuner: times the fused kernel (apirl_em_project_backproject, `repeats`
@@ -207,6 +225,11 @@ apirl_status apirl_project(apirl_projector* p, const float* d_image, float* d_si
  * for 2D).  Accumulates into d_image, as the reference does. */
 apirl_status apirl_backproject(apirl_projector* p, const float* d_sino, float* d_image, int subset, int nsubsets,
                                void* stream);
+/* d_image += A^T 1 over the subset's bins: the sensitivity image without
+ * multiplicative factors (OsemSinogram3d.cpp:327-346 with no
+ * setMultiplicativeProjection), and the geometry image G_s of the sparse pass
+ * (APIRL_SPARSE_GEOMETRY).  Needs no sinogram buffer. */
+apirl_status apirl_backproject_ones(apirl_projector* p, float* d_image, int subset, int nsubsets, void* stream);
 /* SiddonProjector::DivideAndBackproject: d_image += A^T (d_meas / d_est)
  * (:571-704 for 3D, :90-144 for 2D, with each reference's zero rules). */
 apirl_status apirl_divide_and_backproject(apirl_projector* p, const float* d_meas, const float* d_est,

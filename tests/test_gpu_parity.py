@@ -579,3 +579,46 @@ def test_drivers_with_given_sensitivity(oracle):
     b, _, _ = ap.mlem_2d(ig2, sg2, meas2, np.ones(ig2.n_voxels, np.float32), 3, sens=s2)
     assert rel(b, a) <= 1e-6
 
+
+@pytest.mark.parametrize("dual,persistent", [(1, 1), (1, 0), (0, 0)])
+def test_nonzero_pass_with_geometry_image(oracle, dual, persistent):
+    """APIRL_OPT_SPARSE_IMAGE = APIRL_SPARSE_GEOMETRY: the sparse pass given
+    G_s = A_s^T 1 (apirl_backproject_ones) and the sum of every bin's additive
+    term equals the full pass: the image up to the atomics' order, the
+    likelihood to 1e-6 relative (sum of m log e over bins with counts minus
+    x . G_s minus that sum)."""
+    from apirl_b200 import _lib
+    ig, sg = small_3d()
+    rng = np.random.default_rng(78)
+    x0 = (rng.random(ig.n_voxels, dtype=np.float32) + 0.5).astype(np.float32)
+    meas = rng.poisson(oracle.project_3d(sg, ig, x0) * 0.3).astype(np.float32)
+    meas[rng.random(meas.size) < 0.3] = 0
+    add = (rng.random(meas.size, dtype=np.float32) * 0.1).astype(np.float32)
+    sens = (rng.random(ig.n_voxels, dtype=np.float32) + 1).astype(np.float32)
+    subset, ns = 2, 5
+    P = ap.SiddonProjector(ig, sg)
+    P.set_option(_lib.APIRL_OPT_DUAL_LAYOUT, dual)
+    P.set_option(_lib.APIRL_OPT_PERSISTENT, persistent)
+    gimg = torch.zeros(ig.n_voxels, dtype=torch.float32, device=DEV)
+    P.backproject_ones(gimg, subset, ns)
+    ones = np.ones(sg.subset_bins(subset, ns), np.float32)
+    assert rel(gimg.cpu().numpy(), oracle.backproject_3d(sg, ig, ones, subset, ns)) <= 1e-5
+    add_sub = add.reshape(sg.n_sinos, sg.n_proj, sg.n_r)[:, subset::ns, :].reshape(-1)
+    for use_add in (False, True):
+        a = t(add) if use_add else None
+        add_sum = torch.tensor([float(add_sub.astype(np.float64).sum()) if use_add else 0.0],
+                               dtype=torch.float64, device=DEV)
+        x_full, x_nz = t(x0), t(x0)
+        bp = torch.zeros(ig.n_voxels, dtype=torch.float32, device=DEV)
+        lik_full = torch.zeros(1, dtype=torch.float64, device=DEV)
+        lik_nz = torch.zeros(1, dtype=torch.float64, device=DEV)
+        P.set_option(_lib.APIRL_OPT_SPARSE_IMAGE, _lib.APIRL_SPARSE_ZERO_COUNT)
+        P.em_pass(t(meas), x_full, bp, t(sens), subset, ns, add=a, lik=lik_full)
+        P.set_option(_lib.APIRL_OPT_SPARSE_IMAGE, _lib.APIRL_SPARSE_GEOMETRY)
+        P.em_pass_sparse(t(meas), x_nz, bp, t(sens), gimg, subset, ns, add=a, zero_add=add_sum, lik=lik_nz)
+        torch.cuda.synchronize()
+        assert rel(x_nz.cpu().numpy(), x_full.cpu().numpy()) <= 1e-6
+        assert abs(lik_nz.item() - lik_full.item()) <= 1e-6 * abs(lik_full.item())
+    with pytest.raises(ap.ApirlError):
+        P.set_option(_lib.APIRL_OPT_SPARSE_IMAGE, 7)
+
