@@ -562,12 +562,14 @@ def test_drivers_with_given_sensitivity(oracle):
     assert rel(sens_all[0], sens0) <= 1e-6  # fp32 atomics: equal up to the order of additions
     img2, lik2, back = ap.osem_3d(ig, sg, meas, init, 2, 4, sens=sens_all, all_sens=True)
     assert np.array_equal(back.view(np.uint32), sens_all.view(np.uint32))
-    assert rel(img2, img) <= 1e-6 and lik2[0] == lik[0]
+    # computed sensitivities without factors let the driver take the
+    # geometry-image pass, whose likelihood sums in another order
+    assert rel(img2, img) <= 1e-6 and abs(lik2[0] - lik[0]) <= 1e-7 * abs(lik[0])
     img3, _, _ = ap.osem_3d(ig, sg, meas, init, 2, 4, sens=sens_all * np.float32(2))
     assert rel(img3, img) > 1e-3
     m_img, m_lik, m_sens = ap.mlem_3d(ig, sg, meas, init, 2)
     m_img2, m_lik2, _ = ap.mlem_3d(ig, sg, meas, init, 2, sens=m_sens)
-    assert rel(m_img2, m_img) <= 1e-6 and m_lik2[0] == m_lik[0]
+    assert rel(m_img2, m_img) <= 1e-6 and abs(m_lik2[0] - m_lik[0]) <= 1e-7 * abs(m_lik[0])
     ig2 = ImageGeom(32, 32, 1, 2.08, 2.08, 1.0)
     sg2 = Sino2DGeom(40, 48, 49.92, 300.0)
     x2 = (rng.random(ig2.n_voxels, dtype=np.float32) + 0.5).astype(np.float32)

@@ -95,4 +95,6 @@ def test_sharded_osem_one_rank_equals_driver(oracle):
     liks = job.run(x, 2)
     want, want_lik, _ = ap.osem_3d(ig, sg, meas, np.ones(ig.n_voxels, np.float32), 2, 4)
     assert rel(x.cpu().numpy(), want) <= 1e-5
-    assert np.allclose(liks, want_lik[:-1], rtol=1e-9)
+    # the driver (no multiplicative or additive term) takes the geometry-image
+    # pass, whose likelihood sums the same terms in another order
+    assert np.allclose(liks, want_lik[:-1], rtol=1e-7)
