@@ -308,6 +308,9 @@ void apirl_projector_destroy(apirl_projector* p) {
   cudaFree(p->d_minmax);
   cudaFree(p->d_scalars);
   cudaFree(p->d_chunk);
+  cudaFree(p->nz.list);
+  cudaFree(p->nz.tiles);
+  cudaFree(p->nz.n_list);
   cudaFree(p->d_lor64);
   cudaFree(p->d_z64);
   for (int k = 0; k < 2; k++) {
@@ -582,7 +585,7 @@ apirl_status fused(apirl_projector* p, SubsetSel ss, const void* d_counts, int d
   }
   CK(apirl::launch_em_pass(p->g, p->t, ss, d_counts, dtype, packed, d_add, d_x, d_bp, 1, p->is3d ? 0 : 1,
                            p->d_partials, d_lik, s, p->pg, dual ? p->pad : apirl::PadBuffers(), p->em_block,
-                           d_zimg, d_zero_add, p->persistent ? p->d_chunk : nullptr, p->sparse_image));
+                           d_zimg, d_zero_add, p->persistent ? p->d_chunk : nullptr, p->sparse_image, p->nz));
   if (p->timing) {
     CK(cudaEventRecord(p->ev1, s));
     p->timed = 1;
@@ -655,6 +658,12 @@ apirl_status apirl_em_pass_sparse(apirl_projector* p, const void* d_counts, int 
   cudaStream_t s = (cudaStream_t)stream;
   SubsetSel ss = make_subset(p, subset, nsubsets);
   const int64_t nv = (int64_t)p->g.nx * p->g.ny * p->g.nz;
+  cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+  CK(cudaStreamIsCapturing(s, &cs));
+  if (cs == cudaStreamCaptureStatusNone) {
+    st = apirl::prepare_nz_list(p, apirl_projector_num_bins(p, subset, nsubsets));
+    if (st) return st;
+  }
   if (use_dual(p)) {
     CK(apirl::launch_pad_copy(p->g, d_x, p->pad, s));
     st = fused(p, ss, d_counts, counts_dtype, counts_packed, d_add, d_x, d_bp, true, d_lik, s, d_zimg, d_zero_add);
@@ -867,3 +876,22 @@ apirl_status apirl_em_pass_host_async(apirl_projector* p, const void* h_counts_s
 }
 
 }  // extern "C"
+
+namespace apirl {
+apirl_status prepare_nz_list(apirl_projector* p, int64_t total) {
+  if (total <= p->nz.cap || !p->is3d) return APIRL_OK;
+  DEVICE_SCOPE(p->device);
+  cudaFree(p->nz.list);
+  cudaFree(p->nz.tiles);
+  p->nz.list = nullptr;
+  p->nz.tiles = nullptr;
+  p->nz.cap = 0;
+  if (!p->nz.n_list) CK(cudaMalloc(&p->nz.n_list, sizeof(int)));
+  const int64_t n_tiles = (total + 8191) / 8192;
+  CK(cudaMalloc(&p->nz.list, (size_t)total * sizeof(int)));
+  CK(cudaMalloc(&p->nz.tiles, (size_t)n_tiles * sizeof(int)));
+  p->nz.cap = total;
+  return APIRL_OK;
+}
+}  // namespace apirl
+

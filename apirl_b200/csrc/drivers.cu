@@ -203,6 +203,9 @@ apirl_status osem_3d(const apirl_image_geom* img, const apirl_sino3d_geom* sino,
     DK(r.alloc(&d_zadd, nsubsets));
     DS(zero_images(r, p, d_meas, d_add, nsubsets, sino->n_proj, d_zimg, d_zadd));
   }
+  // Room for the list of bins with counts, made before the passes are
+  // captured (subset 0 has the most angles).
+  if (d_zimg) DS(apirl::prepare_nz_list(p, apirl_projector_num_bins(p, nsubsets > 1 ? 0 : -1, nsubsets)));
   for (int s = 0; s < nsubsets; s++)
     DS(capture_pass(r, p, d_meas, d_add, d_x, d_bp, d_sens + nv * s, nullptr, 0.f, 1, s, nsubsets, d_slot + s,
                     d_zimg ? d_zimg + nv * s : nullptr, d_zadd ? d_zadd + s : nullptr));
@@ -283,6 +286,7 @@ apirl_status mlem_3d(const apirl_image_geom* img, const apirl_sino3d_geom* sino,
     DK(r.alloc(&d_zadd, 1));
     DS(zero_images(r, p, d_meas, d_add, 1, sino->n_proj, d_zimg, d_zadd));
   }
+  if (d_zimg) DS(apirl::prepare_nz_list(p, apirl_projector_num_bins(p, -1, 1)));
   DS(capture_pass(r, p, d_meas, d_add, d_x, d_bp, d_sens, d_thr, 0.f, 1, -1, 1, d_slot, d_zimg, d_zadd));
   std::vector<float> h_tmp;
   for (int t = 0; t < iters; t++) {

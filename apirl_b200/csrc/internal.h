@@ -101,13 +101,22 @@ struct PadBuffers {
   float* bT = nullptr;
   unsigned lim = 0;
 };
+// Room for the list of a subset's bins with counts (sparse passes of the
+// persistent kernel): `list` holds cap int32 bin numbers, `tiles` one int per
+// 8192 bins of cap, `n_list` one int.
+struct NzList {
+  int* list = nullptr;
+  int* tiles = nullptr;
+  int* n_list = nullptr;
+  int64_t cap = 0;
+};
 // lik_mode: 0 = over e != 0, 1 = over e > 0, 2 = over ratio > 0.  back = 0: no backprojection.
 cudaError_t launch_em_pass(const ImgGeom& g, const LorTable& t, SubsetSel s, const void* counts, int counts_dtype,
                            int counts_packed, const float* add, const float* x, float* bp, int back, int lik_mode,
                            double* partials, double* lik, cudaStream_t st, const PreciseGeom& pg = PreciseGeom(),
                            const PadBuffers& pad = PadBuffers(), int block = 0, const float* zimg = nullptr,
                            const double* zero_add = nullptr, unsigned long long* persist_counter = nullptr,
-                           int zimg_all_bins = 0);
+                           int zimg_all_bins = 0, const NzList& nz = NzList());
 // Fits the shared-memory carveout of the persistent fused kernels to `block`
 // threads per block (called outside graph capture, when a projector is made
 // or its block size changes).
@@ -210,6 +219,7 @@ struct apirl_projector {
   int persistent = 1;            // APIRL_OPT_PERSISTENT: warps pull 32-bin chunks (padded 3D pass)
   unsigned long long* d_chunk = nullptr;  // chunk counter of the persistent pass
   int sparse_image = 0;          // APIRL_OPT_SPARSE_IMAGE: 0 = zero-count image Z_s, 1 = geometry image G_s
+  apirl::NzList nz;              // list of a subset's bins with counts (sparse passes), grown on demand
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
   // Counts staged ahead of apirl_em_pass_host (apirl_stage_counts): copied on
   // copy_stream; each slot's event is recorded after its copy.
@@ -236,3 +246,10 @@ struct apirl_projector {
 
 // Records `msg` as the calling thread's last error and returns `code`.
 apirl_status apirl_internal_fail(apirl_status code, const char* msg);
+
+namespace apirl {
+// Room in p->nz for the list of `total` bins (cudaMalloc: call outside graph
+// capture; a captured sparse pass without room walks every bin's chunk).
+apirl_status prepare_nz_list(apirl_projector* p, int64_t total);
+}  // namespace apirl
+

@@ -438,19 +438,126 @@ __global__ void __launch_bounds__(kBlock) k_em_pass_rays(ImgGeom g, LorTable t, 
   if ((threadIdx.x & 31) == 0) partials[((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5] = term;
 }
 
+// ---- list of the bins with counts (the sparse pass's persistent form) -----
+// Tiles of kNzTile consecutive bins of the subset: k_nz_tiles counts each
+// tile's bins with counts, k_nz_scan turns the counts into the tiles' first
+// list positions and the list length, k_nz_write writes the bin numbers in
+// bin order.  Deterministic: the list depends on the counts alone.
+constexpr int kNzTile = 8192;
+constexpr int kNzBlock = 256;
+
+template <typename CT>
+__device__ __forceinline__ bool bin_has_count(int64_t b, const LorTable& t, const SubsetSel& s, const CT* counts,
+                                              int counts_packed) {
+  const BinPos p = decode(b, t, s);
+  const int64_t row = counts_packed ? ((int64_t)(p.g - t.g0) * s.nk + p.k) : ((int64_t)p.g * t.n_proj + p.a);
+  return load_count<CT>(counts, row * t.n_r + p.l) != 0.f;
+}
+
+template <typename CT>
+__global__ void __launch_bounds__(kNzBlock) k_nz_tiles(LorTable t, SubsetSel s, const CT* __restrict__ counts,
+                                                       int counts_packed, int64_t total, int* __restrict__ tiles) {
+  __shared__ int warp_n[kNzBlock / 32];
+  const int64_t base = (int64_t)blockIdx.x * kNzTile;
+  int n = 0;
+  for (int i = threadIdx.x; i < kNzTile; i += kNzBlock) {
+    const int64_t b = base + i;
+    n += (b < total && bin_has_count<CT>(b, t, s, counts, counts_packed)) ? 1 : 0;
+  }
+  #pragma unroll
+  for (int o = 16; o > 0; o >>= 1) n += __shfl_down_sync(0xffffffffu, n, o);
+  if ((threadIdx.x & 31) == 0) warp_n[threadIdx.x >> 5] = n;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    int sum = 0;
+    for (int w = 0; w < kNzBlock / 32; w++) sum += warp_n[w];
+    tiles[blockIdx.x] = sum;
+  }
+}
+
+// One block: tiles[i] <- sum of tiles[0..i-1]; *n_list <- sum of all.
+__global__ void __launch_bounds__(1024) k_nz_scan(int* __restrict__ tiles, int n_tiles, int* __restrict__ n_list) {
+  __shared__ int warp_sum[32];
+  __shared__ int carry;
+  if (threadIdx.x == 0) carry = 0;
+  __syncthreads();
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  for (int base = 0; base < n_tiles; base += 1024) {
+    const int i = base + (int)threadIdx.x;
+    const int v = i < n_tiles ? tiles[i] : 0;
+    int incl = v;
+    #pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const int u = __shfl_up_sync(0xffffffffu, incl, o);
+      if (lane >= o) incl += u;
+    }
+    if (lane == 31) warp_sum[warp] = incl;
+    __syncthreads();
+    if (warp == 0) {
+      int w = warp_sum[lane];
+      #pragma unroll
+      for (int o = 1; o < 32; o <<= 1) {
+        const int u = __shfl_up_sync(0xffffffffu, w, o);
+        if (lane >= o) w += u;
+      }
+      warp_sum[lane] = w;  // inclusive over warps
+    }
+    __syncthreads();
+    const int before = carry + (warp > 0 ? warp_sum[warp - 1] : 0) + incl - v;
+    if (i < n_tiles) tiles[i] = before;
+    __syncthreads();
+    if (threadIdx.x == 0) carry += warp_sum[31];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) *n_list = carry;
+}
+
+template <typename CT>
+__global__ void __launch_bounds__(kNzBlock) k_nz_write(LorTable t, SubsetSel s, const CT* __restrict__ counts,
+                                                       int counts_packed, int64_t total,
+                                                       const int* __restrict__ tiles, int* __restrict__ list) {
+  __shared__ int warp_n[kNzBlock / 32];
+  __shared__ int run;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  if (threadIdx.x == 0) run = tiles[blockIdx.x];
+  __syncthreads();
+  const int64_t base = (int64_t)blockIdx.x * kNzTile;
+  for (int i = 0; i < kNzTile; i += kNzBlock) {
+    const int64_t b = base + i + threadIdx.x;
+    const bool has = b < total && bin_has_count<CT>(b, t, s, counts, counts_packed);
+    const unsigned mask = __ballot_sync(0xffffffffu, has);
+    if (lane == 0) warp_n[warp] = __popc(mask);
+    __syncthreads();
+    int off = run;
+    for (int w = 0; w < warp; w++) off += warp_n[w];
+    if (has) list[off + __popc(mask & ((1u << lane) - 1u))] = (int)b;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      int sum = 0;
+      for (int w = 0; w < kNzBlock / 32; w++) sum += warp_n[w];
+      run += sum;
+    }
+    __syncthreads();
+  }
+}
+
 // The padded-layout fused pass as a persistent kernel: each warp takes the
 // next chunk of 32 consecutive bins from *chunk_counter until none are left,
 // so that warps never wait for the rest of their block and the SM keeps its
 // full complement of warps until the end of the pass.  The bins of a chunk
 // are those of one warp in k_em_pass, and the chunk's likelihood partial goes
 // to partials[chunk]: results are identical to k_em_pass's.
-template <typename CT>
+template <typename CT, bool LIST>
 __global__ void __launch_bounds__(kBlock, kPersistMinBlocks) k_em_pass_persist(
     ImgGeom g, LorTable t, SubsetSel s, const CT* __restrict__ counts, int counts_packed,
     const float* __restrict__ add, PadBuffers pad, int back, double* __restrict__ partials, int64_t total,
-    int skip_zero, unsigned long long* __restrict__ chunk_counter) {
+    int skip_zero, unsigned long long* __restrict__ chunk_counter, const int* __restrict__ list,
+    const int* __restrict__ n_list) {
   const int lane = threadIdx.x & 31;
-  const int64_t nchunks = (total + 31) >> 5;
+  // LIST: the chunks are 32 consecutive entries of the subset's list of bins
+  // with counts (k_nz_write), so every lane of a chunk walks.
+  const int64_t n_items = LIST ? (int64_t)*n_list : total;
+  const int64_t nchunks = (n_items + 31) >> 5;
   const int px = g.nx + 2 * kPad, py = g.ny + 2 * kPad;
   const int uz = px * py;
   for (;;) {
@@ -458,9 +565,10 @@ __global__ void __launch_bounds__(kBlock, kPersistMinBlocks) k_em_pass_persist(
     if (lane == 0) c = atomicAdd(chunk_counter, 1ULL);
     c = __shfl_sync(0xffffffffu, c, 0);
     if ((int64_t)c >= nchunks) break;
-    const int64_t b = (int64_t)c * 32 + lane;
+    const int64_t item = (int64_t)c * 32 + lane;
     double term = 0.0;
-    if (b < total) {
+    if (item < n_items) {
+      const int64_t b = LIST ? (int64_t)list[item] : item;
       const BinPos p = decode(b, t, s);
       const int64_t row = counts_packed ? ((int64_t)(p.g - t.g0) * s.nk + p.k) : ((int64_t)p.g * t.n_proj + p.a);
       const int64_t ci = row * t.n_r + p.l;
@@ -933,8 +1041,10 @@ inline unsigned stream_grid(int64_t n) {
 }  // namespace
 
 cudaError_t prepare_em_kernels(int block) {
-  for (const void* f : {(const void*)k_em_pass_persist<float>, (const void*)k_em_pass_persist<uint32_t>,
-                        (const void*)k_em_pass_persist<uint16_t>}) {
+  for (const void* f :
+       {(const void*)k_em_pass_persist<float, false>, (const void*)k_em_pass_persist<uint32_t, false>,
+        (const void*)k_em_pass_persist<uint16_t, false>, (const void*)k_em_pass_persist<float, true>,
+        (const void*)k_em_pass_persist<uint32_t, true>, (const void*)k_em_pass_persist<uint16_t, true>}) {
     cudaError_t e = fit_carveout(f, block, 0);
     if (e != cudaSuccess) return e;
   }
@@ -983,7 +1093,7 @@ cudaError_t launch_em_pass(const ImgGeom& g, const LorTable& t, SubsetSel s, con
                            int counts_packed, const float* add, const float* x, float* bp, int back, int lik_mode,
                            double* partials, double* lik, cudaStream_t st, const PreciseGeom& pg,
                            const PadBuffers& pad, int block, const float* zimg, const double* zero_add,
-                           unsigned long long* persist_counter, int zimg_all_bins) {
+                           unsigned long long* persist_counter, int zimg_all_bins, const NzList& nz) {
   const int skip = zimg ? (zimg_all_bins ? 2 : 1) : 0;
   const int64_t total = (int64_t)t.n_sinos * s.nk * t.n_r;
   if (block < 32 || block > kBlock || block % 32) block = kBlock;
@@ -1013,9 +1123,19 @@ cudaError_t launch_em_pass(const ImgGeom& g, const LorTable& t, SubsetSel s, con
     prefer_l1();
     // Persistent form: as many blocks of this size as fit on the current
     // device's SMs at once (a host-side query of a few microseconds).
-    const void* pf = counts_dtype == APIRL_F32   ? (const void*)k_em_pass_persist<float>
-                     : counts_dtype == APIRL_U32 ? (const void*)k_em_pass_persist<uint32_t>
-                                                 : (const void*)k_em_pass_persist<uint16_t>;
+    // Sparse passes walk a list of the subset's bins with counts when the
+    // projector gives room for one (bin numbers are int32).
+    const bool use_list = skip && nz.list && nz.tiles && nz.n_list && total <= nz.cap && total < ((int64_t)1 << 31);
+    const void* pf;
+    switch (counts_dtype) {
+      case APIRL_F32: pf = use_list ? (const void*)k_em_pass_persist<float, true>
+                                    : (const void*)k_em_pass_persist<float, false>; break;
+      case APIRL_U32: pf = use_list ? (const void*)k_em_pass_persist<uint32_t, true>
+                                    : (const void*)k_em_pass_persist<uint32_t, false>; break;
+      case APIRL_U16: pf = use_list ? (const void*)k_em_pass_persist<uint16_t, true>
+                                    : (const void*)k_em_pass_persist<uint16_t, false>; break;
+      default: return cudaErrorInvalidValue;
+    }
     // Fitted here unless the launch is being captured into a graph (the
     // projector fits it ahead for its block size: prepare_em_kernels).
     cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
@@ -1023,11 +1143,7 @@ cudaError_t launch_em_pass(const ImgGeom& g, const LorTable& t, SubsetSel s, con
     if (fe != cudaSuccess) return fe;
     if (cs == cudaStreamCaptureStatusNone && (fe = fit_carveout(pf, block, 0)) != cudaSuccess) return fe;
     int per_sm = 0, dev = 0, sms = 0;
-    cudaError_t oe = counts_dtype == APIRL_F32
-        ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_em_pass_persist<float>, block, 0)
-        : (counts_dtype == APIRL_U32
-               ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_em_pass_persist<uint32_t>, block, 0)
-               : cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_em_pass_persist<uint16_t>, block, 0));
+    cudaError_t oe = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, pf, block, 0);
     if (oe != cudaSuccess) return oe;
     if ((oe = cudaGetDevice(&dev)) != cudaSuccess) return oe;
     if ((oe = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev)) != cudaSuccess) return oe;
@@ -1037,23 +1153,58 @@ cudaError_t launch_em_pass(const ImgGeom& g, const LorTable& t, SubsetSel s, con
     const unsigned pgrid = (unsigned)(need < resident ? need : resident);
     cudaError_t me = cudaMemsetAsync(persist_counter, 0, sizeof(unsigned long long), st);
     if (me != cudaSuccess) return me;
+    if (use_list) {
+      // The list, and zeros in the partials of the chunks the list leaves
+      // out (the sum below runs over as many partials as the full pass has).
+      const unsigned n_tiles = (unsigned)((total + kNzTile - 1) / kNzTile);
+      switch (counts_dtype) {
+        case APIRL_F32:
+          k_nz_tiles<float><<<n_tiles, kNzBlock, 0, st>>>(t, s, (const float*)counts, counts_packed, total, nz.tiles);
+          break;
+        case APIRL_U32:
+          k_nz_tiles<uint32_t><<<n_tiles, kNzBlock, 0, st>>>(t, s, (const uint32_t*)counts, counts_packed, total,
+                                                             nz.tiles);
+          break;
+        default:
+          k_nz_tiles<uint16_t><<<n_tiles, kNzBlock, 0, st>>>(t, s, (const uint16_t*)counts, counts_packed, total,
+                                                             nz.tiles);
+          break;
+      }
+      k_nz_scan<<<1, 1024, 0, st>>>(nz.tiles, (int)n_tiles, nz.n_list);
+      switch (counts_dtype) {
+        case APIRL_F32:
+          k_nz_write<float><<<n_tiles, kNzBlock, 0, st>>>(t, s, (const float*)counts, counts_packed, total, nz.tiles,
+                                                          nz.list);
+          break;
+        case APIRL_U32:
+          k_nz_write<uint32_t><<<n_tiles, kNzBlock, 0, st>>>(t, s, (const uint32_t*)counts, counts_packed, total,
+                                                             nz.tiles, nz.list);
+          break;
+        default:
+          k_nz_write<uint16_t><<<n_tiles, kNzBlock, 0, st>>>(t, s, (const uint16_t*)counts, counts_packed, total,
+                                                             nz.tiles, nz.list);
+          break;
+      }
+      if ((me = cudaMemsetAsync(partials, 0, (size_t)chunks * sizeof(double), st)) != cudaSuccess) return me;
+    }
+#define APIRL_PERSIST(CT)                                                                                       \
+  do {                                                                                                          \
+    if (use_list)                                                                                               \
+      k_em_pass_persist<CT, true><<<pgrid, block, 0, st>>>(g, t, s, (const CT*)counts, counts_packed, add, pad,  \
+                                                           back, partials, total, skip, persist_counter,        \
+                                                           nz.list, nz.n_list);                                 \
+    else                                                                                                        \
+      k_em_pass_persist<CT, false><<<pgrid, block, 0, st>>>(g, t, s, (const CT*)counts, counts_packed, add, pad, \
+                                                            back, partials, total, skip, persist_counter,       \
+                                                            nullptr, nullptr);                                  \
+  } while (0)
     switch (counts_dtype) {
-      case APIRL_F32:
-        k_em_pass_persist<float><<<pgrid, block, 0, st>>>(g, t, s, (const float*)counts, counts_packed, add, pad,
-                                                          back, partials, total, skip, persist_counter);
-        break;
-      case APIRL_U32:
-        k_em_pass_persist<uint32_t><<<pgrid, block, 0, st>>>(g, t, s, (const uint32_t*)counts, counts_packed, add,
-                                                             pad, back, partials, total, skip,
-                                                             persist_counter);
-        break;
-      case APIRL_U16:
-        k_em_pass_persist<uint16_t><<<pgrid, block, 0, st>>>(g, t, s, (const uint16_t*)counts, counts_packed, add,
-                                                             pad, back, partials, total, skip,
-                                                             persist_counter);
-        break;
+      case APIRL_F32: APIRL_PERSIST(float); break;
+      case APIRL_U32: APIRL_PERSIST(uint32_t); break;
+      case APIRL_U16: APIRL_PERSIST(uint16_t); break;
       default: return cudaErrorInvalidValue;
     }
+#undef APIRL_PERSIST
     cudaError_t pe = cudaGetLastError();
     if (pe != cudaSuccess || !lik) return pe;
     int64_t np = chunks;
