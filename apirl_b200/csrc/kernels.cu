@@ -446,12 +446,22 @@ __global__ void __launch_bounds__(kBlock) k_em_pass_rays(ImgGeom g, LorTable t, 
 constexpr int kNzTile = 8192;
 constexpr int kNzBlock = 256;
 
+// The list is used for fewer than 2^31 bins, so bin numbers decode in 32-bit
+// integer arithmetic here (decode's 64-bit divisions made these streaming
+// kernels instruction-bound).
 template <typename CT>
-__device__ __forceinline__ bool bin_has_count(int64_t b, const LorTable& t, const SubsetSel& s, const CT* counts,
+__device__ __forceinline__ bool bin_has_count(int64_t b64, const LorTable& t, const SubsetSel& s, const CT* counts,
                                               int counts_packed) {
-  const BinPos p = decode(b, t, s);
-  const int64_t row = counts_packed ? ((int64_t)(p.g - t.g0) * s.nk + p.k) : ((int64_t)p.g * t.n_proj + p.a);
-  return load_count<CT>(counts, row * t.n_r + p.l) != 0.f;
+  const int b = (int)b64;
+  const int per = s.nk * t.n_r;
+  const int gl = b / per;
+  const int rem = b - gl * per;
+  const int k = rem / t.n_r;
+  const int l = rem - k * t.n_r;
+  const int g = t.g0 + gl;
+  const int a = s.subset < 0 ? k : s.subset + s.nsub * k;
+  const int64_t row = counts_packed ? ((int64_t)gl * s.nk + k) : ((int64_t)g * t.n_proj + a);
+  return load_count<CT>(counts, row * t.n_r + l) != 0.f;
 }
 
 template <typename CT>

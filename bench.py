@@ -522,7 +522,9 @@ def run_gpu(args):
             "cpu_baseline": cpu,
             # per step: layout copy, fused kernel, (zero-count dot,) two-level
             # likelihood sum, reduce/update; plus one zero-count kernel per subset
-            "gpu_launches": (6 * args.steps + NSUB) if sparse else (6 * args.steps if nonzero else 5 * args.steps),
+            # per pass: layout copy, [list: tiles, scan, write], fused kernel,
+            # [dot product], two-level sum, update
+            "gpu_launches": (9 * args.steps + NSUB) if sparse else (9 * args.steps if nonzero else 5 * args.steps),
             "clocks": clock,
         }
         print(json.dumps(line), flush=True)
