@@ -38,6 +38,12 @@ constexpr int kSumLevel2 = 296;  // first-level blocks of the two-level partial 
 #define APIRL_EM_MIN_BLOCKS 5
 #endif
 constexpr int kPersistMinBlocks = APIRL_PERSIST_MIN_BLOCKS;
+// The persistent kernel over a list of the bins with counts (sparse passes)
+// is bound by memory latency rather than issue: 5 blocks (48 registers, no
+// spill) with six gather segments in flight, measured 0.8 % faster there
+// than the full pass's 6 blocks with four segments.
+constexpr int kListMinBlocks = 5;
+constexpr int kListGatherUnroll = 6;
 constexpr int kEmMinBlocks = APIRL_EM_MIN_BLOCKS;
 // 1: the fused 3D pass sets the walk up a second time for the backprojection
 // (fewer live registers during the forward walk).
@@ -558,7 +564,7 @@ __global__ void __launch_bounds__(kNzBlock) k_nz_write(LorTable t, SubsetSel s, 
 // are those of one warp in k_em_pass, and the chunk's likelihood partial goes
 // to partials[chunk]: results are identical to k_em_pass's.
 template <typename CT, bool LIST>
-__global__ void __launch_bounds__(kBlock, kPersistMinBlocks) k_em_pass_persist(
+__global__ void __launch_bounds__(kBlock, LIST ? kListMinBlocks : kPersistMinBlocks) k_em_pass_persist(
     ImgGeom g, LorTable t, SubsetSel s, const CT* __restrict__ counts, int counts_packed,
     const float* __restrict__ add, PadBuffers pad, int back, double* __restrict__ partials, int64_t total,
     int skip_zero, unsigned long long* __restrict__ chunk_counter, const int* __restrict__ list,
@@ -591,7 +597,8 @@ __global__ void __launch_bounds__(kBlock, kPersistMinBlocks) k_em_pass_persist(
         const int ux = tr ? py : 1, uy = tr ? 1 : px;
         Walk3 w;
         siddon3_setup(L.x, L.y, z.x, vx, vy, A_SUB(z.y, z.x), g, w);
-        float e = siddon3_gather_pad(w, g, ux, uy, uz, pad.lim, tr ? pad.pT : pad.pA);
+        float e = siddon3_gather_pad<LIST ? kListGatherUnroll : APIRL_GATHER_UNROLL>(w, g, ux, uy, uz, pad.lim,
+                                                                                   tr ? pad.pT : pad.pA);
         if (add) e = A_ADD(e, __ldg(add + ci));
         const float r = (m != 0.f && e != 0.f) ? A_DIV(m, e) : 0.f;
         if (e != 0.f) term = lik_term(m, e, skip_zero);

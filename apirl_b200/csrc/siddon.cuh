@@ -124,13 +124,13 @@ __device__ __forceinline__ float next_crossing(const Walk3& w, bool& cx, bool& c
 #ifndef APIRL_GATHER_UNROLL
 #define APIRL_GATHER_UNROLL 4
 #endif
+template <int U = APIRL_GATHER_UNROLL>
 __device__ __forceinline__ float siddon3_gather_pad(Walk3 w, const ImgGeom& g, int ux, int uy, int uz, unsigned lim,
                                                     const float* __restrict__ img) {
   const int sx = w.iinc * ux, sy = w.jinc * uy, sz = w.kinc * uz;
   int idx = (w.k + kPad) * uz + (w.j + kPad) * uy + (w.i + kPad) * ux;
   float acc = 0.f;
   if (w.guarded) {
-    constexpr int U = APIRL_GATHER_UNROLL;
     int m = 0;
     for (; m + U <= w.n; m += U) {
       int ia[U];
