@@ -472,8 +472,7 @@ apirl_status apirl_backproject(apirl_projector* p, const float* d_sino, float* d
   if (st) return st;
   if (!d_image || !d_sino) return fail(APIRL_ERR_INVALID, "null image or sinogram");
   DEVICE_SCOPE(p->device);
-  CK(apirl::launch_backproject(p->g, p->t, make_subset(p, subset, nsubsets), d_sino, 0, nullptr, 0, d_image,
-                               (cudaStream_t)stream, p->pg));
+  CK(apirl::backproject_sino(p, make_subset(p, subset, nsubsets), d_sino, 0, d_image, (cudaStream_t)stream));
   return APIRL_OK;
 }
 
@@ -482,8 +481,7 @@ apirl_status apirl_backproject_ones(apirl_projector* p, float* d_image, int subs
   if (st) return st;
   if (!d_image) return fail(APIRL_ERR_INVALID, "null image");
   DEVICE_SCOPE(p->device);
-  CK(apirl::launch_backproject(p->g, p->t, make_subset(p, subset, nsubsets), nullptr, 2, nullptr, 0, d_image,
-                               (cudaStream_t)stream, p->pg));
+  CK(apirl::backproject_sino(p, make_subset(p, subset, nsubsets), nullptr, 2, d_image, (cudaStream_t)stream));
   return APIRL_OK;
 }
 
@@ -892,6 +890,14 @@ apirl_status prepare_nz_list(apirl_projector* p, int64_t total) {
   CK(cudaMalloc(&p->nz.tiles, (size_t)n_tiles * sizeof(int)));
   p->nz.cap = total;
   return APIRL_OK;
+}
+}  // namespace apirl
+
+namespace apirl {
+cudaError_t backproject_sino(apirl_projector* p, SubsetSel ss, const float* vin, int vin_mode, float* img,
+                             cudaStream_t st) {
+  if (use_dual(p)) return launch_backproject_pad(p->g, p->t, ss, vin, vin_mode, img, p->pad, p->d_chunk, st);
+  return launch_backproject(p->g, p->t, ss, vin, vin_mode, nullptr, 0, img, st, p->pg);
 }
 }  // namespace apirl
 

@@ -188,8 +188,7 @@ apirl_status osem_3d(const apirl_image_geom* img, const apirl_sino3d_geom* sino,
     } else {
       SubsetSel ss;
       ss.subset = s; ss.nsub = nsubsets; ss.nk = apirl::subset_nproj(sino->n_proj, s, nsubsets);
-      DK(apirl::launch_backproject(p->g, p->t, ss, d_mult, d_mult ? 1 : 2, nullptr, 0, d_sens + nv * s, r.st,
-                                   p->pg));
+      DK(apirl::backproject_sino(p, ss, d_mult, d_mult ? 1 : 2, d_sens + nv * s, r.st));
     }
     DK(apirl::launch_force_positive(nv, d_sens + nv * s, r.st));
   }
@@ -273,7 +272,7 @@ apirl_status mlem_3d(const apirl_image_geom* img, const apirl_sino3d_geom* sino,
   if (h_sens_in)
     DK(cudaMemcpyAsync(d_sens, h_sens_in, nv * sizeof(float), cudaMemcpyHostToDevice, r.st));
   else
-    DK(apirl::launch_backproject(p->g, p->t, all, d_mult, d_mult ? 1 : 2, nullptr, 0, d_sens, r.st));
+    DK(apirl::backproject_sino(p, all, d_mult, d_mult ? 1 : 2, d_sens, r.st));
   DS(apirl_mlem_threshold(nv, d_sens, d_thr, r.st));
   double* d_slot = d_lik + iters + 1;
   float* d_zimg = nullptr;

@@ -134,6 +134,11 @@ cudaError_t launch_pad_copy(const ImgGeom& g, const float* x, const PadBuffers& 
 // mode 0: EM update of x from bA + bT (threshold rule); mode 1: bp += bA + bT.  Clears bA, bT.
 cudaError_t launch_pad_reduce(const ImgGeom& g, const PadBuffers& pad, int mode, float* x, float* bp,
                               const float* sens, const float* thr_ptr, float thr_value, int ge, cudaStream_t st);
+// 3D backprojection img += A^T v through the padded pair (3D float walk, one
+// ray per bin): a persistent scatter, then k_pad_reduce folds the pair into
+// img and clears it.  `counter` is the projector's chunk counter.
+cudaError_t launch_backproject_pad(const ImgGeom& g, const LorTable& t, SubsetSel s, const float* vin, int vin_mode,
+                                   float* img, const PadBuffers& pad, unsigned long long* counter, cudaStream_t st);
 cudaError_t launch_inverse_divide(int64_t n, const float* meas, float* est, cudaStream_t st);
 cudaError_t launch_add_bins(int64_t n, const float* add, float* est, cudaStream_t st);
 cudaError_t launch_likelihood(int64_t n, const float* est, const float* meas, int gt0, double* partials,
@@ -251,5 +256,9 @@ namespace apirl {
 // Room in p->nz for the list of `total` bins (cudaMalloc: call outside graph
 // capture; a captured sparse pass without room walks every bin's chunk).
 apirl_status prepare_nz_list(apirl_projector* p, int64_t total);
+// img += A_s^T v (vin_mode as load_bin): through the padded pair when the
+// projector has it (launch_backproject_pad), else launch_backproject.
+cudaError_t backproject_sino(apirl_projector* p, SubsetSel ss, const float* vin, int vin_mode, float* img,
+                             cudaStream_t st);
 }  // namespace apirl
 

@@ -444,6 +444,42 @@ __global__ void __launch_bounds__(kBlock) k_em_pass_rays(ImgGeom g, LorTable t, 
   if ((threadIdx.x & 31) == 0) partials[((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5] = term;
 }
 
+// ---- backprojection over the padded pair (3D, one float ray per bin) -------
+// The fused pass's scatter alone: warps pull 32-bin chunks from a counter
+// and scatter seg * v into the padded backprojection pair (rays running
+// mostly along x into the transposed one), which k_pad_reduce then folds
+// into the image.  v is the bin's value (vin_mode as load_bin); bins with
+// v == 0 are not walked, as SiddonProjector::Backproject skips them
+// (SiddonProjector.cpp:496).
+__global__ void __launch_bounds__(kBlock, kPersistMinBlocks) k_scatter_persist(
+    ImgGeom g, LorTable t, SubsetSel s, const float* __restrict__ vin, int vin_mode, PadBuffers pad, int64_t total,
+    unsigned long long* __restrict__ chunk_counter) {
+  const int lane = threadIdx.x & 31;
+  const int64_t nchunks = (total + 31) >> 5;
+  const int px = g.nx + 2 * kPad, py = g.ny + 2 * kPad;
+  const int uz = px * py;
+  for (;;) {
+    unsigned long long c = 0;
+    if (lane == 0) c = atomicAdd(chunk_counter, 1ULL);
+    c = __shfl_sync(0xffffffffu, c, 0);
+    if ((int64_t)c >= nchunks) break;
+    const int64_t b = (int64_t)c * 32 + lane;
+    if (b < total) {
+      const BinPos p = decode(b, t, s);
+      const float v = load_bin(vin, vin_mode, b, p, t);
+      if (v != 0.f) {
+        const float4 L = t.lor[(int64_t)p.a * t.n_r + p.l];
+        const float2 z = t.z[p.g];
+        const float vx = A_SUB(L.z, L.x), vy = A_SUB(L.w, L.y);
+        const bool tr = fabsf(vx) >= fabsf(vy);
+        Walk3 w;
+        siddon3_setup(L.x, L.y, z.x, vx, vy, A_SUB(z.y, z.x), g, w);
+        siddon3_scatter_pad(w, g, tr ? py : 1, tr ? 1 : px, uz, pad.lim, v, tr ? pad.bT : pad.bA);
+      }
+    }
+  }
+}
+
 // ---- list of the bins with counts (the sparse pass's persistent form) -----
 // Tiles of kNzTile consecutive bins of the subset: k_nz_tiles counts each
 // tile's bins with counts, k_nz_scan turns the counts into the tiles' first
@@ -1097,6 +1133,24 @@ cudaError_t launch_backproject(const ImgGeom& g, const LorTable& t, SubsetSel s,
     k_backproject3<false><<<grid_for(total), kBlock, 0, st>>>(g, t, s, pg, vin, vin_mode, vest, divide, img, total);
   else k_backproject2<<<grid_for(total), kBlock, 0, st>>>(g, t, s, vin, vin_mode, vest, divide, img, total);
   return cudaGetLastError();
+}
+
+cudaError_t launch_backproject_pad(const ImgGeom& g, const LorTable& t, SubsetSel s, const float* vin, int vin_mode,
+                                   float* img, const PadBuffers& pad, unsigned long long* counter, cudaStream_t st) {
+  const int64_t total = (int64_t)t.n_sinos * s.nk * t.n_r;
+  if (total == 0) return cudaSuccess;
+  int per_sm = 0, dev = 0, sms = 0;
+  cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_scatter_persist, 128, 0);
+  if (e != cudaSuccess) return e;
+  if ((e = cudaGetDevice(&dev)) != cudaSuccess) return e;
+  if ((e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev)) != cudaSuccess) return e;
+  const int64_t resident = (int64_t)(per_sm < 1 ? 1 : per_sm) * sms;
+  const int64_t need = ((total + 31) / 32 * 32 + 127) / 128;
+  if ((e = cudaMemsetAsync(counter, 0, sizeof(unsigned long long), st)) != cudaSuccess) return e;
+  k_scatter_persist<<<(unsigned)(need < resident ? need : resident), 128, 0, st>>>(g, t, s, vin, vin_mode, pad, total,
+                                                                                 counter);
+  if ((e = cudaGetLastError()) != cudaSuccess) return e;
+  return launch_pad_reduce(g, pad, 1, nullptr, img, nullptr, nullptr, 0.f, 0, st);
 }
 
 cudaError_t launch_count_steps(const ImgGeom& g, const LorTable& t, SubsetSel s, int32_t* steps, cudaStream_t st) {
