@@ -35,7 +35,10 @@ apirl_status bfail(apirl_status code, const char* what, cudaError_t e = cudaSucc
 size_t count_elem_size(int dtype) { return dtype == APIRL_U16 ? 2 : 4; }
 
 // Passes with at least this many bins get a launch of their own.
-constexpr int64_t kOwnLaunchBins = 1 << 20;
+#ifndef APIRL_BATCH_OWN_BINS
+#define APIRL_BATCH_OWN_BINS (1 << 20)
+#endif
+constexpr int64_t kOwnLaunchBins = APIRL_BATCH_OWN_BINS;
 
 enum class Stage { Queued, Sens, Passes, Final, Done };
 
@@ -70,6 +73,13 @@ int64_t footprint_of(const apirl_image_geom& img, const apirl_sino3d_geom& sino,
   b += pv * 4 * 4;                                        // padded two-layout image and backprojection copies
   b += (int64_t)sino.n_proj * sino.n_r * 16;              // LOR table
   b += ((nbins + 255) / 256) * 8 + 4096;                  // partials, small tables
+  // The geometry-image sparse pass of jobs without factors walks a list of
+  // the bins with counts (room for the largest subset).
+  if (!mult && !add && sino.n_proj > 0) {
+    const int64_t per_angle = nbins / sino.n_proj;
+    const int ns = nsub > 0 ? nsub : 1;
+    b += per_angle * ((sino.n_proj + ns - 1) / ns) * 4 + 4096;
+  }
   return b;
 }
 
@@ -127,6 +137,12 @@ apirl_status admit(apirl_batch* b, Job& j) {
     BK(apirl::launch_fill(j.nvox, j.d_x, 1.f, b->st));
   BK(cudaMemsetAsync(j.d_bp, 0, j.nvox * sizeof(float), b->st));
   BK(cudaMemsetAsync(j.d_sens, 0, j.nvox * j.nsub * sizeof(float), b->st));
+  // Without factors each sensitivity image is A_s^T 1, the geometry image of
+  // the sparse pass: big jobs' passes then walk only their bins with counts.
+  if (!j.h_mult && !j.h_add) {
+    s = apirl_projector_set_option(j.p, APIRL_OPT_SPARSE_IMAGE, APIRL_SPARSE_GEOMETRY);
+    if (s != APIRL_OK) return s;
+  }
   j.stage = Stage::Sens;
   b->used += j.footprint;
   return APIRL_OK;
@@ -308,9 +324,13 @@ apirl_status apirl_batch_step(apirl_batch* b, int* n_active, int* n_queued) {
   }
   for (Job* j : big) {
     const int sub = j->pass % j->nsub;
-    apirl_status es = apirl_em_pass(j->p, j->d_counts, j->dtype, 0, j->d_add, j->d_x, j->d_bp,
-                                    j->d_sens + (int64_t)sub * j->nvox, nullptr, 0.f, 1, sub, j->nsub,
-                                    j->d_lik + j->pass, b->st);
+    float* sens_s = j->d_sens + (int64_t)sub * j->nvox;
+    apirl_status es = (!j->d_mult && !j->d_add)
+                          ? apirl_em_pass_sparse(j->p, j->d_counts, j->dtype, 0, nullptr, j->d_x, j->d_bp, sens_s,
+                                                 sens_s, nullptr, nullptr, 0.f, 1, sub, j->nsub, j->d_lik + j->pass,
+                                                 b->st)
+                          : apirl_em_pass(j->p, j->d_counts, j->dtype, 0, j->d_add, j->d_x, j->d_bp, sens_s, nullptr,
+                                          0.f, 1, sub, j->nsub, j->d_lik + j->pass, b->st);
     if (es != APIRL_OK) return es;
   }
   if (nu) {
