@@ -885,7 +885,7 @@ apirl_status prepare_nz_list(apirl_projector* p, int64_t total) {
   p->nz.tiles = nullptr;
   p->nz.cap = 0;
   if (!p->nz.n_list) CK(cudaMalloc(&p->nz.n_list, sizeof(int)));
-  const int64_t n_tiles = (total + 8191) / 8192;
+  const int64_t n_tiles = (total + apirl::kNzTile - 1) / apirl::kNzTile;
   CK(cudaMalloc(&p->nz.list, (size_t)total * sizeof(int)));
   CK(cudaMalloc(&p->nz.tiles, (size_t)n_tiles * sizeof(int)));
   p->nz.cap = total;

@@ -101,9 +101,11 @@ struct PadBuffers {
   float* bT = nullptr;
   unsigned lim = 0;
 };
+// Bins per tile of the list building (one block each).
+constexpr int kNzTile = 2048;
 // Room for the list of a subset's bins with counts (sparse passes of the
 // persistent kernel): `list` holds cap int32 bin numbers, `tiles` one int per
-// 8192 bins of cap, `n_list` one int.
+// kNzTile bins of cap, `n_list` one int.
 struct NzList {
   int* list = nullptr;
   int* tiles = nullptr;

@@ -481,11 +481,10 @@ __global__ void __launch_bounds__(kBlock, kPersistMinBlocks) k_scatter_persist(
 }
 
 // ---- list of the bins with counts (the sparse pass's persistent form) -----
-// Tiles of kNzTile consecutive bins of the subset: k_nz_tiles counts each
+// Tiles of kNzTile (internal.h) consecutive bins of the subset: k_nz_tiles counts each
 // tile's bins with counts, k_nz_scan turns the counts into the tiles' first
 // list positions and the list length, k_nz_write writes the bin numbers in
 // bin order.  Deterministic: the list depends on the counts alone.
-constexpr int kNzTile = 8192;
 constexpr int kNzBlock = 256;
 
 // The list is used for fewer than 2^31 bins, so bin numbers decode in 32-bit
