@@ -308,8 +308,15 @@ apirl_status apirl_em_pass(apirl_projector* p, const void* d_counts, int counts_
  * from apirl_zero_count_image for the same counts, subset and additive term
  * (it accumulates into d_zimg: zero it first; d_zero_add may be NULL when
  * there is no additive term).
+ * With APIRL_OPT_SPARSE_IMAGE = APIRL_SPARSE_GEOMETRY, d_zimg is instead
+ * G_s = A_s^T 1 (apirl_backproject_ones: the geometry alone) and *d_zero_add
+ * the sum of every bin's additive term.  Either way the walked bins are
+ * listed first (a per-pass list of the bins with counts, in bin order, in a
+ * buffer the projector grows outside graph capture), so each warp walks 32
+ * bins with counts at a time.
  * The image update equals apirl_em_pass's up to the order of fp32 additions;
- * the FP64 likelihood equals it up to the rounding of Z_s (~1e-7 relative). */
+ * the FP64 likelihood equals it up to the rounding of the image dot product
+ * (~1e-7 relative). */
 apirl_status apirl_zero_count_image(apirl_projector* p, const void* d_counts, int counts_dtype, int counts_packed,
                                     const float* d_add, float* d_zimg, double* d_zero_add, int subset, int nsubsets,
                                     void* stream);
