@@ -396,6 +396,31 @@ def run_gpu(args):
         if world > 1:
             dist.barrier()
         clock = clocks.stop()
+        # The same sub-iterations walking every bin (the full pass), timed
+        # the same way right after, reported beside the headline.
+        full_cmp = None
+        if nonzero:
+            fev = [[torch.cuda.Event(enable_timing=True) for _ in range(2)] for _ in range(args.steps)]
+            fkern = []
+            for i in range(args.steps):
+                flush.zero_()
+                fev[i][0].record(stream)
+                P.em_pass(counts, x, bp, sens[subs[i]], subs[i], NSUB, thr_value=0.0, ge=UPDATE_GE, lik=lik,
+                          stream=stream)
+                fev[i][1].record(stream)
+                fkern.append(P.last_kernel_ms())
+            torch.cuda.synchronize(dev)
+            if world > 1:
+                dist.barrier()
+            f_value, _ = whole_job_value(args.steps, sum(fev[i][0].elapsed_time(fev[i][1])
+                                                         for i in range(args.steps)),
+                                         world, dist if world > 1 else None, dev)
+            fb = statistics.mean(step_bytes(w, s_, False)[0] for s_ in subs)
+            f_ach = fb / (statistics.mean(fkern) / 1e3) / 1e9
+            full_cmp = {"value": f_value, "unit": UNIT, "kernel_ms": statistics.mean(fkern),
+                        "roofline_achieved": f_ach, "roofline_frac": f_ach / peaks()[0],
+                        "traffic": FULL_TRAFFIC_BYTES if args.max_ring_diff is None else None,
+                        "pass": "full: every bin walked, every estimate summed (--pass full)"}
     step_ms = [evs[i][0].elapsed_time(evs[i][1]) for i in range(args.steps)]
     pre_ms = pre[0].elapsed_time(pre[1]) if sparse else 0.0
     value, total_ms = whole_job_value(args.steps, sum(step_ms) + pre_ms, world, dist if world > 1 else None, dev)
@@ -512,6 +537,7 @@ def run_gpu(args):
                                  "no ray of subsets 3 and 16 crosses)",
                        "parallelism": f"replicas x{world}"},
             "siddon_gsteps_per_s": gsteps,
+            "full_pass": full_cmp,
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak,
                          "traffic": args.traffic_bytes if args.traffic_bytes is not None else
