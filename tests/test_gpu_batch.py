@@ -84,3 +84,28 @@ def test_serve_continuous_batching(small_jobs):
         solo, _, _ = ap.osem_3d(j.image_geom, j.sino_geom, j.counts.astype(np.float32),
                                 np.ones(j.image_geom.n_voxels, np.float32), j.iters, j.nsubsets)
         assert rel(img, solo) <= 1e-4
+
+
+def test_batch_big_job_matches_solo():
+    """A job whose passes run on their own (2^20 or more bins per pass) and has
+    no multiplicative or additive sinogram takes the geometry-image sparse
+    pass, beside a small job in the shared launch; both match their solo runs
+    (which take the same pass form)."""
+    if not torch.cuda.is_available():
+        pytest.skip("no CUDA device")
+    specs = [dict(n=128, z=41, seed=7, counts=3e6, iters=2, nsubsets=3),
+             dict(n=32, z=9, seed=8, counts=1e5, iters=2, nsubsets=3)]
+    jobs = make_jobs(specs)
+    P = ap.SiddonProjector(jobs[0].image_geom, jobs[0].sino_geom)
+    assert P.num_bins(0, 3) >= 1 << 20
+    P.close()
+    b = Batch(0, budget_bytes=16 << 30)
+    res = b.run_all(jobs)
+    b.close()
+    for j, (img, lik) in zip(jobs, res):
+        solo, solo_lik, _ = ap.osem_3d(j.image_geom, j.sino_geom, j.counts.astype(np.float32),
+                                       np.ones(j.image_geom.n_voxels, np.float32), j.iters, j.nsubsets)
+        finite = np.isfinite(solo)
+        assert np.array_equal(np.isfinite(img), finite), j.tag
+        assert rel(img[finite], solo[finite]) <= 1e-4, j.tag
+        assert np.allclose(lik[:-1], solo_lik[:-1], rtol=1e-6), j.tag
