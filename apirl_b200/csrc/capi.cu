@@ -675,6 +675,34 @@ apirl_status apirl_em_pass_sparse(apirl_projector* p, const void* d_counts, int 
   return APIRL_OK;
 }
 
+apirl_status apirl_em_project_backproject_sparse(apirl_projector* p, const void* d_counts, int counts_dtype,
+                                                 int counts_packed, const float* d_add, const float* d_x, float* d_bp,
+                                                 const float* d_zimg, const double* d_zero_add, int subset,
+                                                 int nsubsets, double* d_lik, void* stream) {
+  apirl_status st = check_em(p, d_counts, counts_dtype, d_x, d_bp, subset, nsubsets);
+  if (st) return st;
+  if (!d_zimg) return fail(APIRL_ERR_INVALID, "null zero-count or geometry image");
+  if (!p->is3d || p->t.lor_s || p->pg.enabled)
+    return fail(APIRL_ERR_NOT_SUPPORTED, "the sparse pass needs a 3D projector with one float ray per bin");
+  DEVICE_SCOPE(p->device);
+  cudaStream_t s = (cudaStream_t)stream;
+  SubsetSel ss = make_subset(p, subset, nsubsets);
+  cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+  CK(cudaStreamIsCapturing(s, &cs));
+  if (cs == cudaStreamCaptureStatusNone) {
+    st = apirl::prepare_nz_list(p, apirl_projector_num_bins(p, subset, nsubsets));
+    if (st) return st;
+  }
+  if (use_dual(p)) {
+    CK(apirl::launch_pad_copy(p->g, d_x, p->pad, s));
+    st = fused(p, ss, d_counts, counts_dtype, counts_packed, d_add, d_x, d_bp, true, d_lik, s, d_zimg, d_zero_add);
+    if (st) return st;
+    CK(apirl::launch_pad_reduce(p->g, p->pad, 1, nullptr, d_bp, nullptr, nullptr, 0.f, 0, s));
+    return APIRL_OK;
+  }
+  return fused(p, ss, d_counts, counts_dtype, counts_packed, d_add, d_x, d_bp, false, d_lik, s, d_zimg, d_zero_add);
+}
+
 apirl_status apirl_em_project_backproject(apirl_projector* p, const void* d_counts, int counts_dtype,
                                           int counts_packed, const float* d_add, const float* d_x, float* d_bp,
                                           int subset, int nsubsets, double* d_lik, void* stream) {

@@ -198,8 +198,14 @@ class SiddonProjector:
         return x
 
     def em_project_backproject(self, counts, x, bp, subset=-1, nsubsets=1, add=None, counts_packed=False, lik=None,
-                               stream=None):
-        """The fused kernel of em_pass alone (bp += A^T (m / (A x + add))); x is not updated."""
+                               stream=None, zimg=None, zero_add=None):
+        """The fused kernel of em_pass alone (bp += A^T (m / (A x + add))); x is
+        not updated.  With zimg: the sparse form (apirl_em_project_backproject_sparse)."""
+        if zimg is not None:
+            check(self.lib.apirl_em_project_backproject_sparse(
+                self.h, _ptr(counts), _counts_dtype(counts), int(counts_packed), _ptr(add), _ptr(x), _ptr(bp),
+                _ptr(zimg), _ptr(zero_add), subset, nsubsets, _ptr(lik), _stream(stream)))
+            return bp
         check(self.lib.apirl_em_project_backproject(self.h, _ptr(counts), _counts_dtype(counts), int(counts_packed),
                                                     _ptr(add), _ptr(x), _ptr(bp), subset, nsubsets, _ptr(lik),
                                                     _stream(stream)))

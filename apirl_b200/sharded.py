@@ -88,7 +88,7 @@ class GpuShard:
     the whole job's counts (and multiplicative term) resident on `device`."""
 
     def __init__(self, image_geom, sino_geom, counts, nsubsets, first, n, device=0, mult=None, stream=None,
-                 ge=True):
+                 ge=True, geometry_sparse=False):
         import torch
         from .projector import SiddonProjector
         self.torch = torch
@@ -102,6 +102,13 @@ class GpuShard:
         self.nsub = nsubsets
         self.stream = stream
         self.ge = ge                  # update where sens >= 0 (the reference's OSEM rule) or > 0
+        # geometry_sparse: passes walk only the shard's bins with counts, the
+        # likelihood from the shard's geometry images G_s = A_s^T 1 (made on
+        # first use, per subset); summed over the shards as the rest is.
+        self.gimg = {} if geometry_sparse else None
+        if geometry_sparse:
+            from . import _lib
+            self.P.set_option(_lib.APIRL_OPT_SPARSE_IMAGE, _lib.APIRL_SPARSE_GEOMETRY)
 
     def zeros_image(self):
         return self.torch.zeros(self.ig.n_voxels, dtype=self.torch.float32, device=self.dev)
@@ -119,8 +126,16 @@ class GpuShard:
             vals = m.contiguous().view(-1)
         self.P.backproject(vals, out, s, self.nsub, stream=self.stream)
 
+    def geometry_image(self, s):
+        if s not in self.gimg:
+            img = self.zeros_image()
+            self.P.backproject_ones(img, s, self.nsub, stream=self.stream)
+            self.gimg[s] = img
+        return self.gimg[s]
+
     def em_pass(self, x, bp, s, lik):
-        self.P.em_project_backproject(self.counts, x, bp, s, self.nsub, lik=lik, stream=self.stream)
+        zimg = self.geometry_image(s) if self.gimg is not None else None
+        self.P.em_project_backproject(self.counts, x, bp, s, self.nsub, lik=lik, stream=self.stream, zimg=zimg)
 
     def force_positive(self, img):
         from .projector import force_positive

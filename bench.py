@@ -228,17 +228,23 @@ def run_sharded(args):
     w = setup_workload(dev, log)
     ig, sg = w["ig"], w["sg"]
     first, n = shard_ranges(sg.n_sinos, world)[rank]
-    backend = GpuShard(ig, sg, w["counts"], NSUB, first, n, device=local, mult=w["atten"], ge=UPDATE_GE)
+    nonzero = args.pass_form == "nonzero"
+    backend = GpuShard(ig, sg, w["counts"], NSUB, first, n, device=local, mult=w["atten"], ge=UPDATE_GE,
+                       geometry_sparse=nonzero)
     backend.P.set_option(_l.APIRL_OPT_KERNEL_TIMING, 1)
     job = ShardedOsem(backend, NSUB, dist if world > 1 else None)
     job.compute_sensitivity()
+    if nonzero:
+        for s_ in range(NSUB):
+            backend.geometry_image(s_)  # the shard's G_s, at set-up like the sensitivity images
     # algorithmic bytes of the fused kernel on this rank's shard, per subset
     cv = w["counts"].view(torch.int32).view(sg.n_sinos, sg.n_proj, sg.n_r)[first:first + n]
     shard_bytes = []
     for s_ in range(NSUB):
         st = backend.P.count_steps(s_, NSUB).view(n, -1, sg.n_r).long()
         fwd, bwd = int(st.sum().item()), int(st[cv[:, s_::NSUB, :] != 0].sum().item())
-        shard_bytes.append(4 * fwd + 8 * bwd + 4 * st.numel())
+        shard_bytes.append(4 * (bwd if nonzero else fwd) + 8 * bwd + 4 * st.numel()
+                           + (8 * ig.n_voxels if nonzero else 0))
     x = torch.ones(ig.n_voxels, dtype=torch.float32, device=dev)
     flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.float32, device=dev)
     for i in range(args.warmup):
@@ -278,12 +284,14 @@ def run_sharded(args):
                        "parallelism": f"LOR shards x{world} (sinograms {first}..{first + n - 1} on rank 0), "
                                       "NCCL all-reduce of the backprojection image and likelihood",
                        "l2": "flushed between timed steps (256 MB write outside the timed events)",
+                       "pass": ("nonzero: each shard walks its bins with counts, its likelihood part from its "
+                                "geometry images A_s^T 1 (set-up)") if nonzero else "full: every bin walked",
                        "update": "x*bp/sens where sens > 0"},
             "roofline": {"bound": "hbm", "kernel": "k_em_pass on rank 0's shard",
                          "kernel_ms": statistics.mean(kern), "peak": peak, "unit": "GB/s",
                          "peak_source": f"{peak_kind} hbm_gbs",
                          "achieved": achieved, "frac": achieved / peak, "traffic": None},
-            "e2e": None, "cpu_baseline": None, "gpu_launches": 5 * args.steps, "clocks": clock,
+            "e2e": None, "cpu_baseline": None, "gpu_launches": (9 if nonzero else 5) * args.steps, "clocks": clock,
         }
         print(json.dumps(line), flush=True)
     if world > 1:

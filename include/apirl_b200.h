@@ -331,6 +331,16 @@ apirl_status apirl_em_project_backproject(apirl_projector* p, const void* d_coun
                                           int counts_packed, const float* d_add, const float* d_x, float* d_bp,
                                           int subset, int nsubsets, double* d_lik, void* stream);
 
+/* apirl_em_project_backproject as the sparse pass (d_zimg, *d_zero_add as
+ * for apirl_em_pass_sparse, per APIRL_OPT_SPARSE_IMAGE): only bins with counts
+ * are walked.  For LOR shards, whose backprojections and likelihoods are
+ * summed over the shards before the update (each shard with its own Z_s or
+ * G_s). */
+apirl_status apirl_em_project_backproject_sparse(apirl_projector* p, const void* d_counts, int counts_dtype,
+                                                 int counts_packed, const float* d_add, const float* d_x, float* d_bp,
+                                                 const float* d_zimg, const double* d_zero_add, int subset,
+                                                 int nsubsets, double* d_lik, void* stream);
+
 /* The same pass with HOST inputs and outputs: copies this pass's subset
  * counts (packed, from pinned or pageable host memory) to the device, runs
  * apirl_em_pass on the projector's resident image / sensitivity buffers, and

@@ -98,3 +98,30 @@ def test_sharded_osem_one_rank_equals_driver(oracle):
     # the driver (no multiplicative or additive term) takes the geometry-image
     # pass, whose likelihood sums the same terms in another order
     assert np.allclose(liks, want_lik[:-1], rtol=1e-7)
+
+
+def test_geometry_sparse_shards_sum_to_whole_pass(oracle):
+    """Shards taking the geometry-image sparse pass (each with its own
+    G_s = A_s^T 1): their backprojections and likelihoods sum to the whole
+    full pass's."""
+    ig, sg = geometry()
+    rng = np.random.default_rng(12)
+    x0 = (rng.random(ig.n_voxels, dtype=np.float32) + 0.5).astype(np.float32)
+    counts = t(rng.poisson(oracle.project_3d(sg, ig, x0) * 0.5).astype(np.uint32))
+    sub, ns = 1, 5
+    P = ap.SiddonProjector(ig, sg)
+    bp_full = torch.zeros(ig.n_voxels, dtype=torch.float32, device=DEV)
+    lik_full = torch.zeros(1, dtype=torch.float64, device=DEV)
+    P.em_project_backproject(counts, t(x0), bp_full, sub, ns, lik=lik_full)
+    bp_sum = torch.zeros_like(bp_full)
+    lik_sum = 0.0
+    for first, n in shard_ranges(sg.n_sinos, 3):
+        b = GpuShard(ig, sg, counts, ns, first, n, geometry_sparse=True)
+        bp = b.zeros_image()
+        lik = b.scalar()
+        b.em_pass(t(x0), bp, sub, lik)
+        bp_sum += bp
+        lik_sum += lik.item()
+    torch.cuda.synchronize()
+    assert rel(bp_sum.cpu().numpy(), bp_full.cpu().numpy()) <= 1e-6
+    assert abs(lik_sum - lik_full.item()) <= 1e-6 * abs(lik_full.item())
