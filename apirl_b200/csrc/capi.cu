@@ -308,6 +308,8 @@ void apirl_projector_destroy(apirl_projector* p) {
   cudaFree(p->d_minmax);
   cudaFree(p->d_scalars);
   cudaFree(p->d_chunk);
+  cudaFree(p->pad2.bA);
+  cudaFree(p->pad2.bT);
   cudaFree(p->nz.list);
   cudaFree(p->nz.tiles);
   cudaFree(p->nz.n_list);
@@ -907,6 +909,8 @@ namespace apirl {
 apirl_status prepare_nz_list(apirl_projector* p, int64_t total) {
   if (total <= p->nz.cap || !p->is3d) return APIRL_OK;
   DEVICE_SCOPE(p->device);
+  cudaFree(p->pad2.bA);
+  cudaFree(p->pad2.bT);
   cudaFree(p->nz.list);
   cudaFree(p->nz.tiles);
   p->nz.list = nullptr;
@@ -926,6 +930,27 @@ cudaError_t backproject_sino(apirl_projector* p, SubsetSel ss, const float* vin,
                              cudaStream_t st) {
   if (use_dual(p)) return launch_backproject_pad(p->g, p->t, ss, vin, vin_mode, img, p->pad, p->d_chunk, st);
   return launch_backproject(p->g, p->t, ss, vin, vin_mode, nullptr, 0, img, st, p->pg);
+}
+}  // namespace apirl
+
+namespace apirl {
+apirl_status backproject_sino_and_ones(apirl_projector* p, SubsetSel ss, const float* vin, int vin_mode, float* img,
+                                       float* gimg, cudaStream_t st) {
+  if (!use_dual(p)) {
+    CK(launch_backproject(p->g, p->t, ss, vin, vin_mode, nullptr, 0, img, st, p->pg));
+    CK(launch_backproject(p->g, p->t, ss, nullptr, 2, nullptr, 0, gimg, st, p->pg));
+    return APIRL_OK;
+  }
+  if (!p->pad2.bA) {
+    const size_t pv = (size_t)p->pad.lim;
+    CK(cudaMalloc(&p->pad2.bA, pv * sizeof(float)));
+    CK(cudaMalloc(&p->pad2.bT, pv * sizeof(float)));
+    CK(cudaMemset(p->pad2.bA, 0, pv * sizeof(float)));
+    CK(cudaMemset(p->pad2.bT, 0, pv * sizeof(float)));
+    p->pad2.lim = p->pad.lim;
+  }
+  CK(launch_backproject_pad(p->g, p->t, ss, vin, vin_mode, img, p->pad, p->d_chunk, st, gimg, p->pad2));
+  return APIRL_OK;
 }
 }  // namespace apirl
 

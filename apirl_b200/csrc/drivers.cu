@@ -93,6 +93,14 @@ bool use_geometry_sparse(const apirl_projector* p, const float* h_mult, const fl
   return !h_mult && !h_add && !h_sens_in && p->is3d && !p->t.lor_s && !p->pg.enabled;
 }
 
+// With a multiplicative term (and no additive one), the sensitivity A_s^T a
+// and the geometry image G_s = A_s^T 1 come out of one set of walks
+// (apirl::backproject_sino_and_ones): the passes are then the geometry sparse
+// pass with G_s beside the sensitivity.
+bool use_geometry_mult(const apirl_projector* p, const float* h_mult, const float* h_add, const float* h_sens_in) {
+  return h_mult && !h_add && !h_sens_in && p->is3d && !p->t.lor_s && !p->pg.enabled;
+}
+
 // Zero-count images and their additive sums of `nsub` subsets of d_meas.
 apirl_status zero_images(Res& r, apirl_projector* p, const float* d_meas, const float* d_add, int nsub, int n_proj,
                          float* d_zimg, double* d_zero_add) {
@@ -180,6 +188,11 @@ apirl_status osem_3d(const apirl_image_geom* img, const apirl_sino3d_geom* sino,
   DK(cudaMemcpyAsync(d_x, h_init, nv * sizeof(float), cudaMemcpyHostToDevice, r.st));
   DK(cudaMemsetAsync(d_bp, 0, nv * sizeof(float), r.st));
   DK(cudaMemsetAsync(d_sens, 0, nv * nsubsets * sizeof(float), r.st));
+  float* d_geom = nullptr;
+  if (use_geometry_mult(p, h_mult, h_add, h_sens_in)) {
+    DK(r.alloc(&d_geom, nv * nsubsets));
+    DK(cudaMemsetAsync(d_geom, 0, nv * nsubsets * sizeof(float), r.st));
+  }
   // Per-subset sensitivity: A_s^T (mult or 1), or the given images, then
   // forcePositive (OsemSinogram3d.cpp:84-116, :327-346).
   for (int s = 0; s < nsubsets; s++) {
@@ -188,15 +201,18 @@ apirl_status osem_3d(const apirl_image_geom* img, const apirl_sino3d_geom* sino,
     } else {
       SubsetSel ss;
       ss.subset = s; ss.nsub = nsubsets; ss.nk = apirl::subset_nproj(sino->n_proj, s, nsubsets);
-      DK(apirl::backproject_sino(p, ss, d_mult, d_mult ? 1 : 2, d_sens + nv * s, r.st));
+      if (d_geom)
+        DS(apirl::backproject_sino_and_ones(p, ss, d_mult, 1, d_sens + nv * s, d_geom + nv * s, r.st));
+      else
+        DK(apirl::backproject_sino(p, ss, d_mult, d_mult ? 1 : 2, d_sens + nv * s, r.st));
     }
     DK(apirl::launch_force_positive(nv, d_sens + nv * s, r.st));
   }
   float* d_zimg = nullptr;
   double* d_zadd = nullptr;
-  if (use_geometry_sparse(p, h_mult, h_add, h_sens_in)) {
+  if (use_geometry_sparse(p, h_mult, h_add, h_sens_in) || d_geom) {
     DS(apirl_projector_set_option(p, APIRL_OPT_SPARSE_IMAGE, APIRL_SPARSE_GEOMETRY));
-    d_zimg = d_sens;
+    d_zimg = d_geom ? d_geom : d_sens;
   } else if (use_sparse(p, iters)) {
     DK(r.alloc(&d_zimg, nv * nsubsets));
     DK(r.alloc(&d_zadd, nsubsets));
@@ -269,17 +285,24 @@ apirl_status mlem_3d(const apirl_image_geom* img, const apirl_sino3d_geom* sino,
   SubsetSel all;
   all.subset = -1; all.nsub = 1; all.nk = sino->n_proj;
   // Sensitivity A^T (mult or 1), or the given image (MlemSinogram3d.cpp:132-151).
+  float* d_geom = nullptr;
+  if (use_geometry_mult(p, h_mult, h_add, h_sens_in)) {
+    DK(r.alloc(&d_geom, nv));
+    DK(cudaMemsetAsync(d_geom, 0, nv * sizeof(float), r.st));
+  }
   if (h_sens_in)
     DK(cudaMemcpyAsync(d_sens, h_sens_in, nv * sizeof(float), cudaMemcpyHostToDevice, r.st));
+  else if (d_geom)
+    DS(apirl::backproject_sino_and_ones(p, all, d_mult, 1, d_sens, d_geom, r.st));
   else
     DK(apirl::backproject_sino(p, all, d_mult, d_mult ? 1 : 2, d_sens, r.st));
   DS(apirl_mlem_threshold(nv, d_sens, d_thr, r.st));
   double* d_slot = d_lik + iters + 1;
   float* d_zimg = nullptr;
   double* d_zadd = nullptr;
-  if (use_geometry_sparse(p, h_mult, h_add, h_sens_in)) {
+  if (use_geometry_sparse(p, h_mult, h_add, h_sens_in) || d_geom) {
     DS(apirl_projector_set_option(p, APIRL_OPT_SPARSE_IMAGE, APIRL_SPARSE_GEOMETRY));
-    d_zimg = d_sens;
+    d_zimg = d_geom ? d_geom : d_sens;
   } else if (use_sparse(p, iters)) {
     DK(r.alloc(&d_zimg, nv));
     DK(r.alloc(&d_zadd, 1));

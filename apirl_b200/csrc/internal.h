@@ -139,8 +139,10 @@ cudaError_t launch_pad_reduce(const ImgGeom& g, const PadBuffers& pad, int mode,
 // 3D backprojection img += A^T v through the padded pair (3D float walk, one
 // ray per bin): a persistent scatter, then k_pad_reduce folds the pair into
 // img and clears it.  `counter` is the projector's chunk counter.
+// img2 / pad2 (its bA, bT) set: the same walks also give img2 += A_s^T 1.
 cudaError_t launch_backproject_pad(const ImgGeom& g, const LorTable& t, SubsetSel s, const float* vin, int vin_mode,
-                                   float* img, const PadBuffers& pad, unsigned long long* counter, cudaStream_t st);
+                                   float* img, const PadBuffers& pad, unsigned long long* counter, cudaStream_t st,
+                                   float* img2 = nullptr, const PadBuffers& pad2 = PadBuffers());
 cudaError_t launch_inverse_divide(int64_t n, const float* meas, float* est, cudaStream_t st);
 cudaError_t launch_add_bins(int64_t n, const float* add, float* est, cudaStream_t st);
 cudaError_t launch_likelihood(int64_t n, const float* est, const float* meas, int gt0, double* partials,
@@ -227,6 +229,7 @@ struct apirl_projector {
   unsigned long long* d_chunk = nullptr;  // chunk counter of the persistent pass
   int sparse_image = 0;          // APIRL_OPT_SPARSE_IMAGE: 0 = zero-count image Z_s, 1 = geometry image G_s
   apirl::NzList nz;              // list of a subset's bins with counts (sparse passes), grown on demand
+  apirl::PadBuffers pad2;        // second padded backprojection pair (bA, bT only), on first use
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
   // Counts staged ahead of apirl_em_pass_host (apirl_stage_counts): copied on
   // copy_stream; each slot's event is recorded after its copy.
@@ -262,5 +265,10 @@ apirl_status prepare_nz_list(apirl_projector* p, int64_t total);
 // projector has it (launch_backproject_pad), else launch_backproject.
 cudaError_t backproject_sino(apirl_projector* p, SubsetSel ss, const float* vin, int vin_mode, float* img,
                              cudaStream_t st);
+// img += A_s^T v and gimg += A_s^T 1 along one set of walks (a second padded
+// backprojection pair, allocated on first use); two backprojections when the
+// projector has no padded layout.
+apirl_status backproject_sino_and_ones(apirl_projector* p, SubsetSel ss, const float* vin, int vin_mode, float* img,
+                                       float* gimg, cudaStream_t st);
 }  // namespace apirl
 

@@ -451,9 +451,11 @@ __global__ void __launch_bounds__(kBlock) k_em_pass_rays(ImgGeom g, LorTable t, 
 // into the image.  v is the bin's value (vin_mode as load_bin); bins with
 // v == 0 are not walked, as SiddonProjector::Backproject skips them
 // (SiddonProjector.cpp:496).
+// b2A / b2T set: the walk also scatters seg into that second padded pair,
+// for every bin (the unweighted image A_s^T 1 beside A_s^T v).
 __global__ void __launch_bounds__(kBlock, kPersistMinBlocks) k_scatter_persist(
     ImgGeom g, LorTable t, SubsetSel s, const float* __restrict__ vin, int vin_mode, PadBuffers pad, int64_t total,
-    unsigned long long* __restrict__ chunk_counter) {
+    unsigned long long* __restrict__ chunk_counter, float* __restrict__ b2A, float* __restrict__ b2T) {
   const int lane = threadIdx.x & 31;
   const int64_t nchunks = (total + 31) >> 5;
   const int px = g.nx + 2 * kPad, py = g.ny + 2 * kPad;
@@ -467,14 +469,17 @@ __global__ void __launch_bounds__(kBlock, kPersistMinBlocks) k_scatter_persist(
     if (b < total) {
       const BinPos p = decode(b, t, s);
       const float v = load_bin(vin, vin_mode, b, p, t);
-      if (v != 0.f) {
+      if (v != 0.f || b2A) {
         const float4 L = t.lor[(int64_t)p.a * t.n_r + p.l];
         const float2 z = t.z[p.g];
         const float vx = A_SUB(L.z, L.x), vy = A_SUB(L.w, L.y);
         const bool tr = fabsf(vx) >= fabsf(vy);
         Walk3 w;
         siddon3_setup(L.x, L.y, z.x, vx, vy, A_SUB(z.y, z.x), g, w);
-        siddon3_scatter_pad(w, g, tr ? py : 1, tr ? 1 : px, uz, pad.lim, v, tr ? pad.bT : pad.bA);
+        if (b2A)
+          siddon3_scatter2_pad(w, g, tr ? py : 1, tr ? 1 : px, uz, pad.lim, v, tr ? pad.bT : pad.bA, tr ? b2T : b2A);
+        else
+          siddon3_scatter_pad(w, g, tr ? py : 1, tr ? 1 : px, uz, pad.lim, v, tr ? pad.bT : pad.bA);
       }
     }
   }
@@ -662,7 +667,10 @@ __global__ void k_sum_partials(const double* __restrict__ partials, int64_t n, d
 
 // out[b] = - (x . z over block b's contiguous chunk of voxels), FP64, fixed
 // order; block 0 also subtracts *zero_add (when given).  The negated
-// zero-count-bin estimates of the sparse pass.
+// zero-count-bin estimates of the sparse pass.  Voxels with z == 0 are
+// skipped: no walked bin reaches them, so an image value there (NaN where the
+// update divided 0 by a zero sensitivity, as the reference's >= 0 test lets
+// it) is in no estimate and stays out of the sum.
 __global__ void __launch_bounds__(kBlock) k_neg_dot(const float* __restrict__ x, const float* __restrict__ z,
                                                     int64_t n, const double* __restrict__ zero_add,
                                                     double* __restrict__ out) {
@@ -670,7 +678,10 @@ __global__ void __launch_bounds__(kBlock) k_neg_dot(const float* __restrict__ x,
   const int64_t lo = (int64_t)blockIdx.x * chunk;
   const int64_t hi = lo + chunk < n ? lo + chunk : n;
   double v = 0.0;
-  for (int64_t i = lo + threadIdx.x; i < hi; i += blockDim.x) v += (double)x[i] * (double)z[i];
+  for (int64_t i = lo + threadIdx.x; i < hi; i += blockDim.x) {
+    const float zi = z[i];
+    if (zi != 0.f) v += (double)x[i] * (double)zi;
+  }
   const double s = block_sum(v);
   if (threadIdx.x == 0) out[blockIdx.x] = -s - ((blockIdx.x == 0 && zero_add) ? *zero_add : 0.0);
 }
@@ -1135,7 +1146,8 @@ cudaError_t launch_backproject(const ImgGeom& g, const LorTable& t, SubsetSel s,
 }
 
 cudaError_t launch_backproject_pad(const ImgGeom& g, const LorTable& t, SubsetSel s, const float* vin, int vin_mode,
-                                   float* img, const PadBuffers& pad, unsigned long long* counter, cudaStream_t st) {
+                                   float* img, const PadBuffers& pad, unsigned long long* counter, cudaStream_t st,
+                                   float* img2, const PadBuffers& pad2) {
   const int64_t total = (int64_t)t.n_sinos * s.nk * t.n_r;
   if (total == 0) return cudaSuccess;
   int per_sm = 0, dev = 0, sms = 0;
@@ -1146,9 +1158,11 @@ cudaError_t launch_backproject_pad(const ImgGeom& g, const LorTable& t, SubsetSe
   const int64_t resident = (int64_t)(per_sm < 1 ? 1 : per_sm) * sms;
   const int64_t need = ((total + 31) / 32 * 32 + 127) / 128;
   if ((e = cudaMemsetAsync(counter, 0, sizeof(unsigned long long), st)) != cudaSuccess) return e;
-  k_scatter_persist<<<(unsigned)(need < resident ? need : resident), 128, 0, st>>>(g, t, s, vin, vin_mode, pad, total,
-                                                                                 counter);
+  const bool two = img2 && pad2.bA && pad2.bT;
+  k_scatter_persist<<<(unsigned)(need < resident ? need : resident), 128, 0, st>>>(
+      g, t, s, vin, vin_mode, pad, total, counter, two ? pad2.bA : nullptr, two ? pad2.bT : nullptr);
   if ((e = cudaGetLastError()) != cudaSuccess) return e;
+  if (two && (e = launch_pad_reduce(g, pad2, 1, nullptr, img2, nullptr, nullptr, 0.f, 0, st)) != cudaSuccess) return e;
   return launch_pad_reduce(g, pad, 1, nullptr, img, nullptr, nullptr, 0.f, 0, st);
 }
 

@@ -206,6 +206,31 @@ __device__ __forceinline__ void siddon3_scatter_pad(Walk3 w, const ImgGeom& g, i
   }
 }
 
+// siddon3_scatter_pad into two images of the same padded layout along one
+// walk: seg * r1 into img1 (skipped when r1 == 0) and seg into img2.
+__device__ __forceinline__ void siddon3_scatter2_pad(Walk3 w, const ImgGeom& g, int ux, int uy, int uz, unsigned lim,
+                                                     float r1, float* __restrict__ img1, float* __restrict__ img2) {
+  const int sx = w.iinc * ux, sy = w.jinc * uy, sz = w.kinc * uz;
+  int idx = (w.k + kPad) * uz + (w.j + kPad) * uy + (w.i + kPad) * ux;
+  const bool first = r1 != 0.f;
+  for (int m = 0; m < w.n; m++) {
+    bool cx, cy;
+    const float an = next_crossing(w, cx, cy);
+    const float seg = A_MUL(A_SUB(an, w.ac), w.L);
+    const bool inb = w.guarded || (((unsigned)w.i < (unsigned)g.nx) & ((unsigned)w.j < (unsigned)g.ny) &
+                                   ((unsigned)w.k < (unsigned)g.nz));
+    if (inb) {
+      const unsigned at = min((unsigned)idx, lim - 1u);
+      if (first) atomicAdd(img1 + at, A_MUL(seg, r1));
+      atomicAdd(img2 + at, seg);
+    }
+    w.ac = an;
+    if (cx) { w.i += w.iinc; idx += sx; w.ax = A_ADD(w.ax, w.axu); }
+    else if (cy) { w.j += w.jinc; idx += sy; w.ay = A_ADD(w.ay, w.ayu); }
+    else { w.k += w.kinc; idx += sz; w.az = A_ADD(w.az, w.azu); }
+  }
+}
+
 template <class V>
 __device__ __forceinline__ void siddon3_walk(Walk3 w, const ImgGeom& g, V&& visit) {
   const int sx = w.iinc, sy = w.jinc * g.nx, sz = w.kinc * g.nx * g.ny;

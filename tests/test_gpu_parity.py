@@ -402,6 +402,57 @@ def test_generate_acf_and_multiplicative_additive_osem(oracle):
     assert np.allclose(lik, olik.astype(np.float64), rtol=1e-4)
 
 
+def test_multiplicative_only_drivers_take_geometry_pass(oracle):
+    """With a multiplicative sinogram and no additive one, the drivers walk
+    the sensitivity A_s^T a and the geometry image A_s^T 1 together and then
+    run the geometry sparse pass: same sensitivities and reconstruction as the
+    oracle, and the same likelihood (1e-7 relative) as the full pass that
+    given sensitivities take."""
+    ig, sg = small_3d()
+    rng = np.random.default_rng(47)
+    mult = (rng.random(sg.n_bins, dtype=np.float32) * 0.7 + 0.3).astype(np.float32)
+    init = np.ones(ig.n_voxels, np.float32)
+    meas = G["s3_meas"]
+    assert (meas == 0).any() and (meas != 0).any()
+    img, lik, sens = ap.osem_3d(ig, sg, meas, init, 2, 4, mult=mult, all_sens=True)
+    o, olik, osens0 = oracle.osem_3d(sg, ig, init, meas, 2, 4, mult=mult)
+    assert rel(sens[0], osens0) <= 1e-5
+    assert rel(img, o) <= 1e-4
+    assert np.allclose(lik, olik.astype(np.float64), rtol=1e-4)
+    img2, lik2, _ = ap.osem_3d(ig, sg, meas, init, 2, 4, mult=mult, sens=sens)
+    assert rel(img, img2) <= 1e-5
+    assert np.allclose(lik, lik2, rtol=1e-7)
+    m, mlik, msens = ap.mlem_3d(ig, sg, meas, init, 3, mult=mult)
+    m2, mlik2, _ = ap.mlem_3d(ig, sg, meas, init, 3, mult=mult, sens=msens)
+    assert rel(m, m2) <= 1e-5
+    assert np.allclose(mlik, mlik2, rtol=1e-7)
+
+
+def test_sparse_likelihood_with_voxels_outside_every_ray(oracle):
+    """End slices of an image longer than the scanner's axial FOV have zero
+    sensitivity in every subset; the reference's >= 0 update turns them into
+    0/0 = NaN, which no ray reaches.  The sparse passes' image dot products
+    skip voxels of zero weight, so their likelihoods stay finite and equal the
+    full pass's and the oracle's."""
+    ig, sg = ImageGeom(48, 48, 13, 2.08, 2.08, 2.03), Sino3DGeom.span1(25, 48, 5, 72.0, 5 * 4.054, 150.0, 3)
+    rng = np.random.default_rng(53)
+    x0 = (rng.random(ig.n_voxels, dtype=np.float32) + 0.5).astype(np.float32)
+    meas = rng.poisson(oracle.project_3d(sg, ig, x0) * 0.5).astype(np.float32)
+    assert (meas == 0).any()
+    init = np.ones(ig.n_voxels, np.float32)
+    mult = (rng.random(sg.n_bins, dtype=np.float32) * 0.7 + 0.3).astype(np.float32)
+    for m in (None, mult):
+        img, lik, sens = ap.osem_3d(ig, sg, meas, init, 2, 4, mult=m, all_sens=True)
+        assert (sens[0] == 0).any() and np.isnan(img).any()
+        img2, lik2, _ = ap.osem_3d(ig, sg, meas, init, 2, 4, mult=m, sens=sens)
+        o, olik, _ = oracle.osem_3d(sg, ig, init, meas, 2, 4, mult=m)
+        assert np.all(np.isfinite(lik)) and np.allclose(lik, lik2, rtol=1e-7)
+        assert np.allclose(lik, olik.astype(np.float64), rtol=1e-4)
+        assert np.array_equal(np.isnan(img), np.isnan(o))
+        ok = ~np.isnan(o)
+        assert rel(img[ok], o[ok]) <= 1e-4
+
+
 def test_dual_layout_pass_equals_single_layout(oracle):
     """The transposed-copy walk (default) changes only the order of fp32
     additions in the backprojection; projections and the likelihood are
