@@ -113,6 +113,7 @@ SIGNATURES = {
     "apirl_em_pass_host_async": (_i, [_vp, _vp, _i, _vp, _vp, _vp, _vp, _vp, _vp, _f, _i, _i, _i, _vp, _vp, _vp]),
     "apirl_set_iteration_hook": (_i, [_vp, _i, _vp]),
     "apirl_backproject_ones": (_i, [_vp, _vp, _i, _i, _vp]),
+    "apirl_backproject_and_ones": (_i, [_vp, _vp, _vp, _vp, _i, _i, _vp]),
     "apirl_em_project_backproject_sparse": (_i, [_vp, _vp, _i, _i, _vp, _vp, _vp, _vp, _vp, _i, _i, _vp, _vp]),
     "apirl_osem_3d": (_i, [ctypes.POINTER(ImageGeomC), ctypes.POINTER(Sino3DGeomC), _vp, _vp, _vp, _vp, _i, _i,
                            _i, _vp, _vp, _vp, ctypes.POINTER(SamplingC)]),

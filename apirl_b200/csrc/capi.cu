@@ -487,6 +487,17 @@ apirl_status apirl_backproject_ones(apirl_projector* p, float* d_image, int subs
   return APIRL_OK;
 }
 
+apirl_status apirl_backproject_and_ones(apirl_projector* p, const float* d_sino, float* d_image, float* d_ones_image,
+                                        int subset, int nsubsets, void* stream) {
+  apirl_status st = check_subset(p, subset, nsubsets);
+  if (st) return st;
+  if (!d_image || !d_sino || !d_ones_image) return fail(APIRL_ERR_INVALID, "null image or sinogram");
+  if (d_image == d_ones_image) return fail(APIRL_ERR_INVALID, "the two images must differ");
+  DEVICE_SCOPE(p->device);
+  return apirl::backproject_sino_and_ones(p, make_subset(p, subset, nsubsets), d_sino, 0, d_image, d_ones_image,
+                                          (cudaStream_t)stream);
+}
+
 apirl_status apirl_divide_and_backproject(apirl_projector* p, const float* d_meas, const float* d_est,
                                           float* d_image, int subset, int nsubsets, void* stream) {
   apirl_status st = check_subset(p, subset, nsubsets);

@@ -156,6 +156,13 @@ class SiddonProjector:
         check(self.lib.apirl_backproject_ones(self.h, _ptr(image), subset, nsubsets, _stream(stream)))
         return image
 
+    def backproject_and_ones(self, sino, image, ones_image, subset=-1, nsubsets=1, stream=None):
+        """image += A_s^T sino and ones_image += A_s^T 1 along one set of walks
+        (a sensitivity with a multiplicative sinogram and G_s together)."""
+        check(self.lib.apirl_backproject_and_ones(self.h, _ptr(sino), _ptr(image), _ptr(ones_image), subset, nsubsets,
+                                                  _stream(stream)))
+        return image, ones_image
+
     def backproject(self, sino, image, subset=-1, nsubsets=1, stream=None):
         """image += A^T sino."""
         check(self.lib.apirl_backproject(self.h, _ptr(sino), _ptr(image), subset, nsubsets, _stream(stream)))

@@ -230,6 +230,13 @@ apirl_status apirl_backproject(apirl_projector* p, const float* d_sino, float* d
  * setMultiplicativeProjection), and the geometry image G_s of the sparse pass
  * (APIRL_SPARSE_GEOMETRY).  Needs no sinogram buffer. */
 apirl_status apirl_backproject_ones(apirl_projector* p, float* d_image, int subset, int nsubsets, void* stream);
+/* apirl_backproject and apirl_backproject_ones along one set of walks:
+ * d_image += A^T d_sino and d_ones_image += A^T 1 (the sensitivity image with
+ * a multiplicative sinogram, OsemSinogram3d.cpp:327-346, and the geometry
+ * image G_s of the sparse pass, for the price of about one backprojection on
+ * the 3D padded layout).  The images must be distinct. */
+apirl_status apirl_backproject_and_ones(apirl_projector* p, const float* d_sino, float* d_image, float* d_ones_image,
+                                        int subset, int nsubsets, void* stream);
 /* SiddonProjector::DivideAndBackproject: d_image += A^T (d_meas / d_est)
  * (:571-704 for 3D, :90-144 for 2D, with each reference's zero rules). */
 apirl_status apirl_divide_and_backproject(apirl_projector* p, const float* d_meas, const float* d_est,

@@ -656,6 +656,12 @@ def test_nonzero_pass_with_geometry_image(oracle, dual, persistent):
     P.backproject_ones(gimg, subset, ns)
     ones = np.ones(sg.subset_bins(subset, ns), np.float32)
     assert rel(gimg.cpu().numpy(), oracle.backproject_3d(sg, ig, ones, subset, ns)) <= 1e-5
+    v = np.random.default_rng(79).random(ones.size, dtype=np.float32)
+    vimg = torch.zeros(ig.n_voxels, dtype=torch.float32, device=DEV)
+    g2 = torch.zeros(ig.n_voxels, dtype=torch.float32, device=DEV)
+    P.backproject_and_ones(t(v), vimg, g2, subset, ns)
+    assert rel(vimg.cpu().numpy(), oracle.backproject_3d(sg, ig, v, subset, ns)) <= 1e-5
+    assert rel(g2.cpu().numpy(), gimg.cpu().numpy()) <= 1e-6
     add_sub = add.reshape(sg.n_sinos, sg.n_proj, sg.n_r)[:, subset::ns, :].reshape(-1)
     for use_add in (False, True):
         a = t(add) if use_add else None
