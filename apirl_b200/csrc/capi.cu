@@ -947,9 +947,12 @@ cudaError_t backproject_sino(apirl_projector* p, SubsetSel ss, const float* vin,
 namespace apirl {
 apirl_status backproject_sino_and_ones(apirl_projector* p, SubsetSel ss, const float* vin, int vin_mode, float* img,
                                        float* gimg, cudaStream_t st) {
-  if (!use_dual(p)) {
-    CK(launch_backproject(p->g, p->t, ss, vin, vin_mode, nullptr, 0, img, st, p->pg));
-    CK(launch_backproject(p->g, p->t, ss, nullptr, 2, nullptr, 0, gimg, st, p->pg));
+  // Sinogram shards (apirl_projector_set_shard) take the two backprojections
+  // one after the other: the one-walk form is verified on whole sinograms.
+  const bool shard = p->t.g0 != 0 || p->t.n_sinos != p->host.n_sinos;
+  if (!use_dual(p) || shard) {
+    CK(backproject_sino(p, ss, vin, vin_mode, img, st));
+    CK(backproject_sino(p, ss, nullptr, 2, gimg, st));
     return APIRL_OK;
   }
   if (!p->pad2.bA) {
