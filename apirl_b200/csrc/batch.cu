@@ -248,6 +248,7 @@ apirl_status apirl_batch_step(apirl_batch* b, int* n_active, int* n_queued) {
   cudaGetDevice(&prev);
   BK(cudaSetDevice(b->device));
   struct Restore { int d; ~Restore() { cudaSetDevice(d); } } restore{prev};
+  if (apirl_status pend = apirl_internal_pending()) return pend;
   // 1. admission: in order, smaller jobs may pass one that does not fit.
   for (auto it = b->queue.begin(); it != b->queue.end();) {
     if (b->used + (*it)->footprint <= b->budget) {

@@ -27,6 +27,21 @@ apirl_status apirl_internal_fail(apirl_status code, const char* msg) {
   return code;
 }
 
+// A CUDA error left pending by an earlier launch (this library's or the
+// caller's) is reported by the next entry point instead of being discarded:
+// that call returns APIRL_ERR_CUDA naming the error and does no work.
+// Reading the error resets a non-sticky one, as cudaGetLastError() does for
+// any caller, so the call after it runs normally.
+apirl_status apirl_internal_pending(void) {
+  const cudaError_t e = cudaGetLastError();
+  if (e == cudaSuccess) return APIRL_OK;
+  char buf[384];
+  snprintf(buf, sizeof buf, "a CUDA error was pending before this call (left by an earlier launch): %s: %s",
+           cudaGetErrorName(e), cudaGetErrorString(e));
+  g_err = buf;
+  return e == cudaErrorMemoryAllocation ? APIRL_ERR_OOM : APIRL_ERR_CUDA;
+}
+
 namespace {
 
 apirl_status fail(apirl_status code, const char* fmt, ...) {
@@ -64,12 +79,17 @@ struct DeviceScope {
   }
 };
 
-// Also clears a launch error left by an earlier, unrelated call, so that the
-// cudaGetLastError() after each of our launches reports that launch only.
-#define DEVICE_SCOPE(dev)                                                   \
-  DeviceScope scope_(dev);                                                  \
+// Also refuses to run over an error pending from an earlier launch
+// (apirl_internal_pending), so that the cudaGetLastError() after each of our
+// launches reports that launch only.
+#define DEVICE_SCOPE(dev)                                                       \
+  DeviceScope scope_(dev);                                                      \
   if (scope_.err != cudaSuccess) return cuda_fail(scope_.err, "cudaSetDevice"); \
-  (void)cudaGetLastError()
+  if (apirl_status pend_ = apirl_internal_pending()) return pend_
+#define NO_PENDING()                                         \
+  do {                                                       \
+    if (apirl_status pend_ = apirl_internal_pending()) return pend_; \
+  } while (0)
 
 bool valid_img(const apirl_image_geom* g) {
   return g && g->nx > 0 && g->ny > 0 && g->nz > 0 && g->dx > 0 && g->dy > 0 && g->dz > 0 &&
@@ -525,14 +545,14 @@ apirl_status apirl_generate_acf(apirl_projector* p, const float* d_mu, float* d_
 
 apirl_status apirl_inverse_divide(int64_t n, const float* d_meas, float* d_est, void* stream) {
   if (n < 0 || (n > 0 && (!d_meas || !d_est))) return fail(APIRL_ERR_INVALID, "bad arguments");
-  (void)cudaGetLastError();  // clear an unrelated earlier launch error
+  NO_PENDING();
   CK(apirl::launch_inverse_divide(n, d_meas, d_est, (cudaStream_t)stream));
   return APIRL_OK;
 }
 
 apirl_status apirl_add_bins(int64_t n, const float* d_add, float* d_est, void* stream) {
   if (n < 0 || (n > 0 && (!d_add || !d_est))) return fail(APIRL_ERR_INVALID, "bad arguments");
-  (void)cudaGetLastError();  // clear an unrelated earlier launch error
+  NO_PENDING();
   CK(apirl::launch_add_bins(n, d_add, d_est, (cudaStream_t)stream));
   return APIRL_OK;
 }
@@ -540,7 +560,7 @@ apirl_status apirl_add_bins(int64_t n, const float* d_add, float* d_est, void* s
 apirl_status apirl_likelihood(int64_t n, const float* d_est, const float* d_meas, int gt0, double* d_out,
                               void* stream) {
   if (n <= 0 || !d_est || !d_meas || !d_out) return fail(APIRL_ERR_INVALID, "bad arguments");
-  (void)cudaGetLastError();  // clear an unrelated earlier launch error
+  NO_PENDING();
   // The per-block partials live in a small allocation owned by this call path.
   const int64_t nb = apirl::likelihood_blocks(n);
   double* part = nullptr;
@@ -553,7 +573,7 @@ apirl_status apirl_likelihood(int64_t n, const float* d_est, const float* d_meas
 
 apirl_status apirl_mlem_threshold(int64_t n, const float* d_sens, float* d_thr, void* stream) {
   if (n <= 0 || !d_sens || !d_thr) return fail(APIRL_ERR_INVALID, "bad arguments");
-  (void)cudaGetLastError();  // clear an unrelated earlier launch error
+  NO_PENDING();
   unsigned* mm = nullptr;
   CK(cudaMallocAsync(&mm, 2 * sizeof(unsigned), (cudaStream_t)stream));
   cudaError_t e = apirl::launch_threshold(n, d_sens, mm, d_thr, (cudaStream_t)stream);
@@ -565,14 +585,14 @@ apirl_status apirl_mlem_threshold(int64_t n, const float* d_sens, float* d_thr, 
 apirl_status apirl_update_pixels(int64_t n, float* d_x, float* d_bp, const float* d_sens, const float* d_thr,
                                  float thr_value, int ge, int zero_bp, void* stream) {
   if (n < 0 || (n > 0 && (!d_x || !d_bp || !d_sens))) return fail(APIRL_ERR_INVALID, "bad arguments");
-  (void)cudaGetLastError();  // clear an unrelated earlier launch error
+  NO_PENDING();
   CK(apirl::launch_update(n, d_x, d_bp, d_sens, d_thr, thr_value, ge, zero_bp, (cudaStream_t)stream));
   return APIRL_OK;
 }
 
 apirl_status apirl_force_positive(int64_t n, float* d_x, void* stream) {
   if (n < 0 || (n > 0 && !d_x)) return fail(APIRL_ERR_INVALID, "bad arguments");
-  (void)cudaGetLastError();  // clear an unrelated earlier launch error
+  NO_PENDING();
   CK(apirl::launch_force_positive(n, d_x, (cudaStream_t)stream));
   return APIRL_OK;
 }
@@ -920,8 +940,6 @@ namespace apirl {
 apirl_status prepare_nz_list(apirl_projector* p, int64_t total) {
   if (total <= p->nz.cap || !p->is3d) return APIRL_OK;
   DEVICE_SCOPE(p->device);
-  cudaFree(p->pad2.bA);
-  cudaFree(p->pad2.bT);
   cudaFree(p->nz.list);
   cudaFree(p->nz.tiles);
   p->nz.list = nullptr;
@@ -947,10 +965,7 @@ cudaError_t backproject_sino(apirl_projector* p, SubsetSel ss, const float* vin,
 namespace apirl {
 apirl_status backproject_sino_and_ones(apirl_projector* p, SubsetSel ss, const float* vin, int vin_mode, float* img,
                                        float* gimg, cudaStream_t st) {
-  // Sinogram shards (apirl_projector_set_shard) take the two backprojections
-  // one after the other: the one-walk form is verified on whole sinograms.
-  const bool shard = p->t.g0 != 0 || p->t.n_sinos != p->host.n_sinos;
-  if (!use_dual(p) || shard) {
+  if (!use_dual(p)) {
     CK(backproject_sino(p, ss, vin, vin_mode, img, st));
     CK(backproject_sino(p, ss, nullptr, 2, gimg, st));
     return APIRL_OK;

@@ -256,6 +256,9 @@ struct apirl_projector {
 
 // Records `msg` as the calling thread's last error and returns `code`.
 apirl_status apirl_internal_fail(apirl_status code, const char* msg);
+// APIRL_OK, or APIRL_ERR_CUDA (with the last-error message set) when a CUDA
+// error was pending from an earlier launch; reading it resets a non-sticky one.
+apirl_status apirl_internal_pending(void);
 
 namespace apirl {
 // Room in p->nz for the list of `total` bins (cudaMalloc: call outside graph

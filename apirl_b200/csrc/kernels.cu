@@ -1029,15 +1029,21 @@ inline unsigned grid_for(int64_t total) { return (unsigned)((total + kBlock - 1)
 // The fused 3D kernels use no shared memory: give the SM's unified L1 /
 // shared storage to L1.  Set once per device (function attributes belong to
 // the device's context).
-void prefer_l1() {
+cudaError_t prefer_l1() {
   static std::atomic<int> done[64];
   int dev = 0;
-  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return;
-  if (done[dev].exchange(1)) return;
-  cudaFuncSetAttribute(k_em_pass<float, true, false>, cudaFuncAttributePreferredSharedMemoryCarveout, 0);
-  cudaFuncSetAttribute(k_em_pass<uint32_t, true, false>, cudaFuncAttributePreferredSharedMemoryCarveout, 0);
-  cudaFuncSetAttribute(k_em_pass<uint16_t, true, false>, cudaFuncAttributePreferredSharedMemoryCarveout, 0);
-  (void)cudaGetLastError();
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return e;
+  if (dev < 0 || dev >= 64 || done[dev].load()) return cudaSuccess;
+  if ((e = cudaFuncSetAttribute(k_em_pass<float, true, false>, cudaFuncAttributePreferredSharedMemoryCarveout, 0)) !=
+          cudaSuccess ||
+      (e = cudaFuncSetAttribute(k_em_pass<uint32_t, true, false>, cudaFuncAttributePreferredSharedMemoryCarveout,
+                                0)) != cudaSuccess ||
+      (e = cudaFuncSetAttribute(k_em_pass<uint16_t, true, false>, cudaFuncAttributePreferredSharedMemoryCarveout,
+                                0)) != cudaSuccess)
+    return e;
+  done[dev].store(1);
+  return cudaSuccess;
 }
 
 // The persistent kernel's carveout: the shared memory that its resident
@@ -1204,7 +1210,7 @@ cudaError_t launch_em_pass(const ImgGeom& g, const LorTable& t, SubsetSel s, con
                                                            total, 0);                                         \
   } while (0)
   if (persist_counter && t.is3d && !t.lor_s && !pg.enabled && pad.pA && lik_mode == 0) {
-    prefer_l1();
+    if (cudaError_t le = prefer_l1()) return le;
     // Persistent form: as many blocks of this size as fit on the current
     // device's SMs at once (a host-side query of a few microseconds).
     // Sparse passes walk a list of the subset's bins with counts when the
@@ -1299,7 +1305,7 @@ cudaError_t launch_em_pass(const ImgGeom& g, const LorTable& t, SubsetSel s, con
     }
     return launch_sum(partials, np, lik, st);
   }
-  prefer_l1();
+  if (cudaError_t le = prefer_l1()) return le;
   switch (counts_dtype) {
     case APIRL_F32: APIRL_EM(float); break;
     case APIRL_U32: APIRL_EM(uint32_t); break;

@@ -117,6 +117,7 @@ extern "C" apirl_status apirl_likelihood_noalloc(int64_t n, const float* d_est, 
              "(use apirl_likelihood)", (long long)n, (long long)APIRL_LIKELIHOOD_NOALLOC_MAX_BINS);
     return apirl_internal_fail(APIRL_ERR_INVALID, buf);
   }
+  if (apirl_status pend = apirl_internal_pending()) return pend;
   double* scratch = nullptr;
   apirl_status st = scratch_for_current_device(&scratch);
   if (st != APIRL_OK) return st;
