@@ -155,7 +155,7 @@ namespace {
 apirl_status osem_3d(const apirl_image_geom* img, const apirl_sino3d_geom* sino, const float* h_meas,
                      const float* h_mult, const float* h_add, const float* h_init, int iters, int nsubsets,
                      int device, float* h_out, double* h_lik, const float* h_sens_in, float* h_sens_out,
-                     int n_sens_out, const apirl_sampling* sampling) {
+                     int n_sens_out, const apirl_sampling* sampling, int update_positive_sens = 0) {
   if (!h_meas || !h_init || !h_out || iters < 0 || nsubsets <= 0)
     return set_err(APIRL_ERR_INVALID, "apirl_osem_3d arguments", cudaSuccess);
   Res r;
@@ -222,7 +222,8 @@ apirl_status osem_3d(const apirl_image_geom* img, const apirl_sino3d_geom* sino,
   // captured (subset 0 has the most angles).
   if (d_zimg) DS(apirl::prepare_nz_list(p, apirl_projector_num_bins(p, nsubsets > 1 ? 0 : -1, nsubsets)));
   for (int s = 0; s < nsubsets; s++)
-    DS(capture_pass(r, p, d_meas, d_add, d_x, d_bp, d_sens + nv * s, nullptr, 0.f, 1, s, nsubsets, d_slot + s,
+    DS(capture_pass(r, p, d_meas, d_add, d_x, d_bp, d_sens + nv * s, nullptr, 0.f, update_positive_sens ? 0 : 1, s,
+                    nsubsets, d_slot + s,
                     d_zimg ? d_zimg + nv * s : nullptr, d_zadd ? d_zadd + s : nullptr));
   std::vector<float> h_tmp;
   for (int t = 0; t < iters; t++) {
@@ -401,9 +402,9 @@ apirl_status apirl_osem_3d(const apirl_image_geom* img, const apirl_sino3d_geom*
 apirl_status apirl_osem_3d_ex(const apirl_image_geom* img, const apirl_sino3d_geom* sino, const float* h_meas,
                               const float* h_mult, const float* h_add, const float* h_init, int iters, int nsubsets,
                               int device, float* h_out, double* h_lik, const apirl_recon_options* opts) {
-  const apirl_recon_options o = opts ? *opts : apirl_recon_options{nullptr, nullptr, nullptr};
+  const apirl_recon_options o = opts ? *opts : apirl_recon_options{nullptr, nullptr, nullptr, 0};
   return osem_3d(img, sino, h_meas, h_mult, h_add, h_init, iters, nsubsets, device, h_out, h_lik, o.h_sens_in,
-                 o.h_sens_out, nsubsets, o.sampling);
+                 o.h_sens_out, nsubsets, o.sampling, o.update_positive_sens);
 }
 
 apirl_status apirl_mlem_3d(const apirl_image_geom* img, const apirl_sino3d_geom* sino, const float* h_meas,
@@ -415,7 +416,7 @@ apirl_status apirl_mlem_3d(const apirl_image_geom* img, const apirl_sino3d_geom*
 apirl_status apirl_mlem_3d_ex(const apirl_image_geom* img, const apirl_sino3d_geom* sino, const float* h_meas,
                               const float* h_mult, const float* h_add, const float* h_init, int iters, int device,
                               float* h_out, double* h_lik, const apirl_recon_options* opts) {
-  const apirl_recon_options o = opts ? *opts : apirl_recon_options{nullptr, nullptr, nullptr};
+  const apirl_recon_options o = opts ? *opts : apirl_recon_options{nullptr, nullptr, nullptr, 0};
   return mlem_3d(img, sino, h_meas, h_mult, h_add, h_init, iters, device, h_out, h_lik, o.h_sens_in, o.h_sens_out,
                  o.sampling);
 }
@@ -429,7 +430,7 @@ apirl_status apirl_mlem_2d(const apirl_image_geom* img, const apirl_sino2d_geom*
 apirl_status apirl_mlem_2d_ex(const apirl_image_geom* img, const apirl_sino2d_geom* sino, const float* h_meas,
                               const float* h_mult, const float* h_add, const float* h_init, int iters, int device,
                               float* h_out, double* h_lik, const apirl_recon_options* opts) {
-  const apirl_recon_options o = opts ? *opts : apirl_recon_options{nullptr, nullptr, nullptr};
+  const apirl_recon_options o = opts ? *opts : apirl_recon_options{nullptr, nullptr, nullptr, 0};
   if (o.sampling) return set_err(APIRL_ERR_NOT_SUPPORTED, "2D reconstructions walk one ray per bin", cudaSuccess);
   return mlem_2d(img, sino, h_meas, h_mult, h_add, h_init, iters, device, h_out, h_lik, o.h_sens_in, o.h_sens_out);
 }

@@ -324,7 +324,7 @@ def _sampling_c(sampling):
     return ctypes.byref(_lib.SamplingC(int(ns), int(nas), int(bool(multi))))
 
 
-def _recon_opts(sampling, sens_in, sens_out):
+def _recon_opts(sampling, sens_in, sens_out, update_positive_sens=False):
     """apirl_recon_options; the ctypes objects are returned with it so they stay alive."""
     smp = None
     if sampling is not None:
@@ -332,23 +332,26 @@ def _recon_opts(sampling, sens_in, sens_out):
         smp = _lib.SamplingC(int(ns), int(nas), int(bool(multi)))
     o = _lib.ReconOptionsC(ctypes.pointer(smp) if smp is not None else None,
                            _np_ptr(sens_in) if sens_in is not None else None,
-                           _np_ptr(sens_out) if sens_out is not None else None)
+                           _np_ptr(sens_out) if sens_out is not None else None,
+                           int(bool(update_positive_sens)))
     return o, smp
 
 
 def osem_3d(image_geom, sino_geom, meas, init, iters, nsubsets, mult=None, add=None, device=0, sampling=None,
-            sens=None, all_sens=False):
+            sens=None, all_sens=False, update_positive_sens=False):
     """OsemSinogram3d::Reconstruct on the GPU.  Returns (image,
     likelihood[iters*nsubsets+1], sensitivity): subset 0's image, or all
     nsubsets images [subset, voxel] with all_sens.  sens: given sensitivity
-    images [subset, voxel] instead of A_s^T (mult or 1) (forcePositive applied)."""
+    images [subset, voxel] instead of A_s^T (mult or 1) (forcePositive applied).
+    update_positive_sens: update where sens > 0 (else 0) instead of the
+    reference's sens >= 0 (NaN where no ray of a subset reaches a voxel)."""
     lib = _lib.load()
     meas, init, mult, add = _f32(meas), _f32(init), _f32(mult), _f32(add)
     nv = image_geom.n_voxels
     out = np.zeros(nv, np.float32)
     lik = np.zeros(iters * nsubsets + 1, np.float64)
     ig, sc = _img_c(image_geom), _sino3d_c(sino_geom)
-    if sens is None and not all_sens:
+    if sens is None and not all_sens and not update_positive_sens:
         sens0 = np.zeros(nv, np.float32)
         check(lib.apirl_osem_3d(ctypes.byref(ig), ctypes.byref(sc), _np_ptr(meas), _np_ptr(mult), _np_ptr(add),
                                 _np_ptr(init), iters, nsubsets, device, _np_ptr(out), _np_ptr(lik), _np_ptr(sens0),
@@ -358,7 +361,7 @@ def osem_3d(image_geom, sino_geom, meas, init, iters, nsubsets, mult=None, add=N
     if sens_in is not None and sens_in.size != nsubsets * nv:
         raise ValueError("sens must hold nsubsets images")
     sens_out = np.zeros((nsubsets, nv), np.float32)
-    opts, _keep = _recon_opts(sampling, sens_in, sens_out)
+    opts, _keep = _recon_opts(sampling, sens_in, sens_out, update_positive_sens)
     check(lib.apirl_osem_3d_ex(ctypes.byref(ig), ctypes.byref(sc), _np_ptr(meas), _np_ptr(mult), _np_ptr(add),
                                _np_ptr(init), iters, nsubsets, device, _np_ptr(out), _np_ptr(lik), ctypes.byref(opts)))
     return out, lik, (sens_out if all_sens else sens_out[0].copy())

@@ -119,6 +119,29 @@ def c2_counts(expected, sino_index, n_per_sino, seed=0):
     return out.reshape(-1)
 
 
+def c2_device_arrays(P, dev):
+    """The 3D workload's attenuation factors (float32) and Poisson counts
+    (uint32 stored in an int32 tensor viewed as uint32), whole sinogram, on
+    `dev`.  P: a SiddonProjector of c2_geometry() (its LOR tables give the
+    chords; its projection of the phantom times the attenuation gives the
+    expected counts)."""
+    import torch
+    ig, sg = P.image_geom, P.sino_geom
+    lor, z = P.tables()
+    phantom = torch.from_numpy(cylinder_phantom_3d(ig, seed=2)).to(dev)
+    chords = cylinder_chords(lor, z)                      # FP64 on the host
+    atten = torch.from_numpy(np.exp(-MU_WATER_PER_MM * chords).astype(np.float32).reshape(-1)).to(dev)
+    del chords
+    expected = torch.empty(P.num_bins(), dtype=torch.float32, device=dev)
+    P.project(phantom, expected)
+    expected.mul_(atten)
+    # Poisson draws per sinogram on the host (seeded by sinogram index), so
+    # that a sample of sinograms can be drawn again identically on its own.
+    counts = torch.from_numpy(c2_counts(expected.cpu().numpy(), range(sg.n_sinos),
+                                        sg.n_proj * sg.n_r).view(np.int32)).to(dev).view(torch.uint32)
+    return atten, counts
+
+
 def poisson_counts(expected, total, seed=0):
     """Scale `expected` to sum `total` and draw Poisson counts (uint32), numpy."""
     lam = expected.astype(np.float64) * (total / float(expected.sum()))

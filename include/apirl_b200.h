@@ -428,6 +428,12 @@ typedef struct {
   const apirl_sampling* sampling;
   const float* h_sens_in;
   float* h_sens_out;
+  /* OSEM pixel update rule.  0: the reference's, x * bp / sens where
+   * sens >= 0 with threshold 0 (OsemSinogram3d.cpp:24-33, :217-237), which
+   * gives 0 * 0 / 0 = NaN at voxels that no ray of a subset crosses;
+   * 1: update where sens > 0, else 0 (those voxels become 0).  Read by
+   * apirl_osem_3d_ex only. */
+  int update_positive_sens;
 } apirl_recon_options;
 apirl_status apirl_osem_3d_ex(const apirl_image_geom* img, const apirl_sino3d_geom* sino, const float* h_meas,
                               const float* h_mult, const float* h_add, const float* h_init, int iters, int nsubsets,

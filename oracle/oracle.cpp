@@ -535,7 +535,7 @@ void gather_subset(const Sino3DG<T>& s, int subset, int nsub, const T* full, T* 
 
 template <typename T>
 int osem3d(const Sino3DG<T>& s, const ImgG<T>& g, const T* init, const T* meas, const T* mult, const T* add,
-           int iters, int nsub, T* out_img, T* out_lik, T* out_sens0, int threads) {
+           int iters, int nsub, T* out_img, T* out_lik, T* out_sens0, int threads, bool ge = true) {
   long nv = (long)g.nx * g.ny * g.nz;
   std::vector<std::vector<T>> sens(nsub, std::vector<T>(nv, 0));
   long maxb = (long)subset_nproj(s.nProj, 0, nsub) * s.nR * s.nSinos;
@@ -557,7 +557,7 @@ int osem3d(const Sino3DG<T>& s, const ImgG<T>& g, const T* init, const T* meas, 
       std::fill(bp.begin(), bp.end(), (T)0);
       inverse_divide<T>(nb, m.data(), est.data());
       backproject3d<T>(s, sb, nsub, g, est.data(), nullptr, bp.data(), threads, 0);
-      update<T>(nv, x.data(), bp.data(), sens[sb].data(), (T)0, true);
+      update<T>(nv, x.data(), bp.data(), sens[sb].data(), (T)0, ge);
     }
   }
   if (out_lik) {
@@ -737,6 +737,15 @@ int or_sino3d_z_f64(const or_sino3d* d, double* z1, double* z2) {
     Sino3DG<T> s = mk<T>(d);                                                                                 \
     return osem3d<T>(s, make_img<T>(nx, ny, nz, dx, dy, dz), init, meas, mult, add, iters, nsub, out_img,    \
                      out_lik, out_sens0, threads);                                                           \
+  }                                                                                                          \
+  /* ge = 0: the update x * bp / sens only where sens > 0 (else 0) instead of    \
+     the reference's sens >= 0 (OsemSinogram3d.cpp:217-237).  */                \
+  int or_osem_3d_rule_##SUF(const or_sino3d* d, int nx, int ny, int nz, float dx, float dy, float dz,       \
+                            const T* init, const T* meas, const T* mult, const T* add, int iters, int nsub, \
+                            T* out_img, T* out_lik, T* out_sens0, int threads, int ge) {                   \
+    Sino3DG<T> s = mk<T>(d);                                                                                 \
+    return osem3d<T>(s, make_img<T>(nx, ny, nz, dx, dy, dz), init, meas, mult, add, iters, nsub, out_img,    \
+                     out_lik, out_sens0, threads, ge != 0);                                                  \
   }                                                                                                          \
   T or_likelihood_##SUF(long n, const T* est, const T* meas, int gt0) {                                      \
     return likelihood<T>(n, est, meas, gt0 != 0);                                                            \

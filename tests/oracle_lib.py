@@ -69,6 +69,8 @@ class Oracle:
                                                         _vp, _vp, _vp, _i]
             getattr(L, f"or_osem_3d_{suf}").argtypes = [_vp, _i, _i, _i, _f, _f, _f, _vp, _vp, _vp, _vp, _i, _i,
                                                         _vp, _vp, _vp, _i]
+            getattr(L, f"or_osem_3d_rule_{suf}").argtypes = [_vp, _i, _i, _i, _f, _f, _f, _vp, _vp, _vp, _vp, _i,
+                                                             _i, _vp, _vp, _vp, _i, _i]
             getattr(L, f"or_likelihood_{suf}").argtypes = [_l, _vp, _vp, _i]
             getattr(L, f"or_likelihood_{suf}").restype = T
             getattr(L, f"or_inverse_divide_{suf}").argtypes = [_l, _vp, _vp]
@@ -182,7 +184,9 @@ class Oracle:
                                             *_img_args(ig), _p(values), _p(img))
         return img
 
-    def osem_3d(self, sg, ig, init, meas, iters, nsub, mult=None, add=None, dtype=np.float32, threads=None):
+    def osem_3d(self, sg, ig, init, meas, iters, nsub, mult=None, add=None, dtype=np.float32, threads=None,
+                ge=True):
+        """ge=False: update only where sens > 0 (else 0) instead of the reference's sens >= 0."""
         dt = np.dtype(dtype)
         cv = lambda a: None if a is None else np.ascontiguousarray(a, dtype=dt)
         init, meas, mult, add = cv(init), cv(meas), cv(mult), cv(add)
@@ -190,9 +194,9 @@ class Oracle:
         lik = np.zeros(iters * nsub + 1, dt)
         sens0 = np.zeros(ig.n_voxels, dt)
         s = _sino3d_struct(sg)
-        getattr(self.L, f"or_osem_3d_{self._suf(dt)}")(ctypes.byref(s), *_img_args(ig), _p(init), _p(meas),
-                                                      _p(mult), _p(add), iters, nsub, _p(out), _p(lik),
-                                                      _p(sens0), threads or self.threads)
+        getattr(self.L, f"or_osem_3d_rule_{self._suf(dt)}")(ctypes.byref(s), *_img_args(ig), _p(init), _p(meas),
+                                                           _p(mult), _p(add), iters, nsub, _p(out), _p(lik),
+                                                           _p(sens0), threads or self.threads, int(bool(ge)))
         return out, lik, sens0
 
     # ---- 2D ------------------------------------------------------------
@@ -277,6 +281,7 @@ class RefHarness:
         L.ref_project_3d.argtypes = [_vp, _i, _i, _i, _i, _i, _f, _f, _f, _vp, _vp]
         L.ref_backproject_3d.argtypes = [_vp, _i, _i, _i, _i, _i, _f, _f, _f, _vp, _vp]
         L.ref_osem_3d_subiteration.argtypes = [_vp, _i, _i, _i, _i, _i, _f, _f, _f, _vp, _vp, _vp]
+        L.ref_osem_3d_subiteration_rule.argtypes = [_vp, _i, _i, _i, _i, _i, _f, _f, _f, _vp, _vp, _vp, _i]
         L.ref_osem_3d.argtypes = [_vp, _i, _i, _i, _f, _f, _f, _vp, _i, _i, ctypes.c_char_p, _vp, _vp, _vp]
         L.ref_sino3d_write.argtypes = [_vp, ctypes.c_char_p]
         L.ref_image_write.argtypes = [_i, _i, _i, _f, _f, _f, _vp, ctypes.c_char_p]
@@ -399,9 +404,10 @@ class RefHarness:
         self.L.ref_mmr_backproject(h, *_img_args(ig), _p(values), _p(img))
         return img
 
-    def osem_subiteration(self, h, ig, subset, nsub, x, sens):
+    def osem_subiteration(self, h, ig, subset, nsub, x, sens, ge=True):
+        """One OSEM sub-iteration in place on x; ge=False updates only where sens > 0."""
         lik = np.zeros(1, np.float32)
-        self.L.ref_osem_3d_subiteration(h, subset, nsub, *_img_args(ig), _p(x), _p(sens), _p(lik))
+        self.L.ref_osem_3d_subiteration_rule(h, subset, nsub, *_img_args(ig), _p(x), _p(sens), _p(lik), int(bool(ge)))
         return float(lik[0])
 
     def write_sino3d(self, h, path_no_ext):
