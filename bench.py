@@ -141,20 +141,8 @@ def setup_workload(dev, log, max_ring_diff=None, alpha="f32"):
     if alpha == "f64":
         P.set_alpha_precision(True)  # precision-study mode: FP64 walk geometry
     nb = P.num_bins()
-    lor, z = P.tables()
     t0 = time.time()
-    phantom = torch.from_numpy(workloads.cylinder_phantom_3d(ig, seed=2)).to(dev)
-    chords = workloads.cylinder_chords(lor, z)                      # FP64 on the host
-    atten = torch.from_numpy(np.exp(-workloads.MU_WATER_PER_MM * chords).astype(np.float32).reshape(-1)).to(dev)
-    del chords
-    expected = torch.empty(nb, dtype=torch.float32, device=dev)
-    P.project(phantom, expected)
-    expected.mul_(atten)
-    # Poisson draws per sinogram on the host (seeded by sinogram index), so
-    # that the CPU reference arm can draw its sample's counts identically.
-    counts = torch.from_numpy(workloads.c2_counts(expected.cpu().numpy(), range(sg.n_sinos),
-                                                  sg.n_proj * sg.n_r).view(np.int32)).to(dev).view(torch.uint32)
-    del expected
+    atten, counts = workloads.c2_device_arrays(P, dev)
     nv = ig.n_voxels
     sens = torch.zeros((NSUB, nv), dtype=torch.float32, device=dev)
     for s in range(NSUB):
@@ -521,7 +509,7 @@ def run_gpu(args):
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        cpu = cpu_baseline(w, log, budget_s=args.cpu_seconds, threads=args.cpu_threads)
+        cpu = cpu_baseline(w, log, budget_s=args.cpu_seconds, threads=args.cpu_threads, first_subset=args.warmup)
 
     if rank == 0:
         line = {
@@ -573,94 +561,108 @@ def run_gpu(args):
 
 
 # ---------------------------------------------------------------------------
-# CPU side: the reference APIRL code on a sample of the same sub-iteration.
-SAMPLE_SEGMENTS = [0, 7, -7, 14, -14]
+# CPU side: the reference APIRL code on whole sub-iterations of the same job.
+class CpuSubiterations:
+    """Whole OSEM sub-iterations of the full workload (all 1261 sinograms) on
+    the host cores: the reference code compiled from its sources
+    (oracle/_ref: getSubset, Project, getLikelihoodValue, inverseDivideBinToBin,
+    Backproject, then the pixel update of OsemSinogram3d.cpp:217-237 with the
+    bench's rule, update where sens > 0), or the oracle restatement where the
+    reference was not built.  Subsets and sensitivity images are those the GPU
+    arm uses."""
 
-
-def _sample_geometry(sg):
-    from apirl_b200.geometry import Sino3DGeom
-    return Sino3DGeom(sg.n_proj, sg.n_r, sg.n_rings, sg.r_fov, sg.axial_fov, sg.r_scanner,
-                      list(SAMPLE_SEGMENTS), list(SAMPLE_SEGMENTS))
-
-
-def _sample_sinograms(sg):
-    """Indices, in the whole sinogram, of the sampled segments' sinograms."""
-    off, parts = 0, {}
-    for rd, n in zip(sg.min_rd, sg.sinos_per_segment):
-        parts[rd] = (off, n)
-        off += n
-    return [g for rd in SAMPLE_SEGMENTS for g in range(parts[rd][0], parts[rd][0] + parts[rd][1])]
-
-
-def _sample_counts(sg, counts_full):
-    """Counts of the sampled segments, in the sample sinogram's layout."""
-    per = sg.n_proj * sg.n_r
-    idx = _sample_sinograms(sg)
-    return counts_full.reshape(sg.n_sinos, per)[idx].reshape(-1).astype(np.float32)
-
-
-class CpuSample:
-    """One sub-iteration (subset 0 of 21) of the reference code restricted to
-    the segments SAMPLE_SEGMENTS; `fraction` is the sample's share of the full
-    sub-iteration's Siddon segments, so subiter/s = fraction / seconds."""
-
-    def __init__(self, counts, log, threads=None):
-        """counts: the sampled segments' counts in the sample sinogram's layout;
-        threads: host threads for the reference's OpenMP loops (default: all)."""
+    def __init__(self, counts_full, log, threads=None):
+        """counts_full: the whole sinogram's counts (any integer or float array)."""
         sys.path.insert(0, os.path.join(ROOT, "tests"))
         from oracle_lib import RefHarness, Oracle, REF_SO
         from apirl_b200 import workloads
         self.ig, self.sg = workloads.c2_geometry()
-        self.sample = _sample_geometry(self.sg)
-        counts = np.ascontiguousarray(counts, np.float32)
-        oracle = Oracle()
-        full_steps = oracle.count_steps_3d(self.sg, self.ig, 0, NSUB)
-        samp_steps = oracle.count_steps_3d(self.sample, self.ig, 0, NSUB)
-        self.fraction = samp_steps / full_steps
+        counts = np.ascontiguousarray(counts_full, np.float32)
         self.cores = threads or os.cpu_count() or 1
         if os.path.exists(REF_SO):
             self.kind = "reference"
             self.R = RefHarness()
             self.R.set_threads(self.cores)
-            self.h = self.R.sino3d(self.sample, counts)
+            t0 = time.perf_counter()
+            self.h = self.R.sino3d(self.sg, counts)
+            log(f"reference sinogram loaded ({counts.size} bins) in {time.perf_counter() - t0:.1f} s")
         else:
             self.kind = "port"
             self.R = None
-            self.oracle = oracle
+            self.oracle = Oracle()
             self.counts = counts
         self.x = np.ones(self.ig.n_voxels, np.float32)
-        self.sens = np.ones(self.ig.n_voxels, np.float32)
-        log(f"cpu sample: segments {SAMPLE_SEGMENTS}, {self.sample.n_sinos} sinograms, "
-            f"{self.fraction:.4f} of a sub-iteration's segments, kind {self.kind}, {self.cores} threads")
 
-    def run(self):
+    def set_threads(self, n):
+        self.cores = n
+        if self.R is not None:
+            self.R.set_threads(n)
+
+    def run(self, subset, sens):
+        """One whole sub-iteration of `subset`, in place on self.x; seconds."""
+        sens = np.ascontiguousarray(sens, np.float32)
         t0 = time.perf_counter()
         if self.R is not None:
-            self.R.osem_subiteration(self.h, self.ig, 0, NSUB, self.x, self.sens)
+            self.R.osem_subiteration(self.h, self.ig, subset, NSUB, self.x, sens, ge=UPDATE_GE)
         else:
-            o, sg, ig = self.oracle, self.sample, self.ig
-            est = o.project_3d(sg, ig, self.x, 0, NSUB, threads=self.cores)
-            m = self.counts.reshape(sg.n_sinos, sg.n_proj, sg.n_r)[:, 0::NSUB, :].reshape(-1)
+            o, sg, ig = self.oracle, self.sg, self.ig
+            est = o.project_3d(sg, ig, self.x, subset, NSUB, threads=self.cores)
+            m = self.counts.reshape(sg.n_sinos, sg.n_proj, sg.n_r)[:, subset::NSUB, :].reshape(-1)
             ratio = o.inverse_divide(m, est)
-            bp = o.backproject_3d(sg, ig, ratio, 0, NSUB, threads=self.cores)
-            self.x = o.update(self.x, bp, self.sens, np.float32(0), True)
+            bp = o.backproject_3d(sg, ig, ratio, subset, NSUB, threads=self.cores)
+            self.x = o.update(self.x, bp, sens, np.float32(0), UPDATE_GE)
         return time.perf_counter() - t0
 
-    def describe(self):
-        return (f"OSEM sub-iteration 0/21 of the full workload restricted to segments {SAMPLE_SEGMENTS} "
-                f"({self.sample.n_sinos} of 1261 sinograms, {self.fraction:.4f} of the sub-iteration's Siddon "
-                f"segments); value scaled to whole sub-iterations")
+    def describe(self, subsets):
+        src = ("the reference APIRL CPU code compiled from its sources (oracle/_ref)" if self.kind == "reference"
+               else "the oracle restatement of the reference (oracle/)")
+        return (f"whole OSEM sub-iterations of the full workload (all 1261 sinograms), subsets {subsets}, through "
+                f"{src}: getSubset, Project, likelihood, ratio, Backproject, pixel update; wall time per "
+                "sub-iteration")
 
 
-def cpu_baseline(w, log, budget_s=15.0, threads=None):
-    counts_full = w["counts"].view(__import__("torch").int32).cpu().numpy()
-    cs = CpuSample(_sample_counts(w["sg"], counts_full), log, threads)
-    times = [cs.run()]
-    while sum(times) < budget_s and len(times) < 20:
-        times.append(cs.run())
-    sec = statistics.median(times)
-    return {"value": cs.fraction / sec, "unit": UNIT, "cores": cs.cores, "kind": cs.kind,
-            "sample": cs.describe() + f"; median of {len(times)} runs, {sec:.2f} s each"}
+def cpu_baseline(w, log, budget_s=15.0, threads=None, first_subset=0):
+    """The reference CPU code on whole sub-iterations of the GPU arm's job (its
+    counts and sensitivity images), subsets in the GPU arm's order, until
+    `budget_s` of CPU time (at least one sub-iteration)."""
+    import torch
+    counts_full = w["counts"].view(torch.int32).cpu().numpy().view(np.uint32)
+    cs = CpuSubiterations(counts_full, log, threads)
+    del counts_full
+    times, subs = [], []
+    while not times or (sum(times) < budget_s and len(times) < NSUB):
+        s = (first_subset + len(times)) % NSUB
+        times.append(cs.run(s, w["sens"][s].cpu().numpy()))
+        subs.append(s)
+    total = sum(times)
+    return {"value": len(times) / total, "unit": UNIT, "cores": cs.cores, "kind": cs.kind,
+            "sample": cs.describe(subs) + f"; {len(times)} sub-iterations in {total:.2f} s"}
+
+
+def _reference_job(log, o, needed_subsets):
+    """The job's counts and the needed subsets' sensitivity images, made on
+    the host exactly as the GPU arm makes them: the oracle's projection of the
+    phantom (bit-identical to the GPU's), the same attenuation factors, the
+    same per-sinogram Poisson seeds; sensitivity = A_s^T a then forcePositive."""
+    from apirl_b200 import workloads
+    ig, sg = workloads.c2_geometry()
+    t0 = time.perf_counter()
+    proj = o.project_3d(sg, ig, workloads.cylinder_phantom_3d(ig, seed=2))
+    lor = o.lor_points_2d(sg.n_proj, sg.n_r, sg.r_fov, sg.r_scanner)
+    z1, z2 = o.sino3d_z(sg)
+    atten = np.exp(-workloads.MU_WATER_PER_MM *
+                   workloads.cylinder_chords(lor, np.stack([z1, z2], 1).astype(np.float32))).astype(np.float32)
+    atten = atten.reshape(-1)
+    proj *= atten
+    counts = workloads.c2_counts(proj, range(sg.n_sinos), sg.n_proj * sg.n_r)
+    del proj
+    sens = {}
+    for s in sorted(set(needed_subsets)):
+        a_s = np.ascontiguousarray(atten.reshape(sg.n_sinos, sg.n_proj, sg.n_r)[:, s::NSUB, :]).reshape(-1)
+        sens[s] = np.maximum(o.backproject_3d(sg, ig, a_s, s, NSUB), np.float32(0))
+    log(f"job made on the host in {time.perf_counter() - t0:.1f} s: {int(counts.sum())} counts, "
+        f"{len(sens)} sensitivity images")
+    return counts, sens
 
 
 def run_reference(args):
@@ -668,34 +670,39 @@ def run_reference(args):
     if rank != 0:
         return
     log = lambda m: print(f"[bench-ref] {m}", file=sys.stderr, flush=True)
-    from apirl_b200 import workloads
-    ig, sg = workloads.c2_geometry()
-    # The sampled segments' counts, drawn on the host exactly as the GPU arm
-    # draws them (this arm does not touch the GPU): the oracle's projection of
-    # the phantom (bit-identical to the GPU's), the same attenuation factors,
-    # the same per-sinogram seeds.
     sys.path.insert(0, os.path.join(ROOT, "tests"))
     from oracle_lib import Oracle
     o = Oracle()
-    sample = _sample_geometry(sg)
-    proj = o.project_3d(sample, ig, workloads.cylinder_phantom_3d(ig, seed=2))
-    lor = o.lor_points_2d(sample.n_proj, sample.n_r, sample.r_fov, sample.r_scanner)
-    z1, z2 = o.sino3d_z(sample)
-    chords = workloads.cylinder_chords(lor, np.stack([z1, z2], 1).astype(np.float32))
-    atten = np.exp(-workloads.MU_WATER_PER_MM * chords).astype(np.float32).reshape(-1)
-    counts = workloads.c2_counts(proj * atten, _sample_sinograms(sg), sg.n_proj * sg.n_r).astype(np.float32)
-    cs = CpuSample(counts, log, args.cpu_threads)
-    for _ in range(args.warmup):
-        cs.run()
-    times = [cs.run() for _ in range(args.steps)]
+    warm = [i % NSUB for i in range(args.warmup)]
+    timed = [(args.warmup + i) % NSUB for i in range(args.steps)]
+    one_thread_subset = (args.warmup + args.steps) % NSUB
+    counts, sens = _reference_job(log, o, warm + timed + [one_thread_subset])
+    cs = CpuSubiterations(counts, log, args.cpu_threads)
+    del counts
+    for s in warm:
+        cs.run(s, sens[s])
+    times = [cs.run(s, sens[s]) for s in timed]
     total = sum(times)
-    value = args.steps * cs.fraction / total
+    value = args.steps / total
+    log(f"{args.steps} sub-iterations on {cs.cores} threads: {total:.2f} s")
+    one = None
+    if not args.no_one_thread:
+        threads = cs.cores
+        cs.set_threads(1)
+        t1 = cs.run(one_thread_subset, sens[one_thread_subset])
+        cs.set_threads(threads)
+        one = {"value": 1.0 / t1, "unit": UNIT, "cores": 1, "sample": f"one whole sub-iteration (subset "
+               f"{one_thread_subset}) on 1 host thread, {t1:.2f} s"}
+        log(f"1 thread: {t1:.2f} s")
     line = {
         "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": 0, "steps": args.steps,
-        "warmup": args.warmup, "ms_per_step": total / args.steps / cs.fraction * 1e3, "higher_is_better": True,
+        "warmup": args.warmup, "ms_per_step": total / args.steps * 1e3, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded phantom, Poisson counts)",
-        "config": {"workload": WORKLOAD, "subsets": NSUB, "parallelism": f"{cs.cores} host threads (OpenMP)"},
-        "cpu_baseline": {"value": value, "unit": UNIT, "cores": cs.cores, "kind": cs.kind, "sample": cs.describe()},
+        "config": {"workload": WORKLOAD, "subsets": NSUB, "update": "x * bp / sens where sens > 0, else 0",
+                   "parallelism": f"{cs.cores} host threads (OpenMP)"},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": cs.cores, "kind": cs.kind,
+                         "sample": cs.describe(timed) + f"; {args.steps} sub-iterations in {total:.2f} s"},
+        "one_thread": one,
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
@@ -857,6 +864,8 @@ def main():
                      help="one job split over the ranks by LOR shards (strong scaling) instead of replicas")
     ap_.add_argument("--alpha", default="f32", choices=["f32", "f64"],
                      help="walk geometry: f32 = the reference's float arithmetic (headline); f64 = precision mode")
+    ap_.add_argument("--no-one-thread", action="store_true",
+                     help="reference arm: skip the extra one-thread sub-iteration")
     ap_.add_argument("--cpu-threads", type=int, default=None,
                      help="host threads of the CPU baseline / reference arm (default: all)")
     ap_.add_argument("--workload", default="osem3d", choices=["osem3d", "batched", "served", "mlem2d"])

@@ -548,8 +548,19 @@ int ref_sampled_3d(void* hv, int ns, int nas, int multi, int mode, int subset, i
 // (recon/src/OsemSinogram3d.cpp:159-237): subset copies, projection,
 // likelihood, ratio, backprojection and the multiplicative update with
 // threshold 0 and >=.  Used as the timed CPU baseline; x_inout is updated.
+int ref_osem_3d_subiteration_rule(void* hv, int subset, int nsubsets, int nx, int ny, int nz, float dx, float dy,
+                                  float dz, float* x_inout, const float* sens, float* out_lik, int ge);
+
 int ref_osem_3d_subiteration(void* hv, int subset, int nsubsets, int nx, int ny, int nz, float dx, float dy,
                              float dz, float* x_inout, const float* sens, float* out_lik) {
+  return ref_osem_3d_subiteration_rule(hv, subset, nsubsets, nx, ny, nz, dx, dy, dz, x_inout, sens, out_lik, 1);
+}
+
+// ge = 0: the pixel update only where sens > 0 (else 0) instead of the
+// reference's sens >= 0, which divides 0 by 0 at voxels no ray of the subset
+// crosses.
+int ref_osem_3d_subiteration_rule(void* hv, int subset, int nsubsets, int nx, int ny, int nz, float dx, float dy,
+                                  float dz, float* x_inout, const float* sens, float* out_lik, int ge) {
   Sinogram3DCylindricalPet* full = ((Sino3DHandle*)hv)->sino;
   Image* x = make_image(nx, ny, nz, dx, dy, dz, x_inout);
   Image* bp = make_image(nx, ny, nz, dx, dy, dz, NULL);
@@ -564,7 +575,7 @@ int ref_osem_3d_subiteration(void* hv, int subset, int nsubsets, int nx, int ny,
   p.Backproject(est, bp);
   float* px = x->getPixelsPtr(); float* pb = bp->getPixelsPtr();
   long n = (long)nx * ny * nz;
-  for (long k = 0; k < n; k++) px[k] = (sens[k] >= 0) ? px[k] * pb[k] / sens[k] : 0;
+  for (long k = 0; k < n; k++) px[k] = (ge ? sens[k] >= 0 : sens[k] > 0) ? px[k] * pb[k] / sens[k] : 0;
   memcpy(x_inout, px, sizeof(float) * n);
   if (out_lik) *out_lik = lik;
   delete x; delete bp;
