@@ -88,12 +88,13 @@ class Batch:
         ids = [self.submit(j) for j in jobs]
         res = {}
         while len(res) < len(ids):
-            self.step()
-            for i in ids:
-                if i not in res:
-                    r = self.result(i)
-                    if r is not None:
-                        res[i] = r
+            na, nq = self.step()
+            if len(ids) - na - nq > len(res):  # some job finished since the last look
+                for i in ids:
+                    if i not in res:
+                        r = self.result(i)
+                        if r is not None:
+                            res[i] = r
         return [res[i] for i in ids]
 
 
@@ -118,15 +119,16 @@ def serve(jobs, arrivals_s, device=0, budget_bytes=64 << 30):
             # nothing in flight: wait for the next arrival
             time.sleep(max(0.0, arrivals_s[order[nxt]] - (time.perf_counter() - t0)))
             continue
-        b.step()
+        na, nq = b.step()
         now = time.perf_counter() - t0
-        for jid, k in list(ids.items()):
-            if k in done_at:
-                continue
-            r = b.result(jid)
-            if r is not None:
-                results[k] = r
-                done_at[k] = now
+        if len(ids) - na - nq > len(done_at):  # some job finished since the last look
+            for jid, k in list(ids.items()):
+                if k in done_at:
+                    continue
+                r = b.result(jid)
+                if r is not None:
+                    results[k] = r
+                    done_at[k] = now
     b.close()
     lat = np.array([done_at[k] - submitted_at[k] for k in range(len(jobs))])
     return [results[k] for k in range(len(jobs))], lat, max(done_at.values())

@@ -155,33 +155,77 @@ cudaError_t launch_force_positive(int64_t n, float* x, cudaStream_t st);
 cudaError_t launch_fill(int64_t n, float* x, float v, cudaStream_t st);
 cudaError_t launch_exp_nonzero(int64_t n, float* v, cudaStream_t st);
 
-// ---- batched passes over many independent jobs --------------------------------
-// Each job's bins (voxels) occupy a range of whole 256-thread blocks of one
-// launch, so a block never straddles two jobs.
-struct EmJob {
+// ---- batched reconstructions (batch.cu) ---------------------------------------
+// One list of bins with counts walked in a batched step: one job's subset list
+// (an EM pass), or one of its subset lists for its final likelihood (back = 0).
+// Its chunks of 32 list entries are chunk_begin .. chunk_begin +
+// ceil(n_list / 32) - 1 of the step; segments are ordered by chunk_begin.
+struct MultiSeg {
   ImgGeom g;
   LorTable t;
   SubsetSel s;
   const void* counts;    // whole sinogram, [sinogram][angle][r]
-  const float* add;      // same layout or null
-  const float* x;
-  float* bp;
-  double* lik;           // output slot of this pass's likelihood
-  int64_t blk_begin;     // first block of this job in the launch
-  int64_t nbins;
+  const float* add;      // same layout, or null
+  PadBuffers pad;        // the job's padded image copies and backprojection pair
+  const int* list;       // the subset's bins with counts, in bin order
+  int64_t n_list;
+  int64_t chunk_begin;
   int counts_dtype;
   int back;
-  int lik_mode;
 };
-struct UpdJob {
+// One job's voxel work in a batched step, in 32 x 32 tiles of its slices:
+// before the walk, x into the padded copies and -x . gimg; after it, with
+// `update`, the EM update of x from the padded backprojection pair; the
+// likelihood = the job's chunk partials + its -x . gimg partials - zero_add.
+struct MultiVox {
+  ImgGeom g;
+  PadBuffers pad;
   float* x;
-  float* bp;
-  const float* sens;
-  int64_t blk_begin;     // first block (each block covers 1024 voxels)
-  int64_t nvox;
-  float thr;
-  int ge;
+  const float* sens;     // the pass's subset sensitivity (update)
+  const float* gimg;     // G_s of the pass's subset, or A^T 1 of all subsets (final likelihood)
+  double* lik;           // the likelihood's slot
+  int64_t tile_begin;    // first tile of the job in the step's tile launches
+  int64_t chunk_begin, n_chunks;  // the job's chunk partials in the walk
+  double zero_add;       // sum over all walked subsets' bins of the additive term
+  int tiles_x, tiles_y;
+  int update, ge;
 };
+// Tiles (blocks of the copy / update launches) of a job: ceil(nx/32) x ceil(ny/32) x nz.
+inline int64_t multi_tiles(const ImgGeom& g) {
+  return (int64_t)((g.nx + 31) / 32) * ((g.ny + 31) / 32) * g.nz;
+}
+// Persistent grid of the batched walk on the current device.
+cudaError_t multi_walk_grid(int* blocks);
+// One batched step: copies and dot products, the walk over every segment's
+// list (counter reset here), the likelihood sums, the updates.
+// chunk_partials: >= total_chunks doubles; tile_partials: >= total_tiles.
+cudaError_t launch_multi_step(const MultiVox* d_vox, int n_vox, int64_t total_tiles, const MultiSeg* d_segs,
+                              int n_segs, int64_t total_chunks, int walk_blocks, unsigned long long* counter,
+                              double* chunk_partials, double* tile_partials, cudaStream_t st);
+// List of the bins with counts of subset s (bin numbers of the subset, in bin
+// order), in two launches per subset: count (tiles: ceil(total / kNzTile)
+// ints kept for the write; *n_list) then write.
+cudaError_t launch_nz_count(const LorTable& t, SubsetSel s, const void* counts, int counts_dtype, int64_t total,
+                            int* tiles, int* n_list, cudaStream_t st);
+cudaError_t launch_nz_write(const LorTable& t, SubsetSel s, const void* counts, int counts_dtype, int64_t total,
+                            const int* tiles, int* list, cudaStream_t st);
+// per_angle[a] += A_a^T 1 for every angle a: n_proj padded images of `lim`
+// voxels (PadBuffers' border), [z][x][y] where tr_of[a] else [z][y][x],
+// cleared by the caller; one warp per 32 bins in angle order.
+cudaError_t launch_scatter_angles(const ImgGeom& g, const LorTable& t, const uint8_t* tr_of, float* per_angle,
+                                  unsigned lim, unsigned long long* counter, cudaStream_t st);
+// out[s] = the interior sum over the angles a = s, s + nsub, ... of those
+// padded images (nsub unpadded images of the geometry).
+cudaError_t launch_sum_angles(const float* per_angle, const uint8_t* tr_of, unsigned lim, int n_proj,
+                              const ImgGeom& g, int nsub, float* out, cudaStream_t st);
+// out[s] = sum over a = s, s + nsub, ... < n_img of img[a] (unpadded images of nvox voxels).
+cudaError_t launch_sum_images(const float* img, int n_img, int64_t nvox, int nsub, float* out, cudaStream_t st);
+// out[s] = sum over subset s's bins of the additive term (whole-sinogram layout), FP64, fixed order.
+cudaError_t launch_subset_sums(const LorTable& t, int nsub, const float* add, double* out, cudaStream_t st);
+
+// Sensitivity of every subset of a job whose sinogram has a multiplicative
+// term, in one pass over its whole sinogram: bin (g, a, l) belongs to subset
+// a % nsub.
 struct SensJob {
   ImgGeom g;
   LorTable t;            // whole sinogram; subset of angle a is a % nsub
@@ -192,11 +236,6 @@ struct SensJob {
   int64_t nvox;
   int nsub;
 };
-constexpr int kBatchBinsPerBlock = 256;
-constexpr int kBatchVoxPerBlock = 1024;
-cudaError_t launch_em_batch(const EmJob* d_jobs, const EmJob* h_jobs, int njobs, int64_t nblocks, double* partials,
-                            cudaStream_t st);
-cudaError_t launch_update_batch(const UpdJob* d_jobs, int njobs, int64_t nblocks, cudaStream_t st);
 cudaError_t launch_sens_batch(const SensJob* d_jobs, int njobs, int64_t nblocks, cudaStream_t st);
 
 }  // namespace apirl

@@ -44,6 +44,13 @@ constexpr int kPersistMinBlocks = APIRL_PERSIST_MIN_BLOCKS;
 // than the full pass's 6 blocks with four segments.
 constexpr int kListMinBlocks = 5;
 constexpr int kListGatherUnroll = 6;
+// The batched walk over many jobs' lists (k_em_multi) reads each segment's
+// geometry at run time: at 5 blocks (48 registers) it spilled 48 bytes, at 4
+// (64 registers) it does not.
+#ifndef APIRL_MULTI_MIN_BLOCKS
+#define APIRL_MULTI_MIN_BLOCKS 4
+#endif
+constexpr int kMultiMinBlocks = APIRL_MULTI_MIN_BLOCKS;
 constexpr int kEmMinBlocks = APIRL_EM_MIN_BLOCKS;
 // 1: the fused 3D pass sets the walk up a second time for the backprojection
 // (fewer live registers during the forward walk).
@@ -597,6 +604,38 @@ __global__ void __launch_bounds__(kNzBlock) k_nz_write(LorTable t, SubsetSel s, 
   }
 }
 
+// One bin of the padded-layout fused pass: forward walk over the padded copy
+// of the image that suits the ray's direction (x-running rays: [z][x][y]),
+// the additive term, the likelihood term, the ratio m / e and the scatter of
+// seg * ratio into the matching padded backprojection.  ci: the bin's index
+// in the counts / additive layout.  Returns the likelihood term (lik_term).
+template <int U>
+__device__ __forceinline__ double em_bin_pad(const ImgGeom& g, const LorTable& t, const BinPos& p, float m,
+                                             int64_t ci, const float* __restrict__ add, const PadBuffers& pad,
+                                             int back, int skip_zero) {
+  const int px = g.nx + 2 * kPad, py = g.ny + 2 * kPad;
+  const int uz = px * py;
+  const float4 L = t.lor[(int64_t)p.a * t.n_r + p.l];
+  const float2 z = t.z[p.g];
+  const float vx = A_SUB(L.z, L.x), vy = A_SUB(L.w, L.y);
+  const bool tr = fabsf(vx) >= fabsf(vy);
+  const int ux = tr ? py : 1, uy = tr ? 1 : px;
+  Walk3 w;
+  siddon3_setup(L.x, L.y, z.x, vx, vy, A_SUB(z.y, z.x), g, w);
+  float e = siddon3_gather_pad<U>(w, g, ux, uy, uz, pad.lim, tr ? pad.pT : pad.pA);
+  if (add) e = A_ADD(e, __ldg(add + ci));
+  const float r = (m != 0.f && e != 0.f) ? A_DIV(m, e) : 0.f;
+  const double term = e != 0.f ? lik_term(m, e, skip_zero) : 0.0;
+  if (back && r != 0.f) {
+    const float4 L2 = __ldcg(t.lor + (int64_t)p.a * t.n_r + p.l);
+    const float2 z2 = __ldcg(t.z + p.g);
+    Walk3 w2;
+    siddon3_setup(L2.x, L2.y, z2.x, A_SUB(L2.z, L2.x), A_SUB(L2.w, L2.y), A_SUB(z2.y, z2.x), g, w2);
+    siddon3_scatter_pad(w2, g, ux, uy, uz, pad.lim, r, tr ? pad.bT : pad.bA);
+  }
+  return term;
+}
+
 // The padded-layout fused pass as a persistent kernel: each warp takes the
 // next chunk of 32 consecutive bins from *chunk_counter until none are left,
 // so that warps never wait for the rest of their block and the SM keeps its
@@ -614,8 +653,6 @@ __global__ void __launch_bounds__(kBlock, LIST ? kListMinBlocks : kPersistMinBlo
   // with counts (k_nz_write), so every lane of a chunk walks.
   const int64_t n_items = LIST ? (int64_t)*n_list : total;
   const int64_t nchunks = (n_items + 31) >> 5;
-  const int px = g.nx + 2 * kPad, py = g.ny + 2 * kPad;
-  const int uz = px * py;
   for (;;) {
     unsigned long long c = 0;
     if (lane == 0) c = atomicAdd(chunk_counter, 1ULL);
@@ -629,27 +666,9 @@ __global__ void __launch_bounds__(kBlock, LIST ? kListMinBlocks : kPersistMinBlo
       const int64_t row = counts_packed ? ((int64_t)(p.g - t.g0) * s.nk + p.k) : ((int64_t)p.g * t.n_proj + p.a);
       const int64_t ci = row * t.n_r + p.l;
       const float m = load_count<CT>(counts, ci);
-      if (!(skip_zero && m == 0.f)) {
-        const float4 L = t.lor[(int64_t)p.a * t.n_r + p.l];
-        const float2 z = t.z[p.g];
-        const float vx = A_SUB(L.z, L.x), vy = A_SUB(L.w, L.y);
-        const bool tr = fabsf(vx) >= fabsf(vy);
-        const int ux = tr ? py : 1, uy = tr ? 1 : px;
-        Walk3 w;
-        siddon3_setup(L.x, L.y, z.x, vx, vy, A_SUB(z.y, z.x), g, w);
-        float e = siddon3_gather_pad<LIST ? kListGatherUnroll : APIRL_GATHER_UNROLL>(w, g, ux, uy, uz, pad.lim,
-                                                                                   tr ? pad.pT : pad.pA);
-        if (add) e = A_ADD(e, __ldg(add + ci));
-        const float r = (m != 0.f && e != 0.f) ? A_DIV(m, e) : 0.f;
-        if (e != 0.f) term = lik_term(m, e, skip_zero);
-        if (back && r != 0.f) {
-          const float4 L2 = __ldcg(t.lor + (int64_t)p.a * t.n_r + p.l);
-          const float2 z2 = __ldcg(t.z + p.g);
-          Walk3 w2;
-          siddon3_setup(L2.x, L2.y, z2.x, A_SUB(L2.z, L2.x), A_SUB(L2.w, L2.y), A_SUB(z2.y, z2.x), g, w2);
-          siddon3_scatter_pad(w2, g, ux, uy, uz, pad.lim, r, tr ? pad.bT : pad.bA);
-        }
-      }
+      if (!(skip_zero && m == 0.f))
+        term = em_bin_pad<LIST ? kListGatherUnroll : APIRL_GATHER_UNROLL>(g, t, p, m, ci, add, pad, back,
+                                                                           skip_zero);
     }
     #pragma unroll
     for (int o = 16; o > 0; o >>= 1) term += __shfl_down_sync(0xffffffffu, term, o);
@@ -846,77 +865,28 @@ __global__ void k_fill(int64_t n, float* __restrict__ x, float v) {
 
 
 // ---------------------------------------------------------------------------
-// Batched passes: many independent jobs in one launch.
+// Batched work over many independent jobs in one launch.
 __device__ __forceinline__ float load_count_any(const void* p, int dtype, int64_t i) {
   if (dtype == APIRL_U32) return (float)__ldg((const uint32_t*)p + i);
   if (dtype == APIRL_U16) return (float)__ldg((const uint16_t*)p + i);
   return __ldg((const float*)p + i);
 }
 
-template <typename J>
-__device__ __forceinline__ int find_job(const J* __restrict__ jobs, int njobs, int64_t blk) {
-  int lo = 0, hi = njobs - 1;
+// The last of n entries whose first (block, tile or chunk) key(e) is <= k;
+// entries are ordered by key.
+template <typename J, class Key>
+__device__ __forceinline__ int find_entry(const J* __restrict__ e, int n, int64_t k, Key key) {
+  int lo = 0, hi = n - 1;
   while (lo < hi) {
     const int mid = (lo + hi + 1) >> 1;
-    if (jobs[mid].blk_begin <= blk) lo = mid; else hi = mid - 1;
+    if (key(e[mid]) <= k) lo = mid; else hi = mid - 1;
   }
   return lo;
 }
 
-__global__ void __launch_bounds__(kBlock) k_em_batch(const EmJob* __restrict__ jobs, int njobs,
-                                                     double* __restrict__ partials) {
-  __shared__ int sj;
-  if (threadIdx.x == 0) sj = find_job(jobs, njobs, blockIdx.x);
-  __syncthreads();
-  const EmJob& J = jobs[sj];
-  const int64_t b = ((int64_t)blockIdx.x - J.blk_begin) * kBlock + threadIdx.x;
-  double term = 0.0;
-  if (b < J.nbins) {
-    const BinPos p = decode(b, J.t, J.s);
-    const int64_t ci = ((int64_t)p.g * J.t.n_proj + p.a) * J.t.n_r + p.l;
-    const float m = load_count_any(J.counts, J.counts_dtype, ci);
-    Walk3 w;
-    float e = ray_sum3(J.g, J.t.lor[(int64_t)p.a * J.t.n_r + p.l], J.t.z[p.g], J.x, w);
-    if (J.add) e = A_ADD(e, __ldg(J.add + ci));
-    const float r = (m != 0.f && e != 0.f) ? A_DIV(m, e) : 0.f;
-    if (J.lik_mode == 1 ? (e > 0.f) : (e != 0.f)) term = (double)m * log((double)e) - (double)e;
-    if (J.back && r != 0.f) {
-      float* bp = J.bp;
-      siddon3_walk(w, J.g, [&](bool inb, int idx, float seg) {
-        if (inb) atomicAdd(bp + idx, A_MUL(seg, r));
-      });
-    }
-  }
-  const double bs = block_sum(term);
-  if (threadIdx.x == 0) partials[blockIdx.x] = bs;
-}
-
-// One block per job: deterministic sum of the job's block partials.
-__global__ void k_sum_batch(const EmJob* __restrict__ jobs, const double* __restrict__ partials) {
-  const EmJob& J = jobs[blockIdx.x];
-  const int64_t nb = (J.nbins + kBlock - 1) / kBlock;
-  double v = 0.0;
-  for (int64_t i = threadIdx.x; i < nb; i += blockDim.x) v += partials[J.blk_begin + i];
-  const double s = block_sum(v);
-  if (threadIdx.x == 0 && J.lik) *J.lik = s;
-}
-
-__global__ void __launch_bounds__(kBlock) k_update_batch(const UpdJob* __restrict__ jobs, int njobs) {
-  __shared__ int sj;
-  if (threadIdx.x == 0) sj = find_job(jobs, njobs, blockIdx.x);
-  __syncthreads();
-  const UpdJob& J = jobs[sj];
-  const int64_t base = ((int64_t)blockIdx.x - J.blk_begin) * kBatchVoxPerBlock;
-  #pragma unroll
-  for (int c = 0; c < kBatchVoxPerBlock / kBlock; c++) {
-    const int64_t i = base + c * kBlock + threadIdx.x;
-    if (i < J.nvox) {
-      const float sv = J.sens[i];
-      const bool okv = J.ge ? (sv >= J.thr) : (sv > J.thr);
-      J.x[i] = okv ? A_DIV(A_MUL(J.x[i], J.bp[i]), sv) : 0.f;
-      J.bp[i] = 0.f;
-    }
-  }
+template <typename J>
+__device__ __forceinline__ int find_job(const J* __restrict__ jobs, int njobs, int64_t blk) {
+  return find_entry(jobs, njobs, blk, [](const J& j) { return j.blk_begin; });
 }
 
 // Sensitivity of every subset of a job in one pass over its whole sinogram:
@@ -955,61 +925,75 @@ struct PadDims {
   }
 };
 
+// One 32 x 32 tile (x0, y0) of slice z, worked by 256 threads as 32 x 8
+// (lx, ly): x ([z][y][x], unpadded) -> the interiors of pA ([z][y][x]) and pT
+// ([z][x][y]).  With gimg: returns the thread's FP64 sum of x * gimg over its
+// voxels where gimg != 0.
+__device__ __forceinline__ double pad_copy_tile(const PadDims& d, const float* __restrict__ x, float* __restrict__ pA,
+                                                float* __restrict__ pT, const float* __restrict__ gimg, int x0, int y0,
+                                                int z, int lx, int ly, float (*tile)[33]) {
+  const int64_t base = (int64_t)z * d.nx * d.ny;
+  double dot = 0.0;
+  for (int r = ly; r < 32; r += 8) {
+    const int yy = y0 + r, xx = x0 + lx;
+    if (xx < d.nx && yy < d.ny) {
+      const int64_t i = base + (int64_t)yy * d.nx + xx;
+      const float v = x[i];
+      tile[r][lx] = v;
+      pA[d.a(xx, yy, z)] = v;
+      if (gimg) {
+        const float gv = gimg[i];
+        if (gv != 0.f) dot += (double)v * (double)gv;
+      }
+    }
+  }
+  __syncthreads();
+  for (int r = ly; r < 32; r += 8) {
+    const int xx = x0 + r, yy = y0 + lx;
+    if (xx < d.nx && yy < d.ny) pT[d.t(xx, yy, z)] = tile[lx][r];
+  }
+  return dot;
+}
+
 // x ([z][y][x], unpadded) -> interiors of pA and pT (32x32 tiles per slice).
 __global__ void __launch_bounds__(256) k_pad_copy(PadDims d, const float* __restrict__ x, float* __restrict__ pA,
                                                   float* __restrict__ pT) {
   __shared__ float tile[32][33];
-  const int z = blockIdx.z, x0 = blockIdx.x * 32, y0 = blockIdx.y * 32;
-  const int64_t base = (int64_t)z * d.nx * d.ny;
-  for (int r = threadIdx.y; r < 32; r += 8) {
-    const int yy = y0 + r, xx = x0 + threadIdx.x;
-    if (xx < d.nx && yy < d.ny) {
-      const float v = x[base + (int64_t)yy * d.nx + xx];
-      tile[r][threadIdx.x] = v;
-      pA[d.a(xx, yy, z)] = v;
-    }
-  }
-  __syncthreads();
-  for (int r = threadIdx.y; r < 32; r += 8) {
-    const int xx = x0 + r, yy = y0 + threadIdx.x;
-    if (xx < d.nx && yy < d.ny) pT[d.t(xx, yy, z)] = tile[threadIdx.x][r];
-  }
+  pad_copy_tile(d, x, pA, pT, nullptr, blockIdx.x * 32, blockIdx.y * 32, blockIdx.z, threadIdx.x, threadIdx.y, tile);
 }
 
-// Sum of the two padded backprojections at every interior voxel, [z][y][x]
-// order, interiors cleared.  mode 0: EM update of x (threshold rule ge/gt);
-// mode 1: bp += sum.  All loads come before the clearing stores (a store to
-// an address whose load is still in flight stalls the thread's later memory
-// operations: clearing in place made this kernel ~8x slower).
-__global__ void __launch_bounds__(256) k_pad_reduce(PadDims d, float* __restrict__ bA, float* __restrict__ bT,
-                                                    int mode, float* __restrict__ x, float* __restrict__ bp,
-                                                    const float* __restrict__ sens, const float* __restrict__ thr_ptr,
-                                                    float thr_value, int ge) {
-  __shared__ float tile[32][33];
-  const int z = blockIdx.z, x0 = blockIdx.x * 32, y0 = blockIdx.y * 32;
+// Sum of the two padded backprojections over one 32 x 32 tile (x0, y0) of
+// slice z, [z][y][x] order, interiors cleared; threads as in pad_copy_tile.
+// mode 0: EM update of x (threshold rule ge/gt); mode 1: bp += sum.  All
+// loads come before the clearing stores (a store to an address whose load is
+// still in flight stalls the thread's later memory operations: clearing in
+// place made this kernel ~8x slower).
+__device__ __forceinline__ void pad_reduce_tile(const PadDims& d, float* __restrict__ bA, float* __restrict__ bT,
+                                                int mode, float* __restrict__ x, float* __restrict__ bp,
+                                                const float* __restrict__ sens, float thr, int ge, int x0, int y0,
+                                                int z, int lx, int ly, float (*tile)[33]) {
   const int64_t base = (int64_t)z * d.nx * d.ny;
-  for (int r = threadIdx.y; r < 32; r += 8) {  // transposed buffer, read along y
-    const int xx = x0 + r, yy = y0 + threadIdx.x;
-    if (xx < d.nx && yy < d.ny) tile[threadIdx.x][r] = bT[d.t(xx, yy, z)];
+  for (int r = ly; r < 32; r += 8) {  // transposed buffer, read along y
+    const int xx = x0 + r, yy = y0 + lx;
+    if (xx < d.nx && yy < d.ny) tile[lx][r] = bT[d.t(xx, yy, z)];
   }
   __syncthreads();
   float bv[4];
   #pragma unroll
   for (int q = 0; q < 4; q++) {
-    const int r = threadIdx.y + 8 * q;
-    const int yy = y0 + r, xx = x0 + threadIdx.x;
-    bv[q] = (xx < d.nx && yy < d.ny) ? A_ADD(bA[d.a(xx, yy, z)], tile[r][threadIdx.x]) : 0.f;
+    const int r = ly + 8 * q;
+    const int yy = y0 + r, xx = x0 + lx;
+    bv[q] = (xx < d.nx && yy < d.ny) ? A_ADD(bA[d.a(xx, yy, z)], tile[r][lx]) : 0.f;
   }
   __syncthreads();
-  const float thr = (mode == 0 && thr_ptr) ? *thr_ptr : thr_value;
   #pragma unroll
   for (int q = 0; q < 4; q++) {
-    const int r = threadIdx.y + 8 * q;
+    const int r = ly + 8 * q;
     {
-      const int xx = x0 + r, yy = y0 + threadIdx.x;
+      const int xx = x0 + r, yy = y0 + lx;
       if (xx < d.nx && yy < d.ny) bT[d.t(xx, yy, z)] = 0.f;
     }
-    const int yy = y0 + r, xx = x0 + threadIdx.x;
+    const int yy = y0 + r, xx = x0 + lx;
     if (xx < d.nx && yy < d.ny) {
       bA[d.a(xx, yy, z)] = 0.f;
       const int64_t i = base + (int64_t)yy * d.nx + xx;
@@ -1022,6 +1006,219 @@ __global__ void __launch_bounds__(256) k_pad_reduce(PadDims d, float* __restrict
       }
     }
   }
+}
+
+__global__ void __launch_bounds__(256) k_pad_reduce(PadDims d, float* __restrict__ bA, float* __restrict__ bT,
+                                                    int mode, float* __restrict__ x, float* __restrict__ bp,
+                                                    const float* __restrict__ sens, const float* __restrict__ thr_ptr,
+                                                    float thr_value, int ge) {
+  __shared__ float tile[32][33];
+  const float thr = (mode == 0 && thr_ptr) ? *thr_ptr : thr_value;
+  pad_reduce_tile(d, bA, bT, mode, x, bp, sens, thr, ge, blockIdx.x * 32, blockIdx.y * 32, blockIdx.z, threadIdx.x,
+                  threadIdx.y, tile);
+}
+
+// ---- batched reconstructions: one step for many jobs ----------------------------
+// Before the walk: every job's image into its padded copies, and the FP64
+// partial -x . gimg of every tile (the likelihood's sum over the bins the
+// walk leaves out).  One block per tile; tiles of a job are consecutive.
+__global__ void __launch_bounds__(256) k_multi_copy(const MultiVox* __restrict__ jobs, int njobs,
+                                                    double* __restrict__ tile_partials) {
+  __shared__ float tile[32][33];
+  __shared__ int sj;
+  if (threadIdx.x == 0) sj = find_entry(jobs, njobs, blockIdx.x, [](const MultiVox& j) { return j.tile_begin; });
+  __syncthreads();
+  const MultiVox& J = jobs[sj];
+  const int64_t tl = (int64_t)blockIdx.x - J.tile_begin;
+  const int tx = (int)(tl % J.tiles_x);
+  const int64_t q = tl / J.tiles_x;
+  const int ty = (int)(q % J.tiles_y), z = (int)(q / J.tiles_y);
+  const PadDims d{J.g.nx, J.g.ny, J.g.nz};
+  const double dot = pad_copy_tile(d, J.x, J.pad.pA, J.pad.pT, J.gimg, tx * 32, ty * 32, z, threadIdx.x & 31,
+                                   threadIdx.x >> 5, tile);
+  const double sum = block_sum(dot);
+  if (threadIdx.x == 0) tile_partials[blockIdx.x] = -sum;
+}
+
+// The walk of a batched step: persistent warps take the next chunk of 32
+// entries of the concatenated lists of all segments, find its segment, and
+// run the fused pass on each listed bin (geometry form of the likelihood: a
+// walked bin adds m log e).  One FP64 partial per chunk, as in
+// k_em_pass_persist.
+__global__ void __launch_bounds__(kBlock, kMultiMinBlocks) k_em_multi(const MultiSeg* __restrict__ segs, int nseg,
+                                                                     int64_t nchunks,
+                                                                     unsigned long long* __restrict__ counter,
+                                                                     double* __restrict__ partials) {
+  // Each warp keeps its chunk's segment in shared memory (the walk reads the
+  // geometry from there instead of holding it in registers).
+  static_assert(sizeof(MultiSeg) % 4 == 0 && sizeof(MultiSeg) <= 64 * 4, "segment copy");
+  __shared__ MultiSeg seg_s[kBlock / 32];
+  const int lane = threadIdx.x & 31;
+  MultiSeg* S = seg_s + (threadIdx.x >> 5);
+  int cur = -1;
+  for (;;) {
+    unsigned long long c = 0;
+    if (lane == 0) c = atomicAdd(counter, 1ULL);
+    c = __shfl_sync(0xffffffffu, c, 0);
+    if ((int64_t)c >= nchunks) break;
+    const int k = find_entry(segs, nseg, (int64_t)c, [](const MultiSeg& e) { return e.chunk_begin; });
+    if (k != cur) {
+      __syncwarp();
+      const int* src = reinterpret_cast<const int*>(segs + k);
+      int* dst = reinterpret_cast<int*>(S);
+      for (int i = lane; i < (int)(sizeof(MultiSeg) / 4); i += 32) dst[i] = __ldg(src + i);
+      __syncwarp();
+      cur = k;
+    }
+    const int64_t item = ((int64_t)c - S->chunk_begin) * 32 + lane;
+    double term = 0.0;
+    if (item < S->n_list) {
+      const BinPos p = decode((int64_t)__ldg(S->list + item), S->t, S->s);
+      const int64_t ci = ((int64_t)p.g * S->t.n_proj + p.a) * S->t.n_r + p.l;
+      const float m = load_count_any(S->counts, S->counts_dtype, ci);
+      if (m != 0.f) term = em_bin_pad<kListGatherUnroll>(S->g, S->t, p, m, ci, S->add, S->pad, S->back, 2);
+    }
+    #pragma unroll
+    for (int o = 16; o > 0; o >>= 1) term += __shfl_down_sync(0xffffffffu, term, o);
+    if (lane == 0) partials[c] = term;
+  }
+}
+
+// One block per job: its likelihood, the fixed-order sum of its chunk
+// partials and its tile partials, minus its additive sum.
+__global__ void __launch_bounds__(256) k_multi_sum(const MultiVox* __restrict__ jobs,
+                                                   const double* __restrict__ chunk_partials,
+                                                   const double* __restrict__ tile_partials) {
+  const MultiVox& J = jobs[blockIdx.x];
+  const int64_t ntiles = (int64_t)J.tiles_x * J.tiles_y * J.g.nz;
+  double v = 0.0;
+  for (int64_t i = threadIdx.x; i < J.n_chunks; i += blockDim.x) v += chunk_partials[J.chunk_begin + i];
+  for (int64_t i = threadIdx.x; i < ntiles; i += blockDim.x) v += tile_partials[J.tile_begin + i];
+  const double s = block_sum(v);
+  if (threadIdx.x == 0 && J.lik) *J.lik = s - J.zero_add;
+}
+
+// After the walk: the EM update of every job with `update` from its padded
+// backprojection pair (threshold 0, rule ge), the pair cleared.
+__global__ void __launch_bounds__(256) k_multi_update(const MultiVox* __restrict__ jobs, int njobs) {
+  __shared__ float tile[32][33];
+  __shared__ int sj;
+  if (threadIdx.x == 0) sj = find_entry(jobs, njobs, blockIdx.x, [](const MultiVox& j) { return j.tile_begin; });
+  __syncthreads();
+  const MultiVox& J = jobs[sj];
+  if (!J.update) return;
+  const int64_t tl = (int64_t)blockIdx.x - J.tile_begin;
+  const int tx = (int)(tl % J.tiles_x);
+  const int64_t q = tl / J.tiles_x;
+  const int ty = (int)(q % J.tiles_y), z = (int)(q / J.tiles_y);
+  const PadDims d{J.g.nx, J.g.ny, J.g.nz};
+  pad_reduce_tile(d, J.pad.bA, J.pad.bT, 0, J.x, nullptr, J.sens, 0.f, J.ge, tx * 32, ty * 32, z, threadIdx.x & 31,
+                  threadIdx.x >> 5, tile);
+}
+
+// per_angle[a] += A_a^T 1 (Backproject of ones, SiddonProjector.cpp:444-568)
+// for every angle a, into padded images (PadBuffers' border and layouts):
+// angle a's image is [z][x][y] when tr[a] (its rays run mostly along x), else
+// [z][y][x], so that the 32 parallel rays of a warp scatter into neighbouring
+// addresses.  Persistent warps take 32-bin chunks in angle order (angle,
+// sinogram, r): the warps write one angle's image at a time and it stays in
+// L2.  Border voxels receive the scatter of guarded walks (see
+// siddon3_gather_pad); nothing reads them.
+__global__ void __launch_bounds__(kBlock) k_scatter_angles(ImgGeom g, LorTable t, const uint8_t* __restrict__ tr_of,
+                                                           float* __restrict__ per_angle, unsigned lim,
+                                                           unsigned long long* __restrict__ counter) {
+  const int lane = threadIdx.x & 31;
+  const int64_t per_a = (int64_t)t.n_sinos * t.n_r;
+  const int64_t total = per_a * t.n_proj;
+  const int64_t nchunks = (total + 31) >> 5;
+  const int px = g.nx + 2 * kPad, py = g.ny + 2 * kPad;
+  for (;;) {
+    unsigned long long c = 0;
+    if (lane == 0) c = atomicAdd(counter, 1ULL);
+    c = __shfl_sync(0xffffffffu, c, 0);
+    if ((int64_t)c >= nchunks) break;
+    const int64_t b = (int64_t)c * 32 + lane;
+    if (b >= total) continue;
+    const int a = (int)(b / per_a);
+    const int64_t rem = b - (int64_t)a * per_a;
+    const int gs = (int)(rem / t.n_r);
+    const int l = (int)(rem - (int64_t)gs * t.n_r);
+    const float4 L = t.lor[(int64_t)a * t.n_r + l];
+    const float2 z = t.z[t.g0 + gs];
+    const bool tr = __ldg(tr_of + a) != 0;
+    Walk3 w;
+    siddon3_setup(L.x, L.y, z.x, A_SUB(L.z, L.x), A_SUB(L.w, L.y), A_SUB(z.y, z.x), g, w);
+    siddon3_scatter_pad(w, g, tr ? py : 1, tr ? 1 : px, px * py, lim, 1.f, per_angle + (int64_t)a * lim);
+  }
+}
+
+// out[s] ([z][y][x], unpadded) = the sum over a = s, s + nsub, ... < n_proj of
+// the interiors of the padded per-angle images (layouts as k_scatter_angles),
+// added in increasing a.  One block per 32 x 32 tile of a slice and subset.
+__global__ void __launch_bounds__(256) k_sum_angles(const float* __restrict__ per_angle, const uint8_t* __restrict__ tr_of,
+                                                    unsigned lim, int n_proj, ImgGeom g, int nsub,
+                                                    float* __restrict__ out) {
+  __shared__ float tile[32][33];
+  const int s = blockIdx.y;
+  const int tiles_x = (g.nx + 31) / 32, tiles_y = (g.ny + 31) / 32;
+  const int tx = blockIdx.x % tiles_x, ty = (blockIdx.x / tiles_x) % tiles_y, z = blockIdx.x / (tiles_x * tiles_y);
+  const int x0 = tx * 32, y0 = ty * 32, lx = threadIdx.x & 31, ly = threadIdx.x >> 5;
+  const PadDims d{g.nx, g.ny, g.nz};
+  float acc[4] = {0.f, 0.f, 0.f, 0.f};
+  for (int a = s; a < n_proj; a += nsub) {
+    const float* P = per_angle + (int64_t)a * lim;
+    if (__ldg(tr_of + a)) {
+      __syncthreads();
+      for (int r = ly; r < 32; r += 8) {  // transposed image, read along y
+        const int xx = x0 + r, yy = y0 + lx;
+        tile[lx][r] = (xx < d.nx && yy < d.ny) ? __ldg(P + d.t(xx, yy, z)) : 0.f;
+      }
+      __syncthreads();
+      #pragma unroll
+      for (int q = 0; q < 4; q++) acc[q] = A_ADD(acc[q], tile[ly + 8 * q][lx]);
+    } else {
+      #pragma unroll
+      for (int q = 0; q < 4; q++) {
+        const int xx = x0 + lx, yy = y0 + ly + 8 * q;
+        acc[q] = A_ADD(acc[q], (xx < d.nx && yy < d.ny) ? __ldg(P + d.a(xx, yy, z)) : 0.f);
+      }
+    }
+  }
+  const int64_t nvox = (int64_t)g.nx * g.ny * g.nz;
+  #pragma unroll
+  for (int q = 0; q < 4; q++) {
+    const int xx = x0 + lx, yy = y0 + ly + 8 * q;
+    if (xx < d.nx && yy < d.ny) out[(int64_t)s * nvox + ((int64_t)z * d.ny + yy) * d.nx + xx] = acc[q];
+  }
+}
+
+// out[s] = sum over images a = s, s + nsub, ... < n_img of img[a] (unpadded
+// images of nvox), added in increasing a.
+__global__ void __launch_bounds__(kBlock) k_sum_images(const float* __restrict__ img, int n_img, int64_t nvox,
+                                                       int nsub, float* __restrict__ out) {
+  const int s = blockIdx.y;
+  for (int64_t v = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; v < nvox; v += (int64_t)gridDim.x * blockDim.x) {
+    float acc = 0.f;
+    for (int a = s; a < n_img; a += nsub) acc = A_ADD(acc, __ldg(img + (int64_t)a * nvox + v));
+    out[(int64_t)s * nvox + v] = acc;
+  }
+}
+
+// out[s] = sum of the additive term over subset s's bins (whole-sinogram
+// layout), one block per subset, FP64, fixed order.
+__global__ void __launch_bounds__(kBlock) k_subset_sums(LorTable t, int nsub, const float* __restrict__ add,
+                                                        double* __restrict__ out) {
+  SubsetSel s;
+  s.subset = blockIdx.x; s.nsub = nsub; s.nk = 0;
+  for (int a = s.subset; a < t.n_proj; a += nsub) s.nk++;
+  const int64_t total = (int64_t)t.n_sinos * s.nk * t.n_r;
+  double v = 0.0;
+  for (int64_t b = threadIdx.x; b < total; b += blockDim.x) {
+    const BinPos p = decode(b, t, s);
+    v += (double)__ldg(add + ((int64_t)p.g * t.n_proj + p.a) * t.n_r + p.l);
+  }
+  const double r = block_sum(v);
+  if (threadIdx.x == 0) out[blockIdx.x] = r;
 }
 
 inline unsigned grid_for(int64_t total) { return (unsigned)((total + kBlock - 1) / kBlock); }
@@ -1430,20 +1627,114 @@ cudaError_t launch_fill(int64_t n, float* x, float v, cudaStream_t st) {
   return cudaGetLastError();
 }
 
-cudaError_t launch_em_batch(const EmJob* d_jobs, const EmJob* h_jobs, int njobs, int64_t nblocks, double* partials,
-                            cudaStream_t st) {
-  (void)h_jobs;
-  if (njobs == 0 || nblocks == 0) return cudaSuccess;
-  k_em_batch<<<(unsigned)nblocks, kBlock, 0, st>>>(d_jobs, njobs, partials);
-  cudaError_t e = cudaGetLastError();
-  if (e != cudaSuccess) return e;
-  k_sum_batch<<<njobs, kBlock, 0, st>>>(d_jobs, partials);
+// Persistent grid of k_em_multi: as many 256-thread blocks as fit on the
+// current device's SMs (its shared-memory carveout fitted to that many).
+cudaError_t multi_walk_grid(int* blocks) {
+  int dev = 0, sms = 0, per_sm = 0;
+  cudaError_t e;
+  if ((e = fit_carveout((const void*)k_em_multi, kBlock, 0)) != cudaSuccess) return e;
+  if ((e = cudaGetDevice(&dev)) != cudaSuccess) return e;
+  if ((e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev)) != cudaSuccess) return e;
+  if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_em_multi, kBlock, 0)) != cudaSuccess) return e;
+  *blocks = (per_sm < 1 ? 1 : per_sm) * sms;
+  return cudaSuccess;
+}
+
+cudaError_t launch_multi_step(const MultiVox* d_vox, int n_vox, int64_t total_tiles, const MultiSeg* d_segs,
+                              int n_segs, int64_t total_chunks, int walk_blocks, unsigned long long* counter,
+                              double* chunk_partials, double* tile_partials, cudaStream_t st) {
+  if (n_vox == 0 || total_tiles == 0) return cudaSuccess;
+  cudaError_t e;
+  k_multi_copy<<<(unsigned)total_tiles, 256, 0, st>>>(d_vox, n_vox, tile_partials);
+  if ((e = cudaGetLastError()) != cudaSuccess) return e;
+  if (total_chunks > 0 && n_segs > 0) {
+    if ((e = cudaMemsetAsync(counter, 0, sizeof(unsigned long long), st)) != cudaSuccess) return e;
+    const int64_t need = (total_chunks * 32 + kBlock - 1) / kBlock;
+    const unsigned grid = (unsigned)(need < walk_blocks ? need : walk_blocks);
+    k_em_multi<<<grid, kBlock, 0, st>>>(d_segs, n_segs, total_chunks, counter, chunk_partials);
+    if ((e = cudaGetLastError()) != cudaSuccess) return e;
+  }
+  k_multi_sum<<<n_vox, 256, 0, st>>>(d_vox, chunk_partials, tile_partials);
+  if ((e = cudaGetLastError()) != cudaSuccess) return e;
+  k_multi_update<<<(unsigned)total_tiles, 256, 0, st>>>(d_vox, n_vox);
   return cudaGetLastError();
 }
 
-cudaError_t launch_update_batch(const UpdJob* d_jobs, int njobs, int64_t nblocks, cudaStream_t st) {
-  if (njobs == 0 || nblocks == 0) return cudaSuccess;
-  k_update_batch<<<(unsigned)nblocks, kBlock, 0, st>>>(d_jobs, njobs);
+cudaError_t launch_nz_count(const LorTable& t, SubsetSel s, const void* counts, int counts_dtype, int64_t total,
+                            int* tiles, int* n_list, cudaStream_t st) {
+  if (total <= 0) return cudaMemsetAsync(n_list, 0, sizeof(int), st);
+  const unsigned n_tiles = (unsigned)((total + kNzTile - 1) / kNzTile);
+  switch (counts_dtype) {
+    case APIRL_F32: k_nz_tiles<float><<<n_tiles, kNzBlock, 0, st>>>(t, s, (const float*)counts, 0, total, tiles); break;
+    case APIRL_U32:
+      k_nz_tiles<uint32_t><<<n_tiles, kNzBlock, 0, st>>>(t, s, (const uint32_t*)counts, 0, total, tiles);
+      break;
+    case APIRL_U16:
+      k_nz_tiles<uint16_t><<<n_tiles, kNzBlock, 0, st>>>(t, s, (const uint16_t*)counts, 0, total, tiles);
+      break;
+    default: return cudaErrorInvalidValue;
+  }
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return e;
+  k_nz_scan<<<1, 1024, 0, st>>>(tiles, (int)n_tiles, n_list);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_nz_write(const LorTable& t, SubsetSel s, const void* counts, int counts_dtype, int64_t total,
+                            const int* tiles, int* list, cudaStream_t st) {
+  if (total <= 0) return cudaSuccess;
+  const unsigned n_tiles = (unsigned)((total + kNzTile - 1) / kNzTile);
+  switch (counts_dtype) {
+    case APIRL_F32:
+      k_nz_write<float><<<n_tiles, kNzBlock, 0, st>>>(t, s, (const float*)counts, 0, total, tiles, list);
+      break;
+    case APIRL_U32:
+      k_nz_write<uint32_t><<<n_tiles, kNzBlock, 0, st>>>(t, s, (const uint32_t*)counts, 0, total, tiles, list);
+      break;
+    case APIRL_U16:
+      k_nz_write<uint16_t><<<n_tiles, kNzBlock, 0, st>>>(t, s, (const uint16_t*)counts, 0, total, tiles, list);
+      break;
+    default: return cudaErrorInvalidValue;
+  }
+  return cudaGetLastError();
+}
+
+cudaError_t launch_scatter_angles(const ImgGeom& g, const LorTable& t, const uint8_t* tr_of, float* per_angle,
+                                  unsigned lim, unsigned long long* counter, cudaStream_t st) {
+  int dev = 0, sms = 0, per_sm = 0;
+  cudaError_t e;
+  if ((e = cudaGetDevice(&dev)) != cudaSuccess) return e;
+  if ((e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev)) != cudaSuccess) return e;
+  if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_scatter_angles, kBlock, 0)) != cudaSuccess)
+    return e;
+  if ((e = cudaMemsetAsync(counter, 0, sizeof(unsigned long long), st)) != cudaSuccess) return e;
+  const int64_t total = (int64_t)t.n_sinos * t.n_r * t.n_proj;
+  const int64_t need = (total + kBlock - 1) / kBlock;
+  const int64_t resident = (int64_t)(per_sm < 1 ? 1 : per_sm) * sms;
+  k_scatter_angles<<<(unsigned)(need < resident ? need : resident), kBlock, 0, st>>>(g, t, tr_of, per_angle, lim,
+                                                                                    counter);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_sum_angles(const float* per_angle, const uint8_t* tr_of, unsigned lim, int n_proj,
+                              const ImgGeom& g, int nsub, float* out, cudaStream_t st) {
+  if (nsub <= 0) return cudaSuccess;
+  const int64_t tiles = multi_tiles(g);
+  k_sum_angles<<<dim3((unsigned)tiles, (unsigned)nsub), 256, 0, st>>>(per_angle, tr_of, lim, n_proj, g, nsub, out);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_sum_images(const float* img, int n_img, int64_t nvox, int nsub, float* out, cudaStream_t st) {
+  if (nvox == 0 || nsub <= 0) return cudaSuccess;
+  int64_t bx = (nvox + kBlock - 1) / kBlock;
+  if (bx > 2048) bx = 2048;
+  k_sum_images<<<dim3((unsigned)bx, (unsigned)nsub), kBlock, 0, st>>>(img, n_img, nvox, nsub, out);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_subset_sums(const LorTable& t, int nsub, const float* add, double* out, cudaStream_t st) {
+  if (nsub <= 0) return cudaSuccess;
+  k_subset_sums<<<nsub, kBlock, 0, st>>>(t, nsub, add, out);
   return cudaGetLastError();
 }
 

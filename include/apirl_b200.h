@@ -447,13 +447,19 @@ apirl_status apirl_mlem_2d_ex(const apirl_image_geom* img, const apirl_sino2d_ge
 
 /* ---- batched and served reconstructions ---------------------------------
  * Many independent 3D OSEM jobs (OsemSinogram3d::Reconstruct each,
- * recon/src/OsemSinogram3d.cpp:36-325) of different geometries advance
- * together: every apirl_batch_step runs one pass of every active job in one
- * launch of the fused kernel and one of the pixel update.  Jobs are admitted
- * in submission order while their device footprint fits the budget, with
- * smaller jobs allowed past one that does not fit; finished jobs release their
- * memory at once.  No counterpart in the reference, which reconstructs one
- * sinogram per process. */
+ * recon/src/OsemSinogram3d.cpp:36-325, pixel update sens >= 0 as there) of
+ * different geometries advance together: every apirl_batch_step runs one pass
+ * of every running job (or its final likelihood) in one persistent walk over
+ * all their lists of bins with counts, with the image copies, likelihood sums
+ * and updates of all jobs in one launch each.  Jobs are admitted in
+ * submission order while their device footprint fits the budget, smaller
+ * jobs allowed past one that does not fit; each job's counts are uploaded by
+ * a worker thread while other jobs run.  Device memory comes from a pool the
+ * batch keeps; finished jobs return theirs to it.  Jobs of one image and
+ * sinogram geometry share its tables and A_a^T 1 of every angle (kept, within
+ * the budget, while no job needs the room), from which any subset split's
+ * sensitivity follows without another walk.  No counterpart in the
+ * reference, which reconstructs one sinogram per process. */
 typedef struct apirl_batch apirl_batch;
 typedef struct apirl_job_desc {
   apirl_image_geom img;
@@ -465,17 +471,21 @@ typedef struct apirl_job_desc {
   const float* h_init;     /* initial image or NULL (ones) */
   int iters, nsubsets;
 } apirl_job_desc;
-/* Device bytes a job holds while active. */
+/* Device bytes a job holds while active (its lists of bins with counts at
+ * their largest, and its subset split's sensitivity images, included). */
 int64_t apirl_job_footprint(const apirl_job_desc* job);
 apirl_status apirl_batch_create(int device, int64_t hbm_budget_bytes, apirl_batch** out);
 void apirl_batch_destroy(apirl_batch* b);
-/* Queues a job; job ids start at 0.  The host arrays are read when the job
- * is admitted (copied to the device), so they must stay valid until then
- * (at the latest until apirl_batch_result reports it done). */
+/* Queues a job; job ids start at 0.  The host arrays are read after the job
+ * is admitted (copied to the device by the batch's worker thread), so they
+ * must stay valid until apirl_batch_result reports it done. */
 apirl_status apirl_batch_submit(apirl_batch* b, const apirl_job_desc* job, int64_t* job_id);
-/* Admits what fits, computes the sensitivity images of newly admitted jobs,
- * runs one pass of every active job, retires finished jobs; returns when the
- * step is done on the device.  Counts after the step go to *n_active,
+/* Admits what fits, moves each job whose previous stage has finished on the
+ * device to its next one (upload -> lists of bins with counts and
+ * sensitivity -> passes -> final likelihood -> result), launches one pass of
+ * every running job, retires finished jobs.  Returns once the work is queued
+ * (at most two steps are in flight; when nothing could be launched it waits
+ * for the oldest outstanding stage).  Counts after the step go to *n_active,
  * *n_queued (either may be NULL). */
 apirl_status apirl_batch_step(apirl_batch* b, int* n_active, int* n_queued);
 /* *done = 1 and the outputs are filled (image, iters*nsubsets+1 likelihood

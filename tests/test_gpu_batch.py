@@ -109,3 +109,51 @@ def test_batch_big_job_matches_solo():
         assert np.array_equal(np.isfinite(img), finite), j.tag
         assert rel(img[finite], solo[finite]) <= 1e-4, j.tag
         assert np.allclose(lik[:-1], solo_lik[:-1], rtol=1e-6), j.tag
+
+
+def test_batch_jobs_with_factors_match_solo():
+    """A job with a multiplicative sinogram (its own sensitivity A_s^T a,
+    beside the shared G_s of the likelihood) and one with an additive sinogram
+    (the likelihood's additive sums per subset), next to a plain one: each
+    equals its solo run through apirl_osem_3d."""
+    if not torch.cuda.is_available():
+        pytest.skip("no CUDA device")
+    specs = [dict(n=32, z=9, seed=11, counts=2e5, iters=2, nsubsets=3),
+             dict(n=32, z=9, seed=12, counts=2e5, iters=2, nsubsets=4),
+             dict(n=32, z=1, seed=13, counts=5e4, iters=3, nsubsets=5)]
+    jobs = make_jobs(specs)
+    rng = np.random.default_rng(14)
+    jobs[0].mult = (rng.random(jobs[0].counts.size, dtype=np.float32) * 0.5 + 0.5).astype(np.float32)
+    jobs[1].add = (rng.random(jobs[1].counts.size, dtype=np.float32) * 0.1).astype(np.float32)
+    b = Batch(0, budget_bytes=8 << 30)
+    res = b.run_all(jobs)
+    b.close()
+    for j, (img, lik) in zip(jobs, res):
+        solo, solo_lik, _ = ap.osem_3d(j.image_geom, j.sino_geom, j.counts.astype(np.float32),
+                                       np.ones(j.image_geom.n_voxels, np.float32), j.iters, j.nsubsets,
+                                       mult=j.mult, add=j.add)
+        finite = np.isfinite(solo)
+        assert np.array_equal(np.isfinite(img), finite), j.tag
+        assert rel(img[finite], solo[finite]) <= 1e-4, j.tag
+        assert np.allclose(lik, solo_lik, rtol=1e-6), j.tag
+
+
+def test_batch_shares_geometry_between_subset_splits():
+    """Jobs of one geometry with different subset counts (their sensitivity
+    images summed from the shared per-angle images) and the same job twice:
+    each equals its solo run."""
+    if not torch.cuda.is_available():
+        pytest.skip("no CUDA device")
+    specs = [dict(n=48, z=9, seed=21 + k, counts=3e5, iters=2, nsubsets=ns) for k, ns in enumerate((3, 5, 7, 5))]
+    jobs = make_jobs(specs)
+    b = Batch(0, budget_bytes=8 << 30)
+    res = b.run_all(jobs)
+    res2 = b.run_all(jobs[:2])  # the same geometry again, images already cached
+    b.close()
+    for j, (img, lik) in zip(jobs + jobs[:2], res + res2):
+        solo, solo_lik, _ = ap.osem_3d(j.image_geom, j.sino_geom, j.counts.astype(np.float32),
+                                       np.ones(j.image_geom.n_voxels, np.float32), j.iters, j.nsubsets)
+        finite = np.isfinite(solo)
+        assert np.array_equal(np.isfinite(img), finite), j.tag
+        assert rel(img[finite], solo[finite]) <= 1e-4, j.tag
+        assert np.allclose(lik, solo_lik, rtol=1e-6), j.tag
