@@ -22,8 +22,12 @@ APIRL_OPT_KERNEL_TIMING = 2
 APIRL_OPT_EM_BLOCK = 3
 APIRL_OPT_PERSISTENT = 4
 APIRL_OPT_SPARSE_IMAGE = 5
+APIRL_OPT_ACCUMULATE = 6
 APIRL_SPARSE_ZERO_COUNT = 0
 APIRL_SPARSE_GEOMETRY = 1
+APIRL_ACC_ATOMIC = 0
+APIRL_ACC_WARP = 1
+APIRL_ACC_COMPENSATED = 2
 
 APIRL_ALPHA_F32 = 0
 APIRL_ALPHA_F64 = 1

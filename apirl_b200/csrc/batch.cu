@@ -435,12 +435,6 @@ GeomKey key_of(const Job& j) {
   return k;
 }
 
-int64_t cache_bytes(const Geom& g) {
-  int64_t b = g.per_angle ? g.per_angle_bytes() : 0;
-  for (auto& kv : g.sets) b += align256((int64_t)kv.first * g.nvox * 4);
-  return b;
-}
-
 // Frees shared images no active job holds, least recently used first, until
 // `need` more bytes fit the budget (or nothing is left to free).
 void evict(apirl_batch* b, int64_t need) {

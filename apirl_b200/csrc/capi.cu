@@ -91,6 +91,16 @@ struct DeviceScope {
     if (apirl_status pend_ = apirl_internal_pending()) return pend_; \
   } while (0)
 
+// The accumulation form set on a projector applies to its padded passes; a
+// projector that no longer takes them (FP64 walk, sampling, dual layout off)
+// refuses to backproject with another form than plain atomics.
+apirl_status check_acc(const apirl_projector* p) {
+  const bool dual = p->is3d && p->dual_layout && !p->pg.enabled && p->pad.pA && !p->t.lor_s;
+  if (p->pad.acc != APIRL_ACC_ATOMIC && !dual)
+    return fail(APIRL_ERR_NOT_SUPPORTED, "the accumulation form needs the padded 3D layouts");
+  return APIRL_OK;
+}
+
 bool valid_img(const apirl_image_geom* g) {
   return g && g->nx > 0 && g->ny > 0 && g->nz > 0 && g->dx > 0 && g->dy > 0 && g->dz > 0 &&
          (int64_t)g->nx * g->ny * g->nz < (int64_t)1 << 31;
@@ -344,6 +354,8 @@ void apirl_projector_destroy(apirl_projector* p) {
   cudaFree(p->pad.pT);
   cudaFree(p->pad.bA);
   cudaFree(p->pad.bT);
+  cudaFree(p->pad.eA);
+  cudaFree(p->pad.eT);
   if (p->ev0) cudaEventDestroy(p->ev0);
   if (p->ev1) cudaEventDestroy(p->ev1);
   if (p->copy_ready) cudaEventDestroy(p->copy_ready);
@@ -492,6 +504,7 @@ apirl_status apirl_backproject(apirl_projector* p, const float* d_sino, float* d
                                void* stream) {
   apirl_status st = check_subset(p, subset, nsubsets);
   if (st) return st;
+  if ((st = check_acc(p))) return st;
   if (!d_image || !d_sino) return fail(APIRL_ERR_INVALID, "null image or sinogram");
   DEVICE_SCOPE(p->device);
   CK(apirl::backproject_sino(p, make_subset(p, subset, nsubsets), d_sino, 0, d_image, (cudaStream_t)stream));
@@ -501,6 +514,7 @@ apirl_status apirl_backproject(apirl_projector* p, const float* d_sino, float* d
 apirl_status apirl_backproject_ones(apirl_projector* p, float* d_image, int subset, int nsubsets, void* stream) {
   apirl_status st = check_subset(p, subset, nsubsets);
   if (st) return st;
+  if ((st = check_acc(p))) return st;
   if (!d_image) return fail(APIRL_ERR_INVALID, "null image");
   DEVICE_SCOPE(p->device);
   CK(apirl::backproject_sino(p, make_subset(p, subset, nsubsets), nullptr, 2, d_image, (cudaStream_t)stream));
@@ -607,6 +621,8 @@ bool use_dual(const apirl_projector* p) {
 apirl_status fused(apirl_projector* p, SubsetSel ss, const void* d_counts, int dtype, int packed, const float* d_add,
                    const float* d_x, float* d_bp, bool dual, double* d_lik, cudaStream_t s,
                    const float* d_zimg = nullptr, const double* d_zero_add = nullptr) {
+  if (p->pad.acc != APIRL_ACC_ATOMIC && !(dual && p->persistent))
+    return fail(APIRL_ERR_NOT_SUPPORTED, "the accumulation form needs the persistent pass over the padded layouts");
   if (p->timing) {
     if (!p->ev0) {
       CK(cudaEventCreate(&p->ev0));
@@ -772,6 +788,23 @@ apirl_status apirl_projector_set_option(apirl_projector* p, int option, int valu
         return fail(APIRL_ERR_INVALID, "unknown sparse image kind %d", value);
       p->sparse_image = value;
       return APIRL_OK;
+    case APIRL_OPT_ACCUMULATE: {
+      if (value != APIRL_ACC_ATOMIC && value != APIRL_ACC_WARP && value != APIRL_ACC_COMPENSATED)
+        return fail(APIRL_ERR_INVALID, "unknown accumulation form %d", value);
+      if (value != APIRL_ACC_ATOMIC && !use_dual(p))  // use_dual: the padded layouts are taken
+        return fail(APIRL_ERR_NOT_SUPPORTED, "accumulation forms need the padded 3D layouts (3D, float walk, one ray "
+                                             "per bin, dual layout)");
+      if (value == APIRL_ACC_COMPENSATED && !p->pad.eA) {
+        DEVICE_SCOPE(p->device);
+        const size_t pv = (size_t)p->pad.lim;
+        CK(cudaMalloc(&p->pad.eA, pv * sizeof(float)));
+        CK(cudaMalloc(&p->pad.eT, pv * sizeof(float)));
+        CK(cudaMemset(p->pad.eA, 0, pv * sizeof(float)));
+        CK(cudaMemset(p->pad.eT, 0, pv * sizeof(float)));
+      }
+      p->pad.acc = value;
+      return APIRL_OK;
+    }
     case APIRL_OPT_EM_BLOCK:
       if (value < 32 || value > 256 || value % 32) return fail(APIRL_ERR_INVALID, "block size must be 32..256, x32");
       p->em_block = value;

@@ -100,6 +100,11 @@ struct PadBuffers {
   float* bA = nullptr;
   float* bT = nullptr;
   unsigned lim = 0;
+  // How scatters into bA / bT accumulate (APIRL_ACC_*); eA / eT: the
+  // rounding errors of the compensated form, same layouts.
+  int acc = 0;
+  float* eA = nullptr;
+  float* eT = nullptr;
 };
 // Bins per tile of the list building (one block each).
 constexpr int kNzTile = 2048;

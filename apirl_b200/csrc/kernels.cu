@@ -460,6 +460,7 @@ __global__ void __launch_bounds__(kBlock) k_em_pass_rays(ImgGeom g, LorTable t, 
 // (SiddonProjector.cpp:496).
 // b2A / b2T set: the walk also scatters seg into that second padded pair,
 // for every bin (the unweighted image A_s^T 1 beside A_s^T v).
+template <int ACC>
 __global__ void __launch_bounds__(kBlock, kPersistMinBlocks) k_scatter_persist(
     ImgGeom g, LorTable t, SubsetSel s, const float* __restrict__ vin, int vin_mode, PadBuffers pad, int64_t total,
     unsigned long long* __restrict__ chunk_counter, float* __restrict__ b2A, float* __restrict__ b2T) {
@@ -486,7 +487,8 @@ __global__ void __launch_bounds__(kBlock, kPersistMinBlocks) k_scatter_persist(
         if (b2A)
           siddon3_scatter2_pad(w, g, tr ? py : 1, tr ? 1 : px, uz, pad.lim, v, tr ? pad.bT : pad.bA, tr ? b2T : b2A);
         else
-          siddon3_scatter_pad(w, g, tr ? py : 1, tr ? 1 : px, uz, pad.lim, v, tr ? pad.bT : pad.bA);
+          siddon3_scatter_pad<ACC>(w, g, tr ? py : 1, tr ? 1 : px, uz, pad.lim, v, tr ? pad.bT : pad.bA,
+                                   tr ? pad.eT : pad.eA);
       }
     }
   }
@@ -609,7 +611,7 @@ __global__ void __launch_bounds__(kNzBlock) k_nz_write(LorTable t, SubsetSel s, 
 // the additive term, the likelihood term, the ratio m / e and the scatter of
 // seg * ratio into the matching padded backprojection.  ci: the bin's index
 // in the counts / additive layout.  Returns the likelihood term (lik_term).
-template <int U>
+template <int U, int ACC>
 __device__ __forceinline__ double em_bin_pad(const ImgGeom& g, const LorTable& t, const BinPos& p, float m,
                                              int64_t ci, const float* __restrict__ add, const PadBuffers& pad,
                                              int back, int skip_zero) {
@@ -631,7 +633,7 @@ __device__ __forceinline__ double em_bin_pad(const ImgGeom& g, const LorTable& t
     const float2 z2 = __ldcg(t.z + p.g);
     Walk3 w2;
     siddon3_setup(L2.x, L2.y, z2.x, A_SUB(L2.z, L2.x), A_SUB(L2.w, L2.y), A_SUB(z2.y, z2.x), g, w2);
-    siddon3_scatter_pad(w2, g, ux, uy, uz, pad.lim, r, tr ? pad.bT : pad.bA);
+    siddon3_scatter_pad<ACC>(w2, g, ux, uy, uz, pad.lim, r, tr ? pad.bT : pad.bA, tr ? pad.eT : pad.eA);
   }
   return term;
 }
@@ -642,7 +644,7 @@ __device__ __forceinline__ double em_bin_pad(const ImgGeom& g, const LorTable& t
 // full complement of warps until the end of the pass.  The bins of a chunk
 // are those of one warp in k_em_pass, and the chunk's likelihood partial goes
 // to partials[chunk]: results are identical to k_em_pass's.
-template <typename CT, bool LIST>
+template <typename CT, bool LIST, int ACC>
 __global__ void __launch_bounds__(kBlock, LIST ? kListMinBlocks : kPersistMinBlocks) k_em_pass_persist(
     ImgGeom g, LorTable t, SubsetSel s, const CT* __restrict__ counts, int counts_packed,
     const float* __restrict__ add, PadBuffers pad, int back, double* __restrict__ partials, int64_t total,
@@ -667,8 +669,8 @@ __global__ void __launch_bounds__(kBlock, LIST ? kListMinBlocks : kPersistMinBlo
       const int64_t ci = row * t.n_r + p.l;
       const float m = load_count<CT>(counts, ci);
       if (!(skip_zero && m == 0.f))
-        term = em_bin_pad<LIST ? kListGatherUnroll : APIRL_GATHER_UNROLL>(g, t, p, m, ci, add, pad, back,
-                                                                           skip_zero);
+        term = em_bin_pad<LIST ? kListGatherUnroll : APIRL_GATHER_UNROLL, ACC>(g, t, p, m, ci, add, pad, back,
+                                                                                skip_zero);
     }
     #pragma unroll
     for (int o = 16; o > 0; o >>= 1) term += __shfl_down_sync(0xffffffffu, term, o);
@@ -968,14 +970,20 @@ __global__ void __launch_bounds__(256) k_pad_copy(PadDims d, const float* __rest
 // loads come before the clearing stores (a store to an address whose load is
 // still in flight stalls the thread's later memory operations: clearing in
 // place made this kernel ~8x slower).
+// eA / eT (may be null): the compensated form's rounding errors of bA / bT,
+// folded in as (bA + eA) + (bT + eT) and cleared too.
 __device__ __forceinline__ void pad_reduce_tile(const PadDims& d, float* __restrict__ bA, float* __restrict__ bT,
                                                 int mode, float* __restrict__ x, float* __restrict__ bp,
                                                 const float* __restrict__ sens, float thr, int ge, int x0, int y0,
-                                                int z, int lx, int ly, float (*tile)[33]) {
+                                                int z, int lx, int ly, float (*tile)[33],
+                                                float* __restrict__ eA = nullptr, float* __restrict__ eT = nullptr) {
   const int64_t base = (int64_t)z * d.nx * d.ny;
   for (int r = ly; r < 32; r += 8) {  // transposed buffer, read along y
     const int xx = x0 + r, yy = y0 + lx;
-    if (xx < d.nx && yy < d.ny) tile[lx][r] = bT[d.t(xx, yy, z)];
+    if (xx < d.nx && yy < d.ny) {
+      const int64_t it = d.t(xx, yy, z);
+      tile[lx][r] = eT ? A_ADD(bT[it], eT[it]) : bT[it];
+    }
   }
   __syncthreads();
   float bv[4];
@@ -983,7 +991,12 @@ __device__ __forceinline__ void pad_reduce_tile(const PadDims& d, float* __restr
   for (int q = 0; q < 4; q++) {
     const int r = ly + 8 * q;
     const int yy = y0 + r, xx = x0 + lx;
-    bv[q] = (xx < d.nx && yy < d.ny) ? A_ADD(bA[d.a(xx, yy, z)], tile[r][lx]) : 0.f;
+    if (xx < d.nx && yy < d.ny) {
+      const int64_t ia = d.a(xx, yy, z);
+      bv[q] = A_ADD(eA ? A_ADD(bA[ia], eA[ia]) : bA[ia], tile[r][lx]);
+    } else {
+      bv[q] = 0.f;
+    }
   }
   __syncthreads();
   #pragma unroll
@@ -991,11 +1004,15 @@ __device__ __forceinline__ void pad_reduce_tile(const PadDims& d, float* __restr
     const int r = ly + 8 * q;
     {
       const int xx = x0 + r, yy = y0 + lx;
-      if (xx < d.nx && yy < d.ny) bT[d.t(xx, yy, z)] = 0.f;
+      if (xx < d.nx && yy < d.ny) {
+        bT[d.t(xx, yy, z)] = 0.f;
+        if (eT) eT[d.t(xx, yy, z)] = 0.f;
+      }
     }
     const int yy = y0 + r, xx = x0 + lx;
     if (xx < d.nx && yy < d.ny) {
       bA[d.a(xx, yy, z)] = 0.f;
+      if (eA) eA[d.a(xx, yy, z)] = 0.f;
       const int64_t i = base + (int64_t)yy * d.nx + xx;
       if (mode == 0) {
         const float sv = sens[i];
@@ -1011,11 +1028,12 @@ __device__ __forceinline__ void pad_reduce_tile(const PadDims& d, float* __restr
 __global__ void __launch_bounds__(256) k_pad_reduce(PadDims d, float* __restrict__ bA, float* __restrict__ bT,
                                                     int mode, float* __restrict__ x, float* __restrict__ bp,
                                                     const float* __restrict__ sens, const float* __restrict__ thr_ptr,
-                                                    float thr_value, int ge) {
+                                                    float thr_value, int ge, float* __restrict__ eA,
+                                                    float* __restrict__ eT) {
   __shared__ float tile[32][33];
   const float thr = (mode == 0 && thr_ptr) ? *thr_ptr : thr_value;
   pad_reduce_tile(d, bA, bT, mode, x, bp, sens, thr, ge, blockIdx.x * 32, blockIdx.y * 32, blockIdx.z, threadIdx.x,
-                  threadIdx.y, tile);
+                  threadIdx.y, tile, eA, eT);
 }
 
 // ---- batched reconstructions: one step for many jobs ----------------------------
@@ -1051,10 +1069,10 @@ __global__ void __launch_bounds__(kBlock, kMultiMinBlocks) k_em_multi(const Mult
                                                                      double* __restrict__ partials) {
   // Each warp keeps its chunk's segment in shared memory (the walk reads the
   // geometry from there instead of holding it in registers).
-  static_assert(sizeof(MultiSeg) % 4 == 0 && sizeof(MultiSeg) <= 64 * 4, "segment copy");
-  __shared__ MultiSeg seg_s[kBlock / 32];
+  static_assert(sizeof(MultiSeg) % 8 == 0 && sizeof(MultiSeg) <= 64 * 4, "segment copy");
+  __shared__ __align__(16) int seg_raw[kBlock / 32][sizeof(MultiSeg) / 4];
   const int lane = threadIdx.x & 31;
-  MultiSeg* S = seg_s + (threadIdx.x >> 5);
+  MultiSeg* S = reinterpret_cast<MultiSeg*>(seg_raw[threadIdx.x >> 5]);
   int cur = -1;
   for (;;) {
     unsigned long long c = 0;
@@ -1076,7 +1094,7 @@ __global__ void __launch_bounds__(kBlock, kMultiMinBlocks) k_em_multi(const Mult
       const BinPos p = decode((int64_t)__ldg(S->list + item), S->t, S->s);
       const int64_t ci = ((int64_t)p.g * S->t.n_proj + p.a) * S->t.n_r + p.l;
       const float m = load_count_any(S->counts, S->counts_dtype, ci);
-      if (m != 0.f) term = em_bin_pad<kListGatherUnroll>(S->g, S->t, p, m, ci, S->add, S->pad, S->back, 2);
+      if (m != 0.f) term = em_bin_pad<kListGatherUnroll, 0>(S->g, S->t, p, m, ci, S->add, S->pad, S->back, 2);
     }
     #pragma unroll
     for (int o = 16; o > 0; o >>= 1) term += __shfl_down_sync(0xffffffffu, term, o);
@@ -1306,14 +1324,24 @@ inline unsigned stream_grid(int64_t n) {
 
 }  // namespace
 
+// The persistent fused kernel for a counts type, list form and accumulation form.
+template <typename CT>
+const void* persist_kernel(bool list, int acc) {
+  if (list)
+    return acc == 1 ? (const void*)k_em_pass_persist<CT, true, 1>
+                    : acc == 2 ? (const void*)k_em_pass_persist<CT, true, 2> : (const void*)k_em_pass_persist<CT, true, 0>;
+  return acc == 1 ? (const void*)k_em_pass_persist<CT, false, 1>
+                  : acc == 2 ? (const void*)k_em_pass_persist<CT, false, 2> : (const void*)k_em_pass_persist<CT, false, 0>;
+}
+
 cudaError_t prepare_em_kernels(int block) {
-  for (const void* f :
-       {(const void*)k_em_pass_persist<float, false>, (const void*)k_em_pass_persist<uint32_t, false>,
-        (const void*)k_em_pass_persist<uint16_t, false>, (const void*)k_em_pass_persist<float, true>,
-        (const void*)k_em_pass_persist<uint32_t, true>, (const void*)k_em_pass_persist<uint16_t, true>}) {
-    cudaError_t e = fit_carveout(f, block, 0);
-    if (e != cudaSuccess) return e;
-  }
+  for (int acc = 0; acc < 3; acc++)
+    for (bool list : {false, true})
+      for (const void* f : {persist_kernel<float>(list, acc), persist_kernel<uint32_t>(list, acc),
+                            persist_kernel<uint16_t>(list, acc)}) {
+        cudaError_t e = fit_carveout(f, block, 0);
+        if (e != cudaSuccess) return e;
+      }
   return cudaSuccess;
 }
 
@@ -1354,7 +1382,7 @@ cudaError_t launch_backproject_pad(const ImgGeom& g, const LorTable& t, SubsetSe
   const int64_t total = (int64_t)t.n_sinos * s.nk * t.n_r;
   if (total == 0) return cudaSuccess;
   int per_sm = 0, dev = 0, sms = 0;
-  cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_scatter_persist, 128, 0);
+  cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_scatter_persist<0>, 128, 0);
   if (e != cudaSuccess) return e;
   if ((e = cudaGetDevice(&dev)) != cudaSuccess) return e;
   if ((e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev)) != cudaSuccess) return e;
@@ -1362,8 +1390,16 @@ cudaError_t launch_backproject_pad(const ImgGeom& g, const LorTable& t, SubsetSe
   const int64_t need = ((total + 31) / 32 * 32 + 127) / 128;
   if ((e = cudaMemsetAsync(counter, 0, sizeof(unsigned long long), st)) != cudaSuccess) return e;
   const bool two = img2 && pad2.bA && pad2.bT;
-  k_scatter_persist<<<(unsigned)(need < resident ? need : resident), 128, 0, st>>>(
-      g, t, s, vin, vin_mode, pad, total, counter, two ? pad2.bA : nullptr, two ? pad2.bT : nullptr);
+  const unsigned grid = (unsigned)(need < resident ? need : resident);
+  // The second pair (img2) takes plain atomics; so does the first beside it.
+  const int acc = two ? 0 : pad.acc;
+  if (acc == 1)
+    k_scatter_persist<1><<<grid, 128, 0, st>>>(g, t, s, vin, vin_mode, pad, total, counter, nullptr, nullptr);
+  else if (acc == 2)
+    k_scatter_persist<2><<<grid, 128, 0, st>>>(g, t, s, vin, vin_mode, pad, total, counter, nullptr, nullptr);
+  else
+    k_scatter_persist<0><<<grid, 128, 0, st>>>(g, t, s, vin, vin_mode, pad, total, counter,
+                                               two ? pad2.bA : nullptr, two ? pad2.bT : nullptr);
   if ((e = cudaGetLastError()) != cudaSuccess) return e;
   if (two && (e = launch_pad_reduce(g, pad2, 1, nullptr, img2, nullptr, nullptr, 0.f, 0, st)) != cudaSuccess) return e;
   return launch_pad_reduce(g, pad, 1, nullptr, img, nullptr, nullptr, 0.f, 0, st);
@@ -1415,12 +1451,9 @@ cudaError_t launch_em_pass(const ImgGeom& g, const LorTable& t, SubsetSel s, con
     const bool use_list = skip && nz.list && nz.tiles && nz.n_list && total <= nz.cap && total < ((int64_t)1 << 31);
     const void* pf;
     switch (counts_dtype) {
-      case APIRL_F32: pf = use_list ? (const void*)k_em_pass_persist<float, true>
-                                    : (const void*)k_em_pass_persist<float, false>; break;
-      case APIRL_U32: pf = use_list ? (const void*)k_em_pass_persist<uint32_t, true>
-                                    : (const void*)k_em_pass_persist<uint32_t, false>; break;
-      case APIRL_U16: pf = use_list ? (const void*)k_em_pass_persist<uint16_t, true>
-                                    : (const void*)k_em_pass_persist<uint16_t, false>; break;
+      case APIRL_F32: pf = persist_kernel<float>(use_list, pad.acc); break;
+      case APIRL_U32: pf = persist_kernel<uint32_t>(use_list, pad.acc); break;
+      case APIRL_U16: pf = persist_kernel<uint16_t>(use_list, pad.acc); break;
       default: return cudaErrorInvalidValue;
     }
     // Fitted here unless the launch is being captured into a graph (the
@@ -1474,16 +1507,22 @@ cudaError_t launch_em_pass(const ImgGeom& g, const LorTable& t, SubsetSel s, con
       }
       if ((me = cudaMemsetAsync(partials, 0, (size_t)chunks * sizeof(double), st)) != cudaSuccess) return me;
     }
-#define APIRL_PERSIST(CT)                                                                                       \
+#define APIRL_PERSIST_ACC(CT, ACC)                                                                              \
   do {                                                                                                          \
     if (use_list)                                                                                               \
-      k_em_pass_persist<CT, true><<<pgrid, block, 0, st>>>(g, t, s, (const CT*)counts, counts_packed, add, pad,  \
-                                                           back, partials, total, skip, persist_counter,        \
-                                                           nz.list, nz.n_list);                                 \
+      k_em_pass_persist<CT, true, ACC><<<pgrid, block, 0, st>>>(g, t, s, (const CT*)counts, counts_packed, add,  \
+                                                                pad, back, partials, total, skip,                \
+                                                                persist_counter, nz.list, nz.n_list);            \
     else                                                                                                        \
-      k_em_pass_persist<CT, false><<<pgrid, block, 0, st>>>(g, t, s, (const CT*)counts, counts_packed, add, pad, \
-                                                            back, partials, total, skip, persist_counter,       \
-                                                            nullptr, nullptr);                                  \
+      k_em_pass_persist<CT, false, ACC><<<pgrid, block, 0, st>>>(g, t, s, (const CT*)counts, counts_packed, add, \
+                                                                 pad, back, partials, total, skip,               \
+                                                                 persist_counter, nullptr, nullptr);             \
+  } while (0)
+#define APIRL_PERSIST(CT)                                  \
+  do {                                                     \
+    if (pad.acc == 1) APIRL_PERSIST_ACC(CT, 1);            \
+    else if (pad.acc == 2) APIRL_PERSIST_ACC(CT, 2);       \
+    else APIRL_PERSIST_ACC(CT, 0);                         \
   } while (0)
     switch (counts_dtype) {
       case APIRL_F32: APIRL_PERSIST(float); break;
@@ -1492,6 +1531,7 @@ cudaError_t launch_em_pass(const ImgGeom& g, const LorTable& t, SubsetSel s, con
       default: return cudaErrorInvalidValue;
     }
 #undef APIRL_PERSIST
+#undef APIRL_PERSIST_ACC
     cudaError_t pe = cudaGetLastError();
     if (pe != cudaSuccess || !lik) return pe;
     int64_t np = chunks;
@@ -1611,7 +1651,8 @@ cudaError_t launch_pad_reduce(const ImgGeom& g, const PadBuffers& pad, int mode,
                               const float* sens, const float* thr_ptr, float thr_value, int ge, cudaStream_t st) {
   dim3 grid((g.nx + 31) / 32, (g.ny + 31) / 32, g.nz), block(32, 8);
   PadDims d{g.nx, g.ny, g.nz};
-  k_pad_reduce<<<grid, block, 0, st>>>(d, pad.bA, pad.bT, mode, x, bp, sens, thr_ptr, thr_value, ge);
+  k_pad_reduce<<<grid, block, 0, st>>>(d, pad.bA, pad.bT, mode, x, bp, sens, thr_ptr, thr_value, ge,
+                                       pad.acc == 2 ? pad.eA : nullptr, pad.acc == 2 ? pad.eT : nullptr);
   return cudaGetLastError();
 }
 

@@ -177,15 +177,44 @@ __device__ __forceinline__ float siddon3_gather_pad(Walk3 w, const ImgGeom& g, i
   return acc;
 }
 
+// How a scatter step adds v into img[at] (APIRL_OPT_ACCUMULATE):
+//  0  one atomic add per segment (the reference's `#pragma omp atomic` float
+//     add, SiddonProjector.cpp:547-548, in the atomics' order);
+//  1  warp-aggregated: the lanes of a warp that add to the same voxel in the
+//     same step sum their values in lane order and one of them adds the sum;
+//  2  compensated: the atomic returns the value it added to, so the rounding
+//     error of that addition (TwoSum, Knuth) is known exactly and goes into
+//     a second image err; img + err is the sum to about twice float precision.
+template <int ACC>
+__device__ __forceinline__ void acc_add(float* __restrict__ img, float* __restrict__ err, unsigned at, float v) {
+  if (ACC == 1) {
+    const unsigned act = __activemask();
+    const unsigned peers = __match_any_sync(act, at);
+    float sum = 0.f;
+    for (unsigned m = peers; m; m &= m - 1u) sum = A_ADD(sum, __shfl_sync(peers, v, __ffs(m) - 1));
+    if ((int)(threadIdx.x & 31) == __ffs(peers) - 1) atomicAdd(img + at, sum);
+  } else if (ACC == 2) {
+    const float old = atomicAdd(img + at, v);
+    const float s = A_ADD(old, v);
+    const float bv = A_SUB(s, old);
+    const float e = A_ADD(A_SUB(old, A_SUB(s, bv)), A_SUB(v, bv));
+    if (e != 0.f) atomicAdd(err + at, e);
+  } else {
+    atomicAdd(img + at, v);
+  }
+}
+
+template <int ACC = 0>
 __device__ __forceinline__ void siddon3_scatter_pad(Walk3 w, const ImgGeom& g, int ux, int uy, int uz, unsigned lim,
-                                                    float r, float* __restrict__ img) {
+                                                    float r, float* __restrict__ img,
+                                                    float* __restrict__ err = nullptr) {
   const int sx = w.iinc * ux, sy = w.jinc * uy, sz = w.kinc * uz;
   int idx = (w.k + kPad) * uz + (w.j + kPad) * uy + (w.i + kPad) * ux;
   if (w.guarded) {
     for (int m = 0; m < w.n; m++) {
       bool cx, cy;
       const float an = next_crossing(w, cx, cy);
-      atomicAdd(img + min((unsigned)idx, lim - 1u), A_MUL(A_MUL(A_SUB(an, w.ac), w.L), r));
+      acc_add<ACC>(img, err, min((unsigned)idx, lim - 1u), A_MUL(A_MUL(A_SUB(an, w.ac), w.L), r));
       w.ac = an;
       if (cx) { idx += sx; w.ax = A_ADD(w.ax, w.axu); }
       else if (cy) { idx += sy; w.ay = A_ADD(w.ay, w.ayu); }
@@ -198,7 +227,7 @@ __device__ __forceinline__ void siddon3_scatter_pad(Walk3 w, const ImgGeom& g, i
     const float an = next_crossing(w, cx, cy);
     const float seg = A_MUL(A_SUB(an, w.ac), w.L);
     if (((unsigned)w.i < (unsigned)g.nx) & ((unsigned)w.j < (unsigned)g.ny) & ((unsigned)w.k < (unsigned)g.nz))
-      atomicAdd(img + idx, A_MUL(seg, r));
+      acc_add<ACC>(img, err, (unsigned)idx, A_MUL(seg, r));
     w.ac = an;
     if (cx) { w.i += w.iinc; idx += sx; w.ax = A_ADD(w.ax, w.axu); }
     else if (cy) { w.j += w.jinc; idx += sy; w.ay = A_ADD(w.ay, w.ayu); }

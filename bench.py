@@ -324,6 +324,9 @@ def run_gpu(args):
     log(f"autotuned fused-kernel block size: {best_block}")
     P.set_option(_l.APIRL_OPT_KERNEL_TIMING, 1)
     P.set_option(_l.APIRL_OPT_PERSISTENT, args.persistent)
+    if args.accumulate != "atomic":
+        P.set_option(_l.APIRL_OPT_ACCUMULATE, {"warp": _l.APIRL_ACC_WARP,
+                                               "compensated": _l.APIRL_ACC_COMPENSATED}[args.accumulate])
 
     sparse = args.pass_form == "sparse"
     nonzero = args.pass_form == "nonzero"
@@ -511,6 +514,17 @@ def run_gpu(args):
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cpu = cpu_baseline(w, log, budget_s=args.cpu_seconds, threads=args.cpu_threads, first_subset=args.warmup)
 
+    # The batched and served forms of the same path, on their mixed-job
+    # workloads, beside the single-job headline (one GPU, rank 0).
+    mixed = {}
+    if rank == 0 and world == 1 and not args.no_mixed:
+        del w, P, counts, sens, x, bp, flush
+        torch.cuda.synchronize(dev)
+        torch.cuda.empty_cache()
+        for kind in ("batched", "served"):
+            mixed[kind] = mixed_jobs(args, kind == "served", log)
+            log(f"{kind}: {mixed[kind]['value']:.0f} recon/h, {mixed[kind]['speedup_vs_plain']:.2f}x the plain driver")
+
     if rank == 0:
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
@@ -519,7 +533,7 @@ def run_gpu(args):
             "config": {"workload": WORKLOAD if args.max_ring_diff is None else
                        WORKLOAD + f" (profiling case: segments |rd| <= {args.max_ring_diff} only)",
                        "subsets": NSUB, "counts_dtype": "uint32", "em_block": best_block,
-                       "alpha": args.alpha, "persistent": args.persistent,
+                       "alpha": args.alpha, "persistent": args.persistent, "accumulate": args.accumulate,
                        "pass": ("sparse: bins with zero counts not walked, their likelihood terms -x.Z_s from "
                                 "per-subset zero-count images Z_s = A_s^T 1[m=0], all 21 computed inside the "
                                 "timed region and amortized over the timed sub-iterations") if sparse else
@@ -554,6 +568,11 @@ def run_gpu(args):
             "gpu_launches": (9 * args.steps + NSUB) if sparse else (9 * args.steps if nonzero else 5 * args.steps),
             "clocks": clock,
         }
+        if mixed:
+            line["batched"] = mixed["batched"]
+            line["served"] = mixed["served"]
+            line["served_p50_s"] = mixed["served"]["p50_latency_s"]
+            line["served_p99_s"] = mixed["served"]["p99_latency_s"]
         print(json.dumps(line), flush=True)
     if world > 1:
         dist.barrier()
@@ -738,16 +757,88 @@ def _make_jobs(specs, dev, log, c2_every=0):
 
 def _plain(jobs, dev):
     """The same jobs one after another through the plain driver (apirl_osem_3d,
-    float32 counts: converted before the clock starts)."""
+    float32 counts: converted before the clock starts).  Returns the images,
+    the total time and each job's own time."""
     import apirl_b200 as ap
     counts = [j.counts.astype(np.float32) for j in jobs]
     init = [np.ones(j.image_geom.n_voxels, np.float32) for j in jobs]
     t0 = time.perf_counter()
-    outs = []
+    outs, each = [], []
     for j, c, x0 in zip(jobs, counts, init):
+        ts = time.perf_counter()
         img, lik, _ = ap.osem_3d(j.image_geom, j.sino_geom, c, x0, j.iters, j.nsubsets, device=dev.index)
+        each.append(time.perf_counter() - ts)
         outs.append(img)
-    return outs, time.perf_counter() - t0
+    return outs, time.perf_counter() - t0, np.array(each)
+
+
+def _fifo(arrivals, service):
+    """Latencies and finish times of one server taking jobs in arrival order,
+    each for its measured service time: the plain driver serving the stream."""
+    order = np.argsort(arrivals)
+    finish = np.zeros(len(arrivals))
+    t = -np.inf
+    for k in order:
+        t = max(t, arrivals[k]) + service[k]
+        finish[k] = t
+    return finish - arrivals, finish
+
+
+def mixed_jobs(args, served, log):
+    """Batched (all jobs at once) or served (Poisson arrivals) OSEM jobs of
+    mixed geometry against the same jobs through the plain driver, one at a
+    time.  Returns the JSON fields of the comparison."""
+    import torch
+    from apirl_b200 import workloads
+    from apirl_b200.batch import Batch, serve
+    dev = torch.device("cuda:0")
+    n = args.jobs
+    specs = workloads.mixed_job_specs(n, seed=5 if served else 4)
+    jobs = _make_jobs(specs, dev, log, c2_every=10 if served else 0)
+    torch.cuda.empty_cache()
+    budget = int(args.budget_gb * (1 << 30))
+    ref, t_plain, each = _plain(jobs, dev)
+    if served:
+        arrivals = np.cumsum(np.random.default_rng(5).exponential(1.0 / args.rate, len(jobs)))
+        res, lat, makespan = serve(jobs, arrivals, budget_bytes=budget)
+        t_new = makespan - float(arrivals[0])
+        plain_lat, plain_finish = _fifo(arrivals, each)
+        plain_stream = float(plain_finish.max() - arrivals.min())
+    else:
+        b = Batch(0, budget_bytes=budget)
+        t0 = time.perf_counter()
+        res = b.run_all(jobs)
+        t_new = time.perf_counter() - t0
+        b.close()
+    errs = []
+    for r, p in zip(res, ref):
+        fin = np.isfinite(p)
+        if not np.array_equal(np.isfinite(r[0]), fin):
+            raise RuntimeError("a batched job's image is not finite where its solo run's is")
+        errs.append(float(np.linalg.norm(r[0][fin].astype(np.float64) - p[fin]) /
+                          np.linalg.norm(p[fin].astype(np.float64))))
+    out = {
+        "value": len(jobs) / t_new * 3600, "unit": "recon/h",
+        "plain_value": len(jobs) / t_plain * 3600, "speedup_vs_plain": t_plain / t_new,
+        "max_rel_l2_vs_plain": max(errs),
+        "workload": ("Poisson arrivals at %.0f jobs/s of " % args.rate if served else "all at once: ") +
+                    f"{len(jobs)} mixed OSEM jobs: images {{64,128,256}}^2 x {{1,41,81}} slices, 1.3N r/angles, "
+                    "span 1, 2-4 iterations x 7-21 subsets, 1e5-1e8 counts uint32" +
+                    ("; every 10th job the full 256x256x81 / 1261x336x336 geometry" if served else ""),
+        "plain": "the same jobs one after another through apirl_osem_3d (float32 counts made before the clock)",
+        "budget_gb": args.budget_gb,
+    }
+    if served:
+        out.update({"p50_latency_s": float(np.percentile(lat, 50)), "p99_latency_s": float(np.percentile(lat, 99)),
+                    "makespan_s": float(t_new),
+                    "plain_p50_latency_s": float(np.percentile(plain_lat, 50)),
+                    "plain_p99_latency_s": float(np.percentile(plain_lat, 99)),
+                    "plain_stream_value": len(jobs) / plain_stream * 3600,
+                    "speedup_vs_plain_stream": plain_stream / t_new,
+                    "plain_stream": "the plain driver serving the same arrivals in order, one job at a time "
+                                    "(each job's measured time; latency = finish - arrival)",
+                    "arrival_span_s": float(arrivals.max() - arrivals.min())})
+    return out
 
 
 def run_mlem2d(args):
@@ -804,46 +895,164 @@ def run_mlem2d(args):
 
 
 def run_batched(args, served=False):
-    import torch
-    from apirl_b200 import workloads
-    from apirl_b200.batch import Batch, serve
-    dev = torch.device("cuda:0")
     log = lambda m: print(f"[bench] {m}", file=sys.stderr, flush=True)
-    n = args.jobs
-    specs = workloads.mixed_job_specs(n, seed=5 if served else 4)
-    jobs = _make_jobs(specs, dev, log, c2_every=10 if served else 0)
-    budget = int(args.budget_gb * (1 << 30))
-    # plain form: one job at a time through the single-job driver
-    ref, t_plain = _plain(jobs, dev)
-    if served:
-        arrivals = np.cumsum(np.random.default_rng(5).exponential(1.0 / args.rate, len(jobs)))
-        res, lat, makespan = serve(jobs, arrivals, budget_bytes=budget)
-        t_new = makespan - float(arrivals[0])
-    else:
-        b = Batch(0, budget_bytes=budget)
-        t0 = time.perf_counter()
-        res = b.run_all(jobs)
-        t_new = time.perf_counter() - t0
-        b.close()
-        lat = None
-    errs = [float(np.linalg.norm(r[0].astype(np.float64) - p) / np.linalg.norm(p.astype(np.float64)))
-            for r, p in zip(res, ref)]
-    line = {
-        "metric": "served OSEM reconstructions/hour" if served else "batched OSEM reconstructions/hour",
-        "value": len(jobs) / t_new * 3600, "unit": "recon/h", "n_gpus": 1, "higher_is_better": True,
-        "plain_value": len(jobs) / t_plain * 3600, "speedup_vs_plain": t_plain / t_new,
-        "max_rel_l2_vs_plain": max(errs), "dtype": "f32", "data": "synthetic (seeded phantoms, Poisson counts)",
-        "config": {"workload": ("Poisson arrivals at %.0f jobs/s of " % args.rate if served else "") +
-                   f"{len(jobs)} mixed OSEM jobs: images {{64,128,256}}^2 x {{1,41,81}} slices, 1.3N r/angles, "
-                   "span 1, 2-4 iterations x 7-21 subsets, 1e5-1e8 counts uint32" +
-                   ("; every 10th job the full 256x256x81 / 1261x336x336 geometry" if served else ""),
-                   "budget_gb": args.budget_gb},
-    }
-    if served:
-        line["p50_latency_s"] = float(np.percentile(lat, 50))
-        line["p99_latency_s"] = float(np.percentile(lat, 99))
-        line["makespan_s"] = float(t_new)
+    r = mixed_jobs(args, served, log)
+    line = {"metric": "served OSEM reconstructions/hour" if served else "batched OSEM reconstructions/hour",
+            "value": r.pop("value"), "unit": r.pop("unit"), "n_gpus": 1, "higher_is_better": True,
+            "dtype": "f32", "data": "synthetic (seeded phantoms, Poisson counts)",
+            "config": {"workload": r.pop("workload"), "budget_gb": r.pop("budget_gb")}}
+    line.update(r)
     print(json.dumps(line), flush=True)
+
+
+# ---------------------------------------------------------------------------
+# Precision study: the full workload's first sub-iterations in several
+# arithmetic forms against the FP64 oracle.
+def _rel(a, b):
+    a = np.asarray(a, np.float64)
+    b = np.asarray(b, np.float64)
+    m = np.isfinite(a) & np.isfinite(b)
+    return float(np.linalg.norm(a[m] - b[m]) / max(np.linalg.norm(b[m]), 1e-300))
+
+
+def _max_abs(a, b):
+    a = np.asarray(a, np.float64)
+    b = np.asarray(b, np.float64)
+    m = np.isfinite(a) & np.isfinite(b)
+    return float(np.max(np.abs(a[m] - b[m])))
+
+
+def precision_study(subiters, log, threads=None):
+    """The first `subiters` OSEM sub-iterations of the 3D workload (from an
+    image of ones) in several GPU forms and in the FP64 oracle (double LOR
+    geometry, double walk, double accumulation).  Returns a dict: per
+    sub-iteration the relative L2 and max-abs error of each form's image
+    against the FP64 image and the relative error of its FP64 likelihood;
+    one ratio sinogram's backprojection in each accumulation form (and the
+    reference's serial float order) against its FP64 backprojection; the
+    adjoint residual of the GPU operators.  Forms:
+      f32          the reference's float arithmetic, fp32 atomics (uint32 counts)
+      f32_warp     the same, warp-aggregated atomics (APIRL_ACC_WARP)
+      f32_comp     the same, compensated atomics (APIRL_ACC_COMPENSATED)
+      u16          uint16 counts (round trip checked bit for bit first)
+      f64alpha     FP64 walk geometry, fp32 projection and accumulation"""
+    import torch
+    import apirl_b200 as ap
+    from apirl_b200 import _lib as _l
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    from oracle_lib import Oracle
+    dev = torch.device("cuda:0")
+    w = setup_workload(dev, log)
+    P, ig, sg = w["P"], w["ig"], w["sg"]
+    nv = ig.n_voxels
+    orc = Oracle()
+    thr = threads or os.cpu_count() or 1
+    counts32 = w["counts"]
+    counts_np = counts32.view(torch.int32).cpu().numpy().astype(np.int64)
+    if counts_np.max() >= 65536:
+        raise RuntimeError("counts do not fit uint16")
+    counts16 = torch.from_numpy(counts_np.astype(np.uint16)).to(dev)
+    u16_round_trip = bool(np.array_equal(counts16.cpu().numpy().astype(np.int64), counts_np))
+    meas64 = counts_np.astype(np.float64).reshape(sg.n_sinos, sg.n_proj, sg.n_r)
+    atten64 = w["atten"].cpu().numpy().astype(np.float64).reshape(sg.n_sinos, sg.n_proj, sg.n_r)
+
+    def projector(acc=None, f64=False):
+        Q = ap.SiddonProjector(ig, sg)
+        if f64:
+            Q.set_alpha_precision(True)
+        if acc is not None:
+            Q.set_option(_l.APIRL_OPT_ACCUMULATE, acc)
+        return Q
+
+    P64 = projector(f64=True)
+    Pw = projector(_l.APIRL_ACC_WARP)
+    Pc = projector(_l.APIRL_ACC_COMPENSATED)
+    sens64 = torch.zeros((NSUB, nv), dtype=torch.float32, device=dev)
+    for s in range(subiters):
+        a_s = w["atten"].view(sg.n_sinos, sg.n_proj, sg.n_r)[:, s::NSUB, :].contiguous().view(-1)
+        P64.backproject(a_s, sens64[s], s, NSUB)
+        ap.force_positive(sens64[s])
+    forms = {"f32": dict(P=P, counts=counts32, sens=w["sens"]),
+             "f32_warp": dict(P=Pw, counts=counts32, sens=w["sens"]),
+             "f32_comp": dict(P=Pc, counts=counts32, sens=w["sens"]),
+             "u16": dict(P=P, counts=counts16, sens=w["sens"]),
+             "f64alpha": dict(P=P64, counts=counts32, sens=sens64)}
+    for f in forms.values():
+        f["x"] = torch.ones(nv, dtype=torch.float32, device=dev)
+        f["bp"] = torch.zeros(nv, dtype=torch.float32, device=dev)
+        f["lik"] = torch.zeros(1, dtype=torch.float64, device=dev)
+    x64 = np.ones(nv, np.float64)
+    rows = []
+    for s in range(subiters):
+        t0 = time.time()
+        # FP64 oracle sub-iteration (OsemSinogram3d.cpp:159-237 in double), update where sens > 0.
+        a_s = np.ascontiguousarray(atten64[:, s::NSUB, :]).reshape(-1)
+        sens_s = orc.backproject_3d(sg, ig, a_s, s, NSUB, dtype=np.float64, threads=thr)
+        est = orc.project_3d(sg, ig, x64, s, NSUB, dtype=np.float64, threads=thr)
+        m_s = np.ascontiguousarray(meas64[:, s::NSUB, :]).reshape(-1)
+        nz = est != 0
+        lik64 = float(np.sum(m_s[nz] * np.log(est[nz]) - est[nz]))
+        ratio = np.where((m_s != 0) & nz, m_s / np.where(nz, est, 1.0), 0.0)
+        bp64 = orc.backproject_3d(sg, ig, ratio, s, NSUB, dtype=np.float64, threads=thr)
+        with np.errstate(invalid="ignore", divide="ignore"):
+            x64 = np.where(sens_s > 0, x64 * bp64 / np.where(sens_s > 0, sens_s, 1.0), 0.0)
+        row = {"subiteration": s, "oracle_s": round(time.time() - t0, 1)}
+        for name, f in forms.items():
+            f["P"].em_pass(f["counts"], f["x"], f["bp"], f["sens"][s], s, NSUB, ge=UPDATE_GE, lik=f["lik"])
+            torch.cuda.synchronize(dev)
+            xg = f["x"].cpu().numpy()
+            row[name] = {"rel_l2": _rel(xg, x64), "max_abs": _max_abs(xg, x64),
+                         "lik_rel": abs(f["lik"].item() - lik64) / abs(lik64)}
+        row["u16_equals_f32"] = bool(np.array_equal(forms["u16"]["x"].cpu().numpy().view(np.uint32),
+                                                    forms["f32"]["x"].cpu().numpy().view(np.uint32)))
+        log(json.dumps(row))
+        rows.append(row)
+
+    # One ratio sinogram of subset 0, backprojected in each accumulation form.
+    s = 0
+    x1 = forms["f32"]["x"].cpu().numpy()
+    est32 = orc.project_3d(sg, ig, x1, s, NSUB, threads=thr)
+    m32 = np.ascontiguousarray(meas64[:, s::NSUB, :]).reshape(-1).astype(np.float32)
+    ratio32 = orc.inverse_divide(m32, est32)
+    bp_exact = orc.backproject_3d(sg, ig, ratio32.astype(np.float64), s, NSUB, dtype=np.float64, threads=thr)
+    acc = {"reference_serial_fp32_rel_l2": _rel(orc.backproject_3d(sg, ig, ratio32, s, NSUB, threads=1), bp_exact)}
+    r_dev = torch.from_numpy(ratio32).to(dev)
+    for name, Q in (("atomic", P), ("warp", Pw), ("compensated", Pc)):
+        bpg = torch.zeros(nv, dtype=torch.float32, device=dev)
+        Q.backproject(r_dev, bpg, s, NSUB)
+        torch.cuda.synchronize(dev)
+        acc[f"gpu_{name}_rel_l2"] = _rel(bpg.cpu().numpy(), bp_exact)
+        acc[f"gpu_{name}_max_abs"] = _max_abs(bpg.cpu().numpy(), bp_exact)
+
+    # Adjoint residual of the GPU operators (FP64 dot products).
+    rng = np.random.default_rng(0)
+    xa = rng.random(nv, dtype=np.float32)
+    ya = rng.random(sg.subset_bins(s, NSUB), dtype=np.float32)
+    adj = {}
+    for name, Q in (("f32", P), ("f64alpha", P64), ("f32_comp", Pc)):
+        Ax = torch.zeros(ya.size, dtype=torch.float32, device=dev)
+        Q.project(torch.from_numpy(xa).to(dev), Ax, s, NSUB)
+        Aty = torch.zeros(nv, dtype=torch.float32, device=dev)
+        Q.backproject(torch.from_numpy(ya).to(dev), Aty, s, NSUB)
+        lhs = float(np.dot(Ax.cpu().numpy().astype(np.float64), ya.astype(np.float64)))
+        rhs = float(np.dot(xa.astype(np.float64), Aty.cpu().numpy().astype(np.float64)))
+        adj[name] = abs(lhs - rhs) / abs(lhs)
+    for Q in (P64, Pw, Pc):
+        Q.close()
+    return {"subiterations": rows, "u16_round_trip": u16_round_trip, "backprojection_accumulation": acc,
+            "adjoint_residual": adj, "oracle_threads": thr}
+
+
+def run_precision(args):
+    log = lambda m: print(f"[precision] {m}", file=sys.stderr, flush=True)
+    r = precision_study(args.precision_subiters, log, args.cpu_threads)
+    first = r["subiterations"][0]
+    print(json.dumps({"metric": "rel L2 vs FP64 oracle after the first sub-iteration (f32, reference arithmetic)",
+                      "value": first["f32"]["rel_l2"], "unit": "relative L2", "higher_is_better": False,
+                      "n_gpus": 1, "dtype": "f32", "data": "synthetic (seeded phantom, Poisson counts)",
+                      "config": {"workload": WORKLOAD, "subiterations": args.precision_subiters,
+                                 "update": "x*bp/sens where sens > 0"},
+                      **r}), flush=True)
 
 
 def main():
@@ -854,6 +1063,8 @@ def main():
     ap_.add_argument("--warmup", type=int, default=5)
     ap_.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap_.add_argument("--no-cpu-baseline", action="store_true")
+    ap_.add_argument("--no-mixed", action="store_true",
+                     help="default workload: skip the batched and served mixed-job runs after the headline")
     ap_.add_argument("--cpu-seconds", type=float, default=15.0)
     ap_.add_argument("--pass", dest="pass_form", default="nonzero", choices=["sparse", "nonzero", "full"],
                      help="nonzero: bins with zero counts are not walked, the likelihood from per-subset geometry "
@@ -869,9 +1080,13 @@ def main():
                      help="walk geometry: f32 = the reference's float arithmetic (headline); f64 = precision mode")
     ap_.add_argument("--no-one-thread", action="store_true",
                      help="reference arm: skip the extra one-thread sub-iteration")
+    ap_.add_argument("--accumulate", default="atomic", choices=["atomic", "warp", "compensated"],
+                     help="how the backprojection scatter accumulates (APIRL_OPT_ACCUMULATE)")
     ap_.add_argument("--cpu-threads", type=int, default=None,
                      help="host threads of the CPU baseline / reference arm (default: all)")
-    ap_.add_argument("--workload", default="osem3d", choices=["osem3d", "batched", "served", "mlem2d"])
+    ap_.add_argument("--workload", default="osem3d", choices=["osem3d", "batched", "served", "mlem2d", "precision"])
+    ap_.add_argument("--precision-subiters", type=int, default=4,
+                     help="precision workload: sub-iterations compared with the FP64 oracle")
     ap_.add_argument("--max-ring-diff", type=int, default=None,
                      help="profiling: keep segments |rd| <= this (smaller case of the same kernels)")
     ap_.add_argument("--jobs", type=int, default=64)
@@ -889,6 +1104,8 @@ def main():
         run_sharded(args)
     elif args.workload == "mlem2d":
         run_mlem2d(args)
+    elif args.workload == "precision":
+        run_precision(args)
     elif args.workload in ("batched", "served"):
         run_batched(args, served=args.workload == "served")
     else:

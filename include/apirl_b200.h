@@ -202,9 +202,24 @@ enum {
   APIRL_OPT_KERNEL_TIMING = 2,
   APIRL_OPT_EM_BLOCK = 3,
   APIRL_OPT_PERSISTENT = 4,
-  APIRL_OPT_SPARSE_IMAGE = 5
+  APIRL_OPT_SPARSE_IMAGE = 5,
+  APIRL_OPT_ACCUMULATE = 6
 };
 enum { APIRL_SPARSE_ZERO_COUNT = 0, APIRL_SPARSE_GEOMETRY = 1 };
+/* APIRL_OPT_ACCUMULATE (default APIRL_ACC_ATOMIC): how the 3D passes over the
+ * padded layouts (the persistent fused pass, its sparse forms, and
+ * apirl_backproject / apirl_backproject_ones) add segment contributions into
+ * the backprojection.  APIRL_ACC_ATOMIC: one fp32 atomic add per segment, as
+ * the reference's `#pragma omp atomic` (recon/src/SiddonProjector.cpp:547-548).
+ * APIRL_ACC_WARP: the lanes of a warp that add to the same voxel in the same
+ * step sum their contributions first and one atomic adds the sum.
+ * APIRL_ACC_COMPENSATED: every atomic add's rounding error (TwoSum on the
+ * value it returns) goes into a second padded pair, folded in when the pass
+ * reduces its pair: the backprojection to about twice float precision.  The
+ * compensated form allocates two more padded images; set it outside graph
+ * capture.  Other paths (2D, FP64 walk, sampled rays, unpadded, the
+ * non-persistent pass) accept only APIRL_ACC_ATOMIC. */
+enum { APIRL_ACC_ATOMIC = 0, APIRL_ACC_WARP = 1, APIRL_ACC_COMPENSATED = 2 };
 apirl_status apirl_projector_set_option(apirl_projector* p, int option, int value);
 apirl_status apirl_projector_kernel_ms(apirl_projector* p, double* ms);
 /* Autotuner: times the fused kernel (apirl_em_project_backproject, `repeats`
