@@ -23,6 +23,8 @@ APIRL_OPT_EM_BLOCK = 3
 APIRL_OPT_PERSISTENT = 4
 APIRL_OPT_SPARSE_IMAGE = 5
 APIRL_OPT_ACCUMULATE = 6
+APIRL_OPT_L2_PERSIST = 7
+APIRL_OPT_LIST_ORDER = 8
 APIRL_SPARSE_ZERO_COUNT = 0
 APIRL_SPARSE_GEOMETRY = 1
 APIRL_ACC_ATOMIC = 0

@@ -132,28 +132,72 @@ struct Pool {
   }
 };
 
-// Page-locked host blocks for results and descriptors, reused by size.
+// Page-locked host memory for results, descriptors and staging: chunks of
+// at least 256 MB, carved first-fit (256-byte units) and coalesced on return,
+// so that jobs coming and going do not page-lock memory each time.
 struct PinnedPool {
-  std::multimap<size_t, void*> free_blocks;
-  void* get(size_t bytes) {
-    auto it = free_blocks.lower_bound(bytes);
-    if (it != free_blocks.end() && it->first <= 2 * bytes + 4096) {
-      void* p = it->second;
-      free_blocks.erase(it);
-      return p;
-    }
+  static constexpr size_t kChunk = (size_t)256 << 20;
+  struct Chunk {
+    char* base;
+    size_t size;
+    std::map<size_t, size_t> free_at;  // offset -> length
+  };
+  std::vector<Chunk> chunks;
+  std::map<void*, std::pair<size_t, size_t>> used;  // block -> (chunk, length)
+
+  bool grow(size_t bytes) {
+    Chunk c;
+    c.size = std::max(kChunk, bytes);
     void* p = nullptr;
-    if (cudaMallocHost(&p, bytes) != cudaSuccess) return nullptr;
-    sizes[p] = bytes;
-    return p;
+    if (cudaMallocHost(&p, c.size) != cudaSuccess) return false;
+    c.base = (char*)p;
+    c.free_at[0] = c.size;
+    chunks.push_back(std::move(c));
+    return true;
+  }
+  void* get(size_t bytes) {
+    bytes = (std::max<size_t>(bytes, 1) + 255) & ~(size_t)255;
+    for (int pass = 0; pass < 2; pass++) {
+      for (size_t k = 0; k < chunks.size(); k++) {
+        Chunk& c = chunks[k];
+        for (auto it = c.free_at.begin(); it != c.free_at.end(); ++it) {
+          if (it->second < bytes) continue;
+          const size_t off = it->first, len = it->second;
+          c.free_at.erase(it);
+          if (len > bytes) c.free_at[off + bytes] = len - bytes;
+          void* p = c.base + off;
+          used[p] = {k, bytes};
+          return p;
+        }
+      }
+      if (pass == 0 && !grow(bytes)) return nullptr;
+    }
+    return nullptr;
   }
   void put(void* p) {
-    if (p) free_blocks.emplace(sizes[p], p);
+    if (!p) return;
+    auto u = used.find(p);
+    if (u == used.end()) return;
+    Chunk& c = chunks[u->second.first];
+    size_t off = (size_t)((char*)p - c.base), len = u->second.second;
+    used.erase(u);
+    auto next = c.free_at.lower_bound(off);
+    if (next != c.free_at.end() && next->first == off + len) {
+      len += next->second;
+      next = c.free_at.erase(next);
+    }
+    if (next != c.free_at.begin()) {
+      auto prev = std::prev(next);
+      if (prev->first + prev->second == off) {
+        prev->second += len;
+        return;
+      }
+    }
+    c.free_at[off] = len;
   }
   ~PinnedPool() {
-    for (auto& kv : sizes) cudaFreeHost(kv.first);
+    for (auto& c : chunks) cudaFreeHost(c.base);
   }
-  std::map<void*, size_t> sizes;
 };
 
 // ---- shared geometry products ---------------------------------------------------
@@ -175,7 +219,10 @@ struct SensSet {
 
 struct Geom {
   GeomKey key;
-  apirl_projector* p = nullptr;  // LOR tables and end-point z on the device
+  ImgGeom g{};                   // the image geometry as the walk takes it
+  LorTable t{};                  // LOR end points and end-point z, on the device (pool)
+  std::vector<float> host_lor;   // the LOR table on the host, [angle][r] (p1x, p1y, p2x, p2y)
+  void* h_tables = nullptr;      // page-locked copy of the tables, the source of their upload
   int64_t nvox = 0, nbins = 0;
   // A_a^T 1 of every angle a (padded images of pv voxels, [z][x][y] where
   // tr[a], else [z][y][x]), then A^T 1 (unpadded); or A^T 1 alone.
@@ -474,7 +521,28 @@ apirl_status geom_for(apirl_batch* b, Job& j, Geom** out) {
     apirl_sino3d_geom sg = j.sino;
     sg.min_ring_diff = g->key.mn.data();
     sg.max_ring_diff = g->key.mx.data();
-    BS(apirl_projector_create_3d(&j.img, &sg, b->device, &g->p));
+    {
+      // The host half of a projector: checks and tables (no device buffers).
+      apirl_projector tables;
+      BS(apirl::setup_3d(&j.img, &sg, &tables));
+      g->g = tables.g;
+      g->t = tables.t;
+      g->host_lor.swap(tables.host.lor);
+      const size_t lor_b = g->host_lor.size() * sizeof(float), z_b = tables.host.z.size() * sizeof(float);
+      g->h_tables = b->pinned.get(lor_b + z_b);
+      if (!g->h_tables) return bfail(APIRL_ERR_OOM, "page-locked geometry tables");
+      memcpy(g->h_tables, g->host_lor.data(), lor_b);
+      memcpy((char*)g->h_tables + lor_b, tables.host.z.data(), z_b);
+      float4* d_lor = nullptr;
+      float2* d_z = nullptr;
+      BK(b->pool.alloc(&d_lor, (int64_t)(lor_b / sizeof(float4)), b->st));
+      BK(b->pool.alloc(&d_z, (int64_t)(z_b / sizeof(float2)), b->st));
+      BK(cudaMemcpyAsync(d_lor, g->h_tables, lor_b, cudaMemcpyHostToDevice, b->st));
+      BK(cudaMemcpyAsync(d_z, (char*)g->h_tables + lor_b, z_b, cudaMemcpyHostToDevice, b->st));
+      g->t.lor = d_lor;
+      g->t.z = d_z;
+      g->t.ok = nullptr;
+    }
     g->nvox = j.nvox;
     g->nbins = j.nbins;
     g->pv = padded_voxels(j.img);
@@ -483,7 +551,7 @@ apirl_status geom_for(apirl_batch* b, Job& j, Geom** out) {
     const int np = g->key.n_proj, nr = g->key.n_r;
     g->h_tr = (uint8_t*)b->pinned.get((size_t)np);
     if (!g->h_tr) return bfail(APIRL_ERR_OOM, "page-locked angle table");
-    const float* lor = g->p->host.lor.data();
+    const float* lor = g->host_lor.data();
     for (int a = 0; a < np; a++) {
       const float* L = lor + ((size_t)a * nr + nr / 2) * 4;
       g->h_tr[a] = fabsf(L[2] - L[0]) >= fabsf(L[3] - L[1]) ? 1 : 0;
@@ -524,7 +592,7 @@ apirl_status sens_walk(apirl_batch* b, Job& j, const ImgGeom& g, const LorTable&
 apirl_status ensure_sensitivity(apirl_batch* b, Job& j) {
   Geom& g = *j.geom;
   g.last_use = ++b->clock;
-  const LorTable& t = g.p->t;
+  const LorTable& t = g.t;
   if (!g.per_angle && !g.per_angle_tried) {
     g.per_angle_tried = true;
     evict(b, g.per_angle_bytes());
@@ -534,8 +602,8 @@ apirl_status ensure_sensitivity(apirl_batch* b, Job& j) {
       b->used += g.per_angle_held;
       g.g_total = g.per_angle + (int64_t)g.key.n_proj * g.pv;
       BK(cudaMemsetAsync(g.per_angle, 0, (size_t)g.key.n_proj * g.pv * 4, b->st));
-      BK(apirl::launch_scatter_angles(g.p->g, t, g.d_tr, g.per_angle, (unsigned)g.pv, b->d_counter, b->st));
-      BK(apirl::launch_sum_angles(g.per_angle, g.d_tr, (unsigned)g.pv, g.key.n_proj, g.p->g, 1, g.g_total, b->st));
+      BK(apirl::launch_scatter_angles(g.g, t, g.d_tr, g.per_angle, (unsigned)g.pv, b->d_counter, b->st));
+      BK(apirl::launch_sum_angles(g.per_angle, g.d_tr, (unsigned)g.pv, g.key.n_proj, g.g, 1, g.g_total, b->st));
     }
   }
   auto it = g.sets.find(j.nsub);
@@ -545,10 +613,10 @@ apirl_status ensure_sensitivity(apirl_batch* b, Job& j) {
     BK(b->pool.alloc(&s.g, (int64_t)j.nsub * g.nvox, b->st));
     b->used += bytes;
     if (g.per_angle && g.g_total != g.per_angle) {
-      BK(apirl::launch_sum_angles(g.per_angle, g.d_tr, (unsigned)g.pv, g.key.n_proj, g.p->g, j.nsub, s.g, b->st));
+      BK(apirl::launch_sum_angles(g.per_angle, g.d_tr, (unsigned)g.pv, g.key.n_proj, g.g, j.nsub, s.g, b->st));
     } else {
       BK(cudaMemsetAsync(s.g, 0, (size_t)j.nsub * g.nvox * 4, b->st));
-      BS(sens_walk(b, j, g.p->g, t, nullptr, s.g, 1));
+      BS(sens_walk(b, j, g.g, t, nullptr, s.g, 1));
     }
     it = g.sets.emplace(j.nsub, s).first;
   }
@@ -622,7 +690,7 @@ apirl_status admit(apirl_batch* b, Job& j) {
   BK(b->pool.alloc(&j.d_nlist, j.nsub, s));
   j.tile_off.assign(j.nsub + 1, 0);
   for (int k = 0; k < j.nsub; k++)
-    j.tile_off[k + 1] = j.tile_off[k] + n_tiles_of((int64_t)j.geom->p->t.n_sinos *
+    j.tile_off[k + 1] = j.tile_off[k] + n_tiles_of((int64_t)j.geom->t.n_sinos *
                                                    apirl::subset_nproj(j.sino.n_proj, k, j.nsub) * j.sino.n_r);
   BK(b->pool.alloc(&j.d_tiles, std::max<int64_t>(j.tile_off[j.nsub], 1), s));
   float* pads[4];
@@ -652,7 +720,7 @@ apirl_status start_counting(apirl_batch* b, Job& j) {
   cudaStream_t s = b->st;
   BK(cudaStreamWaitEvent(s, j.up_ev, 0));
   if (!j.h_init) BK(apirl::launch_fill(j.nvox, j.d_x, 1.f, s));
-  const LorTable& t = j.geom->p->t;
+  const LorTable& t = j.geom->t;
   for (int k = 0; k < j.nsub; k++) {
     SubsetSel ss;
     ss.subset = k; ss.nsub = j.nsub; ss.nk = apirl::subset_nproj(j.sino.n_proj, k, j.nsub);
@@ -666,7 +734,7 @@ apirl_status start_counting(apirl_batch* b, Job& j) {
   if (j.d_mult) {
     // sens_s = A_s^T (factors of subset s), then forcePositive (OsemSinogram3d.cpp:327-346, :115)
     BK(cudaMemsetAsync(j.d_sens, 0, (size_t)j.nvox * j.nsub * 4, s));
-    BS(sens_walk(b, j, j.geom->p->g, t, j.d_mult, j.d_sens, 0));
+    BS(sens_walk(b, j, j.geom->g, t, j.d_mult, j.d_sens, 0));
     BK(apirl::launch_force_positive(j.nvox * j.nsub, j.d_sens, s));
   }
   BK(cudaEventRecord(j.ev, s));
@@ -687,7 +755,7 @@ apirl_status start_running(apirl_batch* b, Job& j) {
   const int64_t unused = align256(j.nbins * 4) - align256(std::max<int64_t>(j.list_off[j.nsub], 1) * 4);
   j.charged -= unused;
   b->used -= unused;
-  const LorTable& t = j.geom->p->t;
+  const LorTable& t = j.geom->t;
   for (int k = 0; k < j.nsub; k++) {
     SubsetSel ss;
     ss.subset = k; ss.nsub = j.nsub; ss.nk = apirl::subset_nproj(j.sino.n_proj, k, j.nsub);
@@ -709,7 +777,13 @@ apirl_status grow(apirl_batch* b, T** d, int64_t* cap, int64_t need) {
   return APIRL_OK;
 }
 
+// Room for nv job and ns segment descriptors in both page-locked slots.  The
+// old blocks go back to the pool only once no copy from either slot is in
+// flight (the other slot's was queued one step ago).
 apirl_status grow_host(apirl_batch* b, int nv, int ns) {
+  if (nv <= b->h_cap_vox && ns <= b->h_cap_segs) return APIRL_OK;
+  BK(cudaEventSynchronize(b->step_ev[0]));
+  BK(cudaEventSynchronize(b->step_ev[1]));
   if (nv > b->h_cap_vox) {
     for (int k = 0; k < 2; k++) {
       b->pinned.put(b->h_vox[k]);
@@ -749,26 +823,26 @@ apirl_status launch_step(apirl_batch* b, std::vector<Job*>& jobs) {
     Job& j = *jobs[q];
     const bool fin = j.stage == Stage::Final;
     const int sub = fin ? 0 : j.pass % j.nsub;
-    const apirl_projector* p = j.geom->p;
+    const Geom& gm = *j.geom;
     MultiVox& V = hv[q];
-    V.g = p->g;
+    V.g = gm.g;
     V.pad = j.pad;
     V.x = j.d_x;
     V.sens = fin ? nullptr : (j.d_sens ? j.d_sens + (int64_t)sub * j.nvox : j.set->g + (int64_t)sub * j.nvox);
     V.gimg = fin ? j.geom->g_total : j.set->g + (int64_t)sub * j.nvox;
     V.lik = j.d_lik + (fin ? (int64_t)j.iters * j.nsub : j.pass);
     V.tile_begin = tiles;
-    V.tiles_x = (p->g.nx + 31) / 32;
-    V.tiles_y = (p->g.ny + 31) / 32;
-    tiles += apirl::multi_tiles(p->g);
+    V.tiles_x = (gm.g.nx + 31) / 32;
+    V.tiles_y = (gm.g.ny + 31) / 32;
+    tiles += apirl::multi_tiles(gm.g);
     V.chunk_begin = chunks;
     V.update = fin ? 0 : 1;
     V.ge = 1;  // OsemSinogram3d's rule: sens >= 0 (threshold 0)
     V.zero_add = 0.0;
     for (int k = fin ? 0 : sub; k < (fin ? j.nsub : sub + 1); k++) {
       MultiSeg& S = hs[si++];
-      S.g = p->g;
-      S.t = p->t;
+      S.g = gm.g;
+      S.t = gm.t;
       S.s.subset = k; S.s.nsub = j.nsub; S.s.nk = apirl::subset_nproj(j.sino.n_proj, k, j.nsub);
       S.counts = j.d_counts;
       S.counts_dtype = j.dtype;
@@ -852,6 +926,7 @@ apirl_status apirl_batch_create(int device, int64_t budget, apirl_batch** out) {
   const size_t want = std::min<size_t>((size_t)budget, free_b / 10 * 9);
   BK(b->pool.reserve(want & ~(size_t)((1 << 21) - 1), b->st));
   BK(apirl::multi_walk_grid(&b->walk_blocks));
+  if (!b->pinned.grow(PinnedPool::kChunk)) return bfail(APIRL_ERR_OOM, "page-locked host memory");
   BK(b->pool.alloc(&b->d_counter, 1, b->st));
   for (int k = 0; k < 2; k++) {
     BK(cudaEventCreateWithFlags(&b->step_ev[k], cudaEventDisableTiming));
@@ -879,6 +954,10 @@ void apirl_batch_destroy(apirl_batch* b) {
     b->pool.release(g.per_angle, b->st);
     b->pool.release(g.d_tr, b->st);
     b->pinned.put(g.h_tr);
+    float4* lor = const_cast<float4*>(g.t.lor);
+    float2* z = const_cast<float2*>(g.t.z);
+    b->pool.release(lor, b->st);
+    b->pool.release(z, b->st);
   }
   b->pool.release(b->d_counter, b->st);
   b->pool.release(b->d_chunk_part, b->st);
@@ -886,7 +965,7 @@ void apirl_batch_destroy(apirl_batch* b) {
   b->pool.release(b->d_vox, b->st);
   b->pool.release(b->d_segs, b->st);
   cudaStreamSynchronize(b->st);
-  for (auto& kv : b->geoms) apirl_projector_destroy(kv.second->p);
+  for (auto& kv : b->geoms) b->pinned.put(kv.second->h_tables);
   for (int k = 0; k < 2; k++) {
     b->pinned.put(b->h_vox[k]);
     b->pinned.put(b->h_segs[k]);

@@ -138,17 +138,19 @@ apirl_status alloc_pad(apirl_projector* p) {
   if (p->pad.pA) return APIRL_OK;
   const int64_t pv = (int64_t)(p->g.nx + 2 * apirl::kPad) * (p->g.ny + 2 * apirl::kPad) * (p->g.nz + 2 * apirl::kPad);
   if (pv > INT_MAX) return APIRL_OK;
-  float* b[4] = {nullptr, nullptr, nullptr, nullptr};
-  for (int i = 0; i < 4; i++) {
-    if (cudaMalloc(&b[i], pv * sizeof(float)) != cudaSuccess || cudaMemset(b[i], 0, pv * sizeof(float)) != cudaSuccess) {
-      for (int k = 0; k <= i; k++) cudaFree(b[k]);
-      return cuda_fail(cudaGetLastError(), "padded layout buffers");
-    }
+  // One block for the four images (an L2 access policy window can then
+  // cover them all: APIRL_OPT_L2_PERSIST).
+  float* b = nullptr;
+  cudaError_t e = cudaMalloc(&b, 4 * pv * sizeof(float));
+  if (e == cudaSuccess) e = cudaMemset(b, 0, 4 * pv * sizeof(float));
+  if (e != cudaSuccess) {
+    cudaFree(b);
+    return cuda_fail(e, "padded layout buffers");
   }
-  p->pad.pA = b[0];
-  p->pad.pT = b[1];
-  p->pad.bA = b[2];
-  p->pad.bT = b[3];
+  p->pad.pA = b;
+  p->pad.pT = b + pv;
+  p->pad.bA = b + 2 * pv;
+  p->pad.bT = b + 3 * pv;
   p->pad.lim = (unsigned)pv;
   return APIRL_OK;
 }
@@ -182,6 +184,58 @@ apirl_status finish_create(apirl_projector* p, apirl_projector** out) {
 }
 
 }  // namespace
+
+namespace apirl {
+// The host half of a 3D projector: checks the image and sinogram geometry
+// (cylindrical or Siemens mMR) and builds the LOR and end-point tables into p
+// (g, host, t's sizes, the geometry as given), touching no device.
+apirl_status setup_3d(const apirl_image_geom* img, const apirl_sino3d_geom* sino, apirl_projector* p) {
+  if (!sino) return fail(APIRL_ERR_INVALID, "invalid 3D sinogram geometry");
+  if (sino->scanner != APIRL_SCANNER_CYLINDRICAL && sino->scanner != APIRL_SCANNER_MMR)
+    return fail(APIRL_ERR_INVALID, "unknown scanner %d", sino->scanner);
+  const bool mmr = sino->scanner == APIRL_SCANNER_MMR;
+  if (!valid_img(img)) return fail(APIRL_ERR_INVALID, "invalid image geometry");
+  if (mmr) {
+    if (sino->n_proj < 2 || sino->n_r <= 0 || sino->n_rings <= 0 || sino->n_segments <= 0 || !sino->min_ring_diff ||
+        !sino->max_ring_diff)
+      return fail(APIRL_ERR_INVALID, "invalid mMR sinogram geometry (need n_proj >= 2, n_r, n_rings, segments)");
+    if (!walk_bounded(img, apirl::kMmrRadius + apirl::kMmrDoi, apirl::kMmrAxialFov))
+      return fail(APIRL_ERR_INVALID, "voxels too small for the scanner size (walks above 1e5 segments)");
+  } else {
+    if (sino->n_proj <= 0 || sino->n_r <= 0 || sino->n_rings <= 0 || sino->n_segments <= 0 ||
+        !sino->min_ring_diff || !sino->max_ring_diff || !(sino->r_fov > 0) || !(sino->axial_fov > 0) ||
+        !(sino->r_scanner > sino->r_fov))
+      return fail(APIRL_ERR_INVALID, "invalid 3D sinogram geometry");
+    if (!walk_bounded(img, sino->r_scanner, sino->axial_fov))
+      return fail(APIRL_ERR_INVALID, "voxels too small for the scanner size (walks above 1e5 segments)");
+  }
+  for (int i = 0; i < sino->n_segments; i++)
+    if (sino->min_ring_diff[i] > sino->max_ring_diff[i])
+      return fail(APIRL_ERR_INVALID, "segment %d: minimum ring difference above maximum", i);
+  p->is3d = 1;
+  p->scanner = sino->scanner;
+  p->g = make_img_geom(img->nx, img->ny, img->nz, img->dx, img->dy, img->dz);
+  const bool built = mmr ? build_tables_mmr(sino->n_proj, sino->n_r, sino->n_rings, sino->n_segments,
+                                            sino->min_ring_diff, sino->max_ring_diff, p->host)
+                         : build_tables_3d(sino->n_proj, sino->n_r, sino->n_rings, sino->r_fov, sino->axial_fov,
+                                           sino->r_scanner, sino->n_segments, sino->min_ring_diff,
+                                           sino->max_ring_diff, p->host);
+  if (!built) return fail(APIRL_ERR_INVALID, "segment table yields no sinograms");
+  p->t.n_proj = sino->n_proj;
+  p->t.n_r = sino->n_r;
+  p->t.n_sinos = p->host.n_sinos;
+  p->t.is3d = 1;
+  p->n_rings = sino->n_rings;
+  p->r_fov = mmr ? kMmrRFov : sino->r_fov;
+  p->axial_fov = mmr ? kMmrAxialFov : sino->axial_fov;
+  p->r_scanner = mmr ? kMmrRadius : sino->r_scanner;
+  p->min_rd.assign(sino->min_ring_diff, sino->min_ring_diff + sino->n_segments);
+  p->max_rd.assign(sino->max_ring_diff, sino->max_ring_diff + sino->n_segments);
+  if ((int64_t)p->t.n_sinos * p->t.n_proj * p->t.n_r >= ((int64_t)1 << 40))
+    return fail(APIRL_ERR_INVALID, "sinogram too large");
+  return APIRL_OK;
+}
+}  // namespace apirl
 
 extern "C" {
 
@@ -245,85 +299,33 @@ apirl_status apirl_mmr_lor_table(int n_proj, int n_r, float* h_lor) {
 apirl_status apirl_projector_create_3d_mmr(const apirl_image_geom* img, int n_proj, int n_r, int n_rings,
                                            int n_segments, const int* min_ring_diff, const int* max_ring_diff,
                                            int device, apirl_projector** out) {
-  if (!out) return fail(APIRL_ERR_INVALID, "null output pointer");
-  *out = nullptr;
-  if (!valid_img(img)) return fail(APIRL_ERR_INVALID, "invalid image geometry");
-  if (n_proj < 2 || n_r <= 0 || n_rings <= 0 || n_segments <= 0 || !min_ring_diff || !max_ring_diff)
-    return fail(APIRL_ERR_INVALID, "invalid mMR sinogram geometry (need n_proj >= 2, n_r, n_rings, segments)");
-  if (!walk_bounded(img, apirl::kMmrRadius + apirl::kMmrDoi, apirl::kMmrAxialFov))
-    return fail(APIRL_ERR_INVALID, "voxels too small for the scanner size (walks above 1e5 segments)");
-  for (int i = 0; i < n_segments; i++)
-    if (min_ring_diff[i] > max_ring_diff[i])
-      return fail(APIRL_ERR_INVALID, "segment %d: minimum ring difference above maximum", i);
-  DEVICE_SCOPE(device);
-  apirl_projector* p = new apirl_projector;
-  p->device = device;
-  p->is3d = 1;
-  p->scanner = APIRL_SCANNER_MMR;
-  p->g = apirl::make_img_geom(img->nx, img->ny, img->nz, img->dx, img->dy, img->dz);
-  if (!apirl::build_tables_mmr(n_proj, n_r, n_rings, n_segments, min_ring_diff, max_ring_diff, p->host)) {
-    delete p;
-    return fail(APIRL_ERR_INVALID, "segment table yields no sinograms");
-  }
-  p->t.n_proj = n_proj;
-  p->t.n_r = n_r;
-  p->t.n_sinos = p->host.n_sinos;
-  p->t.is3d = 1;
-  p->n_rings = n_rings;
-  p->r_fov = apirl::kMmrRFov;
-  p->axial_fov = apirl::kMmrAxialFov;
-  p->r_scanner = apirl::kMmrRadius;
-  p->min_rd.assign(min_ring_diff, min_ring_diff + n_segments);
-  p->max_rd.assign(max_ring_diff, max_ring_diff + n_segments);
-  apirl_status st = finish_create(p, out);
-  if (st != APIRL_OK) { std::string m = g_err; apirl_projector_destroy(p); g_err = m; }
-  return st;
+  apirl_sino3d_geom sino;
+  memset(&sino, 0, sizeof sino);
+  sino.n_proj = n_proj;
+  sino.n_r = n_r;
+  sino.n_rings = n_rings;
+  sino.n_segments = n_segments;
+  sino.min_ring_diff = min_ring_diff;
+  sino.max_ring_diff = max_ring_diff;
+  sino.scanner = APIRL_SCANNER_MMR;
+  return apirl_projector_create_3d(img, &sino, device, out);
 }
 
 apirl_status apirl_projector_create_3d(const apirl_image_geom* img, const apirl_sino3d_geom* sino, int device,
                                        apirl_projector** out) {
   if (!out) return fail(APIRL_ERR_INVALID, "null output pointer");
   *out = nullptr;
-  if (sino && sino->scanner == APIRL_SCANNER_MMR)
-    return apirl_projector_create_3d_mmr(img, sino->n_proj, sino->n_r, sino->n_rings, sino->n_segments,
-                                         sino->min_ring_diff, sino->max_ring_diff, device, out);
-  if (sino && sino->scanner != APIRL_SCANNER_CYLINDRICAL) return fail(APIRL_ERR_INVALID, "unknown scanner %d", sino->scanner);
-  if (!valid_img(img)) return fail(APIRL_ERR_INVALID, "invalid image geometry");
-  if (!sino || sino->n_proj <= 0 || sino->n_r <= 0 || sino->n_rings <= 0 || sino->n_segments <= 0 ||
-      !sino->min_ring_diff || !sino->max_ring_diff || !(sino->r_fov > 0) || !(sino->axial_fov > 0) ||
-      !(sino->r_scanner > sino->r_fov))
-    return fail(APIRL_ERR_INVALID, "invalid 3D sinogram geometry");
-  if (!walk_bounded(img, sino->r_scanner, sino->axial_fov))
-    return fail(APIRL_ERR_INVALID, "voxels too small for the scanner size (walks above 1e5 segments)");
-  for (int i = 0; i < sino->n_segments; i++)
-    if (sino->min_ring_diff[i] > sino->max_ring_diff[i])
-      return fail(APIRL_ERR_INVALID, "segment %d: minimum ring difference above maximum", i);
-  DEVICE_SCOPE(device);
   apirl_projector* p = new apirl_projector;
-  p->device = device;
-  p->is3d = 1;
-  p->g = apirl::make_img_geom(img->nx, img->ny, img->nz, img->dx, img->dy, img->dz);
-  if (!apirl::build_tables_3d(sino->n_proj, sino->n_r, sino->n_rings, sino->r_fov, sino->axial_fov,
-                              sino->r_scanner, sino->n_segments, sino->min_ring_diff, sino->max_ring_diff,
-                              p->host)) {
+  apirl_status st = apirl::setup_3d(img, sino, p);
+  if (st != APIRL_OK) {
     delete p;
-    return fail(APIRL_ERR_INVALID, "segment table yields no sinograms");
+    return st;
   }
-  p->t.n_proj = sino->n_proj;
-  p->t.n_r = sino->n_r;
-  p->t.n_sinos = p->host.n_sinos;
-  p->t.is3d = 1;
-  p->n_rings = sino->n_rings;
-  p->r_fov = sino->r_fov;
-  p->axial_fov = sino->axial_fov;
-  p->r_scanner = sino->r_scanner;
-  p->min_rd.assign(sino->min_ring_diff, sino->min_ring_diff + sino->n_segments);
-  p->max_rd.assign(sino->max_ring_diff, sino->max_ring_diff + sino->n_segments);
-  if ((int64_t)p->t.n_sinos * p->t.n_proj * p->t.n_r >= ((int64_t)1 << 40)) {
-    delete p;
-    return fail(APIRL_ERR_INVALID, "sinogram too large");
+  {
+    DEVICE_SCOPE(device);
+    p->device = device;
+    st = finish_create(p, out);
   }
-  apirl_status st = finish_create(p, out);
   if (st != APIRL_OK) { std::string m = g_err; apirl_projector_destroy(p); g_err = m; }
   return st;
 }
@@ -350,10 +352,7 @@ void apirl_projector_destroy(apirl_projector* p) {
     cudaFree(p->d_zs[k]);
     cudaFree(p->d_zoff[k]);
   }
-  cudaFree(p->pad.pA);
-  cudaFree(p->pad.pT);
-  cudaFree(p->pad.bA);
-  cudaFree(p->pad.bT);
+  cudaFree(p->pad.pA);  // the block of all four padded images
   cudaFree(p->pad.eA);
   cudaFree(p->pad.eT);
   if (p->ev0) cudaEventDestroy(p->ev0);
@@ -787,6 +786,32 @@ apirl_status apirl_projector_set_option(apirl_projector* p, int option, int valu
       if (value != APIRL_SPARSE_ZERO_COUNT && value != APIRL_SPARSE_GEOMETRY)
         return fail(APIRL_ERR_INVALID, "unknown sparse image kind %d", value);
       p->sparse_image = value;
+      return APIRL_OK;
+    case APIRL_OPT_L2_PERSIST: {
+      if (value && !use_dual(p))
+        return fail(APIRL_ERR_NOT_SUPPORTED, "the L2 window covers the padded 3D layouts");
+      DEVICE_SCOPE(p->device);
+      p->pad.window = 0;
+      p->pad.hit_ratio = 0.f;
+      if (value) {
+        int max_window = 0, max_persist = 0;
+        CK(cudaDeviceGetAttribute(&max_window, cudaDevAttrMaxAccessPolicyWindowSize, p->device));
+        CK(cudaDeviceGetAttribute(&max_persist, cudaDevAttrMaxPersistingL2CacheSize, p->device));
+        const size_t want = (size_t)4 * p->pad.lim * sizeof(float);
+        const size_t win = want < (size_t)max_window ? want : (size_t)max_window;
+        const size_t aside = win < (size_t)max_persist ? win : (size_t)max_persist;
+        if (win == 0 || aside == 0) return fail(APIRL_ERR_NOT_SUPPORTED, "this device has no persisting L2");
+        // The set-aside is a limit of this process's context on the device.
+        CK(cudaDeviceSetLimit(cudaLimitPersistingL2CacheSize, aside));
+        p->pad.window = win;
+        p->pad.hit_ratio = (float)((double)aside / (double)win);
+      }
+      return APIRL_OK;
+    }
+    case APIRL_OPT_LIST_ORDER:
+      if (value != 0 && (value < 32 || value > apirl::kNzTile || (value & (value - 1))))
+        return fail(APIRL_ERR_INVALID, "list order: 0, or a power of two from 32 to %d", apirl::kNzTile);
+      p->nz.order = value;
       return APIRL_OK;
     case APIRL_OPT_ACCUMULATE: {
       if (value != APIRL_ACC_ATOMIC && value != APIRL_ACC_WARP && value != APIRL_ACC_COMPENSATED)

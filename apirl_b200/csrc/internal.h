@@ -105,6 +105,11 @@ struct PadBuffers {
   int acc = 0;
   float* eA = nullptr;
   float* eT = nullptr;
+  // window > 0 (APIRL_OPT_L2_PERSIST): the padded kernels launch with an L2
+  // access policy window of that many bytes from pA (the four images are one
+  // block pA, pT, bA, bT), hit_ratio of it persisting.
+  size_t window = 0;
+  float hit_ratio = 0.f;
 };
 // Bins per tile of the list building (one block each).
 constexpr int kNzTile = 2048;
@@ -116,6 +121,7 @@ struct NzList {
   int* tiles = nullptr;
   int* n_list = nullptr;
   int64_t cap = 0;
+  int order = 0;  // APIRL_OPT_LIST_ORDER: 0 = bin order, else groups of this size by walk length
 };
 // lik_mode: 0 = over e != 0, 1 = over e > 0, 2 = over ratio > 0.  back = 0: no backprojection.
 cudaError_t launch_em_pass(const ImgGeom& g, const LorTable& t, SubsetSel s, const void* counts, int counts_dtype,
@@ -246,6 +252,8 @@ cudaError_t launch_sens_batch(const SensJob* d_jobs, int njobs, int64_t nblocks,
 }  // namespace apirl
 
 typedef int apirl_status;
+struct apirl_image_geom;
+struct apirl_sino3d_geom;
 
 // Projector object behind the opaque apirl_projector handle.
 struct apirl_projector {
@@ -305,6 +313,9 @@ apirl_status apirl_internal_fail(apirl_status code, const char* msg);
 apirl_status apirl_internal_pending(void);
 
 namespace apirl {
+// The host half of apirl_projector_create_3d: geometry checks and host tables
+// into p (no device work; p->device and the device tables are not set).
+apirl_status setup_3d(const apirl_image_geom* img, const apirl_sino3d_geom* sino, apirl_projector* p);
 // Room in p->nz for the list of `total` bins (cudaMalloc: call outside graph
 // capture; a captured sparse pass without room walks every bin's chunk).
 apirl_status prepare_nz_list(apirl_projector* p, int64_t total);

@@ -13,8 +13,10 @@
 #include <cuda_runtime.h>
 #include <cstdint>
 #include <cfloat>
+#include <climits>
 #include <atomic>
 #include <mutex>
+#include <utility>
 #include <vector>
 #include "internal.h"
 #include "siddon.cuh"
@@ -451,6 +453,24 @@ __global__ void __launch_bounds__(kBlock) k_em_pass_rays(ImgGeom g, LorTable t, 
   if ((threadIdx.x & 31) == 0) partials[((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5] = term;
 }
 
+// The warp-aggregated scatter of one bin's ratio r along its ray; every lane
+// of the warp calls it (live == false: nothing to add).
+__device__ __forceinline__ void scatter_bin_warp(const ImgGeom& g, const LorTable& t, const BinPos& p, bool live,
+                                                 float r, const PadBuffers& pad) {
+  const int px = g.nx + 2 * kPad, py = g.ny + 2 * kPad;
+  Walk3 w;
+  w.n = 0;
+  bool tr = false;
+  if (live) {
+    const float4 L = __ldcg(t.lor + (int64_t)p.a * t.n_r + p.l);
+    const float2 z = __ldcg(t.z + p.g);
+    const float vx = A_SUB(L.z, L.x), vy = A_SUB(L.w, L.y);
+    tr = fabsf(vx) >= fabsf(vy);
+    siddon3_setup(L.x, L.y, z.x, vx, vy, A_SUB(z.y, z.x), g, w);
+  }
+  siddon3_scatter_pad_warp(w, g, tr ? py : 1, tr ? 1 : px, px * py, pad.lim, r, tr ? pad.bT : pad.bA, live);
+}
+
 // ---- backprojection over the padded pair (3D, one float ray per bin) -------
 // The fused pass's scatter alone: warps pull 32-bin chunks from a counter
 // and scatter seg * v into the padded backprojection pair (rays running
@@ -474,6 +494,16 @@ __global__ void __launch_bounds__(kBlock, kPersistMinBlocks) k_scatter_persist(
     c = __shfl_sync(0xffffffffu, c, 0);
     if ((int64_t)c >= nchunks) break;
     const int64_t b = (int64_t)c * 32 + lane;
+    if (ACC == 1) {  // warp-aggregated: the whole warp scatters together
+      BinPos p{0, 0, 0, 0};
+      float v = 0.f;
+      if (b < total) {
+        p = decode(b, t, s);
+        v = load_bin(vin, vin_mode, b, p, t);
+      }
+      scatter_bin_warp(g, t, p, v != 0.f, v, pad);
+      continue;
+    }
     if (b < total) {
       const BinPos p = decode(b, t, s);
       const float v = load_bin(vin, vin_mode, b, p, t);
@@ -611,10 +641,12 @@ __global__ void __launch_bounds__(kNzBlock) k_nz_write(LorTable t, SubsetSel s, 
 // the additive term, the likelihood term, the ratio m / e and the scatter of
 // seg * ratio into the matching padded backprojection.  ci: the bin's index
 // in the counts / additive layout.  Returns the likelihood term (lik_term).
+// Accumulation form 1 (warp-aggregated) scatters outside, with the whole
+// warp (scatter_bin_warp): the ratio is handed back in *r_out instead.
 template <int U, int ACC>
 __device__ __forceinline__ double em_bin_pad(const ImgGeom& g, const LorTable& t, const BinPos& p, float m,
                                              int64_t ci, const float* __restrict__ add, const PadBuffers& pad,
-                                             int back, int skip_zero) {
+                                             int back, int skip_zero, float* r_out = nullptr) {
   const int px = g.nx + 2 * kPad, py = g.ny + 2 * kPad;
   const int uz = px * py;
   const float4 L = t.lor[(int64_t)p.a * t.n_r + p.l];
@@ -628,6 +660,10 @@ __device__ __forceinline__ double em_bin_pad(const ImgGeom& g, const LorTable& t
   if (add) e = A_ADD(e, __ldg(add + ci));
   const float r = (m != 0.f && e != 0.f) ? A_DIV(m, e) : 0.f;
   const double term = e != 0.f ? lik_term(m, e, skip_zero) : 0.0;
+  if (ACC == 1) {
+    *r_out = r;
+    return term;
+  }
   if (back && r != 0.f) {
     const float4 L2 = __ldcg(t.lor + (int64_t)p.a * t.n_r + p.l);
     const float2 z2 = __ldcg(t.z + p.g);
@@ -636,6 +672,80 @@ __device__ __forceinline__ double em_bin_pad(const ImgGeom& g, const LorTable& t
     siddon3_scatter_pad<ACC>(w2, g, ux, uy, uz, pad.lim, r, tr ? pad.bT : pad.bA, tr ? pad.eT : pad.eA);
   }
   return term;
+}
+
+// k_nz_write with the tile's entries ordered by walk length (APIRL_OPT_LIST_ORDER):
+// the tile's bins with counts are gathered in bin order into shared memory,
+// each gets its walk's segment count as key, and every aligned group of
+// `group` entries (a power of two <= kNzTile) is sorted, longest walk first
+// (ties: lower bin first), by a bitonic network; the entries keep their
+// tile's place in the list.
+template <typename CT>
+__global__ void __launch_bounds__(kNzBlock) k_nz_write_sorted(ImgGeom g, LorTable t, SubsetSel s,
+                                                              const CT* __restrict__ counts, int counts_packed,
+                                                              int64_t total, const int* __restrict__ tiles,
+                                                              int* __restrict__ list, int group) {
+  __shared__ int key[kNzTile];
+  __shared__ int val[kNzTile];
+  __shared__ int warp_n[kNzBlock / 32];
+  __shared__ int run;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  if (threadIdx.x == 0) run = 0;
+  __syncthreads();
+  const int64_t base = (int64_t)blockIdx.x * kNzTile;
+  for (int i = 0; i < kNzTile; i += kNzBlock) {
+    const int64_t b = base + i + threadIdx.x;
+    const bool has = b < total && bin_has_count<CT>(b, t, s, counts, counts_packed);
+    const unsigned mask = __ballot_sync(0xffffffffu, has);
+    if (lane == 0) warp_n[warp] = __popc(mask);
+    __syncthreads();
+    int off = run;
+    for (int w = 0; w < warp; w++) off += warp_n[w];
+    if (has) val[off + __popc(mask & ((1u << lane) - 1u))] = (int)b;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      int sum = 0;
+      for (int w = 0; w < kNzBlock / 32; w++) sum += warp_n[w];
+      run += sum;
+    }
+    __syncthreads();
+  }
+  const int cnt = run;
+  for (int i = threadIdx.x; i < kNzTile; i += kNzBlock) {
+    if (i < cnt) {
+      const BinPos p = decode((int64_t)val[i], t, s);
+      const float4 L = t.lor[(int64_t)p.a * t.n_r + p.l];
+      const float2 z = t.z[p.g];
+      Walk3 w;
+      siddon3_setup(L.x, L.y, z.x, A_SUB(L.z, L.x), A_SUB(L.w, L.y), A_SUB(z.y, z.x), g, w);
+      key[i] = w.n;
+    } else {
+      key[i] = -1;  // after every real entry of its group
+      val[i] = INT_MAX;
+    }
+  }
+  __syncthreads();
+  // entry a goes before entry b: the longer walk, then the lower bin
+  auto before = [](int ka, int va, int kb, int vb) { return ka > kb || (ka == kb && va < vb); };
+  for (int k = 2; k <= group; k <<= 1)
+    for (int j = k >> 1; j > 0; j >>= 1) {
+      for (int i = threadIdx.x; i < kNzTile; i += kNzBlock) {
+        const int l = i ^ j;
+        if (l > i) {
+          // final stage: every group in the same direction
+          const bool fwd = k == group || (i & k) == 0;
+          const bool swap = fwd ? before(key[l], val[l], key[i], val[i]) : before(key[i], val[i], key[l], val[l]);
+          if (swap) {
+            const int tk = key[i], tv = val[i];
+            key[i] = key[l]; val[i] = val[l];
+            key[l] = tk; val[l] = tv;
+          }
+        }
+      }
+      __syncthreads();
+    }
+  const int off = tiles[blockIdx.x];
+  for (int i = threadIdx.x; i < cnt; i += kNzBlock) list[off + i] = val[i];
 }
 
 // The padded-layout fused pass as a persistent kernel: each warp takes the
@@ -662,16 +772,19 @@ __global__ void __launch_bounds__(kBlock, LIST ? kListMinBlocks : kPersistMinBlo
     if ((int64_t)c >= nchunks) break;
     const int64_t item = (int64_t)c * 32 + lane;
     double term = 0.0;
+    BinPos p{0, 0, 0, 0};
+    float r = 0.f;
     if (item < n_items) {
       const int64_t b = LIST ? (int64_t)list[item] : item;
-      const BinPos p = decode(b, t, s);
+      p = decode(b, t, s);
       const int64_t row = counts_packed ? ((int64_t)(p.g - t.g0) * s.nk + p.k) : ((int64_t)p.g * t.n_proj + p.a);
       const int64_t ci = row * t.n_r + p.l;
       const float m = load_count<CT>(counts, ci);
       if (!(skip_zero && m == 0.f))
         term = em_bin_pad<LIST ? kListGatherUnroll : APIRL_GATHER_UNROLL, ACC>(g, t, p, m, ci, add, pad, back,
-                                                                                skip_zero);
+                                                                                skip_zero, &r);
     }
+    if (ACC == 1) scatter_bin_warp(g, t, p, back && r != 0.f, r, pad);  // the whole warp
     #pragma unroll
     for (int o = 16; o > 0; o >>= 1) term += __shfl_down_sync(0xffffffffu, term, o);
     if (lane == 0) partials[c] = term;
@@ -1241,6 +1354,31 @@ __global__ void __launch_bounds__(kBlock) k_subset_sums(LorTable t, int nsub, co
 
 inline unsigned grid_for(int64_t total) { return (unsigned)((total + kBlock - 1) / kBlock); }
 
+// Launch of a kernel over the padded layouts: with pad.window
+// (APIRL_OPT_L2_PERSIST), an L2 access policy window over the block of the
+// four padded images, hits persisting, misses streaming.
+template <typename... KArgs, typename... Args>
+cudaError_t pad_launch(const PadBuffers& pad, dim3 grid, dim3 block, cudaStream_t st, void (*kernel)(KArgs...),
+                       Args&&... args) {
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = grid;
+  cfg.blockDim = block;
+  cfg.dynamicSmemBytes = 0;
+  cfg.stream = st;
+  cudaLaunchAttribute at[1];
+  if (pad.window) {
+    at[0].id = cudaLaunchAttributeAccessPolicyWindow;
+    at[0].val.accessPolicyWindow.base_ptr = pad.pA;
+    at[0].val.accessPolicyWindow.num_bytes = pad.window;
+    at[0].val.accessPolicyWindow.hitRatio = pad.hit_ratio;
+    at[0].val.accessPolicyWindow.hitProp = cudaAccessPropertyPersisting;
+    at[0].val.accessPolicyWindow.missProp = cudaAccessPropertyStreaming;
+    cfg.attrs = at;
+    cfg.numAttrs = 1;
+  }
+  return cudaLaunchKernelEx(&cfg, kernel, std::forward<Args>(args)...);
+}
+
 // The fused 3D kernels use no shared memory: give the SM's unified L1 /
 // shared storage to L1.  Set once per device (function attributes belong to
 // the device's context).
@@ -1393,13 +1531,17 @@ cudaError_t launch_backproject_pad(const ImgGeom& g, const LorTable& t, SubsetSe
   const unsigned grid = (unsigned)(need < resident ? need : resident);
   // The second pair (img2) takes plain atomics; so does the first beside it.
   const int acc = two ? 0 : pad.acc;
+  float* none = nullptr;
   if (acc == 1)
-    k_scatter_persist<1><<<grid, 128, 0, st>>>(g, t, s, vin, vin_mode, pad, total, counter, nullptr, nullptr);
+    e = pad_launch(pad, dim3(grid), dim3(128), st, k_scatter_persist<1>, g, t, s, vin, vin_mode, pad, total, counter,
+                   none, none);
   else if (acc == 2)
-    k_scatter_persist<2><<<grid, 128, 0, st>>>(g, t, s, vin, vin_mode, pad, total, counter, nullptr, nullptr);
+    e = pad_launch(pad, dim3(grid), dim3(128), st, k_scatter_persist<2>, g, t, s, vin, vin_mode, pad, total, counter,
+                   none, none);
   else
-    k_scatter_persist<0><<<grid, 128, 0, st>>>(g, t, s, vin, vin_mode, pad, total, counter,
-                                               two ? pad2.bA : nullptr, two ? pad2.bT : nullptr);
+    e = pad_launch(pad, dim3(grid), dim3(128), st, k_scatter_persist<0>, g, t, s, vin, vin_mode, pad, total, counter,
+                   two ? pad2.bA : none, two ? pad2.bT : none);
+  if (e != cudaSuccess) return e;
   if ((e = cudaGetLastError()) != cudaSuccess) return e;
   if (two && (e = launch_pad_reduce(g, pad2, 1, nullptr, img2, nullptr, nullptr, 0.f, 0, st)) != cudaSuccess) return e;
   return launch_pad_reduce(g, pad, 1, nullptr, img, nullptr, nullptr, 0.f, 0, st);
@@ -1491,7 +1633,22 @@ cudaError_t launch_em_pass(const ImgGeom& g, const LorTable& t, SubsetSel s, con
           break;
       }
       k_nz_scan<<<1, 1024, 0, st>>>(nz.tiles, (int)n_tiles, nz.n_list);
-      switch (counts_dtype) {
+      if (nz.order > 0) {
+        switch (counts_dtype) {
+          case APIRL_F32:
+            k_nz_write_sorted<float><<<n_tiles, kNzBlock, 0, st>>>(g, t, s, (const float*)counts, counts_packed, total,
+                                                                   nz.tiles, nz.list, nz.order);
+            break;
+          case APIRL_U32:
+            k_nz_write_sorted<uint32_t><<<n_tiles, kNzBlock, 0, st>>>(g, t, s, (const uint32_t*)counts, counts_packed,
+                                                                      total, nz.tiles, nz.list, nz.order);
+            break;
+          default:
+            k_nz_write_sorted<uint16_t><<<n_tiles, kNzBlock, 0, st>>>(g, t, s, (const uint16_t*)counts, counts_packed,
+                                                                      total, nz.tiles, nz.list, nz.order);
+            break;
+        }
+      } else switch (counts_dtype) {
         case APIRL_F32:
           k_nz_write<float><<<n_tiles, kNzBlock, 0, st>>>(t, s, (const float*)counts, counts_packed, total, nz.tiles,
                                                           nz.list);
@@ -1509,14 +1666,15 @@ cudaError_t launch_em_pass(const ImgGeom& g, const LorTable& t, SubsetSel s, con
     }
 #define APIRL_PERSIST_ACC(CT, ACC)                                                                              \
   do {                                                                                                          \
+    const int* no_list = nullptr;                                                                               \
     if (use_list)                                                                                               \
-      k_em_pass_persist<CT, true, ACC><<<pgrid, block, 0, st>>>(g, t, s, (const CT*)counts, counts_packed, add,  \
-                                                                pad, back, partials, total, skip,                \
-                                                                persist_counter, nz.list, nz.n_list);            \
+      le = pad_launch(pad, dim3(pgrid), dim3(block), st, k_em_pass_persist<CT, true, ACC>, g, t, s,             \
+                      (const CT*)counts, counts_packed, add, pad, back, partials, total, skip, persist_counter,   \
+                      (const int*)nz.list, (const int*)nz.n_list);                                              \
     else                                                                                                        \
-      k_em_pass_persist<CT, false, ACC><<<pgrid, block, 0, st>>>(g, t, s, (const CT*)counts, counts_packed, add, \
-                                                                 pad, back, partials, total, skip,               \
-                                                                 persist_counter, nullptr, nullptr);             \
+      le = pad_launch(pad, dim3(pgrid), dim3(block), st, k_em_pass_persist<CT, false, ACC>, g, t, s,            \
+                      (const CT*)counts, counts_packed, add, pad, back, partials, total, skip, persist_counter,   \
+                      no_list, no_list);                                                                        \
   } while (0)
 #define APIRL_PERSIST(CT)                                  \
   do {                                                     \
@@ -1524,6 +1682,7 @@ cudaError_t launch_em_pass(const ImgGeom& g, const LorTable& t, SubsetSel s, con
     else if (pad.acc == 2) APIRL_PERSIST_ACC(CT, 2);       \
     else APIRL_PERSIST_ACC(CT, 0);                         \
   } while (0)
+    cudaError_t le = cudaSuccess;
     switch (counts_dtype) {
       case APIRL_F32: APIRL_PERSIST(float); break;
       case APIRL_U32: APIRL_PERSIST(uint32_t); break;
@@ -1532,6 +1691,7 @@ cudaError_t launch_em_pass(const ImgGeom& g, const LorTable& t, SubsetSel s, con
     }
 #undef APIRL_PERSIST
 #undef APIRL_PERSIST_ACC
+    if (le != cudaSuccess) return le;
     cudaError_t pe = cudaGetLastError();
     if (pe != cudaSuccess || !lik) return pe;
     int64_t np = chunks;
@@ -1643,17 +1803,17 @@ cudaError_t launch_force_positive(int64_t n, float* x, cudaStream_t st) {
 cudaError_t launch_pad_copy(const ImgGeom& g, const float* x, const PadBuffers& pad, cudaStream_t st) {
   dim3 grid((g.nx + 31) / 32, (g.ny + 31) / 32, g.nz), block(32, 8);
   PadDims d{g.nx, g.ny, g.nz};
-  k_pad_copy<<<grid, block, 0, st>>>(d, x, pad.pA, pad.pT);
-  return cudaGetLastError();
+  return pad_launch(pad, grid, block, st, k_pad_copy, d, x, pad.pA, pad.pT);
 }
 
 cudaError_t launch_pad_reduce(const ImgGeom& g, const PadBuffers& pad, int mode, float* x, float* bp,
                               const float* sens, const float* thr_ptr, float thr_value, int ge, cudaStream_t st) {
   dim3 grid((g.nx + 31) / 32, (g.ny + 31) / 32, g.nz), block(32, 8);
   PadDims d{g.nx, g.ny, g.nz};
-  k_pad_reduce<<<grid, block, 0, st>>>(d, pad.bA, pad.bT, mode, x, bp, sens, thr_ptr, thr_value, ge,
-                                       pad.acc == 2 ? pad.eA : nullptr, pad.acc == 2 ? pad.eT : nullptr);
-  return cudaGetLastError();
+  float* eA = pad.acc == 2 ? pad.eA : nullptr;
+  float* eT = pad.acc == 2 ? pad.eT : nullptr;
+  return pad_launch(pad, grid, block, st, k_pad_reduce, d, pad.bA, pad.bT, mode, x, bp, sens, thr_ptr, thr_value, ge,
+                    eA, eT);
 }
 
 cudaError_t launch_exp_nonzero(int64_t n, float* v, cudaStream_t st) {

@@ -180,20 +180,13 @@ __device__ __forceinline__ float siddon3_gather_pad(Walk3 w, const ImgGeom& g, i
 // How a scatter step adds v into img[at] (APIRL_OPT_ACCUMULATE):
 //  0  one atomic add per segment (the reference's `#pragma omp atomic` float
 //     add, SiddonProjector.cpp:547-548, in the atomics' order);
-//  1  warp-aggregated: the lanes of a warp that add to the same voxel in the
-//     same step sum their values in lane order and one of them adds the sum;
+//  1  warp-aggregated (siddon3_scatter_pad_warp below, not here);
 //  2  compensated: the atomic returns the value it added to, so the rounding
 //     error of that addition (TwoSum, Knuth) is known exactly and goes into
 //     a second image err; img + err is the sum to about twice float precision.
 template <int ACC>
 __device__ __forceinline__ void acc_add(float* __restrict__ img, float* __restrict__ err, unsigned at, float v) {
-  if (ACC == 1) {
-    const unsigned act = __activemask();
-    const unsigned peers = __match_any_sync(act, at);
-    float sum = 0.f;
-    for (unsigned m = peers; m; m &= m - 1u) sum = A_ADD(sum, __shfl_sync(peers, v, __ffs(m) - 1));
-    if ((int)(threadIdx.x & 31) == __ffs(peers) - 1) atomicAdd(img + at, sum);
-  } else if (ACC == 2) {
+  if (ACC == 2) {
     const float old = atomicAdd(img + at, v);
     const float s = A_ADD(old, v);
     const float bv = A_SUB(s, old);
@@ -232,6 +225,55 @@ __device__ __forceinline__ void siddon3_scatter_pad(Walk3 w, const ImgGeom& g, i
     if (cx) { w.i += w.iinc; idx += sx; w.ax = A_ADD(w.ax, w.axu); }
     else if (cy) { w.j += w.jinc; idx += sy; w.ay = A_ADD(w.ay, w.ayu); }
     else { w.k += w.kinc; idx += sz; w.az = A_ADD(w.az, w.azu); }
+  }
+}
+
+// The warp-aggregated scatter (accumulation form 1): all 32 lanes of the warp
+// call it together, each with its own walk (live == false: a lane that adds
+// nothing), and step through their walks in lockstep to the longest one.  At
+// each step the lanes whose segments fall on the same address (same image and
+// voxel: the lanes of a warp may scatter into different images) sum their
+// values in lane order (through a per-lane slot of shared memory; blocks of
+// at most 256 threads) and the lowest of them adds the sum with one atomic.
+// Bounds: the guarded walk's clamp, else the reference's six-sided test.
+__device__ __forceinline__ void siddon3_scatter_pad_warp(Walk3 w, const ImgGeom& g, int ux, int uy, int uz,
+                                                         unsigned lim, float r, float* __restrict__ img, bool live) {
+  __shared__ float slot[256];
+  const int lane = (int)(threadIdx.x & 31), warp0 = (int)threadIdx.x - lane;
+  const int n = live ? w.n : 0;
+  const int nmax = __reduce_max_sync(0xffffffffu, n);
+  const int sx = w.iinc * ux, sy = w.jinc * uy, sz = w.kinc * uz;
+  int idx = live ? (w.k + kPad) * uz + (w.j + kPad) * uy + (w.i + kPad) * ux : 0;
+  for (int m = 0; m < nmax; m++) {
+    unsigned at = lim;  // no voxel: this lane adds nothing this step
+    float v = 0.f;
+    if (m < n) {
+      bool cx, cy;
+      const float an = next_crossing(w, cx, cy);
+      const float seg = A_MUL(A_SUB(an, w.ac), w.L);
+      const bool inb = w.guarded || (((unsigned)w.i < (unsigned)g.nx) & ((unsigned)w.j < (unsigned)g.ny) &
+                                     ((unsigned)w.k < (unsigned)g.nz));
+      if (inb) {
+        at = min((unsigned)idx, lim - 1u);
+        v = A_MUL(seg, r);
+      }
+      w.ac = an;
+      if (cx) { w.i += w.iinc; idx += sx; w.ax = A_ADD(w.ax, w.axu); }
+      else if (cy) { w.j += w.jinc; idx += sy; w.ay = A_ADD(w.ay, w.ayu); }
+      else { w.k += w.kinc; idx += sz; w.az = A_ADD(w.az, w.azu); }
+    }
+    // the address, or a value no address has (one group per idle lane)
+    const unsigned long long key =
+        at < lim ? (unsigned long long)(uintptr_t)(img + at) : ~0ull - (unsigned long long)lane;
+    const unsigned peers = __match_any_sync(0xffffffffu, key);
+    slot[threadIdx.x] = v;
+    __syncwarp();
+    if (at < lim && lane == __ffs(peers) - 1) {
+      float sum = 0.f;
+      for (unsigned q = peers; q; q &= q - 1u) sum = A_ADD(sum, slot[warp0 + __ffs(q) - 1]);
+      atomicAdd(img + at, sum);
+    }
+    __syncwarp();
   }
 }
 

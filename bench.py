@@ -324,6 +324,10 @@ def run_gpu(args):
     log(f"autotuned fused-kernel block size: {best_block}")
     P.set_option(_l.APIRL_OPT_KERNEL_TIMING, 1)
     P.set_option(_l.APIRL_OPT_PERSISTENT, args.persistent)
+    if args.l2_persist:
+        P.set_option(_l.APIRL_OPT_L2_PERSIST, 1)
+    if args.list_order:
+        P.set_option(_l.APIRL_OPT_LIST_ORDER, args.list_order)
     if args.accumulate != "atomic":
         P.set_option(_l.APIRL_OPT_ACCUMULATE, {"warp": _l.APIRL_ACC_WARP,
                                                "compensated": _l.APIRL_ACC_COMPENSATED}[args.accumulate])
@@ -534,6 +538,7 @@ def run_gpu(args):
                        WORKLOAD + f" (profiling case: segments |rd| <= {args.max_ring_diff} only)",
                        "subsets": NSUB, "counts_dtype": "uint32", "em_block": best_block,
                        "alpha": args.alpha, "persistent": args.persistent, "accumulate": args.accumulate,
+                       "l2_persist": bool(args.l2_persist), "list_order": args.list_order,
                        "pass": ("sparse: bins with zero counts not walked, their likelihood terms -x.Z_s from "
                                 "per-subset zero-count images Z_s = A_s^T 1[m=0], all 21 computed inside the "
                                 "timed region and amortized over the timed sub-iterations") if sparse else
@@ -797,7 +802,10 @@ def mixed_jobs(args, served, log):
     jobs = _make_jobs(specs, dev, log, c2_every=10 if served else 0)
     torch.cuda.empty_cache()
     budget = int(args.budget_gb * (1 << 30))
-    ref, t_plain, each = _plain(jobs, dev)
+    if args.no_plain:  # (profiler captures of the batched form alone)
+        ref, t_plain, each = None, float("nan"), np.full(len(jobs), np.nan)
+    else:
+        ref, t_plain, each = _plain(jobs, dev)
     if served:
         arrivals = np.cumsum(np.random.default_rng(5).exponential(1.0 / args.rate, len(jobs)))
         res, lat, makespan = serve(jobs, arrivals, budget_bytes=budget)
@@ -811,7 +819,7 @@ def mixed_jobs(args, served, log):
         t_new = time.perf_counter() - t0
         b.close()
     errs = []
-    for r, p in zip(res, ref):
+    for r, p in zip(res, ref if ref is not None else []):
         fin = np.isfinite(p)
         if not np.array_equal(np.isfinite(r[0]), fin):
             raise RuntimeError("a batched job's image is not finite where its solo run's is")
@@ -820,7 +828,7 @@ def mixed_jobs(args, served, log):
     out = {
         "value": len(jobs) / t_new * 3600, "unit": "recon/h",
         "plain_value": len(jobs) / t_plain * 3600, "speedup_vs_plain": t_plain / t_new,
-        "max_rel_l2_vs_plain": max(errs),
+        "max_rel_l2_vs_plain": max(errs) if errs else None,
         "workload": ("Poisson arrivals at %.0f jobs/s of " % args.rate if served else "all at once: ") +
                     f"{len(jobs)} mixed OSEM jobs: images {{64,128,256}}^2 x {{1,41,81}} slices, 1.3N r/angles, "
                     "span 1, 2-4 iterations x 7-21 subsets, 1e5-1e8 counts uint32" +
@@ -1003,19 +1011,25 @@ def precision_study(subiters, log, threads=None):
             xg = f["x"].cpu().numpy()
             row[name] = {"rel_l2": _rel(xg, x64), "max_abs": _max_abs(xg, x64),
                          "lik_rel": abs(f["lik"].item() - lik64) / abs(lik64)}
-        row["u16_equals_f32"] = bool(np.array_equal(forms["u16"]["x"].cpu().numpy().view(np.uint32),
-                                                    forms["f32"]["x"].cpu().numpy().view(np.uint32)))
+        # same arithmetic; only the atomics' order differs between the two runs
+        row["u16_vs_f32_rel_l2"] = _rel(forms["u16"]["x"].cpu().numpy(), forms["f32"]["x"].cpu().numpy())
         log(json.dumps(row))
         rows.append(row)
 
-    # One ratio sinogram of subset 0, backprojected in each accumulation form.
+    # One ratio sinogram of subset 0, backprojected in each accumulation form,
+    # against the exact (FP64) sum of the float contributions the float walk
+    # makes, so that only the accumulation's rounding is measured (against the
+    # FP64 walk, the geometry's 1e-2 would hide it).
     s = 0
     x1 = forms["f32"]["x"].cpu().numpy()
     est32 = orc.project_3d(sg, ig, x1, s, NSUB, threads=thr)
     m32 = np.ascontiguousarray(meas64[:, s::NSUB, :]).reshape(-1).astype(np.float32)
     ratio32 = orc.inverse_divide(m32, est32)
-    bp_exact = orc.backproject_3d(sg, ig, ratio32.astype(np.float64), s, NSUB, dtype=np.float64, threads=thr)
-    acc = {"reference_serial_fp32_rel_l2": _rel(orc.backproject_3d(sg, ig, ratio32, s, NSUB, threads=1), bp_exact)}
+    bp_exact = orc.backproject_3d_exact_sum(sg, ig, ratio32, s, NSUB, threads=thr)
+    bp_fp64walk = orc.backproject_3d(sg, ig, ratio32.astype(np.float64), s, NSUB, dtype=np.float64, threads=thr)
+    acc = {"reference_serial_fp32_rel_l2": _rel(orc.backproject_3d(sg, ig, ratio32, s, NSUB, threads=1), bp_exact),
+           "fp64_walk_vs_float_walk_rel_l2": _rel(bp_fp64walk, bp_exact),
+           "against": "the FP64 sum of the float walk's own contributions"}
     r_dev = torch.from_numpy(ratio32).to(dev)
     for name, Q in (("atomic", P), ("warp", Pw), ("compensated", Pc)):
         bpg = torch.zeros(nv, dtype=torch.float32, device=dev)
@@ -1080,6 +1094,10 @@ def main():
                      help="walk geometry: f32 = the reference's float arithmetic (headline); f64 = precision mode")
     ap_.add_argument("--no-one-thread", action="store_true",
                      help="reference arm: skip the extra one-thread sub-iteration")
+    ap_.add_argument("--l2-persist", action="store_true",
+                     help="L2 persisting window over the padded images (APIRL_OPT_L2_PERSIST)")
+    ap_.add_argument("--list-order", type=int, default=0,
+                     help="sparse passes: list entries by walk length within groups of this size (0: bin order)")
     ap_.add_argument("--accumulate", default="atomic", choices=["atomic", "warp", "compensated"],
                      help="how the backprojection scatter accumulates (APIRL_OPT_ACCUMULATE)")
     ap_.add_argument("--cpu-threads", type=int, default=None,
@@ -1090,6 +1108,8 @@ def main():
     ap_.add_argument("--max-ring-diff", type=int, default=None,
                      help="profiling: keep segments |rd| <= this (smaller case of the same kernels)")
     ap_.add_argument("--jobs", type=int, default=64)
+    ap_.add_argument("--no-plain", action="store_true",
+                     help="batched / served workloads: skip the plain-driver comparison (profiler captures)")
     ap_.add_argument("--rate", type=float, default=20.0, help="served: mean arrivals per second")
     ap_.add_argument("--budget-gb", type=float, default=96.0)
     ap_.add_argument("--traffic-bytes", type=float, default=None,

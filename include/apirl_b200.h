@@ -203,8 +203,20 @@ enum {
   APIRL_OPT_EM_BLOCK = 3,
   APIRL_OPT_PERSISTENT = 4,
   APIRL_OPT_SPARSE_IMAGE = 5,
-  APIRL_OPT_ACCUMULATE = 6
+  APIRL_OPT_ACCUMULATE = 6,
+  APIRL_OPT_L2_PERSIST = 7,
+  APIRL_OPT_LIST_ORDER = 8
 };
+/* APIRL_OPT_L2_PERSIST (default 0): 1 = the padded 3D passes launch with an L2
+ * access policy window over the projector's padded images and
+ * backprojections (persisting lines), and the process's persisting-L2 limit
+ * on the device is set to that window (as far as the device allows).
+ * APIRL_OPT_LIST_ORDER (default 0): order of the sparse passes' list of bins
+ * with counts within each tile of 2048 bins.  0 = bin order (neighbouring
+ * lanes walk neighbouring rays); n > 0 = within groups of n entries (a power
+ * of two, 32..2048) by walk length, longest first (the lanes of a warp walk
+ * rays of similar lengths).  Results equal bin order's up to the atomics'
+ * order; the likelihood partials then sum in another order. */
 enum { APIRL_SPARSE_ZERO_COUNT = 0, APIRL_SPARSE_GEOMETRY = 1 };
 /* APIRL_OPT_ACCUMULATE (default APIRL_ACC_ATOMIC): how the 3D passes over the
  * padded layouts (the persistent fused pass, its sparse forms, and

@@ -397,6 +397,43 @@ void backproject3d(const Sino3DG<T>& s, int subset, int nsub, const ImgG<T>& g, 
       for (long v = 0; v < nvox; v++) img[v] += part[t][v];
 }
 
+// Backproject (mode 0) with the float walk and float contributions w * 1 * m
+// of backproject3d<float>, summed in double: the exact sum, to double
+// rounding, of the very values the float backprojection adds (so that the
+// error of a float accumulation can be told apart from the geometry's).
+void backproject3d_f32_acc64(const Sino3DG<float>& s, int subset, int nsub, const ImgG<float>& g, const float* vin,
+                             double* img, int threads) {
+  const int nk = subset_nproj(s.nProj, subset, nsub);
+  const long per = (long)nk * s.nR;
+  const long total = per * s.nSinos;
+  const long nvox = (long)g.nx * g.ny * g.nz;
+  if (threads < 1) threads = 1;
+  std::vector<std::vector<double>> part(threads);
+  #pragma omp parallel num_threads(threads)
+  {
+    const int t = omp_get_thread_num();
+    part[t].assign(nvox, 0.0);
+    double* dst = part[t].data();
+    const long lo = total * t / threads, hi = total * (t + 1) / threads;
+    for (long b = lo; b < hi; b++) {
+      const float m = vin[b];
+      if (m == 0) continue;
+      const int gsino = (int)(b / per);
+      const int k = (int)((b % per) / s.nR), l = (int)(b % s.nR);
+      const int a = subset_angle(k, subset, nsub);
+      for_rays(s, gsino, a, l, Sampling(), false, [&](const Lor<float>& L, float za, float zb) {
+        siddon3d<float>(L.p1x, L.p1y, za, L.p2x - L.p1x, L.p2y - L.p1y, zb - za, g, [&](int i, int j, int kk, float w) {
+          if (!inb(i, j, kk, g.nx, g.ny, g.nz)) return;
+          const float v = w * 1.0f * m;
+          dst[((long)kk * g.ny + j) * g.nx + i] += (double)v;
+        });
+      });
+    }
+  }
+  for (int t = 0; t < threads; t++)
+    for (long v = 0; v < nvox; v++) img[v] += part[t][v];
+}
+
 // ---------------------------------------------------------------------------
 // 2D projector.  Bins [angle][r].
 template <typename T>
@@ -758,6 +795,12 @@ int or_sino3d_z_f64(const or_sino3d* d, double* z1, double* z2) {
 
 OR_FWD3(f32, float)
 OR_FWD3(f64, double)
+
+int or_backproject_3d_f32_acc64(const or_sino3d* d, int subset, int nsub, int nx, int ny, int nz, float dx,
+                                float dy, float dz, const float* vin, double* img, int threads) {
+  backproject3d_f32_acc64(mk<float>(d), subset, nsub, make_img<float>(nx, ny, nz, dx, dy, dz), vin, img, threads);
+  return 0;
+}
 
 int or_project_3d_tables_f32(int nSinos, int nProj, int nR, const float* lor, const float* z, int subset, int nsub,
                              int nx, int ny, int nz, float dx, float dy, float dz, const float* img, float* out,

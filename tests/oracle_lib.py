@@ -77,6 +77,7 @@ class Oracle:
             getattr(L, f"or_mlem_threshold_{suf}").argtypes = [_l, _vp]
             getattr(L, f"or_mlem_threshold_{suf}").restype = T
             getattr(L, f"or_update_{suf}").argtypes = [_l, _vp, _vp, _vp, T, _i]
+        L.or_backproject_3d_f32_acc64.argtypes = [_vp, _i, _i, _i, _i, _i, _f, _f, _f, _vp, _vp, _i]
         for suf in ("f32", "f64"):
             getattr(L, f"or_sampled_3d_{suf}").argtypes = [_vp, _i, _i, _i, _i, _i, _i, _i, _i, _i, _f, _f, _f,
                                                            _vp, _vp, _vp, _i]
@@ -135,6 +136,17 @@ class Oracle:
         s = _sino3d_struct(sg)
         getattr(self.L, f"or_backproject_3d_{self._suf(dt)}")(ctypes.byref(s), subset, nsub, *_img_args(ig),
                                                              _p(values), _p(img), threads or self.threads)
+        return img
+
+    def backproject_3d_exact_sum(self, sg, ig, values, subset=-1, nsub=1, threads=None):
+        """The float backprojection's own contributions (float walk, float
+        segment * value) summed in double: what a float accumulation of them
+        would give without rounding."""
+        values = np.ascontiguousarray(values, dtype=np.float32)
+        img = np.zeros(ig.n_voxels, np.float64)
+        s = _sino3d_struct(sg)
+        self.L.or_backproject_3d_f32_acc64(ctypes.byref(s), subset, nsub, *_img_args(ig), _p(values), _p(img),
+                                           threads or self.threads)
         return img
 
     def divide_and_backproject_3d(self, sg, ig, vin, vest, subset=-1, nsub=1, dtype=np.float32, threads=None):

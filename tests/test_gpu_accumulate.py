@@ -4,7 +4,8 @@ add's rounding error kept in a second padded pair).
 
 Tolerances
   backprojection, fused pass (any form) vs the oracle ..... rel L2 <= 1e-5
-  compensated backprojection vs an FP64 sum of the same float segments:
+  compensated backprojection vs the FP64 sum of the same float contributions
+  (float walk, float segment * value, summed in double):
     no worse than plain atomics, and <= 1e-7 relative L2
   forms that a projector's path cannot take are refused (APIRL_ERR_NOT_SUPPORTED)
 """
@@ -59,7 +60,7 @@ def test_backprojection_forms(oracle, form):
     got = img.cpu().numpy()
     assert rel(got, oracle.backproject_3d(sg, ig, v, sub, ns)) <= 1e-5
     assert rel(ones.cpu().numpy(), oracle.backproject_3d(sg, ig, np.ones_like(v), sub, ns)) <= 1e-5
-    exact = oracle.backproject_3d(sg, ig, v.astype(np.float64), sub, ns, dtype=np.float64)
+    exact = oracle.backproject_3d_exact_sum(sg, ig, v, sub, ns)
     err = rel(got, exact)
     if form == _lib.APIRL_ACC_COMPENSATED:
         Pa = ap.SiddonProjector(ig, sg)

@@ -149,18 +149,20 @@ def test_precision_first_subiteration():
       reference float arithmetic ....... image rel L2 <= 2e-2, likelihood <= 1e-4
       FP64 walk geometry ............... image rel L2 <= 2e-6, likelihood <= 1e-6
       uint16 counts .................... bit-exact round trip, image equal to uint32's
-      one ratio backprojection ......... compensated atomics no worse than plain
-                                         atomics, and <= 1e-6 relative L2
+                                         up to the atomics' order (rel L2 <= 1e-6)
+      one ratio backprojection ......... against the FP64 sum of the float walk's own
+                                         contributions: compensated atomics better
+                                         than plain atomics, and <= 1e-7 relative L2
       adjoint residual of the operators  <= 1e-6"""
     import bench
     r = bench.precision_study(1, lambda m: None)
     row = r["subiterations"][0]
-    assert r["u16_round_trip"] and row["u16_equals_f32"]
+    assert r["u16_round_trip"] and row["u16_vs_f32_rel_l2"] <= 1e-6
     assert row["f32"]["rel_l2"] <= 2e-2 and row["f32"]["lik_rel"] <= 1e-4
     assert row["f64alpha"]["rel_l2"] <= 2e-6 and row["f64alpha"]["lik_rel"] <= 1e-6
     for form in ("f32_warp", "f32_comp"):
         assert row[form]["rel_l2"] <= 2e-2
         assert abs(row[form]["rel_l2"] - row["f32"]["rel_l2"]) <= 1e-5
     acc = r["backprojection_accumulation"]
-    assert acc["gpu_compensated_rel_l2"] <= acc["gpu_atomic_rel_l2"] and acc["gpu_compensated_rel_l2"] <= 1e-6
+    assert acc["gpu_compensated_rel_l2"] < acc["gpu_atomic_rel_l2"] and acc["gpu_compensated_rel_l2"] <= 1e-7
     assert all(v <= 1e-6 for v in r["adjoint_residual"].values())

@@ -1,0 +1,84 @@
+"""Projector options that change how the padded passes run, not what they
+compute: the L2 persisting window (APIRL_OPT_L2_PERSIST) and the order of the
+sparse passes' list of bins (APIRL_OPT_LIST_ORDER, by walk length within
+groups).  Each gives the default's image to the atomics' order (rel L2 <=
+1e-6) and likelihood to 1e-7 relative (the geometry image of each run is its
+own atomics' sum), over two passes in a row."""
+import numpy as np
+import pytest
+
+torch = pytest.importorskip("torch")
+pytestmark = pytest.mark.gpu
+
+import apirl_b200 as ap  # noqa: E402
+from apirl_b200 import _lib  # noqa: E402
+from apirl_b200.geometry import ImageGeom, Sino3DGeom  # noqa: E402
+
+DEV = torch.device("cuda:0")
+
+
+def t(a):
+    return torch.from_numpy(np.ascontiguousarray(a)).to(DEV)
+
+
+def rel(a, b):
+    a = np.asarray(a, np.float64)
+    b = np.asarray(b, np.float64)
+    return float(np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-300))
+
+
+@pytest.fixture(scope="module", autouse=True)
+def _gpu():
+    if not torch.cuda.is_available():
+        pytest.skip("no CUDA device")
+    ap.load_library()
+
+
+def run_passes(option, value, sparse):
+    ig, sg = ImageGeom(64, 64, 13, 2.08, 2.08, 2.03), Sino3DGeom.span1(40, 72, 7, 66.56, 7 * 4.054, 200.0, 6)
+    rng = np.random.default_rng(21)
+    P = ap.SiddonProjector(ig, sg)
+    x0 = (rng.random(ig.n_voxels, dtype=np.float32) + 0.5).astype(np.float32)
+    est = torch.zeros(P.num_bins(), dtype=torch.float32, device=DEV)
+    P.project(t(x0), est)
+    meas = rng.poisson(est.cpu().numpy() * 0.3).astype(np.uint32)
+    if option is not None:
+        P.set_option(option, value)
+    sub, ns = 1, 4
+    g = torch.zeros(ig.n_voxels, dtype=torch.float32, device=DEV)
+    P.backproject_ones(g, sub, ns)
+    x = t(x0)
+    bp = torch.zeros(ig.n_voxels, dtype=torch.float32, device=DEV)
+    liks = []
+    P.set_option(_lib.APIRL_OPT_SPARSE_IMAGE, _lib.APIRL_SPARSE_GEOMETRY)
+    for _ in range(2):
+        lik = torch.zeros(1, dtype=torch.float64, device=DEV)
+        if sparse:
+            P.em_pass_sparse(t(meas), x, bp, g, g, sub, ns, lik=lik)
+        else:
+            P.em_pass(t(meas), x, bp, g, sub, ns, lik=lik)
+        torch.cuda.synchronize()
+        liks.append(lik.item())
+    return x.cpu().numpy(), np.array(liks)
+
+
+@pytest.mark.parametrize("sparse", [False, True])
+def test_l2_window_changes_nothing(sparse):
+    ref, lref = run_passes(None, 0, sparse)
+    got, lgot = run_passes(_lib.APIRL_OPT_L2_PERSIST, 1, sparse)
+    assert rel(got, ref) <= 1e-6 and np.allclose(lgot, lref, rtol=1e-7, atol=0)
+
+
+@pytest.mark.parametrize("group", [32, 256, 2048])
+def test_list_order_changes_nothing(group):
+    ref, lref = run_passes(None, 0, True)
+    got, lgot = run_passes(_lib.APIRL_OPT_LIST_ORDER, group, True)
+    assert rel(got, ref) <= 1e-6 and np.allclose(lgot, lref, rtol=1e-7, atol=0)
+
+
+def test_list_order_rejects_other_sizes():
+    ig, sg = ImageGeom(16, 16, 3, 2.0, 2.0, 2.0), Sino3DGeom.span1(8, 16, 3, 16.0, 3 * 4.0, 100.0, 1)
+    P = ap.SiddonProjector(ig, sg)
+    for bad in (16, 100, 4096, -1):
+        with pytest.raises(ap.ApirlError):
+            P.set_option(_lib.APIRL_OPT_LIST_ORDER, bad)
