@@ -25,6 +25,7 @@ APIRL_OPT_SPARSE_IMAGE = 5
 APIRL_OPT_ACCUMULATE = 6
 APIRL_OPT_L2_PERSIST = 7
 APIRL_OPT_LIST_ORDER = 8
+APIRL_OPT_GATHER_UNROLL = 9
 APIRL_SPARSE_ZERO_COUNT = 0
 APIRL_SPARSE_GEOMETRY = 1
 APIRL_ACC_ATOMIC = 0
@@ -73,6 +74,11 @@ class ReconOptionsC(ctypes.Structure):
                 ("update_positive_sens", _i)]
 
 
+class TuneC(ctypes.Structure):
+    """apirl_tune: the fused pass's launch shape picked by apirl_projector_autotune_ex."""
+    _fields_ = [("block", _i), ("unroll", _i), ("ms", ctypes.c_double)]
+
+
 class JobDescC(ctypes.Structure):
     _fields_ = [("img", ImageGeomC), ("sino", Sino3DGeomC), ("h_counts", _vp), ("counts_dtype", _i),
                 ("h_mult", _vp), ("h_add", _vp), ("h_init", _vp), ("iters", _i), ("nsubsets", _i)]
@@ -99,6 +105,7 @@ SIGNATURES = {
     "apirl_projector_set_option": (_i, [_vp, _i, _i]),
     "apirl_projector_kernel_ms": (_i, [_vp, ctypes.POINTER(ctypes.c_double)]),
     "apirl_projector_autotune": (_i, [_vp, _vp, _i, _vp, _i, _i, _i, ctypes.POINTER(_i), _vp]),
+    "apirl_projector_autotune_ex": (_i, [_vp, _vp, _i, _vp, _vp, _i, _i, _i, ctypes.POINTER(TuneC), _vp]),
     "apirl_count_steps": (_i, [_vp, _i, _i, _vp, _vp]),
     "apirl_project": (_i, [_vp, _vp, _vp, _i, _i, _vp]),
     "apirl_backproject": (_i, [_vp, _vp, _vp, _i, _i, _vp]),

@@ -808,6 +808,11 @@ apirl_status apirl_projector_set_option(apirl_projector* p, int option, int valu
       }
       return APIRL_OK;
     }
+    case APIRL_OPT_GATHER_UNROLL:
+      if (value != 0 && value != 4 && value != 6 && value != 8)
+        return fail(APIRL_ERR_INVALID, "gather segments in flight: 0, 4, 6 or 8");
+      p->pad.unroll = value;
+      return APIRL_OK;
     case APIRL_OPT_LIST_ORDER:
       if (value != 0 && (value < 32 || value > apirl::kNzTile || (value & (value - 1))))
         return fail(APIRL_ERR_INVALID, "list order: 0, or a power of two from 32 to %d", apirl::kNzTile);
@@ -885,6 +890,75 @@ apirl_status apirl_projector_autotune(apirl_projector* p, const void* d_counts, 
   cudaFree(bp);
   if (st) return st;
   if (best_block) *best_block = best_b;
+  return APIRL_OK;
+}
+
+apirl_status apirl_projector_autotune_ex(apirl_projector* p, const void* d_counts, int counts_dtype,
+                                        const float* d_x, const float* d_zimg, int subset, int nsubsets, int repeats,
+                                        apirl_tune* out, void* stream) {
+  apirl_status st = check_em(p, d_counts, counts_dtype, d_x, d_x, subset, nsubsets);
+  if (st) return st;
+  if (!use_dual(p) || !p->persistent || p->pad.acc != APIRL_ACC_ATOMIC)
+    return fail(APIRL_ERR_NOT_SUPPORTED, "the launch shape is tuned for the persistent pass over the padded layouts "
+                                         "with plain atomics");
+  DEVICE_SCOPE(p->device);
+  cudaStream_t s = (cudaStream_t)stream;
+  const int64_t nv = (int64_t)p->g.nx * p->g.ny * p->g.nz;
+  float* bp = nullptr;
+  CK(cudaMalloc(&bp, nv * sizeof(float)));
+  cudaEvent_t a = nullptr, b = nullptr;
+  cudaError_t ce = cudaEventCreate(&a);
+  if (ce == cudaSuccess) ce = cudaEventCreate(&b);
+  const int blocks[] = {64, 96, 128, 192, 256};
+  const int unrolls[] = {4, 6, 8};
+  const int saved_timing = p->timing, saved_block = p->em_block, saved_unroll = p->pad.unroll;
+  p->timing = 0;
+  float best = 1e30f;
+  int best_b = p->em_block, best_u = p->pad.unroll;
+  if (repeats < 1) repeats = 1;
+  auto pass = [&]() {
+    return d_zimg ? apirl_em_project_backproject_sparse(p, d_counts, counts_dtype, 0, nullptr, d_x, bp, d_zimg,
+                                                        nullptr, subset, nsubsets, nullptr, s)
+                  : apirl_em_project_backproject(p, d_counts, counts_dtype, 0, nullptr, d_x, bp, subset, nsubsets,
+                                                 nullptr, s);
+  };
+  for (int blk : blocks) {
+    if (ce != cudaSuccess) break;
+    p->em_block = blk;
+    if ((ce = apirl::prepare_em_kernels(blk)) != cudaSuccess) break;
+    for (int u : unrolls) {
+      p->pad.unroll = u;
+      if ((ce = cudaMemsetAsync(bp, 0, nv * sizeof(float), s)) != cudaSuccess) break;
+      if ((st = pass())) break;  // warm-up (and the list, for the sparse pass)
+      if ((ce = cudaEventRecord(a, s)) != cudaSuccess) break;
+      for (int r = 0; r < repeats && !st; r++) st = pass();
+      if (st) break;
+      if ((ce = cudaEventRecord(b, s)) != cudaSuccess || (ce = cudaEventSynchronize(b)) != cudaSuccess) break;
+      float ms = 0;
+      if ((ce = cudaEventElapsedTime(&ms, a, b)) != cudaSuccess) break;
+      if (ms < best) { best = ms; best_b = blk; best_u = u; }
+    }
+    if (st) break;
+  }
+  p->timing = saved_timing;
+  if (!st && ce == cudaSuccess) {
+    p->em_block = best_b;
+    p->pad.unroll = best_u;
+    ce = apirl::prepare_em_kernels(best_b);
+  } else {
+    p->em_block = saved_block;
+    p->pad.unroll = saved_unroll;
+  }
+  if (a) cudaEventDestroy(a);
+  if (b) cudaEventDestroy(b);
+  cudaFree(bp);
+  if (st) return st;
+  if (ce != cudaSuccess) return cuda_fail(ce, "autotune");
+  if (out) {
+    out->block = best_b;
+    out->unroll = best_u;
+    out->ms = best / repeats;
+  }
   return APIRL_OK;
 }
 

@@ -110,6 +110,9 @@ struct PadBuffers {
   // block pA, pT, bA, bT), hit_ratio of it persisting.
   size_t window = 0;
   float hit_ratio = 0.f;
+  // Gather segments in flight of the fused pass (APIRL_OPT_GATHER_UNROLL: 4,
+  // 6 or 8; 0 = the pass kind's default).
+  int unroll = 0;
 };
 // Bins per tile of the list building (one block each).
 constexpr int kNzTile = 2048;

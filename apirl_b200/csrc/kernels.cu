@@ -754,7 +754,9 @@ __global__ void __launch_bounds__(kNzBlock) k_nz_write_sorted(ImgGeom g, LorTabl
 // full complement of warps until the end of the pass.  The bins of a chunk
 // are those of one warp in k_em_pass, and the chunk's likelihood partial goes
 // to partials[chunk]: results are identical to k_em_pass's.
-template <typename CT, bool LIST, int ACC>
+// UNROLL: gather segments in flight (0: the default of the pass kind,
+// kListGatherUnroll listed, APIRL_GATHER_UNROLL full).
+template <typename CT, bool LIST, int ACC, int UNROLL>
 __global__ void __launch_bounds__(kBlock, LIST ? kListMinBlocks : kPersistMinBlocks) k_em_pass_persist(
     ImgGeom g, LorTable t, SubsetSel s, const CT* __restrict__ counts, int counts_packed,
     const float* __restrict__ add, PadBuffers pad, int back, double* __restrict__ partials, int64_t total,
@@ -781,8 +783,8 @@ __global__ void __launch_bounds__(kBlock, LIST ? kListMinBlocks : kPersistMinBlo
       const int64_t ci = row * t.n_r + p.l;
       const float m = load_count<CT>(counts, ci);
       if (!(skip_zero && m == 0.f))
-        term = em_bin_pad<LIST ? kListGatherUnroll : APIRL_GATHER_UNROLL, ACC>(g, t, p, m, ci, add, pad, back,
-                                                                                skip_zero, &r);
+        term = em_bin_pad<UNROLL ? UNROLL : (LIST ? kListGatherUnroll : APIRL_GATHER_UNROLL), ACC>(
+            g, t, p, m, ci, add, pad, back, skip_zero, &r);
     }
     if (ACC == 1) scatter_bin_warp(g, t, p, back && r != 0.f, r, pad);  // the whole warp
     #pragma unroll
@@ -1462,23 +1464,34 @@ inline unsigned stream_grid(int64_t n) {
 
 }  // namespace
 
-// The persistent fused kernel for a counts type, list form and accumulation form.
+// The persistent fused kernel for a counts type, list form, accumulation form
+// and gather segments in flight (4, 6 or 8 with plain atomics; 0: default).
+template <typename CT, bool LIST>
+const void* persist_kernel_l(int acc, int unroll) {
+  if (acc == 1) return (const void*)k_em_pass_persist<CT, LIST, 1, 0>;
+  if (acc == 2) return (const void*)k_em_pass_persist<CT, LIST, 2, 0>;
+  switch (unroll) {
+    case 4: return (const void*)k_em_pass_persist<CT, LIST, 0, 4>;
+    case 6: return (const void*)k_em_pass_persist<CT, LIST, 0, 6>;
+    case 8: return (const void*)k_em_pass_persist<CT, LIST, 0, 8>;
+    default: return (const void*)k_em_pass_persist<CT, LIST, 0, 0>;
+  }
+}
 template <typename CT>
-const void* persist_kernel(bool list, int acc) {
-  if (list)
-    return acc == 1 ? (const void*)k_em_pass_persist<CT, true, 1>
-                    : acc == 2 ? (const void*)k_em_pass_persist<CT, true, 2> : (const void*)k_em_pass_persist<CT, true, 0>;
-  return acc == 1 ? (const void*)k_em_pass_persist<CT, false, 1>
-                  : acc == 2 ? (const void*)k_em_pass_persist<CT, false, 2> : (const void*)k_em_pass_persist<CT, false, 0>;
+const void* persist_kernel(bool list, int acc, int unroll) {
+  return list ? persist_kernel_l<CT, true>(acc, unroll) : persist_kernel_l<CT, false>(acc, unroll);
 }
 
 cudaError_t prepare_em_kernels(int block) {
   for (int acc = 0; acc < 3; acc++)
-    for (bool list : {false, true})
-      for (const void* f : {persist_kernel<float>(list, acc), persist_kernel<uint32_t>(list, acc),
-                            persist_kernel<uint16_t>(list, acc)}) {
-        cudaError_t e = fit_carveout(f, block, 0);
-        if (e != cudaSuccess) return e;
+    for (int unroll : {0, 4, 6, 8})
+      for (bool list : {false, true}) {
+        if (acc && unroll) continue;
+        for (const void* f : {persist_kernel<float>(list, acc, unroll), persist_kernel<uint32_t>(list, acc, unroll),
+                              persist_kernel<uint16_t>(list, acc, unroll)}) {
+          cudaError_t e = fit_carveout(f, block, 0);
+          if (e != cudaSuccess) return e;
+        }
       }
   return cudaSuccess;
 }
@@ -1593,9 +1606,9 @@ cudaError_t launch_em_pass(const ImgGeom& g, const LorTable& t, SubsetSel s, con
     const bool use_list = skip && nz.list && nz.tiles && nz.n_list && total <= nz.cap && total < ((int64_t)1 << 31);
     const void* pf;
     switch (counts_dtype) {
-      case APIRL_F32: pf = persist_kernel<float>(use_list, pad.acc); break;
-      case APIRL_U32: pf = persist_kernel<uint32_t>(use_list, pad.acc); break;
-      case APIRL_U16: pf = persist_kernel<uint16_t>(use_list, pad.acc); break;
+      case APIRL_F32: pf = persist_kernel<float>(use_list, pad.acc, pad.unroll); break;
+      case APIRL_U32: pf = persist_kernel<uint32_t>(use_list, pad.acc, pad.unroll); break;
+      case APIRL_U16: pf = persist_kernel<uint16_t>(use_list, pad.acc, pad.unroll); break;
       default: return cudaErrorInvalidValue;
     }
     // Fitted here unless the launch is being captured into a graph (the
@@ -1664,23 +1677,26 @@ cudaError_t launch_em_pass(const ImgGeom& g, const LorTable& t, SubsetSel s, con
       }
       if ((me = cudaMemsetAsync(partials, 0, (size_t)chunks * sizeof(double), st)) != cudaSuccess) return me;
     }
-#define APIRL_PERSIST_ACC(CT, ACC)                                                                              \
+#define APIRL_PERSIST_ACC(CT, ACC, U)                                                                           \
   do {                                                                                                          \
     const int* no_list = nullptr;                                                                               \
     if (use_list)                                                                                               \
-      le = pad_launch(pad, dim3(pgrid), dim3(block), st, k_em_pass_persist<CT, true, ACC>, g, t, s,             \
+      le = pad_launch(pad, dim3(pgrid), dim3(block), st, k_em_pass_persist<CT, true, ACC, U>, g, t, s,          \
                       (const CT*)counts, counts_packed, add, pad, back, partials, total, skip, persist_counter,   \
                       (const int*)nz.list, (const int*)nz.n_list);                                              \
     else                                                                                                        \
-      le = pad_launch(pad, dim3(pgrid), dim3(block), st, k_em_pass_persist<CT, false, ACC>, g, t, s,            \
+      le = pad_launch(pad, dim3(pgrid), dim3(block), st, k_em_pass_persist<CT, false, ACC, U>, g, t, s,         \
                       (const CT*)counts, counts_packed, add, pad, back, partials, total, skip, persist_counter,   \
                       no_list, no_list);                                                                        \
   } while (0)
 #define APIRL_PERSIST(CT)                                  \
   do {                                                     \
-    if (pad.acc == 1) APIRL_PERSIST_ACC(CT, 1);            \
-    else if (pad.acc == 2) APIRL_PERSIST_ACC(CT, 2);       \
-    else APIRL_PERSIST_ACC(CT, 0);                         \
+    if (pad.acc == 1) APIRL_PERSIST_ACC(CT, 1, 0);         \
+    else if (pad.acc == 2) APIRL_PERSIST_ACC(CT, 2, 0);    \
+    else if (pad.unroll == 4) APIRL_PERSIST_ACC(CT, 0, 4); \
+    else if (pad.unroll == 6) APIRL_PERSIST_ACC(CT, 0, 6); \
+    else if (pad.unroll == 8) APIRL_PERSIST_ACC(CT, 0, 8); \
+    else APIRL_PERSIST_ACC(CT, 0, 0);                      \
   } while (0)
     cudaError_t le = cudaSuccess;
     switch (counts_dtype) {

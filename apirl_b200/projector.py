@@ -132,6 +132,16 @@ class SiddonProjector:
                                                 repeats, ctypes.byref(best), _stream(stream)))
         return best.value
 
+    def autotune_shape(self, counts, x, zimg=None, subset=0, nsubsets=1, repeats=2, stream=None):
+        """apirl_projector_autotune_ex: block size and gather segments in flight
+        of the fused pass (the sparse pass over bins with counts when zimg is
+        given), timed on these counts; the projector keeps the fastest.
+        Returns (block, unroll, ms per pass)."""
+        out = _lib.TuneC()
+        check(self.lib.apirl_projector_autotune_ex(self.h, _ptr(counts), _counts_dtype(counts), _ptr(x), _ptr(zimg),
+                                                   subset, nsubsets, repeats, ctypes.byref(out), _stream(stream)))
+        return out.block, out.unroll, out.ms
+
     def last_kernel_ms(self):
         """CUDA-event duration of the last fused kernel (needs APIRL_OPT_KERNEL_TIMING)."""
         ms = ctypes.c_double()

@@ -348,6 +348,18 @@ def run_gpu(args):
         gev[1].record(stream)
         torch.cuda.synchronize(dev)
         geometry_ms = gev[0].elapsed_time(gev[1])
+    # The listed pass's launch shape (block size and gather segments in
+    # flight), tuned on this job's own data and geometry image, outside the
+    # timed region (apirl_projector_autotune_ex).
+    gather_unroll = None
+    if (nonzero and not args.em_block and args.persistent and args.alpha == "f32" and args.accumulate == "atomic"
+            and args.max_ring_diff is None):
+        best_block, gather_unroll, tune_ms = P.autotune_shape(counts, x, zimg=zimg[0], subset=0, nsubsets=NSUB,
+                                                              repeats=2, stream=stream)
+        bp.zero_()
+        torch.cuda.synchronize(dev)
+        log(f"autotuned listed pass: {best_block} threads per block, {gather_unroll} segments in flight, "
+            f"{tune_ms:.3f} ms")
 
     def zero_images():
         # Per-subset zero-count images of the sparse pass (once per
@@ -537,6 +549,7 @@ def run_gpu(args):
             "config": {"workload": WORKLOAD if args.max_ring_diff is None else
                        WORKLOAD + f" (profiling case: segments |rd| <= {args.max_ring_diff} only)",
                        "subsets": NSUB, "counts_dtype": "uint32", "em_block": best_block,
+                       "gather_unroll": gather_unroll if gather_unroll is not None else "default (6 listed, 4 full)",
                        "alpha": args.alpha, "persistent": args.persistent, "accumulate": args.accumulate,
                        "l2_persist": bool(args.l2_persist), "list_order": args.list_order,
                        "pass": ("sparse: bins with zero counts not walked, their likelihood terms -x.Z_s from "

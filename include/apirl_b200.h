@@ -205,8 +205,13 @@ enum {
   APIRL_OPT_SPARSE_IMAGE = 5,
   APIRL_OPT_ACCUMULATE = 6,
   APIRL_OPT_L2_PERSIST = 7,
-  APIRL_OPT_LIST_ORDER = 8
+  APIRL_OPT_LIST_ORDER = 8,
+  APIRL_OPT_GATHER_UNROLL = 9
 };
+/* APIRL_OPT_GATHER_UNROLL (default 0): segments of a walk whose image loads
+ * the persistent fused 3D pass issues before it adds any of them: 4, 6 or 8,
+ * or 0 for the pass kind's default (6 over a list of bins, 4 over every bin).
+ * Results do not depend on it.  Plain atomics only. */
 /* APIRL_OPT_L2_PERSIST (default 0): 1 = the padded 3D passes launch with an L2
  * access policy window over the projector's padded images and
  * backprojections (persisting lines), and the process's persisting-L2 limit
@@ -239,6 +244,24 @@ apirl_status apirl_projector_kernel_ms(apirl_projector* p, double* ms);
  * keeps the fastest; its size goes to *best_block.  Allocates one scratch image. */
 apirl_status apirl_projector_autotune(apirl_projector* p, const void* d_counts, int counts_dtype, const float* d_x,
                                      int subset, int nsubsets, int repeats, int* best_block, void* stream);
+/* The launch shape of the persistent fused 3D pass that runs fastest on this
+ * projector's own data: every block size of 64, 96, 128, 192, 256 threads
+ * with 4, 6 and 8 gather segments in flight (APIRL_OPT_EM_BLOCK,
+ * APIRL_OPT_GATHER_UNROLL), each timed over `repeats` passes of subset
+ * `subset` on `stream`: the sparse pass over the bins with counts when
+ * d_zimg is given (the zero-count or geometry image, as APIRL_OPT_SPARSE_IMAGE
+ * says), else the full pass; the image is not changed.  The projector keeps
+ * the fastest; it goes to *out (block, unroll, ms per pass).  Allocates one
+ * scratch image.  No counterpart in the reference, whose block sizes come
+ * from its .par files (reconGPU/src/CuMlemSinogram3d.cu:157-170). */
+typedef struct {
+  int block;
+  int unroll;
+  double ms;
+} apirl_tune;
+apirl_status apirl_projector_autotune_ex(apirl_projector* p, const void* d_counts, int counts_dtype,
+                                        const float* d_x, const float* d_zimg, int subset, int nsubsets, int repeats,
+                                        apirl_tune* out, void* stream);
 /* Number of Siddon segments of every bin of a subset, written to d_steps (int32). */
 apirl_status apirl_count_steps(apirl_projector* p, int subset, int nsubsets, int32_t* d_steps, void* stream);
 

@@ -82,3 +82,43 @@ def test_list_order_rejects_other_sizes():
     for bad in (16, 100, 4096, -1):
         with pytest.raises(ap.ApirlError):
             P.set_option(_lib.APIRL_OPT_LIST_ORDER, bad)
+
+
+@pytest.mark.parametrize("unroll", [4, 6, 8])
+@pytest.mark.parametrize("sparse", [False, True])
+def test_gather_unroll_changes_nothing(unroll, sparse):
+    ref, lref = run_passes(None, 0, sparse)
+    got, lgot = run_passes(_lib.APIRL_OPT_GATHER_UNROLL, unroll, sparse)
+    assert rel(got, ref) <= 1e-6 and np.allclose(lgot, lref, rtol=1e-7, atol=0)
+
+
+def test_autotune_shape_keeps_the_fastest_and_the_image():
+    """apirl_projector_autotune_ex on the listed pass: a block size and gather
+    depth from the candidates, a positive time, the input image unchanged;
+    passes afterwards equal the default's."""
+    ig, sg = ImageGeom(64, 64, 13, 2.08, 2.08, 2.03), Sino3DGeom.span1(40, 72, 7, 66.56, 7 * 4.054, 200.0, 6)
+    rng = np.random.default_rng(21)
+    P = ap.SiddonProjector(ig, sg)
+    x0 = (rng.random(ig.n_voxels, dtype=np.float32) + 0.5).astype(np.float32)
+    est = torch.zeros(P.num_bins(), dtype=torch.float32, device=DEV)
+    P.project(t(x0), est)
+    meas = t(rng.poisson(est.cpu().numpy() * 0.3).astype(np.uint32))
+    P.set_option(_lib.APIRL_OPT_SPARSE_IMAGE, _lib.APIRL_SPARSE_GEOMETRY)
+    g = torch.zeros(ig.n_voxels, dtype=torch.float32, device=DEV)
+    P.backproject_ones(g, 1, 4)
+    x = t(x0)
+    block, unroll, ms = P.autotune_shape(meas, x, zimg=g, subset=1, nsubsets=4)
+    torch.cuda.synchronize()
+    assert block in (64, 96, 128, 192, 256) and unroll in (4, 6, 8) and ms > 0
+    assert np.array_equal(x.cpu().numpy(), x0)
+    bp = torch.zeros(ig.n_voxels, dtype=torch.float32, device=DEV)
+    lik = torch.zeros(1, dtype=torch.float64, device=DEV)
+    P.em_pass_sparse(meas, x, bp, g, g, 1, 4, lik=lik)
+    Q = ap.SiddonProjector(ig, sg)
+    Q.set_option(_lib.APIRL_OPT_SPARSE_IMAGE, _lib.APIRL_SPARSE_GEOMETRY)
+    xq = t(x0)
+    lq = torch.zeros(1, dtype=torch.float64, device=DEV)
+    Q.em_pass_sparse(meas, xq, bp, g, g, 1, 4, lik=lq)
+    torch.cuda.synchronize()
+    assert rel(x.cpu().numpy(), xq.cpu().numpy()) <= 1e-6
+    assert abs(lik.item() - lq.item()) <= 1e-9 * abs(lq.item())
