@@ -1051,20 +1051,31 @@ __device__ __forceinline__ double pad_copy_tile(const PadDims& d, const float* _
                                                 int z, int lx, int ly, float (*tile)[33]) {
   const int64_t base = (int64_t)z * d.nx * d.ny;
   double dot = 0.0;
-  for (int r = ly; r < 32; r += 8) {
-    const int yy = y0 + r, xx = x0 + lx;
+  // The tile's loads (x, and gimg for the dot) are all issued before its
+  // first store.
+  float xv[4], gv[4];
+  #pragma unroll
+  for (int q = 0; q < 4; q++) {
+    const int yy = y0 + ly + 8 * q, xx = x0 + lx;
+    xv[q] = gv[q] = 0.f;
     if (xx < d.nx && yy < d.ny) {
       const int64_t i = base + (int64_t)yy * d.nx + xx;
-      const float v = x[i];
-      tile[r][lx] = v;
-      pA[d.a(xx, yy, z)] = v;
-      if (gimg) {
-        const float gv = gimg[i];
-        if (gv != 0.f) dot += (double)v * (double)gv;
-      }
+      xv[q] = x[i];
+      if (gimg) gv[q] = gimg[i];
+    }
+  }
+  #pragma unroll
+  for (int q = 0; q < 4; q++) {
+    const int r = ly + 8 * q;
+    const int yy = y0 + r, xx = x0 + lx;
+    if (xx < d.nx && yy < d.ny) {
+      tile[r][lx] = xv[q];
+      pA[d.a(xx, yy, z)] = xv[q];
+      if (gv[q] != 0.f) dot += (double)xv[q] * (double)gv[q];
     }
   }
   __syncthreads();
+  #pragma unroll
   for (int r = ly; r < 32; r += 8) {
     const int xx = x0 + r, yy = y0 + lx;
     if (xx < d.nx && yy < d.ny) pT[d.t(xx, yy, z)] = tile[lx][r];
@@ -1093,26 +1104,38 @@ __device__ __forceinline__ void pad_reduce_tile(const PadDims& d, float* __restr
                                                 int z, int lx, int ly, float (*tile)[33],
                                                 float* __restrict__ eA = nullptr, float* __restrict__ eT = nullptr) {
   const int64_t base = (int64_t)z * d.nx * d.ny;
-  for (int r = ly; r < 32; r += 8) {  // transposed buffer, read along y
-    const int xx = x0 + r, yy = y0 + lx;
+  // Every load of the tile (both padded backprojections, and x and sens for
+  // the update or bp for the sum) is issued before the first barrier, so
+  // that all are in flight together.
+  float av[4], xv[4], sv[4];
+  #pragma unroll
+  for (int q = 0; q < 4; q++) {
+    const int r = ly + 8 * q;
+    {
+      const int xx = x0 + r, yy = y0 + lx;  // transposed buffer, read along y
+      if (xx < d.nx && yy < d.ny) {
+        const int64_t it = d.t(xx, yy, z);
+        tile[lx][r] = eT ? A_ADD(bT[it], eT[it]) : bT[it];
+      }
+    }
+    const int yy = y0 + r, xx = x0 + lx;
+    av[q] = xv[q] = sv[q] = 0.f;
     if (xx < d.nx && yy < d.ny) {
-      const int64_t it = d.t(xx, yy, z);
-      tile[lx][r] = eT ? A_ADD(bT[it], eT[it]) : bT[it];
+      const int64_t ia = d.a(xx, yy, z);
+      av[q] = eA ? A_ADD(bA[ia], eA[ia]) : bA[ia];
+      const int64_t i = base + (int64_t)yy * d.nx + xx;
+      if (mode == 0) {
+        xv[q] = x[i];
+        sv[q] = sens[i];
+      } else {
+        xv[q] = bp[i];
+      }
     }
   }
   __syncthreads();
   float bv[4];
   #pragma unroll
-  for (int q = 0; q < 4; q++) {
-    const int r = ly + 8 * q;
-    const int yy = y0 + r, xx = x0 + lx;
-    if (xx < d.nx && yy < d.ny) {
-      const int64_t ia = d.a(xx, yy, z);
-      bv[q] = A_ADD(eA ? A_ADD(bA[ia], eA[ia]) : bA[ia], tile[r][lx]);
-    } else {
-      bv[q] = 0.f;
-    }
-  }
+  for (int q = 0; q < 4; q++) bv[q] = A_ADD(av[q], tile[ly + 8 * q][lx]);
   __syncthreads();
   #pragma unroll
   for (int q = 0; q < 4; q++) {
@@ -1130,11 +1153,10 @@ __device__ __forceinline__ void pad_reduce_tile(const PadDims& d, float* __restr
       if (eA) eA[d.a(xx, yy, z)] = 0.f;
       const int64_t i = base + (int64_t)yy * d.nx + xx;
       if (mode == 0) {
-        const float sv = sens[i];
-        const bool okv = ge ? (sv >= thr) : (sv > thr);
-        x[i] = okv ? A_DIV(A_MUL(x[i], bv[q]), sv) : 0.f;
+        const bool okv = ge ? (sv[q] >= thr) : (sv[q] > thr);
+        x[i] = okv ? A_DIV(A_MUL(xv[q], bv[q]), sv[q]) : 0.f;
       } else {
-        bp[i] = A_ADD(bp[i], bv[q]);
+        bp[i] = A_ADD(xv[q], bv[q]);
       }
     }
   }
