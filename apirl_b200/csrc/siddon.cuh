@@ -107,6 +107,30 @@ __device__ __forceinline__ float next_crossing(const Walk3& w, bool& cx, bool& c
 #endif
 }
 
+// One step of a guarded padded walk past its next crossing (x when cx, y
+// when cy, else z): the linear index moves one voxel along that axis and the
+// axis's crossing parameter advances by its increment.  APIRL_STEP_SELECT
+// computes all three candidate parameters and selects (no divergent branch;
+// the same float additions on the same operands, so the walk is unchanged):
+// on B200 0.5 % faster on the listed pass and 4 % slower on the full pass
+// than the branch, so it is off by default.
+#ifndef APIRL_STEP_SELECT
+#define APIRL_STEP_SELECT 0
+#endif
+__device__ __forceinline__ void step_pad(Walk3& w, int& idx, bool cx, bool cy, int sx, int sy, int sz) {
+#if APIRL_STEP_SELECT
+  const float ax = A_ADD(w.ax, w.axu), ay = A_ADD(w.ay, w.ayu), az = A_ADD(w.az, w.azu);
+  idx += cx ? sx : (cy ? sy : sz);
+  w.ax = cx ? ax : w.ax;
+  w.ay = cy ? ay : w.ay;
+  w.az = (cx | cy) ? w.az : az;
+#else
+  if (cx) { idx += sx; w.ax = A_ADD(w.ax, w.axu); }
+  else if (cy) { idx += sy; w.ay = A_ADD(w.ay, w.ayu); }
+  else { idx += sz; w.az = A_ADD(w.az, w.azu); }
+#endif
+}
+
 // Walks over an image padded with a kPad-voxel zero border on every side
 // (padded sizes n+2 kPad; unit strides ux, uy, uz of the padded layout; `lim`
 // = number of padded voxels).  When w.guarded the entry and exit indices lie
@@ -142,9 +166,7 @@ __device__ __forceinline__ float siddon3_gather_pad(Walk3 w, const ImgGeom& g, i
         sa[u] = A_MUL(A_SUB(an, w.ac), w.L);
         ia[u] = idx;
         w.ac = an;
-        if (cx) { idx += sx; w.ax = A_ADD(w.ax, w.axu); }
-        else if (cy) { idx += sy; w.ay = A_ADD(w.ay, w.ayu); }
-        else { idx += sz; w.az = A_ADD(w.az, w.azu); }
+        step_pad(w, idx, cx, cy, sx, sy, sz);
       }
       #pragma unroll
       for (int u = 0; u < U; u++) va[u] = __ldg(img + min((unsigned)ia[u], lim - 1u));
@@ -157,9 +179,7 @@ __device__ __forceinline__ float siddon3_gather_pad(Walk3 w, const ImgGeom& g, i
       const float v = __ldg(img + min((unsigned)idx, lim - 1u));
       acc = A_ADD(acc, A_MUL(A_MUL(A_SUB(an, w.ac), w.L), v));
       w.ac = an;
-      if (cx) { idx += sx; w.ax = A_ADD(w.ax, w.axu); }
-      else if (cy) { idx += sy; w.ay = A_ADD(w.ay, w.ayu); }
-      else { idx += sz; w.az = A_ADD(w.az, w.azu); }
+      step_pad(w, idx, cx, cy, sx, sy, sz);
     }
     return acc;
   }
@@ -209,9 +229,7 @@ __device__ __forceinline__ void siddon3_scatter_pad(Walk3 w, const ImgGeom& g, i
       const float an = next_crossing(w, cx, cy);
       acc_add<ACC>(img, err, min((unsigned)idx, lim - 1u), A_MUL(A_MUL(A_SUB(an, w.ac), w.L), r));
       w.ac = an;
-      if (cx) { idx += sx; w.ax = A_ADD(w.ax, w.axu); }
-      else if (cy) { idx += sy; w.ay = A_ADD(w.ay, w.ayu); }
-      else { idx += sz; w.az = A_ADD(w.az, w.azu); }
+      step_pad(w, idx, cx, cy, sx, sy, sz);
     }
     return;
   }
