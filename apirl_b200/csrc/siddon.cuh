@@ -150,13 +150,16 @@ __device__ __forceinline__ void step_pad(Walk3& w, int& idx, bool cx, bool cy, i
 #endif
 template <int U = APIRL_GATHER_UNROLL>
 __device__ __forceinline__ float siddon3_gather_pad(Walk3 w, const ImgGeom& g, int ux, int uy, int uz, unsigned lim,
-                                                    const float* __restrict__ img) {
+                                                    const float* __restrict__ img, int delay = 0) {
   const int sx = w.iinc * ux, sy = w.jinc * uy, sz = w.kinc * uz;
   int idx = (w.k + kPad) * uz + (w.j + kPad) * uy + (w.i + kPad) * ux;
   float acc = 0.f;
   if (w.guarded) {
-    int m = 0;
+    // `delay` idle iterations first (walk_delay): the segments and their sum
+    // order are unchanged.
+    int m = -(delay / U) * U;
     for (; m + U <= w.n; m += U) {
+      if (m < 0) continue;
       int ia[U];
       float sa[U], va[U];
       #pragma unroll
@@ -197,6 +200,32 @@ __device__ __forceinline__ float siddon3_gather_pad(Walk3 w, const ImgGeom& g, i
   return acc;
 }
 
+// Start delay of a walk, in crossings, that lines up the walks of a warp's
+// lanes.  The lanes of a warp walk parallel rays side by side (consecutive r
+// of one angle and sinogram), but where the rays enter the square field of
+// view through different faces, their entries lie rows apart along the main
+// axis of travel (y when |vy| > |vx|, else x), and so do their steps m: the
+// accesses of one warp step then fall in as many sectors as rows.  A lane
+// whose entry lies further along the main axis waits as many crossings as
+// separate it from the first-entering lane of its group (the lanes with the
+// same `key`): the entry's main-axis coordinate in the direction of travel
+// (mm) times the ray's crossings per mm of main-axis travel.  Capped at
+// kMaxWalkDelay.  This changes only when a lane issues its steps, never
+// which steps or in what order.  All lanes that are converged at the call
+// take part.
+constexpr int kMaxWalkDelay = 128;
+__device__ __forceinline__ int walk_delay(const Walk3& w, const ImgGeom& g, float p0x, float p0y, float vx, float vy,
+                                          float vz, unsigned key) {
+  const float ax = fabsf(vx), ay = fabsf(vy);
+  const bool xmain = ax >= ay;
+  const float entry = xmain ? (vx > 0.f ? 1.f : -1.f) * (p0x + vx * w.ac) : (vy > 0.f ? 1.f : -1.f) * (p0y + vy * w.ac);
+  const float per_mm = (ax / g.dx + ay / g.dy + fabsf(vz) / g.dz) / (xmain ? ax : ay);
+  const int k = __float2int_rn(entry * per_mm);
+  const unsigned group = __match_any_sync(__activemask(), key);
+  const int kmin = __reduce_min_sync(group, k);
+  return min(k - kmin, kMaxWalkDelay);
+}
+
 // How a scatter step adds v into img[at] (APIRL_OPT_ACCUMULATE):
 //  0  one atomic add per segment (the reference's `#pragma omp atomic` float
 //     add, SiddonProjector.cpp:547-548, in the atomics' order);
@@ -220,11 +249,15 @@ __device__ __forceinline__ void acc_add(float* __restrict__ img, float* __restri
 template <int ACC = 0>
 __device__ __forceinline__ void siddon3_scatter_pad(Walk3 w, const ImgGeom& g, int ux, int uy, int uz, unsigned lim,
                                                     float r, float* __restrict__ img,
-                                                    float* __restrict__ err = nullptr) {
+                                                    float* __restrict__ err = nullptr, int delay = 0) {
   const int sx = w.iinc * ux, sy = w.jinc * uy, sz = w.kinc * uz;
   int idx = (w.k + kPad) * uz + (w.j + kPad) * uy + (w.i + kPad) * ux;
   if (w.guarded) {
-    for (int m = 0; m < w.n; m++) {
+    // `delay` idle iterations first (walk_delay); a lane's adds go to
+    // distinct voxels, so when they are issued changes nothing but the
+    // (already unordered) interleaving with other lanes' adds.
+    for (int m = -delay; m < w.n; m++) {
+      if (m < 0) continue;
       bool cx, cy;
       const float an = next_crossing(w, cx, cy);
       acc_add<ACC>(img, err, min((unsigned)idx, lim - 1u), A_MUL(A_MUL(A_SUB(an, w.ac), w.L), r));
