@@ -926,7 +926,13 @@ apirl_status apirl_batch_create(int device, int64_t budget, apirl_batch** out) {
   const size_t want = std::min<size_t>((size_t)budget, free_b / 10 * 9);
   BK(b->pool.reserve(want & ~(size_t)((1 << 21) - 1), b->st));
   BK(apirl::multi_walk_grid(&b->walk_blocks));
-  if (!b->pinned.grow(PinnedPool::kChunk)) return bfail(APIRL_ERR_OOM, "page-locked host memory");
+  BK(apirl::load_batch_kernels());
+  // Page-locked memory for the resident jobs' results and descriptors, sized
+  // with the budget (1/64 of it, 256 MB to 2 GB) so that admitting jobs
+  // rarely has to page-lock more.
+  const size_t host_want = std::min<size_t>(std::max<size_t>((size_t)budget / 64, PinnedPool::kChunk),
+                                            (size_t)2 << 30);
+  if (!b->pinned.grow(host_want)) return bfail(APIRL_ERR_OOM, "page-locked host memory");
   BK(b->pool.alloc(&b->d_counter, 1, b->st));
   for (int k = 0; k < 2; k++) {
     BK(cudaEventCreateWithFlags(&b->step_ev[k], cudaEventDisableTiming));

@@ -210,6 +210,9 @@ inline int64_t multi_tiles(const ImgGeom& g) {
 }
 // Persistent grid of the batched walk on the current device.
 cudaError_t multi_walk_grid(int* blocks);
+// Loads the batch engine's kernels into the context (instead of at their
+// first launch).
+cudaError_t load_batch_kernels();
 // One batched step: copies and dot products, the walk over every segment's
 // list (counter reset here), the likelihood sums, the updates.
 // chunk_partials: >= total_chunks doubles; tile_partials: >= total_tiles.

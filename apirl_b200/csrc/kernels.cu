@@ -1887,6 +1887,24 @@ cudaError_t launch_fill(int64_t n, float* x, float v, cudaStream_t st) {
 
 // Persistent grid of k_em_multi: as many 256-thread blocks as fit on the
 // current device's SMs (its shared-memory carveout fitted to that many).
+cudaError_t load_batch_kernels() {
+  // CUDA loads a kernel's code at its first launch by default; asking for
+  // each kernel's attributes loads it now instead.
+  const void* fns[] = {
+      (const void*)k_em_multi,          (const void*)k_multi_copy,         (const void*)k_multi_sum,
+      (const void*)k_multi_update,      (const void*)k_scatter_angles,     (const void*)k_sum_angles,
+      (const void*)k_sum_images,        (const void*)k_subset_sums,        (const void*)k_sens_batch,
+      (const void*)k_nz_scan,           (const void*)k_nz_tiles<float>,    (const void*)k_nz_tiles<uint16_t>,
+      (const void*)k_nz_tiles<uint32_t>, (const void*)k_nz_write<float>,   (const void*)k_nz_write<uint16_t>,
+      (const void*)k_nz_write<uint32_t>};
+  for (const void* f : fns) {
+    cudaFuncAttributes a;
+    const cudaError_t e = cudaFuncGetAttributes(&a, f);
+    if (e != cudaSuccess) return e;
+  }
+  return cudaSuccess;
+}
+
 cudaError_t multi_walk_grid(int* blocks) {
   int dev = 0, sms = 0, per_sm = 0;
   cudaError_t e;
