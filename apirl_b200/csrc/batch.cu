@@ -932,7 +932,8 @@ apirl_status apirl_batch_create(int device, int64_t budget, apirl_batch** out) {
   // rarely has to page-lock more.
   const size_t host_want = std::min<size_t>(std::max<size_t>((size_t)budget / 64, PinnedPool::kChunk),
                                             (size_t)2 << 30);
-  if (!b->pinned.grow(host_want)) return bfail(APIRL_ERR_OOM, "page-locked host memory");
+  if (!b->pinned.grow(host_want) && !b->pinned.grow(PinnedPool::kChunk))
+    return bfail(APIRL_ERR_OOM, "page-locked host memory");
   BK(b->pool.alloc(&b->d_counter, 1, b->st));
   for (int k = 0; k < 2; k++) {
     BK(cudaEventCreateWithFlags(&b->step_ev[k], cudaEventDisableTiming));
