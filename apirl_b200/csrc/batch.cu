@@ -149,7 +149,10 @@ struct PinnedPool {
     Chunk c;
     c.size = std::max(kChunk, bytes);
     void* p = nullptr;
-    if (cudaMallocHost(&p, c.size) != cudaSuccess) return false;
+    if (cudaMallocHost(&p, c.size) != cudaSuccess) {
+      (void)cudaGetLastError();  // handled here: the caller reports it, or tries a smaller size
+      return false;
+    }
     c.base = (char*)p;
     c.free_at[0] = c.size;
     chunks.push_back(std::move(c));
