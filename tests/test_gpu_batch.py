@@ -157,3 +157,26 @@ def test_batch_shares_geometry_between_subset_splits():
         assert np.array_equal(np.isfinite(img), finite), j.tag
         assert rel(img[finite], solo[finite]) <= 1e-4, j.tag
         assert np.allclose(lik, solo_lik, rtol=1e-6), j.tag
+
+
+def test_job_without_counts_in_a_batch(small_jobs):
+    """Empty input in the batch: a job whose counts are all zero (every
+    subset's list of bins empty) runs beside jobs with counts, and each
+    result equals its solo run (the empty job: the same images, NaN where
+    the reference's rule divides 0 by a zero sensitivity, and likelihoods)."""
+    ig, sg = workloads.job_geometry(32, 9)
+    empty = Job(ig, sg, np.zeros(sg.n_bins, np.uint32), 2, 3, tag="no counts")
+    jobs = [small_jobs[0], empty, small_jobs[1]]
+    b = Batch(0, budget_bytes=8 << 30)
+    res = b.run_all(jobs)
+    b.close()
+    for j, (img, lik) in zip(jobs, res):
+        solo, solo_lik, _ = ap.osem_3d(j.image_geom, j.sino_geom, j.counts.astype(np.float32),
+                                       np.ones(j.image_geom.n_voxels, np.float32), j.iters, j.nsubsets)
+        assert np.array_equal(np.isnan(img), np.isnan(solo)), j.tag
+        fin = ~np.isnan(solo)
+        if j is empty:
+            assert not img[fin].any() and not solo[fin].any()
+        else:
+            assert rel(img[fin], solo[fin]) <= 1e-4, j.tag
+        assert np.allclose(lik, solo_lik, rtol=1e-6), j.tag

@@ -103,3 +103,46 @@ def test_invalid_geometries_rejected():
     for first, n in ((5, 5), (-1, 2), (0, 0)):
         with pytest.raises(ap.ApirlError):
             P.set_shard(first, n)
+
+
+@pytest.mark.parametrize("dtype", [np.uint32, np.uint16, np.float32])
+def test_listed_pass_with_no_counts(oracle, dtype):
+    """Empty input: a subset whose counts are all zero gives the listed pass
+    (geometry image) an empty list of bins.  The update equals the oracle's
+    (every ratio 0: x becomes 0 where the sensitivity passes) and the FP64
+    likelihood is -x . G_s, the reference's sum of m log e - e over e != 0
+    with m = 0 (against the FP64 sum of the oracle's float estimates, 1e-6).
+    The next subset, with counts, on the same projector (its list grows back
+    from empty) matches the oracle too."""
+    ig, sg = CASES["non_square"]
+    rng = np.random.default_rng(6)
+    x0 = (rng.random(ig.n_voxels, dtype=np.float32) + 0.5).astype(np.float32)
+    ns = 3
+    m3 = rng.poisson(oracle.project_3d(sg, ig, x0) * 2).astype(dtype).reshape(sg.n_sinos, sg.n_proj, sg.n_r)
+    m3[:, 0::ns, :] = 0  # subset 0 without counts
+    meas = m3.reshape(-1)
+    sens = (rng.random(ig.n_voxels, dtype=np.float32) + 1).astype(np.float32)
+    P = ap.SiddonProjector(ig, sg)
+    P.set_option(_lib.APIRL_OPT_SPARSE_IMAGE, _lib.APIRL_SPARSE_GEOMETRY)
+    for s in (0, 1):
+        gimg = torch.zeros(ig.n_voxels, dtype=torch.float32, device=DEV)
+        P.backproject_ones(gimg, s, ns)
+        x = t(x0)
+        bp = torch.zeros(ig.n_voxels, dtype=torch.float32, device=DEV)
+        lik = torch.zeros(1, dtype=torch.float64, device=DEV)
+        P.em_pass_sparse(t(meas), x, bp, t(sens), gimg, s, ns, lik=lik)
+        torch.cuda.synchronize()
+        m_sub = m3[:, s::ns, :].reshape(-1).astype(np.float32)
+        est = oracle.project_3d(sg, ig, x0, s, ns)
+        want_x = oracle.update(x0, oracle.backproject_3d(sg, ig, oracle.inverse_divide(m_sub, est), s, ns,
+                                                         threads=1), sens, np.float32(0), True)
+        got = x.cpu().numpy()
+        if s == 0:
+            assert not m_sub.any()
+            assert np.array_equal(got, want_x) and not got.any()
+        else:
+            assert rel(got, want_x) <= 1e-5
+        e = est.astype(np.float64)
+        nz = est != 0
+        want_lik = float(np.sum(m_sub[nz].astype(np.float64) * np.log(e[nz]) - e[nz]))
+        assert abs(lik.item() - want_lik) <= 1e-6 * abs(want_lik)
