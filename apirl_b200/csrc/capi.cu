@@ -333,6 +333,7 @@ apirl_status apirl_projector_create_3d(const apirl_image_geom* img, const apirl_
 void apirl_projector_destroy(apirl_projector* p) {
   if (!p) return;
   DeviceScope scope(p->device);
+  if (p->l2_limit_set) cudaDeviceSetLimit(cudaLimitPersistingL2CacheSize, p->l2_limit_prev);
   cudaFree(p->d_lor);
   cudaFree(p->d_z);
   cudaFree(p->d_ok);
@@ -793,6 +794,10 @@ apirl_status apirl_projector_set_option(apirl_projector* p, int option, int valu
       DEVICE_SCOPE(p->device);
       p->pad.window = 0;
       p->pad.hit_ratio = 0.f;
+      if (p->l2_limit_set) {
+        CK(cudaDeviceSetLimit(cudaLimitPersistingL2CacheSize, p->l2_limit_prev));
+        p->l2_limit_set = false;
+      }
       if (value) {
         int max_window = 0, max_persist = 0;
         CK(cudaDeviceGetAttribute(&max_window, cudaDevAttrMaxAccessPolicyWindowSize, p->device));
@@ -802,7 +807,9 @@ apirl_status apirl_projector_set_option(apirl_projector* p, int option, int valu
         const size_t aside = win < (size_t)max_persist ? win : (size_t)max_persist;
         if (win == 0 || aside == 0) return fail(APIRL_ERR_NOT_SUPPORTED, "this device has no persisting L2");
         // The set-aside is a limit of this process's context on the device.
+        CK(cudaDeviceGetLimit(&p->l2_limit_prev, cudaLimitPersistingL2CacheSize));
         CK(cudaDeviceSetLimit(cudaLimitPersistingL2CacheSize, aside));
+        p->l2_limit_set = true;
         p->pad.window = win;
         p->pad.hit_ratio = (float)((double)aside / (double)win);
       }

@@ -265,6 +265,10 @@ struct apirl_sino3d_geom;
 struct apirl_projector {
   int device = 0;
   int is3d = 0;
+  // The context's persisting-L2 limit before APIRL_OPT_L2_PERSIST raised it
+  // (put back when the option is turned off or the projector destroyed).
+  bool l2_limit_set = false;
+  size_t l2_limit_prev = 0;
   apirl::ImgGeom g{};
   apirl::HostTables host;
   float4* d_lor = nullptr;

@@ -69,6 +69,30 @@ def test_l2_window_changes_nothing(sparse):
     assert rel(got, ref) <= 1e-6 and np.allclose(lgot, lref, rtol=1e-7, atol=0)
 
 
+def _persisting_l2_limit():
+    """The context's cudaLimitPersistingL2CacheSize (enum value 6)."""
+    import ctypes
+    rt = ctypes.CDLL("libcudart.so.12")
+    v = ctypes.c_size_t(0)
+    assert rt.cudaDeviceGetLimit(ctypes.byref(v), 6) == 0
+    return v.value
+
+
+def test_l2_window_puts_the_limit_back():
+    """The option raises the context's persisting-L2 limit and puts the value
+    it found back when it is turned off and when the projector goes."""
+    ig, sg = ImageGeom(32, 32, 5, 2.08, 2.08, 2.03), Sino3DGeom.span1(16, 32, 3, 33.28, 3 * 4.054, 150.0, 2)
+    before = _persisting_l2_limit()
+    P = ap.SiddonProjector(ig, sg)
+    P.set_option(_lib.APIRL_OPT_L2_PERSIST, 1)
+    assert _persisting_l2_limit() > 0
+    P.set_option(_lib.APIRL_OPT_L2_PERSIST, 0)
+    assert _persisting_l2_limit() == before
+    P.set_option(_lib.APIRL_OPT_L2_PERSIST, 1)
+    P.close()
+    assert _persisting_l2_limit() == before
+
+
 @pytest.mark.parametrize("group", [32, 256, 2048])
 def test_list_order_changes_nothing(group):
     ref, lref = run_passes(None, 0, True)
