@@ -53,6 +53,11 @@ constexpr int kListGatherUnroll = 6;
 #define APIRL_MULTI_MIN_BLOCKS 4
 #endif
 constexpr int kMultiMinBlocks = APIRL_MULTI_MIN_BLOCKS;
+// Gather segments in flight of the batched walk.
+#ifndef APIRL_MULTI_UNROLL
+#define APIRL_MULTI_UNROLL 6
+#endif
+constexpr int kMultiGatherUnroll = APIRL_MULTI_UNROLL;
 constexpr int kEmMinBlocks = APIRL_EM_MIN_BLOCKS;
 // 1: the fused 3D pass sets the walk up a second time for the backprojection
 // (fewer live registers during the forward walk).
@@ -134,7 +139,7 @@ __device__ __forceinline__ void rays_scatter3(const ImgGeom& g, const LorTable& 
       if (!inb) return;
       float val = A_MUL(seg, v);
       if (divide) val = A_DIV(val, e);
-      atomicAdd(img + idx, val);
+      red_add_global(img + idx, val);
     });
   });
 }
@@ -242,7 +247,7 @@ __global__ void __launch_bounds__(kBlock) k_backproject3(ImgGeom g, LorTable t, 
     if (!inb) return;
     float val = A_MUL(seg, v);
     if (divide && e != 0.f) val = A_DIV(val, e);
-    atomicAdd(img + idx, val);
+    red_add_global(img + idx, val);
   };
   if (F64A) {
     const ImgGeomD gd = geom_d(pg);
@@ -281,7 +286,7 @@ __global__ void __launch_bounds__(kBlock) k_backproject2(ImgGeom g, LorTable t, 
     if (!inb) return;
     float val = A_MUL(seg, v);
     if (divide) val = A_DIV(val, e);
-    atomicAdd(img + idx, val);
+    red_add_global(img + idx, val);
   });
 }
 
@@ -361,7 +366,7 @@ __global__ void __launch_bounds__(kBlock, kEmMinBlocks) k_em_pass(ImgGeom g, Lor
       else if (lik_mode == 1 ? (e > 0.f) : (e != 0.f)) term = (double)m * log((double)e) - (double)e;
       if (back && r != 0.f)
         siddon3d_walk(w, gd, [&](bool inb, int idx, float seg) {
-          if (inb) atomicAdd(bp + idx, A_MUL(seg, r));
+          if (inb) red_add_global(bp + idx, A_MUL(seg, r));
         });
     } else if (IS3D && pad.pA) {
       // Two padded layouts: rays running mostly along x use the transposed
@@ -401,7 +406,7 @@ __global__ void __launch_bounds__(kBlock, kEmMinBlocks) k_em_pass(ImgGeom g, Lor
       else if (lik_mode == 1 ? (e > 0.f) : (e != 0.f)) term = lik_term(m, e, skip_zero);
       if (back && r != 0.f)
         siddon3_walk(w, g, [&](bool inb, int idx, float seg) {
-          if (inb) atomicAdd(bp + idx, A_MUL(seg, r));
+          if (inb) red_add_global(bp + idx, A_MUL(seg, r));
         });
     } else {
       Walk2 w;
@@ -414,7 +419,7 @@ __global__ void __launch_bounds__(kBlock, kEmMinBlocks) k_em_pass(ImgGeom g, Lor
       else if (lik_mode == 1 ? (e > 0.f) : (e != 0.f)) term = (double)m * log((double)e) - (double)e;
       if (back && ray && r != 0.f)
         siddon2_walk(w, g, [&](bool inb, int idx, float seg) {
-          if (inb) atomicAdd(bp + idx, A_MUL(seg, r));
+          if (inb) red_add_global(bp + idx, A_MUL(seg, r));
         });
     }
   }
@@ -870,7 +875,7 @@ __global__ void __launch_bounds__(kBlock) k_zero_bins(ImgGeom g, LorTable t, Sub
         siddon3_scatter_pad(w, g, tr ? py : 1, tr ? 1 : px, px * py, pad.lim, 1.f, tr ? pad.bT : pad.bA);
       } else {
         siddon3_walk(w, g, [&](bool inb, int idx, float seg) {
-          if (inb) atomicAdd(img + idx, seg);
+          if (inb) red_add_global(img + idx, seg);
         });
       }
     }
@@ -1045,7 +1050,7 @@ __global__ void __launch_bounds__(kBlock) k_sens_batch(const SensJob* __restrict
   Walk3 w;
   siddon3_setup(L.x, L.y, z.x, A_SUB(L.z, L.x), A_SUB(L.w, L.y), A_SUB(z.y, z.x), J.g, w);
   siddon3_walk(w, J.g, [&](bool inb, int idx, float seg) {
-    if (inb) atomicAdd(sens + idx, A_MUL(seg, v));
+    if (inb) red_add_global(sens + idx, A_MUL(seg, v));
   });
 }
 
@@ -1250,7 +1255,7 @@ __global__ void __launch_bounds__(kBlock, kMultiMinBlocks) k_em_multi(const Mult
       const BinPos p = decode((int64_t)__ldg(S->list + item), S->t, S->s);
       const int64_t ci = ((int64_t)p.g * S->t.n_proj + p.a) * S->t.n_r + p.l;
       const float m = load_count_any(S->counts, S->counts_dtype, ci);
-      if (m != 0.f) term = em_bin_pad<kListGatherUnroll, 0>(S->g, S->t, p, m, ci, S->add, S->pad, S->back, 2);
+      if (m != 0.f) term = em_bin_pad<kMultiGatherUnroll, 0>(S->g, S->t, p, m, ci, S->add, S->pad, S->back, 2);
     }
     #pragma unroll
     for (int o = 16; o > 0; o >>= 1) term += __shfl_down_sync(0xffffffffu, term, o);

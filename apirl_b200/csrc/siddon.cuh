@@ -233,6 +233,22 @@ __device__ __forceinline__ int walk_delay(const Walk3& w, const ImgGeom& g, floa
 //  2  compensated: the atomic returns the value it added to, so the rounding
 //     error of that addition (TwoSum, Knuth) is known exactly and goes into
 //     a second image err; img + err is the sum to about twice float precision.
+// A float add into global memory whose result nobody reads: a reduction
+// (red.global), which the SM issues without waiting for a reply.  Stated
+// explicitly because atomicAdd on a pointer the compiler cannot place (one
+// read from shared memory, as in the batched walk's per-job descriptors)
+// becomes a generic atomic instead.
+#ifndef APIRL_RED_GLOBAL
+#define APIRL_RED_GLOBAL 1
+#endif
+__device__ __forceinline__ void red_add_global(float* p, float v) {
+#if APIRL_RED_GLOBAL
+  asm volatile("red.relaxed.gpu.global.add.f32 [%0], %1;" ::"l"(__cvta_generic_to_global(p)), "f"(v) : "memory");
+#else
+  atomicAdd(p, v);
+#endif
+}
+
 template <int ACC>
 __device__ __forceinline__ void acc_add(float* __restrict__ img, float* __restrict__ err, unsigned at, float v) {
   if (ACC == 2) {
@@ -240,9 +256,9 @@ __device__ __forceinline__ void acc_add(float* __restrict__ img, float* __restri
     const float s = A_ADD(old, v);
     const float bv = A_SUB(s, old);
     const float e = A_ADD(A_SUB(old, A_SUB(s, bv)), A_SUB(v, bv));
-    if (e != 0.f) atomicAdd(err + at, e);
+    if (e != 0.f) red_add_global(err + at, e);
   } else {
-    atomicAdd(img + at, v);
+    red_add_global(img + at, v);
   }
 }
 
@@ -322,7 +338,7 @@ __device__ __forceinline__ void siddon3_scatter_pad_warp(Walk3 w, const ImgGeom&
     if (at < lim && lane == __ffs(peers) - 1) {
       float sum = 0.f;
       for (unsigned q = peers; q; q &= q - 1u) sum = A_ADD(sum, slot[warp0 + __ffs(q) - 1]);
-      atomicAdd(img + at, sum);
+      red_add_global(img + at, sum);
     }
     __syncwarp();
   }
@@ -343,8 +359,8 @@ __device__ __forceinline__ void siddon3_scatter2_pad(Walk3 w, const ImgGeom& g, 
                                    ((unsigned)w.k < (unsigned)g.nz));
     if (inb) {
       const unsigned at = min((unsigned)idx, lim - 1u);
-      if (first) atomicAdd(img1 + at, A_MUL(seg, r1));
-      atomicAdd(img2 + at, seg);
+      if (first) red_add_global(img1 + at, A_MUL(seg, r1));
+      red_add_global(img2 + at, seg);
     }
     w.ac = an;
     if (cx) { w.i += w.iinc; idx += sx; w.ax = A_ADD(w.ax, w.axu); }
