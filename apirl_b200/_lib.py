@@ -81,7 +81,8 @@ class TuneC(ctypes.Structure):
 
 class JobDescC(ctypes.Structure):
     _fields_ = [("img", ImageGeomC), ("sino", Sino3DGeomC), ("h_counts", _vp), ("counts_dtype", _i),
-                ("h_mult", _vp), ("h_add", _vp), ("h_init", _vp), ("iters", _i), ("nsubsets", _i)]
+                ("h_mult", _vp), ("h_add", _vp), ("h_init", _vp), ("iters", _i), ("nsubsets", _i),
+                ("update_positive_sens", _i)]
 
 
 # name -> (restype, argtypes)

@@ -19,8 +19,12 @@ _DT = {np.dtype(np.float32): _lib.APIRL_F32, np.dtype(np.uint32): _lib.APIRL_U32
 
 
 class Job:
-    def __init__(self, image_geom, sino_geom, counts, iters, nsubsets, mult=None, add=None, init=None, tag=None):
+    def __init__(self, image_geom, sino_geom, counts, iters, nsubsets, mult=None, add=None, init=None, tag=None,
+                 update_positive_sens=False):
+        """update_positive_sens: update only where sens > 0 (else the reference's
+        sens >= 0, which gives NaN where no ray of a subset crosses a voxel)."""
         self.image_geom, self.sino_geom = image_geom, sino_geom
+        self.update_positive_sens = bool(update_positive_sens)
         self.counts = np.ascontiguousarray(counts)
         if self.counts.dtype not in _DT:
             raise TypeError("counts must be float32, uint32 or uint16")
@@ -32,7 +36,7 @@ class Job:
         sc = _sino3d_c(self.sino_geom)
         p = lambda a: None if a is None else a.ctypes.data_as(ctypes.c_void_p)
         d = JobDescC(_img_c(self.image_geom), sc, p(self.counts), _DT[self.counts.dtype], p(self.mult), p(self.add),
-                     p(self.init), self.iters, self.nsubsets)
+                     p(self.init), self.iters, self.nsubsets, int(self.update_positive_sens))
         d._keep = (sc,)
         return d
 

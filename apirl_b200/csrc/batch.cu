@@ -253,6 +253,7 @@ struct Job {
   const float *h_mult = nullptr, *h_add = nullptr, *h_init = nullptr;
   int dtype = APIRL_F32;
   int iters = 0, nsub = 1;
+  bool positive = false;  // update where sens > 0 (else the reference's sens >= 0)
   int64_t nbins = 0, nvox = 0, footprint = 0, charged = 0;
   Stage stage = Stage::Queued;
   int pass = 0;
@@ -840,7 +841,7 @@ apirl_status launch_step(apirl_batch* b, std::vector<Job*>& jobs) {
     tiles += apirl::multi_tiles(gm.g);
     V.chunk_begin = chunks;
     V.update = fin ? 0 : 1;
-    V.ge = 1;  // OsemSinogram3d's rule: sens >= 0 (threshold 0)
+    V.ge = j.positive ? 0 : 1;  // OsemSinogram3d's rule: sens >= 0 (threshold 0), or sens > 0
     V.zero_add = 0.0;
     for (int k = fin ? 0 : sub; k < (fin ? j.nsub : sub + 1); k++) {
       MultiSeg& S = hs[si++];
@@ -1015,6 +1016,7 @@ apirl_status apirl_batch_submit(apirl_batch* b, const apirl_job_desc* d, int64_t
   j->h_mult = d->h_mult;
   j->h_add = d->h_add;
   j->h_init = d->h_init;
+  j->positive = d->update_positive_sens != 0;
   j->iters = d->iters;
   j->nsub = d->nsubsets;
   j->footprint = footprint_of(d->img, d->sino, d->counts_dtype, d->h_mult, d->h_add, d->nsubsets, j->nbins, d->iters);

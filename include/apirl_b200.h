@@ -520,6 +520,10 @@ typedef struct apirl_job_desc {
   const float* h_add;      /* additive sinogram or NULL */
   const float* h_init;     /* initial image or NULL (ones) */
   int iters, nsubsets;
+  /* 0: the reference's pixel update, sens >= 0 (OsemSinogram3d.cpp:217-237,
+   * threshold 0), which gives NaN at voxels no ray of a subset crosses; 1:
+   * update only where sens > 0 (apirl_recon_options.update_positive_sens). */
+  int update_positive_sens;
 } apirl_job_desc;
 /* Device bytes a job holds while active (its lists of bins with counts at
  * their largest, and its subset split's sensitivity images, included). */
