@@ -71,7 +71,7 @@ class SamplingC(ctypes.Structure):
 class ReconOptionsC(ctypes.Structure):
     """apirl_recon_options: rays per bin, given / returned sensitivity images."""
     _fields_ = [("sampling", ctypes.POINTER(SamplingC)), ("h_sens_in", _vp), ("h_sens_out", _vp),
-                ("update_positive_sens", _i)]
+                ("update_positive_sens", _i), ("n_sens_out", _i)]
 
 
 class TuneC(ctypes.Structure):

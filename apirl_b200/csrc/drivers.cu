@@ -402,9 +402,10 @@ apirl_status apirl_osem_3d(const apirl_image_geom* img, const apirl_sino3d_geom*
 apirl_status apirl_osem_3d_ex(const apirl_image_geom* img, const apirl_sino3d_geom* sino, const float* h_meas,
                               const float* h_mult, const float* h_add, const float* h_init, int iters, int nsubsets,
                               int device, float* h_out, double* h_lik, const apirl_recon_options* opts) {
-  const apirl_recon_options o = opts ? *opts : apirl_recon_options{nullptr, nullptr, nullptr, 0};
+  const apirl_recon_options o = opts ? *opts : apirl_recon_options{nullptr, nullptr, nullptr, 0, 0};
+  const int n_out = o.n_sens_out > 0 && o.n_sens_out < nsubsets ? o.n_sens_out : nsubsets;
   return osem_3d(img, sino, h_meas, h_mult, h_add, h_init, iters, nsubsets, device, h_out, h_lik, o.h_sens_in,
-                 o.h_sens_out, nsubsets, o.sampling, o.update_positive_sens);
+                 o.h_sens_out, n_out, o.sampling, o.update_positive_sens);
 }
 
 apirl_status apirl_mlem_3d(const apirl_image_geom* img, const apirl_sino3d_geom* sino, const float* h_meas,
@@ -416,7 +417,7 @@ apirl_status apirl_mlem_3d(const apirl_image_geom* img, const apirl_sino3d_geom*
 apirl_status apirl_mlem_3d_ex(const apirl_image_geom* img, const apirl_sino3d_geom* sino, const float* h_meas,
                               const float* h_mult, const float* h_add, const float* h_init, int iters, int device,
                               float* h_out, double* h_lik, const apirl_recon_options* opts) {
-  const apirl_recon_options o = opts ? *opts : apirl_recon_options{nullptr, nullptr, nullptr, 0};
+  const apirl_recon_options o = opts ? *opts : apirl_recon_options{nullptr, nullptr, nullptr, 0, 0};
   return mlem_3d(img, sino, h_meas, h_mult, h_add, h_init, iters, device, h_out, h_lik, o.h_sens_in, o.h_sens_out,
                  o.sampling);
 }
@@ -430,7 +431,7 @@ apirl_status apirl_mlem_2d(const apirl_image_geom* img, const apirl_sino2d_geom*
 apirl_status apirl_mlem_2d_ex(const apirl_image_geom* img, const apirl_sino2d_geom* sino, const float* h_meas,
                               const float* h_mult, const float* h_add, const float* h_init, int iters, int device,
                               float* h_out, double* h_lik, const apirl_recon_options* opts) {
-  const apirl_recon_options o = opts ? *opts : apirl_recon_options{nullptr, nullptr, nullptr, 0};
+  const apirl_recon_options o = opts ? *opts : apirl_recon_options{nullptr, nullptr, nullptr, 0, 0};
   if (o.sampling) return set_err(APIRL_ERR_NOT_SUPPORTED, "2D reconstructions walk one ray per bin", cudaSuccess);
   return mlem_2d(img, sino, h_meas, h_mult, h_add, h_init, iters, device, h_out, h_lik, o.h_sens_in, o.h_sens_out);
 }

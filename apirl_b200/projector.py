@@ -334,7 +334,7 @@ def _sampling_c(sampling):
     return ctypes.byref(_lib.SamplingC(int(ns), int(nas), int(bool(multi))))
 
 
-def _recon_opts(sampling, sens_in, sens_out, update_positive_sens=False):
+def _recon_opts(sampling, sens_in, sens_out, update_positive_sens=False, n_sens_out=0):
     """apirl_recon_options; the ctypes objects are returned with it so they stay alive."""
     smp = None
     if sampling is not None:
@@ -343,7 +343,7 @@ def _recon_opts(sampling, sens_in, sens_out, update_positive_sens=False):
     o = _lib.ReconOptionsC(ctypes.pointer(smp) if smp is not None else None,
                            _np_ptr(sens_in) if sens_in is not None else None,
                            _np_ptr(sens_out) if sens_out is not None else None,
-                           int(bool(update_positive_sens)))
+                           int(bool(update_positive_sens)), int(n_sens_out))
     return o, smp
 
 
@@ -370,8 +370,9 @@ def osem_3d(image_geom, sino_geom, meas, init, iters, nsubsets, mult=None, add=N
     sens_in = None if sens is None else np.ascontiguousarray(sens, np.float32).reshape(-1)
     if sens_in is not None and sens_in.size != nsubsets * nv:
         raise ValueError("sens must hold nsubsets images")
-    sens_out = np.zeros((nsubsets, nv), np.float32)
-    opts, _keep = _recon_opts(sampling, sens_in, sens_out, update_positive_sens)
+    # all subsets' sensitivity images back only when asked for (a C2-size job's are 446 MB)
+    sens_out = np.zeros((nsubsets if all_sens else 1, nv), np.float32)
+    opts, _keep = _recon_opts(sampling, sens_in, sens_out, update_positive_sens, 0 if all_sens else 1)
     check(lib.apirl_osem_3d_ex(ctypes.byref(ig), ctypes.byref(sc), _np_ptr(meas), _np_ptr(mult), _np_ptr(add),
                                _np_ptr(init), iters, nsubsets, device, _np_ptr(out), _np_ptr(lik), ctypes.byref(opts)))
     return out, lik, (sens_out if all_sens else sens_out[0].copy())

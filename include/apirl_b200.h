@@ -484,6 +484,9 @@ typedef struct {
    * 1: update where sens > 0, else 0 (those voxels become 0).  Read by
    * apirl_osem_3d_ex only. */
   int update_positive_sens;
+  /* Sensitivity images h_sens_out receives: 0 = all of them, n > 0 = the
+   * first n subsets' (OSEM). */
+  int n_sens_out;
 } apirl_recon_options;
 apirl_status apirl_osem_3d_ex(const apirl_image_geom* img, const apirl_sino3d_geom* sino, const float* h_meas,
                               const float* h_mult, const float* h_add, const float* h_init, int iters, int nsubsets,

@@ -208,3 +208,20 @@ def test_update_rule_positive_sens(small_jobs):
             assert np.isfinite(img).all()
             assert rel(img, solo) <= 1e-4
             assert np.allclose(lik, solo_lik, rtol=1e-6)
+
+
+def test_sensitivity_images_returned_as_asked(small_jobs):
+    """apirl_recon_options.n_sens_out: the driver writes the first n subsets'
+    sensitivity images (osem_3d asks for subset 0's alone unless all_sens),
+    the same images as when all are returned, and the same reconstruction
+    (two runs: equal up to the order of the fp32 atomic adds)."""
+    j = small_jobs[3]
+    c = j.counts.astype(np.float32)
+    x0 = np.ones(j.image_geom.n_voxels, np.float32)
+    img1, lik1, s0 = ap.osem_3d(j.image_geom, j.sino_geom, c, x0, j.iters, j.nsubsets, update_positive_sens=True)
+    img2, lik2, sall = ap.osem_3d(j.image_geom, j.sino_geom, c, x0, j.iters, j.nsubsets, update_positive_sens=True,
+                                  all_sens=True)
+    assert sall.shape == (j.nsubsets, j.image_geom.n_voxels)
+    assert s0.shape == sall[0].shape and s0.any()
+    assert rel(s0, sall[0]) <= 1e-6
+    assert rel(img1, img2) <= 1e-6 and np.allclose(lik1, lik2, rtol=1e-7)
