@@ -921,6 +921,39 @@ def run_mlem2d(args):
                       "cpu_baseline": cpu}), flush=True)
 
 
+def run_batched_c2(args):
+    """--workload batched-c2: the 3D OSEM job of the default line (or its
+    --max-ring-diff profiling case), 1 iteration x 21 subsets, as the only job
+    of a batch, for comparing the batched walk with the single-job kernel on
+    the same counts (profiler captures).  Prints the batch's wall time."""
+    import torch
+    import apirl_b200 as ap
+    from apirl_b200 import workloads
+    from apirl_b200.batch import Batch, Job
+    from apirl_b200.geometry import Sino3DGeom
+    dev = torch.device("cuda:0")
+    ap.load_library()
+    ig, sg = workloads.c2_geometry()
+    if args.max_ring_diff is not None and args.max_ring_diff < 20:
+        sg = Sino3DGeom.span1(sg.n_proj, sg.n_r, sg.n_rings, sg.r_fov, sg.axial_fov, sg.r_scanner, args.max_ring_diff)
+    P = ap.SiddonProjector(ig, sg, device=dev.index)
+    _, counts = workloads.c2_device_arrays(P, dev)
+    h = counts.view(torch.int32).cpu().numpy().view(np.uint32)
+    P.close()
+    del counts
+    torch.cuda.synchronize(dev)
+    b = Batch(0, budget_bytes=int(args.budget_gb * (1 << 30)))
+    t0 = time.perf_counter()
+    b.run_all([Job(ig, sg, h, 1, NSUB, update_positive_sens=True)])
+    sec = time.perf_counter() - t0
+    b.close()
+    print(json.dumps({"metric": "batch of one 3D OSEM job (1 iteration x 21 subsets)", "value": sec, "unit": "s",
+                      "n_gpus": 1, "higher_is_better": False,
+                      "config": {"workload": WORKLOAD if args.max_ring_diff is None else
+                                 WORKLOAD + f" (profiling case: segments |rd| <= {args.max_ring_diff} only)"}}),
+          flush=True)
+
+
 def run_batched(args, served=False):
     log = lambda m: print(f"[bench] {m}", file=sys.stderr, flush=True)
     r = mixed_jobs(args, served, log)
@@ -1121,7 +1154,8 @@ def main():
                      help="how the backprojection scatter accumulates (APIRL_OPT_ACCUMULATE)")
     ap_.add_argument("--cpu-threads", type=int, default=None,
                      help="host threads of the CPU baseline / reference arm (default: all)")
-    ap_.add_argument("--workload", default="osem3d", choices=["osem3d", "batched", "served", "mlem2d", "precision"])
+    ap_.add_argument("--workload", default="osem3d",
+                     choices=["osem3d", "batched", "served", "mlem2d", "precision", "batched-c2"])
     ap_.add_argument("--precision-subiters", type=int, default=4,
                      help="precision workload: sub-iterations compared with the FP64 oracle")
     ap_.add_argument("--max-ring-diff", type=int, default=None,
@@ -1147,6 +1181,8 @@ def main():
         run_precision(args)
     elif args.workload in ("batched", "served"):
         run_batched(args, served=args.workload == "served")
+    elif args.workload == "batched-c2":
+        run_batched_c2(args)
     else:
         run_gpu(args)
 
