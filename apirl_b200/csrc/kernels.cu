@@ -554,16 +554,49 @@ __device__ __forceinline__ bool bin_has_count(int64_t b64, const LorTable& t, co
   return load_count<CT>(counts, row * t.n_r + l) != 0.f;
 }
 
+// Whether each of a thread's kNzTile / kNzBlock bins of its tile (bins
+// base + threadIdx.x + kNzBlock * i) has counts.  The first bin is decoded
+// once and the others by stepping (r, then subset angle, then sinogram)
+// without dividing, and every count is loaded before any is tested, so that
+// the thread's loads are in flight together.
+constexpr int kNzPerThread = kNzTile / kNzBlock;
+template <typename CT>
+__device__ __forceinline__ void tile_has_counts(int64_t base, int64_t total, const LorTable& t, const SubsetSel& s,
+                                                const CT* __restrict__ counts, int counts_packed,
+                                                bool (&has)[kNzPerThread]) {
+  const int per = s.nk * t.n_r;
+  const int b0 = (int)base + (int)threadIdx.x;
+  int gl = b0 / per;
+  int rem = b0 - gl * per;
+  int k = rem / t.n_r;
+  int l = rem - k * t.n_r;
+  float m[kNzPerThread];
+  #pragma unroll
+  for (int i = 0; i < kNzPerThread; i++) {
+    const bool in = base + threadIdx.x + (int64_t)kNzBlock * i < total;
+    const int a = s.subset < 0 ? k : s.subset + s.nsub * k;
+    const int64_t row = counts_packed ? ((int64_t)gl * s.nk + k) : ((int64_t)(t.g0 + gl) * t.n_proj + a);
+    m[i] = in ? load_count<CT>(counts, row * t.n_r + l) : 0.f;
+    l += kNzBlock;
+    while (l >= t.n_r) {
+      l -= t.n_r;
+      if (++k == s.nk) { k = 0; ++gl; }
+    }
+  }
+  #pragma unroll
+  for (int i = 0; i < kNzPerThread; i++) has[i] = m[i] != 0.f;
+}
+
 template <typename CT>
 __global__ void __launch_bounds__(kNzBlock) k_nz_tiles(LorTable t, SubsetSel s, const CT* __restrict__ counts,
                                                        int counts_packed, int64_t total, int* __restrict__ tiles) {
   __shared__ int warp_n[kNzBlock / 32];
   const int64_t base = (int64_t)blockIdx.x * kNzTile;
+  bool has[kNzPerThread];
+  tile_has_counts<CT>(base, total, t, s, counts, counts_packed, has);
   int n = 0;
-  for (int i = threadIdx.x; i < kNzTile; i += kNzBlock) {
-    const int64_t b = base + i;
-    n += (b < total && bin_has_count<CT>(b, t, s, counts, counts_packed)) ? 1 : 0;
-  }
+  #pragma unroll
+  for (int i = 0; i < kNzPerThread; i++) n += has[i] ? 1 : 0;
   #pragma unroll
   for (int o = 16; o > 0; o >>= 1) n += __shfl_down_sync(0xffffffffu, n, o);
   if ((threadIdx.x & 31) == 0) warp_n[threadIdx.x >> 5] = n;
@@ -616,29 +649,35 @@ template <typename CT>
 __global__ void __launch_bounds__(kNzBlock) k_nz_write(LorTable t, SubsetSel s, const CT* __restrict__ counts,
                                                        int counts_packed, int64_t total,
                                                        const int* __restrict__ tiles, int* __restrict__ list) {
-  __shared__ int warp_n[kNzBlock / 32];
-  __shared__ int run;
+  // Entries go to the list in bin order: sub-tile q (bins base + kNzBlock q
+  // + thread), then warp, then lane.  cnt[q][w]: warp w's entries in sub-tile
+  // q, turned into the tile-relative offset of that group in one pass.
+  __shared__ int cnt[kNzPerThread][kNzBlock / 32];
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  if (threadIdx.x == 0) run = tiles[blockIdx.x];
-  __syncthreads();
   const int64_t base = (int64_t)blockIdx.x * kNzTile;
-  for (int i = 0; i < kNzTile; i += kNzBlock) {
-    const int64_t b = base + i + threadIdx.x;
-    const bool has = b < total && bin_has_count<CT>(b, t, s, counts, counts_packed);
-    const unsigned mask = __ballot_sync(0xffffffffu, has);
-    if (lane == 0) warp_n[warp] = __popc(mask);
-    __syncthreads();
-    int off = run;
-    for (int w = 0; w < warp; w++) off += warp_n[w];
-    if (has) list[off + __popc(mask & ((1u << lane) - 1u))] = (int)b;
-    __syncthreads();
-    if (threadIdx.x == 0) {
-      int sum = 0;
-      for (int w = 0; w < kNzBlock / 32; w++) sum += warp_n[w];
-      run += sum;
-    }
-    __syncthreads();
+  bool hs[kNzPerThread];
+  tile_has_counts<CT>(base, total, t, s, counts, counts_packed, hs);
+  unsigned mask[kNzPerThread];
+  #pragma unroll
+  for (int q = 0; q < kNzPerThread; q++) {
+    mask[q] = __ballot_sync(0xffffffffu, hs[q]);
+    if (lane == 0) cnt[q][warp] = __popc(mask[q]);
   }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    int run = tiles[blockIdx.x];
+    for (int q = 0; q < kNzPerThread; q++)
+      for (int w = 0; w < kNzBlock / 32; w++) {
+        const int c = cnt[q][w];
+        cnt[q][w] = run;
+        run += c;
+      }
+  }
+  __syncthreads();
+  const unsigned below = (1u << lane) - 1u;
+  #pragma unroll
+  for (int q = 0; q < kNzPerThread; q++)
+    if (hs[q]) list[cnt[q][warp] + __popc(mask[q] & below)] = (int)(base + (int64_t)kNzBlock * q + threadIdx.x);
 }
 
 // One bin of the padded-layout fused pass: forward walk over the padded copy
