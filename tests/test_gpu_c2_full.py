@@ -23,6 +23,8 @@ sensitivity; 5e8 Poisson counts as uint32).
 * The whole job: 3 iterations x 21 subsets through apirl_osem_3d (sensitivity
   A_s^T a, update where sens > 0) against the oracle's OSEM with the same
   rule: rel L2 <= 1e-4.
+* The batch engine on the same job (1 iteration x 21 subsets) against
+  apirl_osem_3d: rel L2 <= 1e-4, likelihoods to 1e-6.
 
 Marked slow: the oracle runs on the host cores (about a minute for the
 sub-iterations, a few minutes for the whole job on 16 threads).
@@ -141,6 +143,24 @@ def test_whole_job_matches_oracle(oracle, c2):
     # in the oracle (the reference's accumulator), whose rounding reaches
     # ~1e-4: they are checked per pass against an FP64 sum above
     assert np.all(np.isfinite(lik))
+
+
+def test_full_size_job_in_a_batch(c2):
+    """The batch engine at full size: the job with its attenuation factors
+    (the batch walks its own sensitivity A_s^T a) as the only job of a batch,
+    1 iteration x 21 subsets, update where sens > 0, against the same job
+    through apirl_osem_3d: image rel L2 <= 1e-4 (the order of the fp32 atomic
+    adds), likelihoods to 1e-6."""
+    from apirl_b200.batch import Batch, Job
+    ig, sg = c2["ig"], c2["sg"]
+    b = Batch(0, budget_bytes=32 << 30)
+    (img, lik), = b.run_all([Job(ig, sg, c2["counts_np"], 1, NSUB, mult=c2["atten_np"], update_positive_sens=True)])
+    b.close()
+    solo, solo_lik, _ = ap.osem_3d(ig, sg, c2["counts_np"].astype(np.float32), np.ones(ig.n_voxels, np.float32), 1,
+                                   NSUB, mult=c2["atten_np"], update_positive_sens=True)
+    assert np.all(np.isfinite(img)) and np.all(np.isfinite(solo))
+    assert rel(img, solo) <= 1e-4, f"batch vs driver rel L2 {rel(img, solo):.3e}"
+    assert np.allclose(lik, solo_lik, rtol=1e-6, atol=0)
 
 
 def test_precision_first_subiteration():
